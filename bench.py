@@ -1,0 +1,368 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 force path on the 1,000,000-atom primitive-model electrolyte.
+
+Workload (one GPU): 1,000,000 atoms (10 % +/-1 ions, neutral LJ solvent, rho = 0.8 sigma^-3,
+L = 107.72 sigma), LJ cutoff 2.5, real-space alpha with erfc(sqrt(alpha) rc) <= 1e-5, plain
+Gaussian RBE with P = 500 k-samples per step, FP32 forces with compensated accumulation, FP64
+velocity-Verlet + Berendsen.  A "step" is one full MD step (kick, drift, cell sort, neighbour
+list, RBE structure factors, near + k-space force, kick, temperature, thermostat).
+
+Metric: atom-steps/s (higher is better).  With --gpus N (torchrun, one process per GPU) every
+rank advances its own independent replica of the workload ("replicas only", weak scaling; no
+data-path collective); value = total atom-steps / max-over-ranks device time.
+
+--impl reference times the reference path's CPU implementation (the oracle restatement of the
+reference's FP32 force path; the reference itself cannot be built here) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "atom-steps/s at equal force RMSE vs FP64 Ewald: learned vs plain RBE"
+N_ATOMS = 1_000_000
+P_PLAIN = 500
+CPU_SAMPLE_ATOMS = 100_000
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--atoms", type=int, default=N_ATOMS)
+    ap.add_argument("--P", type=int, default=P_PLAIN)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    return ap.parse_args()
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for k, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(k)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+# algorithmic bytes / operations per atom of each phase (DESIGN.md lists the derivation)
+def algorithmic(n_nbr_mean, P):
+    return {
+        # neighbour list: read own pos4 + cell ranges, write n entries (4 B) + count
+        "neighbor_list": {"bytes": 16 + 4 * n_nbr_mean + 4 + 8},
+        # near + fused RBE force: list (4 B/nbr), own pos4 + frac + meta + slot id + count,
+        # force write (24 B); unique neighbour positions are read once (the own pos4 term)
+        "force": {"bytes": 4 * n_nbr_mean + 16 + 16 + 8 + 4 + 4 + 24, "sincos": P},
+        # structure factors: frac (16 B) once per k tile (L2), P sincos
+        "kspace": {"bytes": 16, "sincos": P},
+        "cell_sort": {"bytes": 24 + 4 + 4 + 4 + 4 + 16 + 16 + 8 + 8 + 8},
+        "integrate": {"bytes": 24 * 4 + 8 + 4 + 4 + 24 * 2},
+    }
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from copy_gpu_b200 import Box, ForceField, systems
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    s = systems.electrolyte(args.atoms, seed=3 + rank)
+    cfg = systems.electrolyte_config(P=args.P, precision="fp32", seed=7 + rank)
+    n = s["pos"].shape[0]
+    t = {k: torch.tensor(s[k], device=dev, dtype=torch.float64).contiguous()
+         for k in ("pos", "vel", "mass", "charge")}
+    t["type"] = torch.tensor(s["type"], device=dev, dtype=torch.int32)
+    t["force"] = torch.zeros((n, 3), device=dev, dtype=torch.float64)
+    t["image"] = torch.zeros((n, 3), device=dev, dtype=torch.int32)
+    ff = ForceField(cfg, Box(tuple(s["lo"]), tuple(s["hi"])))
+    ff.set_pair_coeffs(s["eps"], s["sigma"])
+    ff.Init(t["pos"], t["force"], vel=t["vel"], mass=t["mass"], charge=t["charge"], type=t["type"],
+            image=t["image"])
+    stream = torch.cuda.current_stream(dev)
+    ff.Execute()                                   # initial force (ExecutionNVT::Init)
+    ff.step(args.warmup)
+    torch.cuda.synchronize(dev)
+    k_per_step = ff.launches_per_step()
+    clocks = Clocks(local)
+    ff.profile(True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ff.step(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    phases = ff.phase_ms()
+    ff.profile(False)
+    flags = ff.status()
+    if world > 1:
+        m = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(m, op=dist.ReduceOp.MAX)
+        ms = float(m.item())
+    value = world * n * args.steps / (ms / 1e3)
+
+    # mean neighbour count (for the algorithmic byte counts)
+    ff.Execute()
+    cnt, _ = ff.neighbors(0)
+    n_nbr = float(cnt.mean())
+
+    # end-to-end through the host-buffer C-ABI call: pinned positions in, pinned forces out
+    pos_h = torch.empty((n, 3), dtype=torch.float64, pin_memory=True)
+    pos_h.copy_(t["pos"].cpu())
+    frc_h = torch.empty((n, 3), dtype=torch.float64, pin_memory=True)
+    ph = pos_h.numpy()
+    fh = frc_h.numpy()
+    ff.compute_host(ph, fh, stream=stream.cuda_stream)
+    torch.cuda.synchronize(dev)
+    w0 = time.perf_counter()
+    a0 = torch.cuda.Event(enable_timing=True)
+    a1 = torch.cuda.Event(enable_timing=True)
+    a0.record(stream)
+    for _ in range(args.e2e_steps):
+        ff.compute_host(ph, fh, stream=stream.cuda_stream)
+    a1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = max(a0.elapsed_time(a1), (time.perf_counter() - w0) * 1e3) / args.e2e_steps
+    if world > 1:
+        m = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(m, op=dist.ReduceOp.MAX)
+        e2e_ms = float(m.item())
+    e2e_value = world * n / (e2e_ms / 1e3)
+
+    out = None
+    if rank == 0:
+        peaks, src = measured_peaks()
+        alg = algorithmic(n_nbr, args.P)
+        # dominant phase by device time
+        per = {k: v[0] for k, v in phases.items() if v[1] > 0}
+        dom = max(per, key=per.get)
+        launches = {k: phases[k][1] for k in phases}
+        sm_mhz = clk["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0)
+        n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
+        mufu_peak = 16 * n_sm * sm_mhz * 1e6 / 2.0 / 1e9        # G sincos/s (2 MUFU ops each)
+        rl = {}
+        for k in ("force", "kspace", "neighbor_list", "cell_sort", "integrate"):
+            if k not in per or launches[k] == 0:
+                continue
+            dur = per[k] / 1e3 / args.steps                      # s per step
+            a = alg[k]
+            ent = {"ms_per_step": per[k] / args.steps}
+            ent["hbm_gbs"] = a["bytes"] * n / dur / 1e9
+            ent["hbm_frac"] = ent["hbm_gbs"] / peaks["hbm_gbs"]
+            if "sincos" in a:
+                ent["gsincos_s"] = a["sincos"] * n / dur / 1e9
+                ent["mufu_frac"] = ent["gsincos_s"] / mufu_peak
+            rl[k] = ent
+        d = rl[dom]
+        if "mufu_frac" in d and d["mufu_frac"] > d["hbm_frac"]:
+            roof = {"bound": "mufu", "achieved": d["gsincos_s"], "peak": mufu_peak, "unit": "Gsincos/s",
+                    "frac": d["mufu_frac"], "kernel": dom,
+                    "peak_source": f"16 MUFU ops/clk/SM x {n_sm} SMs x median loaded {sm_mhz:.0f} MHz / 2",
+                    "traffic": None}
+        else:
+            roof = {"bound": "hbm", "achieved": d["hbm_gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                    "frac": d["hbm_frac"], "kernel": dom, "peak_source": f"{src} hbm_gbs", "traffic": None}
+        tr_path = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tr_path):
+            with open(tr_path) as fh:
+                trd = json.load(fh)
+            if dom in trd:
+                roof["traffic"] = trd[dom]
+        out = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "atom-steps/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"electrolyte {n} atoms, plain Gaussian RBE P={args.P}, full MD step",
+                       "atoms_per_gpu": n, "P": args.P, "proposal": "gauss", "rc": 2.5,
+                       "alpha": cfg["hyper_parameters"]["coulomb"]["alpha"], "box": float(s["hi"][0]),
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (neighbour list %.0f MB + state %.0f MB)"
+                             % (4 * n_nbr * n / 1e6, 72 * n / 1e6)},
+            "roofline": roof,
+            "phases": rl,
+            "e2e": {"value": e2e_value, "unit": "atom-steps/s", "h2d_bytes_per_step": 24 * n,
+                    "d2h_bytes_per_step": 24 * n,
+                    "what": "rbmd_force_compute_host: pinned host positions in, forces out, one force evaluation per step"},
+            "gpu_launches": k_per_step * args.steps,
+            "kernels_per_step": k_per_step,
+            "status_flags": flags,
+            "clocks": clk,
+            "mean_neighbors": n_nbr,
+        }
+        if not args.no_cpu and world == 1:
+            out["cpu_baseline"] = cpu_baseline(args.P)
+    ff.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return out
+
+
+def cpu_force_eval(n_atoms, P, seed=3):
+    """One force evaluation of the reference path's CPU restatement (FP32 semantics):
+    neighbour list, LJ + erfc near force, RBE structure factors and force.  Returns seconds."""
+    import oracle
+    from copy_gpu_b200 import systems
+    s = systems.electrolyte(n_atoms, seed=seed)
+    cfg = systems.electrolyte_config(P=P)
+    alpha = cfg["hyper_parameters"]["coulomb"]["alpha"]
+    L = s["hi"] - s["lo"]
+    m = oracle.rbe_sample(alpha, L, 7, 0, 0, P)
+    pos32 = s["pos"].astype(np.float32)
+    t0 = time.perf_counter()
+    nl = oracle.neighbors(pos32, s["lo"], s["hi"], 2.5, "fp32")
+    oracle.near_force(pos32, s["lo"], s["hi"], 2.5, nl, type=s["type"], charge=s["charge"], eps=s["eps"],
+                      sigma=s["sigma"], with_coul=True, alpha=alpha, sum_mode=0, prec="fp32")
+    rho = oracle.rhok(pos32, s["charge"], L, m, prec="fp32")
+    oracle.rbe_force(pos32, s["charge"], L, alpha, 1.0, m, rho, prec="fp32")
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(P):
+    import oracle
+    oracle.build()
+    cores = os.cpu_count() or 1
+    oracle.set_threads(cores)
+    sec = cpu_force_eval(CPU_SAMPLE_ATOMS, P)
+    return {"value": CPU_SAMPLE_ATOMS / sec, "unit": "atom-steps/s", "cores": cores, "kind": "port",
+            "sample": f"one force evaluation (list + LJ/erfc near + RBE P={P}) of a {CPU_SAMPLE_ATOMS}-atom "
+                      f"electrolyte of the same composition and density, FP32 oracle, {cores} OpenMP threads, "
+                      f"{sec:.2f} s"}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    import oracle
+    oracle.build()
+    cores = os.cpu_count() or 1
+    oracle.set_threads(cores)
+    n = CPU_SAMPLE_ATOMS
+    for _ in range(max(args.warmup, 0) and 1):
+        cpu_force_eval(n, args.P)
+    times = [cpu_force_eval(n, args.P, seed=3) for _ in range(args.steps)]
+    tot = sum(times)
+    value = n * args.steps / tot
+    return {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": "atom-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": tot / args.steps * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"electrolyte {args.atoms} atoms, plain Gaussian RBE P={args.P}, full MD step",
+                   "sample_atoms": n, "P": args.P},
+        "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": cores, "kind": "port",
+                         "sample": f"per step one force evaluation of a {n}-atom sample of the workload "
+                                   f"(same composition and density), FP32 oracle restatement of the "
+                                   f"reference path, {cores} OpenMP threads"},
+        "e2e": {"value": value, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    out = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

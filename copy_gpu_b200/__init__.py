@@ -1,0 +1,343 @@
+"""copy_gpu_b200 -- RBMD's per-timestep force path on B200 (sm_100a), behind a C ABI.
+
+The compute lives in ``librbmd_b200.so`` (CUDA kernels + C++ host driver, declared in
+``include/rbmd_force.h``).  This module is the thin Python host mirror of the reference's
+force-field interface: :class:`ForceField` is configured from RBMD's JSON text and exposes
+``Init`` / ``Execute`` like the HIP tree's ``class Force``
+(rbmd-gpu-clone/rbmd-gpu/src/force/include/force.h:8-25) plus the full step of
+``ExecutionNVT::Solve`` (rbmd/framework/run/ExecutionNVT.cpp:133-159).
+
+There is no CPU fallback: importing works without a GPU (for building and symbol checks), but
+every compute call requires the CUDA library and a device and raises otherwise.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+from dataclasses import dataclass
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "librbmd_b200.so")
+
+RBMD_OK = 0
+STATUS_NAMES = {1: "ERR_ARG", 2: "ERR_CONFIG", 3: "ERR_CUDA", 4: "ERR_STATE", 5: "ERR_DEVICE",
+                6: "ERR_FILE"}
+FLAG_LIST_OVERFLOW = 0x01
+FLAG_CELL_OVERFLOW = 0x02
+FLAG_SHAKE_NOCONV = 0x04
+FLAG_NONFINITE = 0x08
+FLAG_OUT_OF_BOX = 0x10
+FLAG_SAMPLER = 0x20
+FLAG_SHAKE_SINGULAR = 0x40
+
+# every symbol include/rbmd_force.h declares
+EXPORTED = [
+    "rbmd_force_create", "rbmd_force_set_pair_coeffs", "rbmd_force_load_funcfl",
+    "rbmd_force_set_water", "rbmd_force_bind", "rbmd_force_set_ksamples",
+    "rbmd_force_set_kweights", "rbmd_force_get_ksamples", "rbmd_force_sample_k",
+    "rbmd_force_compute", "rbmd_force_compute_host", "rbmd_force_step",
+    "rbmd_force_sync_velocities", "rbmd_force_energy", "rbmd_force_status",
+    "rbmd_force_get_neighbors", "rbmd_force_get_rhok", "rbmd_force_profile",
+    "rbmd_force_phase_ms", "rbmd_force_launch_count",
+    "rbmd_force_destroy", "rbmd_version", "rbmd_last_error",
+]
+
+
+class RbmdError(RuntimeError):
+    pass
+
+
+class rbmd_box(ctypes.Structure):
+    _fields_ = [("lo", ctypes.c_double * 3), ("hi", ctypes.c_double * 3)]
+
+
+class rbmd_atoms_dev(ctypes.Structure):
+    _fields_ = [
+        ("n_atoms", ctypes.c_int64),
+        ("n_replicas", ctypes.c_int32),
+        ("replica_offsets", ctypes.POINTER(ctypes.c_int64)),
+        ("pos", ctypes.c_void_p),
+        ("vel", ctypes.c_void_p),
+        ("force", ctypes.c_void_p),
+        ("mass", ctypes.c_void_p),
+        ("charge", ctypes.c_void_p),
+        ("type", ctypes.c_void_p),
+        ("molecule", ctypes.c_void_p),
+        ("image", ctypes.c_void_p),
+    ]
+
+
+class rbmd_energy(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in (
+        "lj", "coul_real", "coul_kspace", "coul_self", "eam_embed", "eam_pair", "bond", "angle",
+        "kinetic", "temperature")]
+
+
+_lib = None
+
+
+def library() -> ctypes.CDLL:
+    """Load the CUDA force library (raises when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RbmdError(f"{LIB_PATH} is missing: run `python -m copy_gpu_b200.build`")
+    lib = ctypes.CDLL(LIB_PATH)
+    P, I32, I64, D, V = ctypes.POINTER, ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
+    sig = {
+        "rbmd_force_create": (I32, [ctypes.c_char_p, I32, P(rbmd_box), P(V)]),
+        "rbmd_force_set_pair_coeffs": (I32, [V, I32, P(D), P(D)]),
+        "rbmd_force_load_funcfl": (I32, [V, ctypes.c_char_p]),
+        "rbmd_force_set_water": (I32, [V, I64, P(I32), D, D, D, D]),
+        "rbmd_force_bind": (I32, [V, P(rbmd_atoms_dev)]),
+        "rbmd_force_set_ksamples": (I32, [V, P(I32), I32]),
+        "rbmd_force_set_kweights": (I32, [V, P(D)]),
+        "rbmd_force_get_ksamples": (I32, [V, P(I32), I32]),
+        "rbmd_force_sample_k": (I32, [V, I64, P(I32), I32]),
+        "rbmd_force_compute": (I32, [V, V]),
+        "rbmd_force_compute_host": (I32, [V, P(D), P(D), V]),
+        "rbmd_force_step": (I32, [V, I32, V]),
+        "rbmd_force_sync_velocities": (I32, [V, V]),
+        "rbmd_force_energy": (I32, [V, P(rbmd_energy), V]),
+        "rbmd_force_status": (I32, [V, P(ctypes.c_uint32), I32, V]),
+        "rbmd_force_get_neighbors": (I32, [V, P(I32), P(I32), I64]),
+        "rbmd_force_get_rhok": (I32, [V, P(D), I32]),
+        "rbmd_force_profile": (I32, [V, I32]),
+        "rbmd_force_phase_ms": (I32, [V, P(D), P(I64), I32]),
+        "rbmd_force_launch_count": (I32, [V, P(I32)]),
+        "rbmd_force_destroy": (None, [V]),
+        "rbmd_version": (ctypes.c_char_p, []),
+        "rbmd_last_error": (ctypes.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(st: int, what: str) -> None:
+    if st != RBMD_OK:
+        msg = library().rbmd_last_error().decode(errors="replace")
+        raise RbmdError(f"{what} failed: {STATUS_NAMES.get(st, st)} {msg}")
+
+
+def _ptr(t, ctype):
+    import numpy as np
+    if isinstance(t, np.ndarray):
+        return t.ctypes.data_as(ctypes.POINTER(ctype))
+    return ctypes.cast(t, ctypes.POINTER(ctype))
+
+
+@dataclass
+class Box:
+    lo: tuple
+    hi: tuple
+
+    def c(self) -> rbmd_box:
+        b = rbmd_box()
+        for d in range(3):
+            b.lo[d] = float(self.lo[d])
+            b.hi[d] = float(self.hi[d])
+        return b
+
+
+class ForceField:
+    """Force path selected by RBMD's configuration (force_field / neighbor / coulomb keys).
+
+    Mirrors ``ExecutionNVT::ComputeAllForce`` (rbmd/framework/run/ExecutionNVT.cpp:185-222):
+    ``LJ/CUT`` -> LJ over the full Verlet list; ``LJ/CUT/COUL/LONG`` -> far (RBE or EWALD) plus
+    near (LJ + erfc); ``CVFF`` -> the same plus intramolecular Coulomb removal, bonds and angles;
+    ``EAM`` -> the two EAM passes.  Atom arrays are torch CUDA tensors owned by the caller.
+    """
+
+    def __init__(self, config, boxes):
+        if isinstance(config, dict):
+            config = json.dumps(config)
+        if isinstance(boxes, Box):
+            boxes = [boxes]
+        self.config_text = config
+        self.boxes = list(boxes)
+        lib = library()
+        arr = (rbmd_box * len(self.boxes))(*[b.c() for b in self.boxes])
+        h = ctypes.c_void_p()
+        _check(lib.rbmd_force_create(config.encode(), len(self.boxes), arr, ctypes.byref(h)),
+               "rbmd_force_create")
+        self._h = h
+        self._keep = []
+
+    # ---- configuration --------------------------------------------------------------
+    def set_pair_coeffs(self, eps, sigma):
+        import numpy as np
+        e = np.ascontiguousarray(eps, dtype=np.float64)
+        s = np.ascontiguousarray(sigma, dtype=np.float64)
+        _check(library().rbmd_force_set_pair_coeffs(self._h, len(e), _ptr(e, ctypes.c_double),
+                                                    _ptr(s, ctypes.c_double)), "set_pair_coeffs")
+
+    def load_funcfl(self, path):
+        _check(library().rbmd_force_load_funcfl(self._h, str(path).encode()), "load_funcfl")
+
+    def set_water(self, hoh, bond_k, bond_r0, angle_k, angle_theta0_deg):
+        import numpy as np
+        t = np.ascontiguousarray(hoh, dtype=np.int32).reshape(-1)
+        _check(library().rbmd_force_set_water(self._h, len(t) // 3, _ptr(t, ctypes.c_int32),
+                                              float(bond_k), float(bond_r0), float(angle_k),
+                                              float(angle_theta0_deg)), "set_water")
+
+    def Init(self, pos, force, *, vel=None, mass=None, charge=None, type=None, molecule=None,
+             image=None, replica_offsets=None):
+        """Bind caller-owned device tensors (ExecutionMD::Init, ExecutionMD.cpp:117-134)."""
+        import numpy as np
+        import torch
+        for t in (pos, force):
+            if not (isinstance(t, torch.Tensor) and t.is_cuda):
+                raise RbmdError("ForceField.Init needs CUDA tensors (no CPU fallback)")
+        a = rbmd_atoms_dev()
+        a.n_atoms = pos.shape[0]
+        nrep = len(self.boxes)
+        a.n_replicas = nrep
+        if nrep > 1:
+            off = np.ascontiguousarray(replica_offsets, dtype=np.int64)
+            self._keep.append(off)
+            a.replica_offsets = off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+        else:
+            a.replica_offsets = None
+
+        def p(t, dt):
+            if t is None:
+                return None
+            if t.dtype != dt or not t.is_contiguous() or not t.is_cuda:
+                raise RbmdError(f"tensor must be contiguous CUDA {dt}")
+            self._keep.append(t)
+            return t.data_ptr()
+        a.pos = p(pos, torch.float64)
+        a.force = p(force, torch.float64)
+        a.vel = p(vel, torch.float64)
+        a.mass = p(mass, torch.float64)
+        a.charge = p(charge, torch.float64)
+        a.type = p(type, torch.int32)
+        a.molecule = p(molecule, torch.int32)
+        a.image = p(image, torch.int32)
+        _check(library().rbmd_force_bind(self._h, ctypes.byref(a)), "rbmd_force_bind")
+        self.n = int(pos.shape[0])
+
+    bind = Init
+
+    # ---- work ---------------------------------------------------------------------------
+    @staticmethod
+    def _stream(stream):
+        if stream is None:
+            import torch
+            return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        return ctypes.c_void_p(int(stream))
+
+    def Execute(self, stream=None):
+        """One force evaluation (Force::Execute / ExecutionNVT::ComputeForce)."""
+        _check(library().rbmd_force_compute(self._h, self._stream(stream)), "rbmd_force_compute")
+
+    compute = Execute
+
+    def compute_host(self, pos_host, force_host, stream=None):
+        _check(library().rbmd_force_compute_host(self._h, _ptr(pos_host, ctypes.c_double),
+                                                 _ptr(force_host, ctypes.c_double),
+                                                 self._stream(stream)), "compute_host")
+
+    def step(self, n_steps=1, stream=None):
+        _check(library().rbmd_force_step(self._h, int(n_steps), self._stream(stream)), "rbmd_force_step")
+
+    def sync_velocities(self, stream=None):
+        _check(library().rbmd_force_sync_velocities(self._h, self._stream(stream)), "sync_velocities")
+
+    # ---- k-space -------------------------------------------------------------------------
+    def set_ksamples(self, m):
+        import numpy as np
+        if m is None:
+            _check(library().rbmd_force_set_ksamples(self._h, None, 0), "set_ksamples")
+            return
+        a = np.ascontiguousarray(m, dtype=np.int32).reshape(-1, 3)
+        P = a.shape[0] // len(self.boxes)
+        _check(library().rbmd_force_set_ksamples(self._h, _ptr(a, ctypes.c_int32), P), "set_ksamples")
+
+    def set_kweights(self, w):
+        import numpy as np
+        if w is None:
+            _check(library().rbmd_force_set_kweights(self._h, None), "set_kweights")
+            return
+        a = np.ascontiguousarray(w, dtype=np.float64)
+        _check(library().rbmd_force_set_kweights(self._h, _ptr(a, ctypes.c_double)), "set_kweights")
+
+    def get_ksamples(self, P):
+        import numpy as np
+        out = np.zeros((len(self.boxes) * P, 3), dtype=np.int32)
+        _check(library().rbmd_force_get_ksamples(self._h, _ptr(out, ctypes.c_int32), P), "get_ksamples")
+        return out
+
+    def sample_k(self, step, P):
+        import numpy as np
+        out = np.zeros((len(self.boxes) * P, 3), dtype=np.int32)
+        _check(library().rbmd_force_sample_k(self._h, int(step), _ptr(out, ctypes.c_int32), P), "sample_k")
+        return out
+
+    def get_rhok(self, P):
+        import numpy as np
+        out = np.zeros((len(self.boxes) * P, 2), dtype=np.float64)
+        _check(library().rbmd_force_get_rhok(self._h, _ptr(out, ctypes.c_double), P), "get_rhok")
+        return out
+
+    # ---- diagnostics ----------------------------------------------------------------------
+    def neighbors(self, cap):
+        import numpy as np
+        counts = np.zeros(self.n, dtype=np.int32)
+        ids = np.full((self.n, cap), -1, dtype=np.int32)
+        st = library().rbmd_force_get_neighbors(self._h, _ptr(counts, ctypes.c_int32),
+                                                _ptr(ids, ctypes.c_int32), cap)
+        if st not in (RBMD_OK, 1):
+            _check(st, "get_neighbors")
+        return counts, ids
+
+    def energy(self, stream=None):
+        e = rbmd_energy()
+        _check(library().rbmd_force_energy(self._h, ctypes.byref(e), self._stream(stream)), "energy")
+        return {k: getattr(e, k) for k, _ in rbmd_energy._fields_}
+
+    def status(self, clear=False, stream=None):
+        f = ctypes.c_uint32()
+        _check(library().rbmd_force_status(self._h, ctypes.byref(f), int(clear), self._stream(stream)),
+               "status")
+        return int(f.value)
+
+    PHASES = ("integrate", "cell_sort", "kspace", "neighbor_list", "force", "molecular")
+
+    def profile(self, enable=True):
+        _check(library().rbmd_force_profile(self._h, int(enable)), "profile")
+
+    def phase_ms(self):
+        import numpy as np
+        ms = np.zeros(8)
+        cnt = np.zeros(8, np.int64)
+        _check(library().rbmd_force_phase_ms(self._h, _ptr(ms, ctypes.c_double),
+                                             _ptr(cnt, ctypes.c_int64), 8), "phase_ms")
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(self.PHASES)}
+
+    def launches_per_step(self):
+        k = ctypes.c_int32()
+        _check(library().rbmd_force_launch_count(self._h, ctypes.byref(k)), "launch_count")
+        return int(k.value)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            library().rbmd_force_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def version() -> str:
+    return library().rbmd_version().decode()

@@ -1,0 +1,262 @@
+// kernels_cells.cuh -- cell binning, deterministic cell sort and the full neighbour list.
+//
+// Reference: ContPointLocator::Build + BinPointsWorklet (rbmd/framework/locator/
+// ContPointLocator.cxx:38-92) does bin -> SortByKey -> Lower/UpperBounds with library calls.
+// Here: fused bin + per-cell atomic count (in the integrator or k_bin), one-block scan, atomic
+// scatter, then a warp per cell ranks its atoms by caller id so the slot order is deterministic
+// (a stable sort by (cell, id)), and the same warp gathers the slot-ordered caches.
+#pragma once
+#include "common.cuh"
+
+namespace rbmd {
+
+// cell index of a position, BinPointsWorklet semantics (truncate, clamp to [0, dims-1])
+template <class R>
+__device__ __forceinline__ int cell_of_pos(const RepDev& rp, R x, R y, R z) {
+  R p[3] = {x, y, z};
+  int ijk[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    int c = (int)div_rn(sub_rn(p[d], Traits<R>::lo(rp, d)), Traits<R>::dx(rp, d));
+    c = max(c, 0);
+    c = min(c, rp.dims[d] - 1);
+    ijk[d] = c;
+  }
+  return rp.cell_base + ijk[0] + ijk[1] * rp.dims[0] + ijk[2] * rp.dims[0] * rp.dims[1];
+}
+
+template <class R>
+__global__ void k_bin(int n, const double* __restrict__ pos, const int* __restrict__ rep_of,
+                      const RepDev* __restrict__ reps, int* __restrict__ cell_of,
+                      int* __restrict__ cell_count, uint32_t* status) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const RepDev& rp = reps[rep_of ? rep_of[i] : 0];
+  double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
+  if (!isfinite(x) || !isfinite(y) || !isfinite(z)) set_flag(status, kFlagNonFinite);
+  int c = cell_of_pos<R>(rp, (R)x, (R)y, (R)z);
+  cell_of[i] = c;
+  atomicAdd(&cell_count[c], 1);
+}
+
+// Exclusive scan of cell counts (one block of 1024 threads, each owning a contiguous chunk),
+// cell_start[ncell] = n.  Also clears the scatter cursors and flags over-full cells.
+__global__ void __launch_bounds__(1024) k_scan_cells(int ncell, const int* __restrict__ count,
+                                                     int* __restrict__ start, int* __restrict__ cursor,
+                                                     uint32_t* status) {
+  __shared__ int warp_sums[32];
+  const int t = threadIdx.x, nt = blockDim.x;
+  const int chunk = (ncell + nt - 1) / nt;
+  const int b = t * chunk, e = min(ncell, b + chunk);
+  int local = 0, mx = 0;
+  for (int c = b; c < e; ++c) {
+    int v = count[c];
+    local += v;
+    mx = max(mx, v);
+  }
+  if (mx > kMaxCellAtoms) set_flag(status, kFlagCellOverflow);
+  // block exclusive scan of `local`
+  int lane = t & 31, w = t >> 5;
+  int incl = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) warp_sums[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    int v = lane < (nt >> 5) ? warp_sums[lane] : 0;
+    int inc2 = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, inc2, o);
+      if (lane >= o) inc2 += y;
+    }
+    warp_sums[lane] = inc2 - v;
+  }
+  __syncthreads();
+  int run = warp_sums[w] + incl - local;
+  for (int c = b; c < e; ++c) {
+    start[c] = run;
+    cursor[c] = 0;
+    run += count[c];
+  }
+  if (t == nt - 1) start[ncell] = run;
+}
+
+__global__ void k_scatter(int n, const int* __restrict__ cell_of, const int* __restrict__ start,
+                          int* __restrict__ cursor, int* __restrict__ tmp_slot_atom) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int c = cell_of[i];
+  int s = start[c] + atomicAdd(&cursor[c], 1);
+  tmp_slot_atom[s] = i;
+}
+
+// One warp per cell: rank the cell's atoms by caller id (ids are distinct) and gather the
+// slot-ordered caches.  Cells above kMaxCellAtoms keep the scatter order (flagged by the scan).
+template <class R>
+__global__ void __launch_bounds__(256) k_cell_sort_gather(
+    int ncell, const int* __restrict__ start, const int* __restrict__ tmp_slot_atom,
+    const double* __restrict__ pos, const double* __restrict__ charge,
+    const int* __restrict__ type, const int* __restrict__ mol, const int* __restrict__ rep_of,
+    const RepDev* __restrict__ reps, int* __restrict__ slot_atom, int* __restrict__ atom_slot,
+    typename Traits<R>::V4* __restrict__ pos4, void* __restrict__ frac_out,
+    int2* __restrict__ meta) {
+  __shared__ int ids[8][kMaxCellAtoms];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int cell = blockIdx.x * 8 + w;
+  if (cell >= ncell) return;
+  const int s0 = start[cell], n = start[cell + 1] - s0;
+  if (n == 0) return;
+  const bool sortable = n <= kMaxCellAtoms;
+  if (sortable)
+    for (int k = lane; k < n; k += 32) ids[w][k] = tmp_slot_atom[s0 + k];
+  __syncwarp();
+  for (int k = lane; k < n; k += 32) {
+    int id = sortable ? ids[w][k] : tmp_slot_atom[s0 + k];
+    int rank = k;
+    if (sortable) {
+      rank = 0;
+      for (int m = 0; m < n; ++m) rank += ids[w][m] < id;
+    }
+    const int slot = s0 + rank;
+    slot_atom[slot] = id;
+    atom_slot[id] = slot;
+    const double x = pos[3 * id], y = pos[3 * id + 1], z = pos[3 * id + 2];
+    const double q = charge ? charge[id] : 0.0;
+    typename Traits<R>::V4 v;
+    v.x = (R)x; v.y = (R)y; v.z = (R)z; v.w = (R)q;
+    pos4[slot] = v;
+    if (meta) meta[slot] = make_int2(type ? type[id] : 0, mol ? mol[id] : id);
+    if (frac_out) {
+      const RepDev& rp = reps[rep_of ? rep_of[id] : 0];
+      double u[3] = {(x - rp.lo_d[0]) / rp.box_d[0], (y - rp.lo_d[1]) / rp.box_d[1],
+                     (z - rp.lo_d[2]) / rp.box_d[2]};
+      if (sizeof(R) == 4) {
+        uint32_t U[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          double f = u[d] - floor(u[d]);
+          double s = f * 4294967296.0;
+          U[d] = s >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)s;
+        }
+        Frac32 fr{U[0], U[1], U[2], (float)q};
+        reinterpret_cast<Frac32*>(frac_out)[slot] = fr;
+      } else {
+        unsigned long long U[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          double f = u[d] - floor(u[d]);
+          double s = f * 18446744073709551616.0;
+          U[d] = s >= 18446744073709549568.0 ? 0xFFFFFFFFFFFFF800ull : (unsigned long long)s;
+        }
+        Frac64 fr{U[0], U[1], U[2], q};
+        reinterpret_cast<Frac64*>(frac_out)[slot] = fr;
+      }
+    }
+  }
+}
+
+// Refresh the slot caches from the master positions without re-binning (list reuse with skin).
+template <class R>
+__global__ void k_regather(int n, const int* __restrict__ slot_atom, const double* __restrict__ pos,
+                           const double* __restrict__ charge, const int* __restrict__ rep_of,
+                           const RepDev* __restrict__ reps, typename Traits<R>::V4* __restrict__ pos4,
+                           void* __restrict__ frac_out) {
+  int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= n) return;
+  int id = slot_atom[slot];
+  const double x = pos[3 * id], y = pos[3 * id + 1], z = pos[3 * id + 2];
+  const double q = charge ? charge[id] : 0.0;
+  typename Traits<R>::V4 v;
+  v.x = (R)x; v.y = (R)y; v.z = (R)z; v.w = (R)q;
+  pos4[slot] = v;
+  if (frac_out) {
+    const RepDev& rp = reps[rep_of ? rep_of[id] : 0];
+    double u[3] = {(x - rp.lo_d[0]) / rp.box_d[0], (y - rp.lo_d[1]) / rp.box_d[1],
+                   (z - rp.lo_d[2]) / rp.box_d[2]};
+    if (sizeof(R) == 4) {
+      uint32_t U[3];
+      for (int d = 0; d < 3; ++d) {
+        double f = u[d] - floor(u[d]);
+        double s = f * 4294967296.0;
+        U[d] = s >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)s;
+      }
+      reinterpret_cast<Frac32*>(frac_out)[slot] = Frac32{U[0], U[1], U[2], (float)q};
+    } else {
+      unsigned long long U[3];
+      for (int d = 0; d < 3; ++d) {
+        double f = u[d] - floor(u[d]);
+        double s = f * 18446744073709551616.0;
+        U[d] = s >= 18446744073709549568.0 ? 0xFFFFFFFFFFFFF800ull : (unsigned long long)s;
+      }
+      reinterpret_cast<Frac64*>(frac_out)[slot] = Frac64{U[0], U[1], U[2], q};
+    }
+  }
+}
+
+// 1e-4 threshold of the neighbour predicate: the reference compares a float against the double
+// literal 0.0001; for float x, (double)x > 1e-4 <=> x > 1e-4f (1e-4f < 1e-4 < nextafterf(1e-4f)).
+__device__ __forceinline__ bool gt_small(float x) { return x > 1.0e-4f; }
+__device__ __forceinline__ bool gt_small(double x) { return x > 1.0e-4; }
+
+// Full Verlet list of slot i: ComputeNeighboursWorklet (rbmd/framework/run/worklet/
+// RunWorklet.cpp:40-96) -- stencil x-offset outermost, z innermost; predicate
+// rc^2 - d^2 > 1e-4 && d^2 > 1e-4 on r = (p_j - offset) - p_i with uncontracted float ops.
+template <class R>
+__global__ void __launch_bounds__(128) k_nlist(
+    int n, const typename Traits<R>::V4* __restrict__ pos4, const int* __restrict__ cell_start,
+    const RepDev* __restrict__ reps, const int* __restrict__ rep_of_slot, int num_cycles, R rc,
+    int cap, int stride, int* __restrict__ nbr, int* __restrict__ count, int* __restrict__ max_count,
+    uint32_t* status) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
+  const typename Traits<R>::V4 pi = pos4[i];
+  const R pix[3] = {pi.x, pi.y, pi.z};
+  int ci[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    ci[d] = (int)div_rn(sub_rn(pix[d], Traits<R>::lo(rp, d)), Traits<R>::dx(rp, d));
+  const R cut2 = mul_rn(rc, rc);
+  int idx = 0;
+  for (int a = -num_cycles; a <= num_cycles; ++a)
+    for (int b = -num_cycles; b <= num_cycles; ++b)
+      for (int c = -num_cycles; c <= num_cycles; ++c) {
+        const int nb[3] = {ci[0] + a, ci[1] + b, ci[2] + c};
+        int wv[3];
+        R off[3];
+        int code = 0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          int dd = rp.dims[d];
+          int w = ((nb[d] % dd) + dd) % dd;
+          wv[d] = w;
+          int delta = w - nb[d];
+          off[d] = mul_rn(Traits<R>::dx(rp, d), (R)delta);
+          code |= (delta > 0 ? 1 : (delta < 0 ? 2 : 0)) << (2 * d);
+        }
+        const int cell = rp.cell_base + wv[0] + wv[1] * rp.dims[0] + wv[2] * rp.dims[0] * rp.dims[1];
+        const int s1 = cell_start[cell + 1];
+        for (int s = cell_start[cell]; s < s1; ++s) {
+          const typename Traits<R>::V4 pj = pos4[s];
+          const R r0 = sub_rn(sub_rn(pj.x, off[0]), pix[0]);
+          const R r1 = sub_rn(sub_rn(pj.y, off[1]), pix[1]);
+          const R r2 = sub_rn(sub_rn(pj.z, off[2]), pix[2]);
+          const R d2 = add_rn(add_rn(mul_rn(r0, r0), mul_rn(r1, r1)), mul_rn(r2, r2));
+          if (gt_small(sub_rn(cut2, d2)) && gt_small(d2)) {
+            if (idx < cap) nbr[(size_t)idx * stride + i] = (s << kShiftBits) | code;
+            ++idx;
+          }
+        }
+      }
+  count[i] = idx;
+  if (idx > cap) {
+    set_flag(status, kFlagListOverflow);
+    atomicMax(max_count, idx);
+  }
+}
+
+}  // namespace rbmd

@@ -1,0 +1,600 @@
+// kernels_force.cuh -- near-field pair force (LJ 12-6 + real-space erfc Coulomb), the RBE
+// k-space force fused into the same per-atom pass, RBE structure factors, the RBE k-sampler,
+// and the EAM density / force passes.
+#pragma once
+#include "common.cuh"
+
+namespace rbmd {
+
+// ------------------------------------------------------------------------------------------
+// k-sample record: integer m vector plus the per-sample force coefficient w*k (w folds S/P,
+// qqr2e, -4 pi / (V k^2), the importance weight and the sign of the phase convention) and the
+// structure factor rho = sum_j q_j e^{i k.r_j}.
+// ------------------------------------------------------------------------------------------
+struct KRec32 { int mx, my, mz, rep; float wx, wy, wz, pad; float re, im, pad2, pad3; };   // 48 B
+struct KRec64 { int mx, my, mz, rep; double wx, wy, wz, re, im, pad; };                    // 64 B
+
+// phase -> (cos, sin) of 2*pi*(t - 1/2) for a 32-bit fixed-point turn t: the top 23 bits form a
+// float in [1, 2), so tf - 1.5 lies in [-0.5, 0.5); MUFU sin/cos are accurate on [-pi, pi].
+__device__ __forceinline__ void turn_sincos(uint32_t ph, float& s, float& c) {
+  float tf = __uint_as_float((ph >> 9) | 0x3F800000u) - 1.5f;
+  float th = tf * 6.28318530717958647692f;
+  __sincosf(th, &s, &c);
+}
+// 64-bit fixed-point turn -> exact double angle 2*pi*(t - 1/2) with t - 1/2 in [-0.5, 0.5)
+__device__ __forceinline__ void turn_sincos(unsigned long long ph, double& s, double& c) {
+  long long sg = (long long)(ph ^ 0x8000000000000000ull);   // (t - 1/2) * 2^64 as signed
+  double t = (double)sg * 5.42101086242752217e-20;           // 2^-64
+  sincospi(2.0 * t, &s, &c);
+}
+
+struct LJTable {
+  float lj24_f[kMaxReplicaTypes * kMaxReplicaTypes];    // -24 sqrt(eps_i eps_j)  (float)
+  float sig6_f[kMaxReplicaTypes * kMaxReplicaTypes];    // ((sig_i + sig_j)/2)^6   (float)
+  double lj24_d[kMaxReplicaTypes * kMaxReplicaTypes];
+  double sig6_d[kMaxReplicaTypes * kMaxReplicaTypes];
+};
+
+struct NearParams {
+  int n, stride, ntypes;
+  int with_lj, with_coul, molecular;
+  double rc, alpha, coul_scale;   // coul_scale multiplies the erfc Coulomb pair force
+  double sqrt_alpha, two_sqrt_alpha_over_sqrt_pi;
+};
+
+template <class R> struct KRec;
+template <> struct KRec<float> { using T = KRec32; };
+template <> struct KRec<double> { using T = KRec64; };
+template <class R> struct FracT;
+template <> struct FracT<float> { using T = Frac32; };
+template <> struct FracT<double> { using T = Frac64; };
+
+__device__ __forceinline__ float erfc_r(float x) { return erfcf(x); }
+__device__ __forceinline__ double erfc_r(double x) { return erfc(x); }
+__device__ __forceinline__ float exp_r(float x) { return expf(x); }
+__device__ __forceinline__ double exp_r(double x) { return exp(x); }
+__device__ __forceinline__ float sqrt_r(float x) { return sqrtf(x); }
+__device__ __forceinline__ double sqrt_r(double x) { return sqrt(x); }
+template <class R> __device__ __forceinline__ R lj24(const LJTable& t, int k);
+template <> __device__ __forceinline__ float lj24<float>(const LJTable& t, int k) { return t.lj24_f[k]; }
+template <> __device__ __forceinline__ double lj24<double>(const LJTable& t, int k) { return t.lj24_d[k]; }
+template <class R> __device__ __forceinline__ R sig6(const LJTable& t, int k);
+template <> __device__ __forceinline__ float sig6<float>(const LJTable& t, int k) { return t.sig6_f[k]; }
+template <> __device__ __forceinline__ double sig6<double>(const LJTable& t, int k) { return t.sig6_d[k]; }
+
+// Per-slot near force (+ fused RBE force).  One thread per slot over its transposed list row.
+// Pair physics: ComputeNearForceVerletWorklet / ComputeLJForceVerletWorklet
+// (rbmd/framework/run/worklet/RunWorklet.cpp:170-303) with ComputeLJForce and
+// ComputeNearEnergyForce (rbmd/framework/forceFunction/ExecForceFunction.h:74-140):
+//   LJ on MinDistanceVec(p_j', p_i) skipped within a molecule; Coulomb on p_j' - p_i for
+//   0.01 < d < rc with G = erfc(sqrt(a) d)/d^2 + 2 sqrt(a) e^{-a d^2}/(sqrt(pi) d).
+// RBE: ComputeNewRBEForceWorklet (RunWorklet.cpp:1508-1548), S/P and qqr2e folded into KRec.
+template <class R, bool LJ, bool COUL, bool RBE, bool MOLEC>
+__global__ void __launch_bounds__(128) k_near_force(
+    NearParams prm, const LJTable* __restrict__ ljt, const typename Traits<R>::V4* __restrict__ pos4,
+    const int2* __restrict__ meta, const int* __restrict__ nbr, const int* __restrict__ count,
+    const RepDev* __restrict__ reps, const int* __restrict__ rep_of_slot,
+    const int* __restrict__ slot_atom, const typename FracT<R>::T* __restrict__ frac,
+    const typename KRec<R>::T* __restrict__ krec, double* __restrict__ force,
+    double* __restrict__ energy_slot, uint32_t* status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= prm.n) return;
+  const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
+  const typename Traits<R>::V4 pi = pos4[i];
+  const int2 mi = (LJ && (MOLEC || prm.ntypes > 1)) ? meta[i] : make_int2(0, 0);
+  const R rc = (R)prm.rc;
+  const R cut2 = rc * rc;
+  const R box[3] = {Traits<R>::box(rp, 0), Traits<R>::box(rp, 1), Traits<R>::box(rp, 2)};
+  const R wrap[3] = {Traits<R>::wrap(rp, 0), Traits<R>::wrap(rp, 1), Traits<R>::wrap(rp, 2)};
+  const R sa = (R)prm.sqrt_alpha, aa = (R)prm.alpha, c2 = (R)prm.two_sqrt_alpha_over_sqrt_pi;
+  const R cs = (R)prm.coul_scale;
+  Acc<R> fx, fy, fz;
+  R e_lj = 0, e_coul = 0;
+  const int cnt = count[i];
+  for (int p = 0; p < cnt; ++p) {
+    const int e = __ldg(nbr + (size_t)p * prm.stride + i);
+    const int j = e >> kShiftBits;
+    const typename Traits<R>::V4 pj = pos4[j];
+    R off[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int cd = (e >> (2 * d)) & 3;
+      off[d] = cd == 1 ? wrap[d] : (cd == 2 ? -wrap[d] : (R)0);
+    }
+    R r0 = (pj.x - off[0]) - pi.x;
+    R r1 = (pj.y - off[1]) - pi.y;
+    R r2 = (pj.z - off[2]) - pi.z;
+    R f = 0;
+    const R d2 = r0 * r0 + r1 * r1 + r2 * r2;
+    if (COUL) {
+      const R dis = sqrt_r(d2);
+      if (dis < rc && dis > (R)0.01) {
+        const R inv = (R)1 / dis;
+        const R ex = exp_r(-aa * d2);
+        const R g = erfc_r(sa * dis) * inv * inv + c2 * ex * inv;
+        f += -pi.w * pj.w * g * inv * cs;
+        e_coul += pi.w * pj.w * erfc_r(sa * dis) * inv * cs;
+      }
+    }
+    R fl0 = 0, fl1 = 0, fl2 = 0;
+    if (LJ) {
+      bool same = false;
+      int tj = 0;
+      if (MOLEC || prm.ntypes > 1) {
+        const int2 mj = meta[j];
+        same = MOLEC && (mj.y == mi.y);
+        tj = mj.x;
+      }
+      if (!same) {
+        R q0 = r0, q1 = r1, q2 = r2;   // MinDistanceVec(p_j', p_i)
+        if (fabs(q0) > box[0] * (R)0.5) q0 -= (q0 > 0 ? box[0] : -box[0]);
+        if (fabs(q1) > box[1] * (R)0.5) q1 -= (q1 > 0 ? box[1] : -box[1]);
+        if (fabs(q2) > box[2] * (R)0.5) q2 -= (q2 > 0 ? box[2] : -box[2]);
+        const R dl2 = q0 * q0 + q1 * q1 + q2 * q2;
+        if (dl2 < cut2 && dl2 > (R)0.0001) {
+          const int k = mi.x * prm.ntypes + tj;
+          const R inv2 = (R)1 / dl2;
+          const R sd6 = sig6<R>(*ljt, k) * inv2 * inv2 * inv2;
+          const R scal = lj24<R>(*ljt, k) * (((R)2 * sd6 - (R)1) * sd6) * inv2;
+          fl0 = scal * q0; fl1 = scal * q1; fl2 = scal * q2;
+          // 4 eps (s6 - 1) s6 with 4 eps = -lj24/6
+          e_lj += -lj24<R>(*ljt, k) / (R)6 * (sd6 - (R)1) * sd6;
+        }
+      }
+    }
+    fx.add(f * r0 + fl0);
+    fy.add(f * r1 + fl1);
+    fz.add(f * r2 + fl2);
+  }
+  double F[3] = {fx.value(), fy.value(), fz.value()};
+  if (RBE) {
+    const typename FracT<R>::T fr = frac[i];
+    R ax = 0, ay = 0, az = 0;
+    const int kb = rp.k_begin, P = rp.P;
+#pragma unroll 4
+    for (int l = 0; l < P; ++l) {
+      const typename KRec<R>::T k = krec[kb + l];
+      R s, c;
+      if (sizeof(R) == 4) {
+        uint32_t ph = (uint32_t)k.mx * (uint32_t)fr.x + (uint32_t)k.my * (uint32_t)fr.y +
+                      (uint32_t)k.mz * (uint32_t)fr.z;
+        float sf, cf;
+        turn_sincos(ph, sf, cf);
+        s = (R)sf; c = (R)cf;
+      } else {
+        unsigned long long ph = (unsigned long long)(long long)k.mx * (unsigned long long)fr.x +
+                                (unsigned long long)(long long)k.my * (unsigned long long)fr.y +
+                                (unsigned long long)(long long)k.mz * (unsigned long long)fr.z;
+        double sd, cd;
+        turn_sincos(ph, sd, cd);
+        s = (R)sd; c = (R)cd;
+      }
+      const R val = c * (R)k.im - s * (R)k.re;
+      ax += val * (R)k.wx;
+      ay += val * (R)k.wy;
+      az += val * (R)k.wz;
+    }
+    const double q = (double)fr.q;
+    F[0] += q * (double)ax;
+    F[1] += q * (double)ay;
+    F[2] += q * (double)az;
+  }
+  if (!isfinite(F[0]) || !isfinite(F[1]) || !isfinite(F[2])) set_flag(status, kFlagNonFinite);
+  const int id = slot_atom[i];
+  force[3 * id] = F[0];
+  force[3 * id + 1] = F[1];
+  force[3 * id + 2] = F[2];
+  if (energy_slot) {
+    energy_slot[2 * i] = 0.5 * (double)e_lj;
+    energy_slot[2 * i + 1] = 0.5 * (double)e_coul;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// RBE structure factors.  Work item = (replica, atom chunk, k tile of KT samples); each thread
+// walks the chunk's atoms with KT (Re, Im) accumulators in registers, then the block reduces
+// them (warp shuffles + shared memory) to one partial per (item, k).  There is no N x P buffer
+// (the reference materialises rho_Re/Im[P*N] and reduces by key, ExecutionMD.cpp:412-448).
+// ------------------------------------------------------------------------------------------
+struct RhoItem { int atom_begin, atom_end, k_first, k_count; };
+
+template <int KT>
+__global__ void __launch_bounds__(256) k_rho_partial32(const RhoItem* __restrict__ items,
+                                                       const Frac32* __restrict__ frac,
+                                                       const KRec32* __restrict__ krec,
+                                                       float2* __restrict__ partial) {
+  const RhoItem it = items[blockIdx.x];
+  uint32_t mx[KT], my[KT], mz[KT];
+#pragma unroll
+  for (int k = 0; k < KT; ++k) {
+    const bool ok = k < it.k_count;
+    mx[k] = ok ? (uint32_t)krec[it.k_first + k].mx : 0u;
+    my[k] = ok ? (uint32_t)krec[it.k_first + k].my : 0u;
+    mz[k] = ok ? (uint32_t)krec[it.k_first + k].mz : 0u;
+  }
+  float re[KT], im[KT];
+#pragma unroll
+  for (int k = 0; k < KT; ++k) { re[k] = 0.f; im[k] = 0.f; }
+  for (int a = it.atom_begin + threadIdx.x; a < it.atom_end; a += blockDim.x) {
+    const Frac32 f = frac[a];
+#pragma unroll
+    for (int k = 0; k < KT; ++k) {
+      const uint32_t ph = mx[k] * f.x + my[k] * f.y + mz[k] * f.z;
+      float s, c;
+      turn_sincos(ph, s, c);
+      re[k] = fmaf(f.q, c, re[k]);
+      im[k] = fmaf(f.q, s, im[k]);
+    }
+  }
+  __shared__ float red[8][2 * KT];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < KT; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      re[k] += __shfl_xor_sync(0xffffffffu, re[k], o);
+      im[k] += __shfl_xor_sync(0xffffffffu, im[k], o);
+    }
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < KT; ++k) { red[w][2 * k] = re[k]; red[w][2 * k + 1] = im[k]; }
+  }
+  __syncthreads();
+  if (threadIdx.x < 2 * KT) {
+    float s = 0.f;
+    const int nw = blockDim.x >> 5;
+    for (int ww = 0; ww < nw; ++ww) s += red[ww][threadIdx.x];
+    reinterpret_cast<float*>(partial)[(size_t)blockIdx.x * 2 * KT + threadIdx.x] = s;
+  }
+}
+
+template <int KT>
+__global__ void __launch_bounds__(256) k_rho_partial64(const RhoItem* __restrict__ items,
+                                                       const Frac64* __restrict__ frac,
+                                                       const KRec64* __restrict__ krec,
+                                                       double2* __restrict__ partial) {
+  const RhoItem it = items[blockIdx.x];
+  long long mx[KT], my[KT], mz[KT];
+#pragma unroll
+  for (int k = 0; k < KT; ++k) {
+    const bool ok = k < it.k_count;
+    mx[k] = ok ? krec[it.k_first + k].mx : 0;
+    my[k] = ok ? krec[it.k_first + k].my : 0;
+    mz[k] = ok ? krec[it.k_first + k].mz : 0;
+  }
+  double re[KT], im[KT];
+#pragma unroll
+  for (int k = 0; k < KT; ++k) { re[k] = 0.0; im[k] = 0.0; }
+  for (int a = it.atom_begin + threadIdx.x; a < it.atom_end; a += blockDim.x) {
+    const Frac64 f = frac[a];
+#pragma unroll
+    for (int k = 0; k < KT; ++k) {
+      const unsigned long long ph = (unsigned long long)mx[k] * f.x +
+                                    (unsigned long long)my[k] * f.y + (unsigned long long)mz[k] * f.z;
+      double s, c;
+      turn_sincos(ph, s, c);
+      re[k] = fma(f.q, c, re[k]);
+      im[k] = fma(f.q, s, im[k]);
+    }
+  }
+  __shared__ double red[8][2 * KT];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < KT; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      re[k] += __shfl_xor_sync(0xffffffffu, re[k], o);
+      im[k] += __shfl_xor_sync(0xffffffffu, im[k], o);
+    }
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < KT; ++k) { red[w][2 * k] = re[k]; red[w][2 * k + 1] = im[k]; }
+  }
+  __syncthreads();
+  if (threadIdx.x < 2 * KT) {
+    double s = 0.0;
+    const int nw = blockDim.x >> 5;
+    for (int ww = 0; ww < nw; ++ww) s += red[ww][threadIdx.x];
+    reinterpret_cast<double*>(partial)[(size_t)blockIdx.x * 2 * KT + threadIdx.x] = s;
+  }
+}
+
+// Per-replica reduction layout: items are ordered (replica, chunk, tile); replica r's partials
+// for tile t and chunk c sit at item_base_r + c * ntiles_r + t.
+struct RhoRep { int item_base, ntiles, nchunks, pad; };
+
+// One thread per k sample: sum the chunk partials in a fixed order (FP64), undo the half-turn
+// phase convention (rho = -sum), then fill the force coefficients of the k record.
+// k-space energy estimate per replica: (S/P) qqr2e sum_l w_l (2 pi / V) |rho_l|^2 / k_l^2.
+template <class R, int KT>
+__global__ void k_rho_finish(int nk_total, const RhoRep* __restrict__ rr, const RepDev* __restrict__ reps,
+                             const void* __restrict__ partial_v, const double* __restrict__ weights,
+                             double qqr2e, typename KRec<R>::T* __restrict__ krec,
+                             double2* __restrict__ rho_out, double* __restrict__ ek_out) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nk_total) return;
+  typename KRec<R>::T k = krec[g];
+  const int r = k.rep;
+  const RepDev& rp = reps[r];
+  const RhoRep q = rr[r];
+  const int l = g - rp.k_begin;
+  const int tile = l / KT, kk = l % KT;
+  double re = 0, im = 0;
+  for (int c = 0; c < q.nchunks; ++c) {
+    const size_t item = (size_t)q.item_base + (size_t)c * q.ntiles + tile;
+    if (sizeof(R) == 4) {
+      const float* p = reinterpret_cast<const float*>(partial_v) + item * 2 * KT + 2 * kk;
+      re += (double)p[0];
+      im += (double)p[1];
+    } else {
+      const double* p = reinterpret_cast<const double*>(partial_v) + item * 2 * KT + 2 * kk;
+      re += p[0];
+      im += p[1];
+    }
+  }
+  re = -re;
+  im = -im;
+  const double twopi = 6.283185307179586476925;
+  const double kx = twopi * k.mx / rp.box_d[0], ky = twopi * k.my / rp.box_d[1],
+               kz = twopi * k.mz / rp.box_d[2];
+  const double k2 = kx * kx + ky * ky + kz * kz;
+  const double wgt = weights ? weights[g] : 1.0;
+  // F_i = q_i (S/P) qqr2e sum_l wgt (-4 pi /(V k^2)) k (cos Im - sin Re); the kernel evaluates
+  // the angle shifted by half a turn, which flips cos and sin: store -w.
+  const double w = -(rp.S / rp.P) * qqr2e * wgt * (-4.0 * 3.14159265358979323846 / (rp.volume * k2));
+  k.wx = (decltype(k.wx))(w * kx);
+  k.wy = (decltype(k.wy))(w * ky);
+  k.wz = (decltype(k.wz))(w * kz);
+  k.re = (decltype(k.re))re;
+  k.im = (decltype(k.im))im;
+  krec[g] = k;
+  if (rho_out) rho_out[g] = make_double2(re, im);
+  if (ek_out)
+    ek_out[g] = (rp.S / rp.P) * qqr2e * wgt * (2.0 * 3.14159265358979323846 / rp.volume) *
+                (re * re + im * im) / k2;
+}
+
+// ------------------------------------------------------------------------------------------
+// RBE k-sampler: RBEPSAMPLE::Fetch_P_Sample + MH_Algorithm (rbmd/framework/model/
+// RBEPSample.h:63-173) with mu = 0, sigma_d = sqrt(alpha/2) L_d / pi.  One block per replica:
+// the Gaussian proposals and acceptance uniforms of the first D draws are generated in
+// parallel (they do not depend on the chain), then thread 0 runs the three per-axis chains in
+// lockstep (the all-zero retry couples the axes).  Draws past D are made inline.
+// ------------------------------------------------------------------------------------------
+struct SamplerRep {
+  double sigma[3];
+  double c[3];      // pi^2 / (alpha L_d^2)
+  int qmax;
+  int q_offset;     // offset of this replica's q tables (3 * (qmax+1) doubles) in qtab
+};
+
+__device__ __forceinline__ double sampler_draw(uint32_t k0, uint32_t k1, long long step, int rep,
+                                               int axis, long long draw, double* ua) {
+  uint32_t c[4] = {(uint32_t)draw, (uint32_t)axis | ((uint32_t)rep << 2), (uint32_t)(unsigned long long)step,
+                   (uint32_t)((unsigned long long)step >> 32)};
+  philox4x32(c, k0, k1);
+  double U1 = ((double)c[0] + 0.5) * (1.0 / 4294967296.0);
+  if (U1 < 1e-6) U1 = ((double)c[3] + 0.5) * (1.0 / 4294967296.0);
+  if (U1 < 1e-6) U1 = 1e-6;
+  const double U2 = ((double)c[1] + 0.5) * (1.0 / 4294967296.0);
+  *ua = ((double)c[2] + 0.5) * (1.0 / 4294967296.0);
+  return sqrt(-2.0 * log(U1)) * cos(2.0 * 3.14159265358979323846 * U2);
+}
+
+template <int D>
+__global__ void __launch_bounds__(256) k_sample(int nrep, const SamplerRep* __restrict__ srep,
+                                                const double* __restrict__ qtab,
+                                                const RepDev* __restrict__ reps, unsigned long long seed,
+                                                long long step, int* __restrict__ kvec_out,
+                                                void* __restrict__ krec, int rec_bytes, uint32_t* status) {
+  const int r = blockIdx.x;
+  if (r >= nrep) return;
+  const SamplerRep s = srep[r];
+  const int P = reps[r].P, kb = reps[r].k_begin;
+  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  __shared__ int mw[3][D];
+  __shared__ double ua[3][D];
+  for (int t = threadIdx.x; t < 3 * D; t += blockDim.x) {
+    const int axis = t / D, d = t % D;
+    double u;
+    const double g = sampler_draw(k0, k1, step, r, axis, d, &u);
+    mw[axis][d] = (int)round(s.sigma[axis] * g);
+    ua[axis][d] = u;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  const double* q = qtab + s.q_offset;
+  auto qv = [&](int axis, int m) -> double {
+    m = abs(m);
+    return m <= s.qmax ? q[axis * (s.qmax + 1) + m] : 0.0;
+  };
+  auto prop = [&](int axis, long long d, double* u) -> int {
+    if (d < D) { *u = ua[axis][d]; return mw[axis][d]; }
+    const double g = sampler_draw(k0, k1, step, r, axis, d, u);
+    return (int)round(s.sigma[axis] * g);
+  };
+  long long draw = 0;
+  int X0[3];
+  for (int guard = 0;; ++guard) {
+    double u;
+    for (int a = 0; a < 3; ++a) X0[a] = prop(a, draw, &u);
+    ++draw;
+    if (!(X0[0] == 0 && X0[1] == 0 && X0[2] == 0)) break;
+    if (guard > 100000) { set_flag(status, kFlagSampler); X0[0] = 1; break; }
+  }
+  auto emit = [&](int i, const int* X) {
+    int* o = kvec_out + 3 * (kb + i);
+    o[0] = X[0]; o[1] = X[1]; o[2] = X[2];
+    int* rec = reinterpret_cast<int*>(reinterpret_cast<char*>(krec) + (size_t)(kb + i) * rec_bytes);
+    rec[0] = X[0]; rec[1] = X[1]; rec[2] = X[2]; rec[3] = r;
+  };
+  emit(0, X0);
+  int i = 1;
+  long long guard = 0;
+  while (i < P) {
+    int X1[3];
+    for (int a = 0; a < 3; ++a) {
+      double u;
+      const int m_w = prop(a, draw, &u);
+      const int m = X0[a];
+      const double qm = qv(a, m), qw = qv(a, m_w);
+      double pr = exp(s.c[a] * ((double)m * m - (double)m_w * m_w)) * (qm / qw);
+      if (!(pr < 1.0)) pr = 1.0;
+      X1[a] = (u <= pr) ? m_w : m;
+    }
+    ++draw;
+    X0[0] = X1[0]; X0[1] = X1[1]; X0[2] = X1[2];
+    if (++guard > 64LL * P + 100000) { set_flag(status, kFlagSampler); break; }
+    if (X1[0] == 0 && X1[1] == 0 && X1[2] == 0) continue;
+    emit(i, X1);
+    ++i;
+  }
+  if (draw > D) set_flag(status, 0);   // inline draws are valid; nothing to report
+}
+
+// ------------------------------------------------------------------------------------------
+// EAM passes (funcfl, 7-coefficient splines): pass 1 = ComputeEAMfpVerletWorklet
+// (RunWorklet.cpp:305-359) -> fp[slot]; pass 2 = ComputeEAMForceVerletWorklet (:361-417).
+// Spline rows are stored as two float4 (c0..c3, c4..c6,0).
+// ------------------------------------------------------------------------------------------
+struct EamDev {
+  const float4* frho;   // 2 float4 per row
+  const float4* rhor;
+  const float4* z2r;
+  int nrho, nr;
+  float rdr, rdrho;
+  double rdr_d, rdrho_d;
+  float rhomax;
+};
+
+template <class R>
+__global__ void __launch_bounds__(128) k_eam_fp(int n, int stride, double rc, EamDev eam,
+                                                const typename Traits<R>::V4* __restrict__ pos4,
+                                                const int* __restrict__ nbr, const int* __restrict__ count,
+                                                const RepDev* __restrict__ reps,
+                                                const int* __restrict__ rep_of_slot, R* __restrict__ fp,
+                                                double* __restrict__ embed_slot) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
+  const typename Traits<R>::V4 pi = pos4[i];
+  const R wrap[3] = {Traits<R>::wrap(rp, 0), Traits<R>::wrap(rp, 1), Traits<R>::wrap(rp, 2)};
+  const R box[3] = {Traits<R>::box(rp, 0), Traits<R>::box(rp, 1), Traits<R>::box(rp, 2)};
+  const R cut2 = (R)rc * (R)rc;
+  const R rdr = sizeof(R) == 4 ? (R)eam.rdr : (R)eam.rdr_d;
+  Acc<R> rho;
+  const int cnt = count[i];
+  for (int p = 0; p < cnt; ++p) {
+    const int e = __ldg(nbr + (size_t)p * stride + i);
+    const int j = e >> kShiftBits;
+    const typename Traits<R>::V4 pj = pos4[j];
+    R r[3];
+    const R pjv[3] = {pj.x, pj.y, pj.z}, piv[3] = {pi.x, pi.y, pi.z};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int cd = (e >> (2 * d)) & 3;
+      const R off = cd == 1 ? wrap[d] : (cd == 2 ? -wrap[d] : (R)0);
+      R v = piv[d] - (pjv[d] - off);
+      if (fabs(v) > box[d] * (R)0.5) v -= (v > 0 ? box[d] : -box[d]);
+      r[d] = v;
+    }
+    const R rsq = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    if (rsq < cut2 && rsq > (R)0.01) {
+      R pp = sqrt_r(rsq) * rdr + (R)1;
+      int m = (int)pp;
+      m = min(m, eam.nr - 1);
+      pp -= (R)m;
+      pp = fmin(pp, (R)1);
+      const float4 b = __ldg(eam.rhor + 2 * m + 0);
+      const float4 c = __ldg(eam.rhor + 2 * m + 1);
+      rho.add((((R)b.w * pp + (R)c.x) * pp + (R)c.y) * pp + (R)c.z);
+    }
+  }
+  const R rr = (R)rho.value();
+  R pp = rr * (sizeof(R) == 4 ? (R)eam.rdrho : (R)eam.rdrho_d) + (R)1;
+  int m = (int)pp;
+  m = max(1, min(m, eam.nrho - 1));
+  pp -= (R)m;
+  pp = fmin(pp, (R)1);
+  const float4 a = __ldg(eam.frho + 2 * m + 0);
+  const float4 b = __ldg(eam.frho + 2 * m + 1);
+  fp[i] = ((R)a.x * pp + (R)a.y) * pp + (R)a.z;
+  if (embed_slot) {
+    double phi = (((double)a.w * pp + (double)b.x) * pp + (double)b.y) * pp + (double)b.z;
+    if ((double)rr > eam.rhomax) phi += (double)fp[i] * ((double)rr - eam.rhomax);
+    embed_slot[i] = phi;
+  }
+}
+
+template <class R>
+__global__ void __launch_bounds__(128) k_eam_force(int n, int stride, double rc, EamDev eam,
+                                                   const typename Traits<R>::V4* __restrict__ pos4,
+                                                   const int* __restrict__ nbr, const int* __restrict__ count,
+                                                   const RepDev* __restrict__ reps,
+                                                   const int* __restrict__ rep_of_slot,
+                                                   const R* __restrict__ fp, const int* __restrict__ slot_atom,
+                                                   double* __restrict__ force, double* __restrict__ pair_slot,
+                                                   uint32_t* status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
+  const typename Traits<R>::V4 pi = pos4[i];
+  const R wrap[3] = {Traits<R>::wrap(rp, 0), Traits<R>::wrap(rp, 1), Traits<R>::wrap(rp, 2)};
+  const R box[3] = {Traits<R>::box(rp, 0), Traits<R>::box(rp, 1), Traits<R>::box(rp, 2)};
+  const R cut2 = (R)rc * (R)rc;
+  const R rdr = sizeof(R) == 4 ? (R)eam.rdr : (R)eam.rdr_d;
+  const R fpi = fp[i];
+  Acc<R> fx, fy, fz;
+  R epair = 0;
+  const int cnt = count[i];
+  for (int p = 0; p < cnt; ++p) {
+    const int e = __ldg(nbr + (size_t)p * stride + i);
+    const int j = e >> kShiftBits;
+    const typename Traits<R>::V4 pj = pos4[j];
+    R r[3];
+    const R pjv[3] = {pj.x, pj.y, pj.z}, piv[3] = {pi.x, pi.y, pi.z};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int cd = (e >> (2 * d)) & 3;
+      const R off = cd == 1 ? wrap[d] : (cd == 2 ? -wrap[d] : (R)0);
+      R v = (pjv[d] - off) - piv[d];
+      if (fabs(v) > box[d] * (R)0.5) v -= (v > 0 ? box[d] : -box[d]);
+      r[d] = v;
+    }
+    const R rsq = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    if (rsq < cut2 && rsq > (R)0.01) {
+      const R rv = sqrt_r(rsq);
+      R pp = rv * rdr + (R)1;
+      int m = (int)pp;
+      m = min(m, eam.nr - 1);
+      pp -= (R)m;
+      pp = fmin(pp, (R)1);
+      const float4 ra = __ldg(eam.rhor + 2 * m + 0);
+      const float4 za = __ldg(eam.z2r + 2 * m + 0);
+      const float4 zb = __ldg(eam.z2r + 2 * m + 1);
+      const R rhop = ((R)ra.x * pp + (R)ra.y) * pp + (R)ra.z;
+      const R z2p = ((R)za.x * pp + (R)za.y) * pp + (R)za.z;
+      const R z2 = (((R)za.w * pp + (R)zb.x) * pp + (R)zb.y) * pp + (R)zb.z;
+      const R recip = (R)1 / rv;
+      const R phi = z2 * recip;
+      const R phip = z2p * recip - phi * recip;
+      const R psip = fpi * rhop + fp[j] * rhop + phip;
+      const R fpair = -psip * recip;
+      fx.add(r[0] * fpair);
+      fy.add(r[1] * fpair);
+      fz.add(r[2] * fpair);
+      epair += phi;
+    }
+  }
+  const double F[3] = {fx.value(), fy.value(), fz.value()};
+  if (!isfinite(F[0]) || !isfinite(F[1]) || !isfinite(F[2])) set_flag(status, kFlagNonFinite);
+  const int id = slot_atom[i];
+  force[3 * id] = F[0];
+  force[3 * id + 1] = F[1];
+  force[3 * id + 2] = F[2];
+  if (pair_slot) pair_slot[i] = 0.5 * (double)epair;
+}
+
+}  // namespace rbmd

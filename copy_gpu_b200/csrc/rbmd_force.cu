@@ -1,0 +1,1277 @@
+// rbmd_force.cu -- C ABI and host driver of the B200 force path (see include/rbmd_force.h).
+//
+// The driver reproduces the dispatch of ExecutionNVT::ComputeAllForce
+// (rbmd/framework/run/ExecutionNVT.cpp:185-222) and the step order of ExecutionNVT::Solve
+// (:133-159) on top of the sm_100a kernels in kernels_*.cuh.  All work of one call is queued on
+// the caller's stream (k-space structure factors on a forked side stream that joins before the
+// force pass); host synchronisation happens only where a call must return host data or check
+// the list capacity.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/rbmd_force.h"
+#include "common.cuh"
+#include "eam_funcfl.hpp"
+#include "json.hpp"
+#include "kernels_cells.cuh"
+#include "kernels_force.cuh"
+#include "kernels_md.cuh"
+
+using namespace rbmd;
+
+namespace {
+
+constexpr int kKT = 16;          // k samples per structure-factor tile
+constexpr int kSamplerD = 1024;  // pre-drawn proposals per axis in the sampler kernel
+constexpr int kMdChunk = 2048;   // atoms per kinetic-energy chunk
+
+#define CK(x)                                                                            \
+  do {                                                                                   \
+    cudaError_t e_ = (x);                                                                \
+    if (e_ != cudaSuccess) {                                                             \
+      std::snprintf(g_last_error, sizeof g_last_error, "%s:%d %s: %s", __FILE__, __LINE__, \
+                    #x, cudaGetErrorString(e_));                                         \
+      return RBMD_ERR_CUDA;                                                              \
+    }                                                                                    \
+  } while (0)
+
+char g_last_error[512] = "";
+
+template <class T>
+cudaError_t dalloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  return cudaMalloc((void**)p, count * sizeof(T));
+}
+template <class T>
+void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+struct Units { double kB, fmt2v, mvv2e, qqr2e; };
+
+// ExecutionMD::InitParameters (rbmd/framework/run/ExecutionMD.cpp:328-353)
+Units units_for(const std::string& u) {
+  if (u == "REAL") return {1.9872067e-3, 4.186e-4, 1.0 / 4.186e-4, 332.06371};
+  if (u == "METAL") return {8.617343e-5, 1.0 / 1.0364269e-4, 1.0364269e-4, 14.399645};
+  return {1.0, 1.0, 1.0, 1.0};
+}
+
+}  // namespace
+
+struct rbmd_force {
+  // ---------------- configuration ----------------
+  std::string ff = "LJ/CUT", nbr_type = "VERLETLIST", coul_type = "RBE", unit = "LJ";
+  std::string shake = "null", init_way = "read_data", tctrl = "";
+  bool far = false, fp64 = false;
+  double rc = 2.5, rs = 2.5, skin = 0.0, alpha = 0.1;
+  int P = 100, kmax = 2;
+  unsigned long long seed = 20240101ull;
+  Units u{1, 1, 1, 1};
+  double dt = 0.005, T0 = 1.0, Tdamp = 1.0;
+  int tstat = 0, dof_mode = 0;
+  double near_coul_scale = 1.0;
+  double shake_tol = 1e-5;
+  int shake_max_iter = 5000;
+  std::string potential_file;
+
+  // ---------------- replicas ----------------
+  int nrep = 1;
+  std::vector<rbmd_box> boxes;
+  std::vector<RepDev> reps_h;
+  int ncell_total = 0, num_cycles = 1;
+
+  // ---------------- per-type LJ ----------------
+  int ntypes = 1;
+  LJTable ljt_h{};
+  bool have_pair_coeffs = false;
+
+  // ---------------- EAM ----------------
+  FuncflTables eam_h;
+  bool eam_loaded = false;
+
+  // ---------------- water ----------------
+  int64_t n_mol = 0;
+  std::vector<int32_t> hoh_h;
+  double bond_k = 0, bond_r0 = 1, angle_k = 0, angle_t0 = 109.47;
+
+  // ---------------- bound atoms ----------------
+  rbmd_atoms_dev at{};
+  std::vector<int64_t> rep_off;
+  bool bound = false;
+  int n = 0, stride = 0, cap = 0;
+  double sum_q2 = 0;
+
+  // ---------------- device buffers ----------------
+  RepDev* d_reps = nullptr;
+  LJTable* d_ljt = nullptr;
+  int *d_rep_of = nullptr, *d_cell_of = nullptr, *d_cell_count = nullptr, *d_cell_start = nullptr,
+      *d_cursor = nullptr, *d_tmp = nullptr, *d_slot_atom = nullptr, *d_atom_slot = nullptr;
+  void* d_pos4 = nullptr;
+  void* d_frac = nullptr;
+  int2* d_meta = nullptr;
+  int *d_nbr = nullptr, *d_count = nullptr, *d_maxcount = nullptr;
+  uint32_t* d_status = nullptr;
+  double* d_eslot = nullptr;   // 2 per slot (lj, coul)
+  double* d_esum = nullptr;    // scratch sums
+  // RBE
+  int Ptot = 0, nitems = 0;
+  void* d_krec = nullptr;
+  int* d_kvec = nullptr;
+  RhoItem* d_items = nullptr;
+  RhoRep* d_rhorep = nullptr;
+  void* d_partial = nullptr;
+  double2* d_rho = nullptr;
+  double* d_ek = nullptr;
+  double* d_weights = nullptr;
+  SamplerRep* d_srep = nullptr;
+  double* d_qtab = nullptr;
+  bool injected = false;
+  // MD
+  MdChunk* d_chunks = nullptr;
+  int nchunks = 0;
+  int* d_chunk_rep_begin = nullptr;
+  double *d_ke_partial = nullptr, *d_ke = nullptr, *d_T = nullptr, *d_lambda = nullptr,
+         *d_xi = nullptr, *d_xold = nullptr, *d_vold = nullptr;
+  bool pending_scale = false;
+  // EAM device
+  float4 *d_frho = nullptr, *d_rhor = nullptr, *d_z2r = nullptr;
+  void* d_fp = nullptr;
+  double *d_emb = nullptr, *d_epair = nullptr;
+  // water device
+  int* d_hoh = nullptr;
+  double *d_ebond = nullptr, *d_eangle = nullptr;
+  // snapshot for step replay
+  double *d_snap = nullptr;
+  int* d_snap_img = nullptr;
+  // host pinned
+  uint32_t* h_status = nullptr;
+  int* h_maxcount = nullptr;
+  // streams
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  long long step_count = 0;
+  int launches = 0;
+  // per-phase CUDA-event profiler (rbmd_force_profile / rbmd_force_phase_ms)
+  bool prof_on = false;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_pairs;
+  double phase_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  long long phase_n[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+
+  bool is_rbe() const { return far && (coul_type == "RBE" || coul_type == "EWALD"); }
+  bool is_eam() const { return ff == "EAM"; }
+  bool is_cvff() const { return ff == "CVFF"; }
+  bool with_coul_near() const { return far && ff != "EAM"; }
+  double list_cut() const { return rc + skin; }
+};
+
+namespace {
+
+// phases: 0 integrate, 1 cell sort, 2 k-space (side stream), 3 neighbour list, 4 force pass,
+// 5 constraints + intramolecular terms
+enum Phase { kPhInt = 0, kPhSort = 1, kPhK = 2, kPhList = 3, kPhForce = 4, kPhMol = 5 };
+
+cudaEvent_t prof_event(rbmd_force* f) {
+  if (f->ev_used == f->ev_pool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    f->ev_pool.push_back(e);
+  }
+  return f->ev_pool[f->ev_used++];
+}
+struct PhaseScope {
+  rbmd_force* f;
+  int ph;
+  cudaStream_t s;
+  cudaEvent_t a = nullptr;
+  PhaseScope(rbmd_force* f_, int ph_, cudaStream_t s_) : f(f_), ph(ph_), s(s_) {
+    if (f->prof_on) {
+      a = prof_event(f);
+      cudaEventRecord(a, s);
+    }
+  }
+  ~PhaseScope() {
+    if (f->prof_on) {
+      cudaEvent_t b = prof_event(f);
+      cudaEventRecord(b, s);
+      f->prof_pairs.push_back({ph, {a, b}});
+    }
+  }
+};
+// after the stream has been synchronised
+void prof_collect(rbmd_force* f) {
+  for (auto& p : f->prof_pairs) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, p.second.first, p.second.second) == cudaSuccess) {
+      f->phase_ms[p.first] += ms;
+      f->phase_n[p.first] += 1;
+    }
+  }
+  f->prof_pairs.clear();
+  f->ev_used = 0;
+}
+
+void free_all(rbmd_force* f) {
+  dfree(f->d_reps); dfree(f->d_ljt);
+  dfree(f->d_rep_of); dfree(f->d_cell_of); dfree(f->d_cell_count); dfree(f->d_cell_start);
+  dfree(f->d_cursor); dfree(f->d_tmp); dfree(f->d_slot_atom); dfree(f->d_atom_slot);
+  if (f->d_pos4) cudaFree(f->d_pos4);
+  f->d_pos4 = nullptr;
+  if (f->d_frac) cudaFree(f->d_frac);
+  f->d_frac = nullptr;
+  dfree(f->d_meta); dfree(f->d_nbr); dfree(f->d_count); dfree(f->d_maxcount); dfree(f->d_status);
+  dfree(f->d_eslot); dfree(f->d_esum);
+  if (f->d_krec) cudaFree(f->d_krec);
+  f->d_krec = nullptr;
+  dfree(f->d_kvec); dfree(f->d_items); dfree(f->d_rhorep);
+  if (f->d_partial) cudaFree(f->d_partial);
+  f->d_partial = nullptr;
+  dfree(f->d_rho); dfree(f->d_ek); dfree(f->d_weights); dfree(f->d_srep); dfree(f->d_qtab);
+  dfree(f->d_chunks); dfree(f->d_chunk_rep_begin); dfree(f->d_ke_partial); dfree(f->d_ke);
+  dfree(f->d_T); dfree(f->d_lambda); dfree(f->d_xi); dfree(f->d_xold); dfree(f->d_vold);
+  dfree(f->d_frho); dfree(f->d_rhor); dfree(f->d_z2r);
+  if (f->d_fp) cudaFree(f->d_fp);
+  f->d_fp = nullptr;
+  dfree(f->d_emb); dfree(f->d_epair); dfree(f->d_hoh); dfree(f->d_ebond); dfree(f->d_eangle);
+  dfree(f->d_snap); dfree(f->d_snap_img);
+  if (f->h_status) cudaFreeHost(f->h_status);
+  f->h_status = nullptr;
+  if (f->h_maxcount) cudaFreeHost(f->h_maxcount);
+  f->h_maxcount = nullptr;
+  if (f->side) cudaStreamDestroy(f->side);
+  f->side = nullptr;
+  for (auto e : f->ev_pool) cudaEventDestroy(e);
+  f->ev_pool.clear();
+  f->ev_used = 0;
+  f->prof_pairs.clear();
+  if (f->ev_fork) cudaEventDestroy(f->ev_fork);
+  if (f->ev_join) cudaEventDestroy(f->ev_join);
+  f->ev_fork = f->ev_join = nullptr;
+}
+
+// Replica geometry: ContPointLocator::SetRange/SetCutOff/SetRs in the reference's float
+// arithmetic (ContPointLocator.h:44-73) for FP32 mode, and the same formulas in double for FP64.
+void setup_replica(const rbmd_box& b, double cut, double rs, bool fp64, RepDev& r, int& ncyc) {
+  std::memset(&r, 0, sizeof r);
+  const float rcf = (float)cut, rsf = (float)rs;
+  ncyc = fp64 ? (int)std::ceil(cut / rs) : (int)std::ceil(rcf / rsf);
+  for (int d = 0; d < 3; ++d) {
+    r.lo_f[d] = (float)b.lo[d];
+    r.hi_f[d] = (float)b.hi[d];
+    const float span = r.hi_f[d] - r.lo_f[d];
+    r.lo_d[d] = b.lo[d];
+    r.hi_d[d] = b.hi[d];
+    r.box_d[d] = b.hi[d] - b.lo[d];
+    int dims = fp64 ? (int)(r.box_d[d] / (cut / (double)ncyc)) : (int)(span / (rcf / (float)ncyc));
+    if (dims < 1) dims = 1;
+    r.dims[d] = dims;
+    r.box_f[d] = span;
+    r.dx_f[d] = span / (float)dims;
+    r.wrap_f[d] = r.dx_f[d] * (float)dims;
+    r.dx_d[d] = r.box_d[d] / (double)dims;
+    r.wrap_d[d] = r.dx_d[d] * (double)dims;
+  }
+  r.volume = r.box_d[0] * r.box_d[1] * r.box_d[2];
+  r.ncell = r.dims[0] * r.dims[1] * r.dims[2];
+}
+
+// RBE normaliser S = prod_d H_d - 1 with H_d = sqrt(a L^2/pi) sum_{|m|<=10} e^{-a L^2 m^2}
+// (ExecForceFunction::Compute_S/Compute_H, rbmd/framework/forceFunction/ExecForceFunction.h:266-294),
+// evaluated in FP64.
+double rbe_S(double alpha, const double* L) {
+  double H[3];
+  for (int i = 0; i < 3; ++i) {
+    const double factor = -(alpha * L[i] * L[i]);
+    double h = 0;
+    for (int m = -10; m <= 10; ++m) h += std::exp((double)(m * m) * factor);
+    H[i] = h * std::sqrt(-factor / M_PI);
+  }
+  return H[0] * H[1] * H[2] - 1.0;
+}
+
+template <class R>
+void launch_nlist(rbmd_force* f, cudaStream_t s) {
+  PhaseScope ps(f, kPhList, s);
+  const int nb = (f->n + 127) / 128;
+  k_nlist<R><<<nb, 128, 0, s>>>(f->n, (const typename Traits<R>::V4*)f->d_pos4, f->d_cell_start,
+                                f->d_reps, f->nrep > 1 ? f->d_rep_of : nullptr, f->num_cycles,
+                                (R)f->list_cut(), f->cap, f->stride, f->d_nbr, f->d_count,
+                                f->d_maxcount, f->d_status);
+  f->launches++;
+}
+
+template <class R>
+void launch_sort(rbmd_force* f, cudaStream_t s, bool bin) {
+  PhaseScope ps(f, kPhSort, s);
+  const int n = f->n;
+  if (bin) {
+    cudaMemsetAsync(f->d_cell_count, 0, sizeof(int) * f->ncell_total, s);
+    k_bin<R><<<(n + 255) / 256, 256, 0, s>>>(n, f->at.pos, f->nrep > 1 ? f->d_rep_of : nullptr,
+                                             f->d_reps, f->d_cell_of, f->d_cell_count, f->d_status);
+    f->launches++;
+  }
+  k_scan_cells<<<1, 1024, 0, s>>>(f->ncell_total, f->d_cell_count, f->d_cell_start, f->d_cursor,
+                                  f->d_status);
+  k_scatter<<<(n + 255) / 256, 256, 0, s>>>(n, f->d_cell_of, f->d_cell_start, f->d_cursor, f->d_tmp);
+  k_cell_sort_gather<R><<<(f->ncell_total + 7) / 8, 256, 0, s>>>(
+      f->ncell_total, f->d_cell_start, f->d_tmp, f->at.pos, f->at.charge, f->at.type, f->at.molecule,
+      f->nrep > 1 ? f->d_rep_of : nullptr, f->d_reps, f->d_slot_atom, f->d_atom_slot,
+      (typename Traits<R>::V4*)f->d_pos4, f->is_rbe() ? f->d_frac : nullptr, f->d_meta);
+  f->launches += 3;
+}
+
+template <class R>
+void launch_regather(rbmd_force* f, cudaStream_t s) {
+  k_regather<R><<<(f->n + 255) / 256, 256, 0, s>>>(
+      f->n, f->d_slot_atom, f->at.pos, f->at.charge, f->nrep > 1 ? f->d_rep_of : nullptr, f->d_reps,
+      (typename Traits<R>::V4*)f->d_pos4, f->is_rbe() ? f->d_frac : nullptr);
+  f->launches++;
+}
+
+template <class R>
+void launch_kspace(rbmd_force* f, cudaStream_t s) {
+  if (!f->is_rbe()) return;
+  PhaseScope ps(f, kPhK, s);
+  const int rec_bytes = sizeof(typename KRec<R>::T);
+  if (!f->injected && f->coul_type == "RBE") {
+    k_sample<kSamplerD><<<f->nrep, 256, 0, s>>>(f->nrep, f->d_srep, f->d_qtab, f->d_reps, f->seed,
+                                                f->step_count, f->d_kvec, f->d_krec, rec_bytes,
+                                                f->d_status);
+    f->launches++;
+  }
+  if (sizeof(R) == 4)
+    k_rho_partial32<kKT><<<f->nitems, 256, 0, s>>>(f->d_items, (const Frac32*)f->d_frac,
+                                                  (const KRec32*)f->d_krec, (float2*)f->d_partial);
+  else
+    k_rho_partial64<kKT><<<f->nitems, 256, 0, s>>>(f->d_items, (const Frac64*)f->d_frac,
+                                                  (const KRec64*)f->d_krec, (double2*)f->d_partial);
+  k_rho_finish<R, kKT><<<(f->Ptot + 127) / 128, 128, 0, s>>>(
+      f->Ptot, f->d_rhorep, f->d_reps, f->d_partial, f->d_weights, f->u.qqr2e,
+      (typename KRec<R>::T*)f->d_krec, f->d_rho, f->d_ek);
+  f->launches += 2;
+}
+
+template <class R, bool LJ, bool COUL, bool RBE, bool MOLEC>
+void launch_near_t(rbmd_force* f, cudaStream_t s) {
+  NearParams p;
+  p.n = f->n;
+  p.stride = f->stride;
+  p.ntypes = f->ntypes;
+  p.with_lj = LJ;
+  p.with_coul = COUL;
+  p.molecular = MOLEC;
+  p.rc = f->rc;
+  p.alpha = f->alpha;
+  p.coul_scale = f->near_coul_scale;
+  p.sqrt_alpha = std::sqrt(f->alpha);
+  p.two_sqrt_alpha_over_sqrt_pi = 2.0 * std::sqrt(f->alpha) / std::sqrt(M_PI);
+  k_near_force<R, LJ, COUL, RBE, MOLEC><<<(f->n + 127) / 128, 128, 0, s>>>(
+      p, f->d_ljt, (const typename Traits<R>::V4*)f->d_pos4, f->d_meta, f->d_nbr, f->d_count,
+      f->d_reps, f->nrep > 1 ? f->d_rep_of : nullptr, f->d_slot_atom,
+      (const typename FracT<R>::T*)f->d_frac, (const typename KRec<R>::T*)f->d_krec, f->at.force,
+      f->d_eslot, f->d_status);
+  f->launches++;
+}
+
+template <class R>
+void launch_near(rbmd_force* f, cudaStream_t s) {
+  const bool rbe = f->is_rbe();
+  const bool coul = f->with_coul_near();
+  const bool molec = f->at.molecule != nullptr;
+  if (!coul) {
+    if (molec) launch_near_t<R, true, false, false, true>(f, s);
+    else launch_near_t<R, true, false, false, false>(f, s);
+  } else if (rbe) {
+    if (molec) launch_near_t<R, true, true, true, true>(f, s);
+    else launch_near_t<R, true, true, true, false>(f, s);
+  } else {
+    if (molec) launch_near_t<R, true, true, false, true>(f, s);
+    else launch_near_t<R, true, true, false, false>(f, s);
+  }
+}
+
+template <class R>
+void launch_eam(rbmd_force* f, cudaStream_t s) {
+  EamDev e;
+  e.frho = f->d_frho;
+  e.rhor = f->d_rhor;
+  e.z2r = f->d_z2r;
+  e.nrho = f->eam_h.nrho;
+  e.nr = f->eam_h.nr;
+  e.rdr = 1.0f / f->eam_h.dr;
+  e.rdrho = 1.0f / f->eam_h.drho;
+  e.rdr_d = 1.0 / (double)f->eam_h.dr;
+  e.rdrho_d = 1.0 / (double)f->eam_h.drho;
+  e.rhomax = f->eam_h.rhomax;
+  const int nb = (f->n + 127) / 128;
+  k_eam_fp<R><<<nb, 128, 0, s>>>(f->n, f->stride, f->rc, e, (const typename Traits<R>::V4*)f->d_pos4,
+                                 f->d_nbr, f->d_count, f->d_reps, f->nrep > 1 ? f->d_rep_of : nullptr,
+                                 (R*)f->d_fp, f->d_emb);
+  k_eam_force<R><<<nb, 128, 0, s>>>(f->n, f->stride, f->rc, e, (const typename Traits<R>::V4*)f->d_pos4,
+                                    f->d_nbr, f->d_count, f->d_reps, f->nrep > 1 ? f->d_rep_of : nullptr,
+                                    (const R*)f->d_fp, f->d_slot_atom, f->at.force, f->d_epair,
+                                    f->d_status);
+  f->launches += 2;
+}
+
+void launch_water(rbmd_force* f, cudaStream_t s) {
+  if (!f->is_cvff() || f->n_mol == 0) return;
+  WaterParams wp;
+  wp.n_mol = (int)f->n_mol;
+  wp.bond_k = f->bond_k;
+  wp.bond_r0 = f->bond_r0;
+  wp.angle_k = f->angle_k;
+  wp.angle_theta0_rad = f->angle_t0 * M_PI / 180.0;
+  wp.coul_const = 332.06371;
+  k_water_extras<<<(wp.n_mol + 127) / 128, 128, 0, s>>>(wp, f->d_hoh, f->at.pos, f->at.charge,
+                                                        f->nrep > 1 ? f->d_rep_of : nullptr, f->d_reps,
+                                                        f->at.force, f->d_ebond, f->d_eangle);
+  f->launches++;
+}
+
+// Force evaluation after the slot caches are current: list, k-space (side stream), pair pass.
+template <class R>
+void launch_force_tail(rbmd_force* f, cudaStream_t s) {
+  const bool kspace = f->is_rbe();
+  if (kspace) {
+    cudaEventRecord(f->ev_fork, s);
+    cudaStreamWaitEvent(f->side, f->ev_fork, 0);
+    launch_kspace<R>(f, f->side);
+    cudaEventRecord(f->ev_join, f->side);
+  }
+  launch_nlist<R>(f, s);
+  if (kspace) cudaStreamWaitEvent(s, f->ev_join, 0);
+  {
+    PhaseScope ps(f, kPhForce, s);
+    if (f->is_eam()) launch_eam<R>(f, s);
+    else launch_near<R>(f, s);
+  }
+  {
+    PhaseScope ps(f, kPhMol, s);
+    launch_water(f, s);
+  }
+}
+
+template <class R>
+void launch_compute(rbmd_force* f, cudaStream_t s) {
+  cudaMemsetAsync(f->d_maxcount, 0, sizeof(int), s);
+  launch_sort<R>(f, s, true);
+  launch_force_tail<R>(f, s);
+}
+
+void launch_compute_any(rbmd_force* f, cudaStream_t s) {
+  if (f->fp64) launch_compute<double>(f, s);
+  else launch_compute<float>(f, s);
+}
+
+rbmd_status grow_list(rbmd_force* f, int need) {
+  const int newcap = ((int)(need * 1.2) + 8 + 7) & ~7;
+  dfree(f->d_nbr);
+  CK(dalloc(&f->d_nbr, (size_t)newcap * f->stride));
+  f->cap = newcap;
+  return RBMD_OK;
+}
+
+// Check the list-capacity flag after a launch sequence; returns 1 when the work must be redone.
+rbmd_status check_overflow(rbmd_force* f, cudaStream_t s, bool* redo) {
+  *redo = false;
+  CK(cudaMemcpyAsync(f->h_status, f->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(f->h_maxcount, f->d_maxcount, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  prof_collect(f);
+  if (*f->h_status & kFlagListOverflow) {
+    rbmd_status st = grow_list(f, *f->h_maxcount);
+    if (st) return st;
+    uint32_t clr = *f->h_status & ~kFlagListOverflow;
+    CK(cudaMemcpyAsync(f->d_status, &clr, sizeof clr, cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    *redo = true;
+  }
+  return RBMD_OK;
+}
+
+template <class R>
+void launch_step(rbmd_force* f, cudaStream_t s) {
+  const int n = f->n;
+  const bool shake = f->shake == "true" && f->n_mol > 0;
+  MdParams mp;
+  mp.n = n;
+  mp.dt = f->dt;
+  mp.fmt2v = f->u.fmt2v;
+  mp.wrap_flags = (f->shake == "null" || f->init_way == "inbuild") ? 1 : 0;
+  mp.save_old = shake ? 1 : 0;
+  mp.apply_scale = f->pending_scale ? 1 : 0;
+  mp.nh = f->tstat == 3;
+  cudaMemsetAsync(f->d_maxcount, 0, sizeof(int), s);
+  cudaMemsetAsync(f->d_cell_count, 0, sizeof(int) * f->ncell_total, s);
+  // stages 1-2: kick, drift + wrap, bin (binning sees the unconstrained positions, as the
+  // reference's locator.SetPosition runs before ConstraintA)
+  {
+    PhaseScope ps(f, kPhInt, s);
+    k_kick_drift<R><<<(n + 255) / 256, 256, 0, s>>>(mp, f->at.pos, f->at.vel, f->at.force, f->at.mass,
+                                                    f->at.image, f->nrep > 1 ? f->d_rep_of : nullptr,
+                                                    f->d_reps, f->d_lambda, f->d_xold, f->d_vold,
+                                                    f->d_cell_of, f->d_cell_count, f->d_status);
+    f->launches++;
+  }
+  launch_sort<R>(f, s, false);
+  if (shake) {
+    PhaseScope ps(f, kPhMol, s);
+    ShakeParams sp;
+    sp.n_mol = (int)f->n_mol;
+    sp.dt = f->dt;
+    sp.fmt2v = f->u.fmt2v;
+    sp.tol = f->shake_tol;
+    sp.max_iter = f->shake_max_iter;
+    k_shake<<<(sp.n_mol + 127) / 128, 128, 0, s>>>(sp, f->d_hoh, f->at.pos, f->at.vel, f->d_xold,
+                                                  f->d_vold, f->at.force, f->at.mass, f->at.image,
+                                                  f->nrep > 1 ? f->d_rep_of : nullptr, f->d_reps,
+                                                  f->d_status);
+    f->launches++;
+    launch_regather<R>(f, s);
+  }
+  // stage 3: force
+  launch_force_tail<R>(f, s);
+  // stage 3: kick (+ RATTLE), temperature, thermostat
+  PhaseScope ps_int(f, kPhInt, s);
+  if (shake) {
+    k_kick_ke<<<f->nchunks, 256, 0, s>>>(mp, f->d_chunks, f->at.vel, f->at.force, f->at.mass, 1,
+                                        nullptr, nullptr);
+    k_rattle<<<((int)f->n_mol + 127) / 128, 128, 0, s>>>((int)f->n_mol, f->d_hoh, f->at.pos, f->at.vel,
+                                                         f->at.mass, f->nrep > 1 ? f->d_rep_of : nullptr,
+                                                         f->d_reps, f->d_status);
+    k_kick_ke<<<f->nchunks, 256, 0, s>>>(mp, f->d_chunks, f->at.vel, f->at.force, f->at.mass, 0,
+                                        nullptr, f->d_ke_partial);
+    f->launches += 3;
+  } else {
+    k_kick_ke<<<f->nchunks, 256, 0, s>>>(mp, f->d_chunks, f->at.vel, f->at.force, f->at.mass, 1,
+                                        nullptr, f->d_ke_partial);
+    f->launches++;
+  }
+  if (f->tstat == 3) {
+    k_kick_ke<<<f->nchunks, 256, 0, s>>>(mp, f->d_chunks, f->at.vel, f->at.force, f->at.mass, 2,
+                                        f->d_xi, nullptr);
+    f->launches++;
+  }
+  ThermoParams tp;
+  tp.nrep = f->nrep;
+  tp.tstat = f->tstat;
+  tp.mvv2e = f->u.mvv2e;
+  tp.kB = f->u.kB;
+  tp.dt = f->dt;
+  tp.Tdamp = f->Tdamp;
+  tp.T0 = f->T0;
+  tp.dof_mode = f->dof_mode;
+  k_thermo<<<(f->nrep + 127) / 128, 128, 0, s>>>(tp, f->d_chunk_rep_begin, f->d_ke_partial, f->d_ke,
+                                                f->d_T, f->d_lambda, f->d_xi, f->d_reps);
+  f->launches++;
+  f->pending_scale = (f->tstat == 1 || f->tstat == 2);
+  f->step_count++;
+}
+
+rbmd_status parse_config(rbmd_force* f, const char* text) {
+  rbmdjson::Value root;
+  std::string err;
+  if (!text || !rbmdjson::parse(text, root, err)) {
+    std::snprintf(g_last_error, sizeof g_last_error, "config: %s", err.c_str());
+    return RBMD_ERR_CONFIG;
+  }
+  using namespace rbmdjson;
+  f->ff = rbmdjson::text(root, "hyper_parameters.force_field.type", "LJ/CUT");
+  f->potential_file = rbmdjson::text(root, "hyper_parameters.force_field.potential_file", "");
+  f->nbr_type = rbmdjson::text(root, "hyper_parameters.neighbor.type", "VERLETLIST");
+  if (f->nbr_type == "VERLET-LIST") f->nbr_type = "VERLETLIST";
+  bool found = false;
+  f->rc = num(root, "hyper_parameters.neighbor.cut_off", 0.0, &found);
+  if (!found || f->rc <= 0) {
+    std::snprintf(g_last_error, sizeof g_last_error, "config: neighbor.cut_off missing");
+    return RBMD_ERR_CONFIG;
+  }
+  f->rs = f->nbr_type == "RBL" ? num(root, "hyper_parameters.neighbor.r_core", f->rc) : f->rc;
+  f->skin = num(root, "hyper_parameters.neighbor.skin", 0.0);
+  f->far = root.path("hyper_parameters.coulomb") != nullptr;
+  if (f->far) {
+    f->coul_type = rbmdjson::text(root, "hyper_parameters.coulomb.type", "RBE");
+    f->P = (int)num(root, "hyper_parameters.coulomb.coulomb_sample_num", 100);
+    f->alpha = num(root, "hyper_parameters.coulomb.alpha", 0.1);
+    f->kmax = (int)num(root, "hyper_parameters.coulomb.kmax", 2);
+    f->seed = (unsigned long long)num(root, "hyper_parameters.coulomb.seed", 20240101.0);
+  }
+  f->shake = rbmdjson::text(root, "hyper_parameters.extend.fix_shake", "null");
+  f->shake_tol = num(root, "hyper_parameters.extend.shake_tolerance", 1e-5);
+  f->shake_max_iter = (int)num(root, "hyper_parameters.extend.shake_max_iter", 5000);
+  std::string prec = rbmdjson::text(root, "precision", "fp32");
+  f->fp64 = prec == "fp64" || prec == "FP64" || prec == "double";
+  if (root.path("init_configuration.inbuild")) {
+    f->init_way = "inbuild";
+    f->unit = rbmdjson::text(root, "init_configuration.inbuild.unit", "LJ");
+  } else {
+    f->init_way = "read_data";
+    f->unit = rbmdjson::text(root, "init_configuration.read_data.unit", "LJ");
+  }
+  f->u = units_for(f->unit);
+  f->dt = num(root, "execution.timestep", 0.005);
+  std::vector<double> T = nums(root, "execution.temperature");
+  f->T0 = T.size() > 0 ? T[0] : 1.0;
+  f->Tdamp = T.size() > 2 ? T[2] : 1.0;
+  std::string ens = rbmdjson::text(root, "execution.ensemble", "NVT");
+  f->tctrl = rbmdjson::text(root, "execution.temp_ctrl_type", "");
+  f->tstat = 0;
+  if (ens != "NVE") {
+    if (f->tctrl == "BERENDSEN") f->tstat = 1;
+    else if (f->tctrl == "TEMP_RESCALE") f->tstat = 2;
+    else if (f->tctrl == "NOSE_HOOVER") f->tstat = 3;
+  }
+  if (f->init_way == "inbuild") f->dof_mode = 3;
+  else if (f->shake == "true") f->dof_mode = 1;
+  else if (f->shake == "false") f->dof_mode = 2;
+  else f->dof_mode = 0;
+  // The Verlet-list near Coulomb of the reference omits qqr2e (RunWorklet.cpp:218,233) while its
+  // RBL path applies it (:807).  Default: physical force (x qqr2e); compat flag restores the
+  // reference's Verlet behaviour.
+  bool compat_noq = false;
+  const Value* c = root.path("compat.verlet_coul_no_qqr2e");
+  if (c && c->kind == Value::Bool) compat_noq = c->b;
+  f->near_coul_scale = compat_noq ? 1.0 : f->u.qqr2e;
+  if (f->ff != "LJ/CUT" && f->ff != "LJ/CUT/COUL/LONG" && f->ff != "CVFF" && f->ff != "EAM") {
+    std::snprintf(g_last_error, sizeof g_last_error, "config: unknown force_field.type %s", f->ff.c_str());
+    return RBMD_ERR_CONFIG;
+  }
+  if (f->ff == "LJ/CUT" || f->ff == "EAM") f->far = false;
+  if (f->far && f->coul_type != "RBE" && f->coul_type != "EWALD") {
+    std::snprintf(g_last_error, sizeof g_last_error, "config: unknown coulomb.type %s", f->coul_type.c_str());
+    return RBMD_ERR_CONFIG;
+  }
+  if (f->nbr_type != "VERLETLIST") {
+    std::snprintf(g_last_error, sizeof g_last_error,
+                  "config: neighbor.type %s is not provided by this build (VERLETLIST only)",
+                  f->nbr_type.c_str());
+    return RBMD_ERR_CONFIG;
+  }
+  if (f->P < 1 || f->P > 65536) return RBMD_ERR_CONFIG;
+  return RBMD_OK;
+}
+
+// Per-type LJ tables in the reference's float arithmetic: -24*sqrt(eps_i*eps_j) and
+// ((sigma_i + sigma_j)/2)^6 as ComputeLJForce forms them (ExecForceFunction.h:74-96).
+void fill_lj(rbmd_force* f, int nt, const double* eps, const double* sig) {
+  f->ntypes = nt;
+  for (int a = 0; a < nt; ++a)
+    for (int b = 0; b < nt; ++b) {
+      const float ea = (float)eps[a], eb = (float)eps[b], sa = (float)sig[a], sb = (float)sig[b];
+      const float sij = (sa + sb) / 2;
+      f->ljt_h.lj24_f[a * nt + b] = (float)(-24) * std::sqrt(ea * eb);
+      f->ljt_h.sig6_f[a * nt + b] = sij * sij * sij * sij * sij * sij;
+      const double sd = (sig[a] + sig[b]) / 2;
+      f->ljt_h.lj24_d[a * nt + b] = -24.0 * std::sqrt(eps[a] * eps[b]);
+      f->ljt_h.sig6_d[a * nt + b] = sd * sd * sd * sd * sd * sd;
+    }
+}
+
+rbmd_status upload_ksamples(rbmd_force* f, const int32_t* m_xyz) {
+  const int recb = f->fp64 ? sizeof(KRec64) : sizeof(KRec32);
+  std::vector<char> buf((size_t)f->Ptot * recb, 0);
+  for (int g = 0; g < f->Ptot; ++g) {
+    int* rec = reinterpret_cast<int*>(buf.data() + (size_t)g * recb);
+    rec[0] = m_xyz[3 * g];
+    rec[1] = m_xyz[3 * g + 1];
+    rec[2] = m_xyz[3 * g + 2];
+    rec[3] = g / f->P;
+    if (rec[0] == 0 && rec[1] == 0 && rec[2] == 0) return RBMD_ERR_ARG;
+  }
+  CK(cudaMemcpy(f->d_krec, buf.data(), buf.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(f->d_kvec, m_xyz, sizeof(int) * 3 * f->Ptot, cudaMemcpyHostToDevice));
+  f->injected = true;
+  return RBMD_OK;
+}
+
+}  // namespace
+
+// ==========================================================================================
+// C ABI
+// ==========================================================================================
+extern "C" {
+
+const char* rbmd_version(void) { return "rbmd-b200 0.1 (sm_100a)"; }
+
+const char* rbmd_last_error(void) { return g_last_error; }
+
+rbmd_status rbmd_force_create(const char* json_text, int32_t n_replicas, const rbmd_box* boxes,
+                              rbmd_force** out) {
+  if (!out || !boxes || n_replicas < 1) return RBMD_ERR_ARG;
+  *out = nullptr;
+  rbmd_force* f = new rbmd_force();
+  rbmd_status st = parse_config(f, json_text);
+  if (st) { delete f; return st; }
+  f->nrep = n_replicas;
+  f->boxes.assign(boxes, boxes + n_replicas);
+  for (int r = 0; r < n_replicas; ++r)
+    for (int d = 0; d < 3; ++d)
+      if (!(boxes[r].hi[d] > boxes[r].lo[d])) { delete f; return RBMD_ERR_ARG; }
+  const double one = 1.0;
+  fill_lj(f, 1, &one, &one);
+  if (f->is_eam() && !f->potential_file.empty()) {
+    if (funcfl_load(f->potential_file, f->eam_h) != 0) {
+      std::snprintf(g_last_error, sizeof g_last_error, "cannot read funcfl file %s",
+                    f->potential_file.c_str());
+      delete f;
+      return RBMD_ERR_FILE;
+    }
+    f->eam_loaded = true;
+  }
+  *out = f;
+  return RBMD_OK;
+}
+
+rbmd_status rbmd_force_set_pair_coeffs(rbmd_force* f, int32_t n_types, const double* epsilon,
+                                       const double* sigma) {
+  if (!f || !epsilon || !sigma || n_types < 1 || n_types > kMaxReplicaTypes) return RBMD_ERR_ARG;
+  fill_lj(f, n_types, epsilon, sigma);
+  f->have_pair_coeffs = true;
+  if (f->d_ljt) CK(cudaMemcpy(f->d_ljt, &f->ljt_h, sizeof(LJTable), cudaMemcpyHostToDevice));
+  return RBMD_OK;
+}
+
+rbmd_status rbmd_force_load_funcfl(rbmd_force* f, const char* path) {
+  if (!f || !path) return RBMD_ERR_ARG;
+  if (funcfl_load(path, f->eam_h) != 0) return RBMD_ERR_FILE;
+  f->eam_loaded = true;
+  f->potential_file = path;
+  return RBMD_OK;
+}
+
+rbmd_status rbmd_force_set_water(rbmd_force* f, int64_t n_mol, const int32_t* hoh, double bond_k,
+                                 double bond_r0, double angle_k, double angle_theta0_deg) {
+  if (!f || n_mol < 0 || (n_mol > 0 && !hoh)) return RBMD_ERR_ARG;
+  f->n_mol = n_mol;
+  f->hoh_h.assign(hoh, hoh + 3 * n_mol);
+  f->bond_k = bond_k;
+  f->bond_r0 = bond_r0;
+  f->angle_k = angle_k;
+  f->angle_t0 = angle_theta0_deg;
+  if (f->bound) {
+    dfree(f->d_hoh);
+    CK(dalloc(&f->d_hoh, (size_t)3 * n_mol));
+    CK(cudaMemcpy(f->d_hoh, f->hoh_h.data(), sizeof(int) * 3 * n_mol, cudaMemcpyHostToDevice));
+    dfree(f->d_ebond); dfree(f->d_eangle);
+    CK(dalloc(&f->d_ebond, (size_t)n_mol));
+    CK(dalloc(&f->d_eangle, (size_t)n_mol));
+  }
+  return RBMD_OK;
+}
+
+rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
+  if (!f || !a || a->n_atoms < 1 || !a->pos || !a->force) return RBMD_ERR_ARG;
+  if (a->n_atoms >= (1LL << (31 - kShiftBits))) return RBMD_ERR_ARG;
+  const int nrep = a->n_replicas < 1 ? 1 : a->n_replicas;
+  if (nrep != f->nrep) return RBMD_ERR_ARG;
+  if (f->is_eam() && !f->eam_loaded) return RBMD_ERR_STATE;
+  free_all(f);
+  f->at = *a;
+  f->n = (int)a->n_atoms;
+  f->rep_off.assign(nrep + 1, 0);
+  if (nrep == 1) {
+    f->rep_off[1] = f->n;
+  } else {
+    if (!a->replica_offsets) return RBMD_ERR_ARG;
+    for (int r = 0; r <= nrep; ++r) f->rep_off[r] = a->replica_offsets[r];
+    if (f->rep_off[0] != 0 || f->rep_off[nrep] != f->n) return RBMD_ERR_ARG;
+    for (int r = 0; r < nrep; ++r)
+      if (f->rep_off[r + 1] <= f->rep_off[r]) return RBMD_ERR_ARG;
+  }
+  f->at.replica_offsets = nullptr;
+  // replica geometry, cells and k ranges
+  f->reps_h.assign(nrep, RepDev{});
+  int cell_base = 0;
+  for (int r = 0; r < nrep; ++r) {
+    RepDev& rp = f->reps_h[r];
+    int ncyc = 1;
+    setup_replica(f->boxes[r], f->list_cut(), f->nbr_type == "RBL" ? f->rs : f->list_cut(), f->fp64, rp,
+                  ncyc);
+    f->num_cycles = ncyc;
+    rp.cell_base = cell_base;
+    cell_base += rp.ncell;
+    rp.atom_begin = (int)f->rep_off[r];
+    rp.atom_end = (int)f->rep_off[r + 1];
+    rp.P = f->P;
+    rp.k_begin = r * f->P;
+    double L[3] = {rp.box_d[0], rp.box_d[1], rp.box_d[2]};
+    rp.S = rbe_S(f->alpha, L);
+  }
+  f->ncell_total = cell_base;
+  f->stride = (f->n + 31) & ~31;
+  // list capacity from the densest replica (reference: rho * ceil(4/3 pi rc^3) + 1,
+  // ExecutionMD.cpp:683); a margin absorbs fluctuations, overflow triggers regrowth.
+  double rho_max = 0;
+  for (int r = 0; r < nrep; ++r)
+    rho_max = std::max(rho_max, (f->rep_off[r + 1] - f->rep_off[r]) / f->reps_h[r].volume);
+  const double lc = f->list_cut();
+  f->cap = ((int)(1.5 * rho_max * 4.0 / 3.0 * M_PI * lc * lc * lc) + 32 + 7) & ~7;
+  const size_t n = f->n;
+  const bool fp64 = f->fp64;
+  CK(dalloc(&f->d_reps, nrep));
+  CK(cudaMemcpy(f->d_reps, f->reps_h.data(), sizeof(RepDev) * nrep, cudaMemcpyHostToDevice));
+  CK(dalloc(&f->d_ljt, 1));
+  CK(cudaMemcpy(f->d_ljt, &f->ljt_h, sizeof(LJTable), cudaMemcpyHostToDevice));
+  std::vector<int> rep_of(n);
+  for (int r = 0; r < nrep; ++r)
+    for (int64_t i = f->rep_off[r]; i < f->rep_off[r + 1]; ++i) rep_of[i] = r;
+  CK(dalloc(&f->d_rep_of, n));
+  CK(cudaMemcpy(f->d_rep_of, rep_of.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+  CK(dalloc(&f->d_cell_of, n));
+  CK(dalloc(&f->d_cell_count, (size_t)f->ncell_total));
+  CK(dalloc(&f->d_cell_start, (size_t)f->ncell_total + 1));
+  CK(dalloc(&f->d_cursor, (size_t)f->ncell_total));
+  CK(dalloc(&f->d_tmp, n));
+  CK(dalloc(&f->d_slot_atom, n));
+  CK(dalloc(&f->d_atom_slot, n));
+  CK(cudaMalloc(&f->d_pos4, n * (fp64 ? sizeof(double4) : sizeof(float4))));
+  CK(dalloc(&f->d_meta, n));
+  CK(dalloc(&f->d_nbr, (size_t)f->cap * f->stride));
+  CK(dalloc(&f->d_count, n));
+  CK(dalloc(&f->d_maxcount, 1));
+  CK(dalloc(&f->d_status, 1));
+  CK(cudaMemset(f->d_status, 0, sizeof(uint32_t)));
+  CK(dalloc(&f->d_eslot, 2 * n));
+  CK(cudaMemset(f->d_eslot, 0, sizeof(double) * 2 * n));
+  CK(dalloc(&f->d_esum, 32));
+  CK(cudaMallocHost(&f->h_status, sizeof(uint32_t)));
+  CK(cudaMallocHost(&f->h_maxcount, sizeof(int)));
+  CK(cudaStreamCreateWithFlags(&f->side, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&f->ev_fork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&f->ev_join, cudaEventDisableTiming));
+  // host-side range checks: every device index derived from these arrays stays in bounds
+  if (a->type) {
+    std::vector<int> ty(n);
+    CK(cudaMemcpy(ty.data(), a->type, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    for (int v : ty)
+      if (v < 0 || v >= f->ntypes) {
+        std::snprintf(g_last_error, sizeof g_last_error, "atom type %d outside [0, %d)", v, f->ntypes);
+        return RBMD_ERR_ARG;
+      }
+  }
+  for (int32_t v : f->hoh_h)
+    if (v < 0 || v >= f->n) {
+      std::snprintf(g_last_error, sizeof g_last_error, "water atom id %d outside [0, %d)", v, f->n);
+      return RBMD_ERR_ARG;
+    }
+  // charges: sum q^2 for the self energy
+  f->sum_q2 = 0;
+  if (a->charge) {
+    std::vector<double> q(n);
+    CK(cudaMemcpy(q.data(), a->charge, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    for (double v : q) f->sum_q2 += v * v;
+  }
+  // k-space
+  if (f->is_rbe()) {
+    CK(cudaMalloc(&f->d_frac, n * (fp64 ? sizeof(Frac64) : sizeof(Frac32))));
+    const int recb = fp64 ? sizeof(KRec64) : sizeof(KRec32);
+    if (f->coul_type == "EWALD") {
+      // EWALD: the cube m in [-kmax, kmax]^3 \ {0} (ExecPointLocator::ExecuteOnKNeighbor,
+      // ExecPointLocator.h:127-145) as a fixed sample set with weights e^{-k^2/4a} and S/P = 1.
+      const int K = f->kmax;
+      f->P = (2 * K + 1) * (2 * K + 1) * (2 * K + 1) - 1;
+      for (int r = 0; r < nrep; ++r) {
+        f->reps_h[r].P = f->P;
+        f->reps_h[r].k_begin = r * f->P;
+        f->reps_h[r].S = f->P;
+      }
+      CK(cudaMemcpy(f->d_reps, f->reps_h.data(), sizeof(RepDev) * nrep, cudaMemcpyHostToDevice));
+    }
+    f->Ptot = nrep * f->P;
+    CK(cudaMalloc(&f->d_krec, (size_t)f->Ptot * recb));
+    CK(cudaMemset(f->d_krec, 0, (size_t)f->Ptot * recb));
+    CK(dalloc(&f->d_kvec, (size_t)3 * f->Ptot));
+    CK(dalloc(&f->d_rho, (size_t)f->Ptot));
+    CK(dalloc(&f->d_ek, (size_t)f->Ptot));
+    // structure-factor work items: (replica, chunk, tile)
+    std::vector<RhoItem> items;
+    std::vector<RhoRep> rr(nrep);
+    const int target = 148 * 8;
+    for (int r = 0; r < nrep; ++r) {
+      const int Nr = (int)(f->rep_off[r + 1] - f->rep_off[r]);
+      const int ntiles = (f->P + kKT - 1) / kKT;
+      int nch = (int)std::lround((double)target * Nr / (double)f->n / ntiles);
+      nch = std::max(1, std::min(nch, (Nr + 255) / 256));
+      rr[r].item_base = (int)items.size();
+      rr[r].ntiles = ntiles;
+      rr[r].nchunks = nch;
+      for (int c = 0; c < nch; ++c) {
+        const int b = (int)f->rep_off[r] + (int)((int64_t)Nr * c / nch);
+        const int e = (int)f->rep_off[r] + (int)((int64_t)Nr * (c + 1) / nch);
+        for (int t = 0; t < ntiles; ++t) {
+          RhoItem it;
+          it.atom_begin = b;
+          it.atom_end = e;
+          it.k_first = f->reps_h[r].k_begin + t * kKT;
+          it.k_count = std::min(kKT, f->P - t * kKT);
+          items.push_back(it);
+        }
+      }
+    }
+    f->nitems = (int)items.size();
+    CK(dalloc(&f->d_items, items.size()));
+    CK(cudaMemcpy(f->d_items, items.data(), sizeof(RhoItem) * items.size(), cudaMemcpyHostToDevice));
+    CK(dalloc(&f->d_rhorep, (size_t)nrep));
+    CK(cudaMemcpy(f->d_rhorep, rr.data(), sizeof(RhoRep) * nrep, cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&f->d_partial, (size_t)f->nitems * 2 * kKT * (fp64 ? sizeof(double) : sizeof(float))));
+    // sampler tables (Distribution_q, rbmd/framework/model/RBEPSample.h:97-114, tabulated in FP64)
+    std::vector<SamplerRep> sr(nrep);
+    std::vector<double> qtab;
+    for (int r = 0; r < nrep; ++r) {
+      const double* L = f->reps_h[r].box_d;
+      SamplerRep& s = sr[r];
+      s.qmax = 0;
+      for (int d = 0; d < 3; ++d) {
+        s.sigma[d] = std::sqrt(f->alpha / 2.0) * L[d] / M_PI;
+        s.c[d] = M_PI * M_PI / (f->alpha * L[d] * L[d]);
+        s.qmax = std::max(s.qmax, (int)std::ceil(14.0 * s.sigma[d]) + 8);
+      }
+      s.q_offset = (int)qtab.size();
+      for (int d = 0; d < 3; ++d) {
+        const double sc = std::sqrt(f->alpha * L[d] * L[d] / (M_PI * M_PI));
+        qtab.push_back(std::erf(0.5 / sc));
+        for (int m = 1; m <= s.qmax; ++m)
+          qtab.push_back((std::erf((0.5 + m) / sc) - std::erf((m - 0.5) / sc)) / 2.0);
+      }
+    }
+    CK(dalloc(&f->d_srep, (size_t)nrep));
+    CK(cudaMemcpy(f->d_srep, sr.data(), sizeof(SamplerRep) * nrep, cudaMemcpyHostToDevice));
+    CK(dalloc(&f->d_qtab, qtab.size()));
+    CK(cudaMemcpy(f->d_qtab, qtab.data(), sizeof(double) * qtab.size(), cudaMemcpyHostToDevice));
+    if (f->coul_type == "EWALD") {
+      // fixed cube sample set with Gaussian weights
+      std::vector<int> m;
+      std::vector<double> w;
+      for (int r = 0; r < nrep; ++r) {
+        const double* L = f->reps_h[r].box_d;
+        const int K = f->kmax;
+        for (int i = -K; i <= K; ++i)
+          for (int j = -K; j <= K; ++j)
+            for (int k = -K; k <= K; ++k) {
+              if (i == 0 && j == 0 && k == 0) continue;
+              m.push_back(i); m.push_back(j); m.push_back(k);
+              const double kx = 2 * M_PI * i / L[0], ky = 2 * M_PI * j / L[1], kz = 2 * M_PI * k / L[2];
+              w.push_back(std::exp(-(kx * kx + ky * ky + kz * kz) / (4 * f->alpha)));
+            }
+      }
+      rbmd_status s2 = upload_ksamples(f, m.data());
+      if (s2) return s2;
+      CK(dalloc(&f->d_weights, w.size()));
+      CK(cudaMemcpy(f->d_weights, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice));
+    }
+  }
+  // MD chunks
+  {
+    std::vector<MdChunk> ch;
+    std::vector<int> crb(nrep + 1);
+    for (int r = 0; r < nrep; ++r) {
+      crb[r] = (int)ch.size();
+      for (int64_t b = f->rep_off[r]; b < f->rep_off[r + 1]; b += kMdChunk) {
+        MdChunk c;
+        c.begin = (int)b;
+        c.end = (int)std::min<int64_t>(b + kMdChunk, f->rep_off[r + 1]);
+        c.rep = r;
+        c.pad = 0;
+        ch.push_back(c);
+      }
+    }
+    crb[nrep] = (int)ch.size();
+    f->nchunks = (int)ch.size();
+    CK(dalloc(&f->d_chunks, ch.size()));
+    CK(cudaMemcpy(f->d_chunks, ch.data(), sizeof(MdChunk) * ch.size(), cudaMemcpyHostToDevice));
+    CK(dalloc(&f->d_chunk_rep_begin, (size_t)nrep + 1));
+    CK(cudaMemcpy(f->d_chunk_rep_begin, crb.data(), sizeof(int) * (nrep + 1), cudaMemcpyHostToDevice));
+    CK(dalloc(&f->d_ke_partial, ch.size()));
+    CK(dalloc(&f->d_ke, (size_t)nrep));
+    CK(dalloc(&f->d_T, (size_t)nrep));
+    CK(dalloc(&f->d_lambda, (size_t)nrep));
+    CK(dalloc(&f->d_xi, (size_t)nrep));
+    CK(cudaMemset(f->d_xi, 0, sizeof(double) * nrep));
+    CK(cudaMemset(f->d_ke, 0, sizeof(double) * nrep));
+    CK(cudaMemset(f->d_T, 0, sizeof(double) * nrep));
+    std::vector<double> ones(nrep, 1.0);
+    CK(cudaMemcpy(f->d_lambda, ones.data(), sizeof(double) * nrep, cudaMemcpyHostToDevice));
+    if (f->shake == "true" && f->n_mol > 0) {
+      CK(dalloc(&f->d_xold, 3 * n));
+      CK(dalloc(&f->d_vold, 3 * n));
+    }
+  }
+  // EAM
+  if (f->is_eam()) {
+    auto up = [&](const std::vector<float>& s, float4** d) -> rbmd_status {
+      const size_t rows = s.size() / 7;
+      std::vector<float4> v(2 * rows);
+      for (size_t m = 0; m < rows; ++m) {
+        v[2 * m] = make_float4(s[7 * m], s[7 * m + 1], s[7 * m + 2], s[7 * m + 3]);
+        v[2 * m + 1] = make_float4(s[7 * m + 4], s[7 * m + 5], s[7 * m + 6], 0.f);
+      }
+      CK(dalloc(d, v.size()));
+      CK(cudaMemcpy(*d, v.data(), sizeof(float4) * v.size(), cudaMemcpyHostToDevice));
+      return RBMD_OK;
+    };
+    rbmd_status s1 = up(f->eam_h.frho, &f->d_frho);
+    if (s1) return s1;
+    s1 = up(f->eam_h.rhor, &f->d_rhor);
+    if (s1) return s1;
+    s1 = up(f->eam_h.z2r, &f->d_z2r);
+    if (s1) return s1;
+    CK(cudaMalloc(&f->d_fp, n * (fp64 ? sizeof(double) : sizeof(float))));
+    CK(dalloc(&f->d_emb, n));
+    CK(dalloc(&f->d_epair, n));
+  }
+  // water
+  if (f->n_mol > 0) {
+    CK(dalloc(&f->d_hoh, (size_t)3 * f->n_mol));
+    CK(cudaMemcpy(f->d_hoh, f->hoh_h.data(), sizeof(int) * 3 * f->n_mol, cudaMemcpyHostToDevice));
+    CK(dalloc(&f->d_ebond, (size_t)f->n_mol));
+    CK(dalloc(&f->d_eangle, (size_t)f->n_mol));
+  }
+  f->bound = true;
+  f->step_count = 0;
+  f->pending_scale = false;
+  return RBMD_OK;
+}
+
+rbmd_status rbmd_force_set_ksamples(rbmd_force* f, const int32_t* m_xyz, int32_t P) {
+  if (!f) return RBMD_ERR_ARG;
+  if (!m_xyz || P == 0) {
+    f->injected = false;
+    return RBMD_OK;
+  }
+  if (!f->bound || !f->is_rbe() || P != f->P || f->coul_type != "RBE") return RBMD_ERR_ARG;
+  return upload_ksamples(f, m_xyz);
+}
+
+rbmd_status rbmd_force_set_kweights(rbmd_force* f, const double* w_host) {
+  if (!f || !f->bound || !f->is_rbe()) return RBMD_ERR_ARG;
+  if (!w_host) { dfree(f->d_weights); return RBMD_OK; }
+  if (!f->d_weights) CK(dalloc(&f->d_weights, (size_t)f->Ptot));
+  CK(cudaMemcpy(f->d_weights, w_host, sizeof(double) * f->Ptot, cudaMemcpyHostToDevice));
+  return RBMD_OK;
+}
+
+rbmd_status rbmd_force_get_ksamples(rbmd_force* f, int32_t* m_xyz, int32_t P) {
+  if (!f || !m_xyz || !f->bound || !f->is_rbe() || P != f->P) return RBMD_ERR_ARG;
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpy(m_xyz, f->d_kvec, sizeof(int) * 3 * f->Ptot, cudaMemcpyDeviceToHost));
+  return RBMD_OK;
+}
+
+rbmd_status rbmd_force_sample_k(rbmd_force* f, int64_t step, int32_t* m_xyz, int32_t P) {
+  if (!f || !f->bound || !f->is_rbe() || P != f->P || f->coul_type != "RBE") return RBMD_ERR_ARG;
+  const int recb = f->fp64 ? sizeof(KRec64) : sizeof(KRec32);
+  k_sample<kSamplerD><<<f->nrep, 256>>>(f->nrep, f->d_srep, f->d_qtab, f->d_reps, f->seed, step,
+                                         f->d_kvec, f->d_krec, recb, f->d_status);
+  CK(cudaGetLastError());
+  CK(cudaDeviceSynchronize());
+  if (m_xyz) CK(cudaMemcpy(m_xyz, f->d_kvec, sizeof(int) * 3 * f->Ptot, cudaMemcpyDeviceToHost));
+  return RBMD_OK;
+}
+
+rbmd_status rbmd_force_compute(rbmd_force* f, void* stream) {
+  if (!f) return RBMD_ERR_ARG;
+  if (!f->bound) return RBMD_ERR_STATE;
+  cudaStream_t s = (cudaStream_t)stream;
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    f->launches = 0;
+    launch_compute_any(f, s);
+    CK(cudaGetLastError());
+    bool redo = false;
+    rbmd_status st = check_overflow(f, s, &redo);
+    if (st) return st;
+    if (!redo) return RBMD_OK;
+  }
+  return RBMD_ERR_DEVICE;
+}
+
+rbmd_status rbmd_force_compute_host(rbmd_force* f, const double* pos_host, double* force_host,
+                                    void* stream) {
+  if (!f || !pos_host || !force_host) return RBMD_ERR_ARG;
+  if (!f->bound) return RBMD_ERR_STATE;
+  cudaStream_t s = (cudaStream_t)stream;
+  CK(cudaMemcpyAsync(f->at.pos, pos_host, sizeof(double) * 3 * f->n, cudaMemcpyHostToDevice, s));
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    f->launches = 0;
+    launch_compute_any(f, s);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(force_host, f->at.force, sizeof(double) * 3 * f->n, cudaMemcpyDeviceToHost, s));
+    bool redo = false;
+    rbmd_status st = check_overflow(f, s, &redo);
+    if (st) return st;
+    if (!redo) return RBMD_OK;
+  }
+  return RBMD_ERR_DEVICE;
+}
+
+rbmd_status rbmd_force_step(rbmd_force* f, int32_t n_steps, void* stream) {
+  if (!f || n_steps < 0) return RBMD_ERR_ARG;
+  if (!f->bound) return RBMD_ERR_STATE;
+  if (!f->at.vel || !f->at.mass) return RBMD_ERR_STATE;
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t n = f->n;
+  if (!f->d_snap) CK(dalloc(&f->d_snap, 9 * n));
+  if (f->at.image && !f->d_snap_img) CK(dalloc(&f->d_snap_img, 3 * n));
+  const long long step0 = f->step_count;
+  const bool pend0 = f->pending_scale;
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    CK(cudaMemcpyAsync(f->d_snap, f->at.pos, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(f->d_snap + 3 * n, f->at.vel, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(f->d_snap + 6 * n, f->at.force, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, s));
+    if (f->at.image)
+      CK(cudaMemcpyAsync(f->d_snap_img, f->at.image, sizeof(int) * 3 * n, cudaMemcpyDeviceToDevice, s));
+    f->launches = 0;
+    for (int k = 0; k < n_steps; ++k) {
+      if (f->fp64) launch_step<double>(f, s);
+      else launch_step<float>(f, s);
+    }
+    CK(cudaGetLastError());
+    bool redo = false;
+    rbmd_status st = check_overflow(f, s, &redo);
+    if (st) return st;
+    if (!redo) {
+      if (n_steps > 0) f->launches /= n_steps;
+      return RBMD_OK;
+    }
+    // replay from the snapshot with the grown list (the sampler is keyed by the step counter)
+    CK(cudaMemcpyAsync(f->at.pos, f->d_snap, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(f->at.vel, f->d_snap + 3 * n, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(f->at.force, f->d_snap + 6 * n, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, s));
+    if (f->at.image)
+      CK(cudaMemcpyAsync(f->at.image, f->d_snap_img, sizeof(int) * 3 * n, cudaMemcpyDeviceToDevice, s));
+    f->step_count = step0;
+    f->pending_scale = pend0;
+  }
+  return RBMD_ERR_DEVICE;
+}
+
+// Apply a deferred thermostat rescale so that the bound velocities are current.
+rbmd_status rbmd_force_sync_velocities(rbmd_force* f, void* stream) {
+  if (!f || !f->bound) return RBMD_ERR_STATE;
+  if (f->pending_scale) {
+    k_scale_vel<<<(f->n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
+        f->n, f->nrep > 1 ? f->d_rep_of : nullptr, f->d_lambda, f->at.vel);
+    CK(cudaGetLastError());
+    f->pending_scale = false;
+  }
+  return RBMD_OK;
+}
+
+rbmd_status rbmd_force_energy(rbmd_force* f, rbmd_energy* out, void* stream) {
+  if (!f || !out) return RBMD_ERR_ARG;
+  if (!f->bound) return RBMD_ERR_STATE;
+  cudaStream_t s = (cudaStream_t)stream;
+  std::memset(out, 0, sizeof *out);
+  CK(cudaMemsetAsync(f->d_esum, 0, sizeof(double) * 32, s));
+  if (!f->is_eam()) {
+    k_sum<<<1, 1024, 0, s>>>(f->n, f->d_eslot, 2, 0, f->d_esum + 0);
+    k_sum<<<1, 1024, 0, s>>>(f->n, f->d_eslot, 2, 1, f->d_esum + 1);
+  } else {
+    k_sum<<<1, 1024, 0, s>>>(f->n, f->d_emb, 1, 0, f->d_esum + 4);
+    k_sum<<<1, 1024, 0, s>>>(f->n, f->d_epair, 1, 0, f->d_esum + 5);
+  }
+  if (f->is_rbe()) k_sum<<<1, 1024, 0, s>>>(f->Ptot, f->d_ek, 1, 0, f->d_esum + 2);
+  if (f->n_mol > 0 && f->is_cvff()) {
+    k_sum<<<1, 1024, 0, s>>>((int)f->n_mol, f->d_ebond, 1, 0, f->d_esum + 6);
+    k_sum<<<1, 1024, 0, s>>>((int)f->n_mol, f->d_eangle, 1, 0, f->d_esum + 7);
+  }
+  k_sum<<<1, 1024, 0, s>>>(f->nrep, f->d_ke, 1, 0, f->d_esum + 8);
+  k_sum<<<1, 1024, 0, s>>>(f->nrep, f->d_T, 1, 0, f->d_esum + 9);
+  CK(cudaGetLastError());
+  double h[16];
+  CK(cudaMemcpyAsync(h, f->d_esum, sizeof(double) * 16, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  out->lj = h[0];
+  out->coul_real = h[1];
+  out->coul_kspace = h[2];
+  out->coul_self = f->is_rbe() ? -std::sqrt(f->alpha / M_PI) * f->sum_q2 * f->u.qqr2e : 0.0;
+  out->eam_embed = h[4];
+  out->eam_pair = h[5];
+  out->bond = h[6];
+  out->angle = h[7];
+  out->kinetic = h[8];
+  out->temperature = h[9] / f->nrep;
+  return RBMD_OK;
+}
+
+rbmd_status rbmd_force_status(rbmd_force* f, uint32_t* flags, int32_t clear, void* stream) {
+  if (!f || !flags) return RBMD_ERR_ARG;
+  if (!f->bound) { *flags = 0; return RBMD_OK; }
+  cudaStream_t s = (cudaStream_t)stream;
+  CK(cudaMemcpyAsync(f->h_status, f->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  *flags = *f->h_status;
+  if (clear) CK(cudaMemsetAsync(f->d_status, 0, sizeof(uint32_t), s));
+  CK(cudaStreamSynchronize(s));
+  return RBMD_OK;
+}
+
+rbmd_status rbmd_force_get_neighbors(rbmd_force* f, int32_t* counts, int32_t* ids, int64_t cap) {
+  if (!f || !counts || !ids || cap < 0) return RBMD_ERR_ARG;
+  if (!f->bound) return RBMD_ERR_STATE;
+  CK(cudaDeviceSynchronize());
+  const size_t n = f->n;
+  std::vector<int> cnt(n), slot_atom(n), nbr((size_t)f->cap * f->stride);
+  CK(cudaMemcpy(cnt.data(), f->d_count, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(slot_atom.data(), f->d_slot_atom, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(nbr.data(), f->d_nbr, sizeof(int) * nbr.size(), cudaMemcpyDeviceToHost));
+  bool too_small = false;
+  for (size_t i = 0; i < n; ++i) {
+    const int id = slot_atom[i];
+    counts[id] = cnt[i];
+    const int m = std::min<int>(cnt[i], f->cap);
+    if (cnt[i] > cap) too_small = true;
+    for (int p = 0; p < m && p < cap; ++p)
+      ids[(size_t)id * cap + p] = slot_atom[nbr[(size_t)p * f->stride + i] >> kShiftBits];
+  }
+  return too_small ? RBMD_ERR_ARG : RBMD_OK;
+}
+
+rbmd_status rbmd_force_get_rhok(rbmd_force* f, double* rho, int32_t P) {
+  if (!f || !rho || !f->bound || !f->is_rbe() || P != f->P) return RBMD_ERR_ARG;
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpy(rho, f->d_rho, sizeof(double2) * f->Ptot, cudaMemcpyDeviceToHost));
+  return RBMD_OK;
+}
+
+rbmd_status rbmd_force_profile(rbmd_force* f, int32_t enable) {
+  if (!f) return RBMD_ERR_ARG;
+  f->prof_on = enable != 0;
+  for (int i = 0; i < 8; ++i) { f->phase_ms[i] = 0; f->phase_n[i] = 0; }
+  return RBMD_OK;
+}
+
+rbmd_status rbmd_force_phase_ms(rbmd_force* f, double* ms, int64_t* counts, int32_t n) {
+  if (!f || !ms || n < 1) return RBMD_ERR_ARG;
+  for (int i = 0; i < n && i < 8; ++i) {
+    ms[i] = f->phase_ms[i];
+    if (counts) counts[i] = f->phase_n[i];
+  }
+  return RBMD_OK;
+}
+
+rbmd_status rbmd_force_launch_count(rbmd_force* f, int32_t* k) {
+  if (!f || !k) return RBMD_ERR_ARG;
+  *k = f->launches;
+  return RBMD_OK;
+}
+
+void rbmd_force_destroy(rbmd_force* f) {
+  if (!f) return;
+  if (f->bound) cudaDeviceSynchronize();
+  free_all(f);
+  delete f;
+}
+
+}  // extern "C"

@@ -1,0 +1,205 @@
+/*
+ * rbmd_force.h -- C ABI of the B200 (sm_100a) per-timestep force path of RBMD.
+ *
+ * The reference selects its force path by string dispatch inside
+ * ExecutionNVT::ComputeAllForce (rbmd/framework/run/ExecutionNVT.cpp:185-222), keyed by
+ * force_field.type, neighbor.type and coulomb.type, and the HIP tree exposes the same path
+ * as `class Force { virtual void Init(); virtual void Execute() = 0; }`
+ * (rbmd-gpu-clone/rbmd-gpu/src/force/include/force.h:8-25).  This header replaces both with
+ * plain C entry points: no C++ types, no CUDA types (streams are passed as `void*` holding a
+ * cudaStream_t), plain pointers and sizes.
+ *
+ * Ownership: the caller owns the atom arrays (device pointers, caller's atom order).  The
+ * library owns cells, neighbour lists, k-space buffers and its workspace.  Every call returns
+ * an rbmd_status; device-side failures are reported through a status word
+ * (rbmd_force_status) and never terminate the process (the reference calls exit(0) from
+ * console::Error, rbmd/framework/Logging.h:45-51).
+ */
+#ifndef RBMD_FORCE_H
+#define RBMD_FORCE_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define RBMD_API __attribute__((visibility("default")))
+#else
+#define RBMD_API
+#endif
+
+typedef int32_t rbmd_status;
+
+/* host-side return codes */
+#define RBMD_OK                 0
+#define RBMD_ERR_ARG            1   /* bad argument (null pointer, size, unknown key value) */
+#define RBMD_ERR_CONFIG         2   /* JSON text could not be parsed or misses a required key */
+#define RBMD_ERR_CUDA           3   /* a CUDA runtime call failed */
+#define RBMD_ERR_STATE          4   /* call order violated (e.g. compute before bind) */
+#define RBMD_ERR_DEVICE         5   /* the device status word holds an error bit */
+#define RBMD_ERR_FILE           6   /* potential / data file unreadable */
+
+/* device status word bits (rbmd_force_status) */
+#define RBMD_FLAG_LIST_OVERFLOW   0x01u  /* an atom had more neighbours than the list capacity */
+#define RBMD_FLAG_CELL_OVERFLOW   0x02u  /* a cell held more atoms than the cell sort supports */
+#define RBMD_FLAG_SHAKE_NOCONV    0x04u  /* SHAKE hit its iteration cap before |dlambda|<tol */
+#define RBMD_FLAG_NONFINITE       0x08u  /* a NaN/Inf force or position was produced */
+#define RBMD_FLAG_OUT_OF_BOX      0x10u  /* an atom moved more than one box length in a step */
+#define RBMD_FLAG_SAMPLER         0x20u  /* the k-sampler ran out of pre-drawn proposals */
+#define RBMD_FLAG_SHAKE_SINGULAR  0x40u  /* |det| of a SHAKE/RATTLE matrix fell below 1e-4 */
+
+typedef struct rbmd_force rbmd_force;
+
+/* Orthorhombic periodic box of one replica: [lo, hi) per axis, as the LAMMPS header
+ * "xlo xhi" lines give it (rbmd/framework/InitCondition/ModelFileInitCondition.cpp:176-221). */
+typedef struct {
+  double lo[3];
+  double hi[3];
+} rbmd_box;
+
+/* Device atom arrays, caller atom order.  Replica r owns atoms
+ * [replica_offsets[r], replica_offsets[r+1]).  Optional pointers may be NULL. */
+typedef struct {
+  int64_t n_atoms;
+  int32_t n_replicas;
+  const int64_t* replica_offsets; /* HOST array, n_replicas+1 entries; NULL when n_replicas==1 */
+  double* pos;                    /* [n_atoms*3] x,y,z interleaved, FP64 master positions   */
+  double* vel;                    /* [n_atoms*3] FP64 velocities (step API only; may be NULL)*/
+  double* force;                  /* [n_atoms*3] output, FP64                                */
+  const double* mass;             /* [n_atoms] per-atom mass (step API only; may be NULL)    */
+  const double* charge;           /* [n_atoms] charge in e (NULL = all zero)                 */
+  const int32_t* type;            /* [n_atoms] 0-based atom type (NULL = all type 0)         */
+  const int32_t* molecule;        /* [n_atoms] 0-based molecule id (NULL = atom index)       */
+  int32_t* image;                 /* [n_atoms*3] periodic image flags (NULL = not tracked)   */
+} rbmd_atoms_dev;
+
+/* Energies of the last compute (device sums, FP64).  Units follow the configured unit set. */
+typedef struct {
+  double lj;           /* 12-6 pair energy                                   */
+  double coul_real;    /* erfc real-space Coulomb (x qqr2e)                   */
+  double coul_kspace;  /* k-space estimate of the Ewald reciprocal energy     */
+  double coul_self;    /* -sqrt(alpha/pi) * sum q^2 (x qqr2e)                 */
+  double eam_embed;    /* sum F(rho_i)                                        */
+  double eam_pair;     /* 1/2 sum phi(r_ij)                                   */
+  double bond;         /* harmonic bonds                                      */
+  double angle;        /* harmonic angles                                     */
+  double kinetic;      /* 1/2 sum m v^2 * mvv2e (step API)                     */
+  double temperature;  /* as ExecutionNVT::ComputeTempe (step API)            */
+} rbmd_energy;
+
+/* Create a force path from RBMD's JSON configuration text (the same "hyper_parameters",
+ * "execution" and "init_configuration" keys as rbmd/framework/hyperparameters/*.cpp and
+ * rbmd/framework/run/ExecutionMD.cpp:144-153 read; optional extra keys: neighbor.skin,
+ * coulomb.seed, precision ("fp32"|"fp64")).  `boxes` holds one box per replica.
+ * Replaces: ExecutionNVT constructor + InitParameters + SetForceFunction
+ * (rbmd/framework/run/ExecutionNVT.cpp:52-58,789-833). */
+RBMD_API rbmd_status rbmd_force_create(const char* json_text, int32_t n_replicas, const rbmd_box* boxes,
+                              rbmd_force** out);
+
+/* Per-type 12-6 parameters, the "Pair Coeffs" section of the data file
+ * (rbmd/framework/InitCondition/ModelFileInitCondition.cpp:297-323). */
+RBMD_API rbmd_status rbmd_force_set_pair_coeffs(rbmd_force* f, int32_t n_types, const double* epsilon,
+                                       const double* sigma);
+
+/* EAM: read a funcfl potential file and build the 7-coefficient splines exactly as
+ * ExecutionNVT::ReadPotentialFile/file2array/array2spline do
+ * (rbmd/framework/run/ExecutionNVT.cpp:903-1107).  Called by create when
+ * force_field.potential_file is set; callable directly to load another file. */
+RBMD_API rbmd_status rbmd_force_load_funcfl(rbmd_force* f, const char* path);
+
+/* Water topology for CVFF: n_mol (H,O,H) angle triples, 0-based caller atom ids, the
+ * "Angles" section order (rbmd/framework/InitCondition/ModelFileInitCondition.cpp:519-540),
+ * plus harmonic bond (k, r0) and angle (k, theta0 in degrees) coefficients of type 0. */
+RBMD_API rbmd_status rbmd_force_set_water(rbmd_force* f, int64_t n_mol, const int32_t* hoh_triples_host,
+                                 double bond_k, double bond_r0, double angle_k,
+                                 double angle_theta0_deg);
+
+/* Attach device atom arrays; sizes the cell grid, neighbour lists and k-space buffers.
+ * Replaces ExecutionMD::Init (rbmd/framework/run/ExecutionMD.cpp:117-134). */
+RBMD_API rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* atoms);
+
+/* Inject the RBE k-samples (integer m vectors, k = 2*pi*m/L) for every replica:
+ * m_xyz_host holds n_replicas*P*3 int32.  After this call compute/step use these samples
+ * instead of the on-device sampler until rbmd_force_set_ksamples(f, NULL, 0) re-enables it.
+ * Replaces the output of RBEPSAMPLE::Fetch_P_Sample (rbmd/framework/model/RBEPSample.h:144-173). */
+RBMD_API rbmd_status rbmd_force_set_ksamples(rbmd_force* f, const int32_t* m_xyz_host, int32_t P);
+
+/* Per-sample importance weights (n_replicas*P doubles, host) multiplying each sample's force
+ * and energy term; NULL restores unit weights.  Used when the k-samples come from a proposal
+ * other than RBE's Gaussian: w = p_gauss(k) / q(k) keeps the estimator unbiased.  No reference
+ * counterpart (the reference samples only from the Gaussian, RBEPSample.h:63-175). */
+RBMD_API rbmd_status rbmd_force_set_kweights(rbmd_force* f, const double* w_host);
+
+/* Read the k-samples of the last compute (n_replicas*P*3 int32 into host memory). */
+RBMD_API rbmd_status rbmd_force_get_ksamples(rbmd_force* f, int32_t* m_xyz_host, int32_t P);
+
+/* Draw the k-samples for `step` with the on-device Metropolis-Hastings sampler (seeded
+ * counter RNG; algorithm of RBEPSAMPLE::Fetch_P_Sample/MH_Algorithm) and copy them out. */
+RBMD_API rbmd_status rbmd_force_sample_k(rbmd_force* f, int64_t step, int32_t* m_xyz_host, int32_t P);
+
+/* One force evaluation on the caller's stream: cell sort, neighbour list, near force, RBE
+ * (or EAM / CVFF extras), sum into atoms->force.  = Force::Execute / ComputeForce
+ * (rbmd/framework/run/ExecutionNVT.cpp:179-222). */
+RBMD_API rbmd_status rbmd_force_compute(rbmd_force* f, void* stream);
+
+/* Same as rbmd_force_compute with HOST positions in and HOST forces out (n_atoms*3 doubles
+ * each); copies are issued on `stream` and the call returns after the force copy landed.
+ * This is the call a host-side MD driver (the reference's ExecutionNVT) makes per step. */
+RBMD_API rbmd_status rbmd_force_compute_host(rbmd_force* f, const double* pos_host, double* force_host,
+                                    void* stream);
+
+/* Advance n_steps velocity-Verlet steps in the order of ExecutionNVT::Solve
+ * (rbmd/framework/run/ExecutionNVT.cpp:133-159): kick, drift+wrap, SHAKE, force, kick,
+ * RATTLE, temperature, thermostat.  Requires vel and mass in the bound atoms. */
+RBMD_API rbmd_status rbmd_force_step(rbmd_force* f, int32_t n_steps, void* stream);
+
+/* The thermostat rescale of the last step is applied lazily at the start of the next step;
+ * call this to make the bound velocity array current before reading it. */
+RBMD_API rbmd_status rbmd_force_sync_velocities(rbmd_force* f, void* stream);
+
+/* Energies of the last compute/step (synchronises the stream). */
+RBMD_API rbmd_status rbmd_force_energy(rbmd_force* f, rbmd_energy* out, void* stream);
+
+/* Device status word (RBMD_FLAG_*), synchronises the stream; clear!=0 resets it. */
+RBMD_API rbmd_status rbmd_force_status(rbmd_force* f, uint32_t* flags, int32_t clear, void* stream);
+
+/* Full neighbour list of the last compute in caller atom ids: counts[n_atoms] and
+ * ids[n_atoms*cap] (row i holds atom i's neighbours), host memory. Returns RBMD_ERR_ARG when
+ * cap is smaller than the longest row (counts are still written). Mirrors the id_verletlist /
+ * num_verletlist output of ComputeNeighboursWorklet (rbmd/framework/run/worklet/RunWorklet.cpp:40-96). */
+RBMD_API rbmd_status rbmd_force_get_neighbors(rbmd_force* f, int32_t* counts_host, int32_t* ids_host,
+                                     int64_t cap);
+
+/* Structure factors of the last compute: rho[n_replicas*P*2] (Re, Im) doubles, host memory,
+ * with the phase origin at each box's lo corner (|rho| equals the reference's
+ * ComputePnumberChargeStructureFactorWorklet + ReduceByKey result,
+ * rbmd/framework/run/worklet/RunWorklet.cpp:1616-1677). */
+RBMD_API rbmd_status rbmd_force_get_rhok(rbmd_force* f, double* rho_host, int32_t P);
+
+/* Per-phase device timing with CUDA events recorded on the stream each phase runs on
+ * (0 integrate, 1 cell sort, 2 k-space, 3 neighbour list, 4 force pass, 5 constraints and
+ * intramolecular terms).  enable resets the accumulators; phase_ms returns the summed
+ * milliseconds and the number of timed intervals per phase since then.  No reference
+ * counterpart beyond its vtkm::cont::Timer aliases (rbmd/framework/Timer.h:32). */
+RBMD_API rbmd_status rbmd_force_profile(rbmd_force* f, int32_t enable);
+RBMD_API rbmd_status rbmd_force_phase_ms(rbmd_force* f, double* ms, int64_t* counts, int32_t n);
+
+/* Library/kernel description for diagnostics: number of kernels the last compute or step
+ * launched per step. */
+RBMD_API rbmd_status rbmd_force_launch_count(rbmd_force* f, int32_t* kernels_per_step);
+
+RBMD_API void rbmd_force_destroy(rbmd_force* f);
+
+/* Version string of the library build. */
+RBMD_API const char* rbmd_version(void);
+
+/* Text of the last host-side error (CUDA call, config key), empty when none. */
+RBMD_API const char* rbmd_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RBMD_FORCE_H */

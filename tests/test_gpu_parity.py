@@ -1,0 +1,126 @@
+"""GPU parity of the force path against the CPU oracle (same inputs, same k-samples).
+
+Bars (written into each assertion):
+* neighbour pair sets: bit-exact per atom (FP32 and FP64);
+* forces: max_i |dF_i| / rms|F| <= 1e-5 in FP32 mode, <= 1e-11 in FP64 mode, against the oracle
+  evaluating the reference's pair terms in the same precision and summing them exactly;
+* k-space in FP32: error against the FP64 oracle no larger than the reference-precision (FP32)
+  oracle's own error, and <= 1e-5 norm-wise;
+* RBE k-samples: the on-device sampler reproduces the oracle's integer samples exactly.
+"""
+import numpy as np
+import pytest
+
+from copy_gpu_b200 import systems
+from tests.helpers import jitter, make_ff, pair_sets_equal, rel_err, to_dev
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp32": 1e-5, "fp64": 1e-11}
+
+
+def _posr(pos, prec):
+    return pos.astype(np.float32) if prec == "fp32" else pos.astype(np.float64)
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_lj_pairs_and_force(cuda, oracle_lib, prec):
+    import torch
+    s = systems.lj_fcc(ncell=8, seed=2)
+    s["pos"] = jitter(s["pos"], s["lo"], s["hi"], 0.08, seed=5)
+    cfg = systems.lj_config(cutoff=2.5, precision=prec)
+    dev = to_dev(s, cuda)
+    ff = make_ff(cfg, s, dev)
+    ff.Execute()
+    torch.cuda.synchronize()
+    assert ff.status() == 0
+    c, ids = ff.neighbors(256)
+    pr = _posr(s["pos"], prec)
+    nl = oracle_lib.neighbors(pr, s["lo"], s["hi"], 2.5, prec)
+    assert pair_sets_equal(c, ids, nl[0], nl[1]) == -1, "neighbour pair sets differ"
+    ref = oracle_lib.near_force(pr, s["lo"], s["hi"], 2.5, nl, prec=prec, sum_mode=1)
+    err = rel_err(dev["force"].cpu().numpy(), ref)
+    assert err <= TOL[prec], f"LJ force rel err {err:.3e} > {TOL[prec]}"
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_pairs_edge_cases(cuda, oracle_lib, prec):
+    """Atoms exactly on the box faces and corners, coincident images, a 3-cell box."""
+    import torch
+    rng = np.random.default_rng(4)
+    L = 7.6  # dims = 3 at rc 2.5
+    pos = rng.uniform(0, L, size=(300, 3))
+    pos[:8] = np.array([[0, 0, 0], [L, 0, 0], [0, L, 0], [0, 0, L], [L, L, L], [L / 2, 0, L],
+                        [2.5, 2.5, 2.5], [5.0, 5.0, 5.0]])
+    pos[8] = pos[9] + np.array([2.5, 0, 0])          # exactly at the cutoff distance
+    s = dict(pos=pos, vel=np.zeros_like(pos), mass=np.ones(300), charge=np.zeros(300),
+             type=np.zeros(300, np.int32), molecule=None, lo=np.zeros(3), hi=np.full(3, L),
+             eps=np.ones(1), sigma=np.ones(1))
+    cfg = systems.lj_config(cutoff=2.5, precision=prec)
+    dev = to_dev(s, cuda)
+    ff = make_ff(cfg, s, dev)
+    ff.Execute()
+    torch.cuda.synchronize()
+    c, ids = ff.neighbors(512)
+    nl = oracle_lib.neighbors(_posr(pos, prec), s["lo"], s["hi"], 2.5, prec)
+    assert pair_sets_equal(c, ids, nl[0], nl[1]) == -1
+
+
+def _electrolyte(n, P, prec, seed=3):
+    s = systems.electrolyte(n, seed=seed)
+    cfg = systems.electrolyte_config(P=P, precision=prec)
+    return s, cfg
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_electrolyte_near_plus_rbe(cuda, oracle_lib, prec):
+    import torch
+    n, P = 3000, 64
+    s, cfg = _electrolyte(n, P, prec)
+    alpha = cfg["hyper_parameters"]["coulomb"]["alpha"]
+    L = s["hi"] - s["lo"]
+    m = oracle_lib.rbe_sample(alpha, L, seed=99, step=0, rep=0, P=P)
+    dev = to_dev(s, cuda)
+    ff = make_ff(cfg, s, dev)
+    ff.set_ksamples(m)
+    ff.Execute()
+    torch.cuda.synchronize()
+    assert ff.status() == 0
+    got = dev["force"].cpu().numpy()
+    pr = _posr(s["pos"], prec)
+    nl = oracle_lib.neighbors(pr, s["lo"], s["hi"], 2.5, prec)
+    near = oracle_lib.near_force(pr, s["lo"], s["hi"], 2.5, nl, type=s["type"], charge=s["charge"],
+                                 eps=s["eps"], sigma=s["sigma"], with_coul=True, alpha=alpha,
+                                 coul_scale=1.0, prec=prec, sum_mode=1)
+    rho64 = oracle_lib.rhok(s["pos"], s["charge"], L, m, prec="fp64")
+    far64 = oracle_lib.rbe_force(s["pos"], s["charge"], L, alpha, 1.0, m, rho64, prec="fp64")
+    # |rho| from the device equals the oracle's (phase origin differs only by a global phase)
+    rho_dev = ff.get_rhok(P)
+    amp_err = np.abs(np.hypot(*rho_dev.T) - np.hypot(*rho64.T)).max() / np.hypot(*rho64.T).max()
+    if prec == "fp64":
+        assert rel_err(got, near + far64) <= TOL["fp64"]
+        assert amp_err <= 1e-11
+    else:
+        rho32 = oracle_lib.rhok(s["pos"], s["charge"], L, m, prec="fp32")
+        far32 = oracle_lib.rbe_force(s["pos"], s["charge"], L, alpha, 1.0, m, rho32, prec="fp32")
+        far_dev = got - near
+        e_dev = rel_err(far_dev, far64)
+        e_ref = rel_err(far32, far64)
+        assert e_dev <= max(e_ref, 1e-5), f"k-space err {e_dev:.3e} vs reference-precision {e_ref:.3e}"
+        assert rel_err(got, near + far64) <= TOL["fp32"]
+        assert amp_err <= 1e-5
+
+
+def test_sampler_matches_oracle(cuda, oracle_lib):
+    n, P = 2000, 200
+    s, cfg = _electrolyte(n, P, "fp32")
+    cfg["hyper_parameters"]["coulomb"]["seed"] = 1234
+    alpha = cfg["hyper_parameters"]["coulomb"]["alpha"]
+    dev = to_dev(s, cuda)
+    ff = make_ff(cfg, s, dev)
+    L = s["hi"] - s["lo"]
+    for step in (0, 1, 17, 123456789):
+        got = ff.sample_k(step, P)
+        ref = oracle_lib.rbe_sample(alpha, L, seed=1234, step=step, rep=0, P=P)
+        assert np.array_equal(got, ref), f"step {step}"
+        assert not np.any(np.all(got == 0, axis=1))
