@@ -2,6 +2,8 @@
 // k-space force fused into the same per-atom pass, RBE structure factors, the RBE k-sampler,
 // and the EAM density / force passes.
 #pragma once
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace rbmd {
@@ -9,10 +11,11 @@ namespace rbmd {
 // ------------------------------------------------------------------------------------------
 // k-sample record: integer m vector plus the per-sample force coefficient w*k (w folds S/P,
 // qqr2e, -4 pi / (V k^2), the importance weight and the sign of the phase convention) and the
-// structure factor rho = sum_j q_j e^{i k.r_j}.
+// structure factor rho = sum_j q_j e^{i k.r_j}.  32 B (FP32) so that a record is two 16-byte
+// shared-memory loads; the owning replica of record g is krep[g].
 // ------------------------------------------------------------------------------------------
-struct KRec32 { int mx, my, mz, rep; float wx, wy, wz, pad; float re, im, pad2, pad3; };   // 48 B
-struct KRec64 { int mx, my, mz, rep; double wx, wy, wz, re, im, pad; };                    // 64 B
+struct KRec32 { int mx, my, mz; float wx, wy, wz, re, im; };                 // 32 B
+struct KRec64 { int mx, my, mz, pad; double wx, wy, wz, re, im, pad2; };     // 64 B
 
 // phase -> (cos, sin) of 2*pi*(t - 1/2) for a 32-bit fixed-point turn t: the top 23 bits form a
 // float in [1, 2), so tf - 1.5 lies in [-0.5, 0.5); MUFU sin/cos are accurate on [-pi, pi].
@@ -40,6 +43,7 @@ struct NearParams {
   int with_lj, with_coul, molecular;
   double rc, alpha, coul_scale;   // coul_scale multiplies the erfc Coulomb pair force
   double sqrt_alpha, two_sqrt_alpha_over_sqrt_pi;
+  int kstage;                     // records of shared memory available for k staging
 };
 
 template <class R> struct KRec;
@@ -49,12 +53,26 @@ template <class R> struct FracT;
 template <> struct FracT<float> { using T = Frac32; };
 template <> struct FracT<double> { using T = Frac64; };
 
-__device__ __forceinline__ float erfc_r(float x) { return erfcf(x); }
-__device__ __forceinline__ double erfc_r(double x) { return erfc(x); }
-__device__ __forceinline__ float exp_r(float x) { return expf(x); }
+__device__ __forceinline__ float exp_r(float x) { return __expf(x); }
 __device__ __forceinline__ double exp_r(double x) { return exp(x); }
+__device__ __forceinline__ float rsqrt_r(float x) { return rsqrtf(x); }
 __device__ __forceinline__ float sqrt_r(float x) { return sqrtf(x); }
 __device__ __forceinline__ double sqrt_r(double x) { return sqrt(x); }
+__device__ __forceinline__ double rsqrt_r(double x) { return 1.0 / sqrt(x); }
+
+// erfc(x) for x >= 0 given e = exp(-x^2).  FP32: Abramowitz & Stegun, Handbook of Mathematical
+// Functions, eq. 7.1.26 (rational approximation in t = 1/(1 + p x), |error| <= 1.5e-7), which
+// reuses the Gaussian factor the real-space force needs anyway.  FP64: the library erfc.
+__device__ __forceinline__ float erfc_shared(float x, float e) {
+  const float t = __frcp_rn(fmaf(0.3275911f, x, 1.0f));
+  float poly = fmaf(1.061405429f, t, -1.453152027f);
+  poly = fmaf(poly, t, 1.421413741f);
+  poly = fmaf(poly, t, -0.284496736f);
+  poly = fmaf(poly, t, 0.254829592f);
+  return poly * t * e;
+}
+__device__ __forceinline__ double erfc_shared(double x, double) { return erfc(x); }
+
 template <class R> __device__ __forceinline__ R lj24(const LJTable& t, int k);
 template <> __device__ __forceinline__ float lj24<float>(const LJTable& t, int k) { return t.lj24_f[k]; }
 template <> __device__ __forceinline__ double lj24<double>(const LJTable& t, int k) { return t.lj24_d[k]; }
@@ -62,14 +80,41 @@ template <class R> __device__ __forceinline__ R sig6(const LJTable& t, int k);
 template <> __device__ __forceinline__ float sig6<float>(const LJTable& t, int k) { return t.sig6_f[k]; }
 template <> __device__ __forceinline__ double sig6<double>(const LJTable& t, int k) { return t.sig6_d[k]; }
 
+// RBE force terms of one atom over k records [0, P) of `kr` (shared or global memory).
+template <class R>
+__device__ __forceinline__ void rbe_terms(const typename FracT<R>::T& fr, const typename KRec<R>::T* kr,
+                                          int P, R& ax, R& ay, R& az) {
+#pragma unroll 4
+  for (int l = 0; l < P; ++l) {
+    const typename KRec<R>::T k = kr[l];
+    R s, c;
+    if constexpr (sizeof(R) == 4) {
+      const uint32_t ph = (uint32_t)k.mx * fr.x + (uint32_t)k.my * fr.y + (uint32_t)k.mz * fr.z;
+      turn_sincos(ph, s, c);
+    } else {
+      const unsigned long long ph = (unsigned long long)(long long)k.mx * fr.x +
+                                    (unsigned long long)(long long)k.my * fr.y +
+                                    (unsigned long long)(long long)k.mz * fr.z;
+      turn_sincos(ph, s, c);
+    }
+    const R val = c * (R)k.im - s * (R)k.re;
+    ax += val * (R)k.wx;
+    ay += val * (R)k.wy;
+    az += val * (R)k.wz;
+  }
+}
+
 // Per-slot near force (+ fused RBE force).  One thread per slot over its transposed list row.
 // Pair physics: ComputeNearForceVerletWorklet / ComputeLJForceVerletWorklet
 // (rbmd/framework/run/worklet/RunWorklet.cpp:170-303) with ComputeLJForce and
 // ComputeNearEnergyForce (rbmd/framework/forceFunction/ExecForceFunction.h:74-140):
 //   LJ on MinDistanceVec(p_j', p_i) skipped within a molecule; Coulomb on p_j' - p_i for
 //   0.01 < d < rc with G = erfc(sqrt(a) d)/d^2 + 2 sqrt(a) e^{-a d^2}/(sqrt(pi) d).
-// RBE: ComputeNewRBEForceWorklet (RunWorklet.cpp:1508-1548), S/P and qqr2e folded into KRec.
-template <class R, bool LJ, bool COUL, bool RBE, bool MOLEC>
+//   MINIMG=false when every replica has >= 3 cells per axis: then each listed |r_d| < rc < L/2
+//   and MinDistanceVec is the identity.
+// RBE: ComputeNewRBEForceWorklet (RunWorklet.cpp:1508-1548), S/P and qqr2e folded into the
+// k records, which the block stages in shared memory when its slots' k range fits.
+template <class R, bool LJ, bool COUL, bool RBE, bool MOLEC, bool MINIMG, bool ENERGY>
 __global__ void __launch_bounds__(128) k_near_force(
     NearParams prm, const LJTable* __restrict__ ljt, const typename Traits<R>::V4* __restrict__ pos4,
     const int2* __restrict__ meta, const int* __restrict__ nbr, const int* __restrict__ count,
@@ -77,7 +122,28 @@ __global__ void __launch_bounds__(128) k_near_force(
     const int* __restrict__ slot_atom, const typename FracT<R>::T* __restrict__ frac,
     const typename KRec<R>::T* __restrict__ krec, double* __restrict__ force,
     double* __restrict__ energy_slot, uint32_t* status) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  extern __shared__ __align__(16) unsigned char ksm_raw[];
+  typename KRec<R>::T* ksm = reinterpret_cast<typename KRec<R>::T*>(ksm_raw);
+  const int i0 = blockIdx.x * blockDim.x;
+  const int i = i0 + threadIdx.x;
+  // k range of this block's replicas
+  int kfirst = 0, kcount = 0;
+  bool staged = false;
+  if (RBE) {
+    const int last = min(prm.n, i0 + (int)blockDim.x) - 1;
+    const int ra = rep_of_slot ? rep_of_slot[i0] : 0;
+    const int rb = rep_of_slot ? rep_of_slot[last] : 0;
+    kfirst = reps[ra].k_begin;
+    kcount = reps[rb].k_begin + reps[rb].P - kfirst;
+    staged = kcount <= prm.kstage;
+    if (staged) {
+      const int nwords = kcount * (int)(sizeof(typename KRec<R>::T) / 16);
+      const int4* src = reinterpret_cast<const int4*>(krec + kfirst);
+      int4* dst = reinterpret_cast<int4*>(ksm);
+      for (int t = threadIdx.x; t < nwords; t += blockDim.x) dst[t] = src[t];
+    }
+    __syncthreads();
+  }
   if (i >= prm.n) return;
   const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
   const typename Traits<R>::V4 pi = pos4[i];
@@ -88,6 +154,7 @@ __global__ void __launch_bounds__(128) k_near_force(
   const R wrap[3] = {Traits<R>::wrap(rp, 0), Traits<R>::wrap(rp, 1), Traits<R>::wrap(rp, 2)};
   const R sa = (R)prm.sqrt_alpha, aa = (R)prm.alpha, c2 = (R)prm.two_sqrt_alpha_over_sqrt_pi;
   const R cs = (R)prm.coul_scale;
+  const R qi = pi.w;
   Acc<R> fx, fy, fz;
   R e_lj = 0, e_coul = 0;
   const int cnt = count[i];
@@ -95,25 +162,28 @@ __global__ void __launch_bounds__(128) k_near_force(
     const int e = __ldg(nbr + (size_t)p * prm.stride + i);
     const int j = e >> kShiftBits;
     const typename Traits<R>::V4 pj = pos4[j];
-    R off[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      const int cd = (e >> (2 * d)) & 3;
-      off[d] = cd == 1 ? wrap[d] : (cd == 2 ? -wrap[d] : (R)0);
+    R px = pj.x, py = pj.y, pz = pj.z;
+    if (e & 63) {   // periodic image: p_j - offset (PeriodicCoordOffset)
+      const int c0 = e & 3, c1 = (e >> 2) & 3, c2b = (e >> 4) & 3;
+      px = px - (c0 == 1 ? wrap[0] : (c0 == 2 ? -wrap[0] : (R)0));
+      py = py - (c1 == 1 ? wrap[1] : (c1 == 2 ? -wrap[1] : (R)0));
+      pz = pz - (c2b == 1 ? wrap[2] : (c2b == 2 ? -wrap[2] : (R)0));
     }
-    R r0 = (pj.x - off[0]) - pi.x;
-    R r1 = (pj.y - off[1]) - pi.y;
-    R r2 = (pj.z - off[2]) - pi.z;
-    R f = 0;
+    const R r0 = px - pi.x, r1 = py - pi.y, r2 = pz - pi.z;
     const R d2 = r0 * r0 + r1 * r1 + r2 * r2;
+    R f = 0;
     if (COUL) {
-      const R dis = sqrt_r(d2);
-      if (dis < rc && dis > (R)0.01) {
-        const R inv = (R)1 / dis;
-        const R ex = exp_r(-aa * d2);
-        const R g = erfc_r(sa * dis) * inv * inv + c2 * ex * inv;
-        f += -pi.w * pj.w * g * inv * cs;
-        e_coul += pi.w * pj.w * erfc_r(sa * dis) * inv * cs;
+      const R qq = qi * pj.w;
+      if (qq != (R)0) {
+        const R inv = rsqrt_r(d2);
+        const R dis = d2 * inv;
+        if (dis < rc && dis > (R)0.01) {
+          const R ex = exp_r(-aa * d2);
+          const R erfcv = erfc_shared(sa * dis, ex);
+          const R g = (erfcv * inv + c2 * ex) * inv;
+          f = -qq * g * inv * cs;
+          if (ENERGY) e_coul += qq * erfcv * inv * cs;
+        }
       }
     }
     R fl0 = 0, fl1 = 0, fl2 = 0;
@@ -127,10 +197,13 @@ __global__ void __launch_bounds__(128) k_near_force(
       }
       if (!same) {
         R q0 = r0, q1 = r1, q2 = r2;   // MinDistanceVec(p_j', p_i)
-        if (fabs(q0) > box[0] * (R)0.5) q0 -= (q0 > 0 ? box[0] : -box[0]);
-        if (fabs(q1) > box[1] * (R)0.5) q1 -= (q1 > 0 ? box[1] : -box[1]);
-        if (fabs(q2) > box[2] * (R)0.5) q2 -= (q2 > 0 ? box[2] : -box[2]);
-        const R dl2 = q0 * q0 + q1 * q1 + q2 * q2;
+        R dl2 = d2;
+        if (MINIMG) {
+          if (fabs(q0) > box[0] * (R)0.5) q0 -= (q0 > 0 ? box[0] : -box[0]);
+          if (fabs(q1) > box[1] * (R)0.5) q1 -= (q1 > 0 ? box[1] : -box[1]);
+          if (fabs(q2) > box[2] * (R)0.5) q2 -= (q2 > 0 ? box[2] : -box[2]);
+          dl2 = q0 * q0 + q1 * q1 + q2 * q2;
+        }
         if (dl2 < cut2 && dl2 > (R)0.0001) {
           const int k = mi.x * prm.ntypes + tj;
           const R inv2 = (R)1 / dl2;
@@ -138,7 +211,7 @@ __global__ void __launch_bounds__(128) k_near_force(
           const R scal = lj24<R>(*ljt, k) * (((R)2 * sd6 - (R)1) * sd6) * inv2;
           fl0 = scal * q0; fl1 = scal * q1; fl2 = scal * q2;
           // 4 eps (s6 - 1) s6 with 4 eps = -lj24/6
-          e_lj += -lj24<R>(*ljt, k) / (R)6 * (sd6 - (R)1) * sd6;
+          if (ENERGY) e_lj += -lj24<R>(*ljt, k) / (R)6 * (sd6 - (R)1) * sd6;
         }
       }
     }
@@ -151,29 +224,8 @@ __global__ void __launch_bounds__(128) k_near_force(
     const typename FracT<R>::T fr = frac[i];
     R ax = 0, ay = 0, az = 0;
     const int kb = rp.k_begin, P = rp.P;
-#pragma unroll 4
-    for (int l = 0; l < P; ++l) {
-      const typename KRec<R>::T k = krec[kb + l];
-      R s, c;
-      if (sizeof(R) == 4) {
-        uint32_t ph = (uint32_t)k.mx * (uint32_t)fr.x + (uint32_t)k.my * (uint32_t)fr.y +
-                      (uint32_t)k.mz * (uint32_t)fr.z;
-        float sf, cf;
-        turn_sincos(ph, sf, cf);
-        s = (R)sf; c = (R)cf;
-      } else {
-        unsigned long long ph = (unsigned long long)(long long)k.mx * (unsigned long long)fr.x +
-                                (unsigned long long)(long long)k.my * (unsigned long long)fr.y +
-                                (unsigned long long)(long long)k.mz * (unsigned long long)fr.z;
-        double sd, cd;
-        turn_sincos(ph, sd, cd);
-        s = (R)sd; c = (R)cd;
-      }
-      const R val = c * (R)k.im - s * (R)k.re;
-      ax += val * (R)k.wx;
-      ay += val * (R)k.wy;
-      az += val * (R)k.wz;
-    }
+    if (staged) rbe_terms<R>(fr, ksm + (kb - kfirst), P, ax, ay, az);
+    else rbe_terms<R>(fr, krec + kb, P, ax, ay, az);
     const double q = (double)fr.q;
     F[0] += q * (double)ax;
     F[1] += q * (double)ay;
@@ -184,121 +236,76 @@ __global__ void __launch_bounds__(128) k_near_force(
   force[3 * id] = F[0];
   force[3 * id + 1] = F[1];
   force[3 * id + 2] = F[2];
-  if (energy_slot) {
+  if (ENERGY && energy_slot) {
     energy_slot[2 * i] = 0.5 * (double)e_lj;
     energy_slot[2 * i + 1] = 0.5 * (double)e_coul;
   }
 }
 
 // ------------------------------------------------------------------------------------------
-// RBE structure factors.  Work item = (replica, atom chunk, k tile of KT samples); each thread
-// walks the chunk's atoms with KT (Re, Im) accumulators in registers, then the block reduces
-// them (warp shuffles + shared memory) to one partial per (item, k).  There is no N x P buffer
-// (the reference materialises rho_Re/Im[P*N] and reduces by key, ExecutionMD.cpp:412-448).
+// RBE structure factors, one k per lane.  Work item = (replica, atom chunk, k tile of
+// 32*KL*warps samples).  Lane l of warp w owns samples w*32*KL + l + 32*j (j < KL): its m
+// vector and (Re, Im) accumulators live in registers.  The block stages the chunk's atoms
+// (fixed-point fractional coordinates + charge) in shared memory, 256 at a time, and every lane
+// reads each staged atom by a broadcast load, so one 16-byte load serves 32*KL (atom, k) pairs.
+// Each (item, k) partial is owned by one lane: no cross-lane reduction.  There is no N x P
+// buffer (the reference materialises rho_Re/Im[P*N] and reduces by key, ExecutionMD.cpp:412-448).
 // ------------------------------------------------------------------------------------------
 struct RhoItem { int atom_begin, atom_end, k_first, k_count; };
+constexpr int kRhoStage = 256;
 
-template <int KT>
-__global__ void __launch_bounds__(256) k_rho_partial32(const RhoItem* __restrict__ items,
-                                                       const Frac32* __restrict__ frac,
-                                                       const KRec32* __restrict__ krec,
-                                                       float2* __restrict__ partial) {
+template <class R, int KL>
+__global__ void __launch_bounds__(256) k_rho_lanes(const RhoItem* __restrict__ items,
+                                                   const typename FracT<R>::T* __restrict__ frac,
+                                                   const typename KRec<R>::T* __restrict__ krec,
+                                                   R* __restrict__ partial, int ktile) {
+  using FT = typename FracT<R>::T;
+  __shared__ FT stage[kRhoStage];
   const RhoItem it = items[blockIdx.x];
-  uint32_t mx[KT], my[KT], mz[KT];
-#pragma unroll
-  for (int k = 0; k < KT; ++k) {
-    const bool ok = k < it.k_count;
-    mx[k] = ok ? (uint32_t)krec[it.k_first + k].mx : 0u;
-    my[k] = ok ? (uint32_t)krec[it.k_first + k].my : 0u;
-    mz[k] = ok ? (uint32_t)krec[it.k_first + k].mz : 0u;
-  }
-  float re[KT], im[KT];
-#pragma unroll
-  for (int k = 0; k < KT; ++k) { re[k] = 0.f; im[k] = 0.f; }
-  for (int a = it.atom_begin + threadIdx.x; a < it.atom_end; a += blockDim.x) {
-    const Frac32 f = frac[a];
-#pragma unroll
-    for (int k = 0; k < KT; ++k) {
-      const uint32_t ph = mx[k] * f.x + my[k] * f.y + mz[k] * f.z;
-      float s, c;
-      turn_sincos(ph, s, c);
-      re[k] = fmaf(f.q, c, re[k]);
-      im[k] = fmaf(f.q, s, im[k]);
-    }
-  }
-  __shared__ float red[8][2 * KT];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  using MT = typename std::conditional<sizeof(R) == 4, uint32_t, unsigned long long>::type;
+  MT mx[KL], my[KL], mz[KL];
+  R re[KL], im[KL];
+  int kk[KL];
+  bool any = false;
 #pragma unroll
-  for (int k = 0; k < KT; ++k) {
+  for (int j = 0; j < KL; ++j) {
+    kk[j] = w * 32 * KL + j * 32 + lane;
+    const bool ok = kk[j] < it.k_count;
+    any |= ok;
+    const typename KRec<R>::T k = ok ? krec[it.k_first + kk[j]] : typename KRec<R>::T{};
+    mx[j] = (MT)(long long)k.mx;
+    my[j] = (MT)(long long)k.my;
+    mz[j] = (MT)(long long)k.mz;
+    re[j] = 0;
+    im[j] = 0;
+  }
+  const bool warp_any = __any_sync(0xffffffffu, any);
+  for (int base = it.atom_begin; base < it.atom_end; base += kRhoStage) {
+    const int cnt = min(kRhoStage, it.atom_end - base);
+    __syncthreads();
+    for (int t = threadIdx.x; t < cnt; t += blockDim.x) stage[t] = frac[base + t];
+    __syncthreads();
+    if (!warp_any) continue;
+#pragma unroll 4
+    for (int a = 0; a < cnt; ++a) {
+      const FT f = stage[a];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      re[k] += __shfl_xor_sync(0xffffffffu, re[k], o);
-      im[k] += __shfl_xor_sync(0xffffffffu, im[k], o);
+      for (int j = 0; j < KL; ++j) {
+        const MT ph = mx[j] * (MT)f.x + my[j] * (MT)f.y + mz[j] * (MT)f.z;
+        R s, c;
+        turn_sincos(ph, s, c);
+        re[j] = fma((R)f.q, c, re[j]);
+        im[j] = fma((R)f.q, s, im[j]);
+      }
     }
   }
-  if (lane == 0) {
 #pragma unroll
-    for (int k = 0; k < KT; ++k) { red[w][2 * k] = re[k]; red[w][2 * k + 1] = im[k]; }
-  }
-  __syncthreads();
-  if (threadIdx.x < 2 * KT) {
-    float s = 0.f;
-    const int nw = blockDim.x >> 5;
-    for (int ww = 0; ww < nw; ++ww) s += red[ww][threadIdx.x];
-    reinterpret_cast<float*>(partial)[(size_t)blockIdx.x * 2 * KT + threadIdx.x] = s;
-  }
-}
-
-template <int KT>
-__global__ void __launch_bounds__(256) k_rho_partial64(const RhoItem* __restrict__ items,
-                                                       const Frac64* __restrict__ frac,
-                                                       const KRec64* __restrict__ krec,
-                                                       double2* __restrict__ partial) {
-  const RhoItem it = items[blockIdx.x];
-  long long mx[KT], my[KT], mz[KT];
-#pragma unroll
-  for (int k = 0; k < KT; ++k) {
-    const bool ok = k < it.k_count;
-    mx[k] = ok ? krec[it.k_first + k].mx : 0;
-    my[k] = ok ? krec[it.k_first + k].my : 0;
-    mz[k] = ok ? krec[it.k_first + k].mz : 0;
-  }
-  double re[KT], im[KT];
-#pragma unroll
-  for (int k = 0; k < KT; ++k) { re[k] = 0.0; im[k] = 0.0; }
-  for (int a = it.atom_begin + threadIdx.x; a < it.atom_end; a += blockDim.x) {
-    const Frac64 f = frac[a];
-#pragma unroll
-    for (int k = 0; k < KT; ++k) {
-      const unsigned long long ph = (unsigned long long)mx[k] * f.x +
-                                    (unsigned long long)my[k] * f.y + (unsigned long long)mz[k] * f.z;
-      double s, c;
-      turn_sincos(ph, s, c);
-      re[k] = fma(f.q, c, re[k]);
-      im[k] = fma(f.q, s, im[k]);
+  for (int j = 0; j < KL; ++j)
+    if (kk[j] < it.k_count) {
+      partial[((size_t)blockIdx.x * ktile + kk[j]) * 2] = re[j];
+      partial[((size_t)blockIdx.x * ktile + kk[j]) * 2 + 1] = im[j];
     }
-  }
-  __shared__ double red[8][2 * KT];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-  for (int k = 0; k < KT; ++k) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      re[k] += __shfl_xor_sync(0xffffffffu, re[k], o);
-      im[k] += __shfl_xor_sync(0xffffffffu, im[k], o);
-    }
-  }
-  if (lane == 0) {
-#pragma unroll
-    for (int k = 0; k < KT; ++k) { red[w][2 * k] = re[k]; red[w][2 * k + 1] = im[k]; }
-  }
-  __syncthreads();
-  if (threadIdx.x < 2 * KT) {
-    double s = 0.0;
-    const int nw = blockDim.x >> 5;
-    for (int ww = 0; ww < nw; ++ww) s += red[ww][threadIdx.x];
-    reinterpret_cast<double*>(partial)[(size_t)blockIdx.x * 2 * KT + threadIdx.x] = s;
-  }
 }
 
 // Per-replica reduction layout: items are ordered (replica, chunk, tile); replica r's partials
@@ -308,31 +315,25 @@ struct RhoRep { int item_base, ntiles, nchunks, pad; };
 // One thread per k sample: sum the chunk partials in a fixed order (FP64), undo the half-turn
 // phase convention (rho = -sum), then fill the force coefficients of the k record.
 // k-space energy estimate per replica: (S/P) qqr2e sum_l w_l (2 pi / V) |rho_l|^2 / k_l^2.
-template <class R, int KT>
-__global__ void k_rho_finish(int nk_total, const RhoRep* __restrict__ rr, const RepDev* __restrict__ reps,
-                             const void* __restrict__ partial_v, const double* __restrict__ weights,
+template <class R>
+__global__ void k_rho_finish(int nk_total, int ktile, const int* __restrict__ krep,
+                             const RhoRep* __restrict__ rr, const RepDev* __restrict__ reps,
+                             const R* __restrict__ partial, const double* __restrict__ weights,
                              double qqr2e, typename KRec<R>::T* __restrict__ krec,
                              double2* __restrict__ rho_out, double* __restrict__ ek_out) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= nk_total) return;
   typename KRec<R>::T k = krec[g];
-  const int r = k.rep;
+  const int r = krep[g];
   const RepDev& rp = reps[r];
   const RhoRep q = rr[r];
   const int l = g - rp.k_begin;
-  const int tile = l / KT, kk = l % KT;
+  const int tile = l / ktile, kk = l % ktile;
   double re = 0, im = 0;
   for (int c = 0; c < q.nchunks; ++c) {
     const size_t item = (size_t)q.item_base + (size_t)c * q.ntiles + tile;
-    if (sizeof(R) == 4) {
-      const float* p = reinterpret_cast<const float*>(partial_v) + item * 2 * KT + 2 * kk;
-      re += (double)p[0];
-      im += (double)p[1];
-    } else {
-      const double* p = reinterpret_cast<const double*>(partial_v) + item * 2 * KT + 2 * kk;
-      re += p[0];
-      im += p[1];
-    }
+    re += (double)partial[(item * ktile + kk) * 2];
+    im += (double)partial[(item * ktile + kk) * 2 + 1];
   }
   re = -re;
   im = -im;
@@ -358,16 +359,19 @@ __global__ void k_rho_finish(int nk_total, const RhoRep* __restrict__ rr, const 
 
 // ------------------------------------------------------------------------------------------
 // RBE k-sampler: RBEPSAMPLE::Fetch_P_Sample + MH_Algorithm (rbmd/framework/model/
-// RBEPSample.h:63-173) with mu = 0, sigma_d = sqrt(alpha/2) L_d / pi.  One block per replica:
-// the Gaussian proposals and acceptance uniforms of the first D draws are generated in
-// parallel (they do not depend on the chain), then thread 0 runs the three per-axis chains in
-// lockstep (the all-zero retry couples the axes).  Draws past D are made inline.
+// RBEPSample.h:63-173) with mu = 0, sigma_d = sqrt(alpha/2) L_d / pi.  The MH ratio
+// (P(m')/P(m)) (q(m)/q(m')) is G(m')/G(m) with G = exp(-pi^2 m^2/(alpha L^2)) / q(m) tabulated
+// on the host (FP64); u <= min(1, ratio) is evaluated as u * G(m) <= G(m').
+// One block per replica: phase 1 draws the Gaussian proposals, their G values and the
+// acceptance uniforms of the first D steps in parallel (they do not depend on the chain);
+// phase 2 (one thread) walks the three per-axis chains in lockstep (the all-zero retry couples
+// the axes) carrying G(m) in registers, so a step has no dependent memory access.  Steps past
+// D draw inline.
 // ------------------------------------------------------------------------------------------
 struct SamplerRep {
   double sigma[3];
-  double c[3];      // pi^2 / (alpha L_d^2)
   int qmax;
-  int q_offset;     // offset of this replica's q tables (3 * (qmax+1) doubles) in qtab
+  int g_offset;     // offset of this replica's G tables (3 * (qmax+1) doubles)
 };
 
 __device__ __forceinline__ double sampler_draw(uint32_t k0, uint32_t k1, long long step, int rep,
@@ -383,75 +387,78 @@ __device__ __forceinline__ double sampler_draw(uint32_t k0, uint32_t k1, long lo
   return sqrt(-2.0 * log(U1)) * cos(2.0 * 3.14159265358979323846 * U2);
 }
 
+__device__ __forceinline__ double sampler_g(const double* g, int qmax, int axis, int m) {
+  m = abs(m);
+  return m <= qmax ? g[axis * (qmax + 1) + m] : __longlong_as_double(0x7ff0000000000000ll);
+}
+
 template <int D>
 __global__ void __launch_bounds__(256) k_sample(int nrep, const SamplerRep* __restrict__ srep,
-                                                const double* __restrict__ qtab,
+                                                const double* __restrict__ gtab,
                                                 const RepDev* __restrict__ reps, unsigned long long seed,
                                                 long long step, int* __restrict__ kvec_out,
-                                                void* __restrict__ krec, int rec_bytes, uint32_t* status) {
+                                                void* __restrict__ krec, int rec_bytes,
+                                                int* __restrict__ krep, uint32_t* status) {
   const int r = blockIdx.x;
   if (r >= nrep) return;
   const SamplerRep s = srep[r];
   const int P = reps[r].P, kb = reps[r].k_begin;
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  const double* g = gtab + s.g_offset;
   __shared__ int mw[3][D];
   __shared__ double ua[3][D];
+  __shared__ double gw[3][D];
   for (int t = threadIdx.x; t < 3 * D; t += blockDim.x) {
     const int axis = t / D, d = t % D;
     double u;
-    const double g = sampler_draw(k0, k1, step, r, axis, d, &u);
-    mw[axis][d] = (int)round(s.sigma[axis] * g);
+    const double gs = sampler_draw(k0, k1, step, r, axis, d, &u);
+    const int m = (int)round(s.sigma[axis] * gs);
+    mw[axis][d] = m;
     ua[axis][d] = u;
+    gw[axis][d] = sampler_g(g, s.qmax, axis, m);
   }
   __syncthreads();
   if (threadIdx.x != 0) return;
-  const double* q = qtab + s.q_offset;
-  auto qv = [&](int axis, int m) -> double {
-    m = abs(m);
-    return m <= s.qmax ? q[axis * (s.qmax + 1) + m] : 0.0;
-  };
-  auto prop = [&](int axis, long long d, double* u) -> int {
-    if (d < D) { *u = ua[axis][d]; return mw[axis][d]; }
-    const double g = sampler_draw(k0, k1, step, r, axis, d, u);
-    return (int)round(s.sigma[axis] * g);
+  auto prop = [&](int axis, long long d, double* u, double* gm) -> int {
+    if (d < D) { *u = ua[axis][d]; *gm = gw[axis][d]; return mw[axis][d]; }
+    const double gs = sampler_draw(k0, k1, step, r, axis, d, u);
+    const int m = (int)round(s.sigma[axis] * gs);
+    *gm = sampler_g(g, s.qmax, axis, m);
+    return m;
   };
   long long draw = 0;
   int X0[3];
+  double G0[3];
   for (int guard = 0;; ++guard) {
     double u;
-    for (int a = 0; a < 3; ++a) X0[a] = prop(a, draw, &u);
+    for (int a = 0; a < 3; ++a) X0[a] = prop(a, draw, &u, &G0[a]);
     ++draw;
     if (!(X0[0] == 0 && X0[1] == 0 && X0[2] == 0)) break;
-    if (guard > 100000) { set_flag(status, kFlagSampler); X0[0] = 1; break; }
+    if (guard > 100000) { set_flag(status, kFlagSampler); X0[0] = 1; G0[0] = sampler_g(g, s.qmax, 0, 1); break; }
   }
   auto emit = [&](int i, const int* X) {
     int* o = kvec_out + 3 * (kb + i);
     o[0] = X[0]; o[1] = X[1]; o[2] = X[2];
     int* rec = reinterpret_cast<int*>(reinterpret_cast<char*>(krec) + (size_t)(kb + i) * rec_bytes);
-    rec[0] = X[0]; rec[1] = X[1]; rec[2] = X[2]; rec[3] = r;
+    rec[0] = X[0]; rec[1] = X[1]; rec[2] = X[2];
+    krep[kb + i] = r;
   };
   emit(0, X0);
   int i = 1;
   long long guard = 0;
   while (i < P) {
-    int X1[3];
+#pragma unroll
     for (int a = 0; a < 3; ++a) {
-      double u;
-      const int m_w = prop(a, draw, &u);
-      const int m = X0[a];
-      const double qm = qv(a, m), qw = qv(a, m_w);
-      double pr = exp(s.c[a] * ((double)m * m - (double)m_w * m_w)) * (qm / qw);
-      if (!(pr < 1.0)) pr = 1.0;
-      X1[a] = (u <= pr) ? m_w : m;
+      double u, gm;
+      const int m_w = prop(a, draw, &u, &gm);
+      if (u * G0[a] <= gm) { X0[a] = m_w; G0[a] = gm; }
     }
     ++draw;
-    X0[0] = X1[0]; X0[1] = X1[1]; X0[2] = X1[2];
     if (++guard > 64LL * P + 100000) { set_flag(status, kFlagSampler); break; }
-    if (X1[0] == 0 && X1[1] == 0 && X1[2] == 0) continue;
-    emit(i, X1);
+    if (X0[0] == 0 && X0[1] == 0 && X0[2] == 0) continue;
+    emit(i, X0);
     ++i;
   }
-  if (draw > D) set_flag(status, 0);   // inline draws are valid; nothing to report
 }
 
 // ------------------------------------------------------------------------------------------

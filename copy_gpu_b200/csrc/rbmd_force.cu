@@ -29,8 +29,9 @@ using namespace rbmd;
 
 namespace {
 
-constexpr int kKT = 16;          // k samples per structure-factor tile
-constexpr int kSamplerD = 1024;  // pre-drawn proposals per axis in the sampler kernel
+constexpr int kKL = 2;           // k samples per lane in the structure-factor kernel
+constexpr int kStageBytes = 48 * 1024;   // shared memory for k staging in the force pass
+constexpr int kSamplerD = 640;   // pre-drawn proposals per axis in the sampler kernel (38 KB smem)
 constexpr int kMdChunk = 2048;   // atoms per kinetic-energy chunk
 
 #define CK(x)                                                                            \
@@ -81,6 +82,7 @@ struct rbmd_force {
   int tstat = 0, dof_mode = 0;
   double near_coul_scale = 1.0;
   double shake_tol = 1e-5;
+  int energy_every = 0;   // energies inside step(): every outputs.thermo_out.interval steps
   int shake_max_iter = 5000;
   std::string potential_file;
 
@@ -124,7 +126,9 @@ struct rbmd_force {
   double* d_eslot = nullptr;   // 2 per slot (lj, coul)
   double* d_esum = nullptr;    // scratch sums
   // RBE
-  int Ptot = 0, nitems = 0;
+  int Ptot = 0, nitems = 0, rho_threads = 64, ktile = 128, kstage = 0;
+  bool minimg = true, want_energy = true;
+  int* d_krep = nullptr;
   void* d_krec = nullptr;
   int* d_kvec = nullptr;
   RhoItem* d_items = nullptr;
@@ -234,7 +238,7 @@ void free_all(rbmd_force* f) {
   dfree(f->d_eslot); dfree(f->d_esum);
   if (f->d_krec) cudaFree(f->d_krec);
   f->d_krec = nullptr;
-  dfree(f->d_kvec); dfree(f->d_items); dfree(f->d_rhorep);
+  dfree(f->d_kvec); dfree(f->d_krep); dfree(f->d_items); dfree(f->d_rhorep);
   if (f->d_partial) cudaFree(f->d_partial);
   f->d_partial = nullptr;
   dfree(f->d_rho); dfree(f->d_ek); dfree(f->d_weights); dfree(f->d_srep); dfree(f->d_qtab);
@@ -347,22 +351,19 @@ void launch_kspace(rbmd_force* f, cudaStream_t s) {
   if (!f->injected && f->coul_type == "RBE") {
     k_sample<kSamplerD><<<f->nrep, 256, 0, s>>>(f->nrep, f->d_srep, f->d_qtab, f->d_reps, f->seed,
                                                 f->step_count, f->d_kvec, f->d_krec, rec_bytes,
-                                                f->d_status);
+                                                f->d_krep, f->d_status);
     f->launches++;
   }
-  if (sizeof(R) == 4)
-    k_rho_partial32<kKT><<<f->nitems, 256, 0, s>>>(f->d_items, (const Frac32*)f->d_frac,
-                                                  (const KRec32*)f->d_krec, (float2*)f->d_partial);
-  else
-    k_rho_partial64<kKT><<<f->nitems, 256, 0, s>>>(f->d_items, (const Frac64*)f->d_frac,
-                                                  (const KRec64*)f->d_krec, (double2*)f->d_partial);
-  k_rho_finish<R, kKT><<<(f->Ptot + 127) / 128, 128, 0, s>>>(
-      f->Ptot, f->d_rhorep, f->d_reps, f->d_partial, f->d_weights, f->u.qqr2e,
-      (typename KRec<R>::T*)f->d_krec, f->d_rho, f->d_ek);
+  k_rho_lanes<R, kKL><<<f->nitems, f->rho_threads, 0, s>>>(
+      f->d_items, (const typename FracT<R>::T*)f->d_frac, (const typename KRec<R>::T*)f->d_krec,
+      (R*)f->d_partial, f->ktile);
+  k_rho_finish<R><<<(f->Ptot + 127) / 128, 128, 0, s>>>(
+      f->Ptot, f->ktile, f->d_krep, f->d_rhorep, f->d_reps, (const R*)f->d_partial, f->d_weights,
+      f->u.qqr2e, (typename KRec<R>::T*)f->d_krec, f->d_rho, f->d_ek);
   f->launches += 2;
 }
 
-template <class R, bool LJ, bool COUL, bool RBE, bool MOLEC>
+template <class R, bool LJ, bool COUL, bool RBE, bool MOLEC, bool MINIMG, bool ENERGY>
 void launch_near_t(rbmd_force* f, cudaStream_t s) {
   NearParams p;
   p.n = f->n;
@@ -376,12 +377,25 @@ void launch_near_t(rbmd_force* f, cudaStream_t s) {
   p.coul_scale = f->near_coul_scale;
   p.sqrt_alpha = std::sqrt(f->alpha);
   p.two_sqrt_alpha_over_sqrt_pi = 2.0 * std::sqrt(f->alpha) / std::sqrt(M_PI);
-  k_near_force<R, LJ, COUL, RBE, MOLEC><<<(f->n + 127) / 128, 128, 0, s>>>(
+  p.kstage = RBE ? f->kstage : 0;
+  const size_t smem = RBE ? (size_t)f->kstage * sizeof(typename KRec<R>::T) : 0;
+  k_near_force<R, LJ, COUL, RBE, MOLEC, MINIMG, ENERGY><<<(f->n + 127) / 128, 128, smem, s>>>(
       p, f->d_ljt, (const typename Traits<R>::V4*)f->d_pos4, f->d_meta, f->d_nbr, f->d_count,
       f->d_reps, f->nrep > 1 ? f->d_rep_of : nullptr, f->d_slot_atom,
       (const typename FracT<R>::T*)f->d_frac, (const typename KRec<R>::T*)f->d_krec, f->at.force,
       f->d_eslot, f->d_status);
   f->launches++;
+}
+
+template <class R, bool LJ, bool COUL, bool RBE, bool MOLEC>
+void launch_near_e(rbmd_force* f, cudaStream_t s) {
+  if (f->minimg) {
+    if (f->want_energy) launch_near_t<R, LJ, COUL, RBE, MOLEC, true, true>(f, s);
+    else launch_near_t<R, LJ, COUL, RBE, MOLEC, true, false>(f, s);
+  } else {
+    if (f->want_energy) launch_near_t<R, LJ, COUL, RBE, MOLEC, false, true>(f, s);
+    else launch_near_t<R, LJ, COUL, RBE, MOLEC, false, false>(f, s);
+  }
 }
 
 template <class R>
@@ -390,14 +404,14 @@ void launch_near(rbmd_force* f, cudaStream_t s) {
   const bool coul = f->with_coul_near();
   const bool molec = f->at.molecule != nullptr;
   if (!coul) {
-    if (molec) launch_near_t<R, true, false, false, true>(f, s);
-    else launch_near_t<R, true, false, false, false>(f, s);
+    if (molec) launch_near_e<R, true, false, false, true>(f, s);
+    else launch_near_e<R, true, false, false, false>(f, s);
   } else if (rbe) {
-    if (molec) launch_near_t<R, true, true, true, true>(f, s);
-    else launch_near_t<R, true, true, true, false>(f, s);
+    if (molec) launch_near_e<R, true, true, true, true>(f, s);
+    else launch_near_e<R, true, true, true, false>(f, s);
   } else {
-    if (molec) launch_near_t<R, true, true, false, true>(f, s);
-    else launch_near_t<R, true, true, false, false>(f, s);
+    if (molec) launch_near_e<R, true, true, false, true>(f, s);
+    else launch_near_e<R, true, true, false, false>(f, s);
   }
 }
 
@@ -465,6 +479,7 @@ void launch_force_tail(rbmd_force* f, cudaStream_t s) {
 
 template <class R>
 void launch_compute(rbmd_force* f, cudaStream_t s) {
+  f->want_energy = true;
   cudaMemsetAsync(f->d_maxcount, 0, sizeof(int), s);
   launch_sort<R>(f, s, true);
   launch_force_tail<R>(f, s);
@@ -513,6 +528,7 @@ void launch_step(rbmd_force* f, cudaStream_t s) {
   mp.save_old = shake ? 1 : 0;
   mp.apply_scale = f->pending_scale ? 1 : 0;
   mp.nh = f->tstat == 3;
+  f->want_energy = f->energy_every > 0 && ((f->step_count + 1) % f->energy_every == 0);
   cudaMemsetAsync(f->d_maxcount, 0, sizeof(int), s);
   cudaMemsetAsync(f->d_cell_count, 0, sizeof(int) * f->ncell_total, s);
   // stages 1-2: kick, drift + wrap, bin (binning sees the unconstrained positions, as the
@@ -622,6 +638,7 @@ rbmd_status parse_config(rbmd_force* f, const char* text) {
   }
   f->u = units_for(f->unit);
   f->dt = num(root, "execution.timestep", 0.005);
+  f->energy_every = (int)num(root, "outputs.thermo_out.interval", 0.0);
   std::vector<double> T = nums(root, "execution.temperature");
   f->T0 = T.size() > 0 ? T[0] : 1.0;
   f->Tdamp = T.size() > 2 ? T[2] : 1.0;
@@ -687,9 +704,11 @@ rbmd_status upload_ksamples(rbmd_force* f, const int32_t* m_xyz) {
     rec[0] = m_xyz[3 * g];
     rec[1] = m_xyz[3 * g + 1];
     rec[2] = m_xyz[3 * g + 2];
-    rec[3] = g / f->P;
     if (rec[0] == 0 && rec[1] == 0 && rec[2] == 0) return RBMD_ERR_ARG;
   }
+  std::vector<int> krep(f->Ptot);
+  for (int g = 0; g < f->Ptot; ++g) krep[g] = g / f->P;
+  CK(cudaMemcpy(f->d_krep, krep.data(), sizeof(int) * f->Ptot, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(f->d_krec, buf.data(), buf.size(), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(f->d_kvec, m_xyz, sizeof(int) * 3 * f->Ptot, cudaMemcpyHostToDevice));
   f->injected = true;
@@ -811,6 +830,11 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
   }
   f->ncell_total = cell_base;
   f->stride = (f->n + 31) & ~31;
+  // MinDistanceVec is the identity for listed pairs when every axis has >= 3 cells
+  f->minimg = false;
+  for (int r = 0; r < nrep; ++r)
+    for (int d = 0; d < 3; ++d)
+      if (f->reps_h[r].dims[d] < 3) f->minimg = true;
   // list capacity from the densest replica (reference: rho * ceil(4/3 pi rc^3) + 1,
   // ExecutionMD.cpp:683); a margin absorbs fluctuations, overflow triggers regrowth.
   double rho_max = 0;
@@ -893,17 +917,27 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
     CK(cudaMalloc(&f->d_krec, (size_t)f->Ptot * recb));
     CK(cudaMemset(f->d_krec, 0, (size_t)f->Ptot * recb));
     CK(dalloc(&f->d_kvec, (size_t)3 * f->Ptot));
+    CK(dalloc(&f->d_krep, (size_t)f->Ptot));
+    {
+      std::vector<int> krep(f->Ptot);
+      for (int g = 0; g < f->Ptot; ++g) krep[g] = g / f->P;
+      CK(cudaMemcpy(f->d_krep, krep.data(), sizeof(int) * f->Ptot, cudaMemcpyHostToDevice));
+    }
     CK(dalloc(&f->d_rho, (size_t)f->Ptot));
     CK(dalloc(&f->d_ek, (size_t)f->Ptot));
-    // structure-factor work items: (replica, chunk, tile)
+    // structure-factor work items (replica, chunk, tile): a block has 32*kKL samples per warp and
+    // at most 8 warps; chunks are sized for about four resident waves of blocks
+    const int warps = std::min(8, (std::min(f->P, 8 * 32 * kKL) + 32 * kKL - 1) / (32 * kKL));
+    f->rho_threads = 32 * warps;
+    f->ktile = f->rho_threads * kKL;
     std::vector<RhoItem> items;
     std::vector<RhoRep> rr(nrep);
-    const int target = 148 * 8;
+    const int ntiles = (f->P + f->ktile - 1) / f->ktile;
+    const double target_blocks = 148.0 * (2048 / f->rho_threads) * 2.0;
+    const double chunk_atoms = std::max(256.0, (double)f->n * ntiles / target_blocks);
     for (int r = 0; r < nrep; ++r) {
       const int Nr = (int)(f->rep_off[r + 1] - f->rep_off[r]);
-      const int ntiles = (f->P + kKT - 1) / kKT;
-      int nch = (int)std::lround((double)target * Nr / (double)f->n / ntiles);
-      nch = std::max(1, std::min(nch, (Nr + 255) / 256));
+      const int nch = std::max(1, (int)std::lround(Nr / chunk_atoms));
       rr[r].item_base = (int)items.size();
       rr[r].ntiles = ntiles;
       rr[r].nchunks = nch;
@@ -914,8 +948,8 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
           RhoItem it;
           it.atom_begin = b;
           it.atom_end = e;
-          it.k_first = f->reps_h[r].k_begin + t * kKT;
-          it.k_count = std::min(kKT, f->P - t * kKT);
+          it.k_first = f->reps_h[r].k_begin + t * f->ktile;
+          it.k_count = std::min(f->ktile, f->P - t * f->ktile);
           items.push_back(it);
         }
       }
@@ -925,8 +959,21 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
     CK(cudaMemcpy(f->d_items, items.data(), sizeof(RhoItem) * items.size(), cudaMemcpyHostToDevice));
     CK(dalloc(&f->d_rhorep, (size_t)nrep));
     CK(cudaMemcpy(f->d_rhorep, rr.data(), sizeof(RhoRep) * nrep, cudaMemcpyHostToDevice));
-    CK(cudaMalloc(&f->d_partial, (size_t)f->nitems * 2 * kKT * (fp64 ? sizeof(double) : sizeof(float))));
-    // sampler tables (Distribution_q, rbmd/framework/model/RBEPSample.h:97-114, tabulated in FP64)
+    CK(cudaMalloc(&f->d_partial, (size_t)f->nitems * f->ktile * 2 * (fp64 ? sizeof(double) : sizeof(float))));
+    // shared-memory staging of k records in the force pass: the largest k range a 128-slot block
+    // spans (slots keep replicas contiguous), capped by kStageBytes
+    {
+      int need = 0;
+      for (int b0 = 0; b0 < f->n; b0 += 128) {
+        const int last = std::min(f->n, b0 + 128) - 1;
+        const int ra = rep_of[b0], rb = rep_of[last];
+        need = std::max(need, (rb - ra + 1) * f->P);
+      }
+      const int cap_recs = kStageBytes / (int)recb;
+      f->kstage = need <= cap_recs ? need : 0;
+    }
+    // sampler tables: G(m) = exp(-pi^2 m^2 / (alpha L^2)) / q(m) with q the rounding pmf of the
+    // Gaussian proposal (Distribution_P / Distribution_q, rbmd/framework/model/RBEPSample.h:86-114)
     std::vector<SamplerRep> sr(nrep);
     std::vector<double> qtab;
     for (int r = 0; r < nrep; ++r) {
@@ -935,15 +982,17 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
       s.qmax = 0;
       for (int d = 0; d < 3; ++d) {
         s.sigma[d] = std::sqrt(f->alpha / 2.0) * L[d] / M_PI;
-        s.c[d] = M_PI * M_PI / (f->alpha * L[d] * L[d]);
         s.qmax = std::max(s.qmax, (int)std::ceil(14.0 * s.sigma[d]) + 8);
       }
-      s.q_offset = (int)qtab.size();
+      s.g_offset = (int)qtab.size();
       for (int d = 0; d < 3; ++d) {
         const double sc = std::sqrt(f->alpha * L[d] * L[d] / (M_PI * M_PI));
-        qtab.push_back(std::erf(0.5 / sc));
-        for (int m = 1; m <= s.qmax; ++m)
-          qtab.push_back((std::erf((0.5 + m) / sc) - std::erf((m - 0.5) / sc)) / 2.0);
+        const double c = M_PI * M_PI / (f->alpha * L[d] * L[d]);
+        for (int m = 0; m <= s.qmax; ++m) {
+          const double q = m == 0 ? std::erf(0.5 / sc)
+                                  : (std::erf((0.5 + m) / sc) - std::erf((m - 0.5) / sc)) / 2.0;
+          qtab.push_back(q > 0 ? std::exp(-c * (double)m * (double)m) / q : INFINITY);
+        }
       }
     }
     CK(dalloc(&f->d_srep, (size_t)nrep));
@@ -1073,7 +1122,7 @@ rbmd_status rbmd_force_sample_k(rbmd_force* f, int64_t step, int32_t* m_xyz, int
   if (!f || !f->bound || !f->is_rbe() || P != f->P || f->coul_type != "RBE") return RBMD_ERR_ARG;
   const int recb = f->fp64 ? sizeof(KRec64) : sizeof(KRec32);
   k_sample<kSamplerD><<<f->nrep, 256>>>(f->nrep, f->d_srep, f->d_qtab, f->d_reps, f->seed, step,
-                                         f->d_kvec, f->d_krec, recb, f->d_status);
+                                         f->d_kvec, f->d_krec, recb, f->d_krep, f->d_status);
   CK(cudaGetLastError());
   CK(cudaDeviceSynchronize());
   if (m_xyz) CK(cudaMemcpy(m_xyz, f->d_kvec, sizeof(int) * 3 * f->Ptot, cudaMemcpyDeviceToHost));

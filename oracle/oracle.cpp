@@ -12,6 +12,7 @@
 // anchored on the reference's own data (ERF table, funcfl files) and on analytic known answers
 // (Madelung constant, Newton's third law, finite differences).  See tests/golden/.
 #include <cmath>
+#include <math.h>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -272,25 +273,30 @@ inline void coul_force(const Real* pi, const Real* pj, Real qi, Real qj, Real rc
 // ------------------------------------------------------------------------------------------
 struct SamplerTables {
   double sigma[3];
-  double c[3];                 // pi^2 / (alpha L^2): log P(m) = -c m^2 + const
-  int qmax;                    // q tabulated for |m| <= qmax
-  std::vector<double> q[3];
+  int qmax;                    // tables cover |m| <= qmax
+  std::vector<double> G[3];    // G[m] = exp(-c m^2) / q(m), c = pi^2 / (alpha L^2)
 };
 
+// Distribution_P / Distribution_q (rbmd/framework/model/RBEPSample.h:86-114): the MH ratio
+// (P(m')/P(m)) (q(m)/q(m')) equals G(m')/G(m) with G = P/q up to the constant 1/H, so
+// u <= min(1, ratio) is evaluated as u * G(m) <= G(m').  Tables in FP64; G = +inf where q
+// underflows (such a proposal is always accepted, as the ratio is infinite).
 SamplerTables sampler_tables(double alpha, const double* L) {
   SamplerTables t;
   t.qmax = 0;
   for (int d = 0; d < 3; ++d) {
     t.sigma[d] = std::sqrt(alpha / 2.0) * L[d] / M_PI;
-    t.c[d] = M_PI * M_PI / (alpha * L[d] * L[d]);
     t.qmax = std::max(t.qmax, (int)std::ceil(14.0 * t.sigma[d]) + 8);
   }
   for (int d = 0; d < 3; ++d) {
-    double s = std::sqrt(alpha * L[d] * L[d] / (M_PI * M_PI));
-    t.q[d].resize(t.qmax + 1);
-    t.q[d][0] = std::erf(0.5 / s);
-    for (int m = 1; m <= t.qmax; ++m)
-      t.q[d][m] = (std::erf((0.5 + m) / s) - std::erf((m - 0.5) / s)) / 2.0;
+    const double s = std::sqrt(alpha * L[d] * L[d] / (M_PI * M_PI));
+    const double c = M_PI * M_PI / (alpha * L[d] * L[d]);
+    t.G[d].resize(t.qmax + 1);
+    for (int m = 0; m <= t.qmax; ++m) {
+      const double q = m == 0 ? std::erf(0.5 / s)
+                              : (std::erf((0.5 + m) / s) - std::erf((m - 0.5) / s)) / 2.0;
+      t.G[d][m] = q > 0 ? std::exp(-c * (double)m * (double)m) / q : INFINITY;
+    }
   }
   return t;
 }
@@ -311,9 +317,9 @@ inline double gauss_draw(uint32_t k0, uint32_t k1, int64_t step, int rep, int ax
   return std::sqrt(-2.0 * std::log(U1)) * std::cos(2.0 * M_PI * U2);
 }
 
-inline double qval(const SamplerTables& t, int d, int m) {
+inline double gval(const SamplerTables& t, int d, int m) {
   m = std::abs(m);
-  return m <= t.qmax ? t.q[d][m] : 0.0;
+  return m <= t.qmax ? t.G[d][m] : INFINITY;
 }
 
 void rbe_sample(const SamplerTables& t, uint64_t seed, int64_t step, int rep, int P, int32_t* out) {
@@ -337,11 +343,7 @@ void rbe_sample(const SamplerTables& t, uint64_t seed, int64_t step, int rep, in
       double ua;
       double g = gauss_draw(k0, k1, step, rep, d, draw, &ua);
       int mw = (int)std::round(t.sigma[d] * g);
-      int m = X0[d];
-      double qm = qval(t, d, m), qw = qval(t, d, mw);
-      double prob = std::exp(t.c[d] * ((double)m * m - (double)mw * mw)) * (qm / qw);
-      if (!(prob < 1.0)) prob = 1.0;
-      X1[d] = (ua <= prob) ? mw : m;
+      X1[d] = (ua * gval(t, d, X0[d]) <= gval(t, d, mw)) ? mw : X0[d];
     }
     ++draw;
     X0[0] = X1[0]; X0[1] = X1[1]; X0[2] = X1[2];
