@@ -39,8 +39,8 @@ CPU_SAMPLE_ATOMS = 100_000
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--atoms", type=int, default=N_ATOMS)
     ap.add_argument("--P", type=int, default=P_PLAIN)

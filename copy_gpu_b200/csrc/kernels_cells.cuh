@@ -39,54 +39,89 @@ __global__ void k_bin(int n, const double* __restrict__ pos, const int* __restri
   atomicAdd(&cell_count[c], 1);
 }
 
-// Exclusive scan of cell counts (one block of 1024 threads, each owning a contiguous chunk),
-// cell_start[ncell] = n.  Also clears the scatter cursors and flags over-full cells.
-__global__ void __launch_bounds__(1024) k_scan_cells(int ncell, const int* __restrict__ count,
-                                                     int* __restrict__ start, int* __restrict__ cursor,
-                                                     uint32_t* status) {
-  __shared__ int warp_sums[32];
-  const int t = threadIdx.x, nt = blockDim.x;
-  const int chunk = (ncell + nt - 1) / nt;
-  const int b = t * chunk, e = min(ncell, b + chunk);
-  int local = 0, mx = 0;
-  for (int c = b; c < e; ++c) {
-    int v = count[c];
-    local += v;
+// Exclusive scan of the cell counts in two parallel passes: k_cell_block_sums reduces blocks of
+// kScanBlock cells; k_cell_scan gives each block its prefix (sum of the preceding block sums)
+// and scans its cells.  cell_start[ncell] = n; scatter cursors are cleared; over-full cells flag.
+// `rebuild` (nullable): skip the pass when the neighbour list is being reused.
+constexpr int kScanBlock = 4096;
+
+__global__ void __launch_bounds__(1024) k_cell_block_sums(int ncell, const int* __restrict__ count,
+                                                          int* __restrict__ block_sums,
+                                                          const int* __restrict__ rebuild,
+                                                          uint32_t* status) {
+  if (rebuild && !*rebuild) return;
+  __shared__ int red[32];
+  const int b0 = blockIdx.x * kScanBlock;
+  int s = 0, mx = 0;
+  for (int c = b0 + threadIdx.x; c < min(ncell, b0 + kScanBlock); c += blockDim.x) {
+    const int v = count[c];
+    s += v;
     mx = max(mx, v);
   }
   if (mx > kMaxCellAtoms) set_flag(status, kFlagCellOverflow);
-  // block exclusive scan of `local`
-  int lane = t & 31, w = t >> 5;
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    block_sums[blockIdx.x] = t;
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_cell_scan(int ncell, const int* __restrict__ count,
+                                                    const int* __restrict__ block_sums,
+                                                    int* __restrict__ start, int* __restrict__ cursor,
+                                                    const int* __restrict__ rebuild) {
+  if (rebuild && !*rebuild) return;
+  __shared__ int warp_sums[32];
+  __shared__ int base_sh;
+  const int t = threadIdx.x, nt = blockDim.x;
+  const int b0 = blockIdx.x * kScanBlock, b1 = min(ncell, b0 + kScanBlock);
+  if (t < 32) {
+    int v = 0;
+    for (int b = t; b < (int)blockIdx.x; b += 32) v += block_sums[b];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (t == 0) base_sh = v;
+  }
+  // each thread owns kScanBlock / nt consecutive cells
+  const int per = kScanBlock / nt;
+  const int c0 = b0 + t * per;
+  int local = 0;
+  for (int c = c0; c < min(b1, c0 + per); ++c) local += count[c];
+  const int lane = t & 31, w = t >> 5;
   int incl = local;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    int y = __shfl_up_sync(0xffffffffu, incl, o);
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
     if (lane >= o) incl += y;
   }
   if (lane == 31) warp_sums[w] = incl;
   __syncthreads();
   if (w == 0) {
-    int v = lane < (nt >> 5) ? warp_sums[lane] : 0;
+    const int v = lane < (nt >> 5) ? warp_sums[lane] : 0;
     int inc2 = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      int y = __shfl_up_sync(0xffffffffu, inc2, o);
+      const int y = __shfl_up_sync(0xffffffffu, inc2, o);
       if (lane >= o) inc2 += y;
     }
     warp_sums[lane] = inc2 - v;
   }
   __syncthreads();
-  int run = warp_sums[w] + incl - local;
-  for (int c = b; c < e; ++c) {
+  int run = base_sh + warp_sums[w] + incl - local;
+  for (int c = c0; c < min(b1, c0 + per); ++c) {
     start[c] = run;
     cursor[c] = 0;
     run += count[c];
   }
-  if (t == nt - 1) start[ncell] = run;
+  if (b1 == ncell && t == nt - 1) start[ncell] = run;
 }
 
 __global__ void k_scatter(int n, const int* __restrict__ cell_of, const int* __restrict__ start,
-                          int* __restrict__ cursor, int* __restrict__ tmp_slot_atom) {
+                          int* __restrict__ cursor, int* __restrict__ tmp_slot_atom,
+                          const int* __restrict__ rebuild) {
+  if (rebuild && !*rebuild) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int c = cell_of[i];
@@ -103,7 +138,8 @@ __global__ void __launch_bounds__(256) k_cell_sort_gather(
     const int* __restrict__ type, const int* __restrict__ mol, const int* __restrict__ rep_of,
     const RepDev* __restrict__ reps, int* __restrict__ slot_atom, int* __restrict__ atom_slot,
     typename Traits<R>::V4* __restrict__ pos4, void* __restrict__ frac_out,
-    int2* __restrict__ meta) {
+    int2* __restrict__ meta, double* __restrict__ xref, const int* __restrict__ rebuild) {
+  if (rebuild && !*rebuild) return;
   __shared__ int ids[8][kMaxCellAtoms];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int cell = blockIdx.x * 8 + w;
@@ -126,6 +162,7 @@ __global__ void __launch_bounds__(256) k_cell_sort_gather(
     atom_slot[id] = slot;
     const double x = pos[3 * id], y = pos[3 * id + 1], z = pos[3 * id + 2];
     const double q = charge ? charge[id] : 0.0;
+    if (xref) { xref[3 * id] = x; xref[3 * id + 1] = y; xref[3 * id + 2] = z; }
     typename Traits<R>::V4 v;
     v.x = (R)x; v.y = (R)y; v.z = (R)z; v.w = (R)q;
     pos4[slot] = v;
@@ -164,7 +201,8 @@ template <class R>
 __global__ void k_regather(int n, const int* __restrict__ slot_atom, const double* __restrict__ pos,
                            const double* __restrict__ charge, const int* __restrict__ rep_of,
                            const RepDev* __restrict__ reps, typename Traits<R>::V4* __restrict__ pos4,
-                           void* __restrict__ frac_out) {
+                           void* __restrict__ frac_out, const int* __restrict__ rebuild) {
+  if (rebuild && *rebuild) return;   // the cell sort refreshed the caches this step
   int slot = blockIdx.x * blockDim.x + threadIdx.x;
   if (slot >= n) return;
   int id = slot_atom[slot];
@@ -210,7 +248,8 @@ __global__ void __launch_bounds__(128) k_nlist(
     int n, const typename Traits<R>::V4* __restrict__ pos4, const int* __restrict__ cell_start,
     const RepDev* __restrict__ reps, const int* __restrict__ rep_of_slot, int num_cycles, R rc,
     int cap, int stride, int* __restrict__ nbr, int* __restrict__ count, int* __restrict__ max_count,
-    uint32_t* status) {
+    uint32_t* status, const int* __restrict__ rebuild) {
+  if (rebuild && !*rebuild) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];

@@ -26,7 +26,8 @@ __global__ void k_kick_drift(MdParams mp, double* __restrict__ pos, double* __re
                              int* __restrict__ image, const int* __restrict__ rep_of,
                              const RepDev* __restrict__ reps, const double* __restrict__ lambda,
                              double* __restrict__ x_old, double* __restrict__ v_old,
-                             int* __restrict__ cell_of, int* __restrict__ cell_count, uint32_t* status) {
+                             int* __restrict__ cell_of, int* __restrict__ cell_count, uint32_t* status,
+                             const double* __restrict__ xref, double half_skin2, int* __restrict__ rebuild) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= mp.n) return;
   const int r = rep_of ? rep_of[i] : 0;
@@ -56,6 +57,16 @@ __global__ void k_kick_drift(MdParams mp, double* __restrict__ pos, double* __re
   }
   if (bad) set_flag(status, kFlagOutOfBox);
   if (!isfinite(x[0]) || !isfinite(x[1]) || !isfinite(x[2])) set_flag(status, kFlagNonFinite);
+  if (xref) {   // Verlet skin: rebuild once any atom moved more than skin/2 since the last build
+    double d2 = 0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      double dd = x[d] - xref[3 * i + d];
+      if (fabs(dd) > 0.5 * rp.box_d[d]) dd -= (dd > 0 ? rp.box_d[d] : -rp.box_d[d]);
+      d2 += dd * dd;
+    }
+    if (d2 > half_skin2 && *rebuild == 0) atomicExch(rebuild, 1);
+  }
   const int c = cell_of_pos<R>(rp, (R)x[0], (R)x[1], (R)x[2]);
   cell_of[i] = c;
   atomicAdd(&cell_count[c], 1);
@@ -117,10 +128,14 @@ __global__ void k_thermo(ThermoParams tp, const int* __restrict__ chunk_begin_of
                          const double* __restrict__ ke_partial, double* __restrict__ ke_out,
                          double* __restrict__ T_out, double* __restrict__ lambda,
                          double* __restrict__ xi, const RepDev* __restrict__ reps) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  // one warp per replica, fixed-order lane sums then a butterfly: deterministic
+  const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
   if (r >= tp.nrep) return;
   double s = 0;
-  for (int c = chunk_begin_of_rep[r]; c < chunk_begin_of_rep[r + 1]; ++c) s += ke_partial[c];
+  for (int c = chunk_begin_of_rep[r] + lane; c < chunk_begin_of_rep[r + 1]; c += 32) s += ke_partial[c];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane != 0) return;
   s *= tp.mvv2e;
   const double n = (double)(reps[r].atom_end - reps[r].atom_begin);
   double T;

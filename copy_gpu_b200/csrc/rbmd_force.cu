@@ -83,6 +83,7 @@ struct rbmd_force {
   double near_coul_scale = 1.0;
   double shake_tol = 1e-5;
   int energy_every = 0;   // energies inside step(): every outputs.thermo_out.interval steps
+  int cap_override = 0;   // neighbor.capacity: initial list capacity (grown on overflow)
   int shake_max_iter = 5000;
   std::string potential_file;
 
@@ -122,6 +123,8 @@ struct rbmd_force {
   void* d_frac = nullptr;
   int2* d_meta = nullptr;
   int *d_nbr = nullptr, *d_count = nullptr, *d_maxcount = nullptr;
+  int *d_rebuild = nullptr, *d_block_sums = nullptr;
+  double* d_xref = nullptr;
   uint32_t* d_status = nullptr;
   double* d_eslot = nullptr;   // 2 per slot (lj, coul)
   double* d_esum = nullptr;    // scratch sums
@@ -235,6 +238,7 @@ void free_all(rbmd_force* f) {
   if (f->d_frac) cudaFree(f->d_frac);
   f->d_frac = nullptr;
   dfree(f->d_meta); dfree(f->d_nbr); dfree(f->d_count); dfree(f->d_maxcount); dfree(f->d_status);
+  dfree(f->d_rebuild); dfree(f->d_block_sums); dfree(f->d_xref);
   dfree(f->d_eslot); dfree(f->d_esum);
   if (f->d_krec) cudaFree(f->d_krec);
   f->d_krec = nullptr;
@@ -311,7 +315,7 @@ void launch_nlist(rbmd_force* f, cudaStream_t s) {
   k_nlist<R><<<nb, 128, 0, s>>>(f->n, (const typename Traits<R>::V4*)f->d_pos4, f->d_cell_start,
                                 f->d_reps, f->nrep > 1 ? f->d_rep_of : nullptr, f->num_cycles,
                                 (R)f->list_cut(), f->cap, f->stride, f->d_nbr, f->d_count,
-                                f->d_maxcount, f->d_status);
+                                f->d_maxcount, f->d_status, f->skin > 0 ? f->d_rebuild : nullptr);
   f->launches++;
 }
 
@@ -319,27 +323,37 @@ template <class R>
 void launch_sort(rbmd_force* f, cudaStream_t s, bool bin) {
   PhaseScope ps(f, kPhSort, s);
   const int n = f->n;
+  const int* rb = f->skin > 0 ? f->d_rebuild : nullptr;
   if (bin) {
     cudaMemsetAsync(f->d_cell_count, 0, sizeof(int) * f->ncell_total, s);
     k_bin<R><<<(n + 255) / 256, 256, 0, s>>>(n, f->at.pos, f->nrep > 1 ? f->d_rep_of : nullptr,
                                              f->d_reps, f->d_cell_of, f->d_cell_count, f->d_status);
     f->launches++;
   }
-  k_scan_cells<<<1, 1024, 0, s>>>(f->ncell_total, f->d_cell_count, f->d_cell_start, f->d_cursor,
-                                  f->d_status);
-  k_scatter<<<(n + 255) / 256, 256, 0, s>>>(n, f->d_cell_of, f->d_cell_start, f->d_cursor, f->d_tmp);
+  const int nblk = (f->ncell_total + kScanBlock - 1) / kScanBlock;
+  k_cell_block_sums<<<nblk, 1024, 0, s>>>(f->ncell_total, f->d_cell_count, f->d_block_sums, rb, f->d_status);
+  k_cell_scan<<<nblk, 1024, 0, s>>>(f->ncell_total, f->d_cell_count, f->d_block_sums, f->d_cell_start,
+                                    f->d_cursor, rb);
+  k_scatter<<<(n + 255) / 256, 256, 0, s>>>(n, f->d_cell_of, f->d_cell_start, f->d_cursor, f->d_tmp, rb);
   k_cell_sort_gather<R><<<(f->ncell_total + 7) / 8, 256, 0, s>>>(
       f->ncell_total, f->d_cell_start, f->d_tmp, f->at.pos, f->at.charge, f->at.type, f->at.molecule,
       f->nrep > 1 ? f->d_rep_of : nullptr, f->d_reps, f->d_slot_atom, f->d_atom_slot,
-      (typename Traits<R>::V4*)f->d_pos4, f->is_rbe() ? f->d_frac : nullptr, f->d_meta);
-  f->launches += 3;
+      (typename Traits<R>::V4*)f->d_pos4, f->is_rbe() ? f->d_frac : nullptr, f->d_meta, f->d_xref, rb);
+  f->launches += 4;
+  if (rb) {
+    // list reuse: refresh the slot caches from the new positions (no-op on rebuild steps)
+    k_regather<R><<<(n + 255) / 256, 256, 0, s>>>(
+        n, f->d_slot_atom, f->at.pos, f->at.charge, f->nrep > 1 ? f->d_rep_of : nullptr, f->d_reps,
+        (typename Traits<R>::V4*)f->d_pos4, f->is_rbe() ? f->d_frac : nullptr, rb);
+    f->launches++;
+  }
 }
 
 template <class R>
 void launch_regather(rbmd_force* f, cudaStream_t s) {
   k_regather<R><<<(f->n + 255) / 256, 256, 0, s>>>(
       f->n, f->d_slot_atom, f->at.pos, f->at.charge, f->nrep > 1 ? f->d_rep_of : nullptr, f->d_reps,
-      (typename Traits<R>::V4*)f->d_pos4, f->is_rbe() ? f->d_frac : nullptr);
+      (typename Traits<R>::V4*)f->d_pos4, f->is_rbe() ? f->d_frac : nullptr, nullptr);
   f->launches++;
 }
 
@@ -481,6 +495,7 @@ template <class R>
 void launch_compute(rbmd_force* f, cudaStream_t s) {
   f->want_energy = true;
   cudaMemsetAsync(f->d_maxcount, 0, sizeof(int), s);
+  if (f->d_rebuild) cudaMemsetAsync(f->d_rebuild, 1, sizeof(int), s);   // nonzero: rebuild
   launch_sort<R>(f, s, true);
   launch_force_tail<R>(f, s);
 }
@@ -531,6 +546,7 @@ void launch_step(rbmd_force* f, cudaStream_t s) {
   f->want_energy = f->energy_every > 0 && ((f->step_count + 1) % f->energy_every == 0);
   cudaMemsetAsync(f->d_maxcount, 0, sizeof(int), s);
   cudaMemsetAsync(f->d_cell_count, 0, sizeof(int) * f->ncell_total, s);
+  if (f->skin > 0) cudaMemsetAsync(f->d_rebuild, 0, sizeof(int), s);
   // stages 1-2: kick, drift + wrap, bin (binning sees the unconstrained positions, as the
   // reference's locator.SetPosition runs before ConstraintA)
   {
@@ -538,7 +554,9 @@ void launch_step(rbmd_force* f, cudaStream_t s) {
     k_kick_drift<R><<<(n + 255) / 256, 256, 0, s>>>(mp, f->at.pos, f->at.vel, f->at.force, f->at.mass,
                                                     f->at.image, f->nrep > 1 ? f->d_rep_of : nullptr,
                                                     f->d_reps, f->d_lambda, f->d_xold, f->d_vold,
-                                                    f->d_cell_of, f->d_cell_count, f->d_status);
+                                                    f->d_cell_of, f->d_cell_count, f->d_status,
+                                                    f->skin > 0 ? f->d_xref : nullptr,
+                                                    0.25 * f->skin * f->skin, f->d_rebuild);
     f->launches++;
   }
   launch_sort<R>(f, s, false);
@@ -589,7 +607,7 @@ void launch_step(rbmd_force* f, cudaStream_t s) {
   tp.Tdamp = f->Tdamp;
   tp.T0 = f->T0;
   tp.dof_mode = f->dof_mode;
-  k_thermo<<<(f->nrep + 127) / 128, 128, 0, s>>>(tp, f->d_chunk_rep_begin, f->d_ke_partial, f->d_ke,
+  k_thermo<<<(f->nrep + 3) / 4, 128, 0, s>>>(tp, f->d_chunk_rep_begin, f->d_ke_partial, f->d_ke,
                                                 f->d_T, f->d_lambda, f->d_xi, f->d_reps);
   f->launches++;
   f->pending_scale = (f->tstat == 1 || f->tstat == 2);
@@ -616,6 +634,7 @@ rbmd_status parse_config(rbmd_force* f, const char* text) {
   }
   f->rs = f->nbr_type == "RBL" ? num(root, "hyper_parameters.neighbor.r_core", f->rc) : f->rc;
   f->skin = num(root, "hyper_parameters.neighbor.skin", 0.0);
+  f->cap_override = (int)num(root, "hyper_parameters.neighbor.capacity", 0.0);
   f->far = root.path("hyper_parameters.coulomb") != nullptr;
   if (f->far) {
     f->coul_type = rbmdjson::text(root, "hyper_parameters.coulomb.type", "RBE");
@@ -842,6 +861,7 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
     rho_max = std::max(rho_max, (f->rep_off[r + 1] - f->rep_off[r]) / f->reps_h[r].volume);
   const double lc = f->list_cut();
   f->cap = ((int)(1.5 * rho_max * 4.0 / 3.0 * M_PI * lc * lc * lc) + 32 + 7) & ~7;
+  if (f->cap_override > 0) f->cap = f->cap_override;
   const size_t n = f->n;
   const bool fp64 = f->fp64;
   CK(dalloc(&f->d_reps, nrep));
@@ -865,6 +885,10 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
   CK(dalloc(&f->d_nbr, (size_t)f->cap * f->stride));
   CK(dalloc(&f->d_count, n));
   CK(dalloc(&f->d_maxcount, 1));
+  CK(dalloc(&f->d_rebuild, 1));
+  CK(cudaMemset(f->d_rebuild, 0, sizeof(int)));
+  CK(dalloc(&f->d_block_sums, (size_t)(f->ncell_total + kScanBlock - 1) / kScanBlock + 1));
+  if (f->skin > 0) CK(dalloc(&f->d_xref, 3 * n));
   CK(dalloc(&f->d_status, 1));
   CK(cudaMemset(f->d_status, 0, sizeof(uint32_t)));
   CK(dalloc(&f->d_eslot, 2 * n));

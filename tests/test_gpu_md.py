@@ -1,0 +1,283 @@
+"""GPU parity of full MD steps (ExecutionNVT::Solve order) against oracle-driven steps, plus the
+Verlet-skin, EAM, batched-replica and status paths.
+
+Bars: FP64 trajectories agree with the oracle to <= 1e-9 absolute in positions after several
+steps (forces agree to <= 1e-11 relative per step; the residual is summation order); FP32 EAM
+forces <= 1e-5 relative (norm-wise, vs the oracle's reference-precision terms summed exactly).
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from copy_gpu_b200 import Box, systems
+from tests.helpers import jitter, make_ff, rel_err, to_dev
+
+pytestmark = pytest.mark.gpu
+
+
+def _wrap(x, lo, hi):
+    L = hi - lo
+    x = np.where(x < lo, x + L, x)
+    x = np.where(x > hi, x - L, x)
+    return x
+
+
+def _oracle_lj_force(o, pos, s, rc):
+    nl = o.neighbors(pos, s["lo"], s["hi"], rc, "fp64")
+    return o.near_force(pos, s["lo"], s["hi"], rc, nl, type=s["type"], eps=s["eps"], sigma=s["sigma"],
+                        prec="fp64")
+
+
+def test_lj_nve_trajectory_fp64(cuda, oracle_lib):
+    import torch
+    s = systems.lj_fcc(ncell=6, seed=3)
+    s["pos"] = jitter(s["pos"], s["lo"], s["hi"], 0.03, seed=1)
+    cfg = systems.lj_config(cutoff=2.5, precision="fp64", ensemble="NVE")
+    dev = to_dev(s, cuda)
+    ff = make_ff(cfg, s, dev)
+    ff.Execute()
+    nsteps, dt = 10, cfg["execution"]["timestep"]
+    ff.step(nsteps)
+    torch.cuda.synchronize()
+    assert ff.status() == 0
+    x, v, m = s["pos"].copy(), s["vel"].copy(), s["mass"][:, None]
+    F = _oracle_lj_force(oracle_lib, x, s, 2.5)
+    for _ in range(nsteps):
+        v = v + 0.5 * F / m * dt * 1.0
+        x = _wrap(x + v * dt, s["lo"], s["hi"])
+        F = _oracle_lj_force(oracle_lib, x, s, 2.5)
+        v = v + 0.5 * F / m * dt * 1.0
+    assert np.abs(dev["pos"].cpu().numpy() - x).max() < 1e-9
+    assert np.abs(dev["vel"].cpu().numpy() - v).max() < 1e-8
+
+
+def test_skin_list_reuse_same_trajectory(cuda):
+    """Skin 0.3 reuses the list between rebuilds; the forces (pairs within rc) are unchanged."""
+    import torch
+    s = systems.lj_fcc(ncell=6, seed=4)
+    out = {}
+    for skin in (0.0, 0.3):
+        cfg = systems.lj_config(cutoff=2.5, skin=skin, precision="fp64", ensemble="NVE")
+        dev = to_dev(s, cuda)
+        ff = make_ff(cfg, s, dev)
+        ff.Execute()
+        ff.step(40)
+        torch.cuda.synchronize()
+        assert ff.status() == 0
+        out[skin] = dev["pos"].cpu().numpy()
+    assert np.abs(out[0.0] - out[0.3]).max() < 1e-9
+
+
+def test_electrolyte_rbe_steps_fp64(cuda, oracle_lib):
+    """Two steps with the on-device sampler: the oracle draws the same k-samples per step."""
+    import torch
+    n, P = 2000, 48
+    s = systems.electrolyte(n, seed=8)
+    cfg = systems.electrolyte_config(P=P, precision="fp64", seed=77, ensemble="NVE")
+    alpha = cfg["hyper_parameters"]["coulomb"]["alpha"]
+    dt = cfg["execution"]["timestep"]
+    L = s["hi"] - s["lo"]
+    dev = to_dev(s, cuda)
+    ff = make_ff(cfg, s, dev)
+    ff.Execute()                       # step counter 0: samples of step 0
+    ff.step(2)                         # steps 0 and 1 of the step counter
+    torch.cuda.synchronize()
+    assert ff.status() == 0
+
+    def force(x, step):
+        nl = oracle_lib.neighbors(x, s["lo"], s["hi"], 2.5, "fp64")
+        near = oracle_lib.near_force(x, s["lo"], s["hi"], 2.5, nl, type=s["type"], charge=s["charge"],
+                                     eps=s["eps"], sigma=s["sigma"], with_coul=True, alpha=alpha, prec="fp64")
+        m = oracle_lib.rbe_sample(alpha, L, 77, step, 0, P)
+        rho = oracle_lib.rhok(x, s["charge"], L, m)
+        return near + oracle_lib.rbe_force(x, s["charge"], L, alpha, 1.0, m, rho)
+
+    x, v, m = s["pos"].copy(), s["vel"].copy(), s["mass"][:, None]
+    F = force(x, 0)
+    for step in range(2):
+        v = v + 0.5 * F / m * dt
+        x = _wrap(x + v * dt, s["lo"], s["hi"])
+        F = force(x, step)
+        v = v + 0.5 * F / m * dt
+    assert np.abs(dev["pos"].cpu().numpy() - x).max() < 1e-9
+    assert rel_err(dev["force"].cpu().numpy(), F) < 1e-10
+
+
+def test_water_shake_rattle_step_fp64(cuda, oracle_lib):
+    import torch
+    s = systems.water(n_mol=300, seed=2)
+    P = 32
+    cfg = systems.water_config(P=P, precision="fp64", shake_tol=1e-10)
+    cfg["execution"]["ensemble"] = "NVE"
+    cfg["hyper_parameters"]["extend"]["shake_max_iter"] = 500
+    alpha = cfg["hyper_parameters"]["coulomb"]["alpha"]
+    rc = cfg["hyper_parameters"]["neighbor"]["cut_off"]
+    dt = cfg["execution"]["timestep"]
+    fmt2v, qqr2e = 4.186e-4, 332.06371
+    L = s["hi"] - s["lo"]
+    m_k = oracle_lib.rbe_sample(alpha, L, 5, 0, 0, P)
+    dev = to_dev(s, cuda)
+    ff = make_ff(cfg, s, dev)
+    ff.set_ksamples(m_k)
+    ff.Execute()
+    F_dev0 = dev["force"].cpu().numpy().copy()
+
+    def force(x):
+        nl = oracle_lib.neighbors(x, s["lo"], s["hi"], rc, "fp64")
+        near = oracle_lib.near_force(x, s["lo"], s["hi"], rc, nl, type=s["type"], mol=s["molecule"],
+                                     charge=s["charge"], eps=s["eps"], sigma=s["sigma"], with_coul=True,
+                                     alpha=alpha, coul_scale=qqr2e, prec="fp64")
+        rho = oracle_lib.rhok(x, s["charge"], L, m_k)
+        far = oracle_lib.rbe_force(x, s["charge"], L, alpha, qqr2e, m_k, rho)
+        ex, _ = oracle_lib.water_extras(s["hoh"], x, s["charge"], s["lo"], s["hi"], *s["bond"], *s["angle"])
+        return near + far + ex
+
+    F0 = force(s["pos"])
+    assert rel_err(F_dev0, F0) < 1e-10
+    ff.step(1)
+    torch.cuda.synchronize()
+    assert ff.status() == 0
+    m = s["mass"][:, None]
+    x_old, v_old = s["pos"].copy(), s["vel"].copy()
+    v = v_old + 0.5 * F0 / m * dt * fmt2v
+    x = _wrap(x_old + v * dt, s["lo"], s["hi"])
+    x, v, _, bad, _ = oracle_lib.shake(s["hoh"], x_old, v_old, F0, s["mass"], s["lo"], s["hi"], dt, fmt2v,
+                                       tol=1e-10, max_iter=500)
+    assert bad == 0
+    F1 = force(x)
+    v = oracle_lib.rattle(s["hoh"], x, v, F1, s["mass"], s["lo"], s["hi"], dt, fmt2v)
+    got_x = dev["pos"].cpu().numpy()
+    got_v = dev["vel"].cpu().numpy()
+    assert np.abs(got_x - x).max() < 1e-9
+    assert np.abs(got_v - v).max() < 1e-9
+    # constraints hold: O-H = 1.0, H-H from 109.47 deg
+    hoh = s["hoh"]
+    d01 = np.linalg.norm(got_x[hoh[:, 1]] - got_x[hoh[:, 0]], axis=1)
+    assert np.abs(d01 - 1.0).max() < 1e-6
+
+
+def test_shake_nonconvergence_flag(cuda):
+    import torch
+    from copy_gpu_b200 import FLAG_SHAKE_NOCONV
+    s = systems.water(n_mol=64, seed=3)
+    cfg = systems.water_config(P=16, precision="fp64", shake_tol=0.0)
+    cfg["hyper_parameters"]["extend"]["shake_max_iter"] = 3
+    dev = to_dev(s, cuda)
+    ff = make_ff(cfg, s, dev)
+    ff.Execute()
+    ff.step(1)
+    torch.cuda.synchronize()
+    assert ff.status() & FLAG_SHAKE_NOCONV
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_eam_johnson(cuda, oracle_lib, tmp_path, prec):
+    import torch
+    pot = systems.write_johnson_funcfl(str(tmp_path / "johnson.eam"))
+    s = systems.eam_fcc(ncell=8, seed=5)
+    cfg = systems.eam_config(pot, precision=prec)
+    dev = to_dev(s, cuda)
+    ff = make_ff(cfg, s, dev)
+    ff.Execute()
+    torch.cuda.synchronize()
+    assert ff.status() == 0
+    pr = s["pos"].astype(np.float32 if prec == "fp32" else np.float64)
+    nl = oracle_lib.neighbors(pr, s["lo"], s["hi"], 5.0, prec)
+    ref, _ = oracle_lib.eam_force(pot, pr, s["lo"], s["hi"], 5.0, nl, prec=prec, sum_mode=1)
+    err = rel_err(dev["force"].cpu().numpy(), ref)
+    assert err < (1e-5 if prec == "fp32" else 1e-11), err
+
+
+def test_batched_replicas_match_single(cuda):
+    """Replica 0 advanced inside a batch equals replica 0 advanced alone (its sampler stream is
+    keyed by replica index 0 in both runs)."""
+    import torch
+    r = systems.replicas(n_rep=6, nmin=500, nmax=1500, seed=5)
+    P = 24
+    cfg = systems.electrolyte_config(P=P, precision="fp64", seed=31, ensemble="NVE")
+    boxes = [Box(tuple(r["lo"][k]), tuple(r["hi"][k])) for k in range(6)]
+    dev = to_dev(r, cuda)
+    ff = make_ff(cfg, r, dev, boxes=boxes, offsets=r["offsets"])
+    ff.Execute()
+    ff.step(3)
+    torch.cuda.synchronize()
+    assert ff.status() == 0
+    got = dev["pos"].cpu().numpy()
+    off = r["offsets"]
+    sl = slice(off[0], off[1])
+    n0 = off[1]
+    s0 = {key: (val[sl] if isinstance(val, np.ndarray) and val.shape[:1] == (off[-1],) else val)
+          for key, val in r.items()}
+    s0["lo"], s0["hi"] = r["lo"][0], r["hi"][0]
+    assert s0["pos"].shape[0] == n0
+    dev0 = to_dev(s0, cuda)
+    ff0 = make_ff(cfg, s0, dev0)
+    ff0.Execute()
+    ff0.step(3)
+    torch.cuda.synchronize()
+    assert np.abs(dev0["pos"].cpu().numpy() - got[sl]).max() < 1e-12
+
+
+def test_batched_replicas_injected_k(cuda, oracle_lib):
+    """With injected k-samples every replica's force equals its stand-alone force."""
+    import torch
+    r = systems.replicas(n_rep=5, nmin=600, nmax=1200, seed=6)
+    P = 20
+    cfg = systems.electrolyte_config(P=P, precision="fp64", seed=3)
+    alpha = cfg["hyper_parameters"]["coulomb"]["alpha"]
+    boxes = [Box(tuple(r["lo"][k]), tuple(r["hi"][k])) for k in range(5)]
+    ks = np.concatenate([oracle_lib.rbe_sample(alpha, r["hi"][k] - r["lo"][k], 9, 0, k, P) for k in range(5)])
+    dev = to_dev(r, cuda)
+    ff = make_ff(cfg, r, dev, boxes=boxes, offsets=r["offsets"])
+    ff.set_ksamples(ks)
+    ff.Execute()
+    torch.cuda.synchronize()
+    F = dev["force"].cpu().numpy()
+    off = r["offsets"]
+    for k in range(5):
+        sl = slice(off[k], off[k + 1])
+        x = r["pos"][sl]
+        L = r["hi"][k] - r["lo"][k]
+        nl = oracle_lib.neighbors(x, r["lo"][k], r["hi"][k], 2.5, "fp64")
+        near = oracle_lib.near_force(x, r["lo"][k], r["hi"][k], 2.5, nl, type=r["type"][sl],
+                                     charge=r["charge"][sl], eps=r["eps"], sigma=r["sigma"],
+                                     with_coul=True, alpha=alpha, prec="fp64")
+        m = ks[k * P:(k + 1) * P]
+        rho = oracle_lib.rhok(x, r["charge"][sl], L, m, origin=r["lo"][k])
+        far = oracle_lib.rbe_force(x, r["charge"][sl], L, alpha, 1.0, m, rho, origin=r["lo"][k])
+        assert rel_err(F[sl], near + far) < 1e-11
+
+
+def test_nonfinite_position_flag(cuda):
+    import torch
+    from copy_gpu_b200 import FLAG_NONFINITE
+    s = systems.lj_fcc(ncell=4)
+    s["pos"][7, 1] = np.nan
+    cfg = systems.lj_config(precision="fp32")
+    dev = to_dev(s, cuda)
+    ff = make_ff(cfg, s, dev)
+    ff.Execute()
+    torch.cuda.synchronize()
+    assert ff.status() & FLAG_NONFINITE
+
+
+def test_list_capacity_regrowth(cuda, oracle_lib):
+    """An initial list capacity of 4 overflows; the library grows it and recomputes."""
+    import torch
+    s = systems.lj_fcc(ncell=5, seed=9)
+    s["pos"] = jitter(s["pos"], s["lo"], s["hi"], 0.05, seed=2)
+    cfg = systems.lj_config(precision="fp64")
+    cfg["hyper_parameters"]["neighbor"]["capacity"] = 4
+    dev = to_dev(s, cuda)
+    ff = make_ff(cfg, s, dev)
+    ff.Execute()
+    torch.cuda.synchronize()
+    assert ff.status() == 0
+    nl = oracle_lib.neighbors(s["pos"], s["lo"], s["hi"], 2.5, "fp64")
+    ref = oracle_lib.near_force(s["pos"], s["lo"], s["hi"], 2.5, nl, prec="fp64")
+    assert rel_err(dev["force"].cpu().numpy(), ref) < 1e-11
+    ff.step(3)
+    torch.cuda.synchronize()
+    assert ff.status() == 0
