@@ -240,9 +240,32 @@ __global__ void k_regather(int n, const int* __restrict__ slot_atom, const doubl
 __device__ __forceinline__ bool gt_small(float x) { return x > 1.0e-4f; }
 __device__ __forceinline__ bool gt_small(double x) { return x > 1.0e-4; }
 
-// Full Verlet list of slot i: ComputeNeighboursWorklet (rbmd/framework/run/worklet/
-// RunWorklet.cpp:40-96) -- stencil x-offset outermost, z innermost; predicate
-// rc^2 - d^2 > 1e-4 && d^2 > 1e-4 on r = (p_j - offset) - p_i with uncontracted float ops.
+// Full Verlet list of slot i with the predicate of ComputeNeighboursWorklet
+// (rbmd/framework/run/worklet/RunWorklet.cpp:40-96): rc^2 - d^2 > 1e-4 && d^2 > 1e-4 on
+// r = (p_j - offset) - p_i with uncontracted float ops and the reference's cell-based periodic
+// offsets (PeriodicCoordOffset).  Traversal: for each of the (2nc+1)^2 (y, z) neighbour rows the
+// x cells ci-nc .. ci+nc are consecutive cell indices, hence one contiguous slot range when no x
+// wrap occurs; rows that wrap in x are walked cell by cell.  The pair set equals the
+// reference's 27-cell stencil; the order inside a row differs (sets are order-free).
+template <class R>
+__device__ __forceinline__ int nlist_range(int s, const int s1, const typename Traits<R>::V4* __restrict__ pos4,
+                                           const R* pix, const R* off, int code, R cut2, int idx, int cap,
+                                           int stride, int i, int* __restrict__ nbr) {
+#pragma unroll 4
+  for (; s < s1; ++s) {
+    const typename Traits<R>::V4 pj = pos4[s];
+    const R r0 = sub_rn(sub_rn(pj.x, off[0]), pix[0]);
+    const R r1 = sub_rn(sub_rn(pj.y, off[1]), pix[1]);
+    const R r2 = sub_rn(sub_rn(pj.z, off[2]), pix[2]);
+    const R d2 = add_rn(add_rn(mul_rn(r0, r0), mul_rn(r1, r1)), mul_rn(r2, r2));
+    if (gt_small(sub_rn(cut2, d2)) && gt_small(d2)) {
+      if (idx < cap) nbr[(size_t)idx * stride + i] = (s << kShiftBits) | code;
+      ++idx;
+    }
+  }
+  return idx;
+}
+
 template <class R>
 __global__ void __launch_bounds__(128) k_nlist(
     int n, const typename Traits<R>::V4* __restrict__ pos4, const int* __restrict__ cell_start,
@@ -260,41 +283,76 @@ __global__ void __launch_bounds__(128) k_nlist(
   for (int d = 0; d < 3; ++d)
     ci[d] = (int)div_rn(sub_rn(pix[d], Traits<R>::lo(rp, d)), Traits<R>::dx(rp, d));
   const R cut2 = mul_rn(rc, rc);
+  const int nc = num_cycles;
+  const int dx0 = rp.dims[0], dx1 = rp.dims[1], dx2 = rp.dims[2];
+  const bool x_contig = ci[0] - nc >= 0 && ci[0] + nc < dx0;
   int idx = 0;
-  for (int a = -num_cycles; a <= num_cycles; ++a)
-    for (int b = -num_cycles; b <= num_cycles; ++b)
-      for (int c = -num_cycles; c <= num_cycles; ++c) {
-        const int nb[3] = {ci[0] + a, ci[1] + b, ci[2] + c};
-        int wv[3];
-        R off[3];
-        int code = 0;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          int dd = rp.dims[d];
-          int w = ((nb[d] % dd) + dd) % dd;
-          wv[d] = w;
-          int delta = w - nb[d];
-          off[d] = mul_rn(Traits<R>::dx(rp, d), (R)delta);
-          code |= (delta > 0 ? 1 : (delta < 0 ? 2 : 0)) << (2 * d);
-        }
-        const int cell = rp.cell_base + wv[0] + wv[1] * rp.dims[0] + wv[2] * rp.dims[0] * rp.dims[1];
-        const int s1 = cell_start[cell + 1];
-        for (int s = cell_start[cell]; s < s1; ++s) {
-          const typename Traits<R>::V4 pj = pos4[s];
-          const R r0 = sub_rn(sub_rn(pj.x, off[0]), pix[0]);
-          const R r1 = sub_rn(sub_rn(pj.y, off[1]), pix[1]);
-          const R r2 = sub_rn(sub_rn(pj.z, off[2]), pix[2]);
-          const R d2 = add_rn(add_rn(mul_rn(r0, r0), mul_rn(r1, r1)), mul_rn(r2, r2));
-          if (gt_small(sub_rn(cut2, d2)) && gt_small(d2)) {
-            if (idx < cap) nbr[(size_t)idx * stride + i] = (s << kShiftBits) | code;
-            ++idx;
-          }
+  for (int b = -nc; b <= nc; ++b)
+    for (int c = -nc; c <= nc; ++c) {
+      R off[3];
+      const int nby = ci[1] + b, nbz = ci[2] + c;
+      const int wy = ((nby % dx1) + dx1) % dx1, wz = ((nbz % dx2) + dx2) % dx2;
+      const int dy = wy - nby, dz = wz - nbz;
+      off[1] = mul_rn(Traits<R>::dx(rp, 1), (R)dy);
+      off[2] = mul_rn(Traits<R>::dx(rp, 2), (R)dz);
+      const int code_yz = ((dy > 0 ? 1 : (dy < 0 ? 2 : 0)) << 2) | ((dz > 0 ? 1 : (dz < 0 ? 2 : 0)) << 4);
+      const int row = rp.cell_base + wy * dx0 + wz * dx0 * dx1;
+      if (x_contig) {
+        off[0] = (R)0;
+        idx = nlist_range<R>(cell_start[row + ci[0] - nc], cell_start[row + ci[0] + nc + 1], pos4, pix,
+                             off, code_yz, cut2, idx, cap, stride, i, nbr);
+      } else {
+        for (int a = -nc; a <= nc; ++a) {
+          const int nbx = ci[0] + a;
+          const int wx = ((nbx % dx0) + dx0) % dx0;
+          const int ddx = wx - nbx;
+          off[0] = mul_rn(Traits<R>::dx(rp, 0), (R)ddx);
+          const int code = code_yz | (ddx > 0 ? 1 : (ddx < 0 ? 2 : 0));
+          idx = nlist_range<R>(cell_start[row + wx], cell_start[row + wx + 1], pos4, pix, off, code, cut2,
+                               idx, cap, stride, i, nbr);
         }
       }
+    }
   count[i] = idx;
   if (idx > cap) {
     set_flag(status, kFlagListOverflow);
     atomicMax(max_count, idx);
+  }
+}
+
+// Fixed-point fractional coordinates + charge in caller order, the input of every k-space
+// phase: U_d = floor(frac((x_d - lo_d) / L_d) * 2^32) (2^64 for FP64).  Integer phases
+// m . U mod 2^32 are exact.
+template <class R>
+__global__ void k_frac(int n, const double* __restrict__ pos, const double* __restrict__ charge,
+                       const int* __restrict__ rep_of, const RepDev* __restrict__ reps,
+                       void* __restrict__ frac_out) {
+  const int id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= n) return;
+  const RepDev& rp = reps[rep_of ? rep_of[id] : 0];
+  const double q = charge ? charge[id] : 0.0;
+  double u[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    u[d] = (pos[3 * id + d] - rp.lo_d[d]) / rp.box_d[d];
+    u[d] -= floor(u[d]);
+  }
+  if (sizeof(R) == 4) {
+    uint32_t U[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double s = u[d] * 4294967296.0;
+      U[d] = s >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)s;
+    }
+    reinterpret_cast<Frac32*>(frac_out)[id] = Frac32{U[0], U[1], U[2], (float)q};
+  } else {
+    unsigned long long U[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double s = u[d] * 18446744073709551616.0;
+      U[d] = s >= 18446744073709549568.0 ? 0xFFFFFFFFFFFFF800ull : (unsigned long long)s;
+    }
+    reinterpret_cast<Frac64*>(frac_out)[id] = Frac64{U[0], U[1], U[2], q};
   }
 }
 

@@ -104,50 +104,53 @@ __device__ __forceinline__ void rbe_terms(const typename FracT<R>::T& fr, const 
   }
 }
 
-// Per-slot near force (+ fused RBE force).  One thread per slot over its transposed list row.
+// Minimum-image handling of the pair vector in the near pass:
+//   kMiNone  every replica has >= 3 cells per axis and the list is rebuilt every step: listed
+//            pairs have |r_d| < rc < L/2, MinDistanceVec is the identity;
+//   kMiLJ    the reference's semantics for small boxes: MinDistanceVec on the LJ vector only;
+//   kMiAll   Verlet skin: atoms wrapped since the last build make the stored image stale, so
+//            the pair vector itself is reduced to the minimum image.
+constexpr int kMiNone = 0, kMiLJ = 1, kMiAll = 2;
+
+template <class R>
+__device__ __forceinline__ void min_image(R& q0, R& q1, R& q2, const R* box) {
+  if (fabs(q0) > box[0] * (R)0.5) q0 -= (q0 > 0 ? box[0] : -box[0]);
+  if (fabs(q1) > box[1] * (R)0.5) q1 -= (q1 > 0 ? box[1] : -box[1]);
+  if (fabs(q2) > box[2] * (R)0.5) q2 -= (q2 > 0 ? box[2] : -box[2]);
+}
+
+__device__ __forceinline__ float rcp_r(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double rcp_r(double x) { return 1.0 / x; }
+
+// Per-slot near force.  One thread per slot over its transposed list row.
 // Pair physics: ComputeNearForceVerletWorklet / ComputeLJForceVerletWorklet
 // (rbmd/framework/run/worklet/RunWorklet.cpp:170-303) with ComputeLJForce and
 // ComputeNearEnergyForce (rbmd/framework/forceFunction/ExecForceFunction.h:74-140):
 //   LJ on MinDistanceVec(p_j', p_i) skipped within a molecule; Coulomb on p_j' - p_i for
-//   0.01 < d < rc with G = erfc(sqrt(a) d)/d^2 + 2 sqrt(a) e^{-a d^2}/(sqrt(pi) d).
-//   MINIMG=false when every replica has >= 3 cells per axis: then each listed |r_d| < rc < L/2
-//   and MinDistanceVec is the identity.
-// RBE: ComputeNewRBEForceWorklet (RunWorklet.cpp:1508-1548), S/P and qqr2e folded into the
-// k records, which the block stages in shared memory when its slots' k range fits.
-template <class R, bool LJ, bool COUL, bool RBE, bool MOLEC, bool MINIMG, bool ENERGY>
+//   0.01 < d < rc with G = erfc(sqrt(a) d)/d^2 + 2 sqrt(a) e^{-a d^2}/(sqrt(pi) d); pairs with
+//   q_i q_j = 0 skip the Coulomb term.  Per-type LJ coefficients are staged in shared memory.
+// Accumulation: groups of four pair forces are summed in FP32 and folded into a two-float
+// (TwoSum) per-atom accumulator.
+template <class R, bool LJ, bool COUL, bool MOLEC, int MI, bool ENERGY>
 __global__ void __launch_bounds__(128) k_near_force(
     NearParams prm, const LJTable* __restrict__ ljt, const typename Traits<R>::V4* __restrict__ pos4,
     const int2* __restrict__ meta, const int* __restrict__ nbr, const int* __restrict__ count,
     const RepDev* __restrict__ reps, const int* __restrict__ rep_of_slot,
-    const int* __restrict__ slot_atom, const typename FracT<R>::T* __restrict__ frac,
-    const typename KRec<R>::T* __restrict__ krec, double* __restrict__ force,
+    const int* __restrict__ slot_atom, double* __restrict__ force,
     double* __restrict__ energy_slot, uint32_t* status) {
-  extern __shared__ __align__(16) unsigned char ksm_raw[];
-  typename KRec<R>::T* ksm = reinterpret_cast<typename KRec<R>::T*>(ksm_raw);
-  const int i0 = blockIdx.x * blockDim.x;
-  const int i = i0 + threadIdx.x;
-  // k range of this block's replicas
-  int kfirst = 0, kcount = 0;
-  bool staged = false;
-  if (RBE) {
-    const int last = min(prm.n, i0 + (int)blockDim.x) - 1;
-    const int ra = rep_of_slot ? rep_of_slot[i0] : 0;
-    const int rb = rep_of_slot ? rep_of_slot[last] : 0;
-    kfirst = reps[ra].k_begin;
-    kcount = reps[rb].k_begin + reps[rb].P - kfirst;
-    staged = kcount <= prm.kstage;
-    if (staged) {
-      const int nwords = kcount * (int)(sizeof(typename KRec<R>::T) / 16);
-      const int4* src = reinterpret_cast<const int4*>(krec + kfirst);
-      int4* dst = reinterpret_cast<int4*>(ksm);
-      for (int t = threadIdx.x; t < nwords; t += blockDim.x) dst[t] = src[t];
-    }
-    __syncthreads();
+  __shared__ R lj_a[kMaxReplicaTypes * kMaxReplicaTypes], lj_s6[kMaxReplicaTypes * kMaxReplicaTypes];
+  const int nt2 = prm.ntypes * prm.ntypes;
+  for (int t = threadIdx.x; t < nt2; t += blockDim.x) {
+    lj_a[t] = lj24<R>(*ljt, t);
+    lj_s6[t] = sig6<R>(*ljt, t);
   }
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= prm.n) return;
   const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
   const typename Traits<R>::V4 pi = pos4[i];
-  const int2 mi = (LJ && (MOLEC || prm.ntypes > 1)) ? meta[i] : make_int2(0, 0);
+  const bool typed = MOLEC || prm.ntypes > 1;
+  const int2 mi = (LJ && typed) ? meta[i] : make_int2(0, 0);
   const R rc = (R)prm.rc;
   const R cut2 = rc * rc;
   const R box[3] = {Traits<R>::box(rp, 0), Traits<R>::box(rp, 1), Traits<R>::box(rp, 2)};
@@ -155,7 +158,9 @@ __global__ void __launch_bounds__(128) k_near_force(
   const R sa = (R)prm.sqrt_alpha, aa = (R)prm.alpha, c2 = (R)prm.two_sqrt_alpha_over_sqrt_pi;
   const R cs = (R)prm.coul_scale;
   const R qi = pi.w;
+  const int trow = mi.x * prm.ntypes;
   Acc<R> fx, fy, fz;
+  R gx = 0, gy = 0, gz = 0;   // FP32 group sum folded into the accumulators every 4 pairs
   R e_lj = 0, e_coul = 0;
   const int cnt = count[i];
   for (int p = 0; p < cnt; ++p) {
@@ -169,7 +174,8 @@ __global__ void __launch_bounds__(128) k_near_force(
       py = py - (c1 == 1 ? wrap[1] : (c1 == 2 ? -wrap[1] : (R)0));
       pz = pz - (c2b == 1 ? wrap[2] : (c2b == 2 ? -wrap[2] : (R)0));
     }
-    const R r0 = px - pi.x, r1 = py - pi.y, r2 = pz - pi.z;
+    R r0 = px - pi.x, r1 = py - pi.y, r2 = pz - pi.z;
+    if (MI == kMiAll) min_image(r0, r1, r2, box);
     const R d2 = r0 * r0 + r1 * r1 + r2 * r2;
     R f = 0;
     if (COUL) {
@@ -190,7 +196,7 @@ __global__ void __launch_bounds__(128) k_near_force(
     if (LJ) {
       bool same = false;
       int tj = 0;
-      if (MOLEC || prm.ntypes > 1) {
+      if (typed) {
         const int2 mj = meta[j];
         same = MOLEC && (mj.y == mi.y);
         tj = mj.x;
@@ -198,39 +204,31 @@ __global__ void __launch_bounds__(128) k_near_force(
       if (!same) {
         R q0 = r0, q1 = r1, q2 = r2;   // MinDistanceVec(p_j', p_i)
         R dl2 = d2;
-        if (MINIMG) {
-          if (fabs(q0) > box[0] * (R)0.5) q0 -= (q0 > 0 ? box[0] : -box[0]);
-          if (fabs(q1) > box[1] * (R)0.5) q1 -= (q1 > 0 ? box[1] : -box[1]);
-          if (fabs(q2) > box[2] * (R)0.5) q2 -= (q2 > 0 ? box[2] : -box[2]);
+        if (MI == kMiLJ) {
+          min_image(q0, q1, q2, box);
           dl2 = q0 * q0 + q1 * q1 + q2 * q2;
         }
         if (dl2 < cut2 && dl2 > (R)0.0001) {
-          const int k = mi.x * prm.ntypes + tj;
-          const R inv2 = (R)1 / dl2;
-          const R sd6 = sig6<R>(*ljt, k) * inv2 * inv2 * inv2;
-          const R scal = lj24<R>(*ljt, k) * (((R)2 * sd6 - (R)1) * sd6) * inv2;
+          const R inv2 = rcp_r(dl2);
+          const R sd6 = lj_s6[trow + tj] * inv2 * inv2 * inv2;
+          const R a24 = lj_a[trow + tj];
+          const R scal = a24 * (((R)2 * sd6 - (R)1) * sd6) * inv2;
           fl0 = scal * q0; fl1 = scal * q1; fl2 = scal * q2;
           // 4 eps (s6 - 1) s6 with 4 eps = -lj24/6
-          if (ENERGY) e_lj += -lj24<R>(*ljt, k) / (R)6 * (sd6 - (R)1) * sd6;
+          if (ENERGY) e_lj += -a24 / (R)6 * (sd6 - (R)1) * sd6;
         }
       }
     }
-    fx.add(f * r0 + fl0);
-    fy.add(f * r1 + fl1);
-    fz.add(f * r2 + fl2);
+    gx += f * r0 + fl0;
+    gy += f * r1 + fl1;
+    gz += f * r2 + fl2;
+    if ((p & 3) == 3) {
+      fx.add(gx); fy.add(gy); fz.add(gz);
+      gx = gy = gz = 0;
+    }
   }
-  double F[3] = {fx.value(), fy.value(), fz.value()};
-  if (RBE) {
-    const typename FracT<R>::T fr = frac[i];
-    R ax = 0, ay = 0, az = 0;
-    const int kb = rp.k_begin, P = rp.P;
-    if (staged) rbe_terms<R>(fr, ksm + (kb - kfirst), P, ax, ay, az);
-    else rbe_terms<R>(fr, krec + kb, P, ax, ay, az);
-    const double q = (double)fr.q;
-    F[0] += q * (double)ax;
-    F[1] += q * (double)ay;
-    F[2] += q * (double)az;
-  }
+  fx.add(gx); fy.add(gy); fz.add(gz);
+  const double F[3] = {fx.value(), fy.value(), fz.value()};
   if (!isfinite(F[0]) || !isfinite(F[1]) || !isfinite(F[2])) set_flag(status, kFlagNonFinite);
   const int id = slot_atom[i];
   force[3 * id] = F[0];
@@ -240,6 +238,58 @@ __global__ void __launch_bounds__(128) k_near_force(
     energy_slot[2 * i] = 0.5 * (double)e_lj;
     energy_slot[2 * i + 1] = 0.5 * (double)e_coul;
   }
+}
+
+// RBE k-space force, one thread per atom in caller order: F_i = q_i sum_l w_l k_l
+// (cos(k_l.r_i) Im rho_l - sin(k_l.r_i) Re rho_l) (ComputeNewRBEForceWorklet,
+// RunWorklet.cpp:1508-1548; S/P and qqr2e are folded into the records).  The block stages the
+// k records of the replicas its atoms belong to in shared memory (two 16-byte broadcast loads
+// per sample) when they fit.  Runs on the k-space stream concurrently with the near pass and
+// writes its own buffer; k_add_far folds it into the force.
+template <class R>
+__global__ void __launch_bounds__(128) k_rbe_force(int n, int kstage, const typename FracT<R>::T* __restrict__ frac,
+                                                   const typename KRec<R>::T* __restrict__ krec,
+                                                   const RepDev* __restrict__ reps,
+                                                   const int* __restrict__ rep_of,
+                                                   double* __restrict__ far_force) {
+  extern __shared__ __align__(16) unsigned char ksm_raw[];
+  typename KRec<R>::T* ksm = reinterpret_cast<typename KRec<R>::T*>(ksm_raw);
+  const int i0 = blockIdx.x * blockDim.x;
+  const int i = i0 + threadIdx.x;
+  const int last = min(n, i0 + (int)blockDim.x) - 1;
+  const int ra = rep_of ? rep_of[i0] : 0;
+  const int rb = rep_of ? rep_of[last] : 0;
+  const int kfirst = reps[ra].k_begin;
+  const int kcount = reps[rb].k_begin + reps[rb].P - kfirst;
+  const bool staged = kcount <= kstage;
+  if (staged) {
+    const int nwords = kcount * (int)(sizeof(typename KRec<R>::T) / 16);
+    const int4* src = reinterpret_cast<const int4*>(krec + kfirst);
+    int4* dst = reinterpret_cast<int4*>(ksm);
+    for (int t = threadIdx.x; t < nwords; t += blockDim.x) dst[t] = src[t];
+  }
+  __syncthreads();
+  if (i >= n) return;
+  const RepDev& rp = reps[rep_of ? rep_of[i] : 0];
+  const typename FracT<R>::T fr = frac[i];
+  R ax = 0, ay = 0, az = 0;
+  if (fr.q != 0) {
+    if (staged) rbe_terms<R>(fr, ksm + (rp.k_begin - kfirst), rp.P, ax, ay, az);
+    else rbe_terms<R>(fr, krec + rp.k_begin, rp.P, ax, ay, az);
+  }
+  const double q = (double)fr.q;
+  far_force[3 * i] = q * (double)ax;
+  far_force[3 * i + 1] = q * (double)ay;
+  far_force[3 * i + 2] = q * (double)az;
+}
+
+__global__ void k_add_far(int n3, const double* __restrict__ far_force, double* __restrict__ force,
+                          uint32_t* status) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n3) return;
+  const double v = force[t] + far_force[t];
+  if (!isfinite(v)) set_flag(status, kFlagNonFinite);
+  force[t] = v;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -312,8 +362,9 @@ __global__ void __launch_bounds__(256) k_rho_lanes(const RhoItem* __restrict__ i
 // for tile t and chunk c sit at item_base_r + c * ntiles_r + t.
 struct RhoRep { int item_base, ntiles, nchunks, pad; };
 
-// One thread per k sample: sum the chunk partials in a fixed order (FP64), undo the half-turn
-// phase convention (rho = -sum), then fill the force coefficients of the k record.
+// One warp per k sample: lanes sum the chunk partials in a fixed strided order (FP64) and a
+// butterfly combines them (deterministic); then undo the half-turn phase convention
+// (rho = -sum) and fill the force coefficients of the k record.
 // k-space energy estimate per replica: (S/P) qqr2e sum_l w_l (2 pi / V) |rho_l|^2 / k_l^2.
 template <class R>
 __global__ void k_rho_finish(int nk_total, int ktile, const int* __restrict__ krep,
@@ -321,20 +372,27 @@ __global__ void k_rho_finish(int nk_total, int ktile, const int* __restrict__ kr
                              const R* __restrict__ partial, const double* __restrict__ weights,
                              double qqr2e, typename KRec<R>::T* __restrict__ krec,
                              double2* __restrict__ rho_out, double* __restrict__ ek_out) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
   if (g >= nk_total) return;
-  typename KRec<R>::T k = krec[g];
   const int r = krep[g];
   const RepDev& rp = reps[r];
   const RhoRep q = rr[r];
   const int l = g - rp.k_begin;
   const int tile = l / ktile, kk = l % ktile;
   double re = 0, im = 0;
-  for (int c = 0; c < q.nchunks; ++c) {
+  for (int c = lane; c < q.nchunks; c += 32) {
     const size_t item = (size_t)q.item_base + (size_t)c * q.ntiles + tile;
     re += (double)partial[(item * ktile + kk) * 2];
     im += (double)partial[(item * ktile + kk) * 2 + 1];
   }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    re += __shfl_xor_sync(0xffffffffu, re, o);
+    im += __shfl_xor_sync(0xffffffffu, im, o);
+  }
+  if (lane != 0) return;
+  typename KRec<R>::T k = krec[g];
   re = -re;
   im = -im;
   const double twopi = 6.283185307179586476925;

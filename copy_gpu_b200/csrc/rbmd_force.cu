@@ -94,7 +94,8 @@ struct rbmd_force {
   int ncell_total = 0, num_cycles = 1;
 
   // ---------------- per-type LJ ----------------
-  int ntypes = 1;
+  int ntypes = 1;          // declared types (atom type ids must lie below)
+  int nt_eff = 1;          // 1 when every type pair has the same LJ coefficients
   LJTable ljt_h{};
   bool have_pair_coeffs = false;
 
@@ -139,6 +140,7 @@ struct rbmd_force {
   void* d_partial = nullptr;
   double2* d_rho = nullptr;
   double* d_ek = nullptr;
+  double* d_far = nullptr;
   double* d_weights = nullptr;
   SamplerRep* d_srep = nullptr;
   double* d_qtab = nullptr;
@@ -245,7 +247,7 @@ void free_all(rbmd_force* f) {
   dfree(f->d_kvec); dfree(f->d_krep); dfree(f->d_items); dfree(f->d_rhorep);
   if (f->d_partial) cudaFree(f->d_partial);
   f->d_partial = nullptr;
-  dfree(f->d_rho); dfree(f->d_ek); dfree(f->d_weights); dfree(f->d_srep); dfree(f->d_qtab);
+  dfree(f->d_rho); dfree(f->d_ek); dfree(f->d_far); dfree(f->d_weights); dfree(f->d_srep); dfree(f->d_qtab);
   dfree(f->d_chunks); dfree(f->d_chunk_rep_begin); dfree(f->d_ke_partial); dfree(f->d_ke);
   dfree(f->d_T); dfree(f->d_lambda); dfree(f->d_xi); dfree(f->d_xold); dfree(f->d_vold);
   dfree(f->d_frho); dfree(f->d_rhor); dfree(f->d_z2r);
@@ -338,28 +340,22 @@ void launch_sort(rbmd_force* f, cudaStream_t s, bool bin) {
   k_cell_sort_gather<R><<<(f->ncell_total + 7) / 8, 256, 0, s>>>(
       f->ncell_total, f->d_cell_start, f->d_tmp, f->at.pos, f->at.charge, f->at.type, f->at.molecule,
       f->nrep > 1 ? f->d_rep_of : nullptr, f->d_reps, f->d_slot_atom, f->d_atom_slot,
-      (typename Traits<R>::V4*)f->d_pos4, f->is_rbe() ? f->d_frac : nullptr, f->d_meta, f->d_xref, rb);
+      (typename Traits<R>::V4*)f->d_pos4, nullptr, f->d_meta, f->d_xref, rb);
   f->launches += 4;
   if (rb) {
     // list reuse: refresh the slot caches from the new positions (no-op on rebuild steps)
     k_regather<R><<<(n + 255) / 256, 256, 0, s>>>(
         n, f->d_slot_atom, f->at.pos, f->at.charge, f->nrep > 1 ? f->d_rep_of : nullptr, f->d_reps,
-        (typename Traits<R>::V4*)f->d_pos4, f->is_rbe() ? f->d_frac : nullptr, rb);
+        (typename Traits<R>::V4*)f->d_pos4, nullptr, rb);
     f->launches++;
   }
 }
 
+// k-space chain on the side stream: sampler (depends only on the step counter, so it runs
+// before the fork wait), fixed-point fractional coordinates, structure factors, coefficients,
+// RBE force into d_far.
 template <class R>
-void launch_regather(rbmd_force* f, cudaStream_t s) {
-  k_regather<R><<<(f->n + 255) / 256, 256, 0, s>>>(
-      f->n, f->d_slot_atom, f->at.pos, f->at.charge, f->nrep > 1 ? f->d_rep_of : nullptr, f->d_reps,
-      (typename Traits<R>::V4*)f->d_pos4, f->is_rbe() ? f->d_frac : nullptr, nullptr);
-  f->launches++;
-}
-
-template <class R>
-void launch_kspace(rbmd_force* f, cudaStream_t s) {
-  if (!f->is_rbe()) return;
+void launch_kspace(rbmd_force* f, cudaStream_t s, cudaEvent_t ready) {
   PhaseScope ps(f, kPhK, s);
   const int rec_bytes = sizeof(typename KRec<R>::T);
   if (!f->injected && f->coul_type == "RBE") {
@@ -368,21 +364,28 @@ void launch_kspace(rbmd_force* f, cudaStream_t s) {
                                                 f->d_krep, f->d_status);
     f->launches++;
   }
+  cudaStreamWaitEvent(s, ready, 0);
+  const int* rep_of = f->nrep > 1 ? f->d_rep_of : nullptr;
+  k_frac<R><<<(f->n + 255) / 256, 256, 0, s>>>(f->n, f->at.pos, f->at.charge, rep_of, f->d_reps, f->d_frac);
   k_rho_lanes<R, kKL><<<f->nitems, f->rho_threads, 0, s>>>(
       f->d_items, (const typename FracT<R>::T*)f->d_frac, (const typename KRec<R>::T*)f->d_krec,
       (R*)f->d_partial, f->ktile);
-  k_rho_finish<R><<<(f->Ptot + 127) / 128, 128, 0, s>>>(
+  k_rho_finish<R><<<(f->Ptot + 3) / 4, 128, 0, s>>>(
       f->Ptot, f->ktile, f->d_krep, f->d_rhorep, f->d_reps, (const R*)f->d_partial, f->d_weights,
       f->u.qqr2e, (typename KRec<R>::T*)f->d_krec, f->d_rho, f->d_ek);
-  f->launches += 2;
+  const size_t smem = (size_t)f->kstage * sizeof(typename KRec<R>::T);
+  k_rbe_force<R><<<(f->n + 127) / 128, 128, smem, s>>>(f->n, f->kstage, (const typename FracT<R>::T*)f->d_frac,
+                                                       (const typename KRec<R>::T*)f->d_krec, f->d_reps,
+                                                       rep_of, f->d_far);
+  f->launches += 4;
 }
 
-template <class R, bool LJ, bool COUL, bool RBE, bool MOLEC, bool MINIMG, bool ENERGY>
+template <class R, bool LJ, bool COUL, bool MOLEC, int MI, bool ENERGY>
 void launch_near_t(rbmd_force* f, cudaStream_t s) {
   NearParams p;
   p.n = f->n;
   p.stride = f->stride;
-  p.ntypes = f->ntypes;
+  p.ntypes = f->nt_eff;
   p.with_lj = LJ;
   p.with_coul = COUL;
   p.molecular = MOLEC;
@@ -391,41 +394,39 @@ void launch_near_t(rbmd_force* f, cudaStream_t s) {
   p.coul_scale = f->near_coul_scale;
   p.sqrt_alpha = std::sqrt(f->alpha);
   p.two_sqrt_alpha_over_sqrt_pi = 2.0 * std::sqrt(f->alpha) / std::sqrt(M_PI);
-  p.kstage = RBE ? f->kstage : 0;
-  const size_t smem = RBE ? (size_t)f->kstage * sizeof(typename KRec<R>::T) : 0;
-  k_near_force<R, LJ, COUL, RBE, MOLEC, MINIMG, ENERGY><<<(f->n + 127) / 128, 128, smem, s>>>(
+  p.kstage = 0;
+  k_near_force<R, LJ, COUL, MOLEC, MI, ENERGY><<<(f->n + 127) / 128, 128, 0, s>>>(
       p, f->d_ljt, (const typename Traits<R>::V4*)f->d_pos4, f->d_meta, f->d_nbr, f->d_count,
-      f->d_reps, f->nrep > 1 ? f->d_rep_of : nullptr, f->d_slot_atom,
-      (const typename FracT<R>::T*)f->d_frac, (const typename KRec<R>::T*)f->d_krec, f->at.force,
-      f->d_eslot, f->d_status);
+      f->d_reps, f->nrep > 1 ? f->d_rep_of : nullptr, f->d_slot_atom, f->at.force, f->d_eslot,
+      f->d_status);
   f->launches++;
 }
 
-template <class R, bool LJ, bool COUL, bool RBE, bool MOLEC>
-void launch_near_e(rbmd_force* f, cudaStream_t s) {
-  if (f->minimg) {
-    if (f->want_energy) launch_near_t<R, LJ, COUL, RBE, MOLEC, true, true>(f, s);
-    else launch_near_t<R, LJ, COUL, RBE, MOLEC, true, false>(f, s);
+template <class R, bool COUL, bool MOLEC>
+void launch_near_m(rbmd_force* f, cudaStream_t s) {
+  const int mi = f->skin > 0 ? kMiAll : (f->minimg ? kMiLJ : kMiNone);
+  if (mi == kMiAll) {
+    if (f->want_energy) launch_near_t<R, true, COUL, MOLEC, kMiAll, true>(f, s);
+    else launch_near_t<R, true, COUL, MOLEC, kMiAll, false>(f, s);
+  } else if (mi == kMiLJ) {
+    if (f->want_energy) launch_near_t<R, true, COUL, MOLEC, kMiLJ, true>(f, s);
+    else launch_near_t<R, true, COUL, MOLEC, kMiLJ, false>(f, s);
   } else {
-    if (f->want_energy) launch_near_t<R, LJ, COUL, RBE, MOLEC, false, true>(f, s);
-    else launch_near_t<R, LJ, COUL, RBE, MOLEC, false, false>(f, s);
+    if (f->want_energy) launch_near_t<R, true, COUL, MOLEC, kMiNone, true>(f, s);
+    else launch_near_t<R, true, COUL, MOLEC, kMiNone, false>(f, s);
   }
 }
 
 template <class R>
 void launch_near(rbmd_force* f, cudaStream_t s) {
-  const bool rbe = f->is_rbe();
   const bool coul = f->with_coul_near();
   const bool molec = f->at.molecule != nullptr;
-  if (!coul) {
-    if (molec) launch_near_e<R, true, false, false, true>(f, s);
-    else launch_near_e<R, true, false, false, false>(f, s);
-  } else if (rbe) {
-    if (molec) launch_near_e<R, true, true, true, true>(f, s);
-    else launch_near_e<R, true, true, true, false>(f, s);
+  if (coul) {
+    if (molec) launch_near_m<R, true, true>(f, s);
+    else launch_near_m<R, true, false>(f, s);
   } else {
-    if (molec) launch_near_e<R, true, true, false, true>(f, s);
-    else launch_near_e<R, true, true, false, false>(f, s);
+    if (molec) launch_near_m<R, false, true>(f, s);
+    else launch_near_m<R, false, false>(f, s);
   }
 }
 
@@ -468,18 +469,19 @@ void launch_water(rbmd_force* f, cudaStream_t s) {
   f->launches++;
 }
 
-// Force evaluation after the slot caches are current: list, k-space (side stream), pair pass.
+// Force evaluation from the current master positions: the k-space chain forks onto the side
+// stream, the cell sort / neighbour list / near pass / intramolecular terms run on the caller's
+// stream, and the far force is folded in after the join.
 template <class R>
-void launch_force_tail(rbmd_force* f, cudaStream_t s) {
+void launch_force_tail(rbmd_force* f, cudaStream_t s, bool bin) {
   const bool kspace = f->is_rbe();
   if (kspace) {
     cudaEventRecord(f->ev_fork, s);
-    cudaStreamWaitEvent(f->side, f->ev_fork, 0);
-    launch_kspace<R>(f, f->side);
+    launch_kspace<R>(f, f->side, f->ev_fork);
     cudaEventRecord(f->ev_join, f->side);
   }
+  launch_sort<R>(f, s, bin);
   launch_nlist<R>(f, s);
-  if (kspace) cudaStreamWaitEvent(s, f->ev_join, 0);
   {
     PhaseScope ps(f, kPhForce, s);
     if (f->is_eam()) launch_eam<R>(f, s);
@@ -489,6 +491,11 @@ void launch_force_tail(rbmd_force* f, cudaStream_t s) {
     PhaseScope ps(f, kPhMol, s);
     launch_water(f, s);
   }
+  if (kspace) {
+    cudaStreamWaitEvent(s, f->ev_join, 0);
+    k_add_far<<<(3 * f->n + 255) / 256, 256, 0, s>>>(3 * f->n, f->d_far, f->at.force, f->d_status);
+    f->launches++;
+  }
 }
 
 template <class R>
@@ -496,8 +503,7 @@ void launch_compute(rbmd_force* f, cudaStream_t s) {
   f->want_energy = true;
   cudaMemsetAsync(f->d_maxcount, 0, sizeof(int), s);
   if (f->d_rebuild) cudaMemsetAsync(f->d_rebuild, 1, sizeof(int), s);   // nonzero: rebuild
-  launch_sort<R>(f, s, true);
-  launch_force_tail<R>(f, s);
+  launch_force_tail<R>(f, s, true);
 }
 
 void launch_compute_any(rbmd_force* f, cudaStream_t s) {
@@ -559,7 +565,6 @@ void launch_step(rbmd_force* f, cudaStream_t s) {
                                                     0.25 * f->skin * f->skin, f->d_rebuild);
     f->launches++;
   }
-  launch_sort<R>(f, s, false);
   if (shake) {
     PhaseScope ps(f, kPhMol, s);
     ShakeParams sp;
@@ -573,10 +578,9 @@ void launch_step(rbmd_force* f, cudaStream_t s) {
                                                   f->nrep > 1 ? f->d_rep_of : nullptr, f->d_reps,
                                                   f->d_status);
     f->launches++;
-    launch_regather<R>(f, s);
   }
-  // stage 3: force
-  launch_force_tail<R>(f, s);
+  // stage 3: force (cell sort of the pre-constraint binning, then list and forces)
+  launch_force_tail<R>(f, s, false);
   // stage 3: kick (+ RATTLE), temperature, thermostat
   PhaseScope ps_int(f, kPhInt, s);
   if (shake) {
@@ -703,6 +707,9 @@ rbmd_status parse_config(rbmd_force* f, const char* text) {
 // ((sigma_i + sigma_j)/2)^6 as ComputeLJForce forms them (ExecForceFunction.h:74-96).
 void fill_lj(rbmd_force* f, int nt, const double* eps, const double* sig) {
   f->ntypes = nt;
+  bool same = true;
+  for (int a = 1; a < nt; ++a) same = same && eps[a] == eps[0] && sig[a] == sig[0];
+  f->nt_eff = same ? 1 : nt;
   for (int a = 0; a < nt; ++a)
     for (int b = 0; b < nt; ++b) {
       const float ea = (float)eps[a], eb = (float)eps[b], sa = (float)sig[a], sb = (float)sig[b];
@@ -924,6 +931,7 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
   // k-space
   if (f->is_rbe()) {
     CK(cudaMalloc(&f->d_frac, n * (fp64 ? sizeof(Frac64) : sizeof(Frac32))));
+    CK(dalloc(&f->d_far, 3 * n));
     const int recb = fp64 ? sizeof(KRec64) : sizeof(KRec32);
     if (f->coul_type == "EWALD") {
       // EWALD: the cube m in [-kmax, kmax]^3 \ {0} (ExecPointLocator::ExecuteOnKNeighbor,
