@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--P", type=int, default=P_PLAIN)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--skin", type=float, default=0.3,
+                    help="Verlet skin; the list is rebuilt when an atom moved more than skin/2 "
+                         "(forces are those of a per-step rebuild); 0 rebuilds every step")
     return ap.parse_args()
 
 
@@ -109,18 +112,21 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
 
 
-# algorithmic bytes / operations per atom of each phase (DESIGN.md lists the derivation)
-def algorithmic(n_nbr_mean, P):
+# Algorithmic bytes / sincos per unit of each phase (derivation in DESIGN.md).  "units" is the
+# number of atoms (or charged atoms) one launch processes.
+def algorithmic(n, nq, n_nbr_mean, P):
     return {
-        # neighbour list: read own pos4 + cell ranges, write n entries (4 B) + count
-        "neighbor_list": {"bytes": 16 + 4 * n_nbr_mean + 4 + 8},
-        # near + fused RBE force: list (4 B/nbr), own pos4 + frac + meta + slot id + count,
-        # force write (24 B); unique neighbour positions are read once (the own pos4 term)
-        "force": {"bytes": 4 * n_nbr_mean + 16 + 16 + 8 + 4 + 4 + 24, "sincos": P},
-        # structure factors: frac (16 B) once per k tile (L2), P sincos
-        "kspace": {"bytes": 16, "sincos": P},
-        "cell_sort": {"bytes": 24 + 4 + 4 + 4 + 4 + 16 + 16 + 8 + 8 + 8},
-        "integrate": {"bytes": 24 * 4 + 8 + 4 + 4 + 24 * 2},
+        # list build: own pos4 (16 B) + cell ranges (8 B) + list entries written (4 B each) + count
+        "neighbor_list": {"units": n, "bytes": 16 + 8 + 4 * n_nbr_mean + 4},
+        # near pass: list entries (4 B/nbr), own pos4 (16 B), count + slot id (8 B), force (24 B);
+        # each neighbour position is some atom's own pos4, counted once
+        "force": {"units": n, "bytes": 4 * n_nbr_mean + 16 + 8 + 24},
+        # structure factors over charged atoms: position (24 B) -> frac (16 B) written and read
+        "kspace": {"units": nq, "bytes": 24 + 16 + 16, "sincos": P},
+        # RBE force over charged atoms: frac (16 B) + far force (24 B)
+        "rbe_force": {"units": nq, "bytes": 16 + 24, "sincos": P},
+        "cell_sort": {"units": n, "bytes": 4 + 4 + 4 + 4 + 4 + 24 + 8 + 16 + 8},
+        "integrate": {"units": n, "bytes": 24 * 4 + 8 + 4 + 4 + 24 * 2},
     }
 
 
@@ -140,6 +146,7 @@ def run_ours(args):
 
     s = systems.electrolyte(args.atoms, seed=3 + rank)
     cfg = systems.electrolyte_config(P=args.P, precision="fp32", seed=7 + rank)
+    cfg["hyper_parameters"]["neighbor"]["skin"] = args.skin
     n = s["pos"].shape[0]
     t = {k: torch.tensor(s[k], device=dev, dtype=torch.float64).contiguous()
          for k in ("pos", "vel", "mass", "charge")}
@@ -156,6 +163,7 @@ def run_ours(args):
     torch.cuda.synchronize(dev)
     k_per_step = ff.launches_per_step()
     clocks = Clocks(local)
+    builds0 = ff.list_builds()
     ff.profile(True)
     if world > 1:
         dist.barrier()
@@ -172,6 +180,7 @@ def run_ours(args):
         dist.barrier()
     clk = clocks.stop()
     ms = e0.elapsed_time(e1)
+    builds = ff.list_builds() - builds0
     phases = ff.phase_ms()
     ff.profile(False)
     flags = ff.status()
@@ -212,27 +221,34 @@ def run_ours(args):
     out = None
     if rank == 0:
         peaks, src = measured_peaks()
-        alg = algorithmic(n_nbr, args.P)
-        # dominant phase by device time
-        per = {k: v[0] for k, v in phases.items() if v[1] > 0}
-        dom = max(per, key=per.get)
+        nq = int((s["charge"] != 0).sum())
+        alg = algorithmic(n, nq, n_nbr, args.P)
         launches = {k: phases[k][1] for k in phases}
         sm_mhz = clk["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0)
         n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
         mufu_peak = 16 * n_sm * sm_mhz * 1e6 / 2.0 / 1e9        # G sincos/s (2 MUFU ops each)
         rl = {}
-        for k in ("force", "kspace", "neighbor_list", "cell_sort", "integrate"):
-            if k not in per or launches[k] == 0:
+        for k, a in alg.items():
+            if k not in phases or launches[k] == 0:
                 continue
-            dur = per[k] / 1e3 / args.steps                      # s per step
-            a = alg[k]
-            ent = {"ms_per_step": per[k] / args.steps}
-            ent["hbm_gbs"] = a["bytes"] * n / dur / 1e9
+            tot_ms = phases[k][0]
+            # per-launch duration (the list phase runs only on rebuild steps)
+            per_launch_s = tot_ms / 1e3 / launches[k]
+            if k == "integrate":
+                per_launch_s = tot_ms / 1e3 / args.steps
+            if k == "neighbor_list":      # early-exit launches on list-reuse steps are ~3 us
+                per_launch_s = tot_ms / 1e3 / max(builds, 1)
+            ent = {"ms_per_step": tot_ms / args.steps, "launches": launches[k],
+                   "ms_per_launch": per_launch_s * 1e3}
+            ent["hbm_gbs"] = a["bytes"] * a["units"] / per_launch_s / 1e9
             ent["hbm_frac"] = ent["hbm_gbs"] / peaks["hbm_gbs"]
             if "sincos" in a:
-                ent["gsincos_s"] = a["sincos"] * n / dur / 1e9
+                ent["gsincos_s"] = a["sincos"] * a["units"] / per_launch_s / 1e9
                 ent["mufu_frac"] = ent["gsincos_s"] / mufu_peak
             rl[k] = ent
+        # dominant single-kernel phase by device time per step
+        single = [k for k in ("force", "neighbor_list", "kspace", "rbe_force") if k in rl]
+        dom = max(single, key=lambda k: rl[k]["ms_per_step"])
         d = rl[dom]
         if "mufu_frac" in d and d["mufu_frac"] > d["hbm_frac"]:
             roof = {"bound": "mufu", "achieved": d["gsincos_s"], "peak": mufu_peak, "unit": "Gsincos/s",
@@ -241,7 +257,8 @@ def run_ours(args):
                     "traffic": None}
         else:
             roof = {"bound": "hbm", "achieved": d["hbm_gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                    "frac": d["hbm_frac"], "kernel": dom, "peak_source": f"{src} hbm_gbs", "traffic": None}
+                    "frac": d["hbm_frac"], "kernel": dom, "peak_source": f"{src} hbm_gbs (MEASURED_PEAKS.json)",
+                    "traffic": None}
         tr_path = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tr_path):
             with open(tr_path) as fh:
@@ -262,7 +279,8 @@ def run_ours(args):
             "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": f"electrolyte {n} atoms, plain Gaussian RBE P={args.P}, full MD step",
-                       "atoms_per_gpu": n, "P": args.P, "proposal": "gauss", "rc": 2.5,
+                       "atoms_per_gpu": n, "P": args.P, "proposal": "gauss", "rc": 2.5, "skin": args.skin,
+                       "list_builds_per_step": builds / args.steps,
                        "alpha": cfg["hyper_parameters"]["coulomb"]["alpha"], "box": float(s["hi"][0]),
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2": "inputs larger than L2 (neighbour list %.0f MB + state %.0f MB)"

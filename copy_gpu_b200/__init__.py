@@ -39,7 +39,7 @@ EXPORTED = [
     "rbmd_force_compute", "rbmd_force_compute_host", "rbmd_force_step",
     "rbmd_force_sync_velocities", "rbmd_force_energy", "rbmd_force_status",
     "rbmd_force_get_neighbors", "rbmd_force_get_rhok", "rbmd_force_profile",
-    "rbmd_force_phase_ms", "rbmd_force_launch_count",
+    "rbmd_force_phase_ms", "rbmd_force_list_builds", "rbmd_force_launch_count",
     "rbmd_force_destroy", "rbmd_version", "rbmd_last_error",
 ]
 
@@ -106,6 +106,7 @@ def library() -> ctypes.CDLL:
         "rbmd_force_get_rhok": (I32, [V, P(D), I32]),
         "rbmd_force_profile": (I32, [V, I32]),
         "rbmd_force_phase_ms": (I32, [V, P(D), P(I64), I32]),
+        "rbmd_force_list_builds": (I32, [V, P(I64)]),
         "rbmd_force_launch_count": (I32, [V, P(I32)]),
         "rbmd_force_destroy": (None, [V]),
         "rbmd_version": (ctypes.c_char_p, []),
@@ -309,7 +310,8 @@ class ForceField:
                "status")
         return int(f.value)
 
-    PHASES = ("integrate", "cell_sort", "kspace", "neighbor_list", "force", "molecular")
+    PHASES = ("integrate", "cell_sort", "kspace", "neighbor_list", "force", "molecular", "sampler",
+              "rbe_force")
 
     def profile(self, enable=True):
         _check(library().rbmd_force_profile(self._h, int(enable)), "profile")
@@ -321,6 +323,11 @@ class ForceField:
         _check(library().rbmd_force_phase_ms(self._h, _ptr(ms, ctypes.c_double),
                                              _ptr(cnt, ctypes.c_int64), 8), "phase_ms")
         return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(self.PHASES)}
+
+    def list_builds(self):
+        k = ctypes.c_int64()
+        _check(library().rbmd_force_list_builds(self._h, ctypes.byref(k)), "list_builds")
+        return int(k.value)
 
     def launches_per_step(self):
         k = ctypes.c_int32()

@@ -271,9 +271,10 @@ __global__ void __launch_bounds__(128) k_nlist(
     int n, const typename Traits<R>::V4* __restrict__ pos4, const int* __restrict__ cell_start,
     const RepDev* __restrict__ reps, const int* __restrict__ rep_of_slot, int num_cycles, R rc,
     int cap, int stride, int* __restrict__ nbr, int* __restrict__ count, int* __restrict__ max_count,
-    uint32_t* status, const int* __restrict__ rebuild) {
+    uint32_t* status, const int* __restrict__ rebuild, unsigned long long* __restrict__ nbuilds) {
   if (rebuild && !*rebuild) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0 && nbuilds) atomicAdd(nbuilds, 1ull);
   if (i >= n) return;
   const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
   const typename Traits<R>::V4 pi = pos4[i];
@@ -320,17 +321,19 @@ __global__ void __launch_bounds__(128) k_nlist(
   }
 }
 
-// Fixed-point fractional coordinates + charge in caller order, the input of every k-space
-// phase: U_d = floor(frac((x_d - lo_d) / L_d) * 2^32) (2^64 for FP64).  Integer phases
-// m . U mod 2^32 are exact.
+// Fixed-point fractional coordinates + charge of the charged atoms (qidx: their caller ids,
+// grouped per replica), the input of every k-space phase: U_d = floor(frac((x_d - lo_d)/L_d)
+// * 2^32) (2^64 for FP64), so integer phases m . U mod 2^32 are exact.  Uncharged atoms add
+// nothing to rho_k or the k-space force and are left out.
 template <class R>
-__global__ void k_frac(int n, const double* __restrict__ pos, const double* __restrict__ charge,
-                       const int* __restrict__ rep_of, const RepDev* __restrict__ reps,
-                       void* __restrict__ frac_out) {
-  const int id = blockIdx.x * blockDim.x + threadIdx.x;
-  if (id >= n) return;
+__global__ void k_frac(int nq, const int* __restrict__ qidx, const double* __restrict__ pos,
+                       const double* __restrict__ charge, const int* __restrict__ rep_of,
+                       const RepDev* __restrict__ reps, void* __restrict__ frac_out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nq) return;
+  const int id = qidx[c];
   const RepDev& rp = reps[rep_of ? rep_of[id] : 0];
-  const double q = charge ? charge[id] : 0.0;
+  const double q = charge[id];
   double u[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -344,7 +347,7 @@ __global__ void k_frac(int n, const double* __restrict__ pos, const double* __re
       const double s = u[d] * 4294967296.0;
       U[d] = s >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)s;
     }
-    reinterpret_cast<Frac32*>(frac_out)[id] = Frac32{U[0], U[1], U[2], (float)q};
+    reinterpret_cast<Frac32*>(frac_out)[c] = Frac32{U[0], U[1], U[2], (float)q};
   } else {
     unsigned long long U[3];
 #pragma unroll
@@ -352,7 +355,7 @@ __global__ void k_frac(int n, const double* __restrict__ pos, const double* __re
       const double s = u[d] * 18446744073709551616.0;
       U[d] = s >= 18446744073709549568.0 ? 0xFFFFFFFFFFFFF800ull : (unsigned long long)s;
     }
-    reinterpret_cast<Frac64*>(frac_out)[id] = Frac64{U[0], U[1], U[2], q};
+    reinterpret_cast<Frac64*>(frac_out)[c] = Frac64{U[0], U[1], U[2], q};
   }
 }
 

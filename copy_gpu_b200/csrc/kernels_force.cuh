@@ -39,7 +39,7 @@ struct LJTable {
 };
 
 struct NearParams {
-  int n, stride, ntypes;
+  int n, stride, ntypes, cap;
   int with_lj, with_coul, molecular;
   double rc, alpha, coul_scale;   // coul_scale multiplies the erfc Coulomb pair force
   double sqrt_alpha, two_sqrt_alpha_over_sqrt_pi;
@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(128) k_near_force(
   Acc<R> fx, fy, fz;
   R gx = 0, gy = 0, gz = 0;   // FP32 group sum folded into the accumulators every 4 pairs
   R e_lj = 0, e_coul = 0;
-  const int cnt = count[i];
+  const int cnt = min(count[i], prm.cap);   // an overflowed row is redone after regrowth
   for (int p = 0; p < cnt; ++p) {
     const int e = __ldg(nbr + (size_t)p * prm.stride + i);
     const int j = e >> kShiftBits;
@@ -240,25 +240,26 @@ __global__ void __launch_bounds__(128) k_near_force(
   }
 }
 
-// RBE k-space force, one thread per atom in caller order: F_i = q_i sum_l w_l k_l
-// (cos(k_l.r_i) Im rho_l - sin(k_l.r_i) Re rho_l) (ComputeNewRBEForceWorklet,
-// RunWorklet.cpp:1508-1548; S/P and qqr2e are folded into the records).  The block stages the
-// k records of the replicas its atoms belong to in shared memory (two 16-byte broadcast loads
-// per sample) when they fit.  Runs on the k-space stream concurrently with the near pass and
-// writes its own buffer; k_add_far folds it into the force.
+// RBE k-space force, one thread per charged atom (compact index c, caller id qidx[c]):
+// F_i = q_i sum_l w_l k_l (cos(k_l.r_i) Im rho_l - sin(k_l.r_i) Re rho_l)
+// (ComputeNewRBEForceWorklet, RunWorklet.cpp:1508-1548; S/P and qqr2e are folded into the
+// records).  The block stages the k records of the replicas its atoms belong to in shared
+// memory (two 16-byte broadcast loads per sample) when they fit.  Runs on the k-space stream
+// concurrently with the near pass and writes far_force[c]; k_add_far folds it into the force.
 template <class R>
-__global__ void __launch_bounds__(128) k_rbe_force(int n, int kstage, const typename FracT<R>::T* __restrict__ frac,
+__global__ void __launch_bounds__(128) k_rbe_force(int nq, int kstage, const int* __restrict__ qidx,
+                                                   const typename FracT<R>::T* __restrict__ frac,
                                                    const typename KRec<R>::T* __restrict__ krec,
                                                    const RepDev* __restrict__ reps,
                                                    const int* __restrict__ rep_of,
                                                    double* __restrict__ far_force) {
   extern __shared__ __align__(16) unsigned char ksm_raw[];
   typename KRec<R>::T* ksm = reinterpret_cast<typename KRec<R>::T*>(ksm_raw);
-  const int i0 = blockIdx.x * blockDim.x;
-  const int i = i0 + threadIdx.x;
-  const int last = min(n, i0 + (int)blockDim.x) - 1;
-  const int ra = rep_of ? rep_of[i0] : 0;
-  const int rb = rep_of ? rep_of[last] : 0;
+  const int c0 = blockIdx.x * blockDim.x;
+  const int c = c0 + threadIdx.x;
+  const int last = min(nq, c0 + (int)blockDim.x) - 1;
+  const int ra = rep_of ? rep_of[qidx[c0]] : 0;
+  const int rb = rep_of ? rep_of[qidx[last]] : 0;
   const int kfirst = reps[ra].k_begin;
   const int kcount = reps[rb].k_begin + reps[rb].P - kfirst;
   const bool staged = kcount <= kstage;
@@ -269,27 +270,27 @@ __global__ void __launch_bounds__(128) k_rbe_force(int n, int kstage, const type
     for (int t = threadIdx.x; t < nwords; t += blockDim.x) dst[t] = src[t];
   }
   __syncthreads();
-  if (i >= n) return;
-  const RepDev& rp = reps[rep_of ? rep_of[i] : 0];
-  const typename FracT<R>::T fr = frac[i];
+  if (c >= nq) return;
+  const RepDev& rp = reps[rep_of ? rep_of[qidx[c]] : 0];
+  const typename FracT<R>::T fr = frac[c];
   R ax = 0, ay = 0, az = 0;
-  if (fr.q != 0) {
-    if (staged) rbe_terms<R>(fr, ksm + (rp.k_begin - kfirst), rp.P, ax, ay, az);
-    else rbe_terms<R>(fr, krec + rp.k_begin, rp.P, ax, ay, az);
-  }
+  if (staged) rbe_terms<R>(fr, ksm + (rp.k_begin - kfirst), rp.P, ax, ay, az);
+  else rbe_terms<R>(fr, krec + rp.k_begin, rp.P, ax, ay, az);
   const double q = (double)fr.q;
-  far_force[3 * i] = q * (double)ax;
-  far_force[3 * i + 1] = q * (double)ay;
-  far_force[3 * i + 2] = q * (double)az;
+  far_force[3 * c] = q * (double)ax;
+  far_force[3 * c + 1] = q * (double)ay;
+  far_force[3 * c + 2] = q * (double)az;
 }
 
-__global__ void k_add_far(int n3, const double* __restrict__ far_force, double* __restrict__ force,
-                          uint32_t* status) {
+__global__ void k_add_far(int nq, const int* __restrict__ qidx, const double* __restrict__ far_force,
+                          double* __restrict__ force, uint32_t* status) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n3) return;
-  const double v = force[t] + far_force[t];
+  if (t >= 3 * nq) return;
+  const int c = t / 3, d = t - 3 * c;
+  const int id = qidx[c];
+  const double v = force[3 * id + d] + far_force[t];
   if (!isfinite(v)) set_flag(status, kFlagNonFinite);
-  force[t] = v;
+  force[3 * id + d] = v;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -535,7 +536,7 @@ struct EamDev {
 };
 
 template <class R>
-__global__ void __launch_bounds__(128) k_eam_fp(int n, int stride, double rc, EamDev eam,
+__global__ void __launch_bounds__(128) k_eam_fp(int n, int stride, int cap, double rc, EamDev eam,
                                                 const typename Traits<R>::V4* __restrict__ pos4,
                                                 const int* __restrict__ nbr, const int* __restrict__ count,
                                                 const RepDev* __restrict__ reps,
@@ -550,7 +551,7 @@ __global__ void __launch_bounds__(128) k_eam_fp(int n, int stride, double rc, Ea
   const R cut2 = (R)rc * (R)rc;
   const R rdr = sizeof(R) == 4 ? (R)eam.rdr : (R)eam.rdr_d;
   Acc<R> rho;
-  const int cnt = count[i];
+  const int cnt = min(count[i], cap);
   for (int p = 0; p < cnt; ++p) {
     const int e = __ldg(nbr + (size_t)p * stride + i);
     const int j = e >> kShiftBits;
@@ -594,7 +595,7 @@ __global__ void __launch_bounds__(128) k_eam_fp(int n, int stride, double rc, Ea
 }
 
 template <class R>
-__global__ void __launch_bounds__(128) k_eam_force(int n, int stride, double rc, EamDev eam,
+__global__ void __launch_bounds__(128) k_eam_force(int n, int stride, int cap, double rc, EamDev eam,
                                                    const typename Traits<R>::V4* __restrict__ pos4,
                                                    const int* __restrict__ nbr, const int* __restrict__ count,
                                                    const RepDev* __restrict__ reps,
@@ -613,7 +614,7 @@ __global__ void __launch_bounds__(128) k_eam_force(int n, int stride, double rc,
   const R fpi = fp[i];
   Acc<R> fx, fy, fz;
   R epair = 0;
-  const int cnt = count[i];
+  const int cnt = min(count[i], cap);
   for (int p = 0; p < cnt; ++p) {
     const int e = __ldg(nbr + (size_t)p * stride + i);
     const int j = e >> kShiftBits;

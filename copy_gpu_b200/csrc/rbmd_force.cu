@@ -125,6 +125,7 @@ struct rbmd_force {
   int2* d_meta = nullptr;
   int *d_nbr = nullptr, *d_count = nullptr, *d_maxcount = nullptr;
   int *d_rebuild = nullptr, *d_block_sums = nullptr;
+  unsigned long long* d_nbuilds = nullptr;
   double* d_xref = nullptr;
   uint32_t* d_status = nullptr;
   double* d_eslot = nullptr;   // 2 per slot (lj, coul)
@@ -133,6 +134,8 @@ struct rbmd_force {
   int Ptot = 0, nitems = 0, rho_threads = 64, ktile = 128, kstage = 0;
   bool minimg = true, want_energy = true;
   int* d_krep = nullptr;
+  int nq = 0;               // charged atoms (the k-space path runs over these only)
+  int* d_qidx = nullptr;
   void* d_krec = nullptr;
   int* d_kvec = nullptr;
   RhoItem* d_items = nullptr;
@@ -187,9 +190,12 @@ struct rbmd_force {
 
 namespace {
 
-// phases: 0 integrate, 1 cell sort, 2 k-space (side stream), 3 neighbour list, 4 force pass,
-// 5 constraints + intramolecular terms
-enum Phase { kPhInt = 0, kPhSort = 1, kPhK = 2, kPhList = 3, kPhForce = 4, kPhMol = 5 };
+// phases: 0 integrate, 1 cell sort, 2 structure factors (side stream), 3 neighbour list,
+// 4 near / EAM force pass, 5 constraints + intramolecular terms, 6 k sampler (side stream),
+// 7 RBE force (side stream)
+enum Phase {
+  kPhInt = 0, kPhSort = 1, kPhK = 2, kPhList = 3, kPhForce = 4, kPhMol = 5, kPhSample = 6, kPhRbeF = 7
+};
 
 cudaEvent_t prof_event(rbmd_force* f) {
   if (f->ev_used == f->ev_pool.size()) {
@@ -240,11 +246,11 @@ void free_all(rbmd_force* f) {
   if (f->d_frac) cudaFree(f->d_frac);
   f->d_frac = nullptr;
   dfree(f->d_meta); dfree(f->d_nbr); dfree(f->d_count); dfree(f->d_maxcount); dfree(f->d_status);
-  dfree(f->d_rebuild); dfree(f->d_block_sums); dfree(f->d_xref);
+  dfree(f->d_rebuild); dfree(f->d_block_sums); dfree(f->d_xref); dfree(f->d_nbuilds);
   dfree(f->d_eslot); dfree(f->d_esum);
   if (f->d_krec) cudaFree(f->d_krec);
   f->d_krec = nullptr;
-  dfree(f->d_kvec); dfree(f->d_krep); dfree(f->d_items); dfree(f->d_rhorep);
+  dfree(f->d_kvec); dfree(f->d_krep); dfree(f->d_qidx); dfree(f->d_items); dfree(f->d_rhorep);
   if (f->d_partial) cudaFree(f->d_partial);
   f->d_partial = nullptr;
   dfree(f->d_rho); dfree(f->d_ek); dfree(f->d_far); dfree(f->d_weights); dfree(f->d_srep); dfree(f->d_qtab);
@@ -317,7 +323,8 @@ void launch_nlist(rbmd_force* f, cudaStream_t s) {
   k_nlist<R><<<nb, 128, 0, s>>>(f->n, (const typename Traits<R>::V4*)f->d_pos4, f->d_cell_start,
                                 f->d_reps, f->nrep > 1 ? f->d_rep_of : nullptr, f->num_cycles,
                                 (R)f->list_cut(), f->cap, f->stride, f->d_nbr, f->d_count,
-                                f->d_maxcount, f->d_status, f->skin > 0 ? f->d_rebuild : nullptr);
+                                f->d_maxcount, f->d_status, f->skin > 0 ? f->d_rebuild : nullptr,
+                                f->d_nbuilds);
   f->launches++;
 }
 
@@ -356,27 +363,35 @@ void launch_sort(rbmd_force* f, cudaStream_t s, bool bin) {
 // RBE force into d_far.
 template <class R>
 void launch_kspace(rbmd_force* f, cudaStream_t s, cudaEvent_t ready) {
-  PhaseScope ps(f, kPhK, s);
   const int rec_bytes = sizeof(typename KRec<R>::T);
   if (!f->injected && f->coul_type == "RBE") {
+    PhaseScope ps(f, kPhSample, s);
     k_sample<kSamplerD><<<f->nrep, 256, 0, s>>>(f->nrep, f->d_srep, f->d_qtab, f->d_reps, f->seed,
                                                 f->step_count, f->d_kvec, f->d_krec, rec_bytes,
                                                 f->d_krep, f->d_status);
     f->launches++;
   }
   cudaStreamWaitEvent(s, ready, 0);
+  if (f->nq == 0) return;
   const int* rep_of = f->nrep > 1 ? f->d_rep_of : nullptr;
-  k_frac<R><<<(f->n + 255) / 256, 256, 0, s>>>(f->n, f->at.pos, f->at.charge, rep_of, f->d_reps, f->d_frac);
-  k_rho_lanes<R, kKL><<<f->nitems, f->rho_threads, 0, s>>>(
-      f->d_items, (const typename FracT<R>::T*)f->d_frac, (const typename KRec<R>::T*)f->d_krec,
-      (R*)f->d_partial, f->ktile);
-  k_rho_finish<R><<<(f->Ptot + 3) / 4, 128, 0, s>>>(
-      f->Ptot, f->ktile, f->d_krep, f->d_rhorep, f->d_reps, (const R*)f->d_partial, f->d_weights,
-      f->u.qqr2e, (typename KRec<R>::T*)f->d_krec, f->d_rho, f->d_ek);
-  const size_t smem = (size_t)f->kstage * sizeof(typename KRec<R>::T);
-  k_rbe_force<R><<<(f->n + 127) / 128, 128, smem, s>>>(f->n, f->kstage, (const typename FracT<R>::T*)f->d_frac,
-                                                       (const typename KRec<R>::T*)f->d_krec, f->d_reps,
-                                                       rep_of, f->d_far);
+  {
+    PhaseScope ps(f, kPhK, s);
+    k_frac<R><<<(f->nq + 255) / 256, 256, 0, s>>>(f->nq, f->d_qidx, f->at.pos, f->at.charge, rep_of,
+                                                   f->d_reps, f->d_frac);
+    k_rho_lanes<R, kKL><<<f->nitems, f->rho_threads, 0, s>>>(
+        f->d_items, (const typename FracT<R>::T*)f->d_frac, (const typename KRec<R>::T*)f->d_krec,
+        (R*)f->d_partial, f->ktile);
+    k_rho_finish<R><<<(f->Ptot + 3) / 4, 128, 0, s>>>(
+        f->Ptot, f->ktile, f->d_krep, f->d_rhorep, f->d_reps, (const R*)f->d_partial, f->d_weights,
+        f->u.qqr2e, (typename KRec<R>::T*)f->d_krec, f->d_rho, f->d_ek);
+  }
+  {
+    PhaseScope ps(f, kPhRbeF, s);
+    const size_t smem = (size_t)f->kstage * sizeof(typename KRec<R>::T);
+    k_rbe_force<R><<<(f->nq + 127) / 128, 128, smem, s>>>(
+        f->nq, f->kstage, f->d_qidx, (const typename FracT<R>::T*)f->d_frac,
+        (const typename KRec<R>::T*)f->d_krec, f->d_reps, rep_of, f->d_far);
+  }
   f->launches += 4;
 }
 
@@ -386,6 +401,7 @@ void launch_near_t(rbmd_force* f, cudaStream_t s) {
   p.n = f->n;
   p.stride = f->stride;
   p.ntypes = f->nt_eff;
+  p.cap = f->cap;
   p.with_lj = LJ;
   p.with_coul = COUL;
   p.molecular = MOLEC;
@@ -444,10 +460,10 @@ void launch_eam(rbmd_force* f, cudaStream_t s) {
   e.rdrho_d = 1.0 / (double)f->eam_h.drho;
   e.rhomax = f->eam_h.rhomax;
   const int nb = (f->n + 127) / 128;
-  k_eam_fp<R><<<nb, 128, 0, s>>>(f->n, f->stride, f->rc, e, (const typename Traits<R>::V4*)f->d_pos4,
+  k_eam_fp<R><<<nb, 128, 0, s>>>(f->n, f->stride, f->cap, f->rc, e, (const typename Traits<R>::V4*)f->d_pos4,
                                  f->d_nbr, f->d_count, f->d_reps, f->nrep > 1 ? f->d_rep_of : nullptr,
                                  (R*)f->d_fp, f->d_emb);
-  k_eam_force<R><<<nb, 128, 0, s>>>(f->n, f->stride, f->rc, e, (const typename Traits<R>::V4*)f->d_pos4,
+  k_eam_force<R><<<nb, 128, 0, s>>>(f->n, f->stride, f->cap, f->rc, e, (const typename Traits<R>::V4*)f->d_pos4,
                                     f->d_nbr, f->d_count, f->d_reps, f->nrep > 1 ? f->d_rep_of : nullptr,
                                     (const R*)f->d_fp, f->d_slot_atom, f->at.force, f->d_epair,
                                     f->d_status);
@@ -493,8 +509,10 @@ void launch_force_tail(rbmd_force* f, cudaStream_t s, bool bin) {
   }
   if (kspace) {
     cudaStreamWaitEvent(s, f->ev_join, 0);
-    k_add_far<<<(3 * f->n + 255) / 256, 256, 0, s>>>(3 * f->n, f->d_far, f->at.force, f->d_status);
-    f->launches++;
+    if (f->nq > 0) {
+      k_add_far<<<(3 * f->nq + 255) / 256, 256, 0, s>>>(f->nq, f->d_qidx, f->d_far, f->at.force, f->d_status);
+      f->launches++;
+    }
   }
 }
 
@@ -892,6 +910,8 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
   CK(dalloc(&f->d_nbr, (size_t)f->cap * f->stride));
   CK(dalloc(&f->d_count, n));
   CK(dalloc(&f->d_maxcount, 1));
+  CK(dalloc(&f->d_nbuilds, 1));
+  CK(cudaMemset(f->d_nbuilds, 0, sizeof(unsigned long long)));
   CK(dalloc(&f->d_rebuild, 1));
   CK(cudaMemset(f->d_rebuild, 0, sizeof(int)));
   CK(dalloc(&f->d_block_sums, (size_t)(f->ncell_total + kScanBlock - 1) / kScanBlock + 1));
@@ -921,17 +941,29 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
       std::snprintf(g_last_error, sizeof g_last_error, "water atom id %d outside [0, %d)", v, f->n);
       return RBMD_ERR_ARG;
     }
-  // charges: sum q^2 for the self energy
+  // charges: sum q^2 for the self energy; compact list of charged atoms per replica
   f->sum_q2 = 0;
+  std::vector<int> qidx;
+  std::vector<int64_t> qoff(nrep + 1, 0);
   if (a->charge) {
     std::vector<double> q(n);
     CK(cudaMemcpy(q.data(), a->charge, sizeof(double) * n, cudaMemcpyDeviceToHost));
     for (double v : q) f->sum_q2 += v * v;
+    for (int r = 0; r < nrep; ++r) {
+      qoff[r] = (int64_t)qidx.size();
+      for (int64_t i = f->rep_off[r]; i < f->rep_off[r + 1]; ++i)
+        if (q[i] != 0.0) qidx.push_back((int)i);
+    }
   }
+  qoff[nrep] = (int64_t)qidx.size();
+  f->nq = (int)qidx.size();
   // k-space
   if (f->is_rbe()) {
-    CK(cudaMalloc(&f->d_frac, n * (fp64 ? sizeof(Frac64) : sizeof(Frac32))));
-    CK(dalloc(&f->d_far, 3 * n));
+    CK(cudaMalloc(&f->d_frac, (size_t)std::max(1, f->nq) * (fp64 ? sizeof(Frac64) : sizeof(Frac32))));
+    CK(dalloc(&f->d_far, 3 * (size_t)std::max(1, f->nq)));
+    CK(dalloc(&f->d_qidx, (size_t)std::max(1, f->nq)));
+    if (f->nq > 0)
+      CK(cudaMemcpy(f->d_qidx, qidx.data(), sizeof(int) * f->nq, cudaMemcpyHostToDevice));
     const int recb = fp64 ? sizeof(KRec64) : sizeof(KRec32);
     if (f->coul_type == "EWALD") {
       // EWALD: the cube m in [-kmax, kmax]^3 \ {0} (ExecPointLocator::ExecuteOnKNeighbor,
@@ -966,16 +998,16 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
     std::vector<RhoRep> rr(nrep);
     const int ntiles = (f->P + f->ktile - 1) / f->ktile;
     const double target_blocks = 148.0 * (2048 / f->rho_threads) * 2.0;
-    const double chunk_atoms = std::max(256.0, (double)f->n * ntiles / target_blocks);
+    const double chunk_atoms = std::max(256.0, (double)std::max(1, f->nq) * ntiles / target_blocks);
     for (int r = 0; r < nrep; ++r) {
-      const int Nr = (int)(f->rep_off[r + 1] - f->rep_off[r]);
+      const int Nr = (int)(qoff[r + 1] - qoff[r]);   // charged atoms of replica r
       const int nch = std::max(1, (int)std::lround(Nr / chunk_atoms));
       rr[r].item_base = (int)items.size();
       rr[r].ntiles = ntiles;
       rr[r].nchunks = nch;
       for (int c = 0; c < nch; ++c) {
-        const int b = (int)f->rep_off[r] + (int)((int64_t)Nr * c / nch);
-        const int e = (int)f->rep_off[r] + (int)((int64_t)Nr * (c + 1) / nch);
+        const int b = (int)qoff[r] + (int)((int64_t)Nr * c / nch);
+        const int e = (int)qoff[r] + (int)((int64_t)Nr * (c + 1) / nch);
         for (int t = 0; t < ntiles; ++t) {
           RhoItem it;
           it.atom_begin = b;
@@ -996,9 +1028,9 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
     // spans (slots keep replicas contiguous), capped by kStageBytes
     {
       int need = 0;
-      for (int b0 = 0; b0 < f->n; b0 += 128) {
-        const int last = std::min(f->n, b0 + 128) - 1;
-        const int ra = rep_of[b0], rb = rep_of[last];
+      for (int b0 = 0; b0 < f->nq; b0 += 128) {
+        const int last = std::min(f->nq, b0 + 128) - 1;
+        const int ra = rep_of[qidx[b0]], rb = rep_of[qidx[last]];
         need = std::max(need, (rb - ra + 1) * f->P);
       }
       const int cap_recs = kStageBytes / (int)recb;
@@ -1339,6 +1371,16 @@ rbmd_status rbmd_force_phase_ms(rbmd_force* f, double* ms, int64_t* counts, int3
     ms[i] = f->phase_ms[i];
     if (counts) counts[i] = f->phase_n[i];
   }
+  return RBMD_OK;
+}
+
+rbmd_status rbmd_force_list_builds(rbmd_force* f, int64_t* builds) {
+  if (!f || !builds) return RBMD_ERR_ARG;
+  if (!f->bound) { *builds = 0; return RBMD_OK; }
+  unsigned long long v = 0;
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpy(&v, f->d_nbuilds, sizeof v, cudaMemcpyDeviceToHost));
+  *builds = (int64_t)v;
   return RBMD_OK;
 }
 

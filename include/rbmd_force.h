@@ -180,12 +180,16 @@ RBMD_API rbmd_status rbmd_force_get_neighbors(rbmd_force* f, int32_t* counts_hos
 RBMD_API rbmd_status rbmd_force_get_rhok(rbmd_force* f, double* rho_host, int32_t P);
 
 /* Per-phase device timing with CUDA events recorded on the stream each phase runs on
- * (0 integrate, 1 cell sort, 2 k-space, 3 neighbour list, 4 force pass, 5 constraints and
- * intramolecular terms).  enable resets the accumulators; phase_ms returns the summed
+ * (0 integrate, 1 cell sort, 2 structure factors, 3 neighbour list, 4 near/EAM force pass,
+ * 5 constraints and intramolecular terms, 6 k sampler, 7 RBE force).  enable resets the accumulators; phase_ms returns the summed
  * milliseconds and the number of timed intervals per phase since then.  No reference
  * counterpart beyond its vtkm::cont::Timer aliases (rbmd/framework/Timer.h:32). */
 RBMD_API rbmd_status rbmd_force_profile(rbmd_force* f, int32_t enable);
 RBMD_API rbmd_status rbmd_force_phase_ms(rbmd_force* f, double* ms, int64_t* counts, int32_t n);
+
+/* Number of neighbour-list builds since bind (with a Verlet skin the list is rebuilt only when
+ * an atom moved more than skin/2; the reference rebuilds on every force call). */
+RBMD_API rbmd_status rbmd_force_list_builds(rbmd_force* f, int64_t* builds);
 
 /* Library/kernel description for diagnostics: number of kernels the last compute or step
  * launched per step. */
