@@ -36,7 +36,7 @@ EXPORTED = [
     "rbmd_force_create", "rbmd_force_set_pair_coeffs", "rbmd_force_load_funcfl",
     "rbmd_force_set_water", "rbmd_force_bind", "rbmd_force_set_ksamples",
     "rbmd_force_set_kweights", "rbmd_force_get_ksamples", "rbmd_force_sample_k",
-    "rbmd_force_compute", "rbmd_force_compute_host", "rbmd_force_step",
+    "rbmd_force_compute", "rbmd_force_autotune", "rbmd_force_compute_host", "rbmd_force_step",
     "rbmd_force_sync_velocities", "rbmd_force_energy", "rbmd_force_status",
     "rbmd_force_get_neighbors", "rbmd_force_get_rhok", "rbmd_force_profile",
     "rbmd_force_phase_ms", "rbmd_force_list_builds", "rbmd_force_launch_count",
@@ -97,6 +97,7 @@ def library() -> ctypes.CDLL:
         "rbmd_force_get_ksamples": (I32, [V, P(I32), I32]),
         "rbmd_force_sample_k": (I32, [V, I64, P(I32), I32]),
         "rbmd_force_compute": (I32, [V, V]),
+        "rbmd_force_autotune": (I32, [V, V, P(I32), P(I32)]),
         "rbmd_force_compute_host": (I32, [V, P(D), P(D), V]),
         "rbmd_force_step": (I32, [V, I32, V]),
         "rbmd_force_sync_velocities": (I32, [V, V]),
@@ -240,6 +241,13 @@ class ForceField:
         _check(library().rbmd_force_compute(self._h, self._stream(stream)), "rbmd_force_compute")
 
     compute = Execute
+
+    def autotune(self, stream=None):
+        """Pick the fastest lanes-per-atom of the list build and force pass; returns both."""
+        a, b = ctypes.c_int32(), ctypes.c_int32()
+        _check(library().rbmd_force_autotune(self._h, self._stream(stream), ctypes.byref(a), ctypes.byref(b)),
+               "autotune")
+        return int(a.value), int(b.value)
 
     def compute_host(self, pos_host, force_host, stream=None):
         _check(library().rbmd_force_compute_host(self._h, _ptr(pos_host, ctypes.c_double),

@@ -119,19 +119,49 @@ __device__ __forceinline__ void min_image(R& q0, R& q1, R& q2, const R* box) {
   if (fabs(q2) > box[2] * (R)0.5) q2 -= (q2 > 0 ? box[2] : -box[2]);
 }
 
+// Nearest image for list reuse: the two atoms of a listed pair may each have wrapped across a
+// face since the build, so the stored vector can be off by up to two box lengths.
+template <class R>
+__device__ __forceinline__ void nearest_image(R& q0, R& q1, R& q2, const R* box) {
+  q0 -= box[0] * rint(q0 / box[0]);
+  q1 -= box[1] * rint(q1 / box[1]);
+  q2 -= box[2] * rint(q2 / box[2]);
+}
+
 __device__ __forceinline__ float rcp_r(float x) { return __frcp_rn(x); }
 __device__ __forceinline__ double rcp_r(double x) { return 1.0 / x; }
 
-// Per-slot near force.  One thread per slot over its transposed list row.
-// Pair physics: ComputeNearForceVerletWorklet / ComputeLJForceVerletWorklet
+// Two-float (hi, lo) reduction over the TPA lanes of a group: TwoSum at every butterfly level.
+template <class R, int TPA>
+__device__ __forceinline__ Acc<R> group_sum(Acc<R> a, unsigned gmask) {
+#pragma unroll
+  for (int o = TPA / 2; o > 0; o >>= 1) {
+    Acc<R> b;
+    b.hi = __shfl_xor_sync(gmask, a.hi, o);
+    if constexpr (sizeof(R) == 4) b.lo = __shfl_xor_sync(gmask, a.lo, o);
+    a.add(b.hi);
+    if constexpr (sizeof(R) == 4) a.lo = add_rn(a.lo, b.lo);
+  }
+  return a;
+}
+template <class R, int TPA>
+__device__ __forceinline__ R group_sum_plain(R v, unsigned gmask) {
+#pragma unroll
+  for (int o = TPA / 2; o > 0; o >>= 1) v += __shfl_xor_sync(gmask, v, o);
+  return v;
+}
+
+// Near force of one slot, TPA lanes per slot, each taking every TPA-th entry of the slot's list
+// row.  Pair physics: ComputeNearForceVerletWorklet / ComputeLJForceVerletWorklet
 // (rbmd/framework/run/worklet/RunWorklet.cpp:170-303) with ComputeLJForce and
 // ComputeNearEnergyForce (rbmd/framework/forceFunction/ExecForceFunction.h:74-140):
 //   LJ on MinDistanceVec(p_j', p_i) skipped within a molecule; Coulomb on p_j' - p_i for
 //   0.01 < d < rc with G = erfc(sqrt(a) d)/d^2 + 2 sqrt(a) e^{-a d^2}/(sqrt(pi) d); pairs with
-//   q_i q_j = 0 skip the Coulomb term.  Per-type LJ coefficients are staged in shared memory.
-// Accumulation: groups of four pair forces are summed in FP32 and folded into a two-float
-// (TwoSum) per-atom accumulator.
-template <class R, bool LJ, bool COUL, bool MOLEC, int MI, bool ENERGY>
+//   q_i q_j = 0 skip the Coulomb term (an uncharged slot skips it for all its lanes).
+// Per-type LJ coefficients are staged in shared memory.  Accumulation: each lane folds groups
+// of four pair forces (FP32 sums) into a two-float accumulator; the lanes' accumulators are
+// combined by a TwoSum butterfly.
+template <class R, int TPA, bool COUL, int MI>
 __global__ void __launch_bounds__(128) k_near_force(
     NearParams prm, const LJTable* __restrict__ ljt, const typename Traits<R>::V4* __restrict__ pos4,
     const int2* __restrict__ meta, const int* __restrict__ nbr, const int* __restrict__ count,
@@ -145,8 +175,14 @@ __global__ void __launch_bounds__(128) k_near_force(
     lj_s6[t] = sig6<R>(*ljt, t);
   }
   __syncthreads();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= prm.n) return;
+  constexpr bool LJ = true;
+  const bool MOLEC = prm.molecular != 0;
+  const bool ENERGY = energy_slot != nullptr;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = gt / TPA, sub = gt % TPA;
+  if (i >= prm.n) return;   // all lanes of a slot leave together
+  const int lane = threadIdx.x & 31;
+  const unsigned gmask = (TPA == 32 ? 0xffffffffu : ((1u << TPA) - 1u)) << (lane - sub);
   const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
   const typename Traits<R>::V4 pi = pos4[i];
   const bool typed = MOLEC || prm.ntypes > 1;
@@ -159,12 +195,14 @@ __global__ void __launch_bounds__(128) k_near_force(
   const R cs = (R)prm.coul_scale;
   const R qi = pi.w;
   const int trow = mi.x * prm.ntypes;
+  const int* row = nbr + (size_t)i * prm.cap;
   Acc<R> fx, fy, fz;
   R gx = 0, gy = 0, gz = 0;   // FP32 group sum folded into the accumulators every 4 pairs
   R e_lj = 0, e_coul = 0;
   const int cnt = min(count[i], prm.cap);   // an overflowed row is redone after regrowth
-  for (int p = 0; p < cnt; ++p) {
-    const int e = __ldg(nbr + (size_t)p * prm.stride + i);
+  int k = 0;
+  for (int p = sub; p < cnt; p += TPA, ++k) {
+    const int e = __ldg(row + p);
     const int j = e >> kShiftBits;
     const typename Traits<R>::V4 pj = pos4[j];
     R px = pj.x, py = pj.y, pz = pj.z;
@@ -175,7 +213,7 @@ __global__ void __launch_bounds__(128) k_near_force(
       pz = pz - (c2b == 1 ? wrap[2] : (c2b == 2 ? -wrap[2] : (R)0));
     }
     R r0 = px - pi.x, r1 = py - pi.y, r2 = pz - pi.z;
-    if (MI == kMiAll) min_image(r0, r1, r2, box);
+    if (MI == kMiAll) nearest_image(r0, r1, r2, box);
     const R d2 = r0 * r0 + r1 * r1 + r2 * r2;
     R f = 0;
     if (COUL) {
@@ -222,19 +260,27 @@ __global__ void __launch_bounds__(128) k_near_force(
     gx += f * r0 + fl0;
     gy += f * r1 + fl1;
     gz += f * r2 + fl2;
-    if ((p & 3) == 3) {
+    if ((k & 3) == 3) {
       fx.add(gx); fy.add(gy); fz.add(gz);
       gx = gy = gz = 0;
     }
   }
   fx.add(gx); fy.add(gy); fz.add(gz);
+  fx = group_sum<R, TPA>(fx, gmask);
+  fy = group_sum<R, TPA>(fy, gmask);
+  fz = group_sum<R, TPA>(fz, gmask);
+  if (ENERGY) {
+    e_lj = group_sum_plain<R, TPA>(e_lj, gmask);
+    e_coul = group_sum_plain<R, TPA>(e_coul, gmask);
+  }
+  if (sub != 0) return;
   const double F[3] = {fx.value(), fy.value(), fz.value()};
   if (!isfinite(F[0]) || !isfinite(F[1]) || !isfinite(F[2])) set_flag(status, kFlagNonFinite);
   const int id = slot_atom[i];
   force[3 * id] = F[0];
   force[3 * id + 1] = F[1];
   force[3 * id + 2] = F[2];
-  if (ENERGY && energy_slot) {
+  if (ENERGY) {
     energy_slot[2 * i] = 0.5 * (double)e_lj;
     energy_slot[2 * i + 1] = 0.5 * (double)e_coul;
   }
@@ -535,25 +581,29 @@ struct EamDev {
   float rhomax;
 };
 
-template <class R>
-__global__ void __launch_bounds__(128) k_eam_fp(int n, int stride, int cap, double rc, EamDev eam,
+template <class R, int TPA>
+__global__ void __launch_bounds__(128) k_eam_fp(int n, int cap, double rc, EamDev eam,
                                                 const typename Traits<R>::V4* __restrict__ pos4,
                                                 const int* __restrict__ nbr, const int* __restrict__ count,
                                                 const RepDev* __restrict__ reps,
                                                 const int* __restrict__ rep_of_slot, R* __restrict__ fp,
                                                 double* __restrict__ embed_slot) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = gt / TPA, sub = gt % TPA;
   if (i >= n) return;
+  const int lane = threadIdx.x & 31;
+  const unsigned gmask = (TPA == 32 ? 0xffffffffu : ((1u << TPA) - 1u)) << (lane - sub);
   const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
   const typename Traits<R>::V4 pi = pos4[i];
   const R wrap[3] = {Traits<R>::wrap(rp, 0), Traits<R>::wrap(rp, 1), Traits<R>::wrap(rp, 2)};
   const R box[3] = {Traits<R>::box(rp, 0), Traits<R>::box(rp, 1), Traits<R>::box(rp, 2)};
   const R cut2 = (R)rc * (R)rc;
   const R rdr = sizeof(R) == 4 ? (R)eam.rdr : (R)eam.rdr_d;
+  const int* row = nbr + (size_t)i * cap;
   Acc<R> rho;
   const int cnt = min(count[i], cap);
-  for (int p = 0; p < cnt; ++p) {
-    const int e = __ldg(nbr + (size_t)p * stride + i);
+  for (int p = sub; p < cnt; p += TPA) {
+    const int e = __ldg(row + p);
     const int j = e >> kShiftBits;
     const typename Traits<R>::V4 pj = pos4[j];
     R r[3];
@@ -563,7 +613,7 @@ __global__ void __launch_bounds__(128) k_eam_fp(int n, int stride, int cap, doub
       const int cd = (e >> (2 * d)) & 3;
       const R off = cd == 1 ? wrap[d] : (cd == 2 ? -wrap[d] : (R)0);
       R v = piv[d] - (pjv[d] - off);
-      if (fabs(v) > box[d] * (R)0.5) v -= (v > 0 ? box[d] : -box[d]);
+      v -= box[d] * rint(v / box[d]);   // MinDistanceVec (nearest image also under list reuse)
       r[d] = v;
     }
     const R rsq = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
@@ -578,6 +628,8 @@ __global__ void __launch_bounds__(128) k_eam_fp(int n, int stride, int cap, doub
       rho.add((((R)b.w * pp + (R)c.x) * pp + (R)c.y) * pp + (R)c.z);
     }
   }
+  rho = group_sum<R, TPA>(rho, gmask);
+  if (sub != 0) return;
   const R rr = (R)rho.value();
   R pp = rr * (sizeof(R) == 4 ? (R)eam.rdrho : (R)eam.rdrho_d) + (R)1;
   int m = (int)pp;
@@ -594,8 +646,8 @@ __global__ void __launch_bounds__(128) k_eam_fp(int n, int stride, int cap, doub
   }
 }
 
-template <class R>
-__global__ void __launch_bounds__(128) k_eam_force(int n, int stride, int cap, double rc, EamDev eam,
+template <class R, int TPA>
+__global__ void __launch_bounds__(128) k_eam_force(int n, int cap, double rc, EamDev eam,
                                                    const typename Traits<R>::V4* __restrict__ pos4,
                                                    const int* __restrict__ nbr, const int* __restrict__ count,
                                                    const RepDev* __restrict__ reps,
@@ -603,8 +655,11 @@ __global__ void __launch_bounds__(128) k_eam_force(int n, int stride, int cap, d
                                                    const R* __restrict__ fp, const int* __restrict__ slot_atom,
                                                    double* __restrict__ force, double* __restrict__ pair_slot,
                                                    uint32_t* status) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = gt / TPA, sub = gt % TPA;
   if (i >= n) return;
+  const int lane = threadIdx.x & 31;
+  const unsigned gmask = (TPA == 32 ? 0xffffffffu : ((1u << TPA) - 1u)) << (lane - sub);
   const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
   const typename Traits<R>::V4 pi = pos4[i];
   const R wrap[3] = {Traits<R>::wrap(rp, 0), Traits<R>::wrap(rp, 1), Traits<R>::wrap(rp, 2)};
@@ -612,11 +667,12 @@ __global__ void __launch_bounds__(128) k_eam_force(int n, int stride, int cap, d
   const R cut2 = (R)rc * (R)rc;
   const R rdr = sizeof(R) == 4 ? (R)eam.rdr : (R)eam.rdr_d;
   const R fpi = fp[i];
+  const int* row = nbr + (size_t)i * cap;
   Acc<R> fx, fy, fz;
   R epair = 0;
   const int cnt = min(count[i], cap);
-  for (int p = 0; p < cnt; ++p) {
-    const int e = __ldg(nbr + (size_t)p * stride + i);
+  for (int p = sub; p < cnt; p += TPA) {
+    const int e = __ldg(row + p);
     const int j = e >> kShiftBits;
     const typename Traits<R>::V4 pj = pos4[j];
     R r[3];
@@ -626,7 +682,7 @@ __global__ void __launch_bounds__(128) k_eam_force(int n, int stride, int cap, d
       const int cd = (e >> (2 * d)) & 3;
       const R off = cd == 1 ? wrap[d] : (cd == 2 ? -wrap[d] : (R)0);
       R v = (pjv[d] - off) - piv[d];
-      if (fabs(v) > box[d] * (R)0.5) v -= (v > 0 ? box[d] : -box[d]);
+      v -= box[d] * rint(v / box[d]);
       r[d] = v;
     }
     const R rsq = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
@@ -654,6 +710,11 @@ __global__ void __launch_bounds__(128) k_eam_force(int n, int stride, int cap, d
       epair += phi;
     }
   }
+  fx = group_sum<R, TPA>(fx, gmask);
+  fy = group_sum<R, TPA>(fy, gmask);
+  fz = group_sum<R, TPA>(fz, gmask);
+  epair = group_sum_plain<R, TPA>(epair, gmask);
+  if (sub != 0) return;
   const double F[3] = {fx.value(), fy.value(), fz.value()};
   if (!isfinite(F[0]) || !isfinite(F[1]) || !isfinite(F[2])) set_flag(status, kFlagNonFinite);
   const int id = slot_atom[i];

@@ -15,6 +15,7 @@
 #include <fstream>
 #include <sstream>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/rbmd_force.h"
@@ -84,6 +85,9 @@ struct rbmd_force {
   double shake_tol = 1e-5;
   int energy_every = 0;   // energies inside step(): every outputs.thermo_out.interval steps
   int cap_override = 0;   // neighbor.capacity: initial list capacity (grown on overflow)
+  int tpa_list = 8, tpa_near = 8;   // lanes per atom of the list build / force pass
+  bool autotune = false;            // "autotune": true tunes them at the first compute
+  bool tuned = false;
   int shake_max_iter = 5000;
   std::string potential_file;
 
@@ -316,15 +320,24 @@ double rbe_S(double alpha, const double* L) {
   return H[0] * H[1] * H[2] - 1.0;
 }
 
+template <class R, int TPA>
+void launch_nlist_t(rbmd_force* f, cudaStream_t s) {
+  const long long threads = (long long)f->n * TPA;
+  k_nlist<R, TPA><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(
+      f->n, (const typename Traits<R>::V4*)f->d_pos4, f->d_cell_start, f->d_reps,
+      f->nrep > 1 ? f->d_rep_of : nullptr, f->num_cycles, (R)f->list_cut(), f->cap, f->d_nbr,
+      f->d_count, f->d_maxcount, f->d_status, f->skin > 0 ? f->d_rebuild : nullptr, f->d_nbuilds);
+}
+
 template <class R>
 void launch_nlist(rbmd_force* f, cudaStream_t s) {
   PhaseScope ps(f, kPhList, s);
-  const int nb = (f->n + 127) / 128;
-  k_nlist<R><<<nb, 128, 0, s>>>(f->n, (const typename Traits<R>::V4*)f->d_pos4, f->d_cell_start,
-                                f->d_reps, f->nrep > 1 ? f->d_rep_of : nullptr, f->num_cycles,
-                                (R)f->list_cut(), f->cap, f->stride, f->d_nbr, f->d_count,
-                                f->d_maxcount, f->d_status, f->skin > 0 ? f->d_rebuild : nullptr,
-                                f->d_nbuilds);
+  switch (f->tpa_list) {
+    case 4: launch_nlist_t<R, 4>(f, s); break;
+    case 16: launch_nlist_t<R, 16>(f, s); break;
+    case 32: launch_nlist_t<R, 32>(f, s); break;
+    default: launch_nlist_t<R, 8>(f, s); break;
+  }
   f->launches++;
 }
 
@@ -395,54 +408,51 @@ void launch_kspace(rbmd_force* f, cudaStream_t s, cudaEvent_t ready) {
   f->launches += 4;
 }
 
-template <class R, bool LJ, bool COUL, bool MOLEC, int MI, bool ENERGY>
+template <class R, int TPA, bool COUL, int MI>
 void launch_near_t(rbmd_force* f, cudaStream_t s) {
   NearParams p;
   p.n = f->n;
   p.stride = f->stride;
   p.ntypes = f->nt_eff;
   p.cap = f->cap;
-  p.with_lj = LJ;
+  p.with_lj = 1;
   p.with_coul = COUL;
-  p.molecular = MOLEC;
+  p.molecular = f->at.molecule != nullptr;
   p.rc = f->rc;
   p.alpha = f->alpha;
   p.coul_scale = f->near_coul_scale;
   p.sqrt_alpha = std::sqrt(f->alpha);
   p.two_sqrt_alpha_over_sqrt_pi = 2.0 * std::sqrt(f->alpha) / std::sqrt(M_PI);
   p.kstage = 0;
-  k_near_force<R, LJ, COUL, MOLEC, MI, ENERGY><<<(f->n + 127) / 128, 128, 0, s>>>(
+  const long long threads = (long long)f->n * TPA;
+  k_near_force<R, TPA, COUL, MI><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(
       p, f->d_ljt, (const typename Traits<R>::V4*)f->d_pos4, f->d_meta, f->d_nbr, f->d_count,
-      f->d_reps, f->nrep > 1 ? f->d_rep_of : nullptr, f->d_slot_atom, f->at.force, f->d_eslot,
-      f->d_status);
+      f->d_reps, f->nrep > 1 ? f->d_rep_of : nullptr, f->d_slot_atom, f->at.force,
+      f->want_energy ? f->d_eslot : nullptr, f->d_status);
   f->launches++;
 }
 
-template <class R, bool COUL, bool MOLEC>
+template <class R, int TPA, bool COUL>
 void launch_near_m(rbmd_force* f, cudaStream_t s) {
   const int mi = f->skin > 0 ? kMiAll : (f->minimg ? kMiLJ : kMiNone);
-  if (mi == kMiAll) {
-    if (f->want_energy) launch_near_t<R, true, COUL, MOLEC, kMiAll, true>(f, s);
-    else launch_near_t<R, true, COUL, MOLEC, kMiAll, false>(f, s);
-  } else if (mi == kMiLJ) {
-    if (f->want_energy) launch_near_t<R, true, COUL, MOLEC, kMiLJ, true>(f, s);
-    else launch_near_t<R, true, COUL, MOLEC, kMiLJ, false>(f, s);
-  } else {
-    if (f->want_energy) launch_near_t<R, true, COUL, MOLEC, kMiNone, true>(f, s);
-    else launch_near_t<R, true, COUL, MOLEC, kMiNone, false>(f, s);
-  }
+  if (mi == kMiAll) launch_near_t<R, TPA, COUL, kMiAll>(f, s);
+  else if (mi == kMiLJ) launch_near_t<R, TPA, COUL, kMiLJ>(f, s);
+  else launch_near_t<R, TPA, COUL, kMiNone>(f, s);
+}
+
+template <class R, int TPA>
+void launch_near_c(rbmd_force* f, cudaStream_t s) {
+  if (f->with_coul_near()) launch_near_m<R, TPA, true>(f, s);
+  else launch_near_m<R, TPA, false>(f, s);
 }
 
 template <class R>
 void launch_near(rbmd_force* f, cudaStream_t s) {
-  const bool coul = f->with_coul_near();
-  const bool molec = f->at.molecule != nullptr;
-  if (coul) {
-    if (molec) launch_near_m<R, true, true>(f, s);
-    else launch_near_m<R, true, false>(f, s);
-  } else {
-    if (molec) launch_near_m<R, false, true>(f, s);
-    else launch_near_m<R, false, false>(f, s);
+  switch (f->tpa_near) {
+    case 4: launch_near_c<R, 4>(f, s); break;
+    case 16: launch_near_c<R, 16>(f, s); break;
+    case 32: launch_near_c<R, 32>(f, s); break;
+    default: launch_near_c<R, 8>(f, s); break;
   }
 }
 
@@ -459,14 +469,22 @@ void launch_eam(rbmd_force* f, cudaStream_t s) {
   e.rdr_d = 1.0 / (double)f->eam_h.dr;
   e.rdrho_d = 1.0 / (double)f->eam_h.drho;
   e.rhomax = f->eam_h.rhomax;
-  const int nb = (f->n + 127) / 128;
-  k_eam_fp<R><<<nb, 128, 0, s>>>(f->n, f->stride, f->cap, f->rc, e, (const typename Traits<R>::V4*)f->d_pos4,
-                                 f->d_nbr, f->d_count, f->d_reps, f->nrep > 1 ? f->d_rep_of : nullptr,
-                                 (R*)f->d_fp, f->d_emb);
-  k_eam_force<R><<<nb, 128, 0, s>>>(f->n, f->stride, f->cap, f->rc, e, (const typename Traits<R>::V4*)f->d_pos4,
-                                    f->d_nbr, f->d_count, f->d_reps, f->nrep > 1 ? f->d_rep_of : nullptr,
-                                    (const R*)f->d_fp, f->d_slot_atom, f->at.force, f->d_epair,
-                                    f->d_status);
+  const int* rp = f->nrep > 1 ? f->d_rep_of : nullptr;
+  auto go = [&](auto tpa_tag) {
+    constexpr int TPA = decltype(tpa_tag)::value;
+    const unsigned nb = (unsigned)(((long long)f->n * TPA + 127) / 128);
+    k_eam_fp<R, TPA><<<nb, 128, 0, s>>>(f->n, f->cap, f->rc, e, (const typename Traits<R>::V4*)f->d_pos4,
+                                        f->d_nbr, f->d_count, f->d_reps, rp, (R*)f->d_fp, f->d_emb);
+    k_eam_force<R, TPA><<<nb, 128, 0, s>>>(f->n, f->cap, f->rc, e, (const typename Traits<R>::V4*)f->d_pos4,
+                                           f->d_nbr, f->d_count, f->d_reps, rp, (const R*)f->d_fp,
+                                           f->d_slot_atom, f->at.force, f->d_epair, f->d_status);
+  };
+  switch (f->tpa_near) {
+    case 4: go(std::integral_constant<int, 4>{}); break;
+    case 16: go(std::integral_constant<int, 16>{}); break;
+    case 32: go(std::integral_constant<int, 32>{}); break;
+    default: go(std::integral_constant<int, 8>{}); break;
+  }
   f->launches += 2;
 }
 
@@ -532,7 +550,7 @@ void launch_compute_any(rbmd_force* f, cudaStream_t s) {
 rbmd_status grow_list(rbmd_force* f, int need) {
   const int newcap = ((int)(need * 1.2) + 8 + 7) & ~7;
   dfree(f->d_nbr);
-  CK(dalloc(&f->d_nbr, (size_t)newcap * f->stride));
+  CK(dalloc(&f->d_nbr, (size_t)newcap * f->n));
   f->cap = newcap;
   return RBMD_OK;
 }
@@ -657,6 +675,14 @@ rbmd_status parse_config(rbmd_force* f, const char* text) {
   f->rs = f->nbr_type == "RBL" ? num(root, "hyper_parameters.neighbor.r_core", f->rc) : f->rc;
   f->skin = num(root, "hyper_parameters.neighbor.skin", 0.0);
   f->cap_override = (int)num(root, "hyper_parameters.neighbor.capacity", 0.0);
+  {
+    const Value* at = root.path("autotune");
+    if (at && at->kind == Value::Bool) f->autotune = at->b;
+    const int tl = (int)num(root, "tuning.list_lanes", 0.0), tn = (int)num(root, "tuning.force_lanes", 0.0);
+    auto ok = [](int t) { return t == 4 || t == 8 || t == 16 || t == 32; };
+    if (ok(tl)) { f->tpa_list = tl; f->autotune = false; }
+    if (ok(tn)) { f->tpa_near = tn; f->autotune = false; }
+  }
   f->far = root.path("hyper_parameters.coulomb") != nullptr;
   if (f->far) {
     f->coul_type = rbmdjson::text(root, "hyper_parameters.coulomb.type", "RBE");
@@ -756,6 +782,55 @@ rbmd_status upload_ksamples(rbmd_force* f, const int32_t* m_xyz) {
   CK(cudaMemcpy(f->d_krec, buf.data(), buf.size(), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(f->d_kvec, m_xyz, sizeof(int) * 3 * f->Ptot, cudaMemcpyHostToDevice));
   f->injected = true;
+  return RBMD_OK;
+}
+
+// Own autotuner: times every lane count of the list build and of the force pass (3 launches
+// each, best taken) on the bound system and keeps the fastest.
+template <class R>
+rbmd_status autotune_impl(rbmd_force* f, cudaStream_t s) {
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  const bool prof = f->prof_on;
+  f->prof_on = false;
+  const int cand[4] = {4, 8, 16, 32};
+  auto best_of = [&](auto launch) -> float {
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+      if (f->d_rebuild) cudaMemsetAsync(f->d_rebuild, 1, sizeof(int), s);
+      cudaEventRecord(a, s);
+      launch();
+      cudaEventRecord(b, s);
+      cudaEventSynchronize(b);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, a, b);
+      if (rep > 0) best = std::min(best, ms);
+    }
+    return best;
+  };
+  float bl = 1e30f, bn = 1e30f;
+  int tl = f->tpa_list, tn = f->tpa_near;
+  for (int t : cand) {
+    f->tpa_list = t;
+    const float ms = best_of([&] { launch_nlist<R>(f, s); });
+    if (ms < bl) { bl = ms; tl = t; }
+  }
+  f->tpa_list = tl;
+  for (int t : cand) {
+    f->tpa_near = t;
+    const float ms = best_of([&] {
+      if (f->is_eam()) launch_eam<R>(f, s);
+      else launch_near<R>(f, s);
+    });
+    if (ms < bn) { bn = ms; tn = t; }
+  }
+  f->tpa_near = tn;
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  f->prof_on = prof;
+  CK(cudaGetLastError());
+  f->tuned = true;
   return RBMD_OK;
 }
 
@@ -907,7 +982,7 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
   CK(dalloc(&f->d_atom_slot, n));
   CK(cudaMalloc(&f->d_pos4, n * (fp64 ? sizeof(double4) : sizeof(float4))));
   CK(dalloc(&f->d_meta, n));
-  CK(dalloc(&f->d_nbr, (size_t)f->cap * f->stride));
+  CK(dalloc(&f->d_nbr, (size_t)f->cap * f->n));
   CK(dalloc(&f->d_count, n));
   CK(dalloc(&f->d_maxcount, 1));
   CK(dalloc(&f->d_nbuilds, 1));
@@ -1193,10 +1268,35 @@ rbmd_status rbmd_force_sample_k(rbmd_force* f, int64_t step, int32_t* m_xyz, int
   return RBMD_OK;
 }
 
+rbmd_status rbmd_force_autotune(rbmd_force* f, void* stream, int32_t* list_lanes, int32_t* force_lanes) {
+  if (!f) return RBMD_ERR_ARG;
+  if (!f->bound) return RBMD_ERR_STATE;
+  cudaStream_t s = (cudaStream_t)stream;
+  f->launches = 0;
+  launch_compute_any(f, s);            // current list and caches
+  bool redo = false;
+  rbmd_status st = check_overflow(f, s, &redo);
+  if (st) return st;
+  if (redo) {
+    launch_compute_any(f, s);
+    st = check_overflow(f, s, &redo);
+    if (st) return st;
+  }
+  st = f->fp64 ? autotune_impl<double>(f, s) : autotune_impl<float>(f, s);
+  if (st) return st;
+  launch_compute_any(f, s);            // leave forces of the chosen configuration
+  st = check_overflow(f, s, &redo);
+  if (st) return st;
+  if (list_lanes) *list_lanes = f->tpa_list;
+  if (force_lanes) *force_lanes = f->tpa_near;
+  return RBMD_OK;
+}
+
 rbmd_status rbmd_force_compute(rbmd_force* f, void* stream) {
   if (!f) return RBMD_ERR_ARG;
   if (!f->bound) return RBMD_ERR_STATE;
   cudaStream_t s = (cudaStream_t)stream;
+  if (f->autotune && !f->tuned) return rbmd_force_autotune(f, stream, nullptr, nullptr);
   for (int attempt = 0; attempt < 4; ++attempt) {
     f->launches = 0;
     launch_compute_any(f, s);
@@ -1335,7 +1435,7 @@ rbmd_status rbmd_force_get_neighbors(rbmd_force* f, int32_t* counts, int32_t* id
   if (!f->bound) return RBMD_ERR_STATE;
   CK(cudaDeviceSynchronize());
   const size_t n = f->n;
-  std::vector<int> cnt(n), slot_atom(n), nbr((size_t)f->cap * f->stride);
+  std::vector<int> cnt(n), slot_atom(n), nbr((size_t)f->cap * n);
   CK(cudaMemcpy(cnt.data(), f->d_count, sizeof(int) * n, cudaMemcpyDeviceToHost));
   CK(cudaMemcpy(slot_atom.data(), f->d_slot_atom, sizeof(int) * n, cudaMemcpyDeviceToHost));
   CK(cudaMemcpy(nbr.data(), f->d_nbr, sizeof(int) * nbr.size(), cudaMemcpyDeviceToHost));
@@ -1346,7 +1446,7 @@ rbmd_status rbmd_force_get_neighbors(rbmd_force* f, int32_t* counts, int32_t* id
     const int m = std::min<int>(cnt[i], f->cap);
     if (cnt[i] > cap) too_small = true;
     for (int p = 0; p < m && p < cap; ++p)
-      ids[(size_t)id * cap + p] = slot_atom[nbr[(size_t)p * f->stride + i] >> kShiftBits];
+      ids[(size_t)id * cap + p] = slot_atom[nbr[(size_t)i * f->cap + p] >> kShiftBits];
   }
   return too_small ? RBMD_ERR_ARG : RBMD_OK;
 }

@@ -23,12 +23,13 @@ def _posr(pos, prec):
     return pos.astype(np.float32) if prec == "fp32" else pos.astype(np.float64)
 
 
-@pytest.mark.parametrize("prec", ["fp32", "fp64"])
-def test_lj_pairs_and_force(cuda, oracle_lib, prec):
+@pytest.mark.parametrize("prec,lanes", [("fp32", 8), ("fp64", 8), ("fp32", 4), ("fp32", 32), ("fp64", 16)])
+def test_lj_pairs_and_force(cuda, oracle_lib, prec, lanes):
     import torch
     s = systems.lj_fcc(ncell=8, seed=2)
     s["pos"] = jitter(s["pos"], s["lo"], s["hi"], 0.08, seed=5)
     cfg = systems.lj_config(cutoff=2.5, precision=prec)
+    cfg["tuning"] = {"list_lanes": lanes, "force_lanes": lanes}
     dev = to_dev(s, cuda)
     ff = make_ff(cfg, s, dev)
     ff.Execute()
@@ -135,6 +136,28 @@ def test_rbe_kspace_accuracy(cuda, oracle_lib, prec):
         e_ref = rel_err(far32, far64)
         assert e_dev <= min(e_ref, 1e-5), f"k-space err {e_dev:.3e}, reference-precision err {e_ref:.3e}"
         assert amp_err <= 1e-5, amp_err
+
+
+def test_autotune_keeps_parity(cuda, oracle_lib):
+    import torch
+    n, P = 3000, 32
+    s, cfg = _electrolyte(n, P, "fp32")
+    alpha = cfg["hyper_parameters"]["coulomb"]["alpha"]
+    L = s["hi"] - s["lo"]
+    m = oracle_lib.rbe_sample(alpha, L, seed=5, step=0, rep=0, P=P)
+    dev = to_dev(s, cuda)
+    ff = make_ff(cfg, s, dev)
+    ff.set_ksamples(m)
+    tl, tn = ff.autotune()
+    assert tl in (4, 8, 16, 32) and tn in (4, 8, 16, 32)
+    torch.cuda.synchronize()
+    pr = _posr(s["pos"], "fp32")
+    nl = oracle_lib.neighbors(pr, s["lo"], s["hi"], 2.5, "fp32")
+    near = oracle_lib.near_force(pr, s["lo"], s["hi"], 2.5, nl, type=s["type"], charge=s["charge"],
+                                 eps=s["eps"], sigma=s["sigma"], with_coul=True, alpha=alpha, prec="fp32")
+    rho = oracle_lib.rhok(s["pos"], s["charge"], L, m)
+    far = oracle_lib.rbe_force(s["pos"], s["charge"], L, alpha, 1.0, m, rho)
+    assert rel_err(dev["force"].cpu().numpy(), near + far) <= TOL["fp32"]
 
 
 def test_sampler_matches_oracle(cuda, oracle_lib):
