@@ -158,7 +158,7 @@ def run_ours(args):
     ff.Init(t["pos"], t["force"], vel=t["vel"], mass=t["mass"], charge=t["charge"], type=t["type"],
             image=t["image"])
     stream = torch.cuda.current_stream(dev)
-    lanes = ff.autotune()                          # own autotuner: lanes per atom of list / force
+    blocks = ff.autotune()                         # own autotuner: threads per block of list / force
     ff.Execute()                                   # initial force (ExecutionNVT::Init)
     ff.step(args.warmup)
     torch.cuda.synchronize(dev)
@@ -282,7 +282,7 @@ def run_ours(args):
             "config": {"workload": f"electrolyte {n} atoms, plain Gaussian RBE P={args.P}, full MD step",
                        "atoms_per_gpu": n, "P": args.P, "proposal": "gauss", "rc": 2.5, "skin": args.skin,
                        "list_builds_per_step": builds / args.steps,
-                       "lanes_per_atom": {"list": lanes[0], "force": lanes[1]},
+                       "threads_per_block": {"list": blocks[0], "force": blocks[1]},
                        "alpha": cfg["hyper_parameters"]["coulomb"]["alpha"], "box": float(s["hi"][0]),
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2": "inputs larger than L2 (neighbour list %.0f MB + state %.0f MB)"

@@ -243,7 +243,7 @@ class ForceField:
     compute = Execute
 
     def autotune(self, stream=None):
-        """Pick the fastest lanes-per-atom of the list build and force pass; returns both."""
+        """Pick the fastest threads-per-block of the list build and force pass; returns both."""
         a, b = ctypes.c_int32(), ctypes.c_int32()
         _check(library().rbmd_force_autotune(self._h, self._stream(stream), ctypes.byref(a), ctypes.byref(b)),
                "autotune")

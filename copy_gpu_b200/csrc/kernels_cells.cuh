@@ -240,55 +240,42 @@ __global__ void k_regather(int n, const int* __restrict__ slot_atom, const doubl
 __device__ __forceinline__ bool gt_small(float x) { return x > 1.0e-4f; }
 __device__ __forceinline__ bool gt_small(double x) { return x > 1.0e-4; }
 
-// Full Verlet list with the predicate of ComputeNeighboursWorklet
+// Full Verlet list of slot i with the predicate of ComputeNeighboursWorklet
 // (rbmd/framework/run/worklet/RunWorklet.cpp:40-96): rc^2 - d^2 > 1e-4 && d^2 > 1e-4 on
 // r = (p_j - offset) - p_i with uncontracted float ops and the reference's cell-based periodic
-// offsets (PeriodicCoordOffset).
-// TPA lanes cooperate on one slot: they test consecutive candidates of a slot range, a ballot
-// over the lane group compacts the hits, and the row nbr[slot * cap + p] is written in
-// candidate order (coalesced).  Traversal: for each of the (2nc+1)^2 (y, z) neighbour rows the
-// x cells ci-nc .. ci+nc are consecutive cell indices, hence one contiguous slot range when no
-// x wrap occurs; rows that wrap in x are walked cell by cell.  The pair set equals the
+// offsets (PeriodicCoordOffset).  Traversal: for each of the (2nc+1)^2 (y, z) neighbour rows the
+// x cells ci-nc .. ci+nc are consecutive cell indices, hence one contiguous slot range when no x
+// wrap occurs; rows that wrap in x are walked cell by cell.  The pair set equals the
 // reference's 27-cell stencil; the order inside a row differs (sets are order-free).
-template <class R, int TPA>
-__device__ __forceinline__ int nlist_range(int s0, const int s1, const typename Traits<R>::V4* __restrict__ pos4,
+template <class R>
+__device__ __forceinline__ int nlist_range(int s, const int s1, const typename Traits<R>::V4* __restrict__ pos4,
                                            const R* pix, const R* off, int code, R cut2, int idx, int cap,
-                                           int sub, unsigned gmask, int gshift, int* __restrict__ row) {
-  for (int base = s0; base < s1; base += TPA) {
-    const int s = base + sub;
-    bool hit = false;
-    if (s < s1) {
-      const typename Traits<R>::V4 pj = pos4[s];
-      const R r0 = sub_rn(sub_rn(pj.x, off[0]), pix[0]);
-      const R r1 = sub_rn(sub_rn(pj.y, off[1]), pix[1]);
-      const R r2 = sub_rn(sub_rn(pj.z, off[2]), pix[2]);
-      const R d2 = add_rn(add_rn(mul_rn(r0, r0), mul_rn(r1, r1)), mul_rn(r2, r2));
-      hit = gt_small(sub_rn(cut2, d2)) && gt_small(d2);
+                                           int stride, int i, int* __restrict__ nbr) {
+#pragma unroll 4
+  for (; s < s1; ++s) {
+    const typename Traits<R>::V4 pj = pos4[s];
+    const R r0 = sub_rn(sub_rn(pj.x, off[0]), pix[0]);
+    const R r1 = sub_rn(sub_rn(pj.y, off[1]), pix[1]);
+    const R r2 = sub_rn(sub_rn(pj.z, off[2]), pix[2]);
+    const R d2 = add_rn(add_rn(mul_rn(r0, r0), mul_rn(r1, r1)), mul_rn(r2, r2));
+    if (gt_small(sub_rn(cut2, d2)) && gt_small(d2)) {
+      if (idx < cap) nbr[(size_t)idx * stride + i] = (s << kShiftBits) | code;
+      ++idx;
     }
-    const unsigned bal = (__ballot_sync(gmask, hit) >> gshift) & (TPA == 32 ? 0xffffffffu : ((1u << TPA) - 1u));
-    if (hit) {
-      const int pos = idx + __popc(bal & ((1u << sub) - 1u));
-      if (pos < cap) row[pos] = (s << kShiftBits) | code;
-    }
-    idx += __popc(bal);
   }
   return idx;
 }
 
-template <class R, int TPA>
-__global__ void __launch_bounds__(128) k_nlist(
+template <class R>
+__global__ void __launch_bounds__(256) k_nlist(
     int n, const typename Traits<R>::V4* __restrict__ pos4, const int* __restrict__ cell_start,
     const RepDev* __restrict__ reps, const int* __restrict__ rep_of_slot, int num_cycles, R rc,
-    int cap, int* __restrict__ nbr, int* __restrict__ count, int* __restrict__ max_count,
+    int cap, int stride, int* __restrict__ nbr, int* __restrict__ count, int* __restrict__ max_count,
     uint32_t* status, const int* __restrict__ rebuild, unsigned long long* __restrict__ nbuilds) {
   if (rebuild && !*rebuild) return;
-  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gt == 0 && nbuilds) atomicAdd(nbuilds, 1ull);
-  const int i = gt / TPA, sub = gt % TPA;
-  if (i >= n) return;   // all TPA lanes of a slot leave together
-  const int lane = threadIdx.x & 31;
-  const int gshift = lane - sub;
-  const unsigned gmask = (TPA == 32 ? 0xffffffffu : ((1u << TPA) - 1u)) << gshift;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0 && nbuilds) atomicAdd(nbuilds, 1ull);
+  if (i >= n) return;
   const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
   const typename Traits<R>::V4 pi = pos4[i];
   const R pix[3] = {pi.x, pi.y, pi.z};
@@ -300,7 +287,6 @@ __global__ void __launch_bounds__(128) k_nlist(
   const int nc = num_cycles;
   const int dx0 = rp.dims[0], dx1 = rp.dims[1], dx2 = rp.dims[2];
   const bool x_contig = ci[0] - nc >= 0 && ci[0] + nc < dx0;
-  int* row = nbr + (size_t)i * cap;
   int idx = 0;
   for (int b = -nc; b <= nc; ++b)
     for (int c = -nc; c <= nc; ++c) {
@@ -311,11 +297,11 @@ __global__ void __launch_bounds__(128) k_nlist(
       off[1] = mul_rn(Traits<R>::dx(rp, 1), (R)dy);
       off[2] = mul_rn(Traits<R>::dx(rp, 2), (R)dz);
       const int code_yz = ((dy > 0 ? 1 : (dy < 0 ? 2 : 0)) << 2) | ((dz > 0 ? 1 : (dz < 0 ? 2 : 0)) << 4);
-      const int rowc = rp.cell_base + wy * dx0 + wz * dx0 * dx1;
+      const int row = rp.cell_base + wy * dx0 + wz * dx0 * dx1;
       if (x_contig) {
         off[0] = (R)0;
-        idx = nlist_range<R, TPA>(cell_start[rowc + ci[0] - nc], cell_start[rowc + ci[0] + nc + 1], pos4,
-                                  pix, off, code_yz, cut2, idx, cap, sub, gmask, gshift, row);
+        idx = nlist_range<R>(cell_start[row + ci[0] - nc], cell_start[row + ci[0] + nc + 1], pos4, pix,
+                             off, code_yz, cut2, idx, cap, stride, i, nbr);
       } else {
         for (int a = -nc; a <= nc; ++a) {
           const int nbx = ci[0] + a;
@@ -323,17 +309,15 @@ __global__ void __launch_bounds__(128) k_nlist(
           const int ddx = wx - nbx;
           off[0] = mul_rn(Traits<R>::dx(rp, 0), (R)ddx);
           const int code = code_yz | (ddx > 0 ? 1 : (ddx < 0 ? 2 : 0));
-          idx = nlist_range<R, TPA>(cell_start[rowc + wx], cell_start[rowc + wx + 1], pos4, pix, off, code,
-                                    cut2, idx, cap, sub, gmask, gshift, row);
+          idx = nlist_range<R>(cell_start[row + wx], cell_start[row + wx + 1], pos4, pix, off, code, cut2,
+                               idx, cap, stride, i, nbr);
         }
       }
     }
-  if (sub == 0) {
-    count[i] = idx;
-    if (idx > cap) {
-      set_flag(status, kFlagListOverflow);
-      atomicMax(max_count, idx);
-    }
+  count[i] = idx;
+  if (idx > cap) {
+    set_flag(status, kFlagListOverflow);
+    atomicMax(max_count, idx);
   }
 }
 

@@ -131,43 +131,27 @@ __device__ __forceinline__ void nearest_image(R& q0, R& q1, R& q2, const R* box)
 __device__ __forceinline__ float rcp_r(float x) { return __frcp_rn(x); }
 __device__ __forceinline__ double rcp_r(double x) { return 1.0 / x; }
 
-// Two-float (hi, lo) reduction over the TPA lanes of a group: TwoSum at every butterfly level.
-template <class R, int TPA>
-__device__ __forceinline__ Acc<R> group_sum(Acc<R> a, unsigned gmask) {
-#pragma unroll
-  for (int o = TPA / 2; o > 0; o >>= 1) {
-    Acc<R> b;
-    b.hi = __shfl_xor_sync(gmask, a.hi, o);
-    if constexpr (sizeof(R) == 4) b.lo = __shfl_xor_sync(gmask, a.lo, o);
-    a.add(b.hi);
-    if constexpr (sizeof(R) == 4) a.lo = add_rn(a.lo, b.lo);
-  }
-  return a;
-}
-template <class R, int TPA>
-__device__ __forceinline__ R group_sum_plain(R v, unsigned gmask) {
-#pragma unroll
-  for (int o = TPA / 2; o > 0; o >>= 1) v += __shfl_xor_sync(gmask, v, o);
-  return v;
-}
-
-// Near force of one slot, TPA lanes per slot, each taking every TPA-th entry of the slot's list
-// row.  Pair physics: ComputeNearForceVerletWorklet / ComputeLJForceVerletWorklet
+// Near force of one slot per thread over its transposed list row (nbr[p * stride + slot]).
+// Pair physics: ComputeNearForceVerletWorklet / ComputeLJForceVerletWorklet
 // (rbmd/framework/run/worklet/RunWorklet.cpp:170-303) with ComputeLJForce and
 // ComputeNearEnergyForce (rbmd/framework/forceFunction/ExecForceFunction.h:74-140):
 //   LJ on MinDistanceVec(p_j', p_i) skipped within a molecule; Coulomb on p_j' - p_i for
 //   0.01 < d < rc with G = erfc(sqrt(a) d)/d^2 + 2 sqrt(a) e^{-a d^2}/(sqrt(pi) d); pairs with
-//   q_i q_j = 0 skip the Coulomb term (an uncharged slot skips it for all its lanes).
-// Per-type LJ coefficients are staged in shared memory.  Accumulation: each lane folds groups
-// of four pair forces (FP32 sums) into a two-float accumulator; the lanes' accumulators are
-// combined by a TwoSum butterfly.
-template <class R, int TPA, bool COUL, int MI>
-__global__ void __launch_bounds__(128) k_near_force(
+//   q_i q_j = 0 skip the Coulomb term.  Under list reuse (MI == kMiAll, list built at rc + skin)
+//   a pair also has to pass the list predicate at rc (rc^2 - d^2 > 1e-4 && d^2 > 1e-4), as the
+//   reference's per-call list would.
+// Per-type LJ coefficients are staged in shared memory.  The loop is software-pipelined: the
+// list entry two iterations ahead and the neighbour position one iteration ahead are in flight
+// while the current pair is evaluated.  Accumulation: groups of four pair forces are summed in
+// FP32 and folded into a two-float (TwoSum) per-atom accumulator.
+template <class R, bool COUL, int MI>
+__global__ void __launch_bounds__(256) k_near_force(
     NearParams prm, const LJTable* __restrict__ ljt, const typename Traits<R>::V4* __restrict__ pos4,
     const int2* __restrict__ meta, const int* __restrict__ nbr, const int* __restrict__ count,
     const RepDev* __restrict__ reps, const int* __restrict__ rep_of_slot,
     const int* __restrict__ slot_atom, double* __restrict__ force,
     double* __restrict__ energy_slot, uint32_t* status) {
+  using V4 = typename Traits<R>::V4;
   __shared__ R lj_a[kMaxReplicaTypes * kMaxReplicaTypes], lj_s6[kMaxReplicaTypes * kMaxReplicaTypes];
   const int nt2 = prm.ntypes * prm.ntypes;
   for (int t = threadIdx.x; t < nt2; t += blockDim.x) {
@@ -175,18 +159,14 @@ __global__ void __launch_bounds__(128) k_near_force(
     lj_s6[t] = sig6<R>(*ljt, t);
   }
   __syncthreads();
-  constexpr bool LJ = true;
   const bool MOLEC = prm.molecular != 0;
   const bool ENERGY = energy_slot != nullptr;
-  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = gt / TPA, sub = gt % TPA;
-  if (i >= prm.n) return;   // all lanes of a slot leave together
-  const int lane = threadIdx.x & 31;
-  const unsigned gmask = (TPA == 32 ? 0xffffffffu : ((1u << TPA) - 1u)) << (lane - sub);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= prm.n) return;
   const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
-  const typename Traits<R>::V4 pi = pos4[i];
+  const V4 pi = pos4[i];
   const bool typed = MOLEC || prm.ntypes > 1;
-  const int2 mi = (LJ && typed) ? meta[i] : make_int2(0, 0);
+  const int2 mi = typed ? meta[i] : make_int2(0, 0);
   const R rc = (R)prm.rc;
   const R cut2 = rc * rc;
   const R box[3] = {Traits<R>::box(rp, 0), Traits<R>::box(rp, 1), Traits<R>::box(rp, 2)};
@@ -195,16 +175,23 @@ __global__ void __launch_bounds__(128) k_near_force(
   const R cs = (R)prm.coul_scale;
   const R qi = pi.w;
   const int trow = mi.x * prm.ntypes;
-  const int* row = nbr + (size_t)i * prm.cap;
+  const int* col = nbr + i;
+  const size_t st = (size_t)prm.stride;
   Acc<R> fx, fy, fz;
   R gx = 0, gy = 0, gz = 0;   // FP32 group sum folded into the accumulators every 4 pairs
   R e_lj = 0, e_coul = 0;
   const int cnt = min(count[i], prm.cap);   // an overflowed row is redone after regrowth
-  int k = 0;
-  for (int p = sub; p < cnt; p += TPA, ++k) {
-    const int e = __ldg(row + p);
-    const int j = e >> kShiftBits;
-    const typename Traits<R>::V4 pj = pos4[j];
+  // pipeline prologue
+  int e_cur = cnt > 0 ? __ldg(col) : 0;
+  int e_nxt = cnt > 1 ? __ldg(col + st) : 0;
+  V4 pj_cur = pos4[cnt > 0 ? (e_cur >> kShiftBits) : i];
+  for (int p = 0; p < cnt; ++p) {
+    const int e = e_cur;
+    const V4 pj = pj_cur;
+    // issue the loads of the next iterations before the arithmetic of this one
+    e_cur = e_nxt;
+    if (p + 1 < cnt) pj_cur = pos4[e_cur >> kShiftBits];
+    if (p + 2 < cnt) e_nxt = __ldg(col + (size_t)(p + 2) * st);
     R px = pj.x, py = pj.y, pz = pj.z;
     if (e & 63) {   // periodic image: p_j - offset (PeriodicCoordOffset)
       const int c0 = e & 3, c1 = (e >> 2) & 3, c2b = (e >> 4) & 3;
@@ -215,6 +202,7 @@ __global__ void __launch_bounds__(128) k_near_force(
     R r0 = px - pi.x, r1 = py - pi.y, r2 = pz - pi.z;
     if (MI == kMiAll) nearest_image(r0, r1, r2, box);
     const R d2 = r0 * r0 + r1 * r1 + r2 * r2;
+    if (MI == kMiAll && !(cut2 - d2 > (R)1.0e-4 && d2 > (R)1.0e-4)) continue;
     R f = 0;
     if (COUL) {
       const R qq = qi * pj.w;
@@ -231,49 +219,39 @@ __global__ void __launch_bounds__(128) k_near_force(
       }
     }
     R fl0 = 0, fl1 = 0, fl2 = 0;
-    if (LJ) {
-      bool same = false;
-      int tj = 0;
-      if (typed) {
-        const int2 mj = meta[j];
-        same = MOLEC && (mj.y == mi.y);
-        tj = mj.x;
+    bool same = false;
+    int tj = 0;
+    if (typed) {
+      const int2 mj = meta[e >> kShiftBits];
+      same = MOLEC && (mj.y == mi.y);
+      tj = mj.x;
+    }
+    if (!same) {
+      R q0 = r0, q1 = r1, q2 = r2;   // MinDistanceVec(p_j', p_i)
+      R dl2 = d2;
+      if (MI == kMiLJ) {
+        min_image(q0, q1, q2, box);
+        dl2 = q0 * q0 + q1 * q1 + q2 * q2;
       }
-      if (!same) {
-        R q0 = r0, q1 = r1, q2 = r2;   // MinDistanceVec(p_j', p_i)
-        R dl2 = d2;
-        if (MI == kMiLJ) {
-          min_image(q0, q1, q2, box);
-          dl2 = q0 * q0 + q1 * q1 + q2 * q2;
-        }
-        if (dl2 < cut2 && dl2 > (R)0.0001) {
-          const R inv2 = rcp_r(dl2);
-          const R sd6 = lj_s6[trow + tj] * inv2 * inv2 * inv2;
-          const R a24 = lj_a[trow + tj];
-          const R scal = a24 * (((R)2 * sd6 - (R)1) * sd6) * inv2;
-          fl0 = scal * q0; fl1 = scal * q1; fl2 = scal * q2;
-          // 4 eps (s6 - 1) s6 with 4 eps = -lj24/6
-          if (ENERGY) e_lj += -a24 / (R)6 * (sd6 - (R)1) * sd6;
-        }
+      if (dl2 < cut2 && dl2 > (R)0.0001) {
+        const R inv2 = rcp_r(dl2);
+        const R sd6 = lj_s6[trow + tj] * inv2 * inv2 * inv2;
+        const R a24 = lj_a[trow + tj];
+        const R scal = a24 * (((R)2 * sd6 - (R)1) * sd6) * inv2;
+        fl0 = scal * q0; fl1 = scal * q1; fl2 = scal * q2;
+        // 4 eps (s6 - 1) s6 with 4 eps = -lj24/6
+        if (ENERGY) e_lj += -a24 / (R)6 * (sd6 - (R)1) * sd6;
       }
     }
     gx += f * r0 + fl0;
     gy += f * r1 + fl1;
     gz += f * r2 + fl2;
-    if ((k & 3) == 3) {
+    if ((p & 3) == 3) {
       fx.add(gx); fy.add(gy); fz.add(gz);
       gx = gy = gz = 0;
     }
   }
   fx.add(gx); fy.add(gy); fz.add(gz);
-  fx = group_sum<R, TPA>(fx, gmask);
-  fy = group_sum<R, TPA>(fy, gmask);
-  fz = group_sum<R, TPA>(fz, gmask);
-  if (ENERGY) {
-    e_lj = group_sum_plain<R, TPA>(e_lj, gmask);
-    e_coul = group_sum_plain<R, TPA>(e_coul, gmask);
-  }
-  if (sub != 0) return;
   const double F[3] = {fx.value(), fy.value(), fz.value()};
   if (!isfinite(F[0]) || !isfinite(F[1]) || !isfinite(F[2])) set_flag(status, kFlagNonFinite);
   const int id = slot_atom[i];
@@ -581,29 +559,25 @@ struct EamDev {
   float rhomax;
 };
 
-template <class R, int TPA>
-__global__ void __launch_bounds__(128) k_eam_fp(int n, int cap, double rc, EamDev eam,
+template <class R>
+__global__ void __launch_bounds__(128) k_eam_fp(int n, int stride, int cap, double rc, EamDev eam,
                                                 const typename Traits<R>::V4* __restrict__ pos4,
                                                 const int* __restrict__ nbr, const int* __restrict__ count,
                                                 const RepDev* __restrict__ reps,
                                                 const int* __restrict__ rep_of_slot, R* __restrict__ fp,
                                                 double* __restrict__ embed_slot) {
-  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = gt / TPA, sub = gt % TPA;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const int lane = threadIdx.x & 31;
-  const unsigned gmask = (TPA == 32 ? 0xffffffffu : ((1u << TPA) - 1u)) << (lane - sub);
   const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
   const typename Traits<R>::V4 pi = pos4[i];
   const R wrap[3] = {Traits<R>::wrap(rp, 0), Traits<R>::wrap(rp, 1), Traits<R>::wrap(rp, 2)};
   const R box[3] = {Traits<R>::box(rp, 0), Traits<R>::box(rp, 1), Traits<R>::box(rp, 2)};
   const R cut2 = (R)rc * (R)rc;
   const R rdr = sizeof(R) == 4 ? (R)eam.rdr : (R)eam.rdr_d;
-  const int* row = nbr + (size_t)i * cap;
   Acc<R> rho;
   const int cnt = min(count[i], cap);
-  for (int p = sub; p < cnt; p += TPA) {
-    const int e = __ldg(row + p);
+  for (int p = 0; p < cnt; ++p) {
+    const int e = __ldg(nbr + (size_t)p * stride + i);
     const int j = e >> kShiftBits;
     const typename Traits<R>::V4 pj = pos4[j];
     R r[3];
@@ -628,8 +602,6 @@ __global__ void __launch_bounds__(128) k_eam_fp(int n, int cap, double rc, EamDe
       rho.add((((R)b.w * pp + (R)c.x) * pp + (R)c.y) * pp + (R)c.z);
     }
   }
-  rho = group_sum<R, TPA>(rho, gmask);
-  if (sub != 0) return;
   const R rr = (R)rho.value();
   R pp = rr * (sizeof(R) == 4 ? (R)eam.rdrho : (R)eam.rdrho_d) + (R)1;
   int m = (int)pp;
@@ -646,8 +618,8 @@ __global__ void __launch_bounds__(128) k_eam_fp(int n, int cap, double rc, EamDe
   }
 }
 
-template <class R, int TPA>
-__global__ void __launch_bounds__(128) k_eam_force(int n, int cap, double rc, EamDev eam,
+template <class R>
+__global__ void __launch_bounds__(128) k_eam_force(int n, int stride, int cap, double rc, EamDev eam,
                                                    const typename Traits<R>::V4* __restrict__ pos4,
                                                    const int* __restrict__ nbr, const int* __restrict__ count,
                                                    const RepDev* __restrict__ reps,
@@ -655,11 +627,8 @@ __global__ void __launch_bounds__(128) k_eam_force(int n, int cap, double rc, Ea
                                                    const R* __restrict__ fp, const int* __restrict__ slot_atom,
                                                    double* __restrict__ force, double* __restrict__ pair_slot,
                                                    uint32_t* status) {
-  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = gt / TPA, sub = gt % TPA;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const int lane = threadIdx.x & 31;
-  const unsigned gmask = (TPA == 32 ? 0xffffffffu : ((1u << TPA) - 1u)) << (lane - sub);
   const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
   const typename Traits<R>::V4 pi = pos4[i];
   const R wrap[3] = {Traits<R>::wrap(rp, 0), Traits<R>::wrap(rp, 1), Traits<R>::wrap(rp, 2)};
@@ -667,12 +636,11 @@ __global__ void __launch_bounds__(128) k_eam_force(int n, int cap, double rc, Ea
   const R cut2 = (R)rc * (R)rc;
   const R rdr = sizeof(R) == 4 ? (R)eam.rdr : (R)eam.rdr_d;
   const R fpi = fp[i];
-  const int* row = nbr + (size_t)i * cap;
   Acc<R> fx, fy, fz;
   R epair = 0;
   const int cnt = min(count[i], cap);
-  for (int p = sub; p < cnt; p += TPA) {
-    const int e = __ldg(row + p);
+  for (int p = 0; p < cnt; ++p) {
+    const int e = __ldg(nbr + (size_t)p * stride + i);
     const int j = e >> kShiftBits;
     const typename Traits<R>::V4 pj = pos4[j];
     R r[3];
@@ -710,11 +678,6 @@ __global__ void __launch_bounds__(128) k_eam_force(int n, int cap, double rc, Ea
       epair += phi;
     }
   }
-  fx = group_sum<R, TPA>(fx, gmask);
-  fy = group_sum<R, TPA>(fy, gmask);
-  fz = group_sum<R, TPA>(fz, gmask);
-  epair = group_sum_plain<R, TPA>(epair, gmask);
-  if (sub != 0) return;
   const double F[3] = {fx.value(), fy.value(), fz.value()};
   if (!isfinite(F[0]) || !isfinite(F[1]) || !isfinite(F[2])) set_flag(status, kFlagNonFinite);
   const int id = slot_atom[i];

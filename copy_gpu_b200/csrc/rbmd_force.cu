@@ -85,8 +85,8 @@ struct rbmd_force {
   double shake_tol = 1e-5;
   int energy_every = 0;   // energies inside step(): every outputs.thermo_out.interval steps
   int cap_override = 0;   // neighbor.capacity: initial list capacity (grown on overflow)
-  int tpa_list = 8, tpa_near = 8;   // lanes per atom of the list build / force pass
-  bool autotune = false;            // "autotune": true tunes them at the first compute
+  int tpa_list = 128, tpa_near = 128;   // threads per block of the list build / force pass
+  bool autotune = false;                // "autotune": true tunes them at the first compute
   bool tuned = false;
   int shake_max_iter = 5000;
   std::string potential_file;
@@ -320,24 +320,14 @@ double rbe_S(double alpha, const double* L) {
   return H[0] * H[1] * H[2] - 1.0;
 }
 
-template <class R, int TPA>
-void launch_nlist_t(rbmd_force* f, cudaStream_t s) {
-  const long long threads = (long long)f->n * TPA;
-  k_nlist<R, TPA><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(
-      f->n, (const typename Traits<R>::V4*)f->d_pos4, f->d_cell_start, f->d_reps,
-      f->nrep > 1 ? f->d_rep_of : nullptr, f->num_cycles, (R)f->list_cut(), f->cap, f->d_nbr,
-      f->d_count, f->d_maxcount, f->d_status, f->skin > 0 ? f->d_rebuild : nullptr, f->d_nbuilds);
-}
-
 template <class R>
 void launch_nlist(rbmd_force* f, cudaStream_t s) {
   PhaseScope ps(f, kPhList, s);
-  switch (f->tpa_list) {
-    case 4: launch_nlist_t<R, 4>(f, s); break;
-    case 16: launch_nlist_t<R, 16>(f, s); break;
-    case 32: launch_nlist_t<R, 32>(f, s); break;
-    default: launch_nlist_t<R, 8>(f, s); break;
-  }
+  const int bs = f->tpa_list;
+  k_nlist<R><<<(f->n + bs - 1) / bs, bs, 0, s>>>(
+      f->n, (const typename Traits<R>::V4*)f->d_pos4, f->d_cell_start, f->d_reps,
+      f->nrep > 1 ? f->d_rep_of : nullptr, f->num_cycles, (R)f->list_cut(), f->cap, f->stride, f->d_nbr,
+      f->d_count, f->d_maxcount, f->d_status, f->skin > 0 ? f->d_rebuild : nullptr, f->d_nbuilds);
   f->launches++;
 }
 
@@ -408,7 +398,7 @@ void launch_kspace(rbmd_force* f, cudaStream_t s, cudaEvent_t ready) {
   f->launches += 4;
 }
 
-template <class R, int TPA, bool COUL, int MI>
+template <class R, bool COUL, int MI>
 void launch_near_t(rbmd_force* f, cudaStream_t s) {
   NearParams p;
   p.n = f->n;
@@ -424,36 +414,26 @@ void launch_near_t(rbmd_force* f, cudaStream_t s) {
   p.sqrt_alpha = std::sqrt(f->alpha);
   p.two_sqrt_alpha_over_sqrt_pi = 2.0 * std::sqrt(f->alpha) / std::sqrt(M_PI);
   p.kstage = 0;
-  const long long threads = (long long)f->n * TPA;
-  k_near_force<R, TPA, COUL, MI><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(
+  const int bs = f->tpa_near;
+  k_near_force<R, COUL, MI><<<(f->n + bs - 1) / bs, bs, 0, s>>>(
       p, f->d_ljt, (const typename Traits<R>::V4*)f->d_pos4, f->d_meta, f->d_nbr, f->d_count,
       f->d_reps, f->nrep > 1 ? f->d_rep_of : nullptr, f->d_slot_atom, f->at.force,
       f->want_energy ? f->d_eslot : nullptr, f->d_status);
   f->launches++;
 }
 
-template <class R, int TPA, bool COUL>
+template <class R, bool COUL>
 void launch_near_m(rbmd_force* f, cudaStream_t s) {
   const int mi = f->skin > 0 ? kMiAll : (f->minimg ? kMiLJ : kMiNone);
-  if (mi == kMiAll) launch_near_t<R, TPA, COUL, kMiAll>(f, s);
-  else if (mi == kMiLJ) launch_near_t<R, TPA, COUL, kMiLJ>(f, s);
-  else launch_near_t<R, TPA, COUL, kMiNone>(f, s);
-}
-
-template <class R, int TPA>
-void launch_near_c(rbmd_force* f, cudaStream_t s) {
-  if (f->with_coul_near()) launch_near_m<R, TPA, true>(f, s);
-  else launch_near_m<R, TPA, false>(f, s);
+  if (mi == kMiAll) launch_near_t<R, COUL, kMiAll>(f, s);
+  else if (mi == kMiLJ) launch_near_t<R, COUL, kMiLJ>(f, s);
+  else launch_near_t<R, COUL, kMiNone>(f, s);
 }
 
 template <class R>
 void launch_near(rbmd_force* f, cudaStream_t s) {
-  switch (f->tpa_near) {
-    case 4: launch_near_c<R, 4>(f, s); break;
-    case 16: launch_near_c<R, 16>(f, s); break;
-    case 32: launch_near_c<R, 32>(f, s); break;
-    default: launch_near_c<R, 8>(f, s); break;
-  }
+  if (f->with_coul_near()) launch_near_m<R, true>(f, s);
+  else launch_near_m<R, false>(f, s);
 }
 
 template <class R>
@@ -470,21 +450,13 @@ void launch_eam(rbmd_force* f, cudaStream_t s) {
   e.rdrho_d = 1.0 / (double)f->eam_h.drho;
   e.rhomax = f->eam_h.rhomax;
   const int* rp = f->nrep > 1 ? f->d_rep_of : nullptr;
-  auto go = [&](auto tpa_tag) {
-    constexpr int TPA = decltype(tpa_tag)::value;
-    const unsigned nb = (unsigned)(((long long)f->n * TPA + 127) / 128);
-    k_eam_fp<R, TPA><<<nb, 128, 0, s>>>(f->n, f->cap, f->rc, e, (const typename Traits<R>::V4*)f->d_pos4,
-                                        f->d_nbr, f->d_count, f->d_reps, rp, (R*)f->d_fp, f->d_emb);
-    k_eam_force<R, TPA><<<nb, 128, 0, s>>>(f->n, f->cap, f->rc, e, (const typename Traits<R>::V4*)f->d_pos4,
-                                           f->d_nbr, f->d_count, f->d_reps, rp, (const R*)f->d_fp,
-                                           f->d_slot_atom, f->at.force, f->d_epair, f->d_status);
-  };
-  switch (f->tpa_near) {
-    case 4: go(std::integral_constant<int, 4>{}); break;
-    case 16: go(std::integral_constant<int, 16>{}); break;
-    case 32: go(std::integral_constant<int, 32>{}); break;
-    default: go(std::integral_constant<int, 8>{}); break;
-  }
+  const int bs = 128;
+  const int nb = (f->n + bs - 1) / bs;
+  k_eam_fp<R><<<nb, bs, 0, s>>>(f->n, f->stride, f->cap, f->rc, e, (const typename Traits<R>::V4*)f->d_pos4,
+                                 f->d_nbr, f->d_count, f->d_reps, rp, (R*)f->d_fp, f->d_emb);
+  k_eam_force<R><<<nb, bs, 0, s>>>(f->n, f->stride, f->cap, f->rc, e, (const typename Traits<R>::V4*)f->d_pos4,
+                                    f->d_nbr, f->d_count, f->d_reps, rp, (const R*)f->d_fp, f->d_slot_atom,
+                                    f->at.force, f->d_epair, f->d_status);
   f->launches += 2;
 }
 
@@ -550,7 +522,7 @@ void launch_compute_any(rbmd_force* f, cudaStream_t s) {
 rbmd_status grow_list(rbmd_force* f, int need) {
   const int newcap = ((int)(need * 1.2) + 8 + 7) & ~7;
   dfree(f->d_nbr);
-  CK(dalloc(&f->d_nbr, (size_t)newcap * f->n));
+  CK(dalloc(&f->d_nbr, (size_t)newcap * f->stride));
   f->cap = newcap;
   return RBMD_OK;
 }
@@ -678,8 +650,8 @@ rbmd_status parse_config(rbmd_force* f, const char* text) {
   {
     const Value* at = root.path("autotune");
     if (at && at->kind == Value::Bool) f->autotune = at->b;
-    const int tl = (int)num(root, "tuning.list_lanes", 0.0), tn = (int)num(root, "tuning.force_lanes", 0.0);
-    auto ok = [](int t) { return t == 4 || t == 8 || t == 16 || t == 32; };
+    const int tl = (int)num(root, "tuning.list_block", 0.0), tn = (int)num(root, "tuning.force_block", 0.0);
+    auto ok = [](int t) { return t == 64 || t == 128 || t == 256; };
     if (ok(tl)) { f->tpa_list = tl; f->autotune = false; }
     if (ok(tn)) { f->tpa_near = tn; f->autotune = false; }
   }
@@ -785,8 +757,9 @@ rbmd_status upload_ksamples(rbmd_force* f, const int32_t* m_xyz) {
   return RBMD_OK;
 }
 
-// Own autotuner: times every lane count of the list build and of the force pass (3 launches
-// each, best taken) on the bound system and keeps the fastest.
+// Own autotuner: times every threads-per-block choice of the list build and of the force pass
+// (three timed launches each after a warm-up, best taken) on the bound system and keeps the
+// fastest.
 template <class R>
 rbmd_status autotune_impl(rbmd_force* f, cudaStream_t s) {
   cudaEvent_t a, b;
@@ -794,7 +767,7 @@ rbmd_status autotune_impl(rbmd_force* f, cudaStream_t s) {
   CK(cudaEventCreate(&b));
   const bool prof = f->prof_on;
   f->prof_on = false;
-  const int cand[4] = {4, 8, 16, 32};
+  const int cand[3] = {64, 128, 256};
   auto best_of = [&](auto launch) -> float {
     float best = 1e30f;
     for (int rep = 0; rep < 4; ++rep) {
@@ -982,7 +955,7 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
   CK(dalloc(&f->d_atom_slot, n));
   CK(cudaMalloc(&f->d_pos4, n * (fp64 ? sizeof(double4) : sizeof(float4))));
   CK(dalloc(&f->d_meta, n));
-  CK(dalloc(&f->d_nbr, (size_t)f->cap * f->n));
+  CK(dalloc(&f->d_nbr, (size_t)f->cap * f->stride));
   CK(dalloc(&f->d_count, n));
   CK(dalloc(&f->d_maxcount, 1));
   CK(dalloc(&f->d_nbuilds, 1));
@@ -1435,7 +1408,7 @@ rbmd_status rbmd_force_get_neighbors(rbmd_force* f, int32_t* counts, int32_t* id
   if (!f->bound) return RBMD_ERR_STATE;
   CK(cudaDeviceSynchronize());
   const size_t n = f->n;
-  std::vector<int> cnt(n), slot_atom(n), nbr((size_t)f->cap * n);
+  std::vector<int> cnt(n), slot_atom(n), nbr((size_t)f->cap * f->stride);
   CK(cudaMemcpy(cnt.data(), f->d_count, sizeof(int) * n, cudaMemcpyDeviceToHost));
   CK(cudaMemcpy(slot_atom.data(), f->d_slot_atom, sizeof(int) * n, cudaMemcpyDeviceToHost));
   CK(cudaMemcpy(nbr.data(), f->d_nbr, sizeof(int) * nbr.size(), cudaMemcpyDeviceToHost));
@@ -1446,7 +1419,7 @@ rbmd_status rbmd_force_get_neighbors(rbmd_force* f, int32_t* counts, int32_t* id
     const int m = std::min<int>(cnt[i], f->cap);
     if (cnt[i] > cap) too_small = true;
     for (int p = 0; p < m && p < cap; ++p)
-      ids[(size_t)id * cap + p] = slot_atom[nbr[(size_t)i * f->cap + p] >> kShiftBits];
+      ids[(size_t)id * cap + p] = slot_atom[nbr[(size_t)p * f->stride + i] >> kShiftBits];
   }
   return too_small ? RBMD_ERR_ARG : RBMD_OK;
 }

@@ -145,13 +145,13 @@ RBMD_API rbmd_status rbmd_force_sample_k(rbmd_force* f, int64_t step, int32_t* m
  * (rbmd/framework/run/ExecutionNVT.cpp:179-222). */
 RBMD_API rbmd_status rbmd_force_compute(rbmd_force* f, void* stream);
 
-/* Time every lanes-per-atom choice (4, 8, 16, 32) of the neighbour-list build and of the
+/* Time every threads-per-block choice (64, 128, 256) of the neighbour-list build and of the
  * force pass on the bound system, keep the fastest, and leave the forces of that choice in
- * atoms->force.  Config "autotune": true runs it at the first compute; "tuning.list_lanes" /
- * "tuning.force_lanes" fix the choices instead (default 8 / 8: runs are bit-reproducible for a
- * fixed choice).  No reference counterpart. */
-RBMD_API rbmd_status rbmd_force_autotune(rbmd_force* f, void* stream, int32_t* list_lanes,
-                                         int32_t* force_lanes);
+ * atoms->force.  Config "autotune": true runs it at the first compute; "tuning.list_block" /
+ * "tuning.force_block" fix the choices instead (default 128 / 128).  Results do not depend on
+ * the choice (one thread per atom, same summation order).  No reference counterpart. */
+RBMD_API rbmd_status rbmd_force_autotune(rbmd_force* f, void* stream, int32_t* list_block,
+                                         int32_t* force_block);
 
 /* Same as rbmd_force_compute with HOST positions in and HOST forces out (n_atoms*3 doubles
  * each); copies are issued on `stream` and the call returns after the force copy landed.

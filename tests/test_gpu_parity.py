@@ -23,13 +23,13 @@ def _posr(pos, prec):
     return pos.astype(np.float32) if prec == "fp32" else pos.astype(np.float64)
 
 
-@pytest.mark.parametrize("prec,lanes", [("fp32", 8), ("fp64", 8), ("fp32", 4), ("fp32", 32), ("fp64", 16)])
-def test_lj_pairs_and_force(cuda, oracle_lib, prec, lanes):
+@pytest.mark.parametrize("prec,block", [("fp32", 128), ("fp64", 128), ("fp32", 64), ("fp32", 256)])
+def test_lj_pairs_and_force(cuda, oracle_lib, prec, block):
     import torch
     s = systems.lj_fcc(ncell=8, seed=2)
     s["pos"] = jitter(s["pos"], s["lo"], s["hi"], 0.08, seed=5)
     cfg = systems.lj_config(cutoff=2.5, precision=prec)
-    cfg["tuning"] = {"list_lanes": lanes, "force_lanes": lanes}
+    cfg["tuning"] = {"list_block": block, "force_block": block}
     dev = to_dev(s, cuda)
     ff = make_ff(cfg, s, dev)
     ff.Execute()
@@ -149,7 +149,7 @@ def test_autotune_keeps_parity(cuda, oracle_lib):
     ff = make_ff(cfg, s, dev)
     ff.set_ksamples(m)
     tl, tn = ff.autotune()
-    assert tl in (4, 8, 16, 32) and tn in (4, 8, 16, 32)
+    assert tl in (64, 128, 256) and tn in (64, 128, 256)
     torch.cuda.synchronize()
     pr = _posr(s["pos"], "fp32")
     nl = oracle_lib.neighbors(pr, s["lo"], s["hi"], 2.5, "fp32")
