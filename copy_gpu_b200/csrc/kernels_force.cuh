@@ -122,13 +122,18 @@ __device__ __forceinline__ void min_image(R& q0, R& q1, R& q2, const R* box) {
 // Nearest image for list reuse: the two atoms of a listed pair may each have wrapped across a
 // face since the build, so the stored vector can be off by up to two box lengths.
 template <class R>
-__device__ __forceinline__ void nearest_image(R& q0, R& q1, R& q2, const R* box) {
-  q0 -= box[0] * rint(q0 / box[0]);
-  q1 -= box[1] * rint(q1 / box[1]);
-  q2 -= box[2] * rint(q2 / box[2]);
+__device__ __forceinline__ void nearest_image(R& q0, R& q1, R& q2, const R* box, const R* ibox) {
+  q0 -= box[0] * rint(q0 * ibox[0]);
+  q1 -= box[1] * rint(q1 * ibox[1]);
+  q2 -= box[2] * rint(q2 * ibox[2]);
 }
 
-__device__ __forceinline__ float rcp_r(float x) { return __frcp_rn(x); }
+// approximate reciprocal (one MUFU op, about 1 ulp): the pair terms carry a 1e-5 budget
+__device__ __forceinline__ float rcp_r(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
 __device__ __forceinline__ double rcp_r(double x) { return 1.0 / x; }
 
 // Near force of one slot per thread over its transposed list row (nbr[p * stride + slot]).
@@ -171,6 +176,7 @@ __global__ void __launch_bounds__(256) k_near_force(
   const R cut2 = rc * rc;
   const R box[3] = {Traits<R>::box(rp, 0), Traits<R>::box(rp, 1), Traits<R>::box(rp, 2)};
   const R wrap[3] = {Traits<R>::wrap(rp, 0), Traits<R>::wrap(rp, 1), Traits<R>::wrap(rp, 2)};
+  const R ibox[3] = {(R)1 / box[0], (R)1 / box[1], (R)1 / box[2]};
   const R sa = (R)prm.sqrt_alpha, aa = (R)prm.alpha, c2 = (R)prm.two_sqrt_alpha_over_sqrt_pi;
   const R cs = (R)prm.coul_scale;
   const R qi = pi.w;
@@ -200,7 +206,7 @@ __global__ void __launch_bounds__(256) k_near_force(
       pz = pz - (c2b == 1 ? wrap[2] : (c2b == 2 ? -wrap[2] : (R)0));
     }
     R r0 = px - pi.x, r1 = py - pi.y, r2 = pz - pi.z;
-    if (MI == kMiAll) nearest_image(r0, r1, r2, box);
+    if (MI == kMiAll) nearest_image(r0, r1, r2, box, ibox);
     const R d2 = r0 * r0 + r1 * r1 + r2 * r2;
     if (MI == kMiAll && !(cut2 - d2 > (R)1.0e-4 && d2 > (R)1.0e-4)) continue;
     R f = 0;

@@ -72,6 +72,24 @@ __global__ void k_kick_drift(MdParams mp, double* __restrict__ pos, double* __re
   atomicAdd(&cell_count[c], 1);
 }
 
+// Verlet-skin check for a force call on externally supplied positions: flag a list rebuild when
+// any atom moved more than skin/2 (nearest image) from its position at the last build.
+__global__ void k_skin_check(int n, const double* __restrict__ pos, const double* __restrict__ xref,
+                             const int* __restrict__ rep_of, const RepDev* __restrict__ reps,
+                             double half_skin2, int* __restrict__ rebuild) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const RepDev& rp = reps[rep_of ? rep_of[i] : 0];
+  double d2 = 0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double dd = pos[3 * i + d] - xref[3 * i + d];
+    dd -= rp.box_d[d] * rint(dd / rp.box_d[d]);
+    d2 += dd * dd;
+  }
+  if (!(d2 <= half_skin2) && *rebuild == 0) atomicExch(rebuild, 1);
+}
+
 // Chunk of atoms inside one replica (kinetic-energy partials, ordered per replica).
 struct MdChunk { int begin, end, rep, pad; };
 

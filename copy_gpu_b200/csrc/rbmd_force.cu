@@ -88,6 +88,7 @@ struct rbmd_force {
   int tpa_list = 128, tpa_near = 128;   // threads per block of the list build / force pass
   bool autotune = false;                // "autotune": true tunes them at the first compute
   bool tuned = false;
+  bool list_valid = false;   // a list (and x_ref) exists from an earlier build
   int shake_max_iter = 5000;
   std::string potential_file;
 
@@ -510,8 +511,18 @@ template <class R>
 void launch_compute(rbmd_force* f, cudaStream_t s) {
   f->want_energy = true;
   cudaMemsetAsync(f->d_maxcount, 0, sizeof(int), s);
-  if (f->d_rebuild) cudaMemsetAsync(f->d_rebuild, 1, sizeof(int), s);   // nonzero: rebuild
+  if (f->skin > 0 && f->list_valid) {
+    // reuse the list when no atom moved more than skin/2 since it was built
+    cudaMemsetAsync(f->d_rebuild, 0, sizeof(int), s);
+    k_skin_check<<<(f->n + 255) / 256, 256, 0, s>>>(f->n, f->at.pos, f->d_xref,
+                                                    f->nrep > 1 ? f->d_rep_of : nullptr, f->d_reps,
+                                                    0.25 * f->skin * f->skin, f->d_rebuild);
+    f->launches++;
+  } else if (f->d_rebuild) {
+    cudaMemsetAsync(f->d_rebuild, 1, sizeof(int), s);   // nonzero: rebuild
+  }
   launch_force_tail<R>(f, s, true);
+  f->list_valid = true;
 }
 
 void launch_compute_any(rbmd_force* f, cudaStream_t s) {
@@ -535,6 +546,7 @@ rbmd_status check_overflow(rbmd_force* f, cudaStream_t s, bool* redo) {
   CK(cudaStreamSynchronize(s));
   prof_collect(f);
   if (*f->h_status & kFlagListOverflow) {
+    f->list_valid = false;
     rbmd_status st = grow_list(f, *f->h_maxcount);
     if (st) return st;
     uint32_t clr = *f->h_status & ~kFlagListOverflow;
@@ -560,7 +572,8 @@ void launch_step(rbmd_force* f, cudaStream_t s) {
   f->want_energy = f->energy_every > 0 && ((f->step_count + 1) % f->energy_every == 0);
   cudaMemsetAsync(f->d_maxcount, 0, sizeof(int), s);
   cudaMemsetAsync(f->d_cell_count, 0, sizeof(int) * f->ncell_total, s);
-  if (f->skin > 0) cudaMemsetAsync(f->d_rebuild, 0, sizeof(int), s);
+  // with a skin the drift kernel decides; a missing or overflowed list forces a rebuild
+  if (f->skin > 0) cudaMemsetAsync(f->d_rebuild, f->list_valid ? 0 : 1, sizeof(int), s);
   // stages 1-2: kick, drift + wrap, bin (binning sees the unconstrained positions, as the
   // reference's locator.SetPosition runs before ConstraintA)
   {
@@ -589,6 +602,7 @@ void launch_step(rbmd_force* f, cudaStream_t s) {
   }
   // stage 3: force (cell sort of the pre-constraint binning, then list and forces)
   launch_force_tail<R>(f, s, false);
+  f->list_valid = true;
   // stage 3: kick (+ RATTLE), temperature, thermostat
   PhaseScope ps_int(f, kPhInt, s);
   if (shake) {
@@ -1200,6 +1214,7 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
     CK(dalloc(&f->d_eangle, (size_t)f->n_mol));
   }
   f->bound = true;
+  f->list_valid = false;
   f->step_count = 0;
   f->pending_scale = false;
   return RBMD_OK;
