@@ -21,6 +21,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "librbmd_b200.so")
 
 RBMD_OK = 0
+RBMD_ERR_ARG, RBMD_ERR_CONFIG, RBMD_ERR_CUDA, RBMD_ERR_STATE, RBMD_ERR_DEVICE, RBMD_ERR_FILE = 1, 2, 3, 4, 5, 6
 STATUS_NAMES = {1: "ERR_ARG", 2: "ERR_CONFIG", 3: "ERR_CUDA", 4: "ERR_STATE", 5: "ERR_DEVICE",
                 6: "ERR_FILE"}
 FLAG_LIST_OVERFLOW = 0x01
@@ -40,7 +41,7 @@ EXPORTED = [
     "rbmd_force_sync_velocities", "rbmd_force_energy", "rbmd_force_status",
     "rbmd_force_get_neighbors", "rbmd_force_get_rhok", "rbmd_force_profile",
     "rbmd_force_phase_ms", "rbmd_force_list_builds", "rbmd_force_launch_count",
-    "rbmd_force_destroy", "rbmd_version", "rbmd_last_error",
+    "rbmd_force_destroy", "rbmd_rhok_noalloc", "rbmd_version", "rbmd_last_error",
 ]
 
 
@@ -110,6 +111,7 @@ def library() -> ctypes.CDLL:
         "rbmd_force_list_builds": (I32, [V, P(I64)]),
         "rbmd_force_launch_count": (I32, [V, P(I32)]),
         "rbmd_force_destroy": (None, [V]),
+        "rbmd_rhok_noalloc": (I32, [V, V, I32, P(rbmd_box), V, I32, V, V]),
         "rbmd_version": (ctypes.c_char_p, []),
         "rbmd_last_error": (ctypes.c_char_p, []),
     }

@@ -35,6 +35,15 @@ constexpr int kStageBytes = 48 * 1024;   // shared memory for k staging in the f
 constexpr int kSamplerD = 640;   // pre-drawn proposals per axis in the sampler kernel (38 KB smem)
 constexpr int kMdChunk = 2048;   // atoms per kinetic-energy chunk
 
+}  // namespace
+
+namespace rbmd_internal {
+char g_last_error[512] = "";
+}
+using rbmd_internal::g_last_error;
+
+namespace {
+
 #define CK(x)                                                                            \
   do {                                                                                   \
     cudaError_t e_ = (x);                                                                \
@@ -44,8 +53,6 @@ constexpr int kMdChunk = 2048;   // atoms per kinetic-energy chunk
       return RBMD_ERR_CUDA;                                                              \
     }                                                                                    \
   } while (0)
-
-char g_last_error[512] = "";
 
 template <class T>
 cudaError_t dalloc(T** p, size_t count) {

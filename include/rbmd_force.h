@@ -205,6 +205,20 @@ RBMD_API rbmd_status rbmd_force_launch_count(rbmd_force* f, int32_t* kernels_per
 
 RBMD_API void rbmd_force_destroy(rbmd_force* f);
 
+/* Structure factors rho_k = sum_j q_j exp(i 2 pi m_k . (r_j - lo) / L) of n atoms in one box
+ * (device positions [n*3] and charges [n]) for P integer vectors m (device int32 [P*3]) into
+ * rho (device double [P*2], Re then Im), enqueued on `stream`, with no device allocation: the
+ * scratch lives in a static device array of the library (8 MiB per device, kept until exit).
+ * For callers that cannot allocate device memory at that point: an engine that owns all device
+ * memory through its own pool or a fixed budget, or a step loop that cannot take the device-wide
+ * synchronisation of cudaFree.  Limits: n <= 262144, P <= 1024, else
+ * RBMD_ERR_ARG.  All calls on a device share the array: calls that overlap on the GPU race.
+ * The first call on each device resolves the array's address and should precede any stream
+ * capture.  No counterpart in the reference. */
+RBMD_API rbmd_status rbmd_rhok_noalloc(const double* pos_dev, const double* charge_dev, int32_t n,
+                                       const rbmd_box* box, const int32_t* m_dev, int32_t P,
+                                       double* rho_dev, void* stream);
+
 /* Version string of the library build. */
 RBMD_API const char* rbmd_version(void);
 
