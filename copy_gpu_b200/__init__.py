@@ -39,7 +39,7 @@ EXPORTED = [
     "rbmd_force_set_kweights", "rbmd_force_get_ksamples", "rbmd_force_sample_k",
     "rbmd_force_compute", "rbmd_force_autotune", "rbmd_force_compute_host", "rbmd_force_step",
     "rbmd_force_sync_velocities", "rbmd_force_energy", "rbmd_force_status",
-    "rbmd_force_get_neighbors", "rbmd_force_get_rhok", "rbmd_force_profile",
+    "rbmd_force_get_neighbors", "rbmd_force_get_rbl", "rbmd_force_get_rhok", "rbmd_force_profile",
     "rbmd_force_phase_ms", "rbmd_force_list_builds", "rbmd_force_launch_count",
     "rbmd_force_destroy", "rbmd_rhok_noalloc", "rbmd_version", "rbmd_last_error",
 ]
@@ -105,6 +105,7 @@ def library() -> ctypes.CDLL:
         "rbmd_force_energy": (I32, [V, P(rbmd_energy), V]),
         "rbmd_force_status": (I32, [V, P(ctypes.c_uint32), I32, V]),
         "rbmd_force_get_neighbors": (I32, [V, P(I32), P(I32), I64]),
+        "rbmd_force_get_rbl": (I32, [V, P(I32), P(I32), P(I64)]),
         "rbmd_force_get_rhok": (I32, [V, P(D), I32]),
         "rbmd_force_profile": (I32, [V, I32]),
         "rbmd_force_phase_ms": (I32, [V, P(D), P(I64), I32]),
@@ -308,6 +309,17 @@ class ForceField:
         if st not in (RBMD_OK, 1):
             _check(st, "get_neighbors")
         return counts, ids
+
+    def rbl_lists(self):
+        """RBL counts per caller atom and the list sizes: (ncore, nshell, sizes) with sizes =
+        (rs_num, rc_num, pice_num, core_cap, shell_cap)."""
+        import numpy as np
+        ncore = np.zeros(self.n, dtype=np.int32)
+        nshell = np.zeros(self.n, dtype=np.int32)
+        sizes = np.zeros(5, dtype=np.int64)
+        _check(library().rbmd_force_get_rbl(self._h, _ptr(ncore, ctypes.c_int32), _ptr(nshell, ctypes.c_int32),
+                                            _ptr(sizes, ctypes.c_int64)), "get_rbl")
+        return ncore, nshell, tuple(int(v) for v in sizes)
 
     def energy(self, stream=None):
         e = rbmd_energy()

@@ -39,7 +39,7 @@ struct RepDev {
   double S;          // RBE normaliser prod_d H_d - 1
   double kT_target;  // thermostat target (kB * T0 units handled on host)
   int ndof_mode;     // unused on device
-  int pad;
+  int rbl_pice;      // RBL: every rbl_pice-th shell pair is kept and weighted by rbl_pice
 };
 
 template <class R> struct Traits;

@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(256) k_near_force(
   const R sa = (R)prm.sqrt_alpha, aa = (R)prm.alpha, c2 = (R)prm.two_sqrt_alpha_over_sqrt_pi;
   const R cs = (R)prm.coul_scale;
   const R qi = pi.w;
-  const int trow = mi.x * prm.ntypes;
+  const int trow = prm.ntypes > 1 ? mi.x * prm.ntypes : 0;   // one LJ type when all types agree
   const int* col = nbr + i;
   const size_t st = (size_t)prm.stride;
   Acc<R> fx, fy, fz;
@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(256) k_near_force(
     if (typed) {
       const int2 mj = meta[e >> kShiftBits];
       same = MOLEC && (mj.y == mi.y);
-      tj = mj.x;
+      tj = prm.ntypes > 1 ? mj.x : 0;
     }
     if (!same) {
       R q0 = r0, q1 = r1, q2 = r2;   // MinDistanceVec(p_j', p_i)
@@ -632,7 +632,7 @@ __global__ void __launch_bounds__(128) k_eam_force(int n, int stride, int cap, d
                                                    const int* __restrict__ rep_of_slot,
                                                    const R* __restrict__ fp, const int* __restrict__ slot_atom,
                                                    double* __restrict__ force, double* __restrict__ pair_slot,
-                                                   uint32_t* status) {
+                                                   uint32_t* status, int ref_sign) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
@@ -655,7 +655,10 @@ __global__ void __launch_bounds__(128) k_eam_force(int n, int stride, int cap, d
     for (int d = 0; d < 3; ++d) {
       const int cd = (e >> (2 * d)) & 3;
       const R off = cd == 1 ? wrap[d] : (cd == 2 ? -wrap[d] : (R)0);
-      R v = (pjv[d] - off) - piv[d];
+      // pair vector p_i - p_j' (the sign for which F = -grad E, as LAMMPS' pair_eam and the
+      // reference's RBL pass, RunWorklet.cpp:1180); ref_sign: the reference's Verlet pass uses
+      // MinDistanceVec(p_j, p_i) (RunWorklet.cpp:402), which reverses the force
+      R v = ref_sign ? (pjv[d] - off) - piv[d] : piv[d] - (pjv[d] - off);
       v -= box[d] * rint(v / box[d]);
       r[d] = v;
     }

@@ -1,0 +1,408 @@
+// kernels_rbl.cuh -- the RBL ("random batch list") near field of RBMD's default neighbor mode:
+// a core list inside r_core plus every pice-th shell pair in [r_core, rc) in the reference's
+// traversal order, the LJ / erfc-Coulomb and EAM passes over it with the shell terms scaled by
+// pice, and the removal of the mean near force.
+#pragma once
+
+#include "common.cuh"
+#include "kernels_cells.cuh"
+#include "kernels_force.cuh"
+#include "kernels_md.cuh"
+
+namespace rbmd {
+
+// RBL list of slot i: ComputeRBLNeighboursOnceWorklet (rbmd/framework/run/worklet/RunWorklet.cpp:
+// 634-708).  The stencil is walked as the reference walks it (x offset outermost, z innermost,
+// the points of a cell in slot order = ascending caller id), because which shell pairs are kept
+// depends on that order: a candidate with rc^2 - d^2 > 1e-4 && d^2 - rs^2 > 1e-4 is a shell pair
+// and is kept when its running shell index is a multiple of pice; otherwise a pair with
+// rs^2 - d^2 > 1e-4 && d^2 > 1e-4 is a core pair.  d^2 is formed with uncontracted ops on
+// (p_j - offset) - p_i, as in the full list.  Core entries fill rows [0, core_cap) of the
+// transposed list, kept shell entries rows [core_cap, core_cap + shell_cap).
+template <class R>
+__global__ void __launch_bounds__(128) k_rbl_list(
+    int n, const typename Traits<R>::V4* __restrict__ pos4, const int* __restrict__ cell_start,
+    const RepDev* __restrict__ reps, const int* __restrict__ rep_of_slot, int num_cycles, R rc, R rs,
+    int core_cap, int shell_cap, int stride, int* __restrict__ nbr, int* __restrict__ ncore,
+    int* __restrict__ nshell, int* __restrict__ max_count, uint32_t* status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
+  const int pice = rp.rbl_pice;
+  const typename Traits<R>::V4 pi = pos4[i];
+  const R pix[3] = {pi.x, pi.y, pi.z};
+  int ci[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    ci[d] = (int)div_rn(sub_rn(pix[d], Traits<R>::lo(rp, d)), Traits<R>::dx(rp, d));
+  const R rc2 = mul_rn(rc, rc), rs2 = mul_rn(rs, rs);
+  const int nc = num_cycles;
+  const int dx0 = rp.dims[0], dx1 = rp.dims[1], dx2 = rp.dims[2];
+  int n_core = 0, n_shell = 0, shell_index = 0;
+  for (int a = -nc; a <= nc; ++a) {
+    const int nbx = ci[0] + a;
+    const int wx = ((nbx % dx0) + dx0) % dx0;
+    const int ddx = wx - nbx;
+    const R off0 = mul_rn(Traits<R>::dx(rp, 0), (R)ddx);
+    const int cx = ddx > 0 ? 1 : (ddx < 0 ? 2 : 0);
+    for (int b = -nc; b <= nc; ++b) {
+      const int nby = ci[1] + b;
+      const int wy = ((nby % dx1) + dx1) % dx1;
+      const int ddy = wy - nby;
+      const R off1 = mul_rn(Traits<R>::dx(rp, 1), (R)ddy);
+      const int cy = ddy > 0 ? 1 : (ddy < 0 ? 2 : 0);
+      for (int c = -nc; c <= nc; ++c) {
+        const int nbz = ci[2] + c;
+        const int wz = ((nbz % dx2) + dx2) % dx2;
+        const int ddz = wz - nbz;
+        const R off2 = mul_rn(Traits<R>::dx(rp, 2), (R)ddz);
+        const int code = cx | (cy << 2) | ((ddz > 0 ? 1 : (ddz < 0 ? 2 : 0)) << 4);
+        const int cell = rp.cell_base + wx + wy * dx0 + wz * dx0 * dx1;
+        const int s1 = cell_start[cell + 1];
+        for (int s = cell_start[cell]; s < s1; ++s) {
+          const typename Traits<R>::V4 pj = pos4[s];
+          const R r0 = sub_rn(sub_rn(pj.x, off0), pix[0]);
+          const R r1 = sub_rn(sub_rn(pj.y, off1), pix[1]);
+          const R r2 = sub_rn(sub_rn(pj.z, off2), pix[2]);
+          const R d2 = add_rn(add_rn(mul_rn(r0, r0), mul_rn(r1, r1)), mul_rn(r2, r2));
+          if (gt_small(sub_rn(rc2, d2)) && gt_small(sub_rn(d2, rs2))) {
+            if (shell_index % pice == 0) {
+              if (n_shell < shell_cap) nbr[(size_t)(core_cap + n_shell) * stride + i] = (s << kShiftBits) | code;
+              ++n_shell;
+            }
+            ++shell_index;
+          } else if (gt_small(sub_rn(rs2, d2)) && gt_small(d2)) {
+            if (n_core < core_cap) nbr[(size_t)n_core * stride + i] = (s << kShiftBits) | code;
+            ++n_core;
+          }
+        }
+      }
+    }
+  }
+  ncore[i] = n_core;
+  nshell[i] = n_shell;
+  if (n_core > core_cap || n_shell > shell_cap) {
+    set_flag(status, kFlagListOverflow);
+    atomicMax(max_count, n_core);
+    atomicMax(max_count + 1, n_shell);
+  }
+}
+
+struct RblParams {
+  int n, stride, ntypes, core_cap, molecular;
+  int table_mode;   // 1: G from the reference's ERF table (alpha 0.1, one value per bucket)
+  int shell_coul;   // 0: shell Coulomb dropped as the reference does; 1: x pice
+  const float* erf_tab;   // 2048 entries of the reference's ERF table (table_mode 1)
+  double rc, rs, alpha, qqr2e;
+  double sqrt_alpha, two_sqrt_alpha_over_sqrt_pi;
+};
+
+// The reference's ERF table (rbmd/framework/staticTable/ExecStaticTable.h:37-39,96-135): the
+// entry index is bits 15..25 of the float distance (3 low exponent bits and 8 mantissa bits), so
+// one entry serves a whole bucket of distances; entries exist for 0.1 <= d < 12 (indices 921..2047
+// below d = 2, 0..639 above) and hold G(alpha = 0.1) at a representative distance of the bucket
+// (tab, built on the host by rbl_erf_table).  Outside that range the reference reads past its
+// arrays; here G(0.1, d) is evaluated exactly instead.
+__device__ __forceinline__ float rbl_table_g(const float* __restrict__ tab, float dis) {
+  if (dis >= 0.1f && dis < 12.0f) return __ldg(tab + ((__float_as_int(dis) & 0x3FF8000) >> 15));
+  const double d = (double)dis, sa = 0.31622776601683794;
+  return (float)(erfc(sa * d) / (d * d) + 2.0 * sa * exp(-0.1 * d * d) / (1.7724538509055160273 * d));
+}
+
+// RBL near force of slot i: ComputeNearForceRBLERFWorklet (RunWorklet.cpp:710-814) and, without
+// charges, ComputeLJForceRBLWorklet (:1218-1302).  Core pairs: Coulomb -q_i q_j G r/d on
+// r = p_j' - p_i for 1e-4 < d^2 < rc^2 with G at |MinDistanceVec(p_j', p_i)|, then (outside the
+// molecule) LJ on MinDistanceVec for 1e-4 < d^2 < rc^2.  Shell pairs: LJ x pice for
+// rs^2 < d^2 < rc^2 (ComputeLJForceRcs) and, unless dropped, Coulomb x pice on the same range.
+// The result is the reference's corr_force = LJ + qqr2e * Coulomb; k_force_sub_mean removes its
+// mean afterwards.
+template <class R, bool COUL>
+__global__ void __launch_bounds__(128) k_rbl_force(
+    RblParams prm, const LJTable* __restrict__ ljt, const typename Traits<R>::V4* __restrict__ pos4,
+    const int2* __restrict__ meta, const int* __restrict__ nbr, const int* __restrict__ ncore,
+    const int* __restrict__ nshell, const RepDev* __restrict__ reps, const int* __restrict__ rep_of_slot,
+    const int* __restrict__ slot_atom, int shell_cap, double* __restrict__ force,
+    double* __restrict__ energy_slot, uint32_t* status) {
+  using V4 = typename Traits<R>::V4;
+  __shared__ R lj_a[kMaxReplicaTypes * kMaxReplicaTypes], lj_s6[kMaxReplicaTypes * kMaxReplicaTypes];
+  const int nt2 = prm.ntypes * prm.ntypes;
+  for (int t = threadIdx.x; t < nt2; t += blockDim.x) {
+    lj_a[t] = lj24<R>(*ljt, t);
+    lj_s6[t] = sig6<R>(*ljt, t);
+  }
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= prm.n) return;
+  const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
+  const R pice = (R)rp.rbl_pice;
+  const V4 pi = pos4[i];
+  const bool MOLEC = prm.molecular != 0;
+  const bool typed = MOLEC || prm.ntypes > 1;
+  const int2 mi = typed ? meta[i] : make_int2(0, 0);
+  const int trow = prm.ntypes > 1 ? mi.x * prm.ntypes : 0;   // one LJ type when all types agree
+  const R rc = (R)prm.rc, rs = (R)prm.rs;
+  const R rc2 = rc * rc, rs2 = rs * rs;
+  const R box[3] = {Traits<R>::box(rp, 0), Traits<R>::box(rp, 1), Traits<R>::box(rp, 2)};
+  const R wrap[3] = {Traits<R>::wrap(rp, 0), Traits<R>::wrap(rp, 1), Traits<R>::wrap(rp, 2)};
+  const R sa = (R)prm.sqrt_alpha, aa = (R)prm.alpha, c2 = (R)prm.two_sqrt_alpha_over_sqrt_pi;
+  const R qqr2e = (R)prm.qqr2e;
+  const R qi = pi.w;
+  const size_t st = (size_t)prm.stride;
+  Acc<R> fx, fy, fz;
+  double e_lj = 0, e_coul = 0;
+  const int nco = min(ncore[i], prm.core_cap), nsh = min(nshell[i], shell_cap);
+  for (int p = 0; p < nco + nsh; ++p) {
+    const bool shell = p >= nco;
+    const int row = shell ? prm.core_cap + (p - nco) : p;
+    const int e = __ldg(nbr + (size_t)row * st + i);
+    const int js = e >> kShiftBits;
+    const V4 pj = pos4[js];
+    R px = pj.x, py = pj.y, pz = pj.z;
+    if (e & 63) {
+      const int k0 = e & 3, k1 = (e >> 2) & 3, k2 = (e >> 4) & 3;
+      px = px - (k0 == 1 ? wrap[0] : (k0 == 2 ? -wrap[0] : (R)0));
+      py = py - (k1 == 1 ? wrap[1] : (k1 == 2 ? -wrap[1] : (R)0));
+      pz = pz - (k2 == 1 ? wrap[2] : (k2 == 2 ? -wrap[2] : (R)0));
+    }
+    const R r0 = px - pi.x, r1 = py - pi.y, r2 = pz - pi.z;
+    R m0 = r0, m1 = r1, m2 = r2;   // MinDistanceVec(p_j', p_i)
+    min_image(m0, m1, m2, box);
+    const R dm2 = m0 * m0 + m1 * m1 + m2 * m2;
+    const R w = shell ? pice : (R)1;
+    R t0 = 0, t1 = 0, t2 = 0;
+    if (COUL && (!shell || prm.shell_coul)) {
+      const R qq = qi * pj.w;
+      const R d2 = r0 * r0 + r1 * r1 + r2 * r2;
+      const bool ok = shell ? (d2 < rc2 && d2 > rs2) : (d2 < rc2 && d2 > (R)1.0e-4);
+      if (qq != (R)0 && ok) {
+        const R dis = sqrt_r(d2);
+        const R dism = sqrt_r(dm2);
+        R g;
+        if (prm.table_mode) {
+          g = (R)rbl_table_g(prm.erf_tab, (float)dism);
+        } else {
+          const R inv = (R)1 / dism;
+          const R ex = exp_r(-aa * dm2);
+          g = (erfc_shared(sa * dism, ex) * inv + c2 * ex) * inv;
+        }
+        const R s = -qq * g / dis * qqr2e * w;
+        t0 += s * r0; t1 += s * r1; t2 += s * r2;
+        if (energy_slot) {
+          const double dd = (double)dism;
+          e_coul += (double)w * (double)qqr2e * (double)qq * erfc(prm.sqrt_alpha * dd) / dd;
+        }
+      }
+    }
+    bool same = false;
+    int tj = 0;
+    if (typed) {
+      const int2 mj = meta[js];
+      same = MOLEC && (mj.y == mi.y);
+      tj = prm.ntypes > 1 ? mj.x : 0;
+    }
+    if (!same) {
+      const bool ok = shell ? (dm2 < rc2 && dm2 > rs2) : (dm2 < rc2 && dm2 > (R)0.0001);
+      if (ok) {
+        const R inv2 = (R)1 / dm2;
+        const R sd6 = lj_s6[trow + tj] * inv2 * inv2 * inv2;
+        const R a24 = lj_a[trow + tj];
+        const R scal = w * (a24 * (((R)2 * sd6 - (R)1) * sd6) * inv2);
+        t0 += scal * m0; t1 += scal * m1; t2 += scal * m2;
+        if (energy_slot) e_lj += (double)w * (double)(-a24 / (R)6 * (sd6 - (R)1) * sd6);
+      }
+    }
+    fx.add(t0); fy.add(t1); fz.add(t2);
+  }
+  const double F[3] = {fx.value(), fy.value(), fz.value()};
+  if (!isfinite(F[0]) || !isfinite(F[1]) || !isfinite(F[2])) set_flag(status, kFlagNonFinite);
+  const int id = slot_atom[i];
+  force[3 * id] = F[0];
+  force[3 * id + 1] = F[1];
+  force[3 * id + 2] = F[2];
+  if (energy_slot) {
+    energy_slot[2 * i] = 0.5 * e_lj;
+    energy_slot[2 * i + 1] = 0.5 * e_coul;
+  }
+}
+
+// EAM over the RBL lists: ComputeEAMfp_Worklet and ComputeEAMRBLWorklet (RunWorklet.cpp:
+// 1052-1216) with ComputeEAMrhoRs / ComputeEAMforceRBL (rbmd/framework/forceFunction/
+// ExecForceFunction.h:358-381,484-520): core pairs as the full-list passes (0.01 < r^2 < rc^2),
+// shell pairs x pice for rs^2 < r^2 < rc^2, pair vector MinDistanceVec(p_i, p_j').
+template <class R>
+__device__ __forceinline__ void rbl_eam_pair(const typename Traits<R>::V4& pi, const typename Traits<R>::V4& pj,
+                                             int e, const R* wrap, const R* box, R* r) {
+  const R pjv[3] = {pj.x, pj.y, pj.z}, piv[3] = {pi.x, pi.y, pi.z};
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int cd = (e >> (2 * d)) & 3;
+    const R off = cd == 1 ? wrap[d] : (cd == 2 ? -wrap[d] : (R)0);
+    r[d] = piv[d] - (pjv[d] - off);
+  }
+  min_image(r[0], r[1], r[2], box);
+}
+
+template <class R>
+__global__ void __launch_bounds__(128) k_rbl_eam_fp(int n, int stride, int core_cap, int shell_cap, double rc,
+                                                    double rs, EamDev eam,
+                                                    const typename Traits<R>::V4* __restrict__ pos4,
+                                                    const int* __restrict__ nbr, const int* __restrict__ ncore,
+                                                    const int* __restrict__ nshell,
+                                                    const RepDev* __restrict__ reps,
+                                                    const int* __restrict__ rep_of_slot, R* __restrict__ fp,
+                                                    double* __restrict__ embed_slot) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
+  const R pice = (R)rp.rbl_pice;
+  const typename Traits<R>::V4 pi = pos4[i];
+  const R wrap[3] = {Traits<R>::wrap(rp, 0), Traits<R>::wrap(rp, 1), Traits<R>::wrap(rp, 2)};
+  const R box[3] = {Traits<R>::box(rp, 0), Traits<R>::box(rp, 1), Traits<R>::box(rp, 2)};
+  const R cut2 = (R)rc * (R)rc, rs2 = (R)rs * (R)rs;
+  const R rdr = sizeof(R) == 4 ? (R)eam.rdr : (R)eam.rdr_d;
+  Acc<R> rho;
+  const int nco = min(ncore[i], core_cap), nsh = min(nshell[i], shell_cap);
+  for (int p = 0; p < nco + nsh; ++p) {
+    const bool shell = p >= nco;
+    const int e = __ldg(nbr + (size_t)(shell ? core_cap + (p - nco) : p) * stride + i);
+    R r[3];
+    rbl_eam_pair<R>(pi, pos4[e >> kShiftBits], e, wrap, box, r);
+    const R rsq = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    const bool ok = shell ? (rsq < cut2 && rsq > rs2) : (rsq < cut2 && rsq > (R)0.01);
+    if (!ok) continue;
+    R pp = sqrt_r(rsq) * rdr + (R)1;
+    int m = min((int)pp, eam.nr - 1);
+    pp -= (R)m;
+    pp = fmin(pp, (R)1);
+    const float4 b = __ldg(eam.rhor + 2 * m + 0);
+    const float4 c = __ldg(eam.rhor + 2 * m + 1);
+    const R v = (((R)b.w * pp + (R)c.x) * pp + (R)c.y) * pp + (R)c.z;
+    rho.add(shell ? pice * v : v);
+  }
+  const R rr = (R)rho.value();
+  R pp = rr * (sizeof(R) == 4 ? (R)eam.rdrho : (R)eam.rdrho_d) + (R)1;
+  int m = max(1, min((int)pp, eam.nrho - 1));
+  pp -= (R)m;
+  pp = fmin(pp, (R)1);
+  const float4 a = __ldg(eam.frho + 2 * m + 0);
+  const float4 b = __ldg(eam.frho + 2 * m + 1);
+  fp[i] = ((R)a.x * pp + (R)a.y) * pp + (R)a.z;
+  if (embed_slot) {
+    double phi = (((double)a.w * pp + (double)b.x) * pp + (double)b.y) * pp + (double)b.z;
+    if ((double)rr > eam.rhomax) phi += (double)fp[i] * ((double)rr - eam.rhomax);
+    embed_slot[i] = phi;
+  }
+}
+
+template <class R>
+__global__ void __launch_bounds__(128) k_rbl_eam_force(int n, int stride, int core_cap, int shell_cap, double rc,
+                                                       double rs, EamDev eam,
+                                                       const typename Traits<R>::V4* __restrict__ pos4,
+                                                       const int* __restrict__ nbr, const int* __restrict__ ncore,
+                                                       const int* __restrict__ nshell,
+                                                       const RepDev* __restrict__ reps,
+                                                       const int* __restrict__ rep_of_slot,
+                                                       const R* __restrict__ fp, const int* __restrict__ slot_atom,
+                                                       double* __restrict__ force, double* __restrict__ pair_slot,
+                                                       uint32_t* status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
+  const R pice = (R)rp.rbl_pice;
+  const typename Traits<R>::V4 pi = pos4[i];
+  const R wrap[3] = {Traits<R>::wrap(rp, 0), Traits<R>::wrap(rp, 1), Traits<R>::wrap(rp, 2)};
+  const R box[3] = {Traits<R>::box(rp, 0), Traits<R>::box(rp, 1), Traits<R>::box(rp, 2)};
+  const R cut2 = (R)rc * (R)rc, rs2 = (R)rs * (R)rs;
+  const R rdr = sizeof(R) == 4 ? (R)eam.rdr : (R)eam.rdr_d;
+  const R fpi = fp[i];
+  Acc<R> fx, fy, fz;
+  double epair = 0;
+  const int nco = min(ncore[i], core_cap), nsh = min(nshell[i], shell_cap);
+  for (int p = 0; p < nco + nsh; ++p) {
+    const bool shell = p >= nco;
+    const int e = __ldg(nbr + (size_t)(shell ? core_cap + (p - nco) : p) * stride + i);
+    const int j = e >> kShiftBits;
+    R r[3];
+    rbl_eam_pair<R>(pi, pos4[j], e, wrap, box, r);
+    const R rsq = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    const bool ok = shell ? (rsq < cut2 && rsq > rs2) : (rsq < cut2 && rsq > (R)0.01);
+    if (!ok) continue;
+    const R rv = sqrt_r(rsq);
+    R pp = rv * rdr + (R)1;
+    int m = min((int)pp, eam.nr - 1);
+    pp -= (R)m;
+    pp = fmin(pp, (R)1);
+    const float4 ra = __ldg(eam.rhor + 2 * m + 0);
+    const float4 za = __ldg(eam.z2r + 2 * m + 0);
+    const float4 zb = __ldg(eam.z2r + 2 * m + 1);
+    const R rhop = ((R)ra.x * pp + (R)ra.y) * pp + (R)ra.z;
+    const R z2p = ((R)za.x * pp + (R)za.y) * pp + (R)za.z;
+    const R z2 = (((R)za.w * pp + (R)zb.x) * pp + (R)zb.y) * pp + (R)zb.z;
+    const R recip = (R)1 / rv;
+    const R phi = z2 * recip;
+    const R phip = z2p * recip - phi * recip;
+    const R psip = fpi * rhop + fp[j] * rhop + phip;
+    const R fpair = -psip * recip;
+    const R w = shell ? pice : (R)1;
+    fx.add(w * (r[0] * fpair));
+    fy.add(w * (r[1] * fpair));
+    fz.add(w * (r[2] * fpair));
+    epair += (double)w * (double)phi;
+  }
+  const double F[3] = {fx.value(), fy.value(), fz.value()};
+  if (!isfinite(F[0]) || !isfinite(F[1]) || !isfinite(F[2])) set_flag(status, kFlagNonFinite);
+  const int id = slot_atom[i];
+  force[3 * id] = F[0];
+  force[3 * id + 1] = F[1];
+  force[3 * id + 2] = F[2];
+  if (pair_slot) pair_slot[i] = 0.5 * epair;
+}
+
+// Mean removal F_i -= (sum_j F_j) / N_replica (SumRBLCorrForceWorklet, RunWorklet.cpp:1304-1321,
+// after the Reduce of ExecutionMD.cpp:568-569): per-chunk FP64 sums in a fixed order, then every
+// block re-sums its replica's chunk partials in chunk order (deterministic) and subtracts.
+__global__ void __launch_bounds__(256) k_force_chunk_sum(const MdChunk* __restrict__ chunks,
+                                                         const double* __restrict__ force,
+                                                         double* __restrict__ partial) {
+  const MdChunk c = chunks[blockIdx.x];
+  double s[3] = {0, 0, 0};
+  for (int a = c.begin + threadIdx.x; a < c.end; a += blockDim.x)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) s[d] += force[3 * a + d];
+  __shared__ double red[3][8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double v = s[d];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[d][warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double v = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[threadIdx.x][w];
+    partial[3 * blockIdx.x + threadIdx.x] = v;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_force_sub_mean(const MdChunk* __restrict__ chunks,
+                                                        const int* __restrict__ chunk_rep_begin,
+                                                        const RepDev* __restrict__ reps,
+                                                        const double* __restrict__ partial,
+                                                        double* __restrict__ force) {
+  const MdChunk c = chunks[blockIdx.x];
+  __shared__ double mean[3];
+  if (threadIdx.x < 3) {
+    double v = 0;
+    for (int k = chunk_rep_begin[c.rep]; k < chunk_rep_begin[c.rep + 1]; ++k) v += partial[3 * k + threadIdx.x];
+    const RepDev& rp = reps[c.rep];
+    mean[threadIdx.x] = v / (double)(rp.atom_end - rp.atom_begin);
+  }
+  __syncthreads();
+  for (int a = c.begin + threadIdx.x; a < c.end; a += blockDim.x)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) force[3 * a + d] -= mean[d];
+}
+
+}  // namespace rbmd

@@ -25,6 +25,7 @@
 #include "kernels_cells.cuh"
 #include "kernels_force.cuh"
 #include "kernels_md.cuh"
+#include "kernels_rbl.cuh"
 
 using namespace rbmd;
 
@@ -83,6 +84,10 @@ struct rbmd_force {
   std::string shake = "null", init_way = "read_data", tctrl = "";
   bool far = false, fp64 = false;
   double rc = 2.5, rs = 2.5, skin = 0.0, alpha = 0.1;
+  double rbl_sample_num = 100;   // neighbor.neighbor_sample_num (RBL)
+  bool rbl_table = false;        // compat.rbl_erf_table: G from the reference's alpha=0.1 table
+  bool rbl_shell_coul = true;    // !compat.rbl_drop_shell_coulomb
+  bool eam_ref_sign = false;     // compat.eam_verlet_pair_vector: reference's reversed EAM force
   int P = 100, kmax = 2;
   unsigned long long seed = 20240101ull;
   Units u{1, 1, 1, 1};
@@ -136,6 +141,14 @@ struct rbmd_force {
   void* d_frac = nullptr;
   int2* d_meta = nullptr;
   int *d_nbr = nullptr, *d_count = nullptr, *d_maxcount = nullptr;
+  // RBL: rows [0, core_cap) of d_nbr hold the core list (counts in d_count), rows
+  // [core_cap, cap) the kept shell pairs (counts in d_count2); rbl_sizes_h = rs_num, rc_num, pice
+  // of the reference's sizing formulas for replica 0
+  int* d_count2 = nullptr;
+  int core_cap = 0, shell_cap = 0;
+  int64_t rbl_sizes_h[3] = {0, 0, 0};
+  double* d_mean_partial = nullptr;
+  float* d_erf_tab = nullptr;   // compat.rbl_erf_table
   int *d_rebuild = nullptr, *d_block_sums = nullptr;
   unsigned long long* d_nbuilds = nullptr;
   double* d_xref = nullptr;
@@ -194,6 +207,7 @@ struct rbmd_force {
   long long phase_n[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 
   bool is_rbe() const { return far && (coul_type == "RBE" || coul_type == "EWALD"); }
+  bool is_rbl() const { return nbr_type == "RBL"; }
   bool is_eam() const { return ff == "EAM"; }
   bool is_cvff() const { return ff == "CVFF"; }
   bool with_coul_near() const { return far && ff != "EAM"; }
@@ -258,6 +272,7 @@ void free_all(rbmd_force* f) {
   if (f->d_frac) cudaFree(f->d_frac);
   f->d_frac = nullptr;
   dfree(f->d_meta); dfree(f->d_nbr); dfree(f->d_count); dfree(f->d_maxcount); dfree(f->d_status);
+  dfree(f->d_count2); dfree(f->d_mean_partial); dfree(f->d_erf_tab);
   dfree(f->d_rebuild); dfree(f->d_block_sums); dfree(f->d_xref); dfree(f->d_nbuilds);
   dfree(f->d_eslot); dfree(f->d_esum);
   if (f->d_krec) cudaFree(f->d_krec);
@@ -314,6 +329,72 @@ void setup_replica(const rbmd_box& b, double cut, double rs, bool fp64, RepDev& 
   r.ncell = r.dims[0] * r.dims[1] * r.dims[2];
 }
 
+// RBL list sizing of ExecutionMD::ComputeRBLNearForce / ComputeRBLLJForce / ComputeRBLEAMForce
+// (rbmd/framework/run/ExecutionMD.cpp:467-486,577-589,724-736) for replica r in the run's Real:
+// rho = N / (Lx Ly Lz); rs_num = round(1 + 0.05/rho - 0.05) * rho * ceil(4/3 pi rs^3) + 1 (the
+// EAM variant has no rounding factor), rc_num likewise, pice = ceil(1 / (sample / (rc_num - rs_num))).
+template <class Real>
+void rbl_sizes_t(int64_t natoms, const Real* box, double rs, double rc, double sample, bool eam, int64_t* z) {
+  const Real rho = (Real)natoms / (box[0] * box[1] * box[2]);
+  const float pif = 3.14159265358979323846f;
+  const Real rs_r = (Real)rs, rc_r = (Real)rc;
+  int64_t coeff = 1;
+  if (!eam) coeff = (int64_t)std::round((Real)(1.0 + (0.05 / (double)rho - 0.05)));
+  const double cs = std::ceil(4.0 / 3.0 * (double)pif * (double)rs_r * (double)rs_r * (double)rs_r);
+  const double cc = std::ceil(4.0 / 3.0 * (double)pif * (double)rc_r * (double)rc_r * (double)rc_r);
+  const double rf = (double)(eam ? rho : (Real)coeff * rho);
+  z[0] = (int64_t)(rf * cs + 1);
+  z[1] = (int64_t)(rf * cc + 1);
+  const Real rate = (Real)sample / (Real)(z[1] - z[0]);
+  z[2] = (int64_t)std::ceil(1.0 / (double)rate);
+}
+void rbl_sizes(const rbmd_force* f, int r, int64_t* z) {
+  const int64_t na = f->rep_off[r + 1] - f->rep_off[r];
+  const rbmd_box& b = f->boxes[r];
+  if (f->fp64) {
+    const double box[3] = {b.hi[0] - b.lo[0], b.hi[1] - b.lo[1], b.hi[2] - b.lo[2]};
+    rbl_sizes_t<double>(na, box, f->rs, f->rc, f->rbl_sample_num, f->is_eam(), z);
+  } else {
+    const float box[3] = {(float)b.hi[0] - (float)b.lo[0], (float)b.hi[1] - (float)b.lo[1],
+                          (float)b.hi[2] - (float)b.lo[2]};
+    rbl_sizes_t<float>(na, box, f->rs, f->rc, f->rbl_sample_num, f->is_eam(), z);
+  }
+}
+
+// The reference's ERF table for the RBL Coulomb term (rbmd/framework/model/ERFTable.h, read by
+// ExecStaticTable::TableGnearValue, rbmd/framework/staticTable/ExecStaticTable.h:96-135): entry k
+// (bits 15..25 of the float distance) holds Gnear(alpha = 0.1, d_k) evaluated as the reference's
+// ExecForceFunction::Gnear does in float ((1.0 - erf(x)) / d^2 in double, the rest in float,
+// rbmd/framework/forceFunction/ExecForceFunction.h:217-224) at d_k = the bucket's lower edge
+// rounded up to 4 decimals below d = 2 and to 3 decimals above, and not below 0.1.  Entries
+// 921..2047 cover 0.1 <= d < 2, entries 0..639 cover 2 <= d < 12; that rule reproduces every
+// entry of the reference's tables to their printed 6 significant digits.
+std::vector<float> rbl_erf_table() {
+  std::vector<float> t(2048, 0.f);
+  auto fill = [&](int k0, int k1, int exp_base, int dec) {
+    for (int k = k0; k < k1; ++k) {
+      const int e3 = k >> 8, man = k & 255;
+      const int ex = exp_base + (e3 >= 3 ? e3 - 3 : e3);
+      const uint32_t bits = ((uint32_t)ex << 23) | ((uint32_t)man << 15);
+      float edge;
+      std::memcpy(&edge, &bits, 4);
+      const double sc = std::pow(10.0, dec);
+      const double v = (double)edge * sc, rv = std::nearbyint(v);
+      double d = (std::fabs(v - rv) < 1e-6 ? rv : std::ceil(v)) / sc;
+      d = std::max(d, 0.1);
+      const float df = (float)d, a = 0.1f;
+      const float x = std::sqrt(a) * df;
+      const double t1 = (1.0 - (double)std::erf(x)) / (double)(df * df);
+      const float pif = 3.14159265358979323846f;
+      const float t2 = 2.0f * std::sqrt(a) * std::exp(-a * df * df) / (std::sqrt(pif) * df);
+      t[k] = (float)(t1 + (double)t2);
+    }
+  };
+  fill(921, 2048, 123, 4);   // exponents 123..127 -> index high bits 3..7
+  fill(0, 640, 128, 3);      // exponents 128..130 -> index high bits 0..2
+  return t;
+}
+
 // RBE normaliser S = prod_d H_d - 1 with H_d = sqrt(a L^2/pi) sum_{|m|<=10} e^{-a L^2 m^2}
 // (ExecForceFunction::Compute_S/Compute_H, rbmd/framework/forceFunction/ExecForceFunction.h:266-294),
 // evaluated in FP64.
@@ -336,6 +417,16 @@ void launch_nlist(rbmd_force* f, cudaStream_t s) {
       f->n, (const typename Traits<R>::V4*)f->d_pos4, f->d_cell_start, f->d_reps,
       f->nrep > 1 ? f->d_rep_of : nullptr, f->num_cycles, (R)f->list_cut(), f->cap, f->stride, f->d_nbr,
       f->d_count, f->d_maxcount, f->d_status, f->skin > 0 ? f->d_rebuild : nullptr, f->d_nbuilds);
+  f->launches++;
+}
+
+template <class R>
+void launch_rbl_list(rbmd_force* f, cudaStream_t s) {
+  PhaseScope ps(f, kPhList, s);
+  k_rbl_list<R><<<(f->n + 127) / 128, 128, 0, s>>>(
+      f->n, (const typename Traits<R>::V4*)f->d_pos4, f->d_cell_start, f->d_reps,
+      f->nrep > 1 ? f->d_rep_of : nullptr, f->num_cycles, (R)f->rc, (R)f->rs, f->core_cap, f->shell_cap,
+      f->stride, f->d_nbr, f->d_count, f->d_count2, f->d_maxcount, f->d_status);
   f->launches++;
 }
 
@@ -464,7 +555,65 @@ void launch_eam(rbmd_force* f, cudaStream_t s) {
                                  f->d_nbr, f->d_count, f->d_reps, rp, (R*)f->d_fp, f->d_emb);
   k_eam_force<R><<<nb, bs, 0, s>>>(f->n, f->stride, f->cap, f->rc, e, (const typename Traits<R>::V4*)f->d_pos4,
                                     f->d_nbr, f->d_count, f->d_reps, rp, (const R*)f->d_fp, f->d_slot_atom,
-                                    f->at.force, f->d_epair, f->d_status);
+                                    f->at.force, f->d_epair, f->d_status, f->eam_ref_sign ? 1 : 0);
+  f->launches += 2;
+}
+
+template <class R>
+void launch_rbl_force(rbmd_force* f, cudaStream_t s) {
+  const int* rp = f->nrep > 1 ? f->d_rep_of : nullptr;
+  const int nb = (f->n + 127) / 128;
+  if (f->is_eam()) {
+    EamDev e;
+    e.frho = f->d_frho;
+    e.rhor = f->d_rhor;
+    e.z2r = f->d_z2r;
+    e.nrho = f->eam_h.nrho;
+    e.nr = f->eam_h.nr;
+    e.rdr = 1.0f / f->eam_h.dr;
+    e.rdrho = 1.0f / f->eam_h.drho;
+    e.rdr_d = 1.0 / (double)f->eam_h.dr;
+    e.rdrho_d = 1.0 / (double)f->eam_h.drho;
+    e.rhomax = f->eam_h.rhomax;
+    k_rbl_eam_fp<R><<<nb, 128, 0, s>>>(f->n, f->stride, f->core_cap, f->shell_cap, f->rc, f->rs, e,
+                                        (const typename Traits<R>::V4*)f->d_pos4, f->d_nbr, f->d_count,
+                                        f->d_count2, f->d_reps, rp, (R*)f->d_fp, f->d_emb);
+    k_rbl_eam_force<R><<<nb, 128, 0, s>>>(f->n, f->stride, f->core_cap, f->shell_cap, f->rc, f->rs, e,
+                                           (const typename Traits<R>::V4*)f->d_pos4, f->d_nbr, f->d_count,
+                                           f->d_count2, f->d_reps, rp, (const R*)f->d_fp, f->d_slot_atom,
+                                           f->at.force, f->d_epair, f->d_status);
+    f->launches += 2;
+  } else {
+    RblParams p;
+    p.n = f->n;
+    p.stride = f->stride;
+    p.ntypes = f->nt_eff;
+    p.core_cap = f->core_cap;
+    p.molecular = f->at.molecule != nullptr;
+    p.table_mode = f->rbl_table ? 1 : 0;
+    p.shell_coul = f->rbl_shell_coul ? 1 : 0;
+    p.erf_tab = f->d_erf_tab;
+    p.rc = f->rc;
+    p.rs = f->rs;
+    p.alpha = f->alpha;
+    p.qqr2e = f->u.qqr2e;
+    p.sqrt_alpha = std::sqrt(f->alpha);
+    p.two_sqrt_alpha_over_sqrt_pi = 2.0 * std::sqrt(f->alpha) / std::sqrt(M_PI);
+    double* es = f->want_energy ? f->d_eslot : nullptr;
+    if (f->with_coul_near())
+      k_rbl_force<R, true><<<nb, 128, 0, s>>>(p, f->d_ljt, (const typename Traits<R>::V4*)f->d_pos4, f->d_meta,
+                                              f->d_nbr, f->d_count, f->d_count2, f->d_reps, rp, f->d_slot_atom,
+                                              f->shell_cap, f->at.force, es, f->d_status);
+    else
+      k_rbl_force<R, false><<<nb, 128, 0, s>>>(p, f->d_ljt, (const typename Traits<R>::V4*)f->d_pos4, f->d_meta,
+                                               f->d_nbr, f->d_count, f->d_count2, f->d_reps, rp, f->d_slot_atom,
+                                               f->shell_cap, f->at.force, es, f->d_status);
+    f->launches++;
+  }
+  // F_i -= mean_j F_j per replica (ExecutionMD.cpp:568-570)
+  k_force_chunk_sum<<<f->nchunks, 256, 0, s>>>(f->d_chunks, f->at.force, f->d_mean_partial);
+  k_force_sub_mean<<<f->nchunks, 256, 0, s>>>(f->d_chunks, f->d_chunk_rep_begin, f->d_reps, f->d_mean_partial,
+                                              f->at.force);
   f->launches += 2;
 }
 
@@ -495,8 +644,12 @@ void launch_force_tail(rbmd_force* f, cudaStream_t s, bool bin) {
     cudaEventRecord(f->ev_join, f->side);
   }
   launch_sort<R>(f, s, bin);
-  launch_nlist<R>(f, s);
-  {
+  if (f->is_rbl()) {
+    launch_rbl_list<R>(f, s);
+    PhaseScope ps(f, kPhForce, s);
+    launch_rbl_force<R>(f, s);
+  } else {
+    launch_nlist<R>(f, s);
     PhaseScope ps(f, kPhForce, s);
     if (f->is_eam()) launch_eam<R>(f, s);
     else launch_near<R>(f, s);
@@ -517,7 +670,7 @@ void launch_force_tail(rbmd_force* f, cudaStream_t s, bool bin) {
 template <class R>
 void launch_compute(rbmd_force* f, cudaStream_t s) {
   f->want_energy = true;
-  cudaMemsetAsync(f->d_maxcount, 0, sizeof(int), s);
+  cudaMemsetAsync(f->d_maxcount, 0, 2 * sizeof(int), s);
   if (f->skin > 0 && f->list_valid) {
     // reuse the list when no atom moved more than skin/2 since it was built
     cudaMemsetAsync(f->d_rebuild, 0, sizeof(int), s);
@@ -537,11 +690,17 @@ void launch_compute_any(rbmd_force* f, cudaStream_t s) {
   else launch_compute<float>(f, s);
 }
 
-rbmd_status grow_list(rbmd_force* f, int need) {
-  const int newcap = ((int)(need * 1.2) + 8 + 7) & ~7;
+rbmd_status grow_list(rbmd_force* f, const int* need) {
+  auto grown = [](int cur, int want) { return std::max(cur, ((int)(want * 1.2) + 8 + 7) & ~7); };
+  if (f->is_rbl()) {
+    f->core_cap = grown(f->core_cap, need[0]);
+    f->shell_cap = grown(f->shell_cap, need[1]);
+    f->cap = f->core_cap + f->shell_cap;
+  } else {
+    f->cap = ((int)(need[0] * 1.2) + 8 + 7) & ~7;
+  }
   dfree(f->d_nbr);
-  CK(dalloc(&f->d_nbr, (size_t)newcap * f->stride));
-  f->cap = newcap;
+  CK(dalloc(&f->d_nbr, (size_t)f->cap * f->stride));
   return RBMD_OK;
 }
 
@@ -549,12 +708,12 @@ rbmd_status grow_list(rbmd_force* f, int need) {
 rbmd_status check_overflow(rbmd_force* f, cudaStream_t s, bool* redo) {
   *redo = false;
   CK(cudaMemcpyAsync(f->h_status, f->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(f->h_maxcount, f->d_maxcount, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(f->h_maxcount, f->d_maxcount, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   prof_collect(f);
   if (*f->h_status & kFlagListOverflow) {
     f->list_valid = false;
-    rbmd_status st = grow_list(f, *f->h_maxcount);
+    rbmd_status st = grow_list(f, f->h_maxcount);
     if (st) return st;
     uint32_t clr = *f->h_status & ~kFlagListOverflow;
     CK(cudaMemcpyAsync(f->d_status, &clr, sizeof clr, cudaMemcpyHostToDevice, s));
@@ -577,7 +736,7 @@ void launch_step(rbmd_force* f, cudaStream_t s) {
   mp.apply_scale = f->pending_scale ? 1 : 0;
   mp.nh = f->tstat == 3;
   f->want_energy = f->energy_every > 0 && ((f->step_count + 1) % f->energy_every == 0);
-  cudaMemsetAsync(f->d_maxcount, 0, sizeof(int), s);
+  cudaMemsetAsync(f->d_maxcount, 0, 2 * sizeof(int), s);
   cudaMemsetAsync(f->d_cell_count, 0, sizeof(int) * f->ncell_total, s);
   // with a skin the drift kernel decides; a missing or overflowed list forces a rebuild
   if (f->skin > 0) cudaMemsetAsync(f->d_rebuild, f->list_valid ? 0 : 1, sizeof(int), s);
@@ -730,12 +889,40 @@ rbmd_status parse_config(rbmd_force* f, const char* text) {
     std::snprintf(g_last_error, sizeof g_last_error, "config: unknown coulomb.type %s", f->coul_type.c_str());
     return RBMD_ERR_CONFIG;
   }
-  if (f->nbr_type != "VERLETLIST") {
+  if (f->nbr_type != "VERLETLIST" && f->nbr_type != "RBL") {
     std::snprintf(g_last_error, sizeof g_last_error,
-                  "config: neighbor.type %s is not provided by this build (VERLETLIST only)",
+                  "config: neighbor.type %s is not provided by this build (VERLETLIST, RBL)",
                   f->nbr_type.c_str());
     return RBMD_ERR_CONFIG;
   }
+  // RBL (Neighbor.cpp:40-44): r_core and neighbor_sample_num; the shell subsample follows the
+  // traversal of the current positions, so the lists are rebuilt at every force evaluation
+  if (f->nbr_type == "RBL") {
+    f->rbl_sample_num = num(root, "hyper_parameters.neighbor.neighbor_sample_num", 100.0);
+    if (!(f->rs > 0) || !(f->rs < f->rc) || !(f->rbl_sample_num >= 1)) {
+      std::snprintf(g_last_error, sizeof g_last_error,
+                    "config: RBL needs 0 < r_core < cut_off and neighbor_sample_num >= 1");
+      return RBMD_ERR_CONFIG;
+    }
+    if (f->skin > 0) {
+      std::snprintf(g_last_error, sizeof g_last_error, "config: neighbor.skin applies to VERLETLIST only");
+      return RBMD_ERR_CONFIG;
+    }
+  }
+  // reference quirks kept behind switches (the defaults are the physical forces):
+  //  * compat.rbl_erf_table: RBL Coulomb G from the reference's ERF table, built for alpha 0.1 and
+  //    holding one value per distance bucket (ExecStaticTable.h:96-135, RunWorklet.cpp:772-773);
+  //  * compat.rbl_drop_shell_coulomb: the shell Coulomb term is computed and discarded
+  //    (RunWorklet.cpp:782);
+  //  * compat.eam_verlet_pair_vector: the Verlet EAM force on MinDistanceVec(p_j, p_i)
+  //    (RunWorklet.cpp:402), which reverses it (the RBL pass uses p_i - p_j, :1180).
+  auto flag = [&](const char* key) {
+    const Value* v = root.path(key);
+    return v && v->kind == Value::Bool && v->b;
+  };
+  f->rbl_table = flag("compat.rbl_erf_table");
+  f->rbl_shell_coul = !flag("compat.rbl_drop_shell_coulomb");
+  f->eam_ref_sign = flag("compat.eam_verlet_pair_vector");
   if (f->P < 1 || f->P > 65536) return RBMD_ERR_CONFIG;
   return RBMD_OK;
 }
@@ -956,6 +1143,27 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
   const double lc = f->list_cut();
   f->cap = ((int)(1.5 * rho_max * 4.0 / 3.0 * M_PI * lc * lc * lc) + 32 + 7) & ~7;
   if (f->cap_override > 0) f->cap = f->cap_override;
+  if (f->is_rbl()) {
+    // pice per replica from the reference's sizing (ExecutionMD.cpp:460-801); capacities from
+    // the density with a margin (the reference's rs_num / rc_num rows have no overflow check)
+    int pice_min = 1 << 30;
+    for (int r = 0; r < nrep; ++r) {
+      int64_t z[3];
+      rbl_sizes(f, r, z);
+      if (z[2] < 1 || z[2] > (1 << 20)) {
+        std::snprintf(g_last_error, sizeof g_last_error, "RBL: pice_num %lld out of range", (long long)z[2]);
+        return RBMD_ERR_CONFIG;
+      }
+      f->reps_h[r].rbl_pice = (int)z[2];
+      pice_min = std::min(pice_min, (int)z[2]);
+      if (r == 0) std::memcpy(f->rbl_sizes_h, z, sizeof z);
+    }
+    const double rs3 = f->rs * f->rs * f->rs, rc3 = f->rc * f->rc * f->rc;
+    f->core_cap = ((int)(1.5 * rho_max * 4.0 / 3.0 * M_PI * rs3) + 32 + 7) & ~7;
+    f->shell_cap = ((int)(1.5 * rho_max * 4.0 / 3.0 * M_PI * (rc3 - rs3) / pice_min) + 32 + 7) & ~7;
+    if (f->cap_override > 0) f->core_cap = f->cap_override;
+    f->cap = f->core_cap + f->shell_cap;
+  }
   const size_t n = f->n;
   const bool fp64 = f->fp64;
   CK(dalloc(&f->d_reps, nrep));
@@ -978,7 +1186,13 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
   CK(dalloc(&f->d_meta, n));
   CK(dalloc(&f->d_nbr, (size_t)f->cap * f->stride));
   CK(dalloc(&f->d_count, n));
-  CK(dalloc(&f->d_maxcount, 1));
+  if (f->is_rbl()) CK(dalloc(&f->d_count2, n));
+  if (f->is_rbl() && f->rbl_table) {
+    const std::vector<float> tab = rbl_erf_table();
+    CK(dalloc(&f->d_erf_tab, tab.size()));
+    CK(cudaMemcpy(f->d_erf_tab, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice));
+  }
+  CK(dalloc(&f->d_maxcount, 2));
   CK(dalloc(&f->d_nbuilds, 1));
   CK(cudaMemset(f->d_nbuilds, 0, sizeof(unsigned long long)));
   CK(dalloc(&f->d_rebuild, 1));
@@ -991,7 +1205,7 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
   CK(cudaMemset(f->d_eslot, 0, sizeof(double) * 2 * n));
   CK(dalloc(&f->d_esum, 32));
   CK(cudaMallocHost(&f->h_status, sizeof(uint32_t)));
-  CK(cudaMallocHost(&f->h_maxcount, sizeof(int)));
+  CK(cudaMallocHost(&f->h_maxcount, 2 * sizeof(int)));
   CK(cudaStreamCreateWithFlags(&f->side, cudaStreamNonBlocking));
   CK(cudaEventCreateWithFlags(&f->ev_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&f->ev_join, cudaEventDisableTiming));
@@ -1176,6 +1390,7 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
     CK(dalloc(&f->d_chunk_rep_begin, (size_t)nrep + 1));
     CK(cudaMemcpy(f->d_chunk_rep_begin, crb.data(), sizeof(int) * (nrep + 1), cudaMemcpyHostToDevice));
     CK(dalloc(&f->d_ke_partial, ch.size()));
+    if (f->is_rbl()) CK(dalloc(&f->d_mean_partial, 3 * ch.size()));
     CK(dalloc(&f->d_ke, (size_t)nrep));
     CK(dalloc(&f->d_T, (size_t)nrep));
     CK(dalloc(&f->d_lambda, (size_t)nrep));
@@ -1430,20 +1645,47 @@ rbmd_status rbmd_force_get_neighbors(rbmd_force* f, int32_t* counts, int32_t* id
   if (!f->bound) return RBMD_ERR_STATE;
   CK(cudaDeviceSynchronize());
   const size_t n = f->n;
-  std::vector<int> cnt(n), slot_atom(n), nbr((size_t)f->cap * f->stride);
+  std::vector<int> cnt(n), cnt2(n, 0), slot_atom(n), nbr((size_t)f->cap * f->stride);
   CK(cudaMemcpy(cnt.data(), f->d_count, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  if (f->is_rbl()) CK(cudaMemcpy(cnt2.data(), f->d_count2, sizeof(int) * n, cudaMemcpyDeviceToHost));
   CK(cudaMemcpy(slot_atom.data(), f->d_slot_atom, sizeof(int) * n, cudaMemcpyDeviceToHost));
   CK(cudaMemcpy(nbr.data(), f->d_nbr, sizeof(int) * nbr.size(), cudaMemcpyDeviceToHost));
   bool too_small = false;
+  // RBL: the core pairs followed by the kept shell pairs, each in traversal order
+  const int cap_a = f->is_rbl() ? f->core_cap : f->cap;
   for (size_t i = 0; i < n; ++i) {
     const int id = slot_atom[i];
-    counts[id] = cnt[i];
-    const int m = std::min<int>(cnt[i], f->cap);
-    if (cnt[i] > cap) too_small = true;
-    for (int p = 0; p < m && p < cap; ++p)
-      ids[(size_t)id * cap + p] = slot_atom[nbr[(size_t)p * f->stride + i] >> kShiftBits];
+    const int ma = std::min<int>(cnt[i], cap_a);
+    const int mb = f->is_rbl() ? std::min<int>(cnt2[i], f->shell_cap) : 0;
+    counts[id] = ma + mb;
+    if (ma + mb > cap) too_small = true;
+    for (int p = 0; p < ma + mb && p < cap; ++p) {
+      const int row = p < ma ? p : cap_a + (p - ma);
+      ids[(size_t)id * cap + p] = slot_atom[nbr[(size_t)row * f->stride + i] >> kShiftBits];
+    }
   }
   return too_small ? RBMD_ERR_ARG : RBMD_OK;
+}
+
+rbmd_status rbmd_force_get_rbl(rbmd_force* f, int32_t* ncore, int32_t* nshell, int64_t* sizes) {
+  if (!f || !sizes) return RBMD_ERR_ARG;
+  if (!f->bound || !f->is_rbl()) return RBMD_ERR_STATE;
+  CK(cudaDeviceSynchronize());
+  const size_t n = f->n;
+  std::vector<int> a(n), b(n), slot_atom(n);
+  CK(cudaMemcpy(a.data(), f->d_count, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(b.data(), f->d_count2, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(slot_atom.data(), f->d_slot_atom, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  for (size_t i = 0; i < n; ++i) {
+    if (ncore) ncore[slot_atom[i]] = a[i];
+    if (nshell) nshell[slot_atom[i]] = b[i];
+  }
+  sizes[0] = f->rbl_sizes_h[0];
+  sizes[1] = f->rbl_sizes_h[1];
+  sizes[2] = f->rbl_sizes_h[2];
+  sizes[3] = f->core_cap;
+  sizes[4] = f->shell_cap;
+  return RBMD_OK;
 }
 
 rbmd_status rbmd_force_get_rhok(rbmd_force* f, double* rho, int32_t P) {

@@ -181,6 +181,16 @@ RBMD_API rbmd_status rbmd_force_status(rbmd_force* f, uint32_t* flags, int32_t c
 RBMD_API rbmd_status rbmd_force_get_neighbors(rbmd_force* f, int32_t* counts_host, int32_t* ids_host,
                                      int64_t cap);
 
+/* RBL lists of the last compute (neighbor.type "RBL"): per caller atom the number of core pairs
+ * (d < r_core) and of kept shell pairs (every pice-th pair in r_core <= d < cut_off, in the
+ * reference's traversal order); rbmd_force_get_neighbors returns the pairs themselves, core first.
+ * sizes[5] = rs_num, rc_num, pice_num of the reference's sizing formulas for replica 0, then the
+ * library's core and shell capacities.  Mirrors num_verletlist[2] of
+ * ComputeRBLNeighboursOnceWorklet (rbmd/framework/run/worklet/RunWorklet.cpp:634-708) and the
+ * sizes of ExecutionMD::ComputeRBLNearForce (rbmd/framework/run/ExecutionMD.cpp:460-486). */
+RBMD_API rbmd_status rbmd_force_get_rbl(rbmd_force* f, int32_t* ncore_host, int32_t* nshell_host,
+                                        int64_t* sizes);
+
 /* Structure factors of the last compute: rho[n_replicas*P*2] (Re, Im) doubles, host memory,
  * with the phase origin at each box's lo corner (|rho| equals the reference's
  * ComputePnumberChargeStructureFactorWorklet + ReduceByKey result,

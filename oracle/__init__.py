@@ -174,7 +174,9 @@ def eam_tables(path):
                 frho=fr[:nrho + 1], rhor=rr[:nrho + 1], z2r=zr[:nr + 1])
 
 
-def eam_force(path, pos, lo, hi, cutoff, nl, prec="fp32", sum_mode=1):
+def eam_force(path, pos, lo, hi, cutoff, nl, prec="fp32", sum_mode=1, ref_sign=False):
+    """EAM forces over a full list.  ref_sign=True uses the reference's Verlet pair vector
+    p_j - p_i (reversed forces); the default p_i - p_j is the sign for which F = -grad E."""
     dt, ct, sfx = _real(prec)
     x = np.ascontiguousarray(pos, dtype=dt)
     counts, ids, codes = nl
@@ -184,9 +186,93 @@ def eam_force(path, pos, lo, hi, cutoff, nl, prec="fp32", sum_mode=1):
     rc = getattr(lib(), "oracle_eam_force_" + sfx)(
         str(path).encode(), ctypes.c_int64(n), _p(x, ct), _p(np.asarray(lo, np.float64), D),
         _p(np.asarray(hi, np.float64), D), D(cutoff), ctypes.c_int64(ids.shape[1]), _p(counts, I32),
-        _p(ids, I32), _p(codes, I32), int(sum_mode), _p(fp, D), _p(out, D))
+        _p(ids, I32), _p(codes, I32), int(sum_mode), _p(fp, D), _p(out, D), int(ref_sign))
     if rc:
         raise RuntimeError(f"oracle eam_force -> {rc}")
+    return out, fp
+
+
+def eam_energy(path, pos, lo, hi, cutoff, nl):
+    """FP64 EAM total energy (embedding + pair) over a full list."""
+    x = np.ascontiguousarray(pos, dtype=np.float64)
+    counts, ids, codes = nl
+    f = lib().oracle_eam_energy_f64
+    f.restype = ctypes.c_double
+    return f(str(path).encode(), ctypes.c_int64(x.shape[0]), _p(x, D), _p(np.asarray(lo, np.float64), D),
+             _p(np.asarray(hi, np.float64), D), D(cutoff), ctypes.c_int64(ids.shape[1]), _p(counts, I32),
+             _p(ids, I32), _p(codes, I32))
+
+
+def rbl_sizes(n, lo, hi, rs, rc, sample_num, eam=False, prec="fp32"):
+    """(rs_num, rc_num, pice_num) of the reference's RBL list sizing."""
+    out = np.zeros(3, np.int64)
+    lib().oracle_rbl_sizes(ctypes.c_int64(n), _p(np.asarray(lo, np.float64), D), _p(np.asarray(hi, np.float64), D),
+                           D(rs), D(rc), D(sample_num), int(eam), int(prec == "fp64"),
+                           out.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+    return tuple(int(v) for v in out)
+
+
+def rbl_list(pos, lo, hi, cutoff, rs, pice, core_cap, shell_cap, prec="fp32"):
+    """RBL core list + every pice-th shell pair in the reference's traversal order.
+    Returns (ncore, nshell, ids[n, core_cap + shell_cap], codes)."""
+    dt, ct, sfx = _real(prec)
+    x = np.ascontiguousarray(pos, dtype=dt)
+    n = x.shape[0]
+    ncore = np.zeros(n, np.int32)
+    nshell = np.zeros(n, np.int32)
+    ids = np.full((n, core_cap + shell_cap), -1, np.int32)
+    codes = np.zeros((n, core_cap + shell_cap), np.int32)
+    getattr(lib(), "oracle_rbl_list_" + sfx)(
+        ctypes.c_int64(n), _p(x, ct), _p(np.asarray(lo, np.float64), D), _p(np.asarray(hi, np.float64), D),
+        D(cutoff), D(rs), ctypes.c_int64(pice), ctypes.c_int64(core_cap), ctypes.c_int64(shell_cap),
+        _p(ncore, I32), _p(nshell, I32), _p(ids, I32), _p(codes, I32))
+    return ncore, nshell, ids, codes
+
+
+def rbl_table_g(dis):
+    """G of the reference's ERF table for a float distance (alpha 0.1, one value per bucket)."""
+    f = lib().oracle_rbl_table_g
+    f.restype = ctypes.c_float
+    f.argtypes = [ctypes.c_float]
+    return float(f(float(dis)))
+
+
+def rbl_near(pos, lo, hi, cutoff, rs, pice, rl, core_cap, *, type=None, mol=None, charge=None, eps=(1.0,),
+             sigma=(1.0,), with_coul=False, alpha=0.0, qqr2e=1.0, table_mode=0, shell_coul=1,
+             remove_mean=True, prec="fp32"):
+    dt, ct, sfx = _real(prec)
+    x = np.ascontiguousarray(pos, dtype=dt)
+    n = x.shape[0]
+    ncore, nshell, ids, codes = rl
+    shell_cap = ids.shape[1] - core_cap
+    out = np.zeros((n, 3))
+    t = None if type is None else np.ascontiguousarray(type, dtype=np.int32)
+    m = None if mol is None else np.ascontiguousarray(mol, dtype=np.int32)
+    q = None if charge is None else np.ascontiguousarray(charge, dtype=np.float64)
+    getattr(lib(), "oracle_rbl_near_" + sfx)(
+        ctypes.c_int64(n), _p(x, ct), _p(np.asarray(lo, np.float64), D), _p(np.asarray(hi, np.float64), D),
+        D(cutoff), D(rs), ctypes.c_int64(pice), _p(t, I32), _p(m, I32), _p(q, D),
+        _p(np.ascontiguousarray(eps, np.float64), D), _p(np.ascontiguousarray(sigma, np.float64), D),
+        ctypes.c_int64(core_cap), ctypes.c_int64(shell_cap), _p(ncore, I32), _p(nshell, I32), _p(ids, I32),
+        _p(codes, I32), int(with_coul), D(alpha), D(qqr2e), int(table_mode), int(shell_coul), int(remove_mean),
+        _p(out, D))
+    return out
+
+
+def rbl_eam(path, pos, lo, hi, cutoff, rs, pice, rl, core_cap, remove_mean=True, prec="fp32"):
+    dt, ct, sfx = _real(prec)
+    x = np.ascontiguousarray(pos, dtype=dt)
+    n = x.shape[0]
+    ncore, nshell, ids, codes = rl
+    fp = np.zeros(n)
+    out = np.zeros((n, 3))
+    rc = getattr(lib(), "oracle_rbl_eam_" + sfx)(
+        str(path).encode(), ctypes.c_int64(n), _p(x, ct), _p(np.asarray(lo, np.float64), D),
+        _p(np.asarray(hi, np.float64), D), D(cutoff), D(rs), ctypes.c_int64(pice), ctypes.c_int64(core_cap),
+        ctypes.c_int64(ids.shape[1] - core_cap), _p(ncore, I32), _p(nshell, I32), _p(ids, I32), _p(codes, I32),
+        int(remove_mean), _p(fp, D), _p(out, D))
+    if rc:
+        raise RuntimeError(f"oracle rbl_eam -> {rc}")
     return out, fp
 
 

@@ -854,7 +854,7 @@ template <class Real>
 static int eam_force_impl(const char* path, int64_t n, const Real* pos, const double* lo,
                           const double* hi, double cutoff, int64_t cap, const int32_t* counts,
                           const int32_t* ids, const int32_t* codes, int sum_mode, double* fp_out,
-                          double* force_out) {
+                          double* force_out, int ref_sign) {
   EamTables t;
   int rc0 = eam_load(path, t);
   if (rc0) return rc0;
@@ -906,8 +906,12 @@ static int eam_force_impl(const char* path, int64_t n, const Real* pos, const do
       Real off[3];
       shift_offset(g, codes[i * cap + p], off);
       Real pj[3] = {pos[3 * j] - off[0], pos[3 * j + 1] - off[1], pos[3 * j + 2] - off[2]};
+      // ref_sign: the reference's MinDistanceVec(p_j, p_i) (RunWorklet.cpp:402), which reverses
+      // the force; otherwise p_i - p_j as in LAMMPS' pair_eam and the reference's own RBL pass
+      // (RunWorklet.cpp:1180), the sign for which F = -grad E.
       Real r[3];
-      min_dist(pj, pos + 3 * i, g.box, r);
+      if (ref_sign) min_dist(pj, pos + 3 * i, g.box, r);
+      else min_dist(pos + 3 * i, pj, g.box, r);
       Real rsq = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
       Real cutsq = rc * rc;
       Real f[3] = {0, 0, 0};
@@ -942,16 +946,66 @@ static int eam_force_impl(const char* path, int64_t n, const Real* pos, const do
 EXPORT int oracle_eam_force_f32(const char* path, int64_t n, const float* pos, const double* lo,
                                 const double* hi, double cutoff, int64_t cap, const int32_t* counts,
                                 const int32_t* ids, const int32_t* codes, int sum_mode,
-                                double* fp_out, double* force_out) {
+                                double* fp_out, double* force_out, int ref_sign) {
   return eam_force_impl<float>(path, n, pos, lo, hi, cutoff, cap, counts, ids, codes, sum_mode,
-                               fp_out, force_out);
+                               fp_out, force_out, ref_sign);
 }
 EXPORT int oracle_eam_force_f64(const char* path, int64_t n, const double* pos, const double* lo,
                                 const double* hi, double cutoff, int64_t cap,
                                 const int32_t* counts, const int32_t* ids, const int32_t* codes,
-                                int sum_mode, double* fp_out, double* force_out) {
+                                int sum_mode, double* fp_out, double* force_out, int ref_sign) {
   return eam_force_impl<double>(path, n, pos, lo, hi, cutoff, cap, counts, ids, codes, sum_mode,
-                                fp_out, force_out);
+                                fp_out, force_out, ref_sign);
+}
+
+// EAM total energy sum_i F(rho_i) + 1/2 sum_ij phi(r_ij) in FP64 over a full list, with the
+// value coefficients (3..6) of the same splines (ComputeEAMrhoOUT and the energy terms of
+// ThermoOutput, rbmd/framework/forceFunction/ExecForceFunction.h:522-613); the finite-difference
+// check of the force sign uses it.
+EXPORT double oracle_eam_energy_f64(const char* path, int64_t n, const double* pos, const double* lo,
+                                    const double* hi, double cutoff, int64_t cap,
+                                    const int32_t* counts, const int32_t* ids, const int32_t* codes) {
+  EamTables t;
+  if (eam_load(path, t)) return NAN;
+  Grid<double> g = make_grid<double>(lo, hi, cutoff, cutoff);
+  auto C = [&](const std::vector<float>& s, int64_t m, int c) -> double { return (double)s[7 * m + c]; };
+  double e = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    double rho = 0, pair = 0;
+    for (int32_t p = 0; p < counts[i]; ++p) {
+      int j = ids[i * cap + p];
+      double off[3];
+      shift_offset(g, codes[i * cap + p], off);
+      double pj[3] = {pos[3 * j] - off[0], pos[3 * j + 1] - off[1], pos[3 * j + 2] - off[2]};
+      double r[3];
+      min_dist(pos + 3 * i, pj, g.box, r);
+      double rsq = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+      if (rsq < cutoff * cutoff && rsq > 0.01) {
+        double rv = std::sqrt(rsq);
+        double pp = rv / (double)t.dr + 1.0;
+        int64_t m = std::min<int64_t>((int64_t)pp, t.nr - 1);
+        pp -= (double)m;
+        pp = std::min(pp, 1.0);
+        rho += ((C(t.rhor_spl, m, 3) * pp + C(t.rhor_spl, m, 4)) * pp + C(t.rhor_spl, m, 5)) * pp +
+               C(t.rhor_spl, m, 6);
+        double z2 = ((C(t.z2r_spl, m, 3) * pp + C(t.z2r_spl, m, 4)) * pp + C(t.z2r_spl, m, 5)) * pp +
+                    C(t.z2r_spl, m, 6);
+        pair += z2 / rv;
+      }
+    }
+    double pp = rho / (double)t.drho + 1.0;
+    int m = std::max(1, std::min((int)pp, t.nrho - 1));
+    pp -= m;
+    pp = std::min(pp, 1.0);
+    double F = ((C(t.frho_spl, m, 3) * pp + C(t.frho_spl, m, 4)) * pp + C(t.frho_spl, m, 5)) * pp +
+               C(t.frho_spl, m, 6);
+    if (rho > t.rhomax) {
+      double fp = (C(t.frho_spl, m, 0) * pp + C(t.frho_spl, m, 1)) * pp + C(t.frho_spl, m, 2);
+      F += fp * (rho - t.rhomax);
+    }
+    e += F + 0.5 * pair;
+  }
+  return e;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1199,4 +1253,368 @@ EXPORT void oracle_set_threads(int n) {
 #else
   (void)n;
 #endif
+}
+
+// ==========================================================================================
+// RBL (random batch list) near field.
+//   * list sizes: ExecutionMD::ComputeRBLNearForce / ComputeRBLLJForce / ComputeRBLEAMForce
+//     (rbmd/framework/run/ExecutionMD.cpp:460-801): rho_system = N / (Lx Ly Lz) in Real,
+//     rs_num = round(1 + 0.05/rho - 0.05) * rho * ceil(4/3 pi rs^3) + 1 (no round factor for
+//     EAM), rc_num likewise, pice_num = ceil(1 / (sample_num / (rc_num - rs_num)));
+//   * list: ComputeRBLNeighboursOnceWorklet (rbmd/framework/run/worklet/RunWorklet.cpp:634-708):
+//     stencil x offset outermost, z innermost, points of a cell in sorted order; a candidate is a
+//     shell pair when rc^2 - d^2 > 1e-4 && d^2 - rs^2 > 1e-4 and is kept when its running shell
+//     index is a multiple of pice_num; otherwise a core pair when rs^2 - d^2 > 1e-4 && d^2 > 1e-4;
+//   * forces: ComputeNearForceRBLERFWorklet (:710-814) and ComputeLJForceRBLWorklet
+//     (:1218-1302): core Coulomb -q_i q_j G(d) r/d for 1e-4 < d^2 < rc^2 on p_j' - p_i (G from the
+//     ERF table at |MinDistanceVec|), core LJ (ComputeLJForce), shell LJ x pice_num
+//     (ComputeLJForceRcs: rs^2 < d^2 < rc^2), LJ skipped within a molecule; corr = LJ + qqr2e * Coul;
+//   * EAM: ComputeEAMfp_Worklet / ComputeEAMRBLWorklet (:1052-1216) with ComputeEAMrhoRs and
+//     ComputeEAMforceRBL (rbmd/framework/forceFunction/ExecForceFunction.h:358-381,484-520);
+//   * mean removal: F_i = corr_i - (sum_j corr_j) / N (SumRBLCorrForceWorklet, RunWorklet.cpp:1304-1321).
+// Reference quirks kept behind switches: table_mode 1 takes G from the reference's ERF table
+// (alpha fixed at 0.1, one value per distance bucket, rbmd/framework/staticTable/
+// ExecStaticTable.h:37-39,96-135); shell_coul 0 drops the shell Coulomb term, whose value the
+// reference computes and discards (RunWorklet.cpp:782).  Defaults of the library: table_mode 0
+// (G at the configured alpha and the exact distance) and shell_coul 1 (shell Coulomb x pice_num).
+// ==========================================================================================
+struct RblSizes { int64_t rs_num, rc_num, pice_num; };
+
+template <class Real>
+RblSizes rbl_sizes(int64_t n, const Real* box, double rs, double rc, double sample_num, bool eam) {
+  const Real rho = (Real)n / (box[0] * box[1] * box[2]);
+  const float pif = 3.14159265358979323846f;
+  const Real rs_r = (Real)rs, rc_r = (Real)rc;
+  int64_t coeff = 1;
+  if (!eam) {
+    const Real c = (Real)(1.0 + (0.05 / (double)rho - 0.05));
+    coeff = (int64_t)std::round(c);
+  }
+  const double cs = std::ceil(4.0 / 3.0 * (double)pif * (double)rs_r * (double)rs_r * (double)rs_r);
+  const double cc = std::ceil(4.0 / 3.0 * (double)pif * (double)rc_r * (double)rc_r * (double)rc_r);
+  RblSizes z;
+  z.rs_num = (int64_t)((double)(eam ? rho : (Real)coeff * rho) * cs + 1);
+  z.rc_num = (int64_t)((double)(eam ? rho : (Real)coeff * rho) * cc + 1);
+  const Real rate = (Real)sample_num / (Real)(z.rc_num - z.rs_num);
+  z.pice_num = (int64_t)std::ceil(1.0 / (double)rate);
+  return z;
+}
+
+template <class Real>
+void rbl_list(const Grid<Real>& g, const Cells<Real>& c, int64_t n, const Real* pos, double cutoff,
+              double rs, int64_t pice, int64_t core_cap, int64_t shell_cap, int32_t* ncore,
+              int32_t* nshell, int32_t* ids, int32_t* codes) {
+  const Real rc = (Real)cutoff, r_s = (Real)rs;
+  const Real rc_2 = rc * rc, rs_2 = r_s * r_s;
+  const int nc = g.num_cycles;
+  const int64_t row = core_cap + shell_cap;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t a = 0; a < n; ++a) {
+    const Real* pi = pos + 3 * a;
+    int ci[3];
+    for (int d = 0; d < 3; ++d) ci[d] = (int)((pi[d] - g.lo[d]) / g.dx[d]);
+    int64_t index_shell = 0, index_random = 0, index_rs = 0;
+    for (int i = -nc; i <= nc; ++i)
+      for (int j = -nc; j <= nc; ++j)
+        for (int k = -nc; k <= nc; ++k) {
+          int nb[3] = {ci[0] + i, ci[1] + j, ci[2] + k};
+          Real off[3];
+          int code = 0, w[3];
+          for (int d = 0; d < 3; ++d) {
+            w[d] = ((nb[d] % g.dims[d]) + g.dims[d]) % g.dims[d];
+            int delta = w[d] - nb[d];
+            off[d] = g.dx[d] * (Real)delta;             // PeriodicCoordOffset
+            int cd = delta > 0 ? 1 : (delta < 0 ? 2 : 0);
+            code |= cd << (2 * d);
+          }
+          int cell = w[0] + w[1] * g.dims[0] + w[2] * g.dims[0] * g.dims[1];
+          for (int s = c.lower[cell]; s < c.upper[cell]; ++s) {
+            int jd = c.point_ids[s];
+            const Real* pj = pos + 3 * jd;
+            Real r0 = (pj[0] - off[0]) - pi[0];
+            Real r1 = (pj[1] - off[1]) - pi[1];
+            Real r2 = (pj[2] - off[2]) - pi[2];
+            const Real dis_2 = r0 * r0 + r1 * r1 + r2 * r2;
+            if ((double)(rc_2 - dis_2) > 0.0001 && (double)(dis_2 - rs_2) > 0.0001) {
+              if (index_shell % pice == 0) {
+                if (index_random < shell_cap) {
+                  ids[a * row + core_cap + index_random] = jd;
+                  codes[a * row + core_cap + index_random] = code;
+                }
+                ++index_random;
+              }
+              ++index_shell;
+            } else if ((double)(rs_2 - dis_2) > 0.0001 && (double)dis_2 > 0.0001) {
+              if (index_rs < core_cap) {
+                ids[a * row + index_rs] = jd;
+                codes[a * row + index_rs] = code;
+              }
+              ++index_rs;
+            }
+          }
+        }
+    ncore[a] = (int32_t)index_rs;
+    nshell[a] = (int32_t)index_random;
+  }
+}
+
+// The reference's ERF table (rbmd/framework/model/ERFTable.h via ExecStaticTable::Extract /
+// TableGnearValue, rbmd/framework/staticTable/ExecStaticTable.h:37-39,96-135): the entry of a
+// float distance is its bits 15..25; the entry's value is the reference's float Gnear(0.1, d_k)
+// with d_k the entry's lower bucket edge rounded up to 4 decimals (d < 2) or 3 decimals (d >= 2),
+// and at least 0.1.  The reference's tables hold entries for 0.1 <= d < 12 only; outside, this
+// evaluates G(0.1, d) in FP64 (the reference would read past its arrays).
+inline float rbl_table_g(float dis) {
+  if (!(dis >= 0.1f && dis < 12.0f)) {
+    const double d = dis;
+    return (float)gnear_fp64<double>(0.1, d);
+  }
+  uint32_t full;
+  std::memcpy(&full, &dis, 4);
+  const uint32_t edge_bits = full & ~0x7FFFu;
+  float edge;
+  std::memcpy(&edge, &edge_bits, 4);
+  const int dec = dis < 2.0f ? 4 : 3;
+  const double sc = std::pow(10.0, dec);
+  const double v = (double)edge * sc, rv = std::nearbyint(v);
+  double d = (std::fabs(v - rv) < 1e-6 ? rv : std::ceil(v)) / sc;
+  if (d < 0.1) d = 0.1;
+  return gnear<float>(0.1f, (float)d);
+}
+
+template <class Real>
+static void rbl_near_impl(int64_t n, const Real* pos, const double* lo, const double* hi,
+                          double cutoff, double rs, int64_t pice, const int32_t* type,
+                          const int32_t* mol, const double* charge, const double* eps,
+                          const double* sig, int64_t core_cap, int64_t shell_cap,
+                          const int32_t* ncore, const int32_t* nshell, const int32_t* ids,
+                          const int32_t* codes, int with_coul, double alpha, double qqr2e,
+                          int table_mode, int shell_coul, int remove_mean, double* force_out) {
+  Grid<Real> g = make_grid<Real>(lo, hi, cutoff, rs);
+  const Real rc = (Real)cutoff, r_s = (Real)rs, a = (Real)alpha;
+  const int64_t row = core_cap + shell_cap;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t i = 0; i < n; ++i) {
+    const Real* pi = pos + 3 * i;
+    int ti = type ? type[i] : 0;
+    int64_t mi = mol ? mol[i] : i;
+    const Real eps_i = (Real)eps[ti], sig_i = (Real)sig[ti];
+    const Real qi = charge ? (Real)charge[i] : (Real)0;
+    double lj[3] = {0, 0, 0}, el[3] = {0, 0, 0};
+    auto pair = [&](int64_t slot, bool shell) {
+      const int j = ids[i * row + slot];
+      Real off[3];
+      shift_offset(g, codes[i * row + slot], off);
+      Real pj[3] = {pos[3 * j] - off[0], pos[3 * j + 1] - off[1], pos[3 * j + 2] - off[2]};
+      const int tj = type ? type[j] : 0;
+      const int64_t mj = mol ? mol[j] : j;
+      Real rm[3];
+      min_dist(pj, pi, g.box, rm);
+      if (with_coul && (!shell || shell_coul)) {
+        const Real qj = charge ? (Real)charge[j] : (Real)0;
+        Real r[3] = {pj[0] - pi[0], pj[1] - pi[1], pj[2] - pi[2]};
+        const Real d2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+        const Real dis = (Real)std::sqrt(d2);
+        const Real dism = (Real)std::sqrt(rm[0] * rm[0] + rm[1] * rm[1] + rm[2] * rm[2]);
+        bool ok = shell ? (d2 < rc * rc && d2 > r_s * r_s) : (d2 < rc * rc && (double)d2 > 0.0001);
+        if (ok) {
+          Real gv;
+          if (table_mode) gv = (Real)rbl_table_g((float)dism);
+          else gv = sizeof(Real) == 4 ? gnear<Real>(a, dism) : gnear_fp64<Real>(a, dism);
+          const Real sc = -qi * qj * gv;
+          const Real w = shell ? (Real)pice : (Real)1;
+          for (int d = 0; d < 3; ++d) el[d] += (double)(w * (sc * r[d] / dis));
+        }
+      }
+      if (mi == mj) return;
+      Real f[3] = {0, 0, 0};
+      if (!shell) {
+        lj_force(rm, eps_i, (Real)eps[tj], sig_i, (Real)sig[tj], rc, f);
+      } else {
+        const Real d2 = rm[0] * rm[0] + rm[1] * rm[1] + rm[2] * rm[2];
+        if (d2 < rc * rc && d2 > r_s * r_s) {
+          Real sg = (sig_i + (Real)sig[tj]) / 2;
+          Real s6 = sg * sg * sg * sg * sg * sg;
+          Real d6 = d2 * d2 * d2;
+          Real sd6 = s6 / d6;
+          Real scal = (Real)(-24) * (Real)std::sqrt(eps_i * (Real)eps[tj]) * (((Real)2 * sd6 - (Real)1) * sd6) / d2;
+          for (int d = 0; d < 3; ++d) f[d] = (Real)pice * (scal * rm[d]);
+        }
+      }
+      for (int d = 0; d < 3; ++d) lj[d] += (double)f[d];
+    };
+    for (int32_t p = 0; p < std::min<int64_t>(ncore[i], core_cap); ++p) pair(p, false);
+    for (int32_t p = 0; p < std::min<int64_t>(nshell[i], shell_cap); ++p) pair(core_cap + p, true);
+    for (int d = 0; d < 3; ++d) force_out[3 * i + d] = lj[d] + qqr2e * el[d];
+  }
+  if (remove_mean) {
+    double m[3] = {0, 0, 0};
+    for (int64_t i = 0; i < n; ++i)
+      for (int d = 0; d < 3; ++d) m[d] += force_out[3 * i + d];
+    for (int64_t i = 0; i < n; ++i)
+      for (int d = 0; d < 3; ++d) force_out[3 * i + d] -= m[d] / (double)n;
+  }
+}
+
+template <class Real>
+static int rbl_eam_impl(const char* path, int64_t n, const Real* pos, const double* lo, const double* hi,
+                        double cutoff, double rs, int64_t pice, int64_t core_cap, int64_t shell_cap,
+                        const int32_t* ncore, const int32_t* nshell, const int32_t* ids,
+                        const int32_t* codes, int remove_mean, double* fp_out, double* force_out) {
+  EamTables t;
+  int rc0 = eam_load(path, t);
+  if (rc0) return rc0;
+  Grid<Real> g = make_grid<Real>(lo, hi, cutoff, rs);
+  const Real rc = (Real)cutoff, r_s = (Real)rs;
+  const int64_t row = core_cap + shell_cap;
+  std::vector<Real> fp(n);
+  const Real rdr = (Real)1 / (Real)t.dr, rdrho = (Real)1 / (Real)t.drho;
+  auto C = [&](const std::vector<float>& s, int64_t m, int c) -> Real { return (Real)s[7 * m + c]; };
+  auto pj_of = [&](int64_t i, int64_t slot, Real* pj) {
+    const int j = ids[i * row + slot];
+    Real off[3];
+    shift_offset(g, codes[i * row + slot], off);
+    for (int d = 0; d < 3; ++d) pj[d] = pos[3 * j + d] - off[d];
+    return j;
+  };
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t i = 0; i < n; ++i) {
+    double rhod = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+      const int64_t cnt = pass == 0 ? std::min<int64_t>(ncore[i], core_cap) : std::min<int64_t>(nshell[i], shell_cap);
+      for (int64_t p = 0; p < cnt; ++p) {
+        Real pj[3];
+        pj_of(i, pass == 0 ? p : core_cap + p, pj);
+        Real r[3];
+        min_dist(pos + 3 * i, pj, g.box, r);
+        const Real rsq = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+        const bool ok = pass == 0 ? (rsq < rc * rc && (double)rsq > 0.01) : (rsq < rc * rc && rsq > r_s * r_s);
+        if (!ok) continue;
+        double pp = (double)((Real)std::sqrt(rsq) * rdr) + 1.0;
+        int64_t m = std::min<int64_t>((int64_t)pp, t.nr - 1);
+        pp -= (double)m;
+        pp = std::min(pp, 1.0);
+        Real v = (Real)(((C(t.rhor_spl, m, 3) * pp + C(t.rhor_spl, m, 4)) * pp + C(t.rhor_spl, m, 5)) * pp +
+                        C(t.rhor_spl, m, 6));
+        rhod += pass == 0 ? (double)v : (double)((Real)pice * v);
+      }
+    }
+    const Real rr = (Real)rhod;
+    double pp = (double)(rr * rdrho) + 1.0;
+    int m = std::max(1, std::min((int)pp, t.nrho - 1));
+    pp -= m;
+    pp = std::min(pp, 1.0);
+    fp[i] = (Real)((C(t.frho_spl, m, 0) * pp + C(t.frho_spl, m, 1)) * pp + C(t.frho_spl, m, 2));
+    if (fp_out) fp_out[i] = (double)fp[i];
+  }
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t i = 0; i < n; ++i) {
+    double acc[3] = {0, 0, 0};
+    for (int pass = 0; pass < 2; ++pass) {
+      const int64_t cnt = pass == 0 ? std::min<int64_t>(ncore[i], core_cap) : std::min<int64_t>(nshell[i], shell_cap);
+      for (int64_t p = 0; p < cnt; ++p) {
+        Real pj[3];
+        const int j = pj_of(i, pass == 0 ? p : core_cap + p, pj);
+        Real r[3];
+        min_dist(pos + 3 * i, pj, g.box, r);   // MinDistanceVec(p_i, p_j) (RunWorklet.cpp:1180)
+        const Real rsq = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+        const bool ok = pass == 0 ? (rsq < rc * rc && (double)rsq > 0.01) : (rsq < rc * rc && rsq > r_s * r_s);
+        if (!ok) continue;
+        Real rv = (Real)std::sqrt(rsq);
+        double pp = (double)(rv * rdr) + 1.0;
+        int m = std::min((int)pp, t.nr - 1);
+        pp -= m;
+        pp = std::min(pp, 1.0);
+        double rhop = (C(t.rhor_spl, m, 0) * pp + C(t.rhor_spl, m, 1)) * pp + C(t.rhor_spl, m, 2);
+        double z2p = (C(t.z2r_spl, m, 0) * pp + C(t.z2r_spl, m, 1)) * pp + C(t.z2r_spl, m, 2);
+        double z2 = ((C(t.z2r_spl, m, 3) * pp + C(t.z2r_spl, m, 4)) * pp + C(t.z2r_spl, m, 5)) * pp +
+                    C(t.z2r_spl, m, 6);
+        double recip = 1.0 / (double)rv;
+        double phi = z2 * recip;
+        double phip = z2p * recip - phi * recip;
+        double psip = (double)fp[i] * rhop + (double)fp[j] * rhop + phip;
+        double fpair = -psip * recip;
+        for (int d = 0; d < 3; ++d) {
+          Real f = (Real)((double)r[d] * fpair);
+          acc[d] += pass == 0 ? (double)f : (double)((Real)pice * f);
+        }
+      }
+    }
+    for (int d = 0; d < 3; ++d) force_out[3 * i + d] = acc[d];
+  }
+  if (remove_mean) {
+    double mm[3] = {0, 0, 0};
+    for (int64_t i = 0; i < n; ++i)
+      for (int d = 0; d < 3; ++d) mm[d] += force_out[3 * i + d];
+    for (int64_t i = 0; i < n; ++i)
+      for (int d = 0; d < 3; ++d) force_out[3 * i + d] -= mm[d] / (double)n;
+  }
+  return 0;
+}
+
+template <class Real>
+static void rbl_list_impl(int64_t n, const Real* pos, const double* lo, const double* hi, double cutoff,
+                          double rs, int64_t pice, int64_t core_cap, int64_t shell_cap, int32_t* ncore,
+                          int32_t* nshell, int32_t* ids, int32_t* codes) {
+  Grid<Real> g = make_grid<Real>(lo, hi, cutoff, rs);
+  Cells<Real> c = build_cells(g, n, pos);
+  rbl_list(g, c, n, pos, cutoff, rs, pice, core_cap, shell_cap, ncore, nshell, ids, codes);
+}
+
+EXPORT void oracle_rbl_sizes(int64_t n, const double* lo, const double* hi, double rs, double rc,
+                             double sample_num, int eam, int fp64, int64_t* out) {
+  RblSizes z;
+  if (fp64) {
+    double box[3] = {hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]};
+    z = rbl_sizes<double>(n, box, rs, rc, sample_num, eam != 0);
+  } else {
+    float box[3] = {(float)hi[0] - (float)lo[0], (float)hi[1] - (float)lo[1], (float)hi[2] - (float)lo[2]};
+    z = rbl_sizes<float>(n, box, rs, rc, sample_num, eam != 0);
+  }
+  out[0] = z.rs_num; out[1] = z.rc_num; out[2] = z.pice_num;
+}
+EXPORT void oracle_rbl_list_f32(int64_t n, const float* pos, const double* lo, const double* hi, double cutoff,
+                                double rs, int64_t pice, int64_t core_cap, int64_t shell_cap, int32_t* ncore,
+                                int32_t* nshell, int32_t* ids, int32_t* codes) {
+  rbl_list_impl<float>(n, pos, lo, hi, cutoff, rs, pice, core_cap, shell_cap, ncore, nshell, ids, codes);
+}
+EXPORT void oracle_rbl_list_f64(int64_t n, const double* pos, const double* lo, const double* hi, double cutoff,
+                                double rs, int64_t pice, int64_t core_cap, int64_t shell_cap, int32_t* ncore,
+                                int32_t* nshell, int32_t* ids, int32_t* codes) {
+  rbl_list_impl<double>(n, pos, lo, hi, cutoff, rs, pice, core_cap, shell_cap, ncore, nshell, ids, codes);
+}
+EXPORT float oracle_rbl_table_g(float dis) { return rbl_table_g(dis); }
+EXPORT void oracle_rbl_near_f32(int64_t n, const float* pos, const double* lo, const double* hi, double cutoff,
+                                double rs, int64_t pice, const int32_t* type, const int32_t* mol,
+                                const double* charge, const double* eps, const double* sig, int64_t core_cap,
+                                int64_t shell_cap, const int32_t* ncore, const int32_t* nshell,
+                                const int32_t* ids, const int32_t* codes, int with_coul, double alpha,
+                                double qqr2e, int table_mode, int shell_coul, int remove_mean, double* out) {
+  rbl_near_impl<float>(n, pos, lo, hi, cutoff, rs, pice, type, mol, charge, eps, sig, core_cap, shell_cap,
+                       ncore, nshell, ids, codes, with_coul, alpha, qqr2e, table_mode, shell_coul,
+                       remove_mean, out);
+}
+EXPORT void oracle_rbl_near_f64(int64_t n, const double* pos, const double* lo, const double* hi, double cutoff,
+                                double rs, int64_t pice, const int32_t* type, const int32_t* mol,
+                                const double* charge, const double* eps, const double* sig, int64_t core_cap,
+                                int64_t shell_cap, const int32_t* ncore, const int32_t* nshell,
+                                const int32_t* ids, const int32_t* codes, int with_coul, double alpha,
+                                double qqr2e, int table_mode, int shell_coul, int remove_mean, double* out) {
+  rbl_near_impl<double>(n, pos, lo, hi, cutoff, rs, pice, type, mol, charge, eps, sig, core_cap, shell_cap,
+                        ncore, nshell, ids, codes, with_coul, alpha, qqr2e, table_mode, shell_coul,
+                        remove_mean, out);
+}
+EXPORT int oracle_rbl_eam_f32(const char* path, int64_t n, const float* pos, const double* lo, const double* hi,
+                              double cutoff, double rs, int64_t pice, int64_t core_cap, int64_t shell_cap,
+                              const int32_t* ncore, const int32_t* nshell, const int32_t* ids,
+                              const int32_t* codes, int remove_mean, double* fp_out, double* force_out) {
+  return rbl_eam_impl<float>(path, n, pos, lo, hi, cutoff, rs, pice, core_cap, shell_cap, ncore, nshell, ids,
+                             codes, remove_mean, fp_out, force_out);
+}
+EXPORT int oracle_rbl_eam_f64(const char* path, int64_t n, const double* pos, const double* lo, const double* hi,
+                              double cutoff, double rs, int64_t pice, int64_t core_cap, int64_t shell_cap,
+                              const int32_t* ncore, const int32_t* nshell, const int32_t* ids,
+                              const int32_t* codes, int remove_mean, double* fp_out, double* force_out) {
+  return rbl_eam_impl<double>(path, n, pos, lo, hi, cutoff, rs, pice, core_cap, shell_cap, ncore, nshell, ids,
+                              codes, remove_mean, fp_out, force_out);
 }

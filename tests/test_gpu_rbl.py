@@ -1,0 +1,151 @@
+"""GPU parity of the RBL near field (neighbor.type "RBL") against the CPU oracle.
+
+Bars:
+* lists: per atom the core pairs and the kept shell pairs equal the oracle's, in the same order
+  (the reference's traversal order decides which shell pairs are kept), FP32 and FP64;
+* pice_num and the reference's rs_num / rc_num equal the oracle's;
+* forces (near part after mean removal, plus the RBE far part with injected k-samples):
+  max_i |dF_i| / rms|F| <= 1e-5 in FP32 and <= 1e-11 in FP64, in the default mode (G at the
+  configured alpha, shell Coulomb x pice) and with the reference's ERF table and dropped shell
+  Coulomb (compat flags);
+* EAM over RBL lists, and the Verlet EAM force with the reference's reversed pair vector.
+"""
+import numpy as np
+import pytest
+
+from copy_gpu_b200 import systems
+from tests.helpers import make_ff, rel_err, to_dev
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp32": 1e-5, "fp64": 1e-11}
+RS, RC, SAMPLE = 1.25, 2.5, 10
+
+
+def _posr(pos, prec):
+    return pos.astype(np.float32) if prec == "fp32" else pos.astype(np.float64)
+
+
+def _rbl_cfg(prec, compat=None, P=32):
+    cfg = systems.electrolyte_config(P=P, precision=prec)
+    cfg["hyper_parameters"]["neighbor"] = {"type": "RBL", "cut_off": RC, "r_core": RS,
+                                           "neighbor_sample_num": SAMPLE}
+    if compat:
+        cfg["compat"] = compat
+    return cfg
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_rbl_lists_match_oracle(cuda, oracle_lib, prec):
+    import torch
+    s = systems.electrolyte(3000, seed=21)
+    cfg = _rbl_cfg(prec)
+    alpha = cfg["hyper_parameters"]["coulomb"]["alpha"]
+    m = oracle_lib.rbe_sample(alpha, s["hi"] - s["lo"], seed=3, step=0, rep=0, P=32)
+    dev = to_dev(s, cuda)
+    ff = make_ff(cfg, s, dev)
+    ff.set_ksamples(m)
+    ff.Execute()
+    torch.cuda.synchronize()
+    assert ff.status() == 0
+    ncore, nshell, sizes = ff.rbl_lists()
+    rs_num, rc_num, pice = oracle_lib.rbl_sizes(len(s["pos"]), s["lo"], s["hi"], RS, RC, SAMPLE, prec=prec)
+    assert sizes[:3] == (rs_num, rc_num, pice)
+    assert pice > 1
+    pr = _posr(s["pos"], prec)
+    oc, osh, oids, _ = oracle_lib.rbl_list(pr, s["lo"], s["hi"], RC, RS, pice, 96, 96, prec=prec)
+    assert np.array_equal(ncore, oc) and np.array_equal(nshell, osh)
+    cap = int((ncore + nshell).max()) + 1
+    counts, ids = ff.neighbors(cap)
+    for i in range(len(pr)):
+        ref = np.concatenate([oids[i, :oc[i]], oids[i, 96:96 + osh[i]]])
+        assert np.array_equal(ids[i, :counts[i]], ref), f"atom {i}"
+
+
+@pytest.mark.parametrize("prec,compat", [("fp32", None), ("fp64", None),
+                                         ("fp32", {"rbl_erf_table": True, "rbl_drop_shell_coulomb": True}),
+                                         ("fp64", {"rbl_drop_shell_coulomb": True})])
+def test_rbl_force_matches_oracle(cuda, oracle_lib, prec, compat):
+    import torch
+    s = systems.electrolyte(3000, seed=22)
+    P = 48
+    cfg = _rbl_cfg(prec, compat, P=P)
+    alpha = cfg["hyper_parameters"]["coulomb"]["alpha"]
+    L = s["hi"] - s["lo"]
+    m = oracle_lib.rbe_sample(alpha, L, seed=8, step=0, rep=0, P=P)
+    dev = to_dev(s, cuda)
+    ff = make_ff(cfg, s, dev)
+    ff.set_ksamples(m)
+    ff.Execute()
+    torch.cuda.synchronize()
+    assert ff.status() == 0
+    pice = ff.rbl_lists()[2][2]
+    pr = _posr(s["pos"], prec)
+    rl = oracle_lib.rbl_list(pr, s["lo"], s["hi"], RC, RS, pice, 96, 96, prec=prec)
+    compat = compat or {}
+    near = oracle_lib.rbl_near(pr, s["lo"], s["hi"], RC, RS, pice, rl, 96, type=s["type"], charge=s["charge"],
+                               eps=s["eps"], sigma=s["sigma"], with_coul=True, alpha=alpha, qqr2e=1.0,
+                               table_mode=int(compat.get("rbl_erf_table", False)),
+                               shell_coul=0 if compat.get("rbl_drop_shell_coulomb") else 1, prec=prec)
+    rho = oracle_lib.rhok(s["pos"], s["charge"], L, m, prec="fp64")
+    far = oracle_lib.rbe_force(s["pos"], s["charge"], L, alpha, 1.0, m, rho, prec="fp64")
+    err = rel_err(dev["force"].cpu().numpy(), near + far)
+    assert err <= TOL[prec], f"RBL total force rel err {err:.3e}"
+
+
+def test_rbl_lj_only_mean_removed(cuda, oracle_lib):
+    """LJ/CUT over RBL lists (ComputeLJForceRBLWorklet): forces match and sum to zero."""
+    import torch
+    s = systems.lj_fcc(ncell=8, seed=6)
+    cfg = systems.lj_config(cutoff=RC, precision="fp32")
+    cfg["hyper_parameters"]["neighbor"] = {"type": "RBL", "cut_off": RC, "r_core": RS, "neighbor_sample_num": 12}
+    dev = to_dev(s, cuda)
+    ff = make_ff(cfg, s, dev)
+    ff.Execute()
+    torch.cuda.synchronize()
+    assert ff.status() == 0
+    pice = ff.rbl_lists()[2][2]
+    pr = s["pos"].astype(np.float32)
+    rl = oracle_lib.rbl_list(pr, s["lo"], s["hi"], RC, RS, pice, 96, 96)
+    ref = oracle_lib.rbl_near(pr, s["lo"], s["hi"], RC, RS, pice, rl, 96)
+    got = dev["force"].cpu().numpy()
+    assert rel_err(got, ref) <= 1e-5
+    assert np.abs(got.sum(0)).max() <= 1e-9 * len(got) * np.abs(got).max()
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_rbl_eam_matches_oracle(cuda, oracle_lib, tmp_path, prec):
+    import torch
+    pot = systems.write_johnson_funcfl(str(tmp_path / "johnson.eam"))
+    s = systems.eam_fcc(ncell=8, seed=7)
+    cfg = systems.eam_config(pot, precision=prec)
+    cfg["hyper_parameters"]["neighbor"] = {"type": "RBL", "cut_off": 5.0, "r_core": 3.0, "neighbor_sample_num": 20}
+    dev = to_dev(s, cuda)
+    ff = make_ff(cfg, s, dev)
+    ff.Execute()
+    torch.cuda.synchronize()
+    assert ff.status() == 0
+    pice = ff.rbl_lists()[2][2]
+    rs_num, rc_num, pice_ref = oracle_lib.rbl_sizes(len(s["pos"]), s["lo"], s["hi"], 3.0, 5.0, 20, eam=True, prec=prec)
+    assert pice == pice_ref and pice > 1
+    pr = _posr(s["pos"], prec)
+    rl = oracle_lib.rbl_list(pr, s["lo"], s["hi"], 5.0, 3.0, pice, 96, 96, prec=prec)
+    ref, _ = oracle_lib.rbl_eam(pot, pr, s["lo"], s["hi"], 5.0, 3.0, pice, rl, 96, prec=prec)
+    err = rel_err(dev["force"].cpu().numpy(), ref)
+    assert err <= (1e-5 if prec == "fp32" else 1e-11), err
+
+
+def test_eam_verlet_reference_pair_vector(cuda, oracle_lib, tmp_path):
+    """compat.eam_verlet_pair_vector reproduces the reference's reversed Verlet EAM force."""
+    import torch
+    pot = systems.write_johnson_funcfl(str(tmp_path / "johnson.eam"))
+    s = systems.eam_fcc(ncell=6, seed=5)
+    cfg = systems.eam_config(pot, precision="fp64")
+    cfg["compat"] = {"eam_verlet_pair_vector": True}
+    dev = to_dev(s, cuda)
+    ff = make_ff(cfg, s, dev)
+    ff.Execute()
+    torch.cuda.synchronize()
+    nl = oracle_lib.neighbors(s["pos"], s["lo"], s["hi"], 5.0, "fp64")
+    ref, _ = oracle_lib.eam_force(pot, s["pos"], s["lo"], s["hi"], 5.0, nl, prec="fp64", ref_sign=True)
+    assert rel_err(dev["force"].cpu().numpy(), ref) <= 1e-11
