@@ -41,7 +41,8 @@ EXPORTED = [
     "rbmd_force_sync_velocities", "rbmd_force_energy", "rbmd_force_status",
     "rbmd_force_get_neighbors", "rbmd_force_get_rbl", "rbmd_force_get_rhok", "rbmd_force_profile",
     "rbmd_force_phase_ms", "rbmd_force_list_builds", "rbmd_force_launch_count",
-    "rbmd_force_destroy", "rbmd_rhok_noalloc", "rbmd_version", "rbmd_last_error",
+    "rbmd_force_destroy", "rbmd_rhok_noalloc", "rbmd_proposal_mlp_eval", "rbmd_version",
+    "rbmd_last_error",
 ]
 
 
@@ -113,6 +114,7 @@ def library() -> ctypes.CDLL:
         "rbmd_force_launch_count": (I32, [V, P(I32)]),
         "rbmd_force_destroy": (None, [V]),
         "rbmd_rhok_noalloc": (I32, [V, V, I32, P(rbmd_box), V, I32, V, V]),
+        "rbmd_proposal_mlp_eval": (I32, [V, V, V, V, I32, I32, V, V, V, V, V]),
         "rbmd_version": (ctypes.c_char_p, []),
         "rbmd_last_error": (ctypes.c_char_p, []),
     }

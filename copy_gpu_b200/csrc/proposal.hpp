@@ -1,0 +1,11 @@
+// proposal.hpp -- launch helpers of the learned k-proposal network (proposal.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "kernels_mlp.cuh"
+
+namespace rbmd {
+cudaError_t mlp_launch(const MlpArgs& a, cudaStream_t s);
+cudaError_t mlp_grad_sum(int groups, const float* partial, float* grad, cudaStream_t s);
+cudaError_t mlp_adam(float* params, const float* grad, float* m, float* v, float lr, int step, cudaStream_t s);
+}  // namespace rbmd

@@ -229,6 +229,18 @@ RBMD_API rbmd_status rbmd_rhok_noalloc(const double* pos_dev, const double* char
                                        const rbmd_box* box, const int32_t* m_dev, int32_t P,
                                        double* rho_dev, void* stream);
 
+/* The learned k-proposal network (16 -> 64 -> 64 -> 1, tanh, BF16 operands on the tensor
+ * cores, FP32 accumulation) on `groups` groups of 256 rows, all pointers on the device:
+ * params[5313] (W1[64][16], b1[64], W2[64][64], b2[64], w3[64], b3), x[groups*256][16] inputs,
+ * h[groups*256] outputs.  With train != 0 also the group losses
+ * loss[g] = log sum_b wbin_b e^{h_b} + log sum_b cbin_b e^{-h_b} and the gradient of their mean
+ * into grad[5313].  status receives 0x80 when an internal wait gave up.  Synchronises the stream.
+ * No reference counterpart (the reference samples k from the Gaussian only,
+ * rbmd/framework/model/RBEPSample.h:63-175). */
+RBMD_API rbmd_status rbmd_proposal_mlp_eval(const float* params, const float* x, const float* wbin,
+                                            const float* cbin, int32_t groups, int32_t train, float* h,
+                                            double* loss, float* grad, uint32_t* status, void* stream);
+
 /* Version string of the library build. */
 RBMD_API const char* rbmd_version(void);
 
