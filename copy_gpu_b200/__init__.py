@@ -41,6 +41,7 @@ EXPORTED = [
     "rbmd_force_sync_velocities", "rbmd_force_energy", "rbmd_force_status",
     "rbmd_force_get_neighbors", "rbmd_force_get_rbl", "rbmd_force_get_rhok", "rbmd_force_profile",
     "rbmd_force_phase_ms", "rbmd_force_list_builds", "rbmd_force_launch_count",
+    "rbmd_force_train_proposal", "rbmd_force_proposal_params", "rbmd_force_get_far",
     "rbmd_force_destroy", "rbmd_rhok_noalloc", "rbmd_proposal_mlp_eval", "rbmd_version",
     "rbmd_last_error",
 ]
@@ -74,6 +75,17 @@ class rbmd_energy(ctypes.Structure):
     _fields_ = [(k, ctypes.c_double) for k in (
         "lj", "coul_real", "coul_kspace", "coul_self", "eam_embed", "eam_pair", "bond", "angle",
         "kinetic", "temperature")]
+
+
+class rbmd_train_opts(ctypes.Structure):
+    _fields_ = [("n_snapshots", ctypes.c_int32), ("steps_between", ctypes.c_int32),
+                ("k_per_snapshot", ctypes.c_int32), ("iterations", ctypes.c_int32),
+                ("learning_rate", ctypes.c_float), ("seed", ctypes.c_uint64)]
+
+
+class rbmd_train_report(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in (
+        "loss_gauss", "loss_first", "loss_final", "loss_optimum", "variance_ratio", "seconds")]
 
 
 _lib = None
@@ -115,6 +127,9 @@ def library() -> ctypes.CDLL:
         "rbmd_force_destroy": (None, [V]),
         "rbmd_rhok_noalloc": (I32, [V, V, I32, P(rbmd_box), V, I32, V, V]),
         "rbmd_proposal_mlp_eval": (I32, [V, V, V, V, I32, I32, V, V, V, V, V]),
+        "rbmd_force_train_proposal": (I32, [V, P(rbmd_train_opts), P(rbmd_train_report), V]),
+        "rbmd_force_proposal_params": (I32, [V, P(ctypes.c_float), P(ctypes.c_float)]),
+        "rbmd_force_get_far": (I32, [V, P(D)]),
         "rbmd_version": (ctypes.c_char_p, []),
         "rbmd_last_error": (ctypes.c_char_p, []),
     }
@@ -299,6 +314,33 @@ class ForceField:
         import numpy as np
         out = np.zeros((len(self.boxes) * P, 2), dtype=np.float64)
         _check(library().rbmd_force_get_rhok(self._h, _ptr(out, ctypes.c_double), P), "get_rhok")
+        return out
+
+    # ---- learned k-proposal ---------------------------------------------------------------
+    def train_proposal(self, n_snapshots=200, steps_between=10, k_per_snapshot=16384, iterations=1500,
+                       learning_rate=3e-3, seed=1, stream=None):
+        """Train the learned proposal on the bound system; returns the report as a dict."""
+        o = rbmd_train_opts(n_snapshots, steps_between, k_per_snapshot, iterations, learning_rate, seed)
+        r = rbmd_train_report()
+        _check(library().rbmd_force_train_proposal(self._h, ctypes.byref(o), ctypes.byref(r),
+                                                    self._stream(stream)), "train_proposal")
+        return {k: getattr(r, k) for k, _ in rbmd_train_report._fields_}
+
+    def proposal_params(self, new=None):
+        """Current network parameters (5313 floats); with `new`, replace them first."""
+        import numpy as np
+        out = np.zeros(5313, dtype=np.float32)
+        src = None if new is None else np.ascontiguousarray(new, dtype=np.float32)
+        _check(library().rbmd_force_proposal_params(self._h, None if src is not None else _ptr(out, ctypes.c_float),
+                                                    None if src is None else _ptr(src, ctypes.c_float)),
+               "proposal_params")
+        return src if src is not None else out
+
+    def far_force(self):
+        """k-space force of the last compute, [n_atoms, 3]."""
+        import numpy as np
+        out = np.zeros((self.n, 3), dtype=np.float64)
+        _check(library().rbmd_force_get_far(self._h, _ptr(out, ctypes.c_double)), "get_far")
         return out
 
     # ---- diagnostics ----------------------------------------------------------------------

@@ -2,7 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
-#include "kernels_mlp.cuh"
+#include "mlp_types.cuh"
 
 namespace rbmd {
 cudaError_t mlp_launch(const MlpArgs& a, cudaStream_t s);

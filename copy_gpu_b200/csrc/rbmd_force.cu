@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
+#include <random>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -26,6 +28,8 @@
 #include "kernels_force.cuh"
 #include "kernels_md.cuh"
 #include "kernels_rbl.cuh"
+#include "kernels_learned.cuh"
+#include "proposal.hpp"
 
 using namespace rbmd;
 
@@ -88,6 +92,20 @@ struct rbmd_force {
   bool rbl_table = false;        // compat.rbl_erf_table: G from the reference's alpha=0.1 table
   bool rbl_shell_coul = true;    // !compat.rbl_drop_shell_coulomb
   bool eam_ref_sign = false;     // compat.eam_verlet_pair_vector: reference's reversed EAM force
+  // k-proposal of the RBE sampler: "gauss" (the reference's Metropolis-Hastings chain over the
+  // Gaussian), "gauss_iid" (exact independent draws from the same Gaussian) or "learned" (the
+  // Gaussian reweighted per |k| bin by the network, importance weights p/q; until trained or
+  // given parameters it draws from the Gaussian with unit weights)
+  std::string proposal = "gauss";
+  bool prop_trained = false;
+  PropRep* d_prep = nullptr;
+  std::vector<PropRep> prep_h;
+  double* d_cdf = nullptr;
+  double* d_wbin = nullptr;         // [nrep][256] Gaussian mass per bin
+  std::vector<double> wbin_h;
+  double* d_pw = nullptr;           // [Ptot] importance weights of the drawn samples
+  float *d_mlp = nullptr, *d_h = nullptr, *d_feat = nullptr, *d_spec = nullptr;
+  int* d_spec_init = nullptr;
   int P = 100, kmax = 2;
   unsigned long long seed = 20240101ull;
   Units u{1, 1, 1, 1};
@@ -273,6 +291,8 @@ void free_all(rbmd_force* f) {
   f->d_frac = nullptr;
   dfree(f->d_meta); dfree(f->d_nbr); dfree(f->d_count); dfree(f->d_maxcount); dfree(f->d_status);
   dfree(f->d_count2); dfree(f->d_mean_partial); dfree(f->d_erf_tab);
+  dfree(f->d_prep); dfree(f->d_cdf); dfree(f->d_wbin); dfree(f->d_pw); dfree(f->d_mlp); dfree(f->d_h);
+  dfree(f->d_feat); dfree(f->d_spec); dfree(f->d_spec_init);
   dfree(f->d_rebuild); dfree(f->d_block_sums); dfree(f->d_xref); dfree(f->d_nbuilds);
   dfree(f->d_eslot); dfree(f->d_esum);
   if (f->d_krec) cudaFree(f->d_krec);
@@ -395,6 +415,191 @@ std::vector<float> rbl_erf_table() {
   return t;
 }
 
+// Tables of the own k-proposal per replica: the 1D Gaussian g_d(m) = exp(-pi^2 m^2 / (alpha L_d^2))
+// on |m| <= M_d with M_d = ceil(6 sqrt(alpha) L_d / pi) (so g_d(M_d) <= e^-36), its cumulative
+// distribution (inverse-CDF sampling), and the mass W_b of p(m) = prod_d g_d(m_d) / (prod_d G_d - 1)
+// (m != 0) in each |k| bin, accumulated over the octant |m_d| with multiplicities (the bin of m
+// depends on |m_d| only).  Network parameters start at zero (h = 0: the Gaussian itself).
+rbmd_status build_proposal_tables(rbmd_force* f, const std::vector<int64_t>& qoff) {
+  const int nrep = f->nrep;
+  f->prep_h.assign(nrep, PropRep{});
+  f->wbin_h.assign((size_t)nrep * kPropBins, 0.0);
+  std::vector<double> cdf;
+  for (int r = 0; r < nrep; ++r) {
+    PropRep& pr = f->prep_h[r];
+    const double* L = f->reps_h[r].box_d;
+    pr.kscale = 1.0 / (2.0 * std::sqrt(f->alpha));
+    pr.nq = (int)(qoff[r + 1] - qoff[r]);
+    std::vector<double> g[3];
+    double G[3];
+    for (int d = 0; d < 3; ++d) {
+      pr.c[d] = 2.0 * M_PI / L[d];
+      pr.M[d] = (int)std::ceil(6.0 * std::sqrt(f->alpha) * L[d] / M_PI);
+      if (pr.M[d] > (1 << 16)) {
+        std::snprintf(g_last_error, sizeof g_last_error, "proposal: box too large for the k tables");
+        return RBMD_ERR_CONFIG;
+      }
+      const double c = M_PI * M_PI / (f->alpha * L[d] * L[d]);
+      g[d].resize(pr.M[d] + 1);
+      for (int m = 0; m <= pr.M[d]; ++m) g[d][m] = std::exp(-c * (double)m * (double)m);
+      G[d] = g[d][0];
+      for (int m = 1; m <= pr.M[d]; ++m) G[d] += 2.0 * g[d][m];
+      pr.cdf_off[d] = (int)cdf.size();
+      double acc = 0;
+      for (int m = -pr.M[d]; m <= pr.M[d]; ++m) {
+        acc += g[d][std::abs(m)];
+        cdf.push_back(acc / G[d]);
+      }
+      cdf.back() = 1.0;
+    }
+    const double Z = G[0] * G[1] * G[2] - 1.0;
+    double* W = f->wbin_h.data() + (size_t)r * kPropBins;
+    for (int a = 0; a <= pr.M[0]; ++a)
+      for (int b = 0; b <= pr.M[1]; ++b) {
+        const double gab = g[0][a] * g[1][b] * (a ? 2.0 : 1.0) * (b ? 2.0 : 1.0);
+        for (int c = 0; c <= pr.M[2]; ++c) {
+          if (a == 0 && b == 0 && c == 0) continue;
+          W[prop_bin(prop_kappa(pr, a, b, c))] += gab * g[2][c] * (c ? 2.0 : 1.0);
+        }
+      }
+    for (int k = 0; k < kPropBins; ++k) W[k] /= Z;
+  }
+  CK(dalloc(&f->d_prep, (size_t)nrep));
+  CK(cudaMemcpy(f->d_prep, f->prep_h.data(), sizeof(PropRep) * nrep, cudaMemcpyHostToDevice));
+  CK(dalloc(&f->d_cdf, cdf.size()));
+  CK(cudaMemcpy(f->d_cdf, cdf.data(), sizeof(double) * cdf.size(), cudaMemcpyHostToDevice));
+  CK(dalloc(&f->d_wbin, f->wbin_h.size()));
+  CK(cudaMemcpy(f->d_wbin, f->wbin_h.data(), sizeof(double) * f->wbin_h.size(), cudaMemcpyHostToDevice));
+  CK(dalloc(&f->d_pw, (size_t)f->Ptot));
+  CK(dalloc(&f->d_mlp, (size_t)kMlpNParam));
+  CK(cudaMemset(f->d_mlp, 0, sizeof(float) * kMlpNParam));
+  CK(dalloc(&f->d_h, (size_t)nrep * kPropBins));
+  CK(dalloc(&f->d_feat, (size_t)nrep * kPropBins * kMlpIn));
+  CK(dalloc(&f->d_spec, (size_t)nrep * kPropBands));
+  CK(cudaMemset(f->d_spec, 0, sizeof(float) * nrep * kPropBands));
+  CK(dalloc(&f->d_spec_init, (size_t)nrep));
+  CK(cudaMemset(f->d_spec_init, 0, sizeof(int) * nrep));
+  f->prop_trained = false;
+  return RBMD_OK;
+}
+
+// Scratch of one training run, freed on every return path.
+struct TrainScratch {
+  std::vector<void*> ptrs;
+  template <class T>
+  cudaError_t get(T** p, size_t count) {
+    cudaError_t e = dalloc(p, count);
+    if (e == cudaSuccess) ptrs.push_back((void*)*p);
+    return e;
+  }
+  ~TrainScratch() {
+    for (void* p : ptrs) cudaFree(p);
+  }
+};
+
+// Fit of the proposal network to S snapshots (cbin, spec on the device): inputs from each
+// snapshot's spectrum, W_b of replica 0, parameters initialised with an output layer of zero
+// (h = 0, the Gaussian, at the start), full-batch Adam with a cosine-decayed learning rate
+// (floor 0.1), mean group loss reported before, at the first step and after the last; the
+// network's conditioning state starts at the mean training spectrum.
+rbmd_status train_fit(rbmd_force* f, const rbmd_train_opts* o, rbmd_train_report* rep, cudaStream_t s,
+                      std::chrono::steady_clock::time_point t0, int S, float* cbin, float* spec, float* wbinf,
+                      float* X, double* loss, float* gpart, float* grad, float* am, float* av) {
+  std::vector<float> wf((size_t)S * kPropBins);
+  for (int sn = 0; sn < S; ++sn)
+    for (int b = 0; b < kPropBins; ++b) wf[(size_t)sn * kPropBins + b] = (float)f->wbin_h[b];
+  CK(cudaMemcpyAsync(wbinf, wf.data(), sizeof(float) * wf.size(), cudaMemcpyHostToDevice, s));
+  k_prop_features<<<(S * kPropBins + 255) / 256, 256, 0, s>>>(S, spec, X);
+  std::vector<float> p(kMlpNParam, 0.f);
+  {
+    std::mt19937_64 rng(o->seed * 0x9E3779B97F4A7C15ull + 17);
+    std::normal_distribution<float> nd(0.f, 1.f);
+    for (int e = 0; e < kMlpHid * kMlpIn; ++e) p[kOW1 + e] = nd(rng) / 4.0f;
+    for (int e = 0; e < kMlpHid * kMlpHid; ++e) p[kOW2 + e] = nd(rng) / 8.0f;
+    for (int j = 0; j < kMlpHid; ++j) {
+      p[kOB1 + j] = 0.1f * nd(rng);
+      p[kOB2 + j] = 0.1f * nd(rng);
+    }
+  }
+  CK(cudaMemcpyAsync(f->d_mlp, p.data(), sizeof(float) * kMlpNParam, cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(am, 0, sizeof(float) * kMlpNParam, s));
+  CK(cudaMemsetAsync(av, 0, sizeof(float) * kMlpNParam, s));
+  MlpArgs a{};
+  a.groups = S;
+  a.train = 1;
+  a.gscale = 1.0f / (float)S;
+  a.params = f->d_mlp;
+  a.x = X;
+  a.wbin = wbinf;
+  a.cbin = cbin;
+  a.h = nullptr;
+  a.loss = loss;
+  a.grad_partial = gpart;
+  a.status = f->d_status;
+  std::vector<double> lh(S);
+  auto mean_loss = [&]() -> double {
+    cudaMemcpyAsync(lh.data(), loss, sizeof(double) * S, cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    double m = 0;
+    for (double v : lh) m += v;
+    return m / S;
+  };
+  const int T = o->iterations;
+  double l_first = 0;
+  for (int it = 1; it <= T; ++it) {
+    CK(mlp_launch(a, s));
+    CK(mlp_grad_sum(S, gpart, grad, s));
+    const float lr = o->learning_rate * (0.1f + 0.45f * (1.0f + std::cos((float)M_PI * (float)(it - 1) / (float)T)));
+    CK(mlp_adam(f->d_mlp, grad, am, av, lr, it, s));
+    if (it == 1) l_first = mean_loss();
+  }
+  CK(mlp_launch(a, s));
+  const double l_final = mean_loss();
+  uint32_t st = 0;
+  CK(cudaMemcpy(&st, f->d_status, sizeof st, cudaMemcpyDeviceToHost));
+  if (st & kFlagMlpTimeout) {
+    std::snprintf(g_last_error, sizeof g_last_error, "train_proposal: a tensor-core wait timed out");
+    return RBMD_ERR_DEVICE;
+  }
+  // reference losses from the data: h = 0 (Gaussian) and the per-snapshot optimum
+  std::vector<float> cb((size_t)S * kPropBins), sp((size_t)S * kPropBands);
+  CK(cudaMemcpy(cb.data(), cbin, sizeof(float) * cb.size(), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(sp.data(), spec, sizeof(float) * sp.size(), cudaMemcpyDeviceToHost));
+  double lg = 0, lo = 0;
+  for (int sn = 0; sn < S; ++sn) {
+    double sw = 0, sc = 0, sq = 0;
+    for (int b = 0; b < kPropBins; ++b) {
+      const double w = f->wbin_h[b], c = cb[(size_t)sn * kPropBins + b];
+      sw += w;
+      sc += c;
+      sq += std::sqrt(w * c);
+    }
+    lg += std::log(sw) + std::log(sc);
+    lo += 2.0 * std::log(sq);
+  }
+  lg /= S;
+  lo /= S;
+  std::vector<float> mean_spec(kPropBands, 0.f);
+  for (int sn = 0; sn < S; ++sn)
+    for (int j = 0; j < kPropBands; ++j) mean_spec[j] += sp[(size_t)sn * kPropBands + j] / (float)S;
+  std::vector<float> spec_all((size_t)f->nrep * kPropBands);
+  for (int r = 0; r < f->nrep; ++r)
+    for (int j = 0; j < kPropBands; ++j) spec_all[(size_t)r * kPropBands + j] = mean_spec[j];
+  CK(cudaMemcpy(f->d_spec, spec_all.data(), sizeof(float) * spec_all.size(), cudaMemcpyHostToDevice));
+  std::vector<int> ones(f->nrep, 1);
+  CK(cudaMemcpy(f->d_spec_init, ones.data(), sizeof(int) * f->nrep, cudaMemcpyHostToDevice));
+  f->prop_trained = true;
+  if (rep) {
+    rep->loss_gauss = lg;
+    rep->loss_first = l_first;
+    rep->loss_final = l_final;
+    rep->loss_optimum = lo;
+    rep->variance_ratio = std::exp(l_final - lg);
+    rep->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+  return RBMD_OK;
+}
+
 // RBE normaliser S = prod_d H_d - 1 with H_d = sqrt(a L^2/pi) sum_{|m|<=10} e^{-a L^2 m^2}
 // (ExecForceFunction::Compute_S/Compute_H, rbmd/framework/forceFunction/ExecForceFunction.h:266-294),
 // evaluated in FP64.
@@ -460,18 +665,47 @@ void launch_sort(rbmd_force* f, cudaStream_t s, bool bin) {
   }
 }
 
+// Samples of the own proposal for `step`: with a trained network the per-bin log-weights h come
+// from the network evaluated on the current conditioning spectrum (tensor cores), then the exact
+// sampler draws from q = p e^h / Z with weights p / q; otherwise it draws from p.
+void launch_prop_sample(rbmd_force* f, cudaStream_t s, long long step, int rec_bytes) {
+  const float* h = nullptr;
+  if (f->proposal == "learned" && f->prop_trained) {
+    k_prop_features<<<(f->nrep * kPropBins + 255) / 256, 256, 0, s>>>(f->nrep, f->d_spec, f->d_feat);
+    MlpArgs a{};
+    a.groups = f->nrep;
+    a.train = 0;
+    a.gscale = 1.f;
+    a.params = f->d_mlp;
+    a.x = f->d_feat;
+    a.h = f->d_h;
+    a.status = f->d_status;
+    mlp_launch(a, s);
+    h = f->d_h;
+    f->launches += 2;
+  }
+  k_prop_sample<<<f->nrep, 256, 0, s>>>(f->nrep, f->d_reps, f->d_prep, f->d_cdf, h, f->d_wbin, f->seed, step,
+                                        4096, f->d_kvec, f->d_krec, rec_bytes, f->d_krep, f->d_pw, f->d_status);
+  f->launches++;
+}
+
 // k-space chain on the side stream: sampler (depends only on the step counter, so it runs
 // before the fork wait), fixed-point fractional coordinates, structure factors, coefficients,
 // RBE force into d_far.
 template <class R>
 void launch_kspace(rbmd_force* f, cudaStream_t s, cudaEvent_t ready) {
   const int rec_bytes = sizeof(typename KRec<R>::T);
+  const bool own_prop = !f->injected && f->coul_type == "RBE" && f->proposal != "gauss";
   if (!f->injected && f->coul_type == "RBE") {
     PhaseScope ps(f, kPhSample, s);
-    k_sample<kSamplerD><<<f->nrep, 256, 0, s>>>(f->nrep, f->d_srep, f->d_qtab, f->d_reps, f->seed,
-                                                f->step_count, f->d_kvec, f->d_krec, rec_bytes,
-                                                f->d_krep, f->d_status);
-    f->launches++;
+    if (!own_prop) {
+      k_sample<kSamplerD><<<f->nrep, 256, 0, s>>>(f->nrep, f->d_srep, f->d_qtab, f->d_reps, f->seed,
+                                                  f->step_count, f->d_kvec, f->d_krec, rec_bytes,
+                                                  f->d_krep, f->d_status);
+      f->launches++;
+    } else {
+      launch_prop_sample(f, s, f->step_count, rec_bytes);
+    }
   }
   cudaStreamWaitEvent(s, ready, 0);
   if (f->nq == 0) return;
@@ -484,8 +718,13 @@ void launch_kspace(rbmd_force* f, cudaStream_t s, cudaEvent_t ready) {
         f->d_items, (const typename FracT<R>::T*)f->d_frac, (const typename KRec<R>::T*)f->d_krec,
         (R*)f->d_partial, f->ktile);
     k_rho_finish<R><<<(f->Ptot + 3) / 4, 128, 0, s>>>(
-        f->Ptot, f->ktile, f->d_krep, f->d_rhorep, f->d_reps, (const R*)f->d_partial, f->d_weights,
-        f->u.qqr2e, (typename KRec<R>::T*)f->d_krec, f->d_rho, f->d_ek);
+        f->Ptot, f->ktile, f->d_krep, f->d_rhorep, f->d_reps, (const R*)f->d_partial,
+        own_prop ? f->d_pw : f->d_weights, f->u.qqr2e, (typename KRec<R>::T*)f->d_krec, f->d_rho, f->d_ek);
+    if (own_prop && f->proposal == "learned" && f->prop_trained) {
+      k_prop_spectrum<<<f->nrep, 32, 0, s>>>(f->nrep, f->d_reps, f->d_prep, f->d_kvec, f->d_rho, f->d_pw, 0.1f,
+                                              f->d_spec, f->d_spec_init);
+      f->launches++;
+    }
   }
   {
     PhaseScope ps(f, kPhRbeF, s);
@@ -842,6 +1081,11 @@ rbmd_status parse_config(rbmd_force* f, const char* text) {
     f->alpha = num(root, "hyper_parameters.coulomb.alpha", 0.1);
     f->kmax = (int)num(root, "hyper_parameters.coulomb.kmax", 2);
     f->seed = (unsigned long long)num(root, "hyper_parameters.coulomb.seed", 20240101.0);
+    f->proposal = rbmdjson::text(root, "hyper_parameters.coulomb.proposal", "gauss");
+    if (f->proposal != "gauss" && f->proposal != "gauss_iid" && f->proposal != "learned") {
+      std::snprintf(g_last_error, sizeof g_last_error, "config: unknown coulomb.proposal %s", f->proposal.c_str());
+      return RBMD_ERR_CONFIG;
+    }
   }
   f->shake = rbmdjson::text(root, "hyper_parameters.extend.fix_shake", "null");
   f->shake_tol = num(root, "hyper_parameters.extend.shake_tolerance", 1e-5);
@@ -1346,6 +1590,10 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
     CK(cudaMemcpy(f->d_srep, sr.data(), sizeof(SamplerRep) * nrep, cudaMemcpyHostToDevice));
     CK(dalloc(&f->d_qtab, qtab.size()));
     CK(cudaMemcpy(f->d_qtab, qtab.data(), sizeof(double) * qtab.size(), cudaMemcpyHostToDevice));
+    if (f->coul_type == "RBE" && f->proposal != "gauss") {
+      rbmd_status st = build_proposal_tables(f, qoff);
+      if (st) return st;
+    }
     if (f->coul_type == "EWALD") {
       // fixed cube sample set with Gaussian weights
       std::vector<int> m;
@@ -1470,8 +1718,11 @@ rbmd_status rbmd_force_get_ksamples(rbmd_force* f, int32_t* m_xyz, int32_t P) {
 rbmd_status rbmd_force_sample_k(rbmd_force* f, int64_t step, int32_t* m_xyz, int32_t P) {
   if (!f || !f->bound || !f->is_rbe() || P != f->P || f->coul_type != "RBE") return RBMD_ERR_ARG;
   const int recb = f->fp64 ? sizeof(KRec64) : sizeof(KRec32);
-  k_sample<kSamplerD><<<f->nrep, 256>>>(f->nrep, f->d_srep, f->d_qtab, f->d_reps, f->seed, step,
-                                         f->d_kvec, f->d_krec, recb, f->d_krep, f->d_status);
+  if (f->proposal != "gauss")
+    launch_prop_sample(f, nullptr, step, recb);
+  else
+    k_sample<kSamplerD><<<f->nrep, 256>>>(f->nrep, f->d_srep, f->d_qtab, f->d_reps, f->seed, step,
+                                           f->d_kvec, f->d_krec, recb, f->d_krep, f->d_status);
   CK(cudaGetLastError());
   CK(cudaDeviceSynchronize());
   if (m_xyz) CK(cudaMemcpy(m_xyz, f->d_kvec, sizeof(int) * 3 * f->Ptot, cudaMemcpyDeviceToHost));
@@ -1685,6 +1936,99 @@ rbmd_status rbmd_force_get_rbl(rbmd_force* f, int32_t* ncore, int32_t* nshell, i
   sizes[2] = f->rbl_sizes_h[2];
   sizes[3] = f->core_cap;
   sizes[4] = f->shell_cap;
+  return RBMD_OK;
+}
+
+rbmd_status rbmd_force_train_proposal(rbmd_force* f, const rbmd_train_opts* o, rbmd_train_report* rep,
+                                      void* stream) {
+  if (!f || !o) return RBMD_ERR_ARG;
+  if (!f->bound || f->proposal != "learned" || !f->d_prep) return RBMD_ERR_STATE;
+  if (o->n_snapshots < 1 || o->k_per_snapshot < 256 || o->iterations < 1 || o->steps_between < 0 ||
+      !(o->learning_rate > 0))
+    return RBMD_ERR_ARG;
+  const auto t0 = std::chrono::steady_clock::now();
+  cudaStream_t s = (cudaStream_t)stream;
+  const int S = o->n_snapshots, K = o->k_per_snapshot, nq0 = f->prep_h[0].nq;
+  if (nq0 < 1) return RBMD_ERR_STATE;
+  const int nch = (nq0 + kTrainChunk - 1) / kTrainChunk;
+  TrainScratch ts;
+  int *kv = nullptr, *krec = nullptr, *krep = nullptr;
+  double *kw = nullptr, *ak = nullptr, *loss = nullptr;
+  double2* rho = nullptr;
+  float *partial = nullptr, *cbin = nullptr, *spec = nullptr, *wbinf = nullptr, *X = nullptr, *gpart = nullptr,
+        *grad = nullptr, *am = nullptr, *av = nullptr;
+  Frac32* frac = nullptr;
+  RepDev* rep1 = nullptr;
+  CK(ts.get(&kv, 3 * (size_t)K));
+  CK(ts.get(&krec, 3 * (size_t)K));
+  CK(ts.get(&krep, (size_t)K));
+  CK(ts.get(&kw, (size_t)K));
+  CK(ts.get(&ak, (size_t)K));
+  CK(ts.get(&rho, (size_t)K));
+  CK(ts.get(&partial, 2 * (size_t)nch * K));
+  CK(ts.get(&cbin, (size_t)S * kPropBins));
+  CK(ts.get(&spec, (size_t)S * kPropBands));
+  CK(ts.get(&wbinf, (size_t)S * kPropBins));
+  CK(ts.get(&X, (size_t)S * kPropBins * kMlpIn));
+  CK(ts.get(&loss, (size_t)S));
+  CK(ts.get(&gpart, (size_t)S * kMlpNParam));
+  CK(ts.get(&grad, (size_t)kMlpNParam));
+  CK(ts.get(&am, (size_t)kMlpNParam));
+  CK(ts.get(&av, (size_t)kMlpNParam));
+  CK(ts.get(&frac, (size_t)nq0));
+  CK(ts.get(&rep1, 1));
+  {
+    RepDev r1 = f->reps_h[0];
+    r1.P = K;
+    r1.k_begin = 0;
+    CK(cudaMemcpy(rep1, &r1, sizeof r1, cudaMemcpyHostToDevice));
+  }
+  const int* rep_of = f->nrep > 1 ? f->d_rep_of : nullptr;
+  // ---- data: per snapshot, K draws from p, exact rho_k, per-sample force norms, bins ----
+  for (int sn = 0; sn < S; ++sn) {
+    if (o->steps_between > 0) {
+      rbmd_status st = rbmd_force_step(f, o->steps_between, stream);
+      if (st) return st;
+    }
+    k_frac<float><<<(nq0 + 255) / 256, 256, 0, s>>>(nq0, f->d_qidx, f->at.pos, f->at.charge, rep_of, f->d_reps,
+                                                     frac);
+    k_prop_sample<<<1, 256, 0, s>>>(1, rep1, f->d_prep, f->d_cdf, nullptr, f->d_wbin, o->seed,
+                                    (1LL << 40) + sn, 4096, kv, krec, 12, krep, kw, f->d_status);
+    const dim3 grid((K + 255) / 256, nch);
+    for (int pass = 0; pass < 2; ++pass) {
+      k_train_pass<<<grid, 256, 0, s>>>(pass, K, nq0, frac, kv, rho, partial);
+      k_train_finish<<<(K + 255) / 256, 256, 0, s>>>(pass, K, nch, f->d_prep, kv, partial, rho, ak);
+    }
+    k_train_bins<<<1, kPropBins, 0, s>>>(K, nq0, f->d_prep, kv, rho, ak, cbin + (size_t)sn * kPropBins,
+                                         spec + (size_t)sn * kPropBands);
+    CK(cudaGetLastError());
+  }
+  return train_fit(f, o, rep, s, t0, S, cbin, spec, wbinf, X, loss, gpart, grad, am, av);
+}
+
+rbmd_status rbmd_force_proposal_params(rbmd_force* f, float* get_host, const float* set_host) {
+  if (!f || (!get_host && !set_host)) return RBMD_ERR_ARG;
+  if (!f->bound || !f->d_mlp) return RBMD_ERR_STATE;
+  if (set_host) {
+    CK(cudaMemcpy(f->d_mlp, set_host, sizeof(float) * kMlpNParam, cudaMemcpyHostToDevice));
+    f->prop_trained = true;
+  }
+  if (get_host) CK(cudaMemcpy(get_host, f->d_mlp, sizeof(float) * kMlpNParam, cudaMemcpyDeviceToHost));
+  return RBMD_OK;
+}
+
+rbmd_status rbmd_force_get_far(rbmd_force* f, double* far_host) {
+  if (!f || !far_host) return RBMD_ERR_ARG;
+  if (!f->bound || !f->is_rbe()) return RBMD_ERR_STATE;
+  CK(cudaDeviceSynchronize());
+  std::memset(far_host, 0, sizeof(double) * 3 * (size_t)f->n);
+  if (f->nq == 0) return RBMD_OK;
+  std::vector<double> far(3 * (size_t)f->nq);
+  std::vector<int> q(f->nq);
+  CK(cudaMemcpy(far.data(), f->d_far, sizeof(double) * far.size(), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(q.data(), f->d_qidx, sizeof(int) * q.size(), cudaMemcpyDeviceToHost));
+  for (int c = 0; c < f->nq; ++c)
+    for (int d = 0; d < 3; ++d) far_host[3 * (size_t)q[c] + d] = far[3 * (size_t)c + d];
   return RBMD_OK;
 }
 

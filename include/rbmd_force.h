@@ -241,6 +241,45 @@ RBMD_API rbmd_status rbmd_proposal_mlp_eval(const float* params, const float* x,
                                             const float* cbin, int32_t groups, int32_t train, float* h,
                                             double* loss, float* grad, uint32_t* status, void* stream);
 
+/* Options and outcome of rbmd_force_train_proposal. */
+typedef struct {
+  int32_t n_snapshots;     /* snapshots of the bound system (groups of the training batch)       */
+  int32_t steps_between;   /* MD steps (rbmd_force_step) before each snapshot; 0: static system  */
+  int32_t k_per_snapshot;  /* k-vectors drawn from the Gaussian per snapshot                      */
+  int32_t iterations;      /* Adam steps on the full batch                                       */
+  float learning_rate;
+  uint64_t seed;           /* network initialisation and k draws                                 */
+} rbmd_train_opts;
+
+typedef struct {
+  double loss_gauss;       /* mean group loss of h = 0 (the Gaussian proposal)                    */
+  double loss_first;       /* after the first Adam step                                          */
+  double loss_final;       /* after the last Adam step                                           */
+  double loss_optimum;     /* lower bound: h_b = log sqrt(C_b / W_b) per snapshot                 */
+  double variance_ratio;   /* exp(loss_final - loss_gauss): learned / Gaussian force variance     */
+  double seconds;          /* wall time of data generation + training                            */
+} rbmd_train_report;
+
+/* Train the learned k-proposal (coulomb.proposal "learned") on the bound system: for each of
+ * n_snapshots snapshots (advancing the system by steps_between MD steps first), draw
+ * k_per_snapshot vectors from RBE's Gaussian, compute their exact structure factors rho_k (the
+ * full Ewald sum's terms) and the squared norm of each sample's force field, bin them into the
+ * per-|k| variance weights C_b and the snapshot's spectrum; then fit the network by Adam on the
+ * log force variance of the reweighted proposal, all on the GPU (tcgen05 forward/backward).
+ * Replica 0 provides the data.  Afterwards every compute/step draws its k-samples from the
+ * trained proposal with importance weights p/q.  No reference counterpart. */
+RBMD_API rbmd_status rbmd_force_train_proposal(rbmd_force* f, const rbmd_train_opts* opts,
+                                               rbmd_train_report* report, void* stream);
+
+/* Read (get_host != NULL) and/or replace (set_host != NULL) the 5313 network parameters of the
+ * learned proposal; setting parameters marks the proposal as trained.  No reference counterpart. */
+RBMD_API rbmd_status rbmd_force_proposal_params(rbmd_force* f, float* get_host, const float* set_host);
+
+/* k-space (RBE) force of the last compute per caller atom, far_host[n_atoms*3] (zero for
+ * uncharged atoms; qqr2e applied).  Two evaluations with different k-sets give the estimator's
+ * noise.  Mirrors the far force of ExecutionNVT::EleNewForce (rbmd/framework/run/ExecutionNVT.cpp:717-733). */
+RBMD_API rbmd_status rbmd_force_get_far(rbmd_force* f, double* far_host);
+
 /* Version string of the library build. */
 RBMD_API const char* rbmd_version(void);
 
