@@ -2,14 +2,20 @@
 """Benchmark of the B200 force path on the 1,000,000-atom primitive-model electrolyte.
 
 Workload (one GPU): 1,000,000 atoms (10 % +/-1 ions, neutral LJ solvent, rho = 0.8 sigma^-3,
-L = 107.72 sigma), LJ cutoff 2.5, real-space alpha with erfc(sqrt(alpha) rc) <= 1e-5, plain
-Gaussian RBE with P = 500 k-samples per step, FP32 forces with compensated accumulation, FP64
-velocity-Verlet + Berendsen.  A "step" is one full MD step (kick, drift, cell sort, neighbour
-list, RBE structure factors, near + k-space force, kick, temperature, thermostat).
+L = 107.72 sigma), LJ cutoff 2.5, real-space alpha with erfc(sqrt(alpha) rc) <= 1e-5, FP32 forces
+with compensated accumulation, FP64 velocity-Verlet + Berendsen.  A "step" is one full MD step
+(kick, drift, cell sort, neighbour list, RBE sampling and structure factors, near + k-space
+force, kick, temperature, thermostat).
 
-Metric: atom-steps/s (higher is better).  With --gpus N (torchrun, one process per GPU) every
-rank advances its own independent replica of the workload ("replicas only", weak scaling; no
-data-path collective); value = total atom-steps / max-over-ranks device time.
+Metric: atom-steps/s at equal k-space force RMSE, learned vs plain RBE.  The plain arm samples
+P = 500 k-vectors per step with the reference's Metropolis-Hastings chain over RBE's Gaussian.
+The learned arm trains the k-proposal network on the workload (200 snapshots 10 MD steps apart),
+measures both proposals' force RMSE at P = 500 (the estimator is unbiased, so its RMS deviation
+over independent k-sets at fixed positions is its error against the exact Ewald k-space force),
+sets P_learned = ceil(500 * MSE_learned / MSE_plain) and times that.  `value` is the learned arm;
+the plain arm's numbers are in `comparison`.  With --gpus N (torchrun, one process per GPU) every
+rank advances its own independent replica ("replicas only", weak scaling; no data-path
+collective); value = total atom-steps / max-over-ranks device time.
 
 --impl reference times the reference path's CPU implementation (the oracle restatement of the
 reference's FP32 force path; the reference itself cannot be built here) on the host cores.
@@ -46,6 +52,10 @@ def parse():
     ap.add_argument("--P", type=int, default=P_PLAIN)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--snapshots", type=int, default=200, help="training snapshots of the learned proposal")
+    ap.add_argument("--train-iters", type=int, default=1500, help="Adam steps of the proposal network")
+    ap.add_argument("--noise-steps", type=int, default=16,
+                    help="k-sets per proposal for the force-RMSE measurement")
     ap.add_argument("--skin", type=float, default=0.3,
                     help="Verlet skin; the list is rebuilt when an atom moved more than skin/2 "
                          "(forces are those of a per-step rebuild); 0 rebuilds every step")
@@ -130,26 +140,22 @@ def algorithmic(n, nq, n_nbr_mean, P):
     }
 
 
-def run_ours(args):
+# Per-atom DRAM traffic of the near-force pass measured by ncu on the 200,000-atom case
+# (69.4 MB per launch, profiles/k_near_force_traffic_electrolyte_200k.md); the full-size launch
+# has the same per-atom traffic (same density and neighbour count).
+NEAR_TRAFFIC_BYTES_PER_ATOM = 69.4e6 / 200_000
+
+
+def make_handle(s, dev, P, proposal, seed, skin, dt=None, ensemble="NVT", params=None):
+    """ForceField over a copy of system s on `dev` (1 replica)."""
     import torch
-    import torch.distributed as dist
     from copy_gpu_b200 import Box, ForceField, systems
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-    dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
-
-    s = systems.electrolyte(args.atoms, seed=3 + rank)
-    cfg = systems.electrolyte_config(P=args.P, precision="fp32", seed=7 + rank)
-    cfg["hyper_parameters"]["neighbor"]["skin"] = args.skin
+    kw = {} if dt is None else {"dt": dt}
+    cfg = systems.electrolyte_config(P=P, precision="fp32", seed=seed, ensemble=ensemble, **kw)
+    cfg["hyper_parameters"]["neighbor"]["skin"] = skin
+    cfg["hyper_parameters"]["coulomb"]["proposal"] = proposal
     n = s["pos"].shape[0]
-    t = {k: torch.tensor(s[k], device=dev, dtype=torch.float64).contiguous()
-         for k in ("pos", "vel", "mass", "charge")}
+    t = {k: torch.tensor(s[k], device=dev, dtype=torch.float64).contiguous() for k in ("pos", "vel", "mass", "charge")}
     t["type"] = torch.tensor(s["type"], device=dev, dtype=torch.int32)
     t["force"] = torch.zeros((n, 3), device=dev, dtype=torch.float64)
     t["image"] = torch.zeros((n, 3), device=dev, dtype=torch.int32)
@@ -157,10 +163,39 @@ def run_ours(args):
     ff.set_pair_coeffs(s["eps"], s["sigma"])
     ff.Init(t["pos"], t["force"], vel=t["vel"], mass=t["mass"], charge=t["charge"], type=t["type"],
             image=t["image"])
+    if params is not None:
+        ff.proposal_params(params)
+    return ff, t, cfg
+
+
+def kspace_noise(ff, steps, warm=3):
+    """Per-atom mean squared deviation of the RBE force estimator at fixed positions (a dt = 0
+    handle): half the mean squared difference of the k-space forces of consecutive steps, whose
+    k-sets are independent.  The estimator is unbiased (importance weights), so this is its
+    mean squared error against the exact Ewald k-space force."""
+    import torch
+    ff.step(warm)
+    prev, acc, cnt = None, 0.0, 0
+    for _ in range(steps):
+        ff.step(1)
+        torch.cuda.synchronize()
+        f = ff.far_force()
+        if prev is not None:
+            acc += float(((f - prev) ** 2).sum()) / 2.0
+            cnt += 1
+        prev = f
+    return acc / cnt
+
+
+def timed_run(ff, t, dev, steps, warmup, world, dist, e2e_steps):
+    """Warm-up, then `steps` timed MD steps (CUDA events, max over ranks), phases, clocks and the
+    end-to-end host-buffer force call."""
+    import torch
+    local = dev.index or 0
     stream = torch.cuda.current_stream(dev)
-    blocks = ff.autotune()                         # own autotuner: threads per block of list / force
-    ff.Execute()                                   # initial force (ExecutionNVT::Init)
-    ff.step(args.warmup)
+    blocks = ff.autotune()
+    ff.Execute()
+    ff.step(warmup)
     torch.cuda.synchronize(dev)
     k_per_step = ff.launches_per_step()
     clocks = Clocks(local)
@@ -174,7 +209,7 @@ def run_ours(args):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    ff.step(args.steps)
+    ff.step(steps)
     e1.record(stream)
     torch.cuda.synchronize(dev)
     if world > 1:
@@ -189,118 +224,194 @@ def run_ours(args):
         m = torch.tensor([ms], device=dev, dtype=torch.float64)
         dist.all_reduce(m, op=dist.ReduceOp.MAX)
         ms = float(m.item())
-    value = world * n * args.steps / (ms / 1e3)
-
-    # mean neighbour count (for the algorithmic byte counts)
+    n = ff.n
     ff.Execute()
     cnt, _ = ff.neighbors(0)
     n_nbr = float(cnt.mean())
-
     # end-to-end through the host-buffer C-ABI call: pinned positions in, pinned forces out
     pos_h = torch.empty((n, 3), dtype=torch.float64, pin_memory=True)
     pos_h.copy_(t["pos"].cpu())
     frc_h = torch.empty((n, 3), dtype=torch.float64, pin_memory=True)
-    ph = pos_h.numpy()
-    fh = frc_h.numpy()
+    ph, fh = pos_h.numpy(), frc_h.numpy()
     ff.compute_host(ph, fh, stream=stream.cuda_stream)
     torch.cuda.synchronize(dev)
     w0 = time.perf_counter()
     a0 = torch.cuda.Event(enable_timing=True)
     a1 = torch.cuda.Event(enable_timing=True)
     a0.record(stream)
-    for _ in range(args.e2e_steps):
+    for _ in range(e2e_steps):
         ff.compute_host(ph, fh, stream=stream.cuda_stream)
     a1.record(stream)
     torch.cuda.synchronize(dev)
-    e2e_ms = max(a0.elapsed_time(a1), (time.perf_counter() - w0) * 1e3) / args.e2e_steps
+    e2e_ms = max(a0.elapsed_time(a1), (time.perf_counter() - w0) * 1e3) / e2e_steps
     if world > 1:
         m = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
         dist.all_reduce(m, op=dist.ReduceOp.MAX)
         e2e_ms = float(m.item())
-    e2e_value = world * n / (e2e_ms / 1e3)
+    return dict(ms=ms, builds=builds, phases=phases, flags=flags, clk=clk, n_nbr=n_nbr, e2e_ms=e2e_ms,
+                k_per_step=k_per_step, blocks=blocks)
 
+
+def roofline(run, n, nq, P, steps, dev):
+    """Per-phase achieved GB/s and sin/cos rates from the CUDA-event phase times, and the roofline
+    object of the dominant kernel.  The k-space phases run on a second stream concurrently with
+    the list build and near pass, so their event intervals include time shared with those
+    kernels; the dominant kernel is taken among the caller-stream force kernels."""
+    import torch
+    peaks, src = measured_peaks()
+    alg = algorithmic(n, nq, run["n_nbr"], P)
+    phases = run["phases"]
+    launches = {k: phases[k][1] for k in phases}
+    sm_mhz = run["clk"]["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0)
+    n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
+    mufu_peak = 16 * n_sm * sm_mhz * 1e6 / 2.0 / 1e9        # G sincos/s (2 MUFU ops each)
+    rl = {}
+    for k, a in alg.items():
+        if k not in phases or launches[k] == 0:
+            continue
+        tot_ms = phases[k][0]
+        per_launch_s = tot_ms / 1e3 / launches[k]
+        if k == "integrate":
+            per_launch_s = tot_ms / 1e3 / steps
+        if k == "neighbor_list":      # early-exit launches on list-reuse steps are ~3 us
+            per_launch_s = tot_ms / 1e3 / max(run["builds"], 1)
+        ent = {"ms_per_step": tot_ms / steps, "launches": launches[k], "ms_per_launch": per_launch_s * 1e3}
+        ent["hbm_gbs"] = a["bytes"] * a["units"] / per_launch_s / 1e9
+        ent["hbm_frac"] = ent["hbm_gbs"] / peaks["hbm_gbs"]
+        if "sincos" in a:
+            ent["gsincos_s"] = a["sincos"] * a["units"] / per_launch_s / 1e9
+            ent["mufu_frac"] = ent["gsincos_s"] / mufu_peak
+            ent["stream"] = "k-space (overlaps the caller stream)"
+        rl[k] = ent
+    single = [k for k in ("force", "neighbor_list") if k in rl]
+    dom = max(single, key=lambda k: rl[k]["ms_per_step"])
+    d = rl[dom]
+    roof = {"bound": "hbm", "achieved": d["hbm_gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": d["hbm_frac"], "kernel": "k_near_force" if dom == "force" else "k_nlist",
+            "peak_source": f"{src} hbm_gbs (MEASURED_PEAKS.json)", "traffic": None,
+            "algorithmic_bytes_per_launch": alg[dom]["bytes"] * alg[dom]["units"]}
+    if dom == "force":
+        roof["traffic"] = NEAR_TRAFFIC_BYTES_PER_ATOM * n
+        roof["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the 200,000-atom "
+                                  "launch scaled by atoms (profiles/k_near_force_traffic_electrolyte_200k.md)")
+    return roof, rl, mufu_peak
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from copy_gpu_b200 import systems
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    s = systems.electrolyte(args.atoms, seed=3 + rank)
+    n = s["pos"].shape[0]
+    nq = int((s["charge"] != 0).sum())
+    P0 = args.P
+
+    # ---- plain arm: the reference's Metropolis-Hastings Gaussian sampler, P = 500 ----
+    ff, t, cfg = make_handle(s, dev, P0, "gauss", 7 + rank, args.skin)
+    plain = timed_run(ff, t, dev, args.steps, args.warmup, world, dist, args.e2e_steps)
+    ff.close()
+    del t
+
+    # ---- learned arm: train on the workload (200 snapshots 10 MD steps apart) ----
+    ff, t, _ = make_handle(s, dev, P0, "learned", 11 + rank, args.skin)
+    ff.Execute()
+    report = ff.train_proposal(n_snapshots=args.snapshots, steps_between=10, k_per_snapshot=16384,
+                               iterations=args.train_iters, learning_rate=3e-3, seed=5 + rank)
+    params = ff.proposal_params()
+    ff.close()
+    del t
+
+    # ---- force RMSE of both proposals at P = 500 (fixed positions, independent k-sets) ----
+    ffn, tn, _ = make_handle(s, dev, P0, "gauss", 13 + rank, 0.0, dt=0.0, ensemble="NVE")
+    ffn.Execute()
+    mse_plain = kspace_noise(ffn, args.noise_steps) / nq
+    ffn.close()
+    ffn, tn, _ = make_handle(s, dev, P0, "learned", 17 + rank, 0.0, dt=0.0, ensemble="NVE", params=params)
+    ffn.Execute()
+    mse_learned = kspace_noise(ffn, args.noise_steps) / nq
+    ffn.close()
+    del tn
+    ratio = mse_learned / mse_plain
+    P_eq = int(np.ceil(P0 * ratio))                 # MSE ~ 1/P: the learned P of equal RMSE
+
+    # ---- timed learned arm at P_eq ----
+    ff, t, cfg_l = make_handle(s, dev, P_eq, "learned", 19 + rank, args.skin, params=params)
+    ffn, tn, _ = make_handle(s, dev, P_eq, "learned", 23 + rank, 0.0, dt=0.0, ensemble="NVE", params=params)
+    ffn.Execute()
+    mse_learned_eq = kspace_noise(ffn, args.noise_steps) / nq
+    ffn.close()
+    del tn
+    learned = timed_run(ff, t, dev, args.steps, args.warmup, world, dist, args.e2e_steps)
+    ff.close()
+
+    v_plain = world * n * args.steps / (plain["ms"] / 1e3)
+    v_learned = world * n * args.steps / (learned["ms"] / 1e3)
     out = None
     if rank == 0:
-        peaks, src = measured_peaks()
-        nq = int((s["charge"] != 0).sum())
-        alg = algorithmic(n, nq, n_nbr, args.P)
-        launches = {k: phases[k][1] for k in phases}
-        sm_mhz = clk["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0)
-        n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
-        mufu_peak = 16 * n_sm * sm_mhz * 1e6 / 2.0 / 1e9        # G sincos/s (2 MUFU ops each)
-        rl = {}
-        for k, a in alg.items():
-            if k not in phases or launches[k] == 0:
-                continue
-            tot_ms = phases[k][0]
-            # per-launch duration (the list phase runs only on rebuild steps)
-            per_launch_s = tot_ms / 1e3 / launches[k]
-            if k == "integrate":
-                per_launch_s = tot_ms / 1e3 / args.steps
-            if k == "neighbor_list":      # early-exit launches on list-reuse steps are ~3 us
-                per_launch_s = tot_ms / 1e3 / max(builds, 1)
-            ent = {"ms_per_step": tot_ms / args.steps, "launches": launches[k],
-                   "ms_per_launch": per_launch_s * 1e3}
-            ent["hbm_gbs"] = a["bytes"] * a["units"] / per_launch_s / 1e9
-            ent["hbm_frac"] = ent["hbm_gbs"] / peaks["hbm_gbs"]
-            if "sincos" in a:
-                ent["gsincos_s"] = a["sincos"] * a["units"] / per_launch_s / 1e9
-                ent["mufu_frac"] = ent["gsincos_s"] / mufu_peak
-            rl[k] = ent
-        # dominant single-kernel phase by device time per step
-        single = [k for k in ("force", "neighbor_list", "kspace", "rbe_force") if k in rl]
-        dom = max(single, key=lambda k: rl[k]["ms_per_step"])
-        d = rl[dom]
-        if "mufu_frac" in d and d["mufu_frac"] > d["hbm_frac"]:
-            roof = {"bound": "mufu", "achieved": d["gsincos_s"], "peak": mufu_peak, "unit": "Gsincos/s",
-                    "frac": d["mufu_frac"], "kernel": dom,
-                    "peak_source": f"16 MUFU ops/clk/SM x {n_sm} SMs x median loaded {sm_mhz:.0f} MHz / 2",
-                    "traffic": None}
-        else:
-            roof = {"bound": "hbm", "achieved": d["hbm_gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                    "frac": d["hbm_frac"], "kernel": dom, "peak_source": f"{src} hbm_gbs (MEASURED_PEAKS.json)",
-                    "traffic": None}
-        tr_path = os.path.join(ROOT, "profiles", "traffic.json")
-        if os.path.exists(tr_path):
-            with open(tr_path) as fh:
-                trd = json.load(fh)
-            if dom in trd:
-                roof["traffic"] = trd[dom]
+        roof, rl, _ = roofline(learned, n, nq, P_eq, args.steps, dev)
         out = {
             "metric": METRIC,
-            "value": value,
+            "value": v_learned,
             "unit": "atom-steps/s",
             "n_gpus": world,
             "steps": args.steps,
             "warmup": args.warmup,
-            "ms_per_step": ms / args.steps,
+            "ms_per_step": learned["ms"] / args.steps,
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": f"electrolyte {n} atoms, plain Gaussian RBE P={args.P}, full MD step",
-                       "atoms_per_gpu": n, "P": args.P, "proposal": "gauss", "rc": 2.5, "skin": args.skin,
-                       "list_builds_per_step": builds / args.steps,
-                       "threads_per_block": {"list": blocks[0], "force": blocks[1]},
+            "config": {"workload": f"electrolyte {n} atoms, full MD step, learned k-proposal at P={P_eq} "
+                                   f"(equal k-space force RMSE to plain Gaussian RBE at P={P0})",
+                       "atoms_per_gpu": n, "P": P_eq, "P_plain": P0, "proposal": "learned", "rc": 2.5,
+                       "skin": args.skin, "list_builds_per_step": learned["builds"] / args.steps,
+                       "threads_per_block": {"list": learned["blocks"][0], "force": learned["blocks"][1]},
                        "alpha": cfg["hyper_parameters"]["coulomb"]["alpha"], "box": float(s["hi"][0]),
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2": "inputs larger than L2 (neighbour list %.0f MB + state %.0f MB)"
-                             % (4 * n_nbr * n / 1e6, 72 * n / 1e6)},
+                             % (4 * learned["n_nbr"] * n / 1e6, 72 * n / 1e6)},
+            "comparison": {
+                "plain": {"value": v_plain, "ms_per_step": plain["ms"] / args.steps, "P": P0,
+                          "sampler": "Metropolis-Hastings over RBE's Gaussian (the reference's)",
+                          "kspace_force_rmse": float(np.sqrt(mse_plain)),
+                          "e2e": world * n / (plain["e2e_ms"] / 1e3)},
+                "learned": {"value": v_learned, "ms_per_step": learned["ms"] / args.steps, "P": P_eq,
+                            "kspace_force_rmse": float(np.sqrt(mse_learned_eq)),
+                            "kspace_force_rmse_at_P_plain": float(np.sqrt(mse_learned)),
+                            "variance_ratio_at_P_plain": ratio,
+                            "training": report},
+                "speedup_at_equal_rmse": v_learned / v_plain,
+                "rmse_how": "per-atom RMS of the RBE estimator's deviation from its mean (unbiased, so from "
+                            "the exact Ewald k-space force): half the mean squared difference of two "
+                            f"independent k-sets at fixed positions, {args.noise_steps - 1} pairs",
+            },
             "roofline": roof,
             "phases": rl,
-            "e2e": {"value": e2e_value, "unit": "atom-steps/s", "h2d_bytes_per_step": 24 * n,
-                    "d2h_bytes_per_step": 24 * n,
+            "phase_ms_per_step": {k: {"learned": learned["phases"][k][0] / args.steps,
+                                      "plain": plain["phases"][k][0] / args.steps}
+                                  for k in learned["phases"] if k in plain["phases"]},
+            "e2e": {"value": world * n / (learned["e2e_ms"] / 1e3), "unit": "atom-steps/s",
+                    "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n,
                     "what": "rbmd_force_compute_host: pinned host positions in, forces out, one force evaluation per step"},
-            "gpu_launches": k_per_step * args.steps,
-            "kernels_per_step": k_per_step,
-            "status_flags": flags,
-            "clocks": clk,
-            "mean_neighbors": n_nbr,
+            "gpu_launches": learned["k_per_step"] * args.steps,
+            "kernels_per_step": learned["k_per_step"],
+            "status_flags": learned["flags"] | plain["flags"],
+            "clocks": learned["clk"],
+            "clocks_plain_arm": plain["clk"],
+            "mean_neighbors": learned["n_nbr"],
         }
         if not args.no_cpu and world == 1:
-            out["cpu_baseline"] = cpu_baseline(args.P)
-    ff.close()
+            out["cpu_baseline"] = cpu_baseline(P0)
     if world > 1:
         dist.destroy_process_group()
     return out

@@ -205,36 +205,56 @@ __global__ void __launch_bounds__(256) k_prop_sample(
   }
 }
 
-// Conditioning spectrum of each replica (one block per replica, thread j < 8 = band j): the
+// Conditioning spectrum of each replica (one block of 256 threads per replica): the
 // importance-weighted mean of |rho_k|^2 / N_q over this step's samples in band j (weights w make
 // it an estimate of the p-average, the quantity the training data record), folded into an
-// exponential moving average of its logarithm (rate beta; the first update replaces).
-__global__ void k_prop_spectrum(int nrep, const RepDev* __restrict__ reps, const PropRep* __restrict__ prep,
-                                const int* __restrict__ kvec, const double2* __restrict__ rho,
-                                const double* __restrict__ weights, float beta, float* __restrict__ spec,
-                                int* __restrict__ spec_init) {
-  const int r = blockIdx.x, j = threadIdx.x;
+// exponential moving average of its logarithm (rate beta; the first update replaces).  Thread t
+// accumulates samples t, t + 256, ...; the per-band partials are summed in thread order.
+__global__ void __launch_bounds__(256) k_prop_spectrum(int nrep, const RepDev* __restrict__ reps,
+                                                       const PropRep* __restrict__ prep,
+                                                       const int* __restrict__ kvec, const double2* __restrict__ rho,
+                                                       const double* __restrict__ weights, float beta,
+                                                       float* __restrict__ spec, int* __restrict__ spec_init) {
+  const int r = blockIdx.x, t = threadIdx.x;
   if (r >= nrep) return;
-  const bool active = j < kPropBands;
   const PropRep pr = prep[r];
   const int P = reps[r].P, kb = reps[r].k_begin;
-  double sw = 0, ss = 0;
-  for (int i = 0; active && i < P; ++i) {
+  __shared__ double sw_s[kPropBands][256], ss_s[kPropBands][256];
+  double sw[kPropBands], ss[kPropBands];
+#pragma unroll
+  for (int j = 0; j < kPropBands; ++j) sw[j] = ss[j] = 0.0;
+  for (int i = t; i < P; i += 256) {
     const int g = kb + i;
-    const double kap = prop_kappa(pr, kvec[3 * g], kvec[3 * g + 1], kvec[3 * g + 2]);
-    if (prop_band(kap) != j) continue;
+    const int j = prop_band(prop_kappa(pr, kvec[3 * g], kvec[3 * g + 1], kvec[3 * g + 2]));
     const double w = weights ? weights[g] : 1.0;
     const double2 z = rho[g];
-    sw += w;
-    ss += w * (z.x * z.x + z.y * z.y);
+#pragma unroll
+    for (int b = 0; b < kPropBands; ++b)
+      if (b == j) {
+        sw[b] += w;
+        ss[b] += w * (z.x * z.x + z.y * z.y);
+      }
   }
-  if (active && sw > 0 && pr.nq > 0) {
-    const float v = (float)log(fmax(ss / (sw * (double)pr.nq), 1e-6));
-    float& s = spec[r * kPropBands + j];
-    s = spec_init[r] ? (1.f - beta) * s + beta * v : v;
+#pragma unroll
+  for (int j = 0; j < kPropBands; ++j) {
+    sw_s[j][t] = sw[j];
+    ss_s[j][t] = ss[j];
   }
   __syncthreads();
-  if (j == 0) spec_init[r] = 1;
+  if (t < kPropBands) {
+    double a = 0, b = 0;
+    for (int k = 0; k < 256; ++k) {
+      a += sw_s[t][k];
+      b += ss_s[t][k];
+    }
+    if (a > 0 && pr.nq > 0) {
+      const float v = (float)log(fmax(b / (a * (double)pr.nq), 1e-6));
+      float& sv = spec[r * kPropBands + t];
+      sv = spec_init[r] ? (1.f - beta) * sv + beta * v : v;
+    }
+  }
+  __syncthreads();
+  if (t == 0) spec_init[r] = 1;
 }
 
 // ---------------- training data of one snapshot ----------------

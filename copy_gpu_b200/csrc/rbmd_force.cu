@@ -720,11 +720,6 @@ void launch_kspace(rbmd_force* f, cudaStream_t s, cudaEvent_t ready) {
     k_rho_finish<R><<<(f->Ptot + 3) / 4, 128, 0, s>>>(
         f->Ptot, f->ktile, f->d_krep, f->d_rhorep, f->d_reps, (const R*)f->d_partial,
         own_prop ? f->d_pw : f->d_weights, f->u.qqr2e, (typename KRec<R>::T*)f->d_krec, f->d_rho, f->d_ek);
-    if (own_prop && f->proposal == "learned" && f->prop_trained) {
-      k_prop_spectrum<<<f->nrep, 32, 0, s>>>(f->nrep, f->d_reps, f->d_prep, f->d_kvec, f->d_rho, f->d_pw, 0.1f,
-                                              f->d_spec, f->d_spec_init);
-      f->launches++;
-    }
   }
   {
     PhaseScope ps(f, kPhRbeF, s);
@@ -734,6 +729,12 @@ void launch_kspace(rbmd_force* f, cudaStream_t s, cudaEvent_t ready) {
         (const typename KRec<R>::T*)f->d_krec, f->d_reps, rep_of, f->d_far);
   }
   f->launches += 4;
+  // conditioning of the next step's proposal, after the force kernels of this one
+  if (own_prop && f->proposal == "learned" && f->prop_trained) {
+    k_prop_spectrum<<<f->nrep, 256, 0, s>>>(f->nrep, f->d_reps, f->d_prep, f->d_kvec, f->d_rho, f->d_pw, 0.1f,
+                                            f->d_spec, f->d_spec_init);
+    f->launches++;
+  }
 }
 
 template <class R, bool COUL, int MI>
