@@ -305,10 +305,11 @@ __global__ void __launch_bounds__(256) k_train_pass(int pass, int K, int nq, con
 }
 
 // fixed-order FP64 sum of the chunk partials; pass 0 -> rho (shifted convention kept), pass 1 ->
-// a_k = sum / |k|^2 (the k-dependent factor of the squared force norm)
+// a_k = sum / |k|^2 (the k-dependent factor of the squared force norm) and the sample's bin and
+// band (bin | band << 16)
 __global__ void k_train_finish(int pass, int K, int nchunks, const PropRep* __restrict__ prep,
                                const int* __restrict__ kv, const float* __restrict__ partial,
-                               double2* __restrict__ rho, double* __restrict__ ak) {
+                               double2* __restrict__ rho, double* __restrict__ ak, int* __restrict__ kbin) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= K) return;
   double a = 0, b = 0;
@@ -323,23 +324,22 @@ __global__ void k_train_finish(int pass, int K, int nchunks, const PropRep* __re
     const double kap = prop_kappa(pr, kv[3 * k], kv[3 * k + 1], kv[3 * k + 2]);
     const double k2 = kap * kap / (pr.kscale * pr.kscale);
     ak[k] = a / k2;
+    kbin[k] = prop_bin(kap) | (prop_band(kap) << 16);
   }
 }
 
 // Per snapshot (one block, thread b = bin): C_b = (1/K) sum of a_k over the samples in bin b (an
 // unbiased estimate of sum_{m in b} a(m) / p(m), since the samples come from p), and the
 // conditioning spectrum of the snapshot (log band means of |rho_k|^2 / N_q).  Deterministic.
-__global__ void k_train_bins(int K, int nq, const PropRep* __restrict__ prep, const int* __restrict__ kv,
-                             const double2* __restrict__ rho, const double* __restrict__ ak,
-                             float* __restrict__ cbin, float* __restrict__ spec) {
+__global__ void k_train_bins(int K, int nq, const int* __restrict__ kbin, const double2* __restrict__ rho,
+                             const double* __restrict__ ak, float* __restrict__ cbin, float* __restrict__ spec) {
   const int b = threadIdx.x;
-  const PropRep pr = prep[0];
   double cs = 0, bs = 0;
   int bn = 0;
   for (int k = 0; k < K; ++k) {
-    const double kap = prop_kappa(pr, kv[3 * k], kv[3 * k + 1], kv[3 * k + 2]);
-    if (prop_bin(kap) == b) cs += ak[k];
-    if (b < kPropBands && prop_band(kap) == b) {
+    const int code = __ldg(kbin + k);
+    if ((code & 0xFFFF) == b) cs += ak[k];
+    if (b < kPropBands && (code >> 16) == b) {
       bs += rho[k].x * rho[k].x + rho[k].y * rho[k].y;
       ++bn;
     }

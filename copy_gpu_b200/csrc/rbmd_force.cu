@@ -1953,7 +1953,7 @@ rbmd_status rbmd_force_train_proposal(rbmd_force* f, const rbmd_train_opts* o, r
   if (nq0 < 1) return RBMD_ERR_STATE;
   const int nch = (nq0 + kTrainChunk - 1) / kTrainChunk;
   TrainScratch ts;
-  int *kv = nullptr, *krec = nullptr, *krep = nullptr;
+  int *kv = nullptr, *krec = nullptr, *krep = nullptr, *kbin = nullptr;
   double *kw = nullptr, *ak = nullptr, *loss = nullptr;
   double2* rho = nullptr;
   float *partial = nullptr, *cbin = nullptr, *spec = nullptr, *wbinf = nullptr, *X = nullptr, *gpart = nullptr,
@@ -1963,6 +1963,7 @@ rbmd_status rbmd_force_train_proposal(rbmd_force* f, const rbmd_train_opts* o, r
   CK(ts.get(&kv, 3 * (size_t)K));
   CK(ts.get(&krec, 3 * (size_t)K));
   CK(ts.get(&krep, (size_t)K));
+  CK(ts.get(&kbin, (size_t)K));
   CK(ts.get(&kw, (size_t)K));
   CK(ts.get(&ak, (size_t)K));
   CK(ts.get(&rho, (size_t)K));
@@ -1998,9 +1999,9 @@ rbmd_status rbmd_force_train_proposal(rbmd_force* f, const rbmd_train_opts* o, r
     const dim3 grid((K + 255) / 256, nch);
     for (int pass = 0; pass < 2; ++pass) {
       k_train_pass<<<grid, 256, 0, s>>>(pass, K, nq0, frac, kv, rho, partial);
-      k_train_finish<<<(K + 255) / 256, 256, 0, s>>>(pass, K, nch, f->d_prep, kv, partial, rho, ak);
+      k_train_finish<<<(K + 255) / 256, 256, 0, s>>>(pass, K, nch, f->d_prep, kv, partial, rho, ak, kbin);
     }
-    k_train_bins<<<1, kPropBins, 0, s>>>(K, nq0, f->d_prep, kv, rho, ak, cbin + (size_t)sn * kPropBins,
+    k_train_bins<<<1, kPropBins, 0, s>>>(K, nq0, kbin, rho, ak, cbin + (size_t)sn * kPropBins,
                                          spec + (size_t)sn * kPropBands);
     CK(cudaGetLastError());
   }
