@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--snapshots", type=int, default=200, help="training snapshots of the learned proposal")
     ap.add_argument("--train-iters", type=int, default=1500, help="Adam steps of the proposal network")
+    ap.add_argument("--no-graph", action="store_true", help="launch every kernel of a step directly "
+                    "instead of replaying the captured step graph")
     ap.add_argument("--noise-steps", type=int, default=16,
                     help="k-sets per proposal for the force-RMSE measurement")
     ap.add_argument("--skin", type=float, default=0.3,
@@ -146,7 +148,7 @@ def algorithmic(n, nq, n_nbr_mean, P):
 NEAR_TRAFFIC_BYTES_PER_ATOM = 69.4e6 / 200_000
 
 
-def make_handle(s, dev, P, proposal, seed, skin, dt=None, ensemble="NVT", params=None):
+def make_handle(s, dev, P, proposal, seed, skin, dt=None, ensemble="NVT", params=None, graph=True):
     """ForceField over a copy of system s on `dev` (1 replica)."""
     import torch
     from copy_gpu_b200 import Box, ForceField, systems
@@ -154,6 +156,7 @@ def make_handle(s, dev, P, proposal, seed, skin, dt=None, ensemble="NVT", params
     cfg = systems.electrolyte_config(P=P, precision="fp32", seed=seed, ensemble=ensemble, **kw)
     cfg["hyper_parameters"]["neighbor"]["skin"] = skin
     cfg["hyper_parameters"]["coulomb"]["proposal"] = proposal
+    cfg["execution"]["cuda_graph"] = graph
     n = s["pos"].shape[0]
     t = {k: torch.tensor(s[k], device=dev, dtype=torch.float64).contiguous() for k in ("pos", "vel", "mass", "charge")}
     t["type"] = torch.tensor(s["type"], device=dev, dtype=torch.int32)
@@ -316,7 +319,7 @@ def run_ours(args):
     P0 = args.P
 
     # ---- plain arm: the reference's Metropolis-Hastings Gaussian sampler, P = 500 ----
-    ff, t, cfg = make_handle(s, dev, P0, "gauss", 7 + rank, args.skin)
+    ff, t, cfg = make_handle(s, dev, P0, "gauss", 7 + rank, args.skin, graph=not args.no_graph)
     plain = timed_run(ff, t, dev, args.steps, args.warmup, world, dist, args.e2e_steps)
     ff.close()
     del t
@@ -344,7 +347,8 @@ def run_ours(args):
     P_eq = int(np.ceil(P0 * ratio))                 # MSE ~ 1/P: the learned P of equal RMSE
 
     # ---- timed learned arm at P_eq ----
-    ff, t, cfg_l = make_handle(s, dev, P_eq, "learned", 19 + rank, args.skin, params=params)
+    ff, t, cfg_l = make_handle(s, dev, P_eq, "learned", 19 + rank, args.skin, params=params,
+                               graph=not args.no_graph)
     ffn, tn, _ = make_handle(s, dev, P_eq, "learned", 23 + rank, 0.0, dt=0.0, ensemble="NVE", params=params)
     ffn.Execute()
     mse_learned_eq = kspace_noise(ffn, args.noise_steps) / nq
@@ -378,6 +382,7 @@ def run_ours(args):
                        "threads_per_block": {"list": learned["blocks"][0], "force": learned["blocks"][1]},
                        "alpha": cfg["hyper_parameters"]["coulomb"]["alpha"], "box": float(s["hi"][0]),
                        "parallelism": "replicas" if world > 1 else "single",
+                       "step_launch": "kernels" if args.no_graph else "cuda graph replay (one launch per step)",
                        "l2": "inputs larger than L2 (neighbour list %.0f MB + state %.0f MB)"
                              % (4 * learned["n_nbr"] * n / 1e6, 72 * n / 1e6)},
             "comparison": {

@@ -485,11 +485,13 @@ template <int D>
 __global__ void __launch_bounds__(256) k_sample(int nrep, const SamplerRep* __restrict__ srep,
                                                 const double* __restrict__ gtab,
                                                 const RepDev* __restrict__ reps, unsigned long long seed,
-                                                long long step, int* __restrict__ kvec_out,
+                                                long long step_arg, const long long* __restrict__ step_dev,
+                                                int* __restrict__ kvec_out,
                                                 void* __restrict__ krec, int rec_bytes,
                                                 int* __restrict__ krep, uint32_t* status) {
   const int r = blockIdx.x;
   if (r >= nrep) return;
+  const long long step = step_dev ? *step_dev : step_arg;   // device counter under graph replay
   const SamplerRep s = srep[r];
   const int P = reps[r].P, kb = reps[r].k_begin;
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);

@@ -100,11 +100,12 @@ __device__ __forceinline__ int cdf_search(const double* cdf, int n, double u) {
 // remaining samples get weight 0 and RBMD_FLAG_SAMPLER is raised.
 __global__ void __launch_bounds__(256) k_prop_sample(
     int nrep, const RepDev* __restrict__ reps, const PropRep* __restrict__ prep, const double* __restrict__ cdf,
-    const float* __restrict__ h, const double* __restrict__ wbin, unsigned long long seed, long long step,
-    int max_rounds, int* __restrict__ kvec_out, void* __restrict__ krec, int rec_bytes, int* __restrict__ krep,
+    const float* __restrict__ h, const double* __restrict__ wbin, unsigned long long seed, long long step_arg,
+    const long long* __restrict__ step_dev, int max_rounds, int* __restrict__ kvec_out, void* __restrict__ krec, int rec_bytes, int* __restrict__ krep,
     double* __restrict__ weights, uint32_t* status) {
   const int r = blockIdx.x;
   if (r >= nrep) return;
+  const long long step = step_dev ? *step_dev : step_arg;   // device counter under graph replay
   const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
   const PropRep pr = prep[r];
   const int P = reps[r].P, kb = reps[r].k_begin;

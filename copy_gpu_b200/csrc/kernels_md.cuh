@@ -90,6 +90,9 @@ __global__ void k_skin_check(int n, const double* __restrict__ pos, const double
   if (!(d2 <= half_skin2) && *rebuild == 0) atomicExch(rebuild, 1);
 }
 
+// Advance the device step counter the k-samplers read (end of a step's k-space chain).
+__global__ void k_step_inc(long long* step) { *step += 1; }
+
 // Chunk of atoms inside one replica (kinetic-energy partials, ordered per replica).
 struct MdChunk { int begin, end, rep, pad; };
 

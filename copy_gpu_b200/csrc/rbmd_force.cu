@@ -215,6 +215,15 @@ struct rbmd_force {
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   long long step_count = 0;
+  long long* d_step = nullptr;   // step index of the k-samplers on the device (graph replay)
+  bool in_step = false;          // launches belong to rbmd_force_step (advance d_step)
+  bool use_graph = true;         // execution.cuda_graph: replay a captured step
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_launches = 0;
+  bool graph_pending = false;    // pending_scale the graph was captured with
+  bool capturing = false;
+  cudaStream_t gstream = nullptr;
+  cudaEvent_t ev_begin = nullptr;
   int launches = 0;
   // per-phase CUDA-event profiler (rbmd_force_profile / rbmd_force_phase_ms)
   bool prof_on = false;
@@ -307,7 +316,13 @@ void free_all(rbmd_force* f) {
   if (f->d_fp) cudaFree(f->d_fp);
   f->d_fp = nullptr;
   dfree(f->d_emb); dfree(f->d_epair); dfree(f->d_hoh); dfree(f->d_ebond); dfree(f->d_eangle);
-  dfree(f->d_snap); dfree(f->d_snap_img);
+  dfree(f->d_snap); dfree(f->d_snap_img); dfree(f->d_step);
+  if (f->graph_exec) cudaGraphExecDestroy(f->graph_exec);
+  f->graph_exec = nullptr;
+  if (f->gstream) cudaStreamDestroy(f->gstream);
+  f->gstream = nullptr;
+  if (f->ev_begin) cudaEventDestroy(f->ev_begin);
+  f->ev_begin = nullptr;
   if (f->h_status) cudaFreeHost(f->h_status);
   f->h_status = nullptr;
   if (f->h_maxcount) cudaFreeHost(f->h_maxcount);
@@ -668,7 +683,8 @@ void launch_sort(rbmd_force* f, cudaStream_t s, bool bin) {
 // Samples of the own proposal for `step`: with a trained network the per-bin log-weights h come
 // from the network evaluated on the current conditioning spectrum (tensor cores), then the exact
 // sampler draws from q = p e^h / Z with weights p / q; otherwise it draws from p.
-void launch_prop_sample(rbmd_force* f, cudaStream_t s, long long step, int rec_bytes) {
+void launch_prop_sample(rbmd_force* f, cudaStream_t s, long long step, int rec_bytes,
+                        const long long* step_dev = nullptr) {
   const float* h = nullptr;
   if (f->proposal == "learned" && f->prop_trained) {
     k_prop_features<<<(f->nrep * kPropBins + 255) / 256, 256, 0, s>>>(f->nrep, f->d_spec, f->d_feat);
@@ -685,7 +701,7 @@ void launch_prop_sample(rbmd_force* f, cudaStream_t s, long long step, int rec_b
     f->launches += 2;
   }
   k_prop_sample<<<f->nrep, 256, 0, s>>>(f->nrep, f->d_reps, f->d_prep, f->d_cdf, h, f->d_wbin, f->seed, step,
-                                        4096, f->d_kvec, f->d_krec, rec_bytes, f->d_krep, f->d_pw, f->d_status);
+                                        step_dev, 4096, f->d_kvec, f->d_krec, rec_bytes, f->d_krep, f->d_pw, f->d_status);
   f->launches++;
 }
 
@@ -695,20 +711,27 @@ void launch_prop_sample(rbmd_force* f, cudaStream_t s, long long step, int rec_b
 template <class R>
 void launch_kspace(rbmd_force* f, cudaStream_t s, cudaEvent_t ready) {
   const int rec_bytes = sizeof(typename KRec<R>::T);
+  if (f->capturing) cudaStreamWaitEvent(s, f->ev_begin, 0);   // the side stream joins the capture
   const bool own_prop = !f->injected && f->coul_type == "RBE" && f->proposal != "gauss";
   if (!f->injected && f->coul_type == "RBE") {
     PhaseScope ps(f, kPhSample, s);
     if (!own_prop) {
       k_sample<kSamplerD><<<f->nrep, 256, 0, s>>>(f->nrep, f->d_srep, f->d_qtab, f->d_reps, f->seed,
-                                                  f->step_count, f->d_kvec, f->d_krec, rec_bytes,
+                                                  f->step_count, f->d_step, f->d_kvec, f->d_krec, rec_bytes,
                                                   f->d_krep, f->d_status);
       f->launches++;
     } else {
-      launch_prop_sample(f, s, f->step_count, rec_bytes);
+      launch_prop_sample(f, s, f->step_count, rec_bytes, f->d_step);
     }
   }
   cudaStreamWaitEvent(s, ready, 0);
-  if (f->nq == 0) return;
+  if (f->nq == 0) {
+    if (f->in_step) {
+      k_step_inc<<<1, 1, 0, s>>>(f->d_step);
+      f->launches++;
+    }
+    return;
+  }
   const int* rep_of = f->nrep > 1 ? f->d_rep_of : nullptr;
   {
     PhaseScope ps(f, kPhK, s);
@@ -733,6 +756,10 @@ void launch_kspace(rbmd_force* f, cudaStream_t s, cudaEvent_t ready) {
   if (own_prop && f->proposal == "learned" && f->prop_trained) {
     k_prop_spectrum<<<f->nrep, 256, 0, s>>>(f->nrep, f->d_reps, f->d_prep, f->d_kvec, f->d_rho, f->d_pw, 0.1f,
                                             f->d_spec, f->d_spec_init);
+    f->launches++;
+  }
+  if (f->in_step) {
+    k_step_inc<<<1, 1, 0, s>>>(f->d_step);
     f->launches++;
   }
 }
@@ -931,6 +958,10 @@ void launch_compute_any(rbmd_force* f, cudaStream_t s) {
 }
 
 rbmd_status grow_list(rbmd_force* f, const int* need) {
+  if (f->graph_exec) {
+    cudaGraphExecDestroy(f->graph_exec);   // buffers move: the captured step is stale
+    f->graph_exec = nullptr;
+  }
   auto grown = [](int cur, int want) { return std::max(cur, ((int)(want * 1.2) + 8 + 7) & ~7); };
   if (f->is_rbl()) {
     f->core_cap = grown(f->core_cap, need[0]);
@@ -965,6 +996,7 @@ rbmd_status check_overflow(rbmd_force* f, cudaStream_t s, bool* redo) {
 
 template <class R>
 void launch_step(rbmd_force* f, cudaStream_t s) {
+  if (f->capturing) cudaEventRecord(f->ev_begin, s);
   const int n = f->n;
   const bool shake = f->shake == "true" && f->n_mol > 0;
   MdParams mp;
@@ -1046,6 +1078,62 @@ void launch_step(rbmd_force* f, cudaStream_t s) {
   f->step_count++;
 }
 
+// n_steps MD steps on stream s.  With execution.cuda_graph (default on) and no per-step host
+// decisions (no energy output, no profiling), the first step runs directly (it brings the lazy
+// thermostat state and the list flag to their steady values), the next step is captured once on
+// an internal stream (the k-space stream joins the capture) and then replayed with one
+// cudaGraphLaunch per step on s.  The samplers read the step index from a device counter that
+// the k-space chain advances, so every replay draws new k-samples.  The captured step is
+// re-captured when the lazy-rescale state differs and dropped when a list grows.
+template <class R>
+rbmd_status run_steps(rbmd_force* f, int n_steps, cudaStream_t s) {
+  const bool graph = f->use_graph && f->energy_every == 0 && !f->prof_on && n_steps > 1;
+  if (!graph) {
+    for (int k = 0; k < n_steps; ++k) launch_step<R>(f, s);
+    return RBMD_OK;
+  }
+  launch_step<R>(f, s);
+  const int per_step = f->launches;
+  if (!f->graph_exec || f->graph_pending != f->pending_scale) {
+    if (f->graph_exec) cudaGraphExecDestroy(f->graph_exec);
+    f->graph_exec = nullptr;
+    if (!f->gstream) CK(cudaStreamCreateWithFlags(&f->gstream, cudaStreamNonBlocking));
+    if (!f->ev_begin) CK(cudaEventCreateWithFlags(&f->ev_begin, cudaEventDisableTiming));
+    const long long sc = f->step_count;
+    const bool pend = f->pending_scale;
+    const int l0 = f->launches;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(f->gstream, cudaStreamCaptureModeThreadLocal));
+    f->capturing = true;
+    launch_step<R>(f, f->gstream);
+    f->capturing = false;
+    const cudaError_t e = cudaStreamEndCapture(f->gstream, &g);
+    f->graph_launches = f->launches - l0;
+    f->launches = l0;
+    f->step_count = sc;
+    f->pending_scale = pend;
+    if (e != cudaSuccess || !g) {
+      std::snprintf(g_last_error, sizeof g_last_error, "step capture: %s", cudaGetErrorString(e));
+      if (g) cudaGraphDestroy(g);
+      return RBMD_ERR_CUDA;
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&f->graph_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+      std::snprintf(g_last_error, sizeof g_last_error, "step graph: %s", cudaGetErrorString(ei));
+      f->graph_exec = nullptr;
+      return RBMD_ERR_CUDA;
+    }
+    f->graph_pending = pend;
+  }
+  for (int k = 1; k < n_steps; ++k) {
+    CK(cudaGraphLaunch(f->graph_exec, s));
+    f->step_count++;
+    f->launches += f->graph_launches ? f->graph_launches : per_step;
+  }
+  return RBMD_OK;
+}
+
 rbmd_status parse_config(rbmd_force* f, const char* text) {
   rbmdjson::Value root;
   std::string err;
@@ -1103,6 +1191,10 @@ rbmd_status parse_config(rbmd_force* f, const char* text) {
   f->u = units_for(f->unit);
   f->dt = num(root, "execution.timestep", 0.005);
   f->energy_every = (int)num(root, "outputs.thermo_out.interval", 0.0);
+  {
+    const Value* g = root.path("execution.cuda_graph");
+    if (g && g->kind == Value::Bool) f->use_graph = g->b;
+  }
   std::vector<double> T = nums(root, "execution.temperature");
   f->T0 = T.size() > 0 ? T[0] : 1.0;
   f->Tdamp = T.size() > 2 ? T[2] : 1.0;
@@ -1446,6 +1538,8 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
   if (f->skin > 0) CK(dalloc(&f->d_xref, 3 * n));
   CK(dalloc(&f->d_status, 1));
   CK(cudaMemset(f->d_status, 0, sizeof(uint32_t)));
+  CK(dalloc(&f->d_step, 1));
+  CK(cudaMemset(f->d_step, 0, sizeof(long long)));
   CK(dalloc(&f->d_eslot, 2 * n));
   CK(cudaMemset(f->d_eslot, 0, sizeof(double) * 2 * n));
   CK(dalloc(&f->d_esum, 32));
@@ -1722,7 +1816,7 @@ rbmd_status rbmd_force_sample_k(rbmd_force* f, int64_t step, int32_t* m_xyz, int
   if (f->proposal != "gauss")
     launch_prop_sample(f, nullptr, step, recb);
   else
-    k_sample<kSamplerD><<<f->nrep, 256>>>(f->nrep, f->d_srep, f->d_qtab, f->d_reps, f->seed, step,
+    k_sample<kSamplerD><<<f->nrep, 256>>>(f->nrep, f->d_srep, f->d_qtab, f->d_reps, f->seed, step, nullptr,
                                            f->d_kvec, f->d_krec, recb, f->d_krep, f->d_status);
   CK(cudaGetLastError());
   CK(cudaDeviceSynchronize());
@@ -1807,10 +1901,12 @@ rbmd_status rbmd_force_step(rbmd_force* f, int32_t n_steps, void* stream) {
     if (f->at.image)
       CK(cudaMemcpyAsync(f->d_snap_img, f->at.image, sizeof(int) * 3 * n, cudaMemcpyDeviceToDevice, s));
     f->launches = 0;
-    for (int k = 0; k < n_steps; ++k) {
-      if (f->fp64) launch_step<double>(f, s);
-      else launch_step<float>(f, s);
-    }
+    CK(cudaMemcpyAsync(f->d_step, &f->step_count, sizeof(long long), cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    f->in_step = true;
+    rbmd_status gs = f->fp64 ? run_steps<double>(f, n_steps, s) : run_steps<float>(f, n_steps, s);
+    f->in_step = false;
+    if (gs) return gs;
     CK(cudaGetLastError());
     bool redo = false;
     rbmd_status st = check_overflow(f, s, &redo);
@@ -1995,7 +2091,7 @@ rbmd_status rbmd_force_train_proposal(rbmd_force* f, const rbmd_train_opts* o, r
     k_frac<float><<<(nq0 + 255) / 256, 256, 0, s>>>(nq0, f->d_qidx, f->at.pos, f->at.charge, rep_of, f->d_reps,
                                                      frac);
     k_prop_sample<<<1, 256, 0, s>>>(1, rep1, f->d_prep, f->d_cdf, nullptr, f->d_wbin, o->seed,
-                                    (1LL << 40) + sn, 4096, kv, krec, 12, krep, kw, f->d_status);
+                                    (1LL << 40) + sn, nullptr, 4096, kv, krec, 12, krep, kw, f->d_status);
     const dim3 grid((K + 255) / 256, nch);
     for (int pass = 0; pass < 2; ++pass) {
       k_train_pass<<<grid, 256, 0, s>>>(pass, K, nq0, frac, kv, rho, partial);

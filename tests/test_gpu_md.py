@@ -286,3 +286,50 @@ def test_list_capacity_regrowth(cuda, oracle_lib):
     ff.step(3)
     torch.cuda.synchronize()
     assert ff.status() == 0
+
+
+@pytest.mark.parametrize("proposal", ["gauss", "learned"])
+def test_cuda_graph_replay_is_bit_identical(cuda, proposal):
+    """rbmd_force_step replays a captured step (one graph launch per step); positions and
+    velocities after 25 steps equal those of direct launches bit for bit (every kernel is
+    deterministic and the samplers read the step index from the device counter)."""
+    import torch
+    from oracle import mlp
+    out = []
+    for graph in (True, False):
+        s = systems.electrolyte(3000, seed=17)
+        cfg = systems.electrolyte_config(P=48, precision="fp32", seed=5)
+        cfg["hyper_parameters"]["neighbor"]["skin"] = 0.3
+        cfg["hyper_parameters"]["coulomb"]["proposal"] = proposal
+        cfg["execution"]["cuda_graph"] = graph
+        dev = to_dev(s, cuda)
+        ff = make_ff(cfg, s, dev)
+        if proposal == "learned":
+            ff.proposal_params(mlp.init_params(2, scale=0.5))
+        ff.Execute()
+        ff.step(25)
+        ff.sync_velocities()
+        torch.cuda.synchronize()
+        assert ff.status() == 0
+        out.append((dev["pos"].cpu().numpy(), dev["vel"].cpu().numpy(), ff.list_builds()))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+    assert out[0][2] == out[1][2]
+
+
+def test_cuda_graph_water_shake(cuda):
+    import torch
+    out = []
+    for graph in (True, False):
+        s = systems.water(n_mol=300, seed=4)
+        cfg = systems.water_config(P=32, precision="fp32")
+        cfg["execution"]["cuda_graph"] = graph
+        dev = to_dev(s, cuda)
+        ff = make_ff(cfg, s, dev)
+        ff.Execute()
+        ff.step(12)
+        ff.sync_velocities()
+        torch.cuda.synchronize()
+        assert ff.status() == 0
+        out.append(dev["pos"].cpu().numpy())
+    assert np.array_equal(out[0], out[1])
