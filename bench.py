@@ -148,6 +148,21 @@ def algorithmic(n, nq, n_nbr_mean, P):
 NEAR_TRAFFIC_BYTES_PER_ATOM = 69.4e6 / 200_000
 
 
+def max_over_ranks(value, dist, device):
+    """Maximum of a per-rank scalar over all ranks (the slowest rank's time); identity on one rank."""
+    import torch
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(value)
+    m = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    dist.all_reduce(m, op=dist.ReduceOp.MAX)
+    return float(m.item())
+
+
+def aggregate_rate(world, atoms_per_rank, steps, max_ms):
+    """Whole-job atom-steps/s: every rank advanced its own replica for `steps` steps."""
+    return world * atoms_per_rank * steps / (max_ms / 1e3)
+
+
 def make_handle(s, dev, P, proposal, seed, skin, dt=None, ensemble="NVT", params=None, graph=True):
     """ForceField over a copy of system s on `dev` (1 replica)."""
     import torch
@@ -224,9 +239,7 @@ def timed_run(ff, t, dev, steps, warmup, world, dist, e2e_steps):
     ff.profile(False)
     flags = ff.status()
     if world > 1:
-        m = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(m, op=dist.ReduceOp.MAX)
-        ms = float(m.item())
+        ms = max_over_ranks(ms, dist, dev)
     n = ff.n
     ff.Execute()
     cnt, _ = ff.neighbors(0)
@@ -248,9 +261,7 @@ def timed_run(ff, t, dev, steps, warmup, world, dist, e2e_steps):
     torch.cuda.synchronize(dev)
     e2e_ms = max(a0.elapsed_time(a1), (time.perf_counter() - w0) * 1e3) / e2e_steps
     if world > 1:
-        m = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(m, op=dist.ReduceOp.MAX)
-        e2e_ms = float(m.item())
+        e2e_ms = max_over_ranks(e2e_ms, dist, dev)
     return dict(ms=ms, builds=builds, phases=phases, flags=flags, clk=clk, n_nbr=n_nbr, e2e_ms=e2e_ms,
                 k_per_step=k_per_step, blocks=blocks)
 
@@ -357,8 +368,8 @@ def run_ours(args):
     learned = timed_run(ff, t, dev, args.steps, args.warmup, world, dist, args.e2e_steps)
     ff.close()
 
-    v_plain = world * n * args.steps / (plain["ms"] / 1e3)
-    v_learned = world * n * args.steps / (learned["ms"] / 1e3)
+    v_plain = aggregate_rate(world, n, args.steps, plain["ms"])
+    v_learned = aggregate_rate(world, n, args.steps, learned["ms"])
     out = None
     if rank == 0:
         roof, rl, _ = roofline(learned, n, nq, P_eq, args.steps, dev)
