@@ -42,7 +42,9 @@ EXPORTED = [
     "rbmd_force_get_neighbors", "rbmd_force_get_rbl", "rbmd_force_get_rhok", "rbmd_force_profile",
     "rbmd_force_phase_ms", "rbmd_force_list_builds", "rbmd_force_launch_count",
     "rbmd_force_train_proposal", "rbmd_force_proposal_params", "rbmd_force_get_far",
-    "rbmd_force_destroy", "rbmd_rhok_noalloc", "rbmd_proposal_mlp_eval", "rbmd_version",
+    "rbmd_force_destroy", "rbmd_rhok_noalloc", "rbmd_proposal_mlp_eval", "rbmd_data_read",
+    "rbmd_data_atoms", "rbmd_data_types", "rbmd_data_topology", "rbmd_data_free", "rbmd_data_write",
+    "rbmd_version",
     "rbmd_last_error",
 ]
 
@@ -75,6 +77,13 @@ class rbmd_energy(ctypes.Structure):
     _fields_ = [(k, ctypes.c_double) for k in (
         "lj", "coul_real", "coul_kspace", "coul_self", "eam_embed", "eam_pair", "bond", "angle",
         "kinetic", "temperature")]
+
+
+class rbmd_data_info(ctypes.Structure):
+    _fields_ = [("n_atoms", ctypes.c_int64), ("n_bonds", ctypes.c_int64), ("n_angles", ctypes.c_int64),
+                ("n_atom_types", ctypes.c_int32), ("n_bond_types", ctypes.c_int32), ("n_angle_types", ctypes.c_int32),
+                ("has_velocities", ctypes.c_int32), ("has_pair_coeffs", ctypes.c_int32), ("has_masses", ctypes.c_int32),
+                ("box", rbmd_box)]
 
 
 class rbmd_train_opts(ctypes.Structure):
@@ -130,6 +139,13 @@ def library() -> ctypes.CDLL:
         "rbmd_force_train_proposal": (I32, [V, P(rbmd_train_opts), P(rbmd_train_report), V]),
         "rbmd_force_proposal_params": (I32, [V, P(ctypes.c_float), P(ctypes.c_float)]),
         "rbmd_force_get_far": (I32, [V, P(D)]),
+        "rbmd_data_read": (I32, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, P(V), P(rbmd_data_info)]),
+        "rbmd_data_atoms": (I32, [V, V, V, V, V, V, V, V]),
+        "rbmd_data_types": (I32, [V, V, V, V]),
+        "rbmd_data_topology": (I32, [V, V, V, V, V, V, V]),
+        "rbmd_data_free": (None, [V]),
+        "rbmd_data_write": (I32, [ctypes.c_char_p, ctypes.c_char_p, P(rbmd_data_info), V, V, V, V, V, V, V, V, V,
+                                  V, V]),
         "rbmd_version": (ctypes.c_char_p, []),
         "rbmd_last_error": (ctypes.c_char_p, []),
     }
@@ -414,3 +430,65 @@ class ForceField:
 
 def version() -> str:
     return library().rbmd_version().decode()
+
+
+# ---- LAMMPS data files ----------------------------------------------------------------------
+def read_data(path, atom_style, unit="LJ"):
+    """Read a LAMMPS data file as the reference's read_data does (rbmd_data_read); returns a dict
+    of numpy arrays (0-based types, molecules and ids) and the box."""
+    import numpy as np
+    lib = library()
+    h = ctypes.c_void_p()
+    info = rbmd_data_info()
+    _check(lib.rbmd_data_read(str(path).encode(), atom_style.encode(), unit.encode(), ctypes.byref(h),
+                              ctypes.byref(info)), "rbmd_data_read")
+    try:
+        n, nt = info.n_atoms, info.n_atom_types
+        out = dict(pos=np.zeros((n, 3)), vel=np.zeros((n, 3)), charge=np.zeros(n), type=np.zeros(n, np.int32),
+                   molecule=np.zeros(n, np.int32), mass=np.zeros(n), image=np.zeros((n, 3), np.int32))
+        dp = lambda a: a.ctypes.data_as(ctypes.c_void_p)   # noqa: E731
+        _check(lib.rbmd_data_atoms(h, dp(out["pos"]), dp(out["vel"]), dp(out["charge"]), dp(out["type"]),
+                                   dp(out["molecule"]), dp(out["mass"]), dp(out["image"])), "rbmd_data_atoms")
+        out["mass_by_type"] = np.zeros(nt)
+        if info.has_pair_coeffs:
+            out["eps"], out["sigma"] = np.zeros(nt), np.zeros(nt)
+            _check(lib.rbmd_data_types(h, dp(out["mass_by_type"]), dp(out["eps"]), dp(out["sigma"])), "types")
+        else:
+            _check(lib.rbmd_data_types(h, dp(out["mass_by_type"]), None, None), "types")
+        out["bonds"] = np.zeros((info.n_bonds, 2), np.int32)
+        out["angles"] = np.zeros((info.n_angles, 3), np.int32)
+        out["bond_coeffs"] = np.zeros((max(info.n_bond_types, 0), 2))
+        out["angle_coeffs"] = np.zeros((max(info.n_angle_types, 0), 2))
+        _check(lib.rbmd_data_topology(h, dp(out["bonds"]), None, dp(out["angles"]), None, dp(out["bond_coeffs"]),
+                                      dp(out["angle_coeffs"])), "topology")
+        out["lo"] = np.array(info.box.lo[:])
+        out["hi"] = np.array(info.box.hi[:])
+        out["has_velocities"] = bool(info.has_velocities)
+        return out
+    finally:
+        lib.rbmd_data_free(h)
+
+
+def write_data(path, atom_style, d):
+    """Write arrays in the dict form of read_data as a LAMMPS data file (rbmd_data_write)."""
+    import numpy as np
+    info = rbmd_data_info()
+    n = d["pos"].shape[0]
+    info.n_atoms = n
+    mt = np.ascontiguousarray(d.get("mass_by_type", np.ones(int(d["type"].max()) + 1)), np.float64)
+    info.n_atom_types = len(mt)
+    bonds = d.get("bonds")
+    angles = d.get("angles")
+    info.n_bonds = 0 if bonds is None else len(bonds)
+    info.n_angles = 0 if angles is None else len(angles)
+    info.n_bond_types = 1
+    info.n_angle_types = 1
+    info.box = rbmd_box(tuple(d["lo"]), tuple(d["hi"]))
+    c = lambda a, t: None if a is None else np.ascontiguousarray(a, t)   # noqa: E731
+    arrs = [c(d["pos"], np.float64), c(d.get("vel"), np.float64), c(d.get("charge"), np.float64),
+            c(d["type"], np.int32), c(d.get("molecule"), np.int32), c(d.get("image"), np.int32), mt,
+            c(d.get("eps"), np.float64), c(d.get("sigma"), np.float64),
+            c(bonds, np.int32) if info.n_bonds else None, c(angles, np.int32) if info.n_angles else None]
+    ptrs = [None if a is None else a.ctypes.data_as(ctypes.c_void_p) for a in arrs]
+    _check(library().rbmd_data_write(str(path).encode(), atom_style.encode(), ctypes.byref(info), *ptrs),
+           "rbmd_data_write")

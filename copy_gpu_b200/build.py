@@ -14,7 +14,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "librbmd_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", f) for f in ("rbmd_force.cu", "rhok_noalloc.cu", "proposal.cu")]
+SOURCES = [os.path.join(HERE, "csrc", f) for f in ("rbmd_force.cu", "rhok_noalloc.cu", "proposal.cu", "data_io.cpp")]
 DEPS = [os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc"))] + [
     os.path.join(ROOT, "include", "rbmd_force.h")
 ]

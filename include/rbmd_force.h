@@ -280,6 +280,38 @@ RBMD_API rbmd_status rbmd_force_proposal_params(rbmd_force* f, float* get_host, 
  * noise.  Mirrors the far force of ExecutionNVT::EleNewForce (rbmd/framework/run/ExecutionNVT.cpp:717-733). */
 RBMD_API rbmd_status rbmd_force_get_far(rbmd_force* f, double* far_host);
 
+/* ---- LAMMPS data files (the reference's read_data input) ------------------------------------
+ * rbmd_data_read parses a data file as ModelFileInitCondition does
+ * (rbmd/framework/InitCondition/ModelFileInitCondition.cpp:120-605): header counts, Masses,
+ * Pair Coeffs, Bond/Angle Coeffs, Atoms in style "atomic" | "charge" | "full", Bonds, Angles,
+ * Velocities; ids, types and molecules 0-based, atoms ordered by id; unit "LJ" sets every mass
+ * to 1 as the reference does.  The accessors copy into caller-allocated host arrays (NULL skips
+ * an array): positions/velocities [n][3], charge/mass [n], type/molecule [n], image flags [n][3]
+ * (optional columns after the coordinates, 0 when absent), per-type masses / epsilon / sigma
+ * [n_atom_types], bonds [n_bonds][2], angles [n_angles][3] (caller atom ids), bond / angle
+ * coefficients [types][2] = (k, r0 | theta0 in degrees).  rbmd_data_write writes the same format
+ * (checkpoints that double as inputs; image flags kept). */
+typedef struct rbmd_data rbmd_data;
+typedef struct {
+  int64_t n_atoms, n_bonds, n_angles;
+  int32_t n_atom_types, n_bond_types, n_angle_types;
+  int32_t has_velocities, has_pair_coeffs, has_masses;
+  rbmd_box box;
+} rbmd_data_info;
+RBMD_API rbmd_status rbmd_data_read(const char* path, const char* atom_style, const char* unit, rbmd_data** out,
+                                    rbmd_data_info* info);
+RBMD_API rbmd_status rbmd_data_atoms(const rbmd_data* d, double* pos, double* vel, double* charge, int32_t* type,
+                                     int32_t* molecule, double* mass, int32_t* image);
+RBMD_API rbmd_status rbmd_data_types(const rbmd_data* d, double* mass_by_type, double* epsilon, double* sigma);
+RBMD_API rbmd_status rbmd_data_topology(const rbmd_data* d, int32_t* bonds, int32_t* bond_type, int32_t* angles,
+                                        int32_t* angle_type, double* bond_coeffs, double* angle_coeffs);
+RBMD_API void rbmd_data_free(rbmd_data* d);
+RBMD_API rbmd_status rbmd_data_write(const char* path, const char* atom_style, const rbmd_data_info* info,
+                                     const double* pos, const double* vel, const double* charge,
+                                     const int32_t* type, const int32_t* molecule, const int32_t* image,
+                                     const double* mass_by_type, const double* epsilon, const double* sigma,
+                                     const int32_t* bonds, const int32_t* angles);
+
 /* Version string of the library build. */
 RBMD_API const char* rbmd_version(void);
 
