@@ -197,11 +197,16 @@ __global__ void __launch_bounds__(256) k_cell_sort_gather(
 }
 
 // Refresh the slot caches from the master positions without re-binning (list reuse with skin).
+// With xref (positions at the last build) the cached position is unwrapped: xref plus the
+// minimum-image displacement since the build.  A listed pair's stored image shift then stays
+// valid however often either atom crossed a face, so the pair kernels need no minimum-image
+// step; the displacement is below skin/2, far under half a box.
 template <class R>
 __global__ void k_regather(int n, const int* __restrict__ slot_atom, const double* __restrict__ pos,
                            const double* __restrict__ charge, const int* __restrict__ rep_of,
                            const RepDev* __restrict__ reps, typename Traits<R>::V4* __restrict__ pos4,
-                           void* __restrict__ frac_out, const int* __restrict__ rebuild) {
+                           void* __restrict__ frac_out, const double* __restrict__ xref,
+                           const int* __restrict__ rebuild) {
   if (rebuild && *rebuild) return;   // the cell sort refreshed the caches this step
   int slot = blockIdx.x * blockDim.x + threadIdx.x;
   if (slot >= n) return;
@@ -209,7 +214,21 @@ __global__ void k_regather(int n, const int* __restrict__ slot_atom, const doubl
   const double x = pos[3 * id], y = pos[3 * id + 1], z = pos[3 * id + 2];
   const double q = charge ? charge[id] : 0.0;
   typename Traits<R>::V4 v;
-  v.x = (R)x; v.y = (R)y; v.z = (R)z; v.w = (R)q;
+  if (xref) {
+    const RepDev& rp = reps[rep_of ? rep_of[id] : 0];
+    double u[3] = {x, y, z};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double r0 = xref[3 * id + d];
+      double dd = u[d] - r0;
+      dd -= rp.box_d[d] * rint(dd / rp.box_d[d]);
+      u[d] = r0 + dd;
+    }
+    v.x = (R)u[0]; v.y = (R)u[1]; v.z = (R)u[2];
+  } else {
+    v.x = (R)x; v.y = (R)y; v.z = (R)z;
+  }
+  v.w = (R)q;
   pos4[slot] = v;
   if (frac_out) {
     const RepDev& rp = reps[rep_of ? rep_of[id] : 0];

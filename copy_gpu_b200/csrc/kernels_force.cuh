@@ -108,8 +108,9 @@ __device__ __forceinline__ void rbe_terms(const typename FracT<R>::T& fr, const 
 //   kMiNone  every replica has >= 3 cells per axis and the list is rebuilt every step: listed
 //            pairs have |r_d| < rc < L/2, MinDistanceVec is the identity;
 //   kMiLJ    the reference's semantics for small boxes: MinDistanceVec on the LJ vector only;
-//   kMiAll   Verlet skin: atoms wrapped since the last build make the stored image stale, so
-//            the pair vector itself is reduced to the minimum image.
+//   kMiAll   Verlet skin: pairs listed at rc + skin are filtered by the list predicate at rc;
+//            the cached positions are unwrapped since the build (k_regather), so the stored
+//            image shift still gives the minimum-image vector.
 constexpr int kMiNone = 0, kMiLJ = 1, kMiAll = 2;
 
 template <class R>
@@ -117,15 +118,6 @@ __device__ __forceinline__ void min_image(R& q0, R& q1, R& q2, const R* box) {
   if (fabs(q0) > box[0] * (R)0.5) q0 -= (q0 > 0 ? box[0] : -box[0]);
   if (fabs(q1) > box[1] * (R)0.5) q1 -= (q1 > 0 ? box[1] : -box[1]);
   if (fabs(q2) > box[2] * (R)0.5) q2 -= (q2 > 0 ? box[2] : -box[2]);
-}
-
-// Nearest image for list reuse: the two atoms of a listed pair may each have wrapped across a
-// face since the build, so the stored vector can be off by up to two box lengths.
-template <class R>
-__device__ __forceinline__ void nearest_image(R& q0, R& q1, R& q2, const R* box, const R* ibox) {
-  q0 -= box[0] * rint(q0 * ibox[0]);
-  q1 -= box[1] * rint(q1 * ibox[1]);
-  q2 -= box[2] * rint(q2 * ibox[2]);
 }
 
 // approximate reciprocal (one MUFU op, about 1 ulp): the pair terms carry a 1e-5 budget
@@ -176,7 +168,6 @@ __global__ void __launch_bounds__(256) k_near_force(
   const R cut2 = rc * rc;
   const R box[3] = {Traits<R>::box(rp, 0), Traits<R>::box(rp, 1), Traits<R>::box(rp, 2)};
   const R wrap[3] = {Traits<R>::wrap(rp, 0), Traits<R>::wrap(rp, 1), Traits<R>::wrap(rp, 2)};
-  const R ibox[3] = {(R)1 / box[0], (R)1 / box[1], (R)1 / box[2]};
   const R sa = (R)prm.sqrt_alpha, aa = (R)prm.alpha, c2 = (R)prm.two_sqrt_alpha_over_sqrt_pi;
   const R cs = (R)prm.coul_scale;
   const R qi = pi.w;
@@ -205,8 +196,7 @@ __global__ void __launch_bounds__(256) k_near_force(
       py = py - (c1 == 1 ? wrap[1] : (c1 == 2 ? -wrap[1] : (R)0));
       pz = pz - (c2b == 1 ? wrap[2] : (c2b == 2 ? -wrap[2] : (R)0));
     }
-    R r0 = px - pi.x, r1 = py - pi.y, r2 = pz - pi.z;
-    if (MI == kMiAll) nearest_image(r0, r1, r2, box, ibox);
+    const R r0 = px - pi.x, r1 = py - pi.y, r2 = pz - pi.z;
     const R d2 = r0 * r0 + r1 * r1 + r2 * r2;
     if (MI == kMiAll && !(cut2 - d2 > (R)1.0e-4 && d2 > (R)1.0e-4)) continue;
     R f = 0;

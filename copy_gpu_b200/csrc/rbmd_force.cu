@@ -675,7 +675,7 @@ void launch_sort(rbmd_force* f, cudaStream_t s, bool bin) {
     // list reuse: refresh the slot caches from the new positions (no-op on rebuild steps)
     k_regather<R><<<(n + 255) / 256, 256, 0, s>>>(
         n, f->d_slot_atom, f->at.pos, f->at.charge, f->nrep > 1 ? f->d_rep_of : nullptr, f->d_reps,
-        (typename Traits<R>::V4*)f->d_pos4, nullptr, rb);
+        (typename Traits<R>::V4*)f->d_pos4, nullptr, f->d_xref, rb);
     f->launches++;
   }
 }

@@ -53,6 +53,7 @@ def test_pairs_edge_cases(cuda, oracle_lib, prec):
     pos = rng.uniform(0, L, size=(300, 3))
     pos[:8] = np.array([[0, 0, 0], [L, 0, 0], [0, L, 0], [0, 0, L], [L, L, L], [L / 2, 0, L],
                         [2.5, 2.5, 2.5], [5.0, 5.0, 5.0]])
+    pos[9] = np.array([1.0, 3.0, 3.0])
     pos[8] = pos[9] + np.array([2.5, 0, 0])          # exactly at the cutoff distance
     s = dict(pos=pos, vel=np.zeros_like(pos), mass=np.ones(300), charge=np.zeros(300),
              type=np.zeros(300, np.int32), molecule=None, lo=np.zeros(3), hi=np.full(3, L),
@@ -173,3 +174,25 @@ def test_sampler_matches_oracle(cuda, oracle_lib):
         ref = oracle_lib.rbe_sample(alpha, L, seed=1234, step=step, rep=0, P=P)
         assert np.array_equal(got, ref), f"step {step}"
         assert not np.any(np.all(got == 0, axis=1))
+
+
+def test_atoms_outside_box(cuda, oracle_lib):
+    """Caller positions up to one cell outside the box: the reference's grid bins them into the
+    boundary cells and meets them there; the pair set is reproduced exactly."""
+    import torch
+    rng = np.random.default_rng(6)
+    L = 9.1
+    pos = rng.uniform(0, L, size=(400, 3))
+    pos[:40] += rng.uniform(-1.0, 1.0, size=(40, 3))
+    s = dict(pos=pos, vel=np.zeros_like(pos), mass=np.ones(400), charge=np.zeros(400),
+             type=np.zeros(400, np.int32), molecule=None, lo=np.zeros(3), hi=np.full(3, L),
+             eps=np.ones(1), sigma=np.ones(1))
+    cfg = systems.lj_config(cutoff=2.5, precision="fp32")
+    dev = to_dev(s, cuda)
+    ff = make_ff(cfg, s, dev)
+    ff.Execute()
+    torch.cuda.synchronize()
+    assert ff.status() == 0
+    c, ids = ff.neighbors(512)
+    nl = oracle_lib.neighbors(_posr(pos, "fp32"), s["lo"], s["hi"], 2.5, "fp32")
+    assert pair_sets_equal(c, ids, nl[0], nl[1]) == -1
