@@ -25,10 +25,12 @@ __device__ __forceinline__ int cell_of_pos(const RepDev& rp, R x, R y, R z) {
   return rp.cell_base + ijk[0] + ijk[1] * rp.dims[0] + ijk[2] * rp.dims[0] * rp.dims[1];
 }
 
+// rebuild (nullable): bin only on list-rebuild steps (Verlet skin).
 template <class R>
 __global__ void k_bin(int n, const double* __restrict__ pos, const int* __restrict__ rep_of,
                       const RepDev* __restrict__ reps, int* __restrict__ cell_of,
-                      int* __restrict__ cell_count, uint32_t* status) {
+                      int* __restrict__ cell_count, uint32_t* status, const int* __restrict__ rebuild) {
+  if (rebuild && !*rebuild) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const RepDev& rp = reps[rep_of ? rep_of[i] : 0];
@@ -221,7 +223,7 @@ __global__ void k_regather(int n, const int* __restrict__ slot_atom, const doubl
     for (int d = 0; d < 3; ++d) {
       const double r0 = xref[3 * id + d];
       double dd = u[d] - r0;
-      dd -= rp.box_d[d] * rint(dd / rp.box_d[d]);
+      if (fabs(dd) > 0.5 * rp.box_d[d]) dd -= (dd > 0 ? rp.box_d[d] : -rp.box_d[d]);
       u[d] = r0 + dd;
     }
     v.x = (R)u[0]; v.y = (R)u[1]; v.z = (R)u[2];
@@ -285,18 +287,13 @@ __device__ __forceinline__ int nlist_range(int s, const int s1, const typename T
   return idx;
 }
 
+// Per-thread traversal of slot i's 27-cell stencil straight from global memory; returns the
+// number of pairs found (entries beyond cap are counted, not stored).
 template <class R>
-__global__ void __launch_bounds__(256) k_nlist(
-    int n, const typename Traits<R>::V4* __restrict__ pos4, const int* __restrict__ cell_start,
-    const RepDev* __restrict__ reps, const int* __restrict__ rep_of_slot, int num_cycles, R rc,
-    int cap, int stride, int* __restrict__ nbr, int* __restrict__ count, int* __restrict__ max_count,
-    uint32_t* status, const int* __restrict__ rebuild, unsigned long long* __restrict__ nbuilds) {
-  if (rebuild && !*rebuild) return;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i == 0 && nbuilds) atomicAdd(nbuilds, 1ull);
-  if (i >= n) return;
-  const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
-  const typename Traits<R>::V4 pi = pos4[i];
+__device__ int nlist_thread(int i, const typename Traits<R>::V4 pi, const RepDev& rp,
+                            const typename Traits<R>::V4* __restrict__ pos4,
+                            const int* __restrict__ cell_start, int num_cycles, R rc, int cap, int stride,
+                            int* __restrict__ nbr) {
   const R pix[3] = {pi.x, pi.y, pi.z};
   int ci[3];
 #pragma unroll
@@ -333,10 +330,154 @@ __global__ void __launch_bounds__(256) k_nlist(
         }
       }
     }
+  return idx;
+}
+
+__device__ __forceinline__ void nlist_finish(int i, int idx, int cap, int* __restrict__ count,
+                                             int* __restrict__ max_count, uint32_t* status) {
   count[i] = idx;
   if (idx > cap) {
     set_flag(status, kFlagListOverflow);
     atomicMax(max_count, idx);
+  }
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_nlist(
+    int n, const typename Traits<R>::V4* __restrict__ pos4, const int* __restrict__ cell_start,
+    const RepDev* __restrict__ reps, const int* __restrict__ rep_of_slot, int num_cycles, R rc,
+    int cap, int stride, int* __restrict__ nbr, int* __restrict__ count, int* __restrict__ max_count,
+    uint32_t* status, const int* __restrict__ rebuild, unsigned long long* __restrict__ nbuilds) {
+  if (rebuild && !*rebuild) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0 && nbuilds) atomicAdd(nbuilds, 1ull);
+  if (i >= n) return;
+  const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
+  const int idx = nlist_thread<R>(i, pos4[i], rp, pos4, cell_start, num_cycles, rc, cap, stride, nbr);
+  nlist_finish(i, idx, cap, count, max_count, status);
+}
+
+// ---- staged list build ------------------------------------------------------------------
+// One block per segment of kSeg consecutive x cells of one (y, z) cell row.  The block copies
+// the positions of its 9 neighbour rows x (segment + 1 cell each side) into shared memory once,
+// already shifted by their periodic offsets and tagged with (slot << 6 | image code), and every
+// atom of the segment walks its 27 cells there.  Cells are visited in the same order, with the
+// same float operations, as k_nlist, so the list is identical entry for entry.  A segment whose
+// staged atoms exceed the shared buffer, or an atom whose own cell index falls outside the
+// segment (binning clamps positions at the upper face), takes k_nlist's global-memory path.
+struct ListSeg { int rep, y, z, x0, x1, pad0, pad1, pad2; };
+constexpr int kStageThreads = 256;
+constexpr int kSegMaxCells = 32;
+constexpr int kStageCells = 9 * (kSegMaxCells + 2);
+
+__device__ __forceinline__ float pack_tag(float, int v) { return __int_as_float(v); }
+__device__ __forceinline__ double pack_tag(double, int v) { return (double)v; }
+__device__ __forceinline__ int unpack_tag(float v) { return __float_as_int(v); }
+__device__ __forceinline__ int unpack_tag(double v) { return (int)v; }
+
+template <class R>
+__global__ void __launch_bounds__(kStageThreads) k_nlist_staged(
+    const ListSeg* __restrict__ segs, int stage_cap, const typename Traits<R>::V4* __restrict__ pos4,
+    const int* __restrict__ cell_start, const RepDev* __restrict__ reps, R rc, int cap, int stride,
+    int* __restrict__ nbr, int* __restrict__ count, int* __restrict__ max_count, uint32_t* status,
+    const int* __restrict__ rebuild, unsigned long long* __restrict__ nbuilds) {
+  using V4 = typename Traits<R>::V4;
+  if (rebuild && !*rebuild) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && nbuilds) atomicAdd(nbuilds, 1ull);
+  extern __shared__ __align__(16) unsigned char stage_raw[];
+  V4* stage = reinterpret_cast<V4*>(stage_raw);
+  __shared__ int cs[kStageCells + 1];     // staged start of staged cell k = row * W + u
+  __shared__ int cell_k[kStageCells];     // its global cell index
+  __shared__ int cnt_k[kStageCells];      // its atom count
+  const ListSeg sg = segs[blockIdx.x];
+  const RepDev& rp = reps[sg.rep];
+  const int S = sg.x1 - sg.x0, W = S + 2, K = 9 * W;
+  const int d0 = rp.dims[0], d1 = rp.dims[1], d2 = rp.dims[2];
+  for (int k = threadIdx.x; k < K; k += blockDim.x) {
+    const int r = k / W, u = k - r * W;
+    const int wy = ((sg.y + r / 3 - 1) % d1 + d1) % d1, wz = ((sg.z + r % 3 - 1) % d2 + d2) % d2;
+    const int wx = ((sg.x0 - 1 + u) % d0 + d0) % d0;
+    const int cell = rp.cell_base + wx + wy * d0 + wz * d0 * d1;
+    cell_k[k] = cell;
+    cnt_k[k] = cell_start[cell + 1] - cell_start[cell];
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {   // exclusive scan of the K counts: lane chunks, then a warp scan
+    const int lane = threadIdx.x, per = (K + 31) / 32, k0 = min(lane * per, K), k1 = min(k0 + per, K);
+    int sum = 0;
+    for (int k = k0; k < k1; ++k) sum += cnt_k[k];
+    int incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    int run = incl - sum;
+    for (int k = k0; k < k1; ++k) {
+      cs[k] = run;
+      run += cnt_k[k];
+    }
+    if (lane == 31) cs[K] = incl;
+  }
+  __syncthreads();
+  const int total = cs[K];
+  const bool staged = total <= stage_cap;
+  const R cut2 = mul_rn(rc, rc);
+  if (staged) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int k = warp; k < K; k += nw) {
+      const int r = k / W, u = k - r * W;
+      const int nby = sg.y + r / 3 - 1, nbz = sg.z + r % 3 - 1, nbx = sg.x0 - 1 + u;
+      const int dy = ((nby % d1) + d1) % d1 - nby, dz = ((nbz % d2) + d2) % d2 - nbz;
+      const int dx = ((nbx % d0) + d0) % d0 - nbx;
+      const R o0 = mul_rn(Traits<R>::dx(rp, 0), (R)dx), o1 = mul_rn(Traits<R>::dx(rp, 1), (R)dy),
+              o2 = mul_rn(Traits<R>::dx(rp, 2), (R)dz);
+      const int code = (dx > 0 ? 1 : (dx < 0 ? 2 : 0)) | ((dy > 0 ? 1 : (dy < 0 ? 2 : 0)) << 2) |
+                       ((dz > 0 ? 1 : (dz < 0 ? 2 : 0)) << 4);
+      const int c0 = cell_start[cell_k[k]], cnt = cnt_k[k], base = cs[k];
+      for (int t = lane; t < cnt; t += 32) {
+        const V4 pj = pos4[c0 + t];
+        V4 v;
+        v.x = sub_rn(pj.x, o0);
+        v.y = sub_rn(pj.y, o1);
+        v.z = sub_rn(pj.z, o2);
+        v.w = pack_tag(v.x, ((c0 + t) << kShiftBits) | code);
+        stage[base + t] = v;
+      }
+    }
+  }
+  __syncthreads();
+  const int row0 = rp.cell_base + sg.y * d0 + sg.z * d0 * d1;
+  const int s0 = cell_start[row0 + sg.x0], s1 = cell_start[row0 + sg.x1];
+  for (int i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
+    const V4 pi = pos4[i];
+    const R pix[3] = {pi.x, pi.y, pi.z};
+    int ci[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      ci[d] = (int)div_rn(sub_rn(pix[d], Traits<R>::lo(rp, d)), Traits<R>::dx(rp, d));
+    int idx = 0;
+    if (staged && ci[1] == sg.y && ci[2] == sg.z && ci[0] >= sg.x0 && ci[0] < sg.x1) {
+      const int u0 = ci[0] - sg.x0;   // staged cells u0 .. u0 + 2 of every row
+      for (int r = 0; r < 9; ++r) {
+        const int t1 = cs[r * W + u0 + 3];
+#pragma unroll 4
+        for (int t = cs[r * W + u0]; t < t1; ++t) {
+          const V4 q = stage[t];
+          const R r0 = sub_rn(q.x, pix[0]);
+          const R r1 = sub_rn(q.y, pix[1]);
+          const R r2 = sub_rn(q.z, pix[2]);
+          const R dd = add_rn(add_rn(mul_rn(r0, r0), mul_rn(r1, r1)), mul_rn(r2, r2));
+          if (gt_small(sub_rn(cut2, dd)) && gt_small(dd)) {
+            if (idx < cap) nbr[(size_t)idx * stride + i] = unpack_tag(q.w);
+            ++idx;
+          }
+        }
+      }
+    } else {
+      idx = nlist_thread<R>(i, pi, rp, pos4, cell_start, 1, rc, cap, stride, nbr);
+    }
+    nlist_finish(i, idx, cap, count, max_count, status);
   }
 }
 

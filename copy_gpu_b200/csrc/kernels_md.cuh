@@ -19,7 +19,11 @@ struct MdParams {
 // Stage 1+2 of ExecutionNVT::Solve (rbmd/framework/run/ExecutionNVT.cpp:136-140):
 // UpdateVelocityWorklet v += 0.5 F/m dt fmt2v (RunWorklet.cpp:1764-1782), then
 // UpdatePosition(Flag)Worklet x += v dt with one wrap per axis (RunWorklet.cpp:1833-1877,
-// ExecPointLocator.h:321-357), fused with the cell binning of the new positions.
+// ExecPointLocator.h:321-357), fused with the cell binning of the new positions (cell_of /
+// cell_count non-null; with a Verlet skin the binning runs only on rebuild steps, in k_bin).
+// With a skin the same pass checks the displacement since the last build and, given pos4,
+// writes the slot cache of the near pass: xref + the minimum-image displacement (unwrapped, as
+// k_regather does) and the charge.
 template <class R>
 __global__ void k_kick_drift(MdParams mp, double* __restrict__ pos, double* __restrict__ vel,
                              const double* __restrict__ force, const double* __restrict__ mass,
@@ -27,7 +31,9 @@ __global__ void k_kick_drift(MdParams mp, double* __restrict__ pos, double* __re
                              const RepDev* __restrict__ reps, const double* __restrict__ lambda,
                              double* __restrict__ x_old, double* __restrict__ v_old,
                              int* __restrict__ cell_of, int* __restrict__ cell_count, uint32_t* status,
-                             const double* __restrict__ xref, double half_skin2, int* __restrict__ rebuild) {
+                             const double* __restrict__ xref, double half_skin2, int* __restrict__ rebuild,
+                             const int* __restrict__ atom_slot, const double* __restrict__ charge,
+                             typename Traits<R>::V4* __restrict__ pos4) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= mp.n) return;
   const int r = rep_of ? rep_of[i] : 0;
@@ -58,18 +64,28 @@ __global__ void k_kick_drift(MdParams mp, double* __restrict__ pos, double* __re
   if (bad) set_flag(status, kFlagOutOfBox);
   if (!isfinite(x[0]) || !isfinite(x[1]) || !isfinite(x[2])) set_flag(status, kFlagNonFinite);
   if (xref) {   // Verlet skin: rebuild once any atom moved more than skin/2 since the last build
-    double d2 = 0;
+    double d2 = 0, u[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      double dd = x[d] - xref[3 * i + d];
+      const double r0 = xref[3 * i + d];
+      double dd = x[d] - r0;
       if (fabs(dd) > 0.5 * rp.box_d[d]) dd -= (dd > 0 ? rp.box_d[d] : -rp.box_d[d]);
       d2 += dd * dd;
+      u[d] = r0 + dd;
     }
     if (d2 > half_skin2 && *rebuild == 0) atomicExch(rebuild, 1);
+    if (pos4) {   // on a rebuild step the cell sort overwrites the whole cache afterwards
+      typename Traits<R>::V4 v;
+      v.x = (R)u[0]; v.y = (R)u[1]; v.z = (R)u[2];
+      v.w = (R)(charge ? charge[i] : 0.0);
+      pos4[atom_slot[i]] = v;
+    }
   }
-  const int c = cell_of_pos<R>(rp, (R)x[0], (R)x[1], (R)x[2]);
-  cell_of[i] = c;
-  atomicAdd(&cell_count[c], 1);
+  if (cell_of) {
+    const int c = cell_of_pos<R>(rp, (R)x[0], (R)x[1], (R)x[2]);
+    cell_of[i] = c;
+    atomicAdd(&cell_count[c], 1);
+  }
 }
 
 // Verlet-skin check for a force call on externally supplied positions: flag a list rebuild when

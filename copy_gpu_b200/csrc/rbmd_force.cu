@@ -115,7 +115,8 @@ struct rbmd_force {
   double shake_tol = 1e-5;
   int energy_every = 0;   // energies inside step(): every outputs.thermo_out.interval steps
   int cap_override = 0;   // neighbor.capacity: initial list capacity (grown on overflow)
-  int tpa_list = 128, tpa_near = 128;   // threads per block of the list build / force pass
+  int tpa_list = 0, tpa_near = 128;     // list build: 0 = staged kernel, else threads per block of
+                                        // k_nlist; threads per block of the force pass
   bool autotune = false;                // "autotune": true tunes them at the first compute
   bool tuned = false;
   bool list_valid = false;   // a list (and x_ref) exists from an earlier build
@@ -169,6 +170,8 @@ struct rbmd_force {
   float* d_erf_tab = nullptr;   // compat.rbl_erf_table
   int *d_rebuild = nullptr, *d_block_sums = nullptr;
   unsigned long long* d_nbuilds = nullptr;
+  ListSeg* d_segs = nullptr;   // staged list build: one block per segment of a cell row
+  int nsegs = 0, stage_cap = 0;
   double* d_xref = nullptr;
   uint32_t* d_status = nullptr;
   double* d_eslot = nullptr;   // 2 per slot (lj, coul)
@@ -176,6 +179,7 @@ struct rbmd_force {
   // RBE
   int Ptot = 0, nitems = 0, rho_threads = 64, ktile = 128, kstage = 0;
   bool minimg = true, want_energy = true;
+  bool kspace_priority = true;   // execution.kspace_priority: side stream at the highest priority
   int* d_krep = nullptr;
   int nq = 0;               // charged atoms (the k-space path runs over these only)
   int* d_qidx = nullptr;
@@ -303,6 +307,8 @@ void free_all(rbmd_force* f) {
   dfree(f->d_prep); dfree(f->d_cdf); dfree(f->d_wbin); dfree(f->d_pw); dfree(f->d_mlp); dfree(f->d_h);
   dfree(f->d_feat); dfree(f->d_spec); dfree(f->d_spec_init);
   dfree(f->d_rebuild); dfree(f->d_block_sums); dfree(f->d_xref); dfree(f->d_nbuilds);
+  dfree(f->d_segs);
+  f->nsegs = 0;
   dfree(f->d_eslot); dfree(f->d_esum);
   if (f->d_krec) cudaFree(f->d_krec);
   f->d_krec = nullptr;
@@ -632,7 +638,16 @@ double rbe_S(double alpha, const double* L) {
 template <class R>
 void launch_nlist(rbmd_force* f, cudaStream_t s) {
   PhaseScope ps(f, kPhList, s);
-  const int bs = f->tpa_list;
+  if (f->tpa_list == 0 && f->nsegs > 0) {
+    const size_t smem = (size_t)f->stage_cap * sizeof(typename Traits<R>::V4);
+    k_nlist_staged<R><<<f->nsegs, kStageThreads, smem, s>>>(
+        f->d_segs, f->stage_cap, (const typename Traits<R>::V4*)f->d_pos4, f->d_cell_start, f->d_reps,
+        (R)f->list_cut(), f->cap, f->stride, f->d_nbr, f->d_count, f->d_maxcount, f->d_status,
+        f->skin > 0 ? f->d_rebuild : nullptr, f->d_nbuilds);
+    f->launches++;
+    return;
+  }
+  const int bs = f->tpa_list > 0 ? f->tpa_list : 128;
   k_nlist<R><<<(f->n + bs - 1) / bs, bs, 0, s>>>(
       f->n, (const typename Traits<R>::V4*)f->d_pos4, f->d_cell_start, f->d_reps,
       f->nrep > 1 ? f->d_rep_of : nullptr, f->num_cycles, (R)f->list_cut(), f->cap, f->stride, f->d_nbr,
@@ -650,15 +665,17 @@ void launch_rbl_list(rbmd_force* f, cudaStream_t s) {
   f->launches++;
 }
 
+// bin: run k_bin (positions given by the caller, or a Verlet skin whose drift does not bin);
+// regather: refresh the slot caches on list-reuse steps (the drift did not write them).
 template <class R>
-void launch_sort(rbmd_force* f, cudaStream_t s, bool bin) {
+void launch_sort(rbmd_force* f, cudaStream_t s, bool bin, bool regather) {
   PhaseScope ps(f, kPhSort, s);
   const int n = f->n;
   const int* rb = f->skin > 0 ? f->d_rebuild : nullptr;
   if (bin) {
     cudaMemsetAsync(f->d_cell_count, 0, sizeof(int) * f->ncell_total, s);
     k_bin<R><<<(n + 255) / 256, 256, 0, s>>>(n, f->at.pos, f->nrep > 1 ? f->d_rep_of : nullptr,
-                                             f->d_reps, f->d_cell_of, f->d_cell_count, f->d_status);
+                                             f->d_reps, f->d_cell_of, f->d_cell_count, f->d_status, rb);
     f->launches++;
   }
   const int nblk = (f->ncell_total + kScanBlock - 1) / kScanBlock;
@@ -671,7 +688,7 @@ void launch_sort(rbmd_force* f, cudaStream_t s, bool bin) {
       f->nrep > 1 ? f->d_rep_of : nullptr, f->d_reps, f->d_slot_atom, f->d_atom_slot,
       (typename Traits<R>::V4*)f->d_pos4, nullptr, f->d_meta, f->d_xref, rb);
   f->launches += 4;
-  if (rb) {
+  if (rb && regather) {
     // list reuse: refresh the slot caches from the new positions (no-op on rebuild steps)
     k_regather<R><<<(n + 255) / 256, 256, 0, s>>>(
         n, f->d_slot_atom, f->at.pos, f->at.charge, f->nrep > 1 ? f->d_rep_of : nullptr, f->d_reps,
@@ -903,14 +920,14 @@ void launch_water(rbmd_force* f, cudaStream_t s) {
 // stream, the cell sort / neighbour list / near pass / intramolecular terms run on the caller's
 // stream, and the far force is folded in after the join.
 template <class R>
-void launch_force_tail(rbmd_force* f, cudaStream_t s, bool bin) {
+void launch_force_tail(rbmd_force* f, cudaStream_t s, bool bin, bool regather) {
   const bool kspace = f->is_rbe();
   if (kspace) {
     cudaEventRecord(f->ev_fork, s);
     launch_kspace<R>(f, f->side, f->ev_fork);
     cudaEventRecord(f->ev_join, f->side);
   }
-  launch_sort<R>(f, s, bin);
+  launch_sort<R>(f, s, bin, regather);
   if (f->is_rbl()) {
     launch_rbl_list<R>(f, s);
     PhaseScope ps(f, kPhForce, s);
@@ -948,7 +965,7 @@ void launch_compute(rbmd_force* f, cudaStream_t s) {
   } else if (f->d_rebuild) {
     cudaMemsetAsync(f->d_rebuild, 1, sizeof(int), s);   // nonzero: rebuild
   }
-  launch_force_tail<R>(f, s, true);
+  launch_force_tail<R>(f, s, true, true);
   f->list_valid = true;
 }
 
@@ -1009,9 +1026,14 @@ void launch_step(rbmd_force* f, cudaStream_t s) {
   mp.nh = f->tstat == 3;
   f->want_energy = f->energy_every > 0 && ((f->step_count + 1) % f->energy_every == 0);
   cudaMemsetAsync(f->d_maxcount, 0, 2 * sizeof(int), s);
-  cudaMemsetAsync(f->d_cell_count, 0, sizeof(int) * f->ncell_total, s);
+  const bool skin = f->skin > 0;
+  // without a skin the drift bins every step; with one it writes the slot caches (unless SHAKE
+  // moves the atoms afterwards) and k_bin bins on rebuild steps only
+  if (!skin) cudaMemsetAsync(f->d_cell_count, 0, sizeof(int) * f->ncell_total, s);
   // with a skin the drift kernel decides; a missing or overflowed list forces a rebuild
-  if (f->skin > 0) cudaMemsetAsync(f->d_rebuild, f->list_valid ? 0 : 1, sizeof(int), s);
+  if (skin) cudaMemsetAsync(f->d_rebuild, f->list_valid ? 0 : 1, sizeof(int), s);
+  // (the slot map exists once a cell sort has run: list_valid)
+  const bool drift_cache = skin && !shake && f->list_valid;
   // stages 1-2: kick, drift + wrap, bin (binning sees the unconstrained positions, as the
   // reference's locator.SetPosition runs before ConstraintA)
   {
@@ -1019,9 +1041,11 @@ void launch_step(rbmd_force* f, cudaStream_t s) {
     k_kick_drift<R><<<(n + 255) / 256, 256, 0, s>>>(mp, f->at.pos, f->at.vel, f->at.force, f->at.mass,
                                                     f->at.image, f->nrep > 1 ? f->d_rep_of : nullptr,
                                                     f->d_reps, f->d_lambda, f->d_xold, f->d_vold,
-                                                    f->d_cell_of, f->d_cell_count, f->d_status,
-                                                    f->skin > 0 ? f->d_xref : nullptr,
-                                                    0.25 * f->skin * f->skin, f->d_rebuild);
+                                                    skin ? nullptr : f->d_cell_of, skin ? nullptr : f->d_cell_count,
+                                                    f->d_status, skin ? f->d_xref : nullptr,
+                                                    0.25 * f->skin * f->skin, f->d_rebuild, f->d_atom_slot,
+                                                    f->at.charge,
+                                                    drift_cache ? (typename Traits<R>::V4*)f->d_pos4 : nullptr);
     f->launches++;
   }
   if (shake) {
@@ -1039,7 +1063,7 @@ void launch_step(rbmd_force* f, cudaStream_t s) {
     f->launches++;
   }
   // stage 3: force (cell sort of the pre-constraint binning, then list and forces)
-  launch_force_tail<R>(f, s, false);
+  launch_force_tail<R>(f, s, skin, skin && !drift_cache);
   f->list_valid = true;
   // stage 3: kick (+ RATTLE), temperature, thermostat
   PhaseScope ps_int(f, kPhInt, s);
@@ -1160,7 +1184,8 @@ rbmd_status parse_config(rbmd_force* f, const char* text) {
     if (at && at->kind == Value::Bool) f->autotune = at->b;
     const int tl = (int)num(root, "tuning.list_block", 0.0), tn = (int)num(root, "tuning.force_block", 0.0);
     auto ok = [](int t) { return t == 64 || t == 128 || t == 256; };
-    if (ok(tl)) { f->tpa_list = tl; f->autotune = false; }
+    const Value* tlv = root.path("tuning.list_block");
+    if (ok(tl) || (tlv && tl == 0)) { f->tpa_list = tl; f->autotune = false; }
     if (ok(tn)) { f->tpa_near = tn; f->autotune = false; }
   }
   f->far = root.path("hyper_parameters.coulomb") != nullptr;
@@ -1192,6 +1217,8 @@ rbmd_status parse_config(rbmd_force* f, const char* text) {
   f->dt = num(root, "execution.timestep", 0.005);
   f->energy_every = (int)num(root, "outputs.thermo_out.interval", 0.0);
   {
+    const Value* kp = root.path("execution.kspace_priority");
+    if (kp && kp->kind == Value::Bool) f->kspace_priority = kp->b;
     const Value* g = root.path("execution.cuda_graph");
     if (g && g->kind == Value::Bool) f->use_graph = g->b;
   }
@@ -1329,7 +1356,9 @@ rbmd_status autotune_impl(rbmd_force* f, cudaStream_t s) {
   };
   float bl = 1e30f, bn = 1e30f;
   int tl = f->tpa_list, tn = f->tpa_near;
-  for (int t : cand) {
+  const int lcand[4] = {0, 64, 128, 256};   // 0: the staged build
+  for (int t : lcand) {
+    if (t == 0 && f->nsegs == 0) continue;
     f->tpa_list = t;
     const float ms = best_of([&] { launch_nlist<R>(f, s); });
     if (ms < bl) { bl = ms; tl = t; }
@@ -1529,6 +1558,30 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
     CK(dalloc(&f->d_erf_tab, tab.size()));
     CK(cudaMemcpy(f->d_erf_tab, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice));
   }
+  if (f->nbr_type != "RBL" && f->num_cycles == 1) {
+    // staged list build: segments of S x cells per (y, z) row, S sized so that a segment holds
+    // about 224 atoms (one 256-thread pass) and its 9 x (S + 2) staged cells fill at most 60 %
+    // of the shared buffer on average
+    f->stage_cap = f->fp64 ? 2048 : 4096;
+    std::vector<ListSeg> sg;
+    for (int r = 0; r < nrep; ++r) {
+      const RepDev& rp = f->reps_h[r];
+      const double apc = std::max(1e-3, (double)(f->rep_off[r + 1] - f->rep_off[r]) / (double)rp.ncell);
+      int S = (int)std::floor(224.0 / apc);
+      S = std::min(S, (int)std::floor(0.6 * f->stage_cap / (9.0 * apc)) - 2);
+      S = std::max(1, std::min(std::min(S, kSegMaxCells), rp.dims[0]));
+      for (int z = 0; z < rp.dims[2]; ++z)
+        for (int y = 0; y < rp.dims[1]; ++y)
+          for (int x0 = 0; x0 < rp.dims[0]; x0 += S)
+            sg.push_back(ListSeg{r, y, z, x0, std::min(x0 + S, rp.dims[0]), 0, 0, 0});
+    }
+    f->nsegs = (int)sg.size();
+    CK(dalloc(&f->d_segs, sg.size()));
+    CK(cudaMemcpy(f->d_segs, sg.data(), sizeof(ListSeg) * sg.size(), cudaMemcpyHostToDevice));
+    const int bytes = f->stage_cap * (f->fp64 ? (int)sizeof(double4) : (int)sizeof(float4));
+    CK(cudaFuncSetAttribute(f->fp64 ? (const void*)k_nlist_staged<double> : (const void*)k_nlist_staged<float>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  }
   CK(dalloc(&f->d_maxcount, 2));
   CK(dalloc(&f->d_nbuilds, 1));
   CK(cudaMemset(f->d_nbuilds, 0, sizeof(unsigned long long)));
@@ -1545,7 +1598,13 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
   CK(dalloc(&f->d_esum, 32));
   CK(cudaMallocHost(&f->h_status, sizeof(uint32_t)));
   CK(cudaMallocHost(&f->h_maxcount, 2 * sizeof(int)));
-  CK(cudaStreamCreateWithFlags(&f->side, cudaStreamNonBlocking));
+  {
+    // the k-space chain is short next to the near pass it overlaps: at the highest priority its
+    // blocks take SMs as soon as near-pass blocks retire, so the join rarely waits
+    int lo_prio = 0, hi_prio = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio));
+    CK(cudaStreamCreateWithPriority(&f->side, cudaStreamNonBlocking, f->kspace_priority ? hi_prio : lo_prio));
+  }
   CK(cudaEventCreateWithFlags(&f->ev_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&f->ev_join, cudaEventDisableTiming));
   // host-side range checks: every device index derived from these arrays stays in bounds

@@ -11,7 +11,7 @@ Bars (written into each assertion):
 import numpy as np
 import pytest
 
-from copy_gpu_b200 import systems
+from copy_gpu_b200 import Box, systems
 from tests.helpers import jitter, make_ff, pair_sets_equal, rel_err, to_dev
 
 pytestmark = pytest.mark.gpu
@@ -23,13 +23,14 @@ def _posr(pos, prec):
     return pos.astype(np.float32) if prec == "fp32" else pos.astype(np.float64)
 
 
-@pytest.mark.parametrize("prec,block", [("fp32", 128), ("fp64", 128), ("fp32", 64), ("fp32", 256)])
+@pytest.mark.parametrize("prec,block", [("fp32", 128), ("fp64", 128), ("fp32", 64), ("fp32", 256), ("fp32", 0),
+                                        ("fp64", 0)])
 def test_lj_pairs_and_force(cuda, oracle_lib, prec, block):
     import torch
     s = systems.lj_fcc(ncell=8, seed=2)
     s["pos"] = jitter(s["pos"], s["lo"], s["hi"], 0.08, seed=5)
     cfg = systems.lj_config(cutoff=2.5, precision=prec)
-    cfg["tuning"] = {"list_block": block, "force_block": block}
+    cfg["tuning"] = {"list_block": block, "force_block": block or 128}
     dev = to_dev(s, cuda)
     ff = make_ff(cfg, s, dev)
     ff.Execute()
@@ -150,7 +151,7 @@ def test_autotune_keeps_parity(cuda, oracle_lib):
     ff = make_ff(cfg, s, dev)
     ff.set_ksamples(m)
     tl, tn = ff.autotune()
-    assert tl in (64, 128, 256) and tn in (64, 128, 256)
+    assert tl in (0, 64, 128, 256) and tn in (64, 128, 256)
     torch.cuda.synchronize()
     pr = _posr(s["pos"], "fp32")
     nl = oracle_lib.neighbors(pr, s["lo"], s["hi"], 2.5, "fp32")
@@ -196,3 +197,31 @@ def test_atoms_outside_box(cuda, oracle_lib):
     c, ids = ff.neighbors(512)
     nl = oracle_lib.neighbors(_posr(pos, "fp32"), s["lo"], s["hi"], 2.5, "fp32")
     assert pair_sets_equal(c, ids, nl[0], nl[1]) == -1
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_staged_list_identical(cuda, prec):
+    """The shared-memory staged list build and the per-atom build give the same list entry for
+    entry (same order, same image codes), hence bit-identical forces, through several steps of
+    Verlet-skin reuse and rebuilds on an electrolyte and on uneven batched replicas."""
+    import torch
+    s = systems.electrolyte(20000, seed=14)
+    r = systems.replicas(n_rep=5, nmin=500, nmax=3000, seed=9)
+    for sysd, boxes, offs in ((s, None, None),
+                              (r, [Box(tuple(r["lo"][k]), tuple(r["hi"][k])) for k in range(5)], r["offsets"])):
+        out = []
+        for block in (0, 128):
+            cfg = systems.electrolyte_config(P=32, precision=prec, seed=5, ensemble="NVE")
+            cfg["hyper_parameters"]["neighbor"]["skin"] = 0.3
+            cfg["tuning"] = {"list_block": block, "force_block": 128}
+            dev = to_dev(sysd, cuda)
+            ff = make_ff(cfg, sysd, dev, boxes=boxes, offsets=offs)
+            ff.Execute()
+            ff.step(40)
+            torch.cuda.synchronize()
+            assert ff.status() == 0
+            c, ids = ff.neighbors(256)
+            out.append((c, ids, dev["force"].cpu().numpy(), ff.list_builds()))
+        assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+        assert np.array_equal(out[0][2], out[1][2])
+        assert out[0][3] == out[1][3] and out[0][3] >= 2
