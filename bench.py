@@ -58,6 +58,10 @@ def parse():
                     "instead of replaying the captured step graph")
     ap.add_argument("--noise-steps", type=int, default=16,
                     help="k-sets per proposal for the force-RMSE measurement")
+    ap.add_argument("--workload", default="electrolyte",
+                    choices=["electrolyte", "lj", "water", "eam", "batched"],
+                    help="electrolyte: the headline metric (default); the others time the remaining "
+                         "configurations (plain MD steps, atom-steps/s) beside the CPU oracle")
     ap.add_argument("--skin", type=float, default=0.3,
                     help="Verlet skin; the list is rebuilt when an atom moved more than skin/2 "
                          "(forces are those of a per-step rebuild); 0 rebuilds every step")
@@ -124,8 +128,9 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
 
 
-# Algorithmic bytes / sincos per unit of each phase (derivation in DESIGN.md).  "units" is the
-# number of atoms (or charged atoms) one launch processes.
+# Algorithmic bytes / sincos per unit of each phase: the bytes a launch must move per unit it
+# processes (each listed in the entry below).  "units" is the number of atoms (or charged atoms)
+# one launch processes.
 def algorithmic(n, nq, n_nbr_mean, P):
     return {
         # list build: own pos4 (16 B) + cell ranges (8 B) + list entries written (4 B each) + count
@@ -143,7 +148,7 @@ def algorithmic(n, nq, n_nbr_mean, P):
 
 
 # Per-atom DRAM traffic of the near-force pass measured by ncu on the 200,000-atom case
-# (69.4 MB per launch, profiles/k_near_force_traffic_electrolyte_200k.md); the full-size launch
+# (dram__bytes_read.sum + dram__bytes_write.sum = 69.4 MB per launch); the full-size launch
 # has the same per-atom traffic (same density and neighbour count).
 NEAR_TRAFFIC_BYTES_PER_ATOM = 69.4e6 / 200_000
 
@@ -307,7 +312,7 @@ def roofline(run, n, nq, P, steps, dev):
     if dom == "force":
         roof["traffic"] = NEAR_TRAFFIC_BYTES_PER_ATOM * n
         roof["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the 200,000-atom "
-                                  "launch scaled by atoms (profiles/k_near_force_traffic_electrolyte_200k.md)")
+                                  "launch (summary committed under profiles/) scaled by atoms")
     return roof, rl, mufu_peak
 
 
@@ -504,8 +509,140 @@ def run_reference(args):
     }
 
 
+# ---- the other configurations: plain MD steps, GPU vs the CPU oracle -------------------------
+def config_system(name, tmpdir):
+    """(system, config, boxes, offsets, description) of a secondary configuration."""
+    from copy_gpu_b200 import Box, systems
+    if name == "lj":
+        s = systems.lj_fcc(ncell=10, seed=1)
+        cfg = systems.lj_config(cutoff=2.5, skin=0.3, precision="fp64", ensemble="NVE")
+        cfg["hyper_parameters"]["neighbor"]["skin"] = 0.3
+        return s, cfg, None, None, "LJ FCC 4000 atoms, rho 0.8442, T 0.72, rc 2.5 + skin 0.3, FP64, NVE"
+    if name == "water":
+        s = systems.water(n_mol=10000, seed=9)
+        cfg = systems.water_config(P=200, precision="fp32")
+        return s, cfg, None, None, ("SPC/E water 10000 molecules (30000 atoms), rc 10 A, RBE P=200, alpha 0.09, "
+                                    "SHAKE, REAL units, FP32 forces")
+    if name == "eam":
+        pot = systems.write_johnson_funcfl(os.path.join(tmpdir, "johnson.eam"))
+        s = systems.eam_fcc(ncell=40, seed=13)
+        cfg = systems.eam_config(pot, precision="fp32")
+        cfg["hyper_parameters"]["neighbor"]["skin"] = 0.3
+        return s, cfg, None, None, ("Johnson EAM Cu FCC 256000 atoms (5000-point funcfl), rc 5.0 A + skin 0.3, "
+                                    "300 K displacements, FP32, NVE")
+    r = systems.replicas(n_rep=512, seed=11)
+    cfg = systems.electrolyte_config(P=100, precision="fp32", ensemble="NVE")
+    cfg["hyper_parameters"]["neighbor"]["skin"] = 0.3
+    boxes = [Box(tuple(r["lo"][k]), tuple(r["hi"][k])) for k in range(512)]
+    return r, cfg, boxes, r["offsets"], (f"512 electrolyte replicas of 500-8000 atoms ({int(r['offsets'][-1])} atoms), "
+                                         "RBE P=100 each, rc 2.5 + skin 0.3, FP32, one step for all replicas")
+
+
+def cpu_config_eval(name, s, cfg, offsets, tmpdir):
+    """Seconds and atoms of one CPU force evaluation of the configuration (oracle restatement of
+    the reference path; the batched case is sampled on its first 16 replicas)."""
+    import oracle
+    hp = cfg["hyper_parameters"]
+    rc = hp["neighbor"]["cut_off"]
+    prec = cfg.get("precision", "fp32")
+    if name == "batched":
+        total, atoms = 0.0, 0
+        for k in range(16):
+            a, b = int(offsets[k]), int(offsets[k + 1])
+            sub = {key: s[key][a:b] for key in ("pos", "charge", "type")}
+            sub.update(lo=s["lo"][k], hi=s["hi"][k], eps=s["eps"], sigma=s["sigma"])
+            sec, n = cpu_config_eval("electrolyte_sub", sub, cfg, None, tmpdir)
+            total += sec
+            atoms += n
+        return total, atoms
+    pos = s["pos"].astype(np.float32 if prec == "fp32" else np.float64)
+    L = s["hi"] - s["lo"]
+    t0 = time.perf_counter()
+    nl = oracle.neighbors(pos, s["lo"], s["hi"], rc, prec)
+    if name == "eam":
+        oracle.eam_force(hp["force_field"]["potential_file"], pos, s["lo"], s["hi"], rc, nl, prec=prec)
+        return time.perf_counter() - t0, len(pos)
+    coul = "coulomb" in hp and name != "lj"
+    alpha = hp["coulomb"]["alpha"] if coul else 0.0
+    oracle.near_force(pos, s["lo"], s["hi"], rc, nl, type=s["type"], mol=s.get("molecule"),
+                      charge=s["charge"] if coul else None, eps=s["eps"], sigma=s["sigma"], with_coul=coul,
+                      alpha=alpha, sum_mode=0, prec=prec)
+    if coul:
+        P = hp["coulomb"]["coulomb_sample_num"]
+        m = oracle.rbe_sample(alpha, L, 7, 0, 0, P)
+        rho = oracle.rhok(pos, s["charge"], L, m, prec=prec)
+        oracle.rbe_force(pos, s["charge"], L, alpha, 1.0, m, rho, prec=prec)
+    if "hoh" in s:
+        oracle.water_extras(s["hoh"], s["pos"], s["charge"], s["lo"], s["hi"], *s["bond"], *s["angle"])
+    return time.perf_counter() - t0, len(pos)
+
+
+def run_config(args):
+    """One of the secondary configurations: `steps` MD steps timed with CUDA events (graph replay,
+    inputs resident), the host-buffer force call end to end, and the CPU oracle single-threaded
+    and on all cores."""
+    import tempfile
+    import torch
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    with tempfile.TemporaryDirectory() as tmpdir:
+        s, cfg, boxes, offs, desc = config_system(args.workload, tmpdir)
+        from copy_gpu_b200 import Box, ForceField
+        n_all = s["pos"].shape[0]
+        t = {k: torch.tensor(s[k], device=dev, dtype=torch.float64).contiguous()
+             for k in ("pos", "vel", "mass", "charge")}
+        t["type"] = torch.tensor(s["type"], device=dev, dtype=torch.int32)
+        t["force"] = torch.zeros((n_all, 3), device=dev, dtype=torch.float64)
+        t["image"] = torch.zeros((n_all, 3), device=dev, dtype=torch.int32)
+        if s.get("molecule") is not None:
+            t["molecule"] = torch.tensor(s["molecule"], device=dev, dtype=torch.int32)
+        ff = ForceField(cfg, boxes or Box(tuple(s["lo"]), tuple(s["hi"])))
+        ff.set_pair_coeffs(s["eps"], s["sigma"])
+        if "hoh" in s:
+            ff.set_water(s["hoh"], s["bond"][0], s["bond"][1], s["angle"][0], s["angle"][1])
+        ff.Init(t["pos"], t["force"], vel=t["vel"], mass=t["mass"], charge=t["charge"], type=t["type"],
+                molecule=t.get("molecule"), image=t["image"], replica_offsets=offs)
+        run = timed_run(ff, t, dev, args.steps, args.warmup, 1, None, args.e2e_steps)
+        n = ff.n
+        value = n * args.steps / (run["ms"] / 1e3)
+        line = {
+            "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": run["ms"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if cfg.get("precision") == "fp64" else "f32",
+            "data": "synthetic",
+            "config": {"workload": desc, "atoms": n, "list_builds_per_step": run["builds"] / args.steps,
+                       "threads_per_block": {"list": run["blocks"][0], "force": run["blocks"][1]},
+                       "step_launch": "cuda graph replay (one launch per step)"},
+            "e2e": {"value": n / (run["e2e_ms"] / 1e3), "unit": "atom-steps/s", "h2d_bytes_per_step": 24 * n,
+                    "d2h_bytes_per_step": 24 * n,
+                    "what": "rbmd_force_compute_host: pinned host positions in, forces out, one force evaluation"},
+            "phase_ms_per_step": {k: v[0] / args.steps for k, v in run["phases"].items() if v[1]},
+            "status_flags": run["flags"], "clocks": run["clk"], "mean_neighbors": run["n_nbr"],
+        }
+        del ff
+        torch.cuda.synchronize(dev)
+        if not args.no_cpu:
+            import oracle
+            oracle.build()
+            cores = os.cpu_count() or 1
+            res = {}
+            for th in (1, cores):
+                oracle.set_threads(th)
+                sec, atoms = cpu_config_eval(args.workload, s, cfg, offs, tmpdir)
+                res[th] = atoms / sec
+            line["cpu_baseline"] = {"value": res[cores], "unit": "atom-steps/s", "cores": cores, "kind": "port",
+                                    "single_thread": res[1],
+                                    "sample": "one force evaluation (list + pair terms (+ RBE, water extras)) "
+                                              "of the same system by the FP32/FP64 oracle restatement"
+                                              + (", first 16 replicas" if args.workload == "batched" else "")}
+    return line
+
+
 def main():
     args = parse()
+    if args.impl != "reference" and args.workload != "electrolyte":
+        print(json.dumps(run_config(args)), flush=True)
+        return
     out = run_reference(args) if args.impl == "reference" else run_ours(args)
     if out is not None:
         print(json.dumps(out), flush=True)
