@@ -521,8 +521,9 @@ def config_system(name, tmpdir):
     if name == "water":
         s = systems.water(n_mol=10000, seed=9)
         cfg = systems.water_config(P=200, precision="fp32")
-        return s, cfg, None, None, ("SPC/E water 10000 molecules (30000 atoms), rc 10 A, RBE P=200, alpha 0.09, "
-                                    "SHAKE, REAL units, FP32 forces")
+        cfg["hyper_parameters"]["neighbor"]["skin"] = 1.0
+        return s, cfg, None, None, ("SPC/E water 10000 molecules (30000 atoms), rc 10 A + skin 1.0, RBE P=200, "
+                                    "alpha 0.09, SHAKE, REAL units, FP32 forces")
     if name == "eam":
         pot = systems.write_johnson_funcfl(os.path.join(tmpdir, "johnson.eam"))
         s = systems.eam_fcc(ncell=40, seed=13)

@@ -357,6 +357,76 @@ __global__ void __launch_bounds__(256) k_nlist(
   nlist_finish(i, idx, cap, count, max_count, status);
 }
 
+// Warp-per-atom list build for systems with few atoms and many candidates per atom (long
+// cutoffs): the 32 lanes test consecutive candidates of a cell range together and a ballot
+// compacts the accepted ones in candidate order, so the list equals k_nlist's entry for entry.
+template <class R>
+__global__ void __launch_bounds__(256) k_nlist_warp(
+    int n, const typename Traits<R>::V4* __restrict__ pos4, const int* __restrict__ cell_start,
+    const RepDev* __restrict__ reps, const int* __restrict__ rep_of_slot, R rc, int cap, int stride,
+    int* __restrict__ nbr, int* __restrict__ count, int* __restrict__ max_count, uint32_t* status,
+    const int* __restrict__ rebuild, unsigned long long* __restrict__ nbuilds) {
+  using V4 = typename Traits<R>::V4;
+  if (rebuild && !*rebuild) return;
+  const int lane = threadIdx.x & 31;
+  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (i == 0 && lane == 0 && nbuilds) atomicAdd(nbuilds, 1ull);
+  if (i >= n) return;
+  const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
+  const V4 pi = pos4[i];
+  const R pix[3] = {pi.x, pi.y, pi.z};
+  int ci[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    ci[d] = (int)div_rn(sub_rn(pix[d], Traits<R>::lo(rp, d)), Traits<R>::dx(rp, d));
+  const R cut2 = mul_rn(rc, rc);
+  const int dx0 = rp.dims[0], dx1 = rp.dims[1], dx2 = rp.dims[2];
+  const bool x_contig = ci[0] - 1 >= 0 && ci[0] + 1 < dx0;
+  const unsigned below = (1u << lane) - 1u;
+  int idx = 0;
+  auto scan = [&](int s0, int s1, R o0, R o1, R o2, int code) {
+    for (int base = s0; base < s1; base += 32) {
+      const int sj = base + lane;
+      bool ok = false;
+      if (sj < s1) {
+        const V4 pj = pos4[sj];
+        const R r0 = sub_rn(sub_rn(pj.x, o0), pix[0]);
+        const R r1 = sub_rn(sub_rn(pj.y, o1), pix[1]);
+        const R r2 = sub_rn(sub_rn(pj.z, o2), pix[2]);
+        const R d2 = add_rn(add_rn(mul_rn(r0, r0), mul_rn(r1, r1)), mul_rn(r2, r2));
+        ok = gt_small(sub_rn(cut2, d2)) && gt_small(d2);
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, ok);
+      if (ok) {
+        const int at = idx + __popc(m & below);
+        if (at < cap) nbr[(size_t)at * stride + i] = (sj << kShiftBits) | code;
+      }
+      idx += __popc(m);
+    }
+  };
+  for (int b = -1; b <= 1; ++b)
+    for (int c = -1; c <= 1; ++c) {
+      const int nby = ci[1] + b, nbz = ci[2] + c;
+      const int wy = ((nby % dx1) + dx1) % dx1, wz = ((nbz % dx2) + dx2) % dx2;
+      const int dy = wy - nby, dz = wz - nbz;
+      const R o1 = mul_rn(Traits<R>::dx(rp, 1), (R)dy), o2 = mul_rn(Traits<R>::dx(rp, 2), (R)dz);
+      const int code_yz = ((dy > 0 ? 1 : (dy < 0 ? 2 : 0)) << 2) | ((dz > 0 ? 1 : (dz < 0 ? 2 : 0)) << 4);
+      const int row = rp.cell_base + wy * dx0 + wz * dx0 * dx1;
+      if (x_contig) {
+        scan(cell_start[row + ci[0] - 1], cell_start[row + ci[0] + 2], (R)0, o1, o2, code_yz);
+      } else {
+        for (int a = -1; a <= 1; ++a) {
+          const int nbx = ci[0] + a;
+          const int wx = ((nbx % dx0) + dx0) % dx0;
+          const int ddx = wx - nbx;
+          scan(cell_start[row + wx], cell_start[row + wx + 1], mul_rn(Traits<R>::dx(rp, 0), (R)ddx), o1, o2,
+               code_yz | (ddx > 0 ? 1 : (ddx < 0 ? 2 : 0)));
+        }
+      }
+    }
+  if (lane == 0) nlist_finish(i, idx, cap, count, max_count, status);
+}
+
 // ---- staged list build ------------------------------------------------------------------
 // One block per segment of kSeg consecutive x cells of one (y, z) cell row.  The block copies
 // the positions of its 9 neighbour rows x (segment + 1 cell each side) into shared memory once,

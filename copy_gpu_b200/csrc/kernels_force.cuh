@@ -260,6 +260,134 @@ __global__ void __launch_bounds__(256) k_near_force(
   }
 }
 
+// Near force with G lanes per atom (G = 4 .. 32) for systems with few atoms and long lists
+// (water at 10 A: ~550 neighbours, 30,000 atoms), where one thread per atom leaves most of the
+// GPU idle.  Lane s of an atom's group takes list entries s, s + G, ...; the pair terms are
+// those of k_near_force (same predicates and arithmetic); each lane accumulates in a two-float
+// accumulator and the group combines its G partial sums in FP64 with a fixed butterfly, so the
+// result does not depend on scheduling.
+template <class R, bool COUL, int MI, int G>
+__global__ void __launch_bounds__(256) k_near_force_group(
+    NearParams prm, const LJTable* __restrict__ ljt, const typename Traits<R>::V4* __restrict__ pos4,
+    const int2* __restrict__ meta, const int* __restrict__ nbr, const int* __restrict__ count,
+    const RepDev* __restrict__ reps, const int* __restrict__ rep_of_slot,
+    const int* __restrict__ slot_atom, double* __restrict__ force,
+    double* __restrict__ energy_slot, uint32_t* status) {
+  using V4 = typename Traits<R>::V4;
+  __shared__ R lj_a[kMaxReplicaTypes * kMaxReplicaTypes], lj_s6[kMaxReplicaTypes * kMaxReplicaTypes];
+  const int nt2 = prm.ntypes * prm.ntypes;
+  for (int t = threadIdx.x; t < nt2; t += blockDim.x) {
+    lj_a[t] = lj24<R>(*ljt, t);
+    lj_s6[t] = sig6<R>(*ljt, t);
+  }
+  __syncthreads();
+  const bool MOLEC = prm.molecular != 0;
+  const bool ENERGY = energy_slot != nullptr;
+  const int gid = (int)((blockIdx.x * blockDim.x + threadIdx.x) / G);
+  const int sub = threadIdx.x % G;
+  const bool active = gid < prm.n;   // inactive groups still join the shuffles below
+  const int i = active ? gid : prm.n - 1;
+  const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
+  const V4 pi = pos4[i];
+  const bool typed = MOLEC || prm.ntypes > 1;
+  const int2 mi = typed ? meta[i] : make_int2(0, 0);
+  const R rc = (R)prm.rc;
+  const R cut2 = rc * rc;
+  const R box[3] = {Traits<R>::box(rp, 0), Traits<R>::box(rp, 1), Traits<R>::box(rp, 2)};
+  const R wrap[3] = {Traits<R>::wrap(rp, 0), Traits<R>::wrap(rp, 1), Traits<R>::wrap(rp, 2)};
+  const R sa = (R)prm.sqrt_alpha, aa = (R)prm.alpha, c2 = (R)prm.two_sqrt_alpha_over_sqrt_pi;
+  const R cs = (R)prm.coul_scale;
+  const R qi = pi.w;
+  const int trow = prm.ntypes > 1 ? mi.x * prm.ntypes : 0;
+  const size_t st = (size_t)prm.stride;
+  Acc<R> fx, fy, fz;
+  R gx = 0, gy = 0, gz = 0;
+  R e_lj = 0, e_coul = 0;
+  const int cnt = active ? min(count[i], prm.cap) : 0;
+  int k = 0;
+  for (int p = sub; p < cnt; p += G, ++k) {
+    const int e = __ldg(nbr + (size_t)p * st + i);
+    const V4 pj = pos4[e >> kShiftBits];
+    R px = pj.x, py = pj.y, pz = pj.z;
+    if (e & 63) {
+      const int c0 = e & 3, c1 = (e >> 2) & 3, c2b = (e >> 4) & 3;
+      px = px - (c0 == 1 ? wrap[0] : (c0 == 2 ? -wrap[0] : (R)0));
+      py = py - (c1 == 1 ? wrap[1] : (c1 == 2 ? -wrap[1] : (R)0));
+      pz = pz - (c2b == 1 ? wrap[2] : (c2b == 2 ? -wrap[2] : (R)0));
+    }
+    const R r0 = px - pi.x, r1 = py - pi.y, r2 = pz - pi.z;
+    const R d2 = r0 * r0 + r1 * r1 + r2 * r2;
+    if (MI == kMiAll && !(cut2 - d2 > (R)1.0e-4 && d2 > (R)1.0e-4)) continue;
+    R f = 0;
+    if (COUL) {
+      const R qq = qi * pj.w;
+      if (qq != (R)0) {
+        const R inv = rsqrt_r(d2);
+        const R dis = d2 * inv;
+        if (dis < rc && dis > (R)0.01) {
+          const R ex = exp_r(-aa * d2);
+          const R erfcv = erfc_shared(sa * dis, ex);
+          const R g = (erfcv * inv + c2 * ex) * inv;
+          f = -qq * g * inv * cs;
+          if (ENERGY) e_coul += qq * erfcv * inv * cs;
+        }
+      }
+    }
+    R fl0 = 0, fl1 = 0, fl2 = 0;
+    bool same = false;
+    int tj = 0;
+    if (typed) {
+      const int2 mj = meta[e >> kShiftBits];
+      same = MOLEC && (mj.y == mi.y);
+      tj = prm.ntypes > 1 ? mj.x : 0;
+    }
+    if (!same) {
+      R q0 = r0, q1 = r1, q2 = r2;
+      R dl2 = d2;
+      if (MI == kMiLJ) {
+        min_image(q0, q1, q2, box);
+        dl2 = q0 * q0 + q1 * q1 + q2 * q2;
+      }
+      if (dl2 < cut2 && dl2 > (R)0.0001) {
+        const R inv2 = rcp_r(dl2);
+        const R sd6 = lj_s6[trow + tj] * inv2 * inv2 * inv2;
+        const R a24 = lj_a[trow + tj];
+        const R scal = a24 * (((R)2 * sd6 - (R)1) * sd6) * inv2;
+        fl0 = scal * q0; fl1 = scal * q1; fl2 = scal * q2;
+        if (ENERGY) e_lj += -a24 / (R)6 * (sd6 - (R)1) * sd6;
+      }
+    }
+    gx += f * r0 + fl0;
+    gy += f * r1 + fl1;
+    gz += f * r2 + fl2;
+    if ((k & 3) == 3) {
+      fx.add(gx); fy.add(gy); fz.add(gz);
+      gx = gy = gz = 0;
+    }
+  }
+  fx.add(gx); fy.add(gy); fz.add(gz);
+  double F[3] = {fx.value(), fy.value(), fz.value()};
+  double el = (double)e_lj, ec = (double)e_coul;
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) {
+    F[0] += __shfl_xor_sync(0xffffffffu, F[0], o);
+    F[1] += __shfl_xor_sync(0xffffffffu, F[1], o);
+    F[2] += __shfl_xor_sync(0xffffffffu, F[2], o);
+    el += __shfl_xor_sync(0xffffffffu, el, o);
+    ec += __shfl_xor_sync(0xffffffffu, ec, o);
+  }
+  if (!active || sub != 0) return;
+  if (!isfinite(F[0]) || !isfinite(F[1]) || !isfinite(F[2])) set_flag(status, kFlagNonFinite);
+  const int id = slot_atom[i];
+  force[3 * id] = F[0];
+  force[3 * id + 1] = F[1];
+  force[3 * id + 2] = F[2];
+  if (ENERGY) {
+    energy_slot[2 * i] = 0.5 * el;
+    energy_slot[2 * i + 1] = 0.5 * ec;
+  }
+}
+
 // RBE k-space force, one thread per charged atom (compact index c, caller id qidx[c]):
 // F_i = q_i sum_l w_l k_l (cos(k_l.r_i) Im rho_l - sin(k_l.r_i) Re rho_l)
 // (ComputeNewRBEForceWorklet, RunWorklet.cpp:1508-1548; S/P and qqr2e are folded into the

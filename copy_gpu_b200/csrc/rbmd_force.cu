@@ -115,7 +115,8 @@ struct rbmd_force {
   double shake_tol = 1e-5;
   int energy_every = 0;   // energies inside step(): every outputs.thermo_out.interval steps
   int cap_override = 0;   // neighbor.capacity: initial list capacity (grown on overflow)
-  int tpa_list = 0, tpa_near = 128;     // list build: 0 = staged kernel, else threads per block of
+  int tpa_list = 0, tpa_near = 128;
+  int near_lanes = 1;                   // near pass lanes per atom: 1, or 4 / 8 / 16 / 32     // list build: 0 = staged kernel, else threads per block of
                                         // k_nlist; threads per block of the force pass
   bool autotune = false;                // "autotune": true tunes them at the first compute
   bool tuned = false;
@@ -647,7 +648,15 @@ void launch_nlist(rbmd_force* f, cudaStream_t s) {
     f->launches++;
     return;
   }
-  const int bs = f->tpa_list > 0 ? f->tpa_list : 128;
+  if (f->tpa_list == 1 && f->num_cycles == 1) {   // warp per atom
+    k_nlist_warp<R><<<(f->n + 7) / 8, 256, 0, s>>>(
+        f->n, (const typename Traits<R>::V4*)f->d_pos4, f->d_cell_start, f->d_reps,
+        f->nrep > 1 ? f->d_rep_of : nullptr, (R)f->list_cut(), f->cap, f->stride, f->d_nbr, f->d_count,
+        f->d_maxcount, f->d_status, f->skin > 0 ? f->d_rebuild : nullptr, f->d_nbuilds);
+    f->launches++;
+    return;
+  }
+  const int bs = f->tpa_list > 1 ? f->tpa_list : 128;
   k_nlist<R><<<(f->n + bs - 1) / bs, bs, 0, s>>>(
       f->n, (const typename Traits<R>::V4*)f->d_pos4, f->d_cell_start, f->d_reps,
       f->nrep > 1 ? f->d_rep_of : nullptr, f->num_cycles, (R)f->list_cut(), f->cap, f->stride, f->d_nbr,
@@ -797,6 +806,19 @@ void launch_near_t(rbmd_force* f, cudaStream_t s) {
   p.sqrt_alpha = std::sqrt(f->alpha);
   p.two_sqrt_alpha_over_sqrt_pi = 2.0 * std::sqrt(f->alpha) / std::sqrt(M_PI);
   p.kstage = 0;
+  if (f->near_lanes > 1) {
+    const long long threads = (long long)f->n * f->near_lanes;
+    const int grid = (int)((threads + 255) / 256);
+    auto kern = f->near_lanes == 4    ? k_near_force_group<R, COUL, MI, 4>
+                : f->near_lanes == 8  ? k_near_force_group<R, COUL, MI, 8>
+                : f->near_lanes == 16 ? k_near_force_group<R, COUL, MI, 16>
+                                      : k_near_force_group<R, COUL, MI, 32>;
+    kern<<<grid, 256, 0, s>>>(p, f->d_ljt, (const typename Traits<R>::V4*)f->d_pos4, f->d_meta, f->d_nbr,
+                              f->d_count, f->d_reps, f->nrep > 1 ? f->d_rep_of : nullptr, f->d_slot_atom,
+                              f->at.force, f->want_energy ? f->d_eslot : nullptr, f->d_status);
+    f->launches++;
+    return;
+  }
   const int bs = f->tpa_near;
   k_near_force<R, COUL, MI><<<(f->n + bs - 1) / bs, bs, 0, s>>>(
       p, f->d_ljt, (const typename Traits<R>::V4*)f->d_pos4, f->d_meta, f->d_nbr, f->d_count,
@@ -1185,8 +1207,10 @@ rbmd_status parse_config(rbmd_force* f, const char* text) {
     const int tl = (int)num(root, "tuning.list_block", 0.0), tn = (int)num(root, "tuning.force_block", 0.0);
     auto ok = [](int t) { return t == 64 || t == 128 || t == 256; };
     const Value* tlv = root.path("tuning.list_block");
-    if (ok(tl) || (tlv && tl == 0)) { f->tpa_list = tl; f->autotune = false; }
+    if (ok(tl) || (tlv && (tl == 0 || tl == 1))) { f->tpa_list = tl; f->autotune = false; }
     if (ok(tn)) { f->tpa_near = tn; f->autotune = false; }
+    const int ln = (int)num(root, "tuning.force_lanes", 0.0);
+    if (ln == 1 || ln == 4 || ln == 8 || ln == 16 || ln == 32) { f->near_lanes = ln; f->autotune = false; }
   }
   f->far = root.path("hyper_parameters.coulomb") != nullptr;
   if (f->far) {
@@ -1356,22 +1380,31 @@ rbmd_status autotune_impl(rbmd_force* f, cudaStream_t s) {
   };
   float bl = 1e30f, bn = 1e30f;
   int tl = f->tpa_list, tn = f->tpa_near;
-  const int lcand[4] = {0, 64, 128, 256};   // 0: the staged build
+  const int lcand[5] = {0, 1, 64, 128, 256};   // 0: the staged build, 1: warp per atom
   for (int t : lcand) {
     if (t == 0 && f->nsegs == 0) continue;
+    if (t == 1 && f->num_cycles != 1) continue;
     f->tpa_list = t;
     const float ms = best_of([&] { launch_nlist<R>(f, s); });
     if (ms < bl) { bl = ms; tl = t; }
   }
   f->tpa_list = tl;
-  for (int t : cand) {
-    f->tpa_near = t;
-    const float ms = best_of([&] {
-      if (f->is_eam()) launch_eam<R>(f, s);
-      else launch_near<R>(f, s);
-    });
-    if (ms < bn) { bn = ms; tn = t; }
+  int tg = f->near_lanes;
+  const int gcand[5] = {1, 4, 8, 16, 32};
+  for (int g : gcand) {
+    if (g > 1 && f->is_eam()) continue;
+    for (int t : cand) {
+      if (g > 1 && t != 256) continue;   // grouped variants run 256-thread blocks
+      f->tpa_near = t;
+      f->near_lanes = g;
+      const float ms = best_of([&] {
+        if (f->is_eam()) launch_eam<R>(f, s);
+        else launch_near<R>(f, s);
+      });
+      if (ms < bn) { bn = ms; tn = t; tg = g; }
+    }
   }
+  f->near_lanes = tg;
   f->tpa_near = tn;
   cudaEventDestroy(a);
   cudaEventDestroy(b);
@@ -1903,7 +1936,7 @@ rbmd_status rbmd_force_autotune(rbmd_force* f, void* stream, int32_t* list_lanes
   st = check_overflow(f, s, &redo);
   if (st) return st;
   if (list_lanes) *list_lanes = f->tpa_list;
-  if (force_lanes) *force_lanes = f->tpa_near;
+  if (force_lanes) *force_lanes = f->near_lanes > 1 ? -f->near_lanes : f->tpa_near;
   return RBMD_OK;
 }
 

@@ -145,13 +145,15 @@ RBMD_API rbmd_status rbmd_force_sample_k(rbmd_force* f, int64_t step, int32_t* m
  * (rbmd/framework/run/ExecutionNVT.cpp:179-222). */
 RBMD_API rbmd_status rbmd_force_compute(rbmd_force* f, void* stream);
 
-/* Time every choice of the neighbour-list build (0: the shared-memory staged kernel, or 64, 128,
- * 256 threads per block of the per-atom kernel) and every threads-per-block choice (64, 128,
- * 256) of the force pass on the bound system, keep the fastest, and leave the forces of that
- * choice in atoms->force.  Config "autotune": true runs it at the first compute;
- * "tuning.list_block" / "tuning.force_block" fix the choices instead (default 0 / 128).  Results
- * do not depend on the choice (identical lists entry for entry, one thread per atom in the force
- * pass, same summation order).  No reference counterpart. */
+/* Time every choice of the neighbour-list build (0: the shared-memory staged kernel, 1: one warp
+ * per atom, or 64, 128, 256 threads per block of the per-atom kernel) and of the force pass (64,
+ * 128, 256 threads per block with one thread per atom, or 4 / 8 / 16 / 32 lanes per atom) on the
+ * bound system, keep the fastest, and leave the forces of that choice in atoms->force.
+ * force_block returns the threads per block, or -G for G lanes per atom.  Config "autotune":
+ * true runs it at the first compute; "tuning.list_block" / "tuning.force_block" /
+ * "tuning.force_lanes" fix the choices instead (default 0 / 128 / 1).  Lists are identical entry
+ * for entry whatever the choice; forces agree to rounding (lanes per atom change the summation
+ * order).  No reference counterpart. */
 RBMD_API rbmd_status rbmd_force_autotune(rbmd_force* f, void* stream, int32_t* list_block,
                                          int32_t* force_block);
 

@@ -24,7 +24,7 @@ def _posr(pos, prec):
 
 
 @pytest.mark.parametrize("prec,block", [("fp32", 128), ("fp64", 128), ("fp32", 64), ("fp32", 256), ("fp32", 0),
-                                        ("fp64", 0)])
+                                        ("fp64", 0), ("fp32", 1), ("fp64", 1)])
 def test_lj_pairs_and_force(cuda, oracle_lib, prec, block):
     import torch
     s = systems.lj_fcc(ncell=8, seed=2)
@@ -151,7 +151,7 @@ def test_autotune_keeps_parity(cuda, oracle_lib):
     ff = make_ff(cfg, s, dev)
     ff.set_ksamples(m)
     tl, tn = ff.autotune()
-    assert tl in (0, 64, 128, 256) and tn in (64, 128, 256)
+    assert tl in (0, 1, 64, 128, 256) and tn in (64, 128, 256, -4, -8, -16, -32)
     torch.cuda.synchronize()
     pr = _posr(s["pos"], "fp32")
     nl = oracle_lib.neighbors(pr, s["lo"], s["hi"], 2.5, "fp32")
@@ -201,16 +201,17 @@ def test_atoms_outside_box(cuda, oracle_lib):
 
 @pytest.mark.parametrize("prec", ["fp32", "fp64"])
 def test_staged_list_identical(cuda, prec):
-    """The shared-memory staged list build and the per-atom build give the same list entry for
-    entry (same order, same image codes), hence bit-identical forces, through several steps of
-    Verlet-skin reuse and rebuilds on an electrolyte and on uneven batched replicas."""
+    """The shared-memory staged list build, the warp-per-atom build and the per-atom build give
+    the same list entry for entry (same order, same image codes), hence bit-identical forces,
+    through several steps of Verlet-skin reuse and rebuilds on an electrolyte and on uneven
+    batched replicas."""
     import torch
     s = systems.electrolyte(20000, seed=14)
     r = systems.replicas(n_rep=5, nmin=500, nmax=3000, seed=9)
     for sysd, boxes, offs in ((s, None, None),
                               (r, [Box(tuple(r["lo"][k]), tuple(r["hi"][k])) for k in range(5)], r["offsets"])):
         out = []
-        for block in (0, 128):
+        for block in (0, 1, 128):
             cfg = systems.electrolyte_config(P=32, precision=prec, seed=5, ensemble="NVE")
             cfg["hyper_parameters"]["neighbor"]["skin"] = 0.3
             cfg["tuning"] = {"list_block": block, "force_block": 128}
@@ -222,6 +223,44 @@ def test_staged_list_identical(cuda, prec):
             assert ff.status() == 0
             c, ids = ff.neighbors(256)
             out.append((c, ids, dev["force"].cpu().numpy(), ff.list_builds()))
-        assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
-        assert np.array_equal(out[0][2], out[1][2])
-        assert out[0][3] == out[1][3] and out[0][3] >= 2
+        for o in out[1:]:
+            assert np.array_equal(out[0][0], o[0]) and np.array_equal(out[0][1], o[1])
+            assert np.array_equal(out[0][2], o[2])
+            assert out[0][3] == o[3] and out[0][3] >= 2
+
+
+@pytest.mark.parametrize("lanes", [4, 8, 16, 32])
+def test_force_lanes_parity(cuda, oracle_lib, lanes):
+    """Lanes-per-atom near pass: water (molecular LJ exclusion, erfc Coulomb, FP64) equals the
+    one-thread-per-atom pass to summation-order rounding; the FP32 electrolyte matches the oracle."""
+    import torch
+    s = systems.water(n_mol=300, seed=3)
+    forces = []
+    for ln in (1, lanes):
+        cfg = systems.water_config(P=16, precision="fp64")
+        cfg["tuning"] = {"force_lanes": ln, "force_block": 128}
+        dev = to_dev(s, cuda)
+        ff = make_ff(cfg, s, dev)
+        ff.Execute()
+        torch.cuda.synchronize()
+        assert ff.status() == 0
+        forces.append(dev["force"].cpu().numpy())
+    assert rel_err(forces[1], forces[0]) < 1e-12
+    n, P = 3000, 32
+    se, cfg = _electrolyte(n, P, "fp32")
+    cfg["tuning"] = {"force_lanes": lanes, "force_block": 128}
+    alpha = cfg["hyper_parameters"]["coulomb"]["alpha"]
+    L = se["hi"] - se["lo"]
+    m = oracle_lib.rbe_sample(alpha, L, seed=5, step=0, rep=0, P=P)
+    dev = to_dev(se, cuda)
+    ff = make_ff(cfg, se, dev)
+    ff.set_ksamples(m)
+    ff.Execute()
+    torch.cuda.synchronize()
+    pr = _posr(se["pos"], "fp32")
+    nl = oracle_lib.neighbors(pr, se["lo"], se["hi"], 2.5, "fp32")
+    near = oracle_lib.near_force(pr, se["lo"], se["hi"], 2.5, nl, type=se["type"], charge=se["charge"],
+                                 eps=se["eps"], sigma=se["sigma"], with_coul=True, alpha=alpha, prec="fp32")
+    rho = oracle_lib.rhok(se["pos"], se["charge"], L, m)
+    far = oracle_lib.rbe_force(se["pos"], se["charge"], L, alpha, 1.0, m, rho)
+    assert rel_err(dev["force"].cpu().numpy(), near + far) <= TOL["fp32"]
