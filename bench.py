@@ -148,9 +148,9 @@ def algorithmic(n, nq, n_nbr_mean, P):
 
 
 # Per-atom DRAM traffic of the near-force pass measured by ncu on the 200,000-atom case
-# (dram__bytes_read.sum + dram__bytes_write.sum = 69.4 MB per launch); the full-size launch
+# (dram__bytes_read.sum + dram__bytes_write.sum = 70.19 MB per launch); the full-size launch
 # has the same per-atom traffic (same density and neighbour count).
-NEAR_TRAFFIC_BYTES_PER_ATOM = 69.4e6 / 200_000
+NEAR_TRAFFIC_BYTES_PER_ATOM = 70.19e6 / 200_000
 
 
 def max_over_ranks(value, dist, device):
