@@ -673,7 +673,10 @@ __global__ void __launch_bounds__(256) k_sample(int nrep, const SamplerRep* __re
 // ------------------------------------------------------------------------------------------
 // EAM passes (funcfl, 7-coefficient splines): pass 1 = ComputeEAMfpVerletWorklet
 // (RunWorklet.cpp:305-359) -> fp[slot]; pass 2 = ComputeEAMForceVerletWorklet (:361-417).
-// Spline rows are stored as two float4 (c0..c3, c4..c6,0).
+// Spline rows are stored as two float4 (c0..c3, c4..c6,0).  MI: MinDistanceVec on the pair
+// vector, needed only when a replica has fewer than 3 cells on an axis (otherwise the stored
+// image shift already gives the nearest image, also under list reuse: the slot cache is
+// unwrapped since the build).  FP32 uses r = rsq * rsqrt(rsq) and 1/r = rsqrt(rsq).
 // ------------------------------------------------------------------------------------------
 struct EamDev {
   const float4* frho;   // 2 float4 per row
@@ -685,7 +688,7 @@ struct EamDev {
   float rhomax;
 };
 
-template <class R>
+template <class R, bool MI>
 __global__ void __launch_bounds__(128) k_eam_fp(int n, int stride, int cap, double rc, EamDev eam,
                                                 const typename Traits<R>::V4* __restrict__ pos4,
                                                 const int* __restrict__ nbr, const int* __restrict__ count,
@@ -698,6 +701,7 @@ __global__ void __launch_bounds__(128) k_eam_fp(int n, int stride, int cap, doub
   const typename Traits<R>::V4 pi = pos4[i];
   const R wrap[3] = {Traits<R>::wrap(rp, 0), Traits<R>::wrap(rp, 1), Traits<R>::wrap(rp, 2)};
   const R box[3] = {Traits<R>::box(rp, 0), Traits<R>::box(rp, 1), Traits<R>::box(rp, 2)};
+  const R ibox[3] = {(R)1 / box[0], (R)1 / box[1], (R)1 / box[2]};
   const R cut2 = (R)rc * (R)rc;
   const R rdr = sizeof(R) == 4 ? (R)eam.rdr : (R)eam.rdr_d;
   Acc<R> rho;
@@ -713,12 +717,12 @@ __global__ void __launch_bounds__(128) k_eam_fp(int n, int stride, int cap, doub
       const int cd = (e >> (2 * d)) & 3;
       const R off = cd == 1 ? wrap[d] : (cd == 2 ? -wrap[d] : (R)0);
       R v = piv[d] - (pjv[d] - off);
-      v -= box[d] * rint(v / box[d]);   // MinDistanceVec (nearest image also under list reuse)
+      if (MI) v -= box[d] * rint(v * ibox[d]);   // MinDistanceVec
       r[d] = v;
     }
     const R rsq = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
     if (rsq < cut2 && rsq > (R)0.01) {
-      R pp = sqrt_r(rsq) * rdr + (R)1;
+      R pp = rsq * rsqrt_r(rsq) * rdr + (R)1;
       int m = (int)pp;
       m = min(m, eam.nr - 1);
       pp -= (R)m;
@@ -744,7 +748,7 @@ __global__ void __launch_bounds__(128) k_eam_fp(int n, int stride, int cap, doub
   }
 }
 
-template <class R>
+template <class R, bool MI>
 __global__ void __launch_bounds__(128) k_eam_force(int n, int stride, int cap, double rc, EamDev eam,
                                                    const typename Traits<R>::V4* __restrict__ pos4,
                                                    const int* __restrict__ nbr, const int* __restrict__ count,
@@ -759,6 +763,7 @@ __global__ void __launch_bounds__(128) k_eam_force(int n, int stride, int cap, d
   const typename Traits<R>::V4 pi = pos4[i];
   const R wrap[3] = {Traits<R>::wrap(rp, 0), Traits<R>::wrap(rp, 1), Traits<R>::wrap(rp, 2)};
   const R box[3] = {Traits<R>::box(rp, 0), Traits<R>::box(rp, 1), Traits<R>::box(rp, 2)};
+  const R ibox[3] = {(R)1 / box[0], (R)1 / box[1], (R)1 / box[2]};
   const R cut2 = (R)rc * (R)rc;
   const R rdr = sizeof(R) == 4 ? (R)eam.rdr : (R)eam.rdr_d;
   const R fpi = fp[i];
@@ -779,12 +784,13 @@ __global__ void __launch_bounds__(128) k_eam_force(int n, int stride, int cap, d
       // reference's RBL pass, RunWorklet.cpp:1180); ref_sign: the reference's Verlet pass uses
       // MinDistanceVec(p_j, p_i) (RunWorklet.cpp:402), which reverses the force
       R v = ref_sign ? (pjv[d] - off) - piv[d] : piv[d] - (pjv[d] - off);
-      v -= box[d] * rint(v / box[d]);
+      if (MI) v -= box[d] * rint(v * ibox[d]);
       r[d] = v;
     }
     const R rsq = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
     if (rsq < cut2 && rsq > (R)0.01) {
-      const R rv = sqrt_r(rsq);
+      const R recip = rsqrt_r(rsq);
+      const R rv = rsq * recip;
       R pp = rv * rdr + (R)1;
       int m = (int)pp;
       m = min(m, eam.nr - 1);
@@ -796,7 +802,6 @@ __global__ void __launch_bounds__(128) k_eam_force(int n, int stride, int cap, d
       const R rhop = ((R)ra.x * pp + (R)ra.y) * pp + (R)ra.z;
       const R z2p = ((R)za.x * pp + (R)za.y) * pp + (R)za.z;
       const R z2 = (((R)za.w * pp + (R)zb.x) * pp + (R)zb.y) * pp + (R)zb.z;
-      const R recip = (R)1 / rv;
       const R phi = z2 * recip;
       const R phip = z2p * recip - phi * recip;
       const R psip = fpi * rhop + fp[j] * rhop + phip;

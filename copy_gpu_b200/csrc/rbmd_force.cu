@@ -857,11 +857,13 @@ void launch_eam(rbmd_force* f, cudaStream_t s) {
   const int* rp = f->nrep > 1 ? f->d_rep_of : nullptr;
   const int bs = 128;
   const int nb = (f->n + bs - 1) / bs;
-  k_eam_fp<R><<<nb, bs, 0, s>>>(f->n, f->stride, f->cap, f->rc, e, (const typename Traits<R>::V4*)f->d_pos4,
-                                 f->d_nbr, f->d_count, f->d_reps, rp, (R*)f->d_fp, f->d_emb);
-  k_eam_force<R><<<nb, bs, 0, s>>>(f->n, f->stride, f->cap, f->rc, e, (const typename Traits<R>::V4*)f->d_pos4,
-                                    f->d_nbr, f->d_count, f->d_reps, rp, (const R*)f->d_fp, f->d_slot_atom,
-                                    f->at.force, f->d_epair, f->d_status, f->eam_ref_sign ? 1 : 0);
+  auto fp_kern = f->minimg ? k_eam_fp<R, true> : k_eam_fp<R, false>;
+  auto force_kern = f->minimg ? k_eam_force<R, true> : k_eam_force<R, false>;
+  fp_kern<<<nb, bs, 0, s>>>(f->n, f->stride, f->cap, f->rc, e, (const typename Traits<R>::V4*)f->d_pos4,
+                            f->d_nbr, f->d_count, f->d_reps, rp, (R*)f->d_fp, f->d_emb);
+  force_kern<<<nb, bs, 0, s>>>(f->n, f->stride, f->cap, f->rc, e, (const typename Traits<R>::V4*)f->d_pos4,
+                               f->d_nbr, f->d_count, f->d_reps, rp, (const R*)f->d_fp, f->d_slot_atom,
+                               f->at.force, f->d_epair, f->d_status, f->eam_ref_sign ? 1 : 0);
   f->launches += 2;
 }
 
