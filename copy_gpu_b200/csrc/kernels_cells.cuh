@@ -131,8 +131,22 @@ __global__ void k_scatter(int n, const int* __restrict__ cell_of, const int* __r
   tmp_slot_atom[s] = i;
 }
 
-// One warp per cell: rank the cell's atoms by caller id (ids are distinct) and gather the
-// slot-ordered caches.  Cells above kMaxCellAtoms keep the scatter order (flagged by the scan).
+// Total order of positions for the cell sort: IEEE bits mapped so that unsigned comparison
+// follows the float order (NaNs land at the ends, so a rank is always a permutation).
+__device__ __forceinline__ uint32_t ord_key(float x) {
+  const uint32_t b = __float_as_uint(x);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ unsigned long long ord_key(double x) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+  return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+
+// One warp per cell: rank the cell's atoms by caller id (ids are distinct), or with sort_x by
+// (x in the run precision, caller id), and gather the slot-ordered caches.  With sort_x every
+// row of consecutive x cells is ordered by x, which lets the list build skip the candidates
+// beyond the cutoff in x by binary search.  Cells above kMaxCellAtoms keep the scatter order
+// (flagged by the scan).
 template <class R>
 __global__ void __launch_bounds__(256) k_cell_sort_gather(
     int ncell, const int* __restrict__ start, const int* __restrict__ tmp_slot_atom,
@@ -140,7 +154,7 @@ __global__ void __launch_bounds__(256) k_cell_sort_gather(
     const int* __restrict__ type, const int* __restrict__ mol, const int* __restrict__ rep_of,
     const RepDev* __restrict__ reps, int* __restrict__ slot_atom, int* __restrict__ atom_slot,
     typename Traits<R>::V4* __restrict__ pos4, void* __restrict__ frac_out,
-    int2* __restrict__ meta, double* __restrict__ xref, const int* __restrict__ rebuild) {
+    int2* __restrict__ meta, double* __restrict__ xref, const int* __restrict__ rebuild, int sort_x) {
   if (rebuild && !*rebuild) return;
   __shared__ int ids[8][kMaxCellAtoms];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -157,7 +171,16 @@ __global__ void __launch_bounds__(256) k_cell_sort_gather(
     int rank = k;
     if (sortable) {
       rank = 0;
-      for (int m = 0; m < n; ++m) rank += ids[w][m] < id;
+      if (sort_x) {
+        const auto kk = ord_key((R)pos[3 * id]);
+        for (int m = 0; m < n; ++m) {
+          const int im = ids[w][m];
+          const auto km = ord_key((R)pos[3 * im]);
+          rank += km < kk || (km == kk && im < id);
+        }
+      } else {
+        for (int m = 0; m < n; ++m) rank += ids[w][m] < id;
+      }
     }
     const int slot = s0 + rank;
     slot_atom[slot] = id;
@@ -289,12 +312,27 @@ __device__ __forceinline__ int nlist_range(int s, const int s1, const typename T
 
 // Per-thread traversal of slot i's 27-cell stencil straight from global memory; returns the
 // number of pairs found (entries beyond cap are counted, not stored).
+// First slot s in [lo, hi) with pos4[s].x >= bound (the range is ordered by x).
+template <class R>
+__device__ __forceinline__ int lower_x(const typename Traits<R>::V4* __restrict__ pos4, int lo, int hi, R bound) {
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (pos4[mid].x < bound) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// trim_x: cells are ordered by x (k_cell_sort_gather with sort_x), so each contiguous x range
+// is cut to the candidates with |x_j' - x_i| below the cutoff plus a rounding margin before the
+// exact predicate runs; the accepted pairs and their order are unchanged.
 template <class R>
 __device__ int nlist_thread(int i, const typename Traits<R>::V4 pi, const RepDev& rp,
                             const typename Traits<R>::V4* __restrict__ pos4,
                             const int* __restrict__ cell_start, int num_cycles, R rc, int cap, int stride,
-                            int* __restrict__ nbr) {
+                            int* __restrict__ nbr, bool trim_x = false) {
   const R pix[3] = {pi.x, pi.y, pi.z};
+  const R xm = rc + (fabs(pix[0]) + (R)2 * rc) * (R)1e-5 + (R)1e-6;   // cutoff + margin in x
   int ci[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d)
@@ -316,8 +354,12 @@ __device__ int nlist_thread(int i, const typename Traits<R>::V4 pi, const RepDev
       const int row = rp.cell_base + wy * dx0 + wz * dx0 * dx1;
       if (x_contig) {
         off[0] = (R)0;
-        idx = nlist_range<R>(cell_start[row + ci[0] - nc], cell_start[row + ci[0] + nc + 1], pos4, pix,
-                             off, code_yz, cut2, idx, cap, stride, i, nbr);
+        int s0 = cell_start[row + ci[0] - nc], s1 = cell_start[row + ci[0] + nc + 1];
+        if (trim_x) {
+          s0 = lower_x<R>(pos4, s0, s1, pix[0] - xm);
+          s1 = lower_x<R>(pos4, s0, s1, pix[0] + xm);
+        }
+        idx = nlist_range<R>(s0, s1, pos4, pix, off, code_yz, cut2, idx, cap, stride, i, nbr);
       } else {
         for (int a = -nc; a <= nc; ++a) {
           const int nbx = ci[0] + a;
@@ -325,8 +367,13 @@ __device__ int nlist_thread(int i, const typename Traits<R>::V4 pi, const RepDev
           const int ddx = wx - nbx;
           off[0] = mul_rn(Traits<R>::dx(rp, 0), (R)ddx);
           const int code = code_yz | (ddx > 0 ? 1 : (ddx < 0 ? 2 : 0));
-          idx = nlist_range<R>(cell_start[row + wx], cell_start[row + wx + 1], pos4, pix, off, code, cut2,
-                               idx, cap, stride, i, nbr);
+          int s0 = cell_start[row + wx], s1 = cell_start[row + wx + 1];
+          if (trim_x) {
+            const R xw = xm + fabs(off[0]) * (R)1e-5;   // the shifted bound rounds at |x_i + offset|
+            s0 = lower_x<R>(pos4, s0, s1, pix[0] + off[0] - xw);
+            s1 = lower_x<R>(pos4, s0, s1, pix[0] + off[0] + xw);
+          }
+          idx = nlist_range<R>(s0, s1, pos4, pix, off, code, cut2, idx, cap, stride, i, nbr);
         }
       }
     }
@@ -347,13 +394,15 @@ __global__ void __launch_bounds__(256) k_nlist(
     int n, const typename Traits<R>::V4* __restrict__ pos4, const int* __restrict__ cell_start,
     const RepDev* __restrict__ reps, const int* __restrict__ rep_of_slot, int num_cycles, R rc,
     int cap, int stride, int* __restrict__ nbr, int* __restrict__ count, int* __restrict__ max_count,
-    uint32_t* status, const int* __restrict__ rebuild, unsigned long long* __restrict__ nbuilds) {
+    uint32_t* status, const int* __restrict__ rebuild, unsigned long long* __restrict__ nbuilds,
+    int trim_x) {
   if (rebuild && !*rebuild) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0 && nbuilds) atomicAdd(nbuilds, 1ull);
   if (i >= n) return;
   const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
-  const int idx = nlist_thread<R>(i, pos4[i], rp, pos4, cell_start, num_cycles, rc, cap, stride, nbr);
+  const int idx = nlist_thread<R>(i, pos4[i], rp, pos4, cell_start, num_cycles, rc, cap, stride, nbr,
+                                  trim_x != 0);
   nlist_finish(i, idx, cap, count, max_count, status);
 }
 
@@ -446,7 +495,7 @@ __device__ __forceinline__ int unpack_tag(float v) { return __float_as_int(v); }
 __device__ __forceinline__ int unpack_tag(double v) { return (int)v; }
 
 template <class R>
-__global__ void __launch_bounds__(kStageThreads) k_nlist_staged(
+__global__ void __launch_bounds__(kStageThreads, 2) k_nlist_staged(
     const ListSeg* __restrict__ segs, int stage_cap, const typename Traits<R>::V4* __restrict__ pos4,
     const int* __restrict__ cell_start, const RepDev* __restrict__ reps, R rc, int cap, int stride,
     int* __restrict__ nbr, int* __restrict__ count, int* __restrict__ max_count, uint32_t* status,

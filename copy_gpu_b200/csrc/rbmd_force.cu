@@ -244,6 +244,8 @@ struct rbmd_force {
   bool is_cvff() const { return ff == "CVFF"; }
   bool with_coul_near() const { return far && ff != "EAM"; }
   double list_cut() const { return rc + skin; }
+  // Verlet lists order cells by x (the RBL lists keep the reference's order by caller id)
+  bool sort_x() const { return nbr_type != "RBL" && num_cycles == 1; }
 };
 
 namespace {
@@ -660,7 +662,8 @@ void launch_nlist(rbmd_force* f, cudaStream_t s) {
   k_nlist<R><<<(f->n + bs - 1) / bs, bs, 0, s>>>(
       f->n, (const typename Traits<R>::V4*)f->d_pos4, f->d_cell_start, f->d_reps,
       f->nrep > 1 ? f->d_rep_of : nullptr, f->num_cycles, (R)f->list_cut(), f->cap, f->stride, f->d_nbr,
-      f->d_count, f->d_maxcount, f->d_status, f->skin > 0 ? f->d_rebuild : nullptr, f->d_nbuilds);
+      f->d_count, f->d_maxcount, f->d_status, f->skin > 0 ? f->d_rebuild : nullptr, f->d_nbuilds,
+      f->sort_x() ? 1 : 0);
   f->launches++;
 }
 
@@ -695,7 +698,7 @@ void launch_sort(rbmd_force* f, cudaStream_t s, bool bin, bool regather) {
   k_cell_sort_gather<R><<<(f->ncell_total + 7) / 8, 256, 0, s>>>(
       f->ncell_total, f->d_cell_start, f->d_tmp, f->at.pos, f->at.charge, f->at.type, f->at.molecule,
       f->nrep > 1 ? f->d_rep_of : nullptr, f->d_reps, f->d_slot_atom, f->d_atom_slot,
-      (typename Traits<R>::V4*)f->d_pos4, nullptr, f->d_meta, f->d_xref, rb);
+      (typename Traits<R>::V4*)f->d_pos4, nullptr, f->d_meta, f->d_xref, rb, f->sort_x() ? 1 : 0);
   f->launches += 4;
   if (rb && regather) {
     // list reuse: refresh the slot caches from the new positions (no-op on rebuild steps)
