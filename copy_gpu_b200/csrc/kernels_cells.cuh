@@ -147,8 +147,10 @@ __device__ __forceinline__ unsigned long long ord_key(double x) {
 // row of consecutive x cells is ordered by x, which lets the list build skip the candidates
 // beyond the cutoff in x by binary search.  Cells above kMaxCellAtoms keep the scatter order
 // (flagged by the scan).
+constexpr int kSortWarps = 4;   // cells (one per warp) per block of k_cell_sort_gather
+
 template <class R>
-__global__ void __launch_bounds__(256) k_cell_sort_gather(
+__global__ void __launch_bounds__(32 * kSortWarps) k_cell_sort_gather(
     int ncell, const int* __restrict__ start, const int* __restrict__ tmp_slot_atom,
     const double* __restrict__ pos, const double* __restrict__ charge,
     const int* __restrict__ type, const int* __restrict__ mol, const int* __restrict__ rep_of,
@@ -156,15 +158,21 @@ __global__ void __launch_bounds__(256) k_cell_sort_gather(
     typename Traits<R>::V4* __restrict__ pos4, void* __restrict__ frac_out,
     int2* __restrict__ meta, double* __restrict__ xref, const int* __restrict__ rebuild, int sort_x) {
   if (rebuild && !*rebuild) return;
-  __shared__ int ids[8][kMaxCellAtoms];
+  using Key = decltype(ord_key((R)0));
+  __shared__ int ids[kSortWarps][kMaxCellAtoms];
+  __shared__ Key keys[kSortWarps][kMaxCellAtoms];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int cell = blockIdx.x * 8 + w;
+  const int cell = blockIdx.x * kSortWarps + w;
   if (cell >= ncell) return;
   const int s0 = start[cell], n = start[cell + 1] - s0;
   if (n == 0) return;
   const bool sortable = n <= kMaxCellAtoms;
   if (sortable)
-    for (int k = lane; k < n; k += 32) ids[w][k] = tmp_slot_atom[s0 + k];
+    for (int k = lane; k < n; k += 32) {
+      const int id = tmp_slot_atom[s0 + k];
+      ids[w][k] = id;
+      if (sort_x) keys[w][k] = ord_key((R)pos[3 * id]);
+    }
   __syncwarp();
   for (int k = lane; k < n; k += 32) {
     int id = sortable ? ids[w][k] : tmp_slot_atom[s0 + k];
@@ -172,11 +180,10 @@ __global__ void __launch_bounds__(256) k_cell_sort_gather(
     if (sortable) {
       rank = 0;
       if (sort_x) {
-        const auto kk = ord_key((R)pos[3 * id]);
+        const Key kk = keys[w][k];
         for (int m = 0; m < n; ++m) {
-          const int im = ids[w][m];
-          const auto km = ord_key((R)pos[3 * im]);
-          rank += km < kk || (km == kk && im < id);
+          const Key km = keys[w][m];
+          rank += km < kk || (km == kk && ids[w][m] < id);
         }
       } else {
         for (int m = 0; m < n; ++m) rank += ids[w][m] < id;
@@ -433,6 +440,8 @@ __global__ void __launch_bounds__(256) k_nlist_warp(
   const bool x_contig = ci[0] - 1 >= 0 && ci[0] + 1 < dx0;
   const unsigned below = (1u << lane) - 1u;
   int idx = 0;
+  // (no x-window search here: a serial binary search per row costs the warp more latency than
+  // the 32-wide candidate test it would save)
   auto scan = [&](int s0, int s1, R o0, R o1, R o2, int code) {
     for (int base = s0; base < s1; base += 32) {
       const int sj = base + lane;
@@ -499,7 +508,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) k_nlist_staged(
     const ListSeg* __restrict__ segs, int stage_cap, const typename Traits<R>::V4* __restrict__ pos4,
     const int* __restrict__ cell_start, const RepDev* __restrict__ reps, R rc, int cap, int stride,
     int* __restrict__ nbr, int* __restrict__ count, int* __restrict__ max_count, uint32_t* status,
-    const int* __restrict__ rebuild, unsigned long long* __restrict__ nbuilds) {
+    const int* __restrict__ rebuild, unsigned long long* __restrict__ nbuilds, int trim_x) {
   using V4 = typename Traits<R>::V4;
   if (rebuild && !*rebuild) return;
   if (blockIdx.x == 0 && threadIdx.x == 0 && nbuilds) atomicAdd(nbuilds, 1ull);
@@ -578,10 +587,27 @@ __global__ void __launch_bounds__(kStageThreads, 2) k_nlist_staged(
     int idx = 0;
     if (staged && ci[1] == sg.y && ci[2] == sg.z && ci[0] >= sg.x0 && ci[0] < sg.x1) {
       const int u0 = ci[0] - sg.x0;   // staged cells u0 .. u0 + 2 of every row
+      // staged x already carries the periodic shift, and a row's cells are ordered by x
+      // (rows that wrap in x are walked whole: atoms outside the box, binned into the last or
+      // first cell, break the order across the wrap)
+      const R xm = rc + (fabs(pix[0]) + (R)2 * rc) * (R)1e-5 + (R)1e-6;
+      const bool trim = trim_x && ci[0] - 1 >= 0 && ci[0] + 1 < d0;
       for (int r = 0; r < 9; ++r) {
-        const int t1 = cs[r * W + u0 + 3];
+        int t0 = cs[r * W + u0], t1 = cs[r * W + u0 + 3];
+        if (trim) {
+          for (int lo = t0, hi = t1; lo < hi;) {
+            const int mid = (lo + hi) >> 1;
+            if (stage[mid].x < pix[0] - xm) lo = t0 = mid + 1;
+            else hi = mid;
+          }
+          for (int lo = t0, hi = t1; lo < hi;) {
+            const int mid = (lo + hi) >> 1;
+            if (stage[mid].x < pix[0] + xm) lo = mid + 1;
+            else hi = t1 = mid;
+          }
+        }
 #pragma unroll 4
-        for (int t = cs[r * W + u0]; t < t1; ++t) {
+        for (int t = t0; t < t1; ++t) {
           const V4 q = stage[t];
           const R r0 = sub_rn(q.x, pix[0]);
           const R r1 = sub_rn(q.y, pix[1]);

@@ -646,7 +646,7 @@ void launch_nlist(rbmd_force* f, cudaStream_t s) {
     k_nlist_staged<R><<<f->nsegs, kStageThreads, smem, s>>>(
         f->d_segs, f->stage_cap, (const typename Traits<R>::V4*)f->d_pos4, f->d_cell_start, f->d_reps,
         (R)f->list_cut(), f->cap, f->stride, f->d_nbr, f->d_count, f->d_maxcount, f->d_status,
-        f->skin > 0 ? f->d_rebuild : nullptr, f->d_nbuilds);
+        f->skin > 0 ? f->d_rebuild : nullptr, f->d_nbuilds, f->sort_x() ? 1 : 0);
     f->launches++;
     return;
   }
@@ -695,7 +695,7 @@ void launch_sort(rbmd_force* f, cudaStream_t s, bool bin, bool regather) {
   k_cell_scan<<<nblk, 1024, 0, s>>>(f->ncell_total, f->d_cell_count, f->d_block_sums, f->d_cell_start,
                                     f->d_cursor, rb);
   k_scatter<<<(n + 255) / 256, 256, 0, s>>>(n, f->d_cell_of, f->d_cell_start, f->d_cursor, f->d_tmp, rb);
-  k_cell_sort_gather<R><<<(f->ncell_total + 7) / 8, 256, 0, s>>>(
+  k_cell_sort_gather<R><<<(f->ncell_total + kSortWarps - 1) / kSortWarps, 32 * kSortWarps, 0, s>>>(
       f->ncell_total, f->d_cell_start, f->d_tmp, f->at.pos, f->at.charge, f->at.type, f->at.molecule,
       f->nrep > 1 ? f->d_rep_of : nullptr, f->d_reps, f->d_slot_atom, f->d_atom_slot,
       (typename Traits<R>::V4*)f->d_pos4, nullptr, f->d_meta, f->d_xref, rb, f->sort_x() ? 1 : 0);
