@@ -617,7 +617,8 @@ def run_config(args):
             "warmup": args.warmup, "ms_per_step": run["ms"] / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if cfg.get("precision") == "fp64" else "f32",
             "data": "synthetic",
-            "config": {"workload": desc, "atoms": n, "list_builds_per_step": run["builds"] / args.steps,
+            "config": {"workload": desc, "atoms": n,
+                       "list_builds_per_step": run["builds"] / args.steps / (len(boxes) if boxes else 1),
                        "threads_per_block": {"list": run["blocks"][0], "force": run["blocks"][1]},
                        "step_launch": "cuda graph replay (one launch per step)"},
             "e2e": {"value": n / (run["e2e_ms"] / 1e3), "unit": "atom-steps/s", "h2d_bytes_per_step": 24 * n,

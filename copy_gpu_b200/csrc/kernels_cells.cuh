@@ -25,15 +25,18 @@ __device__ __forceinline__ int cell_of_pos(const RepDev& rp, R x, R y, R z) {
   return rp.cell_base + ijk[0] + ijk[1] * rp.dims[0] + ijk[2] * rp.dims[0] * rp.dims[1];
 }
 
-// rebuild (nullable): bin only on list-rebuild steps (Verlet skin).
+// Verlet-skin rebuild flags: rebuild[r] for replica r and rebuild[n_replicas] for "any replica";
+// a replica whose atoms all stayed within skin/2 keeps its cells, slots and list.
+// rebuild (nullable): bin only the atoms of rebuilding replicas.
 template <class R>
 __global__ void k_bin(int n, const double* __restrict__ pos, const int* __restrict__ rep_of,
                       const RepDev* __restrict__ reps, int* __restrict__ cell_of,
                       int* __restrict__ cell_count, uint32_t* status, const int* __restrict__ rebuild) {
-  if (rebuild && !*rebuild) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const RepDev& rp = reps[rep_of ? rep_of[i] : 0];
+  const int r = rep_of ? rep_of[i] : 0;
+  if (rebuild && !rebuild[r]) return;
+  const RepDev& rp = reps[r];
   double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
   if (!isfinite(x) || !isfinite(y) || !isfinite(z)) set_flag(status, kFlagNonFinite);
   int c = cell_of_pos<R>(rp, (R)x, (R)y, (R)z);
@@ -44,8 +47,27 @@ __global__ void k_bin(int n, const double* __restrict__ pos, const int* __restri
 // Exclusive scan of the cell counts in two parallel passes: k_cell_block_sums reduces blocks of
 // kScanBlock cells; k_cell_scan gives each block its prefix (sum of the preceding block sums)
 // and scans its cells.  cell_start[ncell] = n; scatter cursors are cleared; over-full cells flag.
-// `rebuild` (nullable): skip the pass when the neighbour list is being reused.
+// `rebuild` (nullable, the "any replica" flag): skip the pass when every list is reused.  Cells
+// of replicas that keep their list keep their counts, so their starts come out unchanged.
 constexpr int kScanBlock = 4096;
+
+// Number of replicas whose list is rebuilt in this pass (the list-build counter counts replica
+// lists: with one replica, the number of rebuilding passes).
+__device__ __forceinline__ unsigned long long rebuilt_replicas(const int* rebuild, int n_rep) {
+  if (!rebuild) return (unsigned long long)n_rep;
+  unsigned long long c = 0;
+  for (int r = 0; r < n_rep; ++r) c += rebuild[r] != 0;
+  return c;
+}
+
+// Zero the cell counts of the rebuilding replicas (all of them when rebuild is null).
+__global__ void k_zero_counts(int ncell, const int* __restrict__ cell_rep, const int* __restrict__ rebuild,
+                              int* __restrict__ cell_count) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  if (rebuild && !rebuild[cell_rep ? cell_rep[c] : 0]) return;
+  cell_count[c] = 0;
+}
 
 __global__ void __launch_bounds__(1024) k_cell_block_sums(int ncell, const int* __restrict__ count,
                                                           int* __restrict__ block_sums,
@@ -122,10 +144,10 @@ __global__ void __launch_bounds__(1024) k_cell_scan(int ncell, const int* __rest
 
 __global__ void k_scatter(int n, const int* __restrict__ cell_of, const int* __restrict__ start,
                           int* __restrict__ cursor, int* __restrict__ tmp_slot_atom,
-                          const int* __restrict__ rebuild) {
-  if (rebuild && !*rebuild) return;
+                          const int* __restrict__ rep_of, const int* __restrict__ rebuild) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (rebuild && !rebuild[rep_of ? rep_of[i] : 0]) return;
   int c = cell_of[i];
   int s = start[c] + atomicAdd(&cursor[c], 1);
   tmp_slot_atom[s] = i;
@@ -156,14 +178,15 @@ __global__ void __launch_bounds__(32 * kSortWarps) k_cell_sort_gather(
     const int* __restrict__ type, const int* __restrict__ mol, const int* __restrict__ rep_of,
     const RepDev* __restrict__ reps, int* __restrict__ slot_atom, int* __restrict__ atom_slot,
     typename Traits<R>::V4* __restrict__ pos4, void* __restrict__ frac_out,
-    int2* __restrict__ meta, double* __restrict__ xref, const int* __restrict__ rebuild, int sort_x) {
-  if (rebuild && !*rebuild) return;
+    int2* __restrict__ meta, double* __restrict__ xref, const int* __restrict__ rebuild, int sort_x,
+    const int* __restrict__ cell_rep) {
   using Key = decltype(ord_key((R)0));
   __shared__ int ids[kSortWarps][kMaxCellAtoms];
   __shared__ Key keys[kSortWarps][kMaxCellAtoms];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int cell = blockIdx.x * kSortWarps + w;
   if (cell >= ncell) return;
+  if (rebuild && !rebuild[cell_rep ? cell_rep[cell] : 0]) return;
   const int s0 = start[cell], n = start[cell + 1] - s0;
   if (n == 0) return;
   const bool sortable = n <= kMaxCellAtoms;
@@ -239,10 +262,10 @@ __global__ void k_regather(int n, const int* __restrict__ slot_atom, const doubl
                            const RepDev* __restrict__ reps, typename Traits<R>::V4* __restrict__ pos4,
                            void* __restrict__ frac_out, const double* __restrict__ xref,
                            const int* __restrict__ rebuild) {
-  if (rebuild && *rebuild) return;   // the cell sort refreshed the caches this step
   int slot = blockIdx.x * blockDim.x + threadIdx.x;
   if (slot >= n) return;
   int id = slot_atom[slot];
+  if (rebuild && rebuild[rep_of ? rep_of[id] : 0]) return;   // the cell sort refreshed these caches
   const double x = pos[3 * id], y = pos[3 * id + 1], z = pos[3 * id + 2];
   const double q = charge ? charge[id] : 0.0;
   typename Traits<R>::V4 v;
@@ -402,12 +425,13 @@ __global__ void __launch_bounds__(256) k_nlist(
     const RepDev* __restrict__ reps, const int* __restrict__ rep_of_slot, int num_cycles, R rc,
     int cap, int stride, int* __restrict__ nbr, int* __restrict__ count, int* __restrict__ max_count,
     uint32_t* status, const int* __restrict__ rebuild, unsigned long long* __restrict__ nbuilds,
-    int trim_x) {
-  if (rebuild && !*rebuild) return;
+    int trim_x, int n_rep) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i == 0 && nbuilds) atomicAdd(nbuilds, 1ull);
+  if (i == 0 && nbuilds) atomicAdd(nbuilds, rebuilt_replicas(rebuild, n_rep));
   if (i >= n) return;
-  const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
+  const int r = rep_of_slot ? rep_of_slot[i] : 0;
+  if (rebuild && !rebuild[r]) return;
+  const RepDev& rp = reps[r];
   const int idx = nlist_thread<R>(i, pos4[i], rp, pos4, cell_start, num_cycles, rc, cap, stride, nbr,
                                   trim_x != 0);
   nlist_finish(i, idx, cap, count, max_count, status);
@@ -421,14 +445,15 @@ __global__ void __launch_bounds__(256) k_nlist_warp(
     int n, const typename Traits<R>::V4* __restrict__ pos4, const int* __restrict__ cell_start,
     const RepDev* __restrict__ reps, const int* __restrict__ rep_of_slot, R rc, int cap, int stride,
     int* __restrict__ nbr, int* __restrict__ count, int* __restrict__ max_count, uint32_t* status,
-    const int* __restrict__ rebuild, unsigned long long* __restrict__ nbuilds) {
+    const int* __restrict__ rebuild, unsigned long long* __restrict__ nbuilds, int n_rep) {
   using V4 = typename Traits<R>::V4;
-  if (rebuild && !*rebuild) return;
   const int lane = threadIdx.x & 31;
   const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (i == 0 && lane == 0 && nbuilds) atomicAdd(nbuilds, 1ull);
+  if (i == 0 && lane == 0 && nbuilds) atomicAdd(nbuilds, rebuilt_replicas(rebuild, n_rep));
   if (i >= n) return;
-  const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
+  const int r = rep_of_slot ? rep_of_slot[i] : 0;
+  if (rebuild && !rebuild[r]) return;
+  const RepDev& rp = reps[r];
   const V4 pi = pos4[i];
   const R pix[3] = {pi.x, pi.y, pi.z};
   int ci[3];
@@ -508,10 +533,10 @@ __global__ void __launch_bounds__(kStageThreads, 2) k_nlist_staged(
     const ListSeg* __restrict__ segs, int stage_cap, const typename Traits<R>::V4* __restrict__ pos4,
     const int* __restrict__ cell_start, const RepDev* __restrict__ reps, R rc, int cap, int stride,
     int* __restrict__ nbr, int* __restrict__ count, int* __restrict__ max_count, uint32_t* status,
-    const int* __restrict__ rebuild, unsigned long long* __restrict__ nbuilds, int trim_x) {
+    const int* __restrict__ rebuild, unsigned long long* __restrict__ nbuilds, int trim_x, int n_rep) {
   using V4 = typename Traits<R>::V4;
-  if (rebuild && !*rebuild) return;
-  if (blockIdx.x == 0 && threadIdx.x == 0 && nbuilds) atomicAdd(nbuilds, 1ull);
+  if (blockIdx.x == 0 && threadIdx.x == 0 && nbuilds) atomicAdd(nbuilds, rebuilt_replicas(rebuild, n_rep));
+  if (rebuild && !rebuild[segs[blockIdx.x].rep]) return;
   extern __shared__ __align__(16) unsigned char stage_raw[];
   V4* stage = reinterpret_cast<V4*>(stage_raw);
   __shared__ int cs[kStageCells + 1];     // staged start of staged cell k = row * W + u

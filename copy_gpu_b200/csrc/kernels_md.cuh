@@ -32,6 +32,7 @@ __global__ void k_kick_drift(MdParams mp, double* __restrict__ pos, double* __re
                              double* __restrict__ x_old, double* __restrict__ v_old,
                              int* __restrict__ cell_of, int* __restrict__ cell_count, uint32_t* status,
                              const double* __restrict__ xref, double half_skin2, int* __restrict__ rebuild,
+                             int n_rep,
                              const int* __restrict__ atom_slot, const double* __restrict__ charge,
                              typename Traits<R>::V4* __restrict__ pos4) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -73,7 +74,10 @@ __global__ void k_kick_drift(MdParams mp, double* __restrict__ pos, double* __re
       d2 += dd * dd;
       u[d] = r0 + dd;
     }
-    if (d2 > half_skin2 && *rebuild == 0) atomicExch(rebuild, 1);
+    if (d2 > half_skin2 && rebuild[r] == 0) {
+      atomicExch(rebuild + r, 1);
+      atomicExch(rebuild + n_rep, 1);
+    }
     if (pos4) {   // on a rebuild step the cell sort overwrites the whole cache afterwards
       typename Traits<R>::V4 v;
       v.x = (R)u[0]; v.y = (R)u[1]; v.z = (R)u[2];
@@ -92,10 +96,11 @@ __global__ void k_kick_drift(MdParams mp, double* __restrict__ pos, double* __re
 // any atom moved more than skin/2 (nearest image) from its position at the last build.
 __global__ void k_skin_check(int n, const double* __restrict__ pos, const double* __restrict__ xref,
                              const int* __restrict__ rep_of, const RepDev* __restrict__ reps,
-                             double half_skin2, int* __restrict__ rebuild) {
+                             double half_skin2, int* __restrict__ rebuild, int n_rep) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const RepDev& rp = reps[rep_of ? rep_of[i] : 0];
+  const int r = rep_of ? rep_of[i] : 0;
+  const RepDev& rp = reps[r];
   double d2 = 0;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -103,7 +108,10 @@ __global__ void k_skin_check(int n, const double* __restrict__ pos, const double
     dd -= rp.box_d[d] * rint(dd / rp.box_d[d]);
     d2 += dd * dd;
   }
-  if (!(d2 <= half_skin2) && *rebuild == 0) atomicExch(rebuild, 1);
+  if (!(d2 <= half_skin2) && rebuild[r] == 0) {
+    atomicExch(rebuild + r, 1);
+    atomicExch(rebuild + n_rep, 1);
+  }
 }
 
 // Advance the device step counter the k-samplers read (end of a step's k-space chain).

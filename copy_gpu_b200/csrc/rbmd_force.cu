@@ -169,7 +169,8 @@ struct rbmd_force {
   int64_t rbl_sizes_h[3] = {0, 0, 0};
   double* d_mean_partial = nullptr;
   float* d_erf_tab = nullptr;   // compat.rbl_erf_table
-  int *d_rebuild = nullptr, *d_block_sums = nullptr;
+  int *d_rebuild = nullptr, *d_block_sums = nullptr;   // d_rebuild[nrep + 1]: per replica, then any
+  int* d_cell_rep = nullptr;                            // replica of each cell (batches only)
   unsigned long long* d_nbuilds = nullptr;
   ListSeg* d_segs = nullptr;   // staged list build: one block per segment of a cell row
   int nsegs = 0, stage_cap = 0;
@@ -309,7 +310,7 @@ void free_all(rbmd_force* f) {
   dfree(f->d_count2); dfree(f->d_mean_partial); dfree(f->d_erf_tab);
   dfree(f->d_prep); dfree(f->d_cdf); dfree(f->d_wbin); dfree(f->d_pw); dfree(f->d_mlp); dfree(f->d_h);
   dfree(f->d_feat); dfree(f->d_spec); dfree(f->d_spec_init);
-  dfree(f->d_rebuild); dfree(f->d_block_sums); dfree(f->d_xref); dfree(f->d_nbuilds);
+  dfree(f->d_rebuild); dfree(f->d_block_sums); dfree(f->d_cell_rep); dfree(f->d_xref); dfree(f->d_nbuilds);
   dfree(f->d_segs);
   f->nsegs = 0;
   dfree(f->d_eslot); dfree(f->d_esum);
@@ -646,7 +647,7 @@ void launch_nlist(rbmd_force* f, cudaStream_t s) {
     k_nlist_staged<R><<<f->nsegs, kStageThreads, smem, s>>>(
         f->d_segs, f->stage_cap, (const typename Traits<R>::V4*)f->d_pos4, f->d_cell_start, f->d_reps,
         (R)f->list_cut(), f->cap, f->stride, f->d_nbr, f->d_count, f->d_maxcount, f->d_status,
-        f->skin > 0 ? f->d_rebuild : nullptr, f->d_nbuilds, f->sort_x() ? 1 : 0);
+        f->skin > 0 ? f->d_rebuild : nullptr, f->d_nbuilds, f->sort_x() ? 1 : 0, f->nrep);
     f->launches++;
     return;
   }
@@ -654,7 +655,7 @@ void launch_nlist(rbmd_force* f, cudaStream_t s) {
     k_nlist_warp<R><<<(f->n + 7) / 8, 256, 0, s>>>(
         f->n, (const typename Traits<R>::V4*)f->d_pos4, f->d_cell_start, f->d_reps,
         f->nrep > 1 ? f->d_rep_of : nullptr, (R)f->list_cut(), f->cap, f->stride, f->d_nbr, f->d_count,
-        f->d_maxcount, f->d_status, f->skin > 0 ? f->d_rebuild : nullptr, f->d_nbuilds);
+        f->d_maxcount, f->d_status, f->skin > 0 ? f->d_rebuild : nullptr, f->d_nbuilds, f->nrep);
     f->launches++;
     return;
   }
@@ -663,7 +664,7 @@ void launch_nlist(rbmd_force* f, cudaStream_t s) {
       f->n, (const typename Traits<R>::V4*)f->d_pos4, f->d_cell_start, f->d_reps,
       f->nrep > 1 ? f->d_rep_of : nullptr, f->num_cycles, (R)f->list_cut(), f->cap, f->stride, f->d_nbr,
       f->d_count, f->d_maxcount, f->d_status, f->skin > 0 ? f->d_rebuild : nullptr, f->d_nbuilds,
-      f->sort_x() ? 1 : 0);
+      f->sort_x() ? 1 : 0, f->nrep);
   f->launches++;
 }
 
@@ -683,22 +684,33 @@ template <class R>
 void launch_sort(rbmd_force* f, cudaStream_t s, bool bin, bool regather) {
   PhaseScope ps(f, kPhSort, s);
   const int n = f->n;
+  // per-replica rebuild flags (Verlet skin): rb[r], and rb[nrep] = any replica
   const int* rb = f->skin > 0 ? f->d_rebuild : nullptr;
+  const int* rb_any = rb ? rb + f->nrep : nullptr;
+  const int* rep_of = f->nrep > 1 ? f->d_rep_of : nullptr;
   if (bin) {
-    cudaMemsetAsync(f->d_cell_count, 0, sizeof(int) * f->ncell_total, s);
-    k_bin<R><<<(n + 255) / 256, 256, 0, s>>>(n, f->at.pos, f->nrep > 1 ? f->d_rep_of : nullptr,
-                                             f->d_reps, f->d_cell_of, f->d_cell_count, f->d_status, rb);
+    if (rb) {
+      k_zero_counts<<<(f->ncell_total + 255) / 256, 256, 0, s>>>(f->ncell_total, f->d_cell_rep, rb,
+                                                                  f->d_cell_count);
+      f->launches++;
+    } else {
+      cudaMemsetAsync(f->d_cell_count, 0, sizeof(int) * f->ncell_total, s);
+    }
+    k_bin<R><<<(n + 255) / 256, 256, 0, s>>>(n, f->at.pos, rep_of, f->d_reps, f->d_cell_of, f->d_cell_count,
+                                             f->d_status, rb);
     f->launches++;
   }
   const int nblk = (f->ncell_total + kScanBlock - 1) / kScanBlock;
-  k_cell_block_sums<<<nblk, 1024, 0, s>>>(f->ncell_total, f->d_cell_count, f->d_block_sums, rb, f->d_status);
+  k_cell_block_sums<<<nblk, 1024, 0, s>>>(f->ncell_total, f->d_cell_count, f->d_block_sums, rb_any,
+                                          f->d_status);
   k_cell_scan<<<nblk, 1024, 0, s>>>(f->ncell_total, f->d_cell_count, f->d_block_sums, f->d_cell_start,
-                                    f->d_cursor, rb);
-  k_scatter<<<(n + 255) / 256, 256, 0, s>>>(n, f->d_cell_of, f->d_cell_start, f->d_cursor, f->d_tmp, rb);
+                                    f->d_cursor, rb_any);
+  k_scatter<<<(n + 255) / 256, 256, 0, s>>>(n, f->d_cell_of, f->d_cell_start, f->d_cursor, f->d_tmp, rep_of,
+                                            rb);
   k_cell_sort_gather<R><<<(f->ncell_total + kSortWarps - 1) / kSortWarps, 32 * kSortWarps, 0, s>>>(
       f->ncell_total, f->d_cell_start, f->d_tmp, f->at.pos, f->at.charge, f->at.type, f->at.molecule,
-      f->nrep > 1 ? f->d_rep_of : nullptr, f->d_reps, f->d_slot_atom, f->d_atom_slot,
-      (typename Traits<R>::V4*)f->d_pos4, nullptr, f->d_meta, f->d_xref, rb, f->sort_x() ? 1 : 0);
+      rep_of, f->d_reps, f->d_slot_atom, f->d_atom_slot, (typename Traits<R>::V4*)f->d_pos4, nullptr,
+      f->d_meta, f->d_xref, rb, f->sort_x() ? 1 : 0, f->d_cell_rep);
   f->launches += 4;
   if (rb && regather) {
     // list reuse: refresh the slot caches from the new positions (no-op on rebuild steps)
@@ -984,13 +996,13 @@ void launch_compute(rbmd_force* f, cudaStream_t s) {
   cudaMemsetAsync(f->d_maxcount, 0, 2 * sizeof(int), s);
   if (f->skin > 0 && f->list_valid) {
     // reuse the list when no atom moved more than skin/2 since it was built
-    cudaMemsetAsync(f->d_rebuild, 0, sizeof(int), s);
+    cudaMemsetAsync(f->d_rebuild, 0, sizeof(int) * (f->nrep + 1), s);
     k_skin_check<<<(f->n + 255) / 256, 256, 0, s>>>(f->n, f->at.pos, f->d_xref,
                                                     f->nrep > 1 ? f->d_rep_of : nullptr, f->d_reps,
-                                                    0.25 * f->skin * f->skin, f->d_rebuild);
+                                                    0.25 * f->skin * f->skin, f->d_rebuild, f->nrep);
     f->launches++;
   } else if (f->d_rebuild) {
-    cudaMemsetAsync(f->d_rebuild, 1, sizeof(int), s);   // nonzero: rebuild
+    cudaMemsetAsync(f->d_rebuild, 1, sizeof(int) * (f->nrep + 1), s);   // nonzero: rebuild
   }
   launch_force_tail<R>(f, s, true, true);
   f->list_valid = true;
@@ -1058,7 +1070,7 @@ void launch_step(rbmd_force* f, cudaStream_t s) {
   // moves the atoms afterwards) and k_bin bins on rebuild steps only
   if (!skin) cudaMemsetAsync(f->d_cell_count, 0, sizeof(int) * f->ncell_total, s);
   // with a skin the drift kernel decides; a missing or overflowed list forces a rebuild
-  if (skin) cudaMemsetAsync(f->d_rebuild, f->list_valid ? 0 : 1, sizeof(int), s);
+  if (skin) cudaMemsetAsync(f->d_rebuild, f->list_valid ? 0 : 1, sizeof(int) * (f->nrep + 1), s);
   // (the slot map exists once a cell sort has run: list_valid)
   const bool drift_cache = skin && !shake && f->list_valid;
   // stages 1-2: kick, drift + wrap, bin (binning sees the unconstrained positions, as the
@@ -1070,7 +1082,8 @@ void launch_step(rbmd_force* f, cudaStream_t s) {
                                                     f->d_reps, f->d_lambda, f->d_xold, f->d_vold,
                                                     skin ? nullptr : f->d_cell_of, skin ? nullptr : f->d_cell_count,
                                                     f->d_status, skin ? f->d_xref : nullptr,
-                                                    0.25 * f->skin * f->skin, f->d_rebuild, f->d_atom_slot,
+                                                    0.25 * f->skin * f->skin, f->d_rebuild, f->nrep,
+                                                    f->d_atom_slot,
                                                     f->at.charge,
                                                     drift_cache ? (typename Traits<R>::V4*)f->d_pos4 : nullptr);
     f->launches++;
@@ -1372,7 +1385,7 @@ rbmd_status autotune_impl(rbmd_force* f, cudaStream_t s) {
   auto best_of = [&](auto launch) -> float {
     float best = 1e30f;
     for (int rep = 0; rep < 4; ++rep) {
-      if (f->d_rebuild) cudaMemsetAsync(f->d_rebuild, 1, sizeof(int), s);
+      if (f->d_rebuild) cudaMemsetAsync(f->d_rebuild, 1, sizeof(int) * (f->nrep + 1), s);
       cudaEventRecord(a, s);
       launch();
       cudaEventRecord(b, s);
@@ -1623,8 +1636,15 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
   CK(dalloc(&f->d_maxcount, 2));
   CK(dalloc(&f->d_nbuilds, 1));
   CK(cudaMemset(f->d_nbuilds, 0, sizeof(unsigned long long)));
-  CK(dalloc(&f->d_rebuild, 1));
-  CK(cudaMemset(f->d_rebuild, 0, sizeof(int)));
+  CK(dalloc(&f->d_rebuild, (size_t)nrep + 1));
+  CK(cudaMemset(f->d_rebuild, 0, sizeof(int) * (nrep + 1)));
+  if (nrep > 1) {
+    std::vector<int> cr(f->ncell_total);
+    for (int r = 0; r < nrep; ++r)
+      for (int c = 0; c < f->reps_h[r].ncell; ++c) cr[f->reps_h[r].cell_base + c] = r;
+    CK(dalloc(&f->d_cell_rep, cr.size()));
+    CK(cudaMemcpy(f->d_cell_rep, cr.data(), sizeof(int) * cr.size(), cudaMemcpyHostToDevice));
+  }
   CK(dalloc(&f->d_block_sums, (size_t)(f->ncell_total + kScanBlock - 1) / kScanBlock + 1));
   if (f->skin > 0) CK(dalloc(&f->d_xref, 3 * n));
   CK(dalloc(&f->d_status, 1));

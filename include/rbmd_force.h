@@ -209,8 +209,9 @@ RBMD_API rbmd_status rbmd_force_get_rhok(rbmd_force* f, double* rho_host, int32_
 RBMD_API rbmd_status rbmd_force_profile(rbmd_force* f, int32_t enable);
 RBMD_API rbmd_status rbmd_force_phase_ms(rbmd_force* f, double* ms, int64_t* counts, int32_t n);
 
-/* Number of neighbour-list builds since bind (with a Verlet skin the list is rebuilt only when
- * an atom moved more than skin/2; the reference rebuilds on every force call). */
+/* Number of neighbour-list builds since bind, counted per replica (with a Verlet skin a
+ * replica's list is rebuilt only when one of its atoms moved more than skin/2, and the other
+ * replicas keep theirs; the reference rebuilds on every force call). */
 RBMD_API rbmd_status rbmd_force_list_builds(rbmd_force* f, int64_t* builds);
 
 /* Library/kernel description for diagnostics: number of kernels the last compute or step

@@ -225,6 +225,45 @@ def test_batched_replicas_match_single(cuda):
     assert np.abs(dev0["pos"].cpu().numpy() - got[sl]).max() < 1e-12
 
 
+def test_per_replica_rebuild_matches_single(cuda):
+    """With a Verlet skin each replica rebuilds its own list when its own atoms moved more than
+    skin/2: after 60 FP32 steps replica 0 of a batch matches replica 0 advanced alone (1e-6 in
+    positions; its k-sampler stream is keyed by replica index 0 in both runs), the batch rebuilt
+    as many replica lists as the replicas alone did, and fewer than one rebuild of every replica
+    per step on which any replica rebuilds."""
+    import torch
+    r = systems.replicas(n_rep=4, nmin=700, nmax=1600, seed=21)
+    cfg = systems.electrolyte_config(P=16, precision="fp32", seed=9, ensemble="NVE")
+    cfg["hyper_parameters"]["neighbor"]["skin"] = 0.3
+    cfg["tuning"] = {"list_block": 128, "force_block": 128}
+    boxes = [Box(tuple(r["lo"][k]), tuple(r["hi"][k])) for k in range(4)]
+    dev = to_dev(r, cuda)
+    ff = make_ff(cfg, r, dev, boxes=boxes, offsets=r["offsets"])
+    ff.Execute()
+    ff.step(60)
+    torch.cuda.synchronize()
+    assert ff.status() == 0
+    got = dev["pos"].cpu().numpy()
+    builds_batch = ff.list_builds()
+    off = r["offsets"]
+    singles = []
+    for k in range(4):
+        sl = slice(off[k], off[k + 1])
+        sk = {key: (val[sl] if isinstance(val, np.ndarray) and val.shape[:1] == (off[-1],) else val)
+              for key, val in r.items()}
+        sk["lo"], sk["hi"] = r["lo"][k], r["hi"][k]
+        devk = to_dev(sk, cuda)
+        ffk = make_ff(cfg, sk, devk)
+        ffk.Execute()
+        ffk.step(60)
+        torch.cuda.synchronize()
+        singles.append(ffk.list_builds())
+        if k == 0:   # the k-sampler streams are keyed by replica index: only replica 0 matches alone
+            assert np.abs(devk["pos"].cpu().numpy() - got[sl]).max() < 1e-6
+    assert abs(builds_batch - sum(singles)) <= 2, (builds_batch, singles)
+    assert builds_batch < 4 * max(singles), (builds_batch, singles)
+
+
 def test_batched_replicas_injected_k(cuda, oracle_lib):
     """With injected k-samples every replica's force equals its stand-alone force."""
     import torch
