@@ -1,4 +1,4 @@
-// eam_funcfl.hpp -- host-side funcfl reader and 7-coefficient spline build.
+// eam_funcfl.hpp -- host-side funcfl and setfl readers and the 7-coefficient spline build.
 //
 // Follows ExecutionNVT::ReadPotentialFile / file2array / interpolate / array2spline
 // (rbmd/framework/run/ExecutionNVT.cpp:903-1107), which is LAMMPS pair_eam's published
@@ -116,6 +116,72 @@ inline int funcfl_load(const std::string& path, FuncflTables& t) {
   funcfl_interpolate(nr, dr, rhor, t.rhor);
   funcfl_interpolate(nr, dr, z2r, t.z2r);
   return 0;
+}
+
+// setfl (LAMMPS eam/alloy) reader for the single-element EAM path: header of three comment lines,
+// "N el_1 .. el_N", "nrho drho nr dr cut", per element a line (number, mass, lattice constant,
+// lattice) then F(rho)[nrho] and rho(r)[nr], then r*phi_ij(r)[nr] for i >= j.  The tables are
+// used on the file's own grids (LAMMPS' file2array copies setfl arrays without resampling), with
+// z2r = r*phi of the first element's self pair; `element` picks another element (0-based).
+// The reference reads funcfl files only (ExecutionNVT.cpp:903-1107): this reader widens the
+// inputs a drop-in user can bring, and shares funcfl_interpolate and the device path.
+inline int setfl_load(const std::string& path, FuncflTables& t, int element = 0) {
+  std::ifstream in(path);
+  if (!in.is_open()) return 1;
+  for (int i = 0; i < 3; ++i) in.ignore(std::numeric_limits<std::streamsize>::max(), '\n');
+  int nel = 0;
+  in >> nel;
+  if (!in || nel < 1 || element < 0 || element >= nel) return 2;
+  in.ignore(std::numeric_limits<std::streamsize>::max(), '\n');   // element names
+  int nrho = 0, nr = 0;
+  float drho = 0, dr = 0, cut = 0;
+  in >> nrho >> drho >> nr >> dr >> cut;
+  if (!in || nrho < 5 || nr < 5 || !(drho > 0) || !(dr > 0)) return 2;
+  std::vector<float> frho(nrho + 1, 0.f), rhor(nr + 1, 0.f), z2r(nr + 1, 0.f);
+  for (int e = 0; e < nel; ++e) {
+    double num, mass, lat;
+    std::string lattice;
+    in >> num >> mass >> lat >> lattice;
+    for (int m = 1; m <= nrho; ++m) {
+      float v;
+      in >> v;
+      if (e == element) frho[m] = v;
+    }
+    for (int m = 1; m <= nr; ++m) {
+      float v;
+      in >> v;
+      if (e == element) rhor[m] = v;
+    }
+    if (!in) return 3;
+  }
+  for (int i = 0; i < nel; ++i)
+    for (int j = 0; j <= i; ++j)
+      for (int m = 1; m <= nr; ++m) {
+        float v;
+        in >> v;
+        if (i == element && j == element) z2r[m] = v;
+      }
+  if (!in) return 3;
+  t.nrho = nrho;
+  t.nr = nr;
+  t.drho = drho;
+  t.dr = dr;
+  t.rhomax = (float)(nrho - 1) * drho;
+  t.cut = cut;
+  funcfl_interpolate(nrho, drho, frho, t.frho);
+  funcfl_interpolate(nr, dr, rhor, t.rhor);
+  funcfl_interpolate(nr, dr, z2r, t.z2r);
+  return 0;
+}
+
+// funcfl unless the name ends in ".alloy" or ".setfl" (or format == "setfl")
+inline int eam_load(const std::string& path, FuncflTables& t, const std::string& format = "") {
+  auto ends = [&](const char* suf) {
+    const std::string s(suf);
+    return path.size() >= s.size() && path.compare(path.size() - s.size(), s.size(), s) == 0;
+  };
+  if (format == "setfl" || (format.empty() && (ends(".alloy") || ends(".setfl")))) return setfl_load(path, t);
+  return funcfl_load(path, t);
 }
 
 }  // namespace rbmd

@@ -122,7 +122,7 @@ struct rbmd_force {
   bool tuned = false;
   bool list_valid = false;   // a list (and x_ref) exists from an earlier build
   int shake_max_iter = 5000;
-  std::string potential_file;
+  std::string potential_file, potential_format;   // format: "", "funcfl" or "setfl"
 
   // ---------------- replicas ----------------
   int nrep = 1;
@@ -1208,6 +1208,7 @@ rbmd_status parse_config(rbmd_force* f, const char* text) {
   using namespace rbmdjson;
   f->ff = rbmdjson::text(root, "hyper_parameters.force_field.type", "LJ/CUT");
   f->potential_file = rbmdjson::text(root, "hyper_parameters.force_field.potential_file", "");
+  f->potential_format = rbmdjson::text(root, "hyper_parameters.force_field.potential_format", "");
   f->nbr_type = rbmdjson::text(root, "hyper_parameters.neighbor.type", "VERLETLIST");
   if (f->nbr_type == "VERLET-LIST") f->nbr_type = "VERLETLIST";
   bool found = false;
@@ -1458,8 +1459,8 @@ rbmd_status rbmd_force_create(const char* json_text, int32_t n_replicas, const r
   const double one = 1.0;
   fill_lj(f, 1, &one, &one);
   if (f->is_eam() && !f->potential_file.empty()) {
-    if (funcfl_load(f->potential_file, f->eam_h) != 0) {
-      std::snprintf(g_last_error, sizeof g_last_error, "cannot read funcfl file %s",
+    if (eam_load(f->potential_file, f->eam_h, f->potential_format) != 0) {
+      std::snprintf(g_last_error, sizeof g_last_error, "cannot read EAM potential file %s",
                     f->potential_file.c_str());
       delete f;
       return RBMD_ERR_FILE;
@@ -1481,7 +1482,7 @@ rbmd_status rbmd_force_set_pair_coeffs(rbmd_force* f, int32_t n_types, const dou
 
 rbmd_status rbmd_force_load_funcfl(rbmd_force* f, const char* path) {
   if (!f || !path) return RBMD_ERR_ARG;
-  if (funcfl_load(path, f->eam_h) != 0) return RBMD_ERR_FILE;
+  if (eam_load(path, f->eam_h, f->potential_format) != 0) return RBMD_ERR_FILE;
   f->eam_loaded = true;
   f->potential_file = path;
   return RBMD_OK;

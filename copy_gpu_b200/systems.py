@@ -221,6 +221,34 @@ def write_johnson_funcfl(path, p=JOHNSON_CU):
     return path
 
 
+def johnson_terms(r, p=JOHNSON_CU):
+    """Johnson's f(r), phi(r) and their derivatives (analytic, for checks)."""
+    f = p["fe"] * np.exp(-p["beta"] * (r / p["re"] - 1.0))
+    phi = p["phi_e"] * np.exp(-p["gamma"] * (r / p["re"] - 1.0))
+    return f, -p["beta"] / p["re"] * f, phi, -p["gamma"] / p["re"] * phi
+
+
+def write_johnson_setfl(path, p=JOHNSON_CU):
+    """The same Johnson EAM as a single-element setfl (eam/alloy) file: F(rho) and rho(r) on the
+    file grids, then r * phi(r)."""
+    n = int(p["npts"])
+    dr = p["cutoff"] / n
+    drho = p["rho_max"] / n
+    r = np.arange(n) * dr
+    rho = np.arange(n) * drho
+    F = -p["Ec"] * np.sqrt(rho / p["rho_e"])
+    f, _, phi, _ = johnson_terms(r, p)
+    with open(path, "w") as fh:
+        fh.write("Johnson analytic EAM (Cu-like), generated\n\n\n")
+        fh.write("1 Cu\n")
+        fh.write(f"{n} {drho:.16e} {n} {dr:.16e} {p['cutoff']:.6f}\n")
+        fh.write(f"29 {p['mass']:.3f} {p['a']:.4f} fcc\n")
+        for arr in (F, f, r * phi):
+            for k in range(0, n, 5):
+                fh.write(" ".join(f"{v:.16e}" for v in arr[k:k + 5]) + "\n")
+    return path
+
+
 def eam_config(potential_file, cutoff=5.0, dt=1.0, precision="fp32"):
     return {
         "init_configuration": {"read_data": {"unit": "METAL", "atom_style": "atomic", "velocity_type": "GAUSS"}},

@@ -107,7 +107,9 @@ RBMD_API rbmd_status rbmd_force_set_pair_coeffs(rbmd_force* f, int32_t n_types, 
 /* EAM: read a funcfl potential file and build the 7-coefficient splines exactly as
  * ExecutionNVT::ReadPotentialFile/file2array/array2spline do
  * (rbmd/framework/run/ExecutionNVT.cpp:903-1107).  Called by create when
- * force_field.potential_file is set; callable directly to load another file. */
+ * force_field.potential_file is set; callable directly to load another file.  A file named
+ * *.alloy or *.setfl (or force_field.potential_format "setfl") is read as a single-element setfl
+ * file instead (tables on the file grids, r*phi given directly; the reference reads funcfl only). */
 RBMD_API rbmd_status rbmd_force_load_funcfl(rbmd_force* f, const char* path);
 
 /* Water topology for CVFF: n_mol (H,O,H) angle triples, 0-based caller atom ids, the

@@ -66,3 +66,17 @@ def test_reference_example_inputs():
         text = open(os.path.join(REF, cfg), encoding="utf-8-sig").read()
         ff = c.ForceField(text, c.Box((0.0, 0.0, 0.0), (30.0, 30.0, 30.0)))
         ff.close()
+
+
+def test_setfl_and_funcfl_files_load(tmp_path):
+    """EAM potential files: funcfl (the reference's format) and single-element setfl are read
+    when the handle is created (no device needed); a truncated file is rejected."""
+    pf = systems.write_johnson_funcfl(str(tmp_path / "j.eam"))
+    ps = systems.write_johnson_setfl(str(tmp_path / "j.eam.alloy"))
+    box = c.Box((0.0, 0.0, 0.0), (20.0, 20.0, 20.0))
+    for path in (pf, ps):
+        c.ForceField(systems.eam_config(path), box).close()
+    bad = tmp_path / "bad.eam.alloy"
+    bad.write_text("".join(open(ps).readlines()[:9]))
+    with pytest.raises(c.RbmdError, match="ERR_FILE"):
+        c.ForceField(systems.eam_config(str(bad)), box)

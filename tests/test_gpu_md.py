@@ -195,6 +195,42 @@ def test_eam_johnson(cuda, oracle_lib, tmp_path, prec):
     assert err < (1e-5 if prec == "fp32" else 1e-11), err
 
 
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_eam_setfl_matches_analytic_johnson(cuda, tmp_path, prec):
+    """A single-element setfl file of Johnson's EAM (tables on the file grid, r*phi given
+    directly) reproduces the analytic forces F_i = -sum_j [(F'(rho_i) + F'(rho_j)) f'(r) + phi'(r)]
+    (r_i - r_j) / r, FP64 in numpy over all minimum-image pairs within the cutoff.  The spline
+    tables are float (as the reference's): their derivative coefficients carry rounding of about
+    4e-5 relative (a difference of values divided by dr = 1e-3), which the near-cancelling pair
+    terms of a crystal amplify to 4e-4 of the rms force, in FP32 and FP64 runs alike; the bar is
+    1e-3.  A table offset by one grid point (the funcfl reader's quirk) would give 8e-3."""
+    import torch
+    p = systems.JOHNSON_CU
+    path = systems.write_johnson_setfl(str(tmp_path / "johnson.eam.alloy"), p)
+    s = systems.eam_fcc(ncell=6, seed=8)
+    cfg = systems.eam_config(path, precision=prec)
+    dev = to_dev(s, cuda)
+    ff = make_ff(cfg, s, dev)
+    ff.Execute()
+    torch.cuda.synchronize()
+    assert ff.status() == 0
+    got = dev["force"].cpu().numpy()
+    x = s["pos"]
+    L = s["hi"] - s["lo"]
+    d = x[:, None, :] - x[None, :, :]            # r_i - r_j
+    d -= L * np.round(d / L)
+    r = np.sqrt((d ** 2).sum(-1))
+    inside = (r < p["cutoff"]) & (r > 0.1)
+    rs = np.where(inside, r, 1.0)
+    f, fp, phi, phip = systems.johnson_terms(rs, p)
+    rho = np.where(inside, f, 0.0).sum(1)
+    Fp = -p["Ec"] / (2.0 * np.sqrt(rho * p["rho_e"]))
+    coef = np.where(inside, (Fp[:, None] + Fp[None, :]) * fp + phip, 0.0) / rs
+    ref = -(coef[:, :, None] * d).sum(1)
+    err = rel_err(got, ref)
+    assert err < 1e-3, err
+
+
 def test_batched_replicas_match_single(cuda):
     """Replica 0 advanced inside a batch equals replica 0 advanced alone (its sampler stream is
     keyed by replica index 0 in both runs)."""
