@@ -5,7 +5,7 @@
 //
 // Every routine is templated on Real: Real=float reproduces the reference's FP32 semantics
 // (rbmd/framework/Types.h:48, Real = vtkm::FloatDefault = float; mixed float/double literals are
-// kept as the reference writes them), Real=double is the FP64 judge.  Build with
+// kept as the reference writes them), Real=double is the FP64 reference answer.  Build with
 // -ffp-contract=off so that products and sums round exactly as written.
 //
 // Parity status: the reference cannot be built here (VTK-m 1.9 is not vendored), so outputs are
