@@ -313,6 +313,10 @@ def roofline(run, n, nq, P, steps, dev):
         roof["traffic"] = NEAR_TRAFFIC_BYTES_PER_ATOM * n
         roof["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the 200,000-atom "
                                   "launch (summary committed under profiles/) scaled by atoms")
+        # what limits the kernel instead of HBM (same ncu capture): instruction issue
+        roof["limiter"] = {"what": "instruction issue and dependent-latency waits in the pair arithmetic",
+                           "smsp__issue_active_pct": 66.7, "sm__throughput_pct": 57.1,
+                           "gpu__dram_throughput_pct": 8.6}
     return roof, rl, mufu_peak
 
 

@@ -53,6 +53,37 @@ def test_lj_nve_trajectory_fp64(cuda, oracle_lib):
     assert np.abs(dev["vel"].cpu().numpy() - v).max() < 1e-8
 
 
+def test_lj_nve_energy_conservation_fp64(cuda):
+    """FP64 LJ (4000 atoms from FCC at rho 0.8442, T 0.72, rc 4.0 + skin 0.3, list reuse,
+    CUDA-graph steps): after 200 steps of melting, 2000 NVE steps of dt = 0.005 keep the total
+    energy (kinetic + LJ) within 2e-4 of its value.  The reference's LJ is truncated without a
+    shift, so the energy jumps by 4 (rc^-12 - rc^-6) = -1e-3 whenever a pair crosses rc; at
+    rc = 4.0 that noise stays well inside the bar, which therefore tests the integrator and the
+    list reuse."""
+    import torch
+    s = systems.lj_fcc(ncell=10, seed=4)
+    cfg = systems.lj_config(cutoff=4.0, precision="fp64", ensemble="NVE")
+    cfg["hyper_parameters"]["neighbor"]["skin"] = 0.3
+    dev = to_dev(s, cuda)
+    ff = make_ff(cfg, s, dev)
+    ff.Execute()
+    ff.step(200)
+    torch.cuda.synchronize()
+
+    def total():
+        ff.Execute()
+        e = ff.energy()
+        return e["kinetic"] + e["lj"]
+
+    e0 = total()
+    for _ in range(4):
+        ff.step(500)
+        torch.cuda.synchronize()
+        assert ff.status() == 0
+        e = total()
+        assert abs(e - e0) <= 2e-4 * abs(e0), (e, e0)
+
+
 def test_skin_list_reuse_same_forces(cuda, oracle_lib):
     """Skin 0.3: the list is rebuilt only when an atom moved more than skin/2, and the forces of
     every step equal a fresh evaluation at the same positions (pairs within rc are unchanged).
