@@ -114,6 +114,49 @@ __global__ void k_skin_check(int n, const double* __restrict__ pos, const double
   }
 }
 
+// Langevin thermostat force (ExecutionNVT::TempConTypeForce, rbmd/framework/run/ExecutionNVT.cpp:
+// 735-747, UnderdampedLangevinWorklet, rbmd/framework/run/worklet/RunWorklet.cpp:1700-1728):
+// F += -m gamma v + sqrt(2 m gamma kBT / dt) xi, added to the total force before the kicks.
+// Default (physical): xi per atom and step, standard normal from Philox keyed by (seed, step,
+// atom), m the atom's mass and kBT = kB T0, with the unit factors of the kick (force * fmt2v / m
+// is an acceleration, m v^2 mvv2e an energy).  shared (the reference's form, compat): m = 1,
+// kBT = 1 and one xi vector for all atoms and steps.
+struct LangevinParams {
+  int n, shared;
+  double gamma, dt, kBT, fmt2v, mvv2e;
+  double xi[3];
+  unsigned long long seed;
+};
+
+__global__ void k_langevin(LangevinParams lp, const double* __restrict__ vel, const double* __restrict__ mass,
+                           const long long* __restrict__ step, double* __restrict__ force) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= lp.n) return;
+  double xi[3] = {lp.xi[0], lp.xi[1], lp.xi[2]};
+  double m = 1.0, conv = 1.0, amp;
+  if (lp.shared) {
+    amp = sqrt(2.0 * lp.gamma * lp.kBT / lp.dt);
+  } else {
+    m = mass ? mass[i] : 1.0;
+    conv = 1.0 / lp.fmt2v;   // force = (m / fmt2v) * acceleration
+    amp = m * conv * sqrt(2.0 * lp.gamma * lp.kBT / (m * lp.mvv2e * lp.dt));
+    const unsigned long long st = (unsigned long long)*step;
+    uint32_t c[4] = {(uint32_t)i, 0x4c414e47u, (uint32_t)st, (uint32_t)(st >> 32)};
+    philox4x32(c, (uint32_t)lp.seed, (uint32_t)(lp.seed >> 32));
+    // Box-Muller on three of the four words (plus one more from a second counter)
+    const double u1 = ((double)c[0] + 0.5) * (1.0 / 4294967296.0);
+    const double u2 = ((double)c[1] + 0.5) * (1.0 / 4294967296.0);
+    const double u3 = ((double)c[2] + 0.5) * (1.0 / 4294967296.0);
+    const double u4 = ((double)c[3] + 0.5) * (1.0 / 4294967296.0);
+    const double r1 = sqrt(-2.0 * log(u1)), r2 = sqrt(-2.0 * log(u3));
+    xi[0] = r1 * cos(2.0 * 3.14159265358979323846 * u2);
+    xi[1] = r1 * sin(2.0 * 3.14159265358979323846 * u2);
+    xi[2] = r2 * cos(2.0 * 3.14159265358979323846 * u4);
+  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) force[3 * i + d] += -m * conv * lp.gamma * vel[3 * i + d] + amp * xi[d];
+}
+
 // Advance the device step counter the k-samplers read (end of a step's k-space chain).
 __global__ void k_step_inc(long long* step) { *step += 1; }
 

@@ -222,6 +222,10 @@ struct rbmd_force {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   long long step_count = 0;
   long long* d_step = nullptr;   // step index of the k-samplers on the device (graph replay)
+  long long* d_lstep = nullptr;  // Langevin noise counter (advanced after every application)
+  double langevin_gamma = 100.0; // execution.langevin_gamma (the reference hard-codes 100)
+  bool langevin_shared = false;  // compat.langevin_reference: m = 1, kBT = 1, one xi for all
+  double langevin_xi[3] = {0, 0, 0};
   bool in_step = false;          // launches belong to rbmd_force_step (advance d_step)
   bool use_graph = true;         // execution.cuda_graph: replay a captured step
   cudaGraphExec_t graph_exec = nullptr;
@@ -326,7 +330,7 @@ void free_all(rbmd_force* f) {
   if (f->d_fp) cudaFree(f->d_fp);
   f->d_fp = nullptr;
   dfree(f->d_emb); dfree(f->d_epair); dfree(f->d_hoh); dfree(f->d_ebond); dfree(f->d_eangle);
-  dfree(f->d_snap); dfree(f->d_snap_img); dfree(f->d_step);
+  dfree(f->d_snap); dfree(f->d_snap_img); dfree(f->d_step); dfree(f->d_lstep);
   if (f->graph_exec) cudaGraphExecDestroy(f->graph_exec);
   f->graph_exec = nullptr;
   if (f->gstream) cudaStreamDestroy(f->gstream);
@@ -988,6 +992,21 @@ void launch_force_tail(rbmd_force* f, cudaStream_t s, bool bin, bool regather) {
       f->launches++;
     }
   }
+  if (f->tstat == 4 && f->at.vel) {   // Langevin force on top of the total force
+    LangevinParams lp;
+    lp.n = f->n;
+    lp.shared = f->langevin_shared ? 1 : 0;
+    lp.gamma = f->langevin_gamma;
+    lp.dt = f->dt;
+    lp.kBT = f->langevin_shared ? 1.0 : f->u.kB * f->T0;
+    lp.fmt2v = f->u.fmt2v;
+    lp.mvv2e = f->u.mvv2e;
+    for (int d = 0; d < 3; ++d) lp.xi[d] = f->langevin_xi[d];
+    lp.seed = f->seed ^ 0x4c616e676576696eull;
+    k_langevin<<<(f->n + 255) / 256, 256, 0, s>>>(lp, f->at.vel, f->at.mass, f->d_lstep, f->at.force);
+    k_step_inc<<<1, 1, 0, s>>>(f->d_lstep);
+    f->launches += 2;
+  }
 }
 
 template <class R>
@@ -1275,6 +1294,16 @@ rbmd_status parse_config(rbmd_force* f, const char* text) {
     if (f->tctrl == "BERENDSEN") f->tstat = 1;
     else if (f->tctrl == "TEMP_RESCALE") f->tstat = 2;
     else if (f->tctrl == "NOSE_HOOVER") f->tstat = 3;
+    else if (f->tctrl == "LANGEVIN") f->tstat = 4;
+  }
+  f->langevin_gamma = num(root, "execution.langevin_gamma", 100.0);
+  {
+    const Value* lr = root.path("compat.langevin_reference");
+    f->langevin_shared = lr && lr->kind == Value::Bool && lr->b;
+    // the reference draws its single noise vector once per run (ExecutionNVT.cpp:346-352)
+    std::mt19937_64 rng(f->seed * 0x9E3779B97F4A7C15ull + 29);
+    std::normal_distribution<double> nd(0.0, 1.0);
+    for (int d = 0; d < 3; ++d) f->langevin_xi[d] = nd(rng);
   }
   if (f->init_way == "inbuild") f->dof_mode = 3;
   else if (f->shake == "true") f->dof_mode = 1;
@@ -1652,6 +1681,8 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
   CK(cudaMemset(f->d_status, 0, sizeof(uint32_t)));
   CK(dalloc(&f->d_step, 1));
   CK(cudaMemset(f->d_step, 0, sizeof(long long)));
+  CK(dalloc(&f->d_lstep, 1));
+  CK(cudaMemset(f->d_lstep, 0, sizeof(long long)));
   CK(dalloc(&f->d_eslot, 2 * n));
   CK(cudaMemset(f->d_eslot, 0, sizeof(double) * 2 * n));
   CK(dalloc(&f->d_esum, 32));
