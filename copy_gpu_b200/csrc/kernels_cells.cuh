@@ -313,6 +313,10 @@ __global__ void k_regather(int n, const int* __restrict__ slot_atom, const doubl
 // literal 0.0001; for float x, (double)x > 1e-4 <=> x > 1e-4f (1e-4f < 1e-4 < nextafterf(1e-4f)).
 __device__ __forceinline__ bool gt_small(float x) { return x > 1.0e-4f; }
 __device__ __forceinline__ bool gt_small(double x) { return x > 1.0e-4; }
+// cut2 - d2 of a candidate: the list keeps it above 1e-4 (ComputeNeighboursWorklet); the
+// "ORIGINAL" neighbour type, which leaves the cutoff to the force function, keeps d2 < cut2
+template <class R>
+__device__ __forceinline__ bool inside_cut(R margin, int orig) { return orig ? margin > (R)0 : gt_small(margin); }
 
 // Full Verlet list of slot i with the predicate of ComputeNeighboursWorklet
 // (rbmd/framework/run/worklet/RunWorklet.cpp:40-96): rc^2 - d^2 > 1e-4 && d^2 > 1e-4 on
@@ -324,7 +328,7 @@ __device__ __forceinline__ bool gt_small(double x) { return x > 1.0e-4; }
 template <class R>
 __device__ __forceinline__ int nlist_range(int s, const int s1, const typename Traits<R>::V4* __restrict__ pos4,
                                            const R* pix, const R* off, int code, R cut2, int idx, int cap,
-                                           int stride, int i, int* __restrict__ nbr) {
+                                           int stride, int i, int* __restrict__ nbr, int orig) {
 #pragma unroll 4
   for (; s < s1; ++s) {
     const typename Traits<R>::V4 pj = pos4[s];
@@ -332,7 +336,7 @@ __device__ __forceinline__ int nlist_range(int s, const int s1, const typename T
     const R r1 = sub_rn(sub_rn(pj.y, off[1]), pix[1]);
     const R r2 = sub_rn(sub_rn(pj.z, off[2]), pix[2]);
     const R d2 = add_rn(add_rn(mul_rn(r0, r0), mul_rn(r1, r1)), mul_rn(r2, r2));
-    if (gt_small(sub_rn(cut2, d2)) && gt_small(d2)) {
+    if (inside_cut(sub_rn(cut2, d2), orig) && gt_small(d2)) {
       if (idx < cap) nbr[(size_t)idx * stride + i] = (s << kShiftBits) | code;
       ++idx;
     }
@@ -360,7 +364,7 @@ template <class R>
 __device__ int nlist_thread(int i, const typename Traits<R>::V4 pi, const RepDev& rp,
                             const typename Traits<R>::V4* __restrict__ pos4,
                             const int* __restrict__ cell_start, int num_cycles, R rc, int cap, int stride,
-                            int* __restrict__ nbr, bool trim_x = false) {
+                            int* __restrict__ nbr, bool trim_x = false, int orig = 0) {
   const R pix[3] = {pi.x, pi.y, pi.z};
   const R xm = rc + (fabs(pix[0]) + (R)2 * rc) * (R)1e-5 + (R)1e-6;   // cutoff + margin in x
   int ci[3];
@@ -389,7 +393,7 @@ __device__ int nlist_thread(int i, const typename Traits<R>::V4 pi, const RepDev
           s0 = lower_x<R>(pos4, s0, s1, pix[0] - xm);
           s1 = lower_x<R>(pos4, s0, s1, pix[0] + xm);
         }
-        idx = nlist_range<R>(s0, s1, pos4, pix, off, code_yz, cut2, idx, cap, stride, i, nbr);
+        idx = nlist_range<R>(s0, s1, pos4, pix, off, code_yz, cut2, idx, cap, stride, i, nbr, orig);
       } else {
         for (int a = -nc; a <= nc; ++a) {
           const int nbx = ci[0] + a;
@@ -403,7 +407,7 @@ __device__ int nlist_thread(int i, const typename Traits<R>::V4 pi, const RepDev
             s0 = lower_x<R>(pos4, s0, s1, pix[0] + off[0] - xw);
             s1 = lower_x<R>(pos4, s0, s1, pix[0] + off[0] + xw);
           }
-          idx = nlist_range<R>(s0, s1, pos4, pix, off, code, cut2, idx, cap, stride, i, nbr);
+          idx = nlist_range<R>(s0, s1, pos4, pix, off, code, cut2, idx, cap, stride, i, nbr, orig);
         }
       }
     }
@@ -425,7 +429,7 @@ __global__ void __launch_bounds__(256) k_nlist(
     const RepDev* __restrict__ reps, const int* __restrict__ rep_of_slot, int num_cycles, R rc,
     int cap, int stride, int* __restrict__ nbr, int* __restrict__ count, int* __restrict__ max_count,
     uint32_t* status, const int* __restrict__ rebuild, unsigned long long* __restrict__ nbuilds,
-    int trim_x, int n_rep) {
+    int trim_x, int n_rep, int orig) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0 && nbuilds) atomicAdd(nbuilds, rebuilt_replicas(rebuild, n_rep));
   if (i >= n) return;
@@ -433,7 +437,7 @@ __global__ void __launch_bounds__(256) k_nlist(
   if (rebuild && !rebuild[r]) return;
   const RepDev& rp = reps[r];
   const int idx = nlist_thread<R>(i, pos4[i], rp, pos4, cell_start, num_cycles, rc, cap, stride, nbr,
-                                  trim_x != 0);
+                                  trim_x != 0, orig);
   nlist_finish(i, idx, cap, count, max_count, status);
 }
 
@@ -445,7 +449,7 @@ __global__ void __launch_bounds__(256) k_nlist_warp(
     int n, const typename Traits<R>::V4* __restrict__ pos4, const int* __restrict__ cell_start,
     const RepDev* __restrict__ reps, const int* __restrict__ rep_of_slot, R rc, int cap, int stride,
     int* __restrict__ nbr, int* __restrict__ count, int* __restrict__ max_count, uint32_t* status,
-    const int* __restrict__ rebuild, unsigned long long* __restrict__ nbuilds, int n_rep) {
+    const int* __restrict__ rebuild, unsigned long long* __restrict__ nbuilds, int n_rep, int orig) {
   using V4 = typename Traits<R>::V4;
   const int lane = threadIdx.x & 31;
   const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -477,7 +481,7 @@ __global__ void __launch_bounds__(256) k_nlist_warp(
         const R r1 = sub_rn(sub_rn(pj.y, o1), pix[1]);
         const R r2 = sub_rn(sub_rn(pj.z, o2), pix[2]);
         const R d2 = add_rn(add_rn(mul_rn(r0, r0), mul_rn(r1, r1)), mul_rn(r2, r2));
-        ok = gt_small(sub_rn(cut2, d2)) && gt_small(d2);
+        ok = inside_cut(sub_rn(cut2, d2), orig) && gt_small(d2);
       }
       const unsigned m = __ballot_sync(0xffffffffu, ok);
       if (ok) {
@@ -533,7 +537,8 @@ __global__ void __launch_bounds__(kStageThreads, 2) k_nlist_staged(
     const ListSeg* __restrict__ segs, int stage_cap, const typename Traits<R>::V4* __restrict__ pos4,
     const int* __restrict__ cell_start, const RepDev* __restrict__ reps, R rc, int cap, int stride,
     int* __restrict__ nbr, int* __restrict__ count, int* __restrict__ max_count, uint32_t* status,
-    const int* __restrict__ rebuild, unsigned long long* __restrict__ nbuilds, int trim_x, int n_rep) {
+    const int* __restrict__ rebuild, unsigned long long* __restrict__ nbuilds, int trim_x, int n_rep,
+    int orig) {
   using V4 = typename Traits<R>::V4;
   if (blockIdx.x == 0 && threadIdx.x == 0 && nbuilds) atomicAdd(nbuilds, rebuilt_replicas(rebuild, n_rep));
   if (rebuild && !rebuild[segs[blockIdx.x].rep]) return;
@@ -638,14 +643,14 @@ __global__ void __launch_bounds__(kStageThreads, 2) k_nlist_staged(
           const R r1 = sub_rn(q.y, pix[1]);
           const R r2 = sub_rn(q.z, pix[2]);
           const R dd = add_rn(add_rn(mul_rn(r0, r0), mul_rn(r1, r1)), mul_rn(r2, r2));
-          if (gt_small(sub_rn(cut2, dd)) && gt_small(dd)) {
+          if (inside_cut(sub_rn(cut2, dd), orig) && gt_small(dd)) {
             if (idx < cap) nbr[(size_t)idx * stride + i] = unpack_tag(q.w);
             ++idx;
           }
         }
       }
     } else {
-      idx = nlist_thread<R>(i, pi, rp, pos4, cell_start, 1, rc, cap, stride, nbr);
+      idx = nlist_thread<R>(i, pi, rp, pos4, cell_start, 1, rc, cap, stride, nbr, false, orig);
     }
     nlist_finish(i, idx, cap, count, max_count, status);
   }

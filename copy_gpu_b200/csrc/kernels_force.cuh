@@ -44,6 +44,7 @@ struct NearParams {
   double rc, alpha, coul_scale;   // coul_scale multiplies the erfc Coulomb pair force
   double sqrt_alpha, two_sqrt_alpha_over_sqrt_pi;
   int kstage;                     // records of shared memory available for k staging
+  int orig;                       // neighbour type "ORIGINAL": pairs with d^2 < rc^2 (no 1e-4 margin)
 };
 
 template <class R> struct KRec;
@@ -198,7 +199,7 @@ __global__ void __launch_bounds__(256) k_near_force(
     }
     const R r0 = px - pi.x, r1 = py - pi.y, r2 = pz - pi.z;
     const R d2 = r0 * r0 + r1 * r1 + r2 * r2;
-    if (MI == kMiAll && !(cut2 - d2 > (R)1.0e-4 && d2 > (R)1.0e-4)) continue;
+    if (MI == kMiAll && !((prm.orig ? cut2 - d2 > (R)0 : cut2 - d2 > (R)1.0e-4) && d2 > (R)1.0e-4)) continue;
     R f = 0;
     if (COUL) {
       const R qq = qi * pj.w;
@@ -317,7 +318,7 @@ __global__ void __launch_bounds__(256) k_near_force_group(
     }
     const R r0 = px - pi.x, r1 = py - pi.y, r2 = pz - pi.z;
     const R d2 = r0 * r0 + r1 * r1 + r2 * r2;
-    if (MI == kMiAll && !(cut2 - d2 > (R)1.0e-4 && d2 > (R)1.0e-4)) continue;
+    if (MI == kMiAll && !((prm.orig ? cut2 - d2 > (R)0 : cut2 - d2 > (R)1.0e-4) && d2 > (R)1.0e-4)) continue;
     R f = 0;
     if (COUL) {
       const R qq = qi * pj.w;

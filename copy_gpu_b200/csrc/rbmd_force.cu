@@ -181,7 +181,8 @@ struct rbmd_force {
   // RBE
   int Ptot = 0, nitems = 0, rho_threads = 64, ktile = 128, kstage = 0;
   bool minimg = true, want_energy = true;
-  bool kspace_priority = true;   // execution.kspace_priority: side stream at the highest priority
+  bool kspace_priority = true;
+  bool orig_pred = false;        // neighbor.type "ORIGINAL": pair predicate d^2 < rc^2   // execution.kspace_priority: side stream at the highest priority
   int* d_krep = nullptr;
   int nq = 0;               // charged atoms (the k-space path runs over these only)
   int* d_qidx = nullptr;
@@ -651,7 +652,7 @@ void launch_nlist(rbmd_force* f, cudaStream_t s) {
     k_nlist_staged<R><<<f->nsegs, kStageThreads, smem, s>>>(
         f->d_segs, f->stage_cap, (const typename Traits<R>::V4*)f->d_pos4, f->d_cell_start, f->d_reps,
         (R)f->list_cut(), f->cap, f->stride, f->d_nbr, f->d_count, f->d_maxcount, f->d_status,
-        f->skin > 0 ? f->d_rebuild : nullptr, f->d_nbuilds, f->sort_x() ? 1 : 0, f->nrep);
+        f->skin > 0 ? f->d_rebuild : nullptr, f->d_nbuilds, f->sort_x() ? 1 : 0, f->nrep, f->orig_pred ? 1 : 0);
     f->launches++;
     return;
   }
@@ -659,7 +660,8 @@ void launch_nlist(rbmd_force* f, cudaStream_t s) {
     k_nlist_warp<R><<<(f->n + 7) / 8, 256, 0, s>>>(
         f->n, (const typename Traits<R>::V4*)f->d_pos4, f->d_cell_start, f->d_reps,
         f->nrep > 1 ? f->d_rep_of : nullptr, (R)f->list_cut(), f->cap, f->stride, f->d_nbr, f->d_count,
-        f->d_maxcount, f->d_status, f->skin > 0 ? f->d_rebuild : nullptr, f->d_nbuilds, f->nrep);
+        f->d_maxcount, f->d_status, f->skin > 0 ? f->d_rebuild : nullptr, f->d_nbuilds, f->nrep,
+        f->orig_pred ? 1 : 0);
     f->launches++;
     return;
   }
@@ -668,7 +670,7 @@ void launch_nlist(rbmd_force* f, cudaStream_t s) {
       f->n, (const typename Traits<R>::V4*)f->d_pos4, f->d_cell_start, f->d_reps,
       f->nrep > 1 ? f->d_rep_of : nullptr, f->num_cycles, (R)f->list_cut(), f->cap, f->stride, f->d_nbr,
       f->d_count, f->d_maxcount, f->d_status, f->skin > 0 ? f->d_rebuild : nullptr, f->d_nbuilds,
-      f->sort_x() ? 1 : 0, f->nrep);
+      f->sort_x() ? 1 : 0, f->nrep, f->orig_pred ? 1 : 0);
   f->launches++;
 }
 
@@ -825,6 +827,7 @@ void launch_near_t(rbmd_force* f, cudaStream_t s) {
   p.sqrt_alpha = std::sqrt(f->alpha);
   p.two_sqrt_alpha_over_sqrt_pi = 2.0 * std::sqrt(f->alpha) / std::sqrt(M_PI);
   p.kstage = 0;
+  p.orig = f->orig_pred ? 1 : 0;
   if (f->near_lanes > 1) {
     const long long threads = (long long)f->n * f->near_lanes;
     const int grid = (int)((threads + 255) / 256);
@@ -1230,6 +1233,13 @@ rbmd_status parse_config(rbmd_force* f, const char* text) {
   f->potential_format = rbmdjson::text(root, "hyper_parameters.force_field.potential_format", "");
   f->nbr_type = rbmdjson::text(root, "hyper_parameters.neighbor.type", "VERLETLIST");
   if (f->nbr_type == "VERLET-LIST") f->nbr_type = "VERLETLIST";
+  // "ORIGINAL" walks the cells on the fly and leaves the cutoff to the force function
+  // (ExecPointLocator::ExecuteOnNeighbor): here a list built with the force function's
+  // predicate d^2 < rc^2 instead of the list's rc^2 - d^2 > 1e-4, otherwise a Verlet list
+  if (f->nbr_type == "ORIGINAL") {
+    f->orig_pred = true;
+    f->nbr_type = "VERLETLIST";
+  }
   bool found = false;
   f->rc = num(root, "hyper_parameters.neighbor.cut_off", 0.0, &found);
   if (!found || f->rc <= 0) {
@@ -1327,7 +1337,7 @@ rbmd_status parse_config(rbmd_force* f, const char* text) {
   }
   if (f->nbr_type != "VERLETLIST" && f->nbr_type != "RBL") {
     std::snprintf(g_last_error, sizeof g_last_error,
-                  "config: neighbor.type %s is not provided by this build (VERLETLIST, RBL)",
+                  "config: neighbor.type %s is not provided by this build (VERLETLIST, ORIGINAL, RBL)",
                   f->nbr_type.c_str());
     return RBMD_ERR_CONFIG;
   }

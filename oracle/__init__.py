@@ -52,8 +52,9 @@ def _real(prec):
     return (np.float32, F, "f32") if prec == "fp32" else (np.float64, D, "f64")
 
 
-def neighbors(pos, lo, hi, cutoff, prec="fp32", cap=None, rs=None):
-    """Full Verlet list (ComputeNeighboursWorklet semantics).  Returns counts, ids, codes."""
+def neighbors(pos, lo, hi, cutoff, prec="fp32", cap=None, rs=None, original=False):
+    """Full Verlet list (ComputeNeighboursWorklet semantics; original=True: the pairs the
+    "ORIGINAL" neighbour type visits, d^2 < rc^2).  Returns counts, ids, codes."""
     dt, ct, sfx = _real(prec)
     x = np.ascontiguousarray(pos, dtype=dt)
     n = x.shape[0]
@@ -70,7 +71,7 @@ def neighbors(pos, lo, hi, cutoff, prec="fp32", cap=None, rs=None):
         dims = np.zeros(3, np.int32)
         rc = getattr(lib(), "oracle_neighbors_" + sfx)(
             ctypes.c_int64(n), _p(x, ct), _p(lo, D), _p(hi, D), D(cutoff), D(rs), ctypes.c_int64(cap),
-            _p(counts, I32), _p(ids, I32), _p(codes, I32), _p(dims, I32))
+            _p(counts, I32), _p(ids, I32), _p(codes, I32), _p(dims, I32), int(original))
         if rc == 0:
             return counts, ids, codes
         cap = int(counts.max()) + 8

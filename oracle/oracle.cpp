@@ -139,8 +139,14 @@ Cells<Real> build_cells(const Grid<Real>& g, int64_t n, const Real* pos) {
 // 0 = no wrap, 1 = cell index wrapped upward (offset +dims), 2 = wrapped downward (-dims).
 // ------------------------------------------------------------------------------------------
 template <class Real>
+// orig: the neighbour type "ORIGINAL" walks the same 27 cells on the fly
+// (ExecPointLocator::ExecuteOnNeighbor, rbmd/framework/locator/ExecPointLocator.h:99-124) and
+// leaves the cutoff to the force function (dis_2 < cut_off_2 && dis_2 > 0.0001,
+// rbmd/framework/forceFunction/ExecForceFunction.h:74-96): the same pairs as the list but for
+// the thin shell rc^2 - 1e-4 <= d^2 < rc^2, which the list predicate drops.
 void neighbor_list(const Grid<Real>& g, const Cells<Real>& c, int64_t n, const Real* pos,
-                   double cutoff, int64_t cap, int32_t* counts, int32_t* ids, int32_t* codes) {
+                   double cutoff, int64_t cap, int32_t* counts, int32_t* ids, int32_t* codes,
+                   int orig = 0) {
   const Real rc = (Real)cutoff;
   const int nc = g.num_cycles;
 #pragma omp parallel for schedule(dynamic, 64)
@@ -172,7 +178,8 @@ void neighbor_list(const Grid<Real>& g, const Cells<Real>& c, int64_t n, const R
             Real r2 = (pj[2] - off[2]) - pi[2];
             const Real dis_2 = r0 * r0 + r1 * r1 + r2 * r2;
             const Real cut_2 = rc * rc;
-            if ((double)(cut_2 - dis_2) > 0.0001 && (double)dis_2 > 0.0001) {
+            const bool inside = orig ? dis_2 < cut_2 : (double)(cut_2 - dis_2) > 0.0001;
+            if (inside && (double)dis_2 > 0.0001) {
               if (index < cap) {
                 ids[a * cap + index] = jd;
                 if (codes) codes[a * cap + index] = code;
@@ -380,10 +387,10 @@ Real compute_S(Real alpha, const Real* box) {
 template <class Real>
 static int neighbors_impl(int64_t n, const Real* pos, const double* lo, const double* hi,
                           double cutoff, double rs, int64_t cap, int32_t* counts, int32_t* ids,
-                          int32_t* codes, int32_t* dims_out) {
+                          int32_t* codes, int32_t* dims_out, int orig) {
   Grid<Real> g = make_grid<Real>(lo, hi, cutoff, rs);
   Cells<Real> c = build_cells(g, n, pos);
-  neighbor_list(g, c, n, pos, cutoff, cap, counts, ids, codes);
+  neighbor_list(g, c, n, pos, cutoff, cap, counts, ids, codes, orig);
   if (dims_out) for (int d = 0; d < 3; ++d) dims_out[d] = g.dims[d];
   int64_t mx = 0;
   for (int64_t i = 0; i < n; ++i) mx = std::max<int64_t>(mx, counts[i]);
@@ -392,13 +399,13 @@ static int neighbors_impl(int64_t n, const Real* pos, const double* lo, const do
 
 EXPORT int oracle_neighbors_f32(int64_t n, const float* pos, const double* lo, const double* hi,
                                 double cutoff, double rs, int64_t cap, int32_t* counts,
-                                int32_t* ids, int32_t* codes, int32_t* dims) {
-  return neighbors_impl<float>(n, pos, lo, hi, cutoff, rs, cap, counts, ids, codes, dims);
+                                int32_t* ids, int32_t* codes, int32_t* dims, int orig) {
+  return neighbors_impl<float>(n, pos, lo, hi, cutoff, rs, cap, counts, ids, codes, dims, orig);
 }
 EXPORT int oracle_neighbors_f64(int64_t n, const double* pos, const double* lo, const double* hi,
                                 double cutoff, double rs, int64_t cap, int32_t* counts,
-                                int32_t* ids, int32_t* codes, int32_t* dims) {
-  return neighbors_impl<double>(n, pos, lo, hi, cutoff, rs, cap, counts, ids, codes, dims);
+                                int32_t* ids, int32_t* codes, int32_t* dims, int orig) {
+  return neighbors_impl<double>(n, pos, lo, hi, cutoff, rs, cap, counts, ids, codes, dims, orig);
 }
 
 EXPORT void oracle_cells_f32(int64_t n, const float* pos, const double* lo, const double* hi,

@@ -264,3 +264,37 @@ def test_force_lanes_parity(cuda, oracle_lib, lanes):
     rho = oracle_lib.rhok(se["pos"], se["charge"], L, m)
     far = oracle_lib.rbe_force(se["pos"], se["charge"], L, alpha, 1.0, m, rho)
     assert rel_err(dev["force"].cpu().numpy(), near + far) <= TOL["fp32"]
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_original_neighbor_type(cuda, oracle_lib, prec):
+    """neighbor.type "ORIGINAL" (cells walked on the fly, cutoff left to the force function,
+    ExecPointLocator::ExecuteOnNeighbor): the pair set is d^2 < rc^2 instead of the list's
+    rc^2 - d^2 > 1e-4, so a pair at d^2 = rc^2 - 5e-5 is met by ORIGINAL only; pair sets and LJ
+    forces match the oracle in both modes."""
+    import torch
+    rng = np.random.default_rng(9)
+    L = 9.0
+    pos = rng.uniform(0.5, L - 0.5, size=(400, 3))
+    pos[1] = pos[0] + np.array([np.sqrt(2.5 ** 2 - 5e-5), 0.0, 0.0])
+    pos[1] = np.mod(pos[1], L)
+    s = dict(pos=pos, vel=np.zeros_like(pos), mass=np.ones(400), charge=np.zeros(400),
+             type=np.zeros(400, np.int32), molecule=None, lo=np.zeros(3), hi=np.full(3, L),
+             eps=np.ones(1), sigma=np.ones(1))
+    pr = _posr(pos, prec)
+    counts = {}
+    for orig in (False, True):
+        cfg = systems.lj_config(cutoff=2.5, precision=prec)
+        cfg["hyper_parameters"]["neighbor"]["type"] = "ORIGINAL" if orig else "VERLETLIST"
+        dev = to_dev(s, cuda)
+        ff = make_ff(cfg, s, dev)
+        ff.Execute()
+        torch.cuda.synchronize()
+        c, ids = ff.neighbors(256)
+        nl = oracle_lib.neighbors(pr, s["lo"], s["hi"], 2.5, prec, original=orig)
+        assert pair_sets_equal(c, ids, nl[0], nl[1]) == -1
+        ref = oracle_lib.near_force(pr, s["lo"], s["hi"], 2.5, nl, prec=prec, sum_mode=1)
+        assert rel_err(dev["force"].cpu().numpy(), ref) <= TOL[prec]
+        counts[orig] = (int(c[0]), 1 in set(ids[0, :c[0]].tolist()))
+    assert counts[True][1] and not counts[False][1], counts
+    assert counts[True][0] == counts[False][0] + 1, counts
