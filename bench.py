@@ -58,6 +58,8 @@ def parse():
                     "instead of replaying the captured step graph")
     ap.add_argument("--noise-steps", type=int, default=16,
                     help="k-sets per proposal for the force-RMSE measurement")
+    ap.add_argument("--ion-frac", type=float, default=0.1,
+                    help="fraction of charged atoms of the electrolyte (0.1 is the headline workload)")
     ap.add_argument("--workload", default="electrolyte",
                     choices=["electrolyte", "lj", "water", "eam", "batched"],
                     help="electrolyte: the headline metric (default); the others time the remaining "
@@ -333,7 +335,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    s = systems.electrolyte(args.atoms, seed=3 + rank)
+    s = systems.electrolyte(args.atoms, ion_frac=args.ion_frac, seed=3 + rank)
     n = s["pos"].shape[0]
     nq = int((s["charge"] != 0).sum())
     P0 = args.P
@@ -395,7 +397,9 @@ def run_ours(args):
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": f"electrolyte {n} atoms, full MD step, learned k-proposal at P={P_eq} "
+            "config": {"workload": f"electrolyte {n} atoms"
+                                   + ("" if args.ion_frac == 0.1 else f" ({args.ion_frac:g} charged)")
+                                   + f", full MD step, learned k-proposal at P={P_eq} "
                                    f"(equal k-space force RMSE to plain Gaussian RBE at P={P0})",
                        "atoms_per_gpu": n, "P": P_eq, "P_plain": P0, "proposal": "learned", "rc": 2.5,
                        "skin": args.skin, "list_builds_per_step": learned["builds"] / args.steps,
