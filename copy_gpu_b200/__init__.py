@@ -35,7 +35,7 @@ FLAG_SHAKE_SINGULAR = 0x40
 # every symbol include/rbmd_force.h declares
 EXPORTED = [
     "rbmd_force_create", "rbmd_force_set_pair_coeffs", "rbmd_force_load_funcfl",
-    "rbmd_force_set_water", "rbmd_force_bind", "rbmd_force_set_ksamples",
+    "rbmd_force_set_water", "rbmd_force_set_topology", "rbmd_force_bind", "rbmd_force_set_ksamples",
     "rbmd_force_set_kweights", "rbmd_force_get_ksamples", "rbmd_force_sample_k",
     "rbmd_force_compute", "rbmd_force_autotune", "rbmd_force_compute_host", "rbmd_force_step",
     "rbmd_force_sync_velocities", "rbmd_force_energy", "rbmd_force_status",
@@ -43,7 +43,8 @@ EXPORTED = [
     "rbmd_force_phase_ms", "rbmd_force_list_builds", "rbmd_force_launch_count",
     "rbmd_force_train_proposal", "rbmd_force_proposal_params", "rbmd_force_get_far",
     "rbmd_force_destroy", "rbmd_rhok_noalloc", "rbmd_proposal_mlp_eval", "rbmd_data_read",
-    "rbmd_data_atoms", "rbmd_data_types", "rbmd_data_topology", "rbmd_data_free", "rbmd_data_write",
+    "rbmd_data_atoms", "rbmd_data_types", "rbmd_data_topology", "rbmd_data_dihedrals", "rbmd_data_free",
+    "rbmd_data_write",
     "rbmd_version",
     "rbmd_last_error",
 ]
@@ -76,14 +77,24 @@ class rbmd_atoms_dev(ctypes.Structure):
 class rbmd_energy(ctypes.Structure):
     _fields_ = [(k, ctypes.c_double) for k in (
         "lj", "coul_real", "coul_kspace", "coul_self", "eam_embed", "eam_pair", "bond", "angle",
-        "kinetic", "temperature")]
+        "kinetic", "temperature", "dihedral", "coul_special")]
 
 
 class rbmd_data_info(ctypes.Structure):
     _fields_ = [("n_atoms", ctypes.c_int64), ("n_bonds", ctypes.c_int64), ("n_angles", ctypes.c_int64),
                 ("n_atom_types", ctypes.c_int32), ("n_bond_types", ctypes.c_int32), ("n_angle_types", ctypes.c_int32),
                 ("has_velocities", ctypes.c_int32), ("has_pair_coeffs", ctypes.c_int32), ("has_masses", ctypes.c_int32),
-                ("box", rbmd_box)]
+                ("box", rbmd_box), ("n_dihedrals", ctypes.c_int64), ("n_dihedral_types", ctypes.c_int32)]
+
+
+class rbmd_topology(ctypes.Structure):
+    _fields_ = [("n_atoms", ctypes.c_int64), ("molecule", ctypes.c_void_p),
+                ("n_bonds", ctypes.c_int64), ("bonds", ctypes.c_void_p), ("bond_type", ctypes.c_void_p),
+                ("n_bond_types", ctypes.c_int32), ("bond_coeffs", ctypes.c_void_p),
+                ("n_angles", ctypes.c_int64), ("angles", ctypes.c_void_p), ("angle_type", ctypes.c_void_p),
+                ("n_angle_types", ctypes.c_int32), ("angle_coeffs", ctypes.c_void_p),
+                ("n_dihedrals", ctypes.c_int64), ("dihedrals", ctypes.c_void_p), ("dihedral_type", ctypes.c_void_p),
+                ("n_dihedral_types", ctypes.c_int32), ("dihedral_coeffs", ctypes.c_void_p)]
 
 
 class rbmd_train_opts(ctypes.Structure):
@@ -114,6 +125,7 @@ def library() -> ctypes.CDLL:
         "rbmd_force_set_pair_coeffs": (I32, [V, I32, P(D), P(D)]),
         "rbmd_force_load_funcfl": (I32, [V, ctypes.c_char_p]),
         "rbmd_force_set_water": (I32, [V, I64, P(I32), D, D, D, D]),
+        "rbmd_force_set_topology": (I32, [V, P(rbmd_topology)]),
         "rbmd_force_bind": (I32, [V, P(rbmd_atoms_dev)]),
         "rbmd_force_set_ksamples": (I32, [V, P(I32), I32]),
         "rbmd_force_set_kweights": (I32, [V, P(D)]),
@@ -143,6 +155,7 @@ def library() -> ctypes.CDLL:
         "rbmd_data_atoms": (I32, [V, V, V, V, V, V, V, V]),
         "rbmd_data_types": (I32, [V, V, V, V]),
         "rbmd_data_topology": (I32, [V, V, V, V, V, V, V]),
+        "rbmd_data_dihedrals": (I32, [V, V, V, V]),
         "rbmd_data_free": (None, [V]),
         "rbmd_data_write": (I32, [ctypes.c_char_p, ctypes.c_char_p, P(rbmd_data_info), V, V, V, V, V, V, V, V, V,
                                   V, V]),
@@ -224,6 +237,23 @@ class ForceField:
         _check(library().rbmd_force_set_water(self._h, len(t) // 3, _ptr(t, ctypes.c_int32),
                                               float(bond_k), float(bond_r0), float(angle_k),
                                               float(angle_theta0_deg)), "set_water")
+
+    def set_topology(self, molecule, bonds=None, bond_type=None, bond_coeffs=None, angles=None, angle_type=None,
+                     angle_coeffs=None, dihedrals=None, dihedral_type=None, dihedral_coeffs=None):
+        """General CVFF topology (rbmd_force_set_topology): 0-based atom ids, per-type harmonic
+        coefficients bond (k, r0), angle (k, theta0 degrees), dihedral (K, sign, multiplicity)."""
+        import numpy as np
+        c = lambda a, t, w: np.zeros((0, w) if w else 0, t) if a is None else np.ascontiguousarray(a, t)  # noqa
+        mol = c(molecule, np.int32, 0)
+        b, bt, bc = c(bonds, np.int32, 2), c(bond_type, np.int32, 0), c(bond_coeffs, np.float64, 2)
+        a, at, ac = c(angles, np.int32, 3), c(angle_type, np.int32, 0), c(angle_coeffs, np.float64, 2)
+        d, dt, dc = c(dihedrals, np.int32, 4), c(dihedral_type, np.int32, 0), c(dihedral_coeffs, np.float64, 3)
+        keep = [mol, b, bt, bc, a, at, ac, d, dt, dc]
+        vp = lambda x: x.ctypes.data_as(ctypes.c_void_p) if x.size else None   # noqa: E731
+        t = rbmd_topology(len(mol), vp(mol), len(b), vp(b), vp(bt), len(bc), vp(bc), len(a), vp(a), vp(at),
+                          len(ac), vp(ac), len(d), vp(d), vp(dt), len(dc), vp(dc))
+        _check(library().rbmd_force_set_topology(self._h, ctypes.byref(t)), "set_topology")
+        del keep
 
     def Init(self, pos, force, *, vel=None, mass=None, charge=None, type=None, molecule=None,
              image=None, replica_offsets=None):
@@ -459,8 +489,16 @@ def read_data(path, atom_style, unit="LJ"):
         out["angles"] = np.zeros((info.n_angles, 3), np.int32)
         out["bond_coeffs"] = np.zeros((max(info.n_bond_types, 0), 2))
         out["angle_coeffs"] = np.zeros((max(info.n_angle_types, 0), 2))
-        _check(lib.rbmd_data_topology(h, dp(out["bonds"]), None, dp(out["angles"]), None, dp(out["bond_coeffs"]),
-                                      dp(out["angle_coeffs"])), "topology")
+        out["bond_type"] = np.zeros(info.n_bonds, np.int32)
+        out["angle_type"] = np.zeros(info.n_angles, np.int32)
+        _check(lib.rbmd_data_topology(h, dp(out["bonds"]), dp(out["bond_type"]), dp(out["angles"]),
+                                      dp(out["angle_type"]), dp(out["bond_coeffs"]), dp(out["angle_coeffs"])),
+               "topology")
+        out["dihedrals"] = np.zeros((info.n_dihedrals, 4), np.int32)
+        out["dihedral_type"] = np.zeros(info.n_dihedrals, np.int32)
+        out["dihedral_coeffs"] = np.zeros((max(info.n_dihedral_types, 0), 3))
+        _check(lib.rbmd_data_dihedrals(h, dp(out["dihedrals"]), dp(out["dihedral_type"]),
+                                       dp(out["dihedral_coeffs"])), "dihedrals")
         out["lo"] = np.array(info.box.lo[:])
         out["hi"] = np.array(info.box.hi[:])
         out["has_velocities"] = bool(info.has_velocities)

@@ -29,8 +29,8 @@ extern char g_last_error[512];
 struct rbmd_data {
   rbmd_data_info info{};
   std::string style;
-  std::vector<double> pos, vel, charge, mass_type, eps, sig, bond_k, bond_r0, angle_k, angle_t0;
-  std::vector<int32_t> type, mol, image, bonds, bond_type, angles, angle_type;
+  std::vector<double> pos, vel, charge, mass_type, eps, sig, bond_k, bond_r0, angle_k, angle_t0, dih_coeffs;
+  std::vector<int32_t> type, mol, image, bonds, bond_type, angles, angle_type, dihedrals, dihedral_type;
 };
 
 namespace {
@@ -94,13 +94,14 @@ RBMD_API rbmd_status rbmd_data_read(const char* path, const char* atom_style, co
     else if (l.find("atom types") != std::string::npos) ss >> h.n_atom_types;
     else if (l.find("bond types") != std::string::npos) ss >> h.n_bond_types;
     else if (l.find("angle types") != std::string::npos) ss >> h.n_angle_types;
-    else if (l.find("dihedral types") != std::string::npos) { }
+    else if (l.find("dihedral types") != std::string::npos) ss >> h.n_dihedral_types;
     else if (l.find("atoms") != std::string::npos) ss >> h.n_atoms;
     else if (l.find("bonds") != std::string::npos) ss >> h.n_bonds;
     else if (l.find("angles") != std::string::npos) ss >> h.n_angles;
     else if (l.find("dihedrals") != std::string::npos) ss >> n_dih;
   }
   for (int k = 0; k < 3; ++k) { h.box.lo[k] = lo[k]; h.box.hi[k] = hi[k]; }
+  h.n_dihedrals = n_dih;
   if (h.n_atoms < 1 || h.n_atom_types < 1 || !(hi[0] > lo[0] && hi[1] > lo[1] && hi[2] > lo[2])) {
     delete d;
     return fail("bad header in", path);
@@ -165,7 +166,19 @@ RBMD_API rbmd_status rbmd_data_read(const char* path, const char* atom_style, co
         d->angle_k[t - 1] = a;
         d->angle_t0[t - 1] = b;
       }
-    } else if (sec.find("Dihedral Coeffs") != std::string::npos || sec.find("group") != std::string::npos) {
+    } else if (sec.find("Dihedral Coeffs") != std::string::npos) {
+      // ModelFileInitCondition::DihedralsCoeffs (ModelFileInitCondition.cpp:359-380): type K d n
+      d->dih_coeffs.assign(3 * (size_t)std::max(h.n_dihedral_types, 0), 0.0);
+      for (int k = 0; k < h.n_dihedral_types; ++k) {
+        if (!next_line(lines, j, l)) return bad("short Dihedral Coeffs");
+        std::istringstream ss(l);
+        int t, sg, m; double kk;
+        if (!(ss >> t >> kk >> sg >> m) || t < 1 || t > h.n_dihedral_types) return bad("bad Dihedral Coeffs line");
+        d->dih_coeffs[3 * (t - 1)] = kk;
+        d->dih_coeffs[3 * (t - 1) + 1] = sg;
+        d->dih_coeffs[3 * (t - 1) + 2] = m;
+      }
+    } else if (sec.find("group") != std::string::npos) {
       j = i + 1;   // not used by the force path: the body is skipped as unknown lines
       continue;
     } else if (sec.find("Atoms") != std::string::npos) {
@@ -224,8 +237,21 @@ RBMD_API rbmd_status rbmd_data_read(const char* path, const char* atom_style, co
         d->angles[3 * k + 2] = (int32_t)(c - 1);
       }
     } else if (sec.find("Dihedrals") != std::string::npos) {
-      for (int64_t k = 0; k < n_dih; ++k)
+      // ModelFileInitCondition::Dihedrals (ModelFileInitCondition.cpp:551-585): id type i j k l
+      d->dihedrals.assign(4 * n_dih, 0);
+      d->dihedral_type.assign(n_dih, 0);
+      for (int64_t k = 0; k < n_dih; ++k) {
         if (!next_line(lines, j, l)) return bad("short Dihedrals");
+        std::istringstream ss(l);
+        int64_t id, q[4]; int t;
+        if (!(ss >> id >> t >> q[0] >> q[1] >> q[2] >> q[3]) || t < 1 || t > std::max(h.n_dihedral_types, 1))
+          return bad("bad Dihedrals line");
+        for (int c = 0; c < 4; ++c) {
+          if (q[c] < 1 || q[c] > n) return bad("bad Dihedrals line");
+          d->dihedrals[4 * k + c] = (int32_t)(q[c] - 1);
+        }
+        d->dihedral_type[k] = t - 1;
+      }
     } else {
       continue;
     }
@@ -279,6 +305,18 @@ RBMD_API rbmd_status rbmd_data_topology(const rbmd_data* d, int32_t* bonds, int3
       angle_coeffs[2 * t] = d->angle_k[t];
       angle_coeffs[2 * t + 1] = d->angle_t0[t];
     }
+  return RBMD_OK;
+}
+
+RBMD_API rbmd_status rbmd_data_dihedrals(const rbmd_data* d, int32_t* dihedrals, int32_t* dihedral_type,
+                                         double* dihedral_coeffs) {
+  if (!d) return RBMD_ERR_ARG;
+  if (dihedrals && !d->dihedrals.empty())
+    std::memcpy(dihedrals, d->dihedrals.data(), sizeof(int32_t) * d->dihedrals.size());
+  if (dihedral_type && !d->dihedral_type.empty())
+    std::memcpy(dihedral_type, d->dihedral_type.data(), sizeof(int32_t) * d->dihedral_type.size());
+  if (dihedral_coeffs && !d->dih_coeffs.empty())
+    std::memcpy(dihedral_coeffs, d->dih_coeffs.data(), sizeof(double) * d->dih_coeffs.size());
   return RBMD_OK;
 }
 

@@ -5,6 +5,7 @@
 #include <type_traits>
 
 #include "common.cuh"
+#include "kernels_bonded.cuh"
 
 namespace rbmd {
 
@@ -45,6 +46,7 @@ struct NearParams {
   double sqrt_alpha, two_sqrt_alpha_over_sqrt_pi;
   int kstage;                     // records of shared memory available for k staging
   int orig;                       // neighbour type "ORIGINAL": pairs with d^2 < rc^2 (no 1e-4 margin)
+  SpecialDev sp;                  // molecular == 2: special-bond partner lists
 };
 
 template <class R> struct KRec;
@@ -113,6 +115,9 @@ __device__ __forceinline__ void rbe_terms(const typename FracT<R>::T& fr, const 
 //            the cached positions are unwrapped since the build (k_regather), so the stored
 //            image shift still gives the minimum-image vector.
 constexpr int kMiNone = 0, kMiLJ = 1, kMiAll = 2;
+// Added to MI: the LJ pairs of one bond-graph component take their special-bond weight
+// (molecular == 2).  A separate instantiation, so the passes without topology carry none of it.
+constexpr int kMiSpecial = 4;
 
 template <class R>
 __device__ __forceinline__ void min_image(R& q0, R& q1, R& q2, const R* box) {
@@ -158,6 +163,7 @@ __global__ void __launch_bounds__(256) k_near_force(
   }
   __syncthreads();
   const bool MOLEC = prm.molecular != 0;
+  constexpr bool SPW = (MI & kMiSpecial) != 0;
   const bool ENERGY = energy_slot != nullptr;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= prm.n) return;
@@ -199,7 +205,7 @@ __global__ void __launch_bounds__(256) k_near_force(
     }
     const R r0 = px - pi.x, r1 = py - pi.y, r2 = pz - pi.z;
     const R d2 = r0 * r0 + r1 * r1 + r2 * r2;
-    if (MI == kMiAll && !((prm.orig ? cut2 - d2 > (R)0 : cut2 - d2 > (R)1.0e-4) && d2 > (R)1.0e-4)) continue;
+    if ((MI & 3) == kMiAll && !((prm.orig ? cut2 - d2 > (R)0 : cut2 - d2 > (R)1.0e-4) && d2 > (R)1.0e-4)) continue;
     R f = 0;
     if (COUL) {
       const R qq = qi * pj.w;
@@ -218,15 +224,20 @@ __global__ void __launch_bounds__(256) k_near_force(
     R fl0 = 0, fl1 = 0, fl2 = 0;
     bool same = false;
     int tj = 0;
+    R wsp = (R)1;   // special-bond LJ weight (molecular == 2: meta.y is the bond-graph component)
     if (typed) {
       const int2 mj = meta[e >> kShiftBits];
       same = MOLEC && (mj.y == mi.y);
       tj = prm.ntypes > 1 ? mj.x : 0;
+      if (SPW && same) {
+        wsp = special_weight<R>(prm.sp, slot_atom[i], slot_atom[e >> kShiftBits]);
+        same = false;
+      }
     }
     if (!same) {
       R q0 = r0, q1 = r1, q2 = r2;   // MinDistanceVec(p_j', p_i)
       R dl2 = d2;
-      if (MI == kMiLJ) {
+      if ((MI & 3) == kMiLJ) {
         min_image(q0, q1, q2, box);
         dl2 = q0 * q0 + q1 * q1 + q2 * q2;
       }
@@ -234,10 +245,11 @@ __global__ void __launch_bounds__(256) k_near_force(
         const R inv2 = rcp_r(dl2);
         const R sd6 = lj_s6[trow + tj] * inv2 * inv2 * inv2;
         const R a24 = lj_a[trow + tj];
-        const R scal = a24 * (((R)2 * sd6 - (R)1) * sd6) * inv2;
+        R scal = a24 * (((R)2 * sd6 - (R)1) * sd6) * inv2;
+        if (SPW) scal *= wsp;
         fl0 = scal * q0; fl1 = scal * q1; fl2 = scal * q2;
         // 4 eps (s6 - 1) s6 with 4 eps = -lj24/6
-        if (ENERGY) e_lj += -a24 / (R)6 * (sd6 - (R)1) * sd6;
+        if (ENERGY) e_lj += (SPW ? wsp : (R)1) * (-a24 / (R)6 * (sd6 - (R)1) * sd6);
       }
     }
     gx += f * r0 + fl0;
@@ -283,6 +295,7 @@ __global__ void __launch_bounds__(256) k_near_force_group(
   }
   __syncthreads();
   const bool MOLEC = prm.molecular != 0;
+  constexpr bool SPW = (MI & kMiSpecial) != 0;
   const bool ENERGY = energy_slot != nullptr;
   const int gid = (int)((blockIdx.x * blockDim.x + threadIdx.x) / G);
   const int sub = threadIdx.x % G;
@@ -318,7 +331,7 @@ __global__ void __launch_bounds__(256) k_near_force_group(
     }
     const R r0 = px - pi.x, r1 = py - pi.y, r2 = pz - pi.z;
     const R d2 = r0 * r0 + r1 * r1 + r2 * r2;
-    if (MI == kMiAll && !((prm.orig ? cut2 - d2 > (R)0 : cut2 - d2 > (R)1.0e-4) && d2 > (R)1.0e-4)) continue;
+    if ((MI & 3) == kMiAll && !((prm.orig ? cut2 - d2 > (R)0 : cut2 - d2 > (R)1.0e-4) && d2 > (R)1.0e-4)) continue;
     R f = 0;
     if (COUL) {
       const R qq = qi * pj.w;
@@ -337,15 +350,20 @@ __global__ void __launch_bounds__(256) k_near_force_group(
     R fl0 = 0, fl1 = 0, fl2 = 0;
     bool same = false;
     int tj = 0;
+    R wsp = (R)1;   // special-bond LJ weight (molecular == 2: meta.y is the bond-graph component)
     if (typed) {
       const int2 mj = meta[e >> kShiftBits];
       same = MOLEC && (mj.y == mi.y);
       tj = prm.ntypes > 1 ? mj.x : 0;
+      if (SPW && same) {
+        wsp = special_weight<R>(prm.sp, slot_atom[i], slot_atom[e >> kShiftBits]);
+        same = false;
+      }
     }
     if (!same) {
       R q0 = r0, q1 = r1, q2 = r2;
       R dl2 = d2;
-      if (MI == kMiLJ) {
+      if ((MI & 3) == kMiLJ) {
         min_image(q0, q1, q2, box);
         dl2 = q0 * q0 + q1 * q1 + q2 * q2;
       }
@@ -353,9 +371,10 @@ __global__ void __launch_bounds__(256) k_near_force_group(
         const R inv2 = rcp_r(dl2);
         const R sd6 = lj_s6[trow + tj] * inv2 * inv2 * inv2;
         const R a24 = lj_a[trow + tj];
-        const R scal = a24 * (((R)2 * sd6 - (R)1) * sd6) * inv2;
+        R scal = a24 * (((R)2 * sd6 - (R)1) * sd6) * inv2;
+        if (SPW) scal *= wsp;
         fl0 = scal * q0; fl1 = scal * q1; fl2 = scal * q2;
-        if (ENERGY) e_lj += -a24 / (R)6 * (sd6 - (R)1) * sd6;
+        if (ENERGY) e_lj += (SPW ? wsp : (R)1) * (-a24 / (R)6 * (sd6 - (R)1) * sd6);
       }
     }
     gx += f * r0 + fl0;

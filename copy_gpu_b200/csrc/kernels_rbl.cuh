@@ -95,6 +95,7 @@ struct RblParams {
   const float* erf_tab;   // 2048 entries of the reference's ERF table (table_mode 1)
   double rc, rs, alpha, qqr2e;
   double sqrt_alpha, two_sqrt_alpha_over_sqrt_pi;
+  SpecialDev sp;    // molecular == 2: special-bond partner lists
 };
 
 // The reference's ERF table (rbmd/framework/staticTable/ExecStaticTable.h:37-39,96-135): the
@@ -116,7 +117,7 @@ __device__ __forceinline__ float rbl_table_g(const float* __restrict__ tab, floa
 // rs^2 < d^2 < rc^2 (ComputeLJForceRcs) and, unless dropped, Coulomb x pice on the same range.
 // The result is the reference's corr_force = LJ + qqr2e * Coulomb; k_force_sub_mean removes its
 // mean afterwards.
-template <class R, bool COUL>
+template <class R, bool COUL, bool SPW>
 __global__ void __launch_bounds__(128) k_rbl_force(
     RblParams prm, const LJTable* __restrict__ ljt, const typename Traits<R>::V4* __restrict__ pos4,
     const int2* __restrict__ meta, const int* __restrict__ nbr, const int* __restrict__ ncore,
@@ -195,10 +196,15 @@ __global__ void __launch_bounds__(128) k_rbl_force(
     }
     bool same = false;
     int tj = 0;
+    R wsp = (R)1;   // special-bond LJ weight (molecular == 2: meta.y is the bond-graph component)
     if (typed) {
       const int2 mj = meta[js];
       same = MOLEC && (mj.y == mi.y);
       tj = prm.ntypes > 1 ? mj.x : 0;
+      if (SPW && same) {
+        wsp = special_weight<R>(prm.sp, slot_atom[i], slot_atom[js]);
+        same = false;
+      }
     }
     if (!same) {
       const bool ok = shell ? (dm2 < rc2 && dm2 > rs2) : (dm2 < rc2 && dm2 > (R)0.0001);
@@ -206,9 +212,10 @@ __global__ void __launch_bounds__(128) k_rbl_force(
         const R inv2 = (R)1 / dm2;
         const R sd6 = lj_s6[trow + tj] * inv2 * inv2 * inv2;
         const R a24 = lj_a[trow + tj];
-        const R scal = w * (a24 * (((R)2 * sd6 - (R)1) * sd6) * inv2);
+        R scal = w * (a24 * (((R)2 * sd6 - (R)1) * sd6) * inv2);
+        if (SPW) scal *= wsp;
         t0 += scal * m0; t1 += scal * m1; t2 += scal * m2;
-        if (energy_slot) e_lj += (double)w * (double)(-a24 / (R)6 * (sd6 - (R)1) * sd6);
+        if (energy_slot) e_lj += (double)(w * wsp) * (double)(-a24 / (R)6 * (sd6 - (R)1) * sd6);
       }
     }
     fx.add(t0); fy.add(t1); fz.add(t2);

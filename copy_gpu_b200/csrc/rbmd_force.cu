@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <functional>
 #include <sstream>
 #include <string>
 #include <type_traits>
@@ -145,6 +146,16 @@ struct rbmd_force {
   std::vector<int32_t> hoh_h;
   double bond_k = 0, bond_r0 = 1, angle_k = 0, angle_t0 = 109.47;
 
+  // ---------------- general CVFF topology (rbmd_force_set_topology) ----------------
+  bool topo = false;                 // bonded terms of a topology replace the water extras
+  bool special = false;              // hyper_parameters.extend.special_bonds given
+  double special_w[3] = {0, 0, 0};
+  int64_t topo_n = 0;
+  int topo_nb = 0, topo_na = 0, topo_nd = 0;
+  std::vector<int32_t> term_atom_h, tmult_h, sc_off_h, sc_id_h, row_off_h, row_idx_h, sp_off_h, sp_id_h,
+      comp_h;
+  std::vector<double> tk_h, ta_h, sc_fac_h, sp_w_h;
+
   // ---------------- bound atoms ----------------
   rbmd_atoms_dev at{};
   std::vector<int64_t> rep_off;
@@ -209,6 +220,12 @@ struct rbmd_force {
   float4 *d_frho = nullptr, *d_rhor = nullptr, *d_z2r = nullptr;
   void* d_fp = nullptr;
   double *d_emb = nullptr, *d_epair = nullptr;
+  // topology device
+  int *d_term_atom = nullptr, *d_tmult = nullptr, *d_sc_off = nullptr, *d_sc_id = nullptr, *d_row_off = nullptr,
+      *d_row_idx = nullptr, *d_sp_off = nullptr, *d_sp_id = nullptr, *d_comp = nullptr;
+  double *d_tk = nullptr, *d_ta = nullptr, *d_sc_fac = nullptr, *d_rows = nullptr, *d_eterm = nullptr,
+         *d_esc = nullptr, *d_sp_wd = nullptr;
+  float* d_sp_wf = nullptr;
   // water device
   int* d_hoh = nullptr;
   double *d_ebond = nullptr, *d_eangle = nullptr;
@@ -303,6 +320,27 @@ void prof_collect(rbmd_force* f) {
   f->ev_used = 0;
 }
 
+SpecialDev special_dev(const rbmd_force* f) {
+  SpecialDev d;
+  d.off = f->d_sp_off;
+  d.id = f->d_sp_id;
+  d.wf = f->d_sp_wf;
+  d.wd = f->d_sp_wd;
+  return d;
+}
+
+// LJ pair mode of the near passes: 0 none, 1 same-molecule exclusion, 2 special-bond weights.
+int molecular_mode(const rbmd_force* f) {
+  if (f->topo && f->special && f->is_cvff()) return 2;
+  return f->at.molecule != nullptr ? 1 : 0;
+}
+
+void free_topology(rbmd_force* f) {
+  dfree(f->d_term_atom); dfree(f->d_tmult); dfree(f->d_sc_off); dfree(f->d_sc_id); dfree(f->d_row_off);
+  dfree(f->d_row_idx); dfree(f->d_sp_off); dfree(f->d_sp_id); dfree(f->d_comp); dfree(f->d_tk); dfree(f->d_ta);
+  dfree(f->d_sc_fac); dfree(f->d_rows); dfree(f->d_eterm); dfree(f->d_esc); dfree(f->d_sp_wd); dfree(f->d_sp_wf);
+}
+
 void free_all(rbmd_force* f) {
   dfree(f->d_reps); dfree(f->d_ljt);
   dfree(f->d_rep_of); dfree(f->d_cell_of); dfree(f->d_cell_count); dfree(f->d_cell_start);
@@ -331,6 +369,7 @@ void free_all(rbmd_force* f) {
   if (f->d_fp) cudaFree(f->d_fp);
   f->d_fp = nullptr;
   dfree(f->d_emb); dfree(f->d_epair); dfree(f->d_hoh); dfree(f->d_ebond); dfree(f->d_eangle);
+  free_topology(f);
   dfree(f->d_snap); dfree(f->d_snap_img); dfree(f->d_step); dfree(f->d_lstep);
   if (f->graph_exec) cudaGraphExecDestroy(f->graph_exec);
   f->graph_exec = nullptr;
@@ -714,7 +753,8 @@ void launch_sort(rbmd_force* f, cudaStream_t s, bool bin, bool regather) {
   k_scatter<<<(n + 255) / 256, 256, 0, s>>>(n, f->d_cell_of, f->d_cell_start, f->d_cursor, f->d_tmp, rep_of,
                                             rb);
   k_cell_sort_gather<R><<<(f->ncell_total + kSortWarps - 1) / kSortWarps, 32 * kSortWarps, 0, s>>>(
-      f->ncell_total, f->d_cell_start, f->d_tmp, f->at.pos, f->at.charge, f->at.type, f->at.molecule,
+      f->ncell_total, f->d_cell_start, f->d_tmp, f->at.pos, f->at.charge, f->at.type,
+      molecular_mode(f) == 2 ? f->d_comp : f->at.molecule,
       rep_of, f->d_reps, f->d_slot_atom, f->d_atom_slot, (typename Traits<R>::V4*)f->d_pos4, nullptr,
       f->d_meta, f->d_xref, rb, f->sort_x() ? 1 : 0, f->d_cell_rep);
   f->launches += 4;
@@ -820,7 +860,8 @@ void launch_near_t(rbmd_force* f, cudaStream_t s) {
   p.cap = f->cap;
   p.with_lj = 1;
   p.with_coul = COUL;
-  p.molecular = f->at.molecule != nullptr;
+  p.molecular = molecular_mode(f);
+  p.sp = special_dev(f);
   p.rc = f->rc;
   p.alpha = f->alpha;
   p.coul_scale = f->near_coul_scale;
@@ -852,6 +893,12 @@ void launch_near_t(rbmd_force* f, cudaStream_t s) {
 template <class R, bool COUL>
 void launch_near_m(rbmd_force* f, cudaStream_t s) {
   const int mi = f->skin > 0 ? kMiAll : (f->minimg ? kMiLJ : kMiNone);
+  if (molecular_mode(f) == 2) {   // special-bond LJ weights: their own instantiations
+    if (mi == kMiAll) launch_near_t<R, COUL, kMiAll | kMiSpecial>(f, s);
+    else if (mi == kMiLJ) launch_near_t<R, COUL, kMiLJ | kMiSpecial>(f, s);
+    else launch_near_t<R, COUL, kMiNone | kMiSpecial>(f, s);
+    return;
+  }
   if (mi == kMiAll) launch_near_t<R, COUL, kMiAll>(f, s);
   else if (mi == kMiLJ) launch_near_t<R, COUL, kMiLJ>(f, s);
   else launch_near_t<R, COUL, kMiNone>(f, s);
@@ -919,7 +966,8 @@ void launch_rbl_force(rbmd_force* f, cudaStream_t s) {
     p.stride = f->stride;
     p.ntypes = f->nt_eff;
     p.core_cap = f->core_cap;
-    p.molecular = f->at.molecule != nullptr;
+    p.molecular = molecular_mode(f);
+    p.sp = special_dev(f);
     p.table_mode = f->rbl_table ? 1 : 0;
     p.shell_coul = f->rbl_shell_coul ? 1 : 0;
     p.erf_tab = f->d_erf_tab;
@@ -930,14 +978,11 @@ void launch_rbl_force(rbmd_force* f, cudaStream_t s) {
     p.sqrt_alpha = std::sqrt(f->alpha);
     p.two_sqrt_alpha_over_sqrt_pi = 2.0 * std::sqrt(f->alpha) / std::sqrt(M_PI);
     double* es = f->want_energy ? f->d_eslot : nullptr;
-    if (f->with_coul_near())
-      k_rbl_force<R, true><<<nb, 128, 0, s>>>(p, f->d_ljt, (const typename Traits<R>::V4*)f->d_pos4, f->d_meta,
-                                              f->d_nbr, f->d_count, f->d_count2, f->d_reps, rp, f->d_slot_atom,
-                                              f->shell_cap, f->at.force, es, f->d_status);
-    else
-      k_rbl_force<R, false><<<nb, 128, 0, s>>>(p, f->d_ljt, (const typename Traits<R>::V4*)f->d_pos4, f->d_meta,
-                                               f->d_nbr, f->d_count, f->d_count2, f->d_reps, rp, f->d_slot_atom,
-                                               f->shell_cap, f->at.force, es, f->d_status);
+    const bool spw = p.molecular == 2;
+    auto kern = f->with_coul_near() ? (spw ? k_rbl_force<R, true, true> : k_rbl_force<R, true, false>)
+                                    : (spw ? k_rbl_force<R, false, true> : k_rbl_force<R, false, false>);
+    kern<<<nb, 128, 0, s>>>(p, f->d_ljt, (const typename Traits<R>::V4*)f->d_pos4, f->d_meta, f->d_nbr, f->d_count,
+                            f->d_count2, f->d_reps, rp, f->d_slot_atom, f->shell_cap, f->at.force, es, f->d_status);
     f->launches++;
   }
   // F_i -= mean_j F_j per replica (ExecutionMD.cpp:568-570)
@@ -947,8 +992,31 @@ void launch_rbl_force(rbmd_force* f, cudaStream_t s) {
   f->launches += 2;
 }
 
+// General topology: per-term forces, then the per-atom gather with the Coulomb correction.
+void launch_bonded(rbmd_force* f, cudaStream_t s) {
+  BondedParams bp;
+  bp.n = f->n;
+  bp.nb = f->topo_nb;
+  bp.na = f->topo_na;
+  bp.nd = f->topo_nd;
+  bp.coul_const = 332.06371;
+  const int* rep_of = f->nrep > 1 ? f->d_rep_of : nullptr;
+  const int nterm = bp.nb + bp.na + bp.nd;
+  if (nterm > 0) {
+    k_bonded_terms<<<(nterm + 255) / 256, 256, 0, s>>>(bp, f->d_term_atom, f->d_tk, f->d_ta, f->d_tmult, f->at.pos,
+                                                       rep_of, f->d_reps, f->d_rows, f->d_eterm);
+    f->launches++;
+  }
+  k_bonded_gather<<<(f->n + 255) / 256, 256, 0, s>>>(bp, f->d_sc_off, f->d_sc_id, f->d_sc_fac, f->d_row_off,
+                                                     f->d_row_idx, f->at.pos, f->at.charge, rep_of, f->d_reps,
+                                                     f->d_rows, f->at.force, f->d_esc);
+  f->launches++;
+}
+
 void launch_water(rbmd_force* f, cudaStream_t s) {
-  if (!f->is_cvff() || f->n_mol == 0) return;
+  if (!f->is_cvff()) return;
+  if (f->topo) { launch_bonded(f, s); return; }
+  if (f->n_mol == 0) return;
   WaterParams wp;
   wp.n_mol = (int)f->n_mol;
   wp.bond_k = f->bond_k;
@@ -1276,6 +1344,13 @@ rbmd_status parse_config(rbmd_force* f, const char* text) {
   f->shake = rbmdjson::text(root, "hyper_parameters.extend.fix_shake", "null");
   f->shake_tol = num(root, "hyper_parameters.extend.shake_tolerance", 1e-5);
   f->shake_max_iter = (int)num(root, "hyper_parameters.extend.shake_max_iter", 5000);
+  {
+    // MDApplication.cpp:157-163: a non-empty special_bonds list turns on the special-bond path
+    // (the reference parses it as integers, Extend.cpp:39; fractional weights are kept here)
+    std::vector<double> sb = nums(root, "hyper_parameters.extend.special_bonds");
+    f->special = !sb.empty();
+    for (int k = 0; k < 3; ++k) f->special_w[k] = k < (int)sb.size() ? sb[k] : 0.0;
+  }
   std::string prec = rbmdjson::text(root, "precision", "fp32");
   f->fp64 = prec == "fp64" || prec == "FP64" || prec == "double";
   if (root.path("init_configuration.inbuild")) {
@@ -1543,6 +1618,210 @@ rbmd_status rbmd_force_set_water(rbmd_force* f, int64_t n_mol, const int32_t* ho
     dfree(f->d_ebond); dfree(f->d_eangle);
     CK(dalloc(&f->d_ebond, (size_t)n_mol));
     CK(dalloc(&f->d_eangle, (size_t)n_mol));
+  }
+  return RBMD_OK;
+}
+
+// Device copies of the topology tables (at bind, or at set_topology once bound).
+static rbmd_status upload_topology(rbmd_force* f) {
+  free_topology(f);
+  if (!f->topo) return RBMD_OK;
+  if (f->topo_n != f->n) {
+    std::snprintf(g_last_error, sizeof g_last_error, "topology has %lld atoms, bound arrays %d",
+                  (long long)f->topo_n, f->n);
+    return RBMD_ERR_ARG;
+  }
+  auto upi = [&](const std::vector<int32_t>& v, int** d) -> cudaError_t {
+    cudaError_t e = dalloc(d, v.size());
+    if (e == cudaSuccess && !v.empty())
+      e = cudaMemcpy(*d, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice);
+    return e;
+  };
+  auto upd = [&](const std::vector<double>& v, double** d) -> cudaError_t {
+    cudaError_t e = dalloc(d, v.size());
+    if (e == cudaSuccess && !v.empty())
+      e = cudaMemcpy(*d, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice);
+    return e;
+  };
+  CK(upi(f->term_atom_h, &f->d_term_atom));
+  CK(upi(f->tmult_h, &f->d_tmult));
+  CK(upd(f->tk_h, &f->d_tk));
+  CK(upd(f->ta_h, &f->d_ta));
+  CK(upi(f->sc_off_h, &f->d_sc_off));
+  CK(upi(f->sc_id_h, &f->d_sc_id));
+  CK(upd(f->sc_fac_h, &f->d_sc_fac));
+  CK(upi(f->row_off_h, &f->d_row_off));
+  CK(upi(f->row_idx_h, &f->d_row_idx));
+  CK(dalloc(&f->d_rows, 3 * f->term_atom_h.size()));
+  CK(dalloc(&f->d_eterm, (size_t)(f->topo_nb + f->topo_na + f->topo_nd)));
+  CK(dalloc(&f->d_esc, (size_t)f->n));
+  CK(cudaMemset(f->d_esc, 0, sizeof(double) * f->n));
+  CK(cudaMemset(f->d_eterm, 0, sizeof(double) * std::max(1, f->topo_nb + f->topo_na + f->topo_nd)));
+  if (f->special) {
+    CK(upi(f->sp_off_h, &f->d_sp_off));
+    CK(upi(f->sp_id_h, &f->d_sp_id));
+    CK(upd(f->sp_w_h, &f->d_sp_wd));
+    std::vector<float> wf(f->sp_w_h.begin(), f->sp_w_h.end());
+    CK(dalloc(&f->d_sp_wf, wf.size()));
+    if (!wf.empty()) CK(cudaMemcpy(f->d_sp_wf, wf.data(), sizeof(float) * wf.size(), cudaMemcpyHostToDevice));
+    CK(upi(f->comp_h, &f->d_comp));
+  }
+  return RBMD_OK;
+}
+
+rbmd_status rbmd_force_set_topology(rbmd_force* f, const rbmd_topology* t) {
+  if (!f || !t || t->n_atoms < 1 || !t->molecule || t->n_bonds < 0 || t->n_angles < 0 || t->n_dihedrals < 0)
+    return RBMD_ERR_ARG;
+  const int64_t n = t->n_atoms;
+  const int64_t nb = t->n_bonds, na = t->n_angles, nd = f->special ? t->n_dihedrals : 0;
+  if ((nb && (!t->bonds || !t->bond_type || !t->bond_coeffs)) ||
+      (na && (!t->angles || !t->angle_type || !t->angle_coeffs)) ||
+      (nd && (!t->dihedrals || !t->dihedral_type || !t->dihedral_coeffs)))
+    return RBMD_ERR_ARG;
+  if (2 * nb + 3 * na + 4 * nd >= (1LL << 31)) return RBMD_ERR_ARG;
+  auto bad_ids = [&](const int32_t* a, int64_t cnt) {
+    for (int64_t k = 0; k < cnt; ++k)
+      if (a[k] < 0 || a[k] >= n) return true;
+    return false;
+  };
+  auto bad_types = [&](const int32_t* a, int64_t cnt, int32_t ntypes) {
+    for (int64_t k = 0; k < cnt; ++k)
+      if (a[k] < 0 || a[k] >= ntypes) return true;
+    return false;
+  };
+  if (bad_ids(t->bonds, 2 * nb) || bad_ids(t->angles, 3 * na) || (nd && bad_ids(t->dihedrals, 4 * nd)) ||
+      bad_types(t->bond_type, nb, t->n_bond_types) || bad_types(t->angle_type, na, t->n_angle_types) ||
+      (nd && bad_types(t->dihedral_type, nd, t->n_dihedral_types))) {
+    std::snprintf(g_last_error, sizeof g_last_error, "topology: atom id or type out of range");
+    return RBMD_ERR_ARG;
+  }
+  // terms: packed atoms and per-term coefficients
+  f->topo_n = n;
+  f->topo_nb = (int)nb; f->topo_na = (int)na; f->topo_nd = (int)nd;
+  f->term_atom_h.assign(t->bonds, t->bonds + 2 * nb);
+  f->term_atom_h.insert(f->term_atom_h.end(), t->angles, t->angles + 3 * na);
+  if (nd) f->term_atom_h.insert(f->term_atom_h.end(), t->dihedrals, t->dihedrals + 4 * nd);
+  const int64_t nterm = nb + na + nd;
+  f->tk_h.assign(nterm, 0.0);
+  f->ta_h.assign(nterm, 0.0);
+  f->tmult_h.assign(nterm, 0);
+  for (int64_t b = 0; b < nb; ++b) {
+    f->tk_h[b] = t->bond_coeffs[2 * t->bond_type[b]];
+    f->ta_h[b] = t->bond_coeffs[2 * t->bond_type[b] + 1];
+  }
+  for (int64_t a = 0; a < na; ++a) {
+    f->tk_h[nb + a] = t->angle_coeffs[2 * t->angle_type[a]];
+    f->ta_h[nb + a] = t->angle_coeffs[2 * t->angle_type[a] + 1] * M_PI / 180.0;
+  }
+  for (int64_t d = 0; d < nd; ++d) {
+    const double* c = t->dihedral_coeffs + 3 * t->dihedral_type[d];
+    f->tk_h[nb + na + d] = c[0];
+    f->ta_h[nb + na + d] = (int)c[1] == 1 ? 1.0 : -1.0;   // cos_shift (ComputeDihedralHarmonicWorklet)
+    f->tmult_h[nb + na + d] = (int)c[2];
+  }
+  // rows of each atom, ascending (bonds, angles, dihedrals)
+  const int64_t nrow = (int64_t)f->term_atom_h.size();
+  f->row_off_h.assign(n + 1, 0);
+  for (int64_t e = 0; e < nrow; ++e) f->row_off_h[f->term_atom_h[e] + 1]++;
+  for (int64_t a = 0; a < n; ++a) f->row_off_h[a + 1] += f->row_off_h[a];
+  f->row_idx_h.assign(nrow, 0);
+  {
+    std::vector<int32_t> cur(f->row_off_h.begin(), f->row_off_h.end() - 1);
+    for (int64_t e = 0; e < nrow; ++e) f->row_idx_h[cur[f->term_atom_h[e]]++] = (int32_t)e;
+  }
+  // molecules
+  std::vector<std::vector<int32_t>> members;
+  {
+    std::vector<int32_t> mol(t->molecule, t->molecule + n);
+    int32_t mmax = -1;
+    for (int32_t m : mol) {
+      if (m < 0) { std::snprintf(g_last_error, sizeof g_last_error, "topology: negative molecule id"); return RBMD_ERR_ARG; }
+      mmax = std::max(mmax, m);
+    }
+    members.assign((size_t)mmax + 1, {});
+    for (int64_t a = 0; a < n; ++a) members[mol[a]].push_back((int32_t)a);
+  }
+  // special-bond lists (ModelFileInitCondition::SetSpecialBonds), reduced to one entry per partner
+  // carrying the weight of its last occurrence, the one the reference's pair loops keep
+  std::vector<std::vector<std::pair<int32_t, double>>> sp(f->special ? n : 0);
+  if (f->special) {
+    std::vector<std::vector<int32_t>> adj(n);
+    for (int64_t b = 0; b < nb; ++b) {
+      adj[t->bonds[2 * b]].push_back(t->bonds[2 * b + 1]);
+      adj[t->bonds[2 * b + 1]].push_back(t->bonds[2 * b]);
+    }
+    for (int64_t a = 0; a < n; ++a) {
+      std::vector<std::pair<int32_t, double>> raw;
+      for (int32_t k1 : adj[a]) {
+        raw.push_back({k1, f->special_w[0]});
+        for (int32_t k2 : adj[k1]) {
+          if (k2 == a) continue;
+          raw.push_back({k2, f->special_w[1]});
+          for (int32_t k3 : adj[k2]) {
+            if (k3 == k1) continue;
+            raw.push_back({k3, f->special_w[2]});
+          }
+        }
+      }
+      for (size_t k = 0; k < raw.size(); ++k) {
+        if (raw[k].first == a) continue;   // never a pair partner
+        bool later = false;
+        for (size_t l = k + 1; l < raw.size() && !later; ++l) later = raw[l].first == raw[k].first;
+        if (!later) sp[a].push_back(raw[k]);
+      }
+    }
+    f->sp_off_h.assign(n + 1, 0);
+    f->sp_id_h.clear();
+    f->sp_w_h.clear();
+    for (int64_t a = 0; a < n; ++a) {
+      for (auto& pr : sp[a])
+        if (pr.second != 1.0) { f->sp_id_h.push_back(pr.first); f->sp_w_h.push_back(pr.second); }
+      f->sp_off_h[a + 1] = (int32_t)f->sp_id_h.size();
+    }
+    // bond-graph components: special partners always share one, so the near passes look up
+    // weights only for pairs inside a component
+    std::vector<int32_t> par(n);
+    for (int64_t a = 0; a < n; ++a) par[a] = (int32_t)a;
+    std::function<int32_t(int32_t)> root = [&](int32_t x) {
+      while (par[x] != x) { par[x] = par[par[x]]; x = par[x]; }
+      return x;
+    };
+    for (int64_t b = 0; b < nb; ++b) {
+      const int32_t r1 = root(t->bonds[2 * b]), r2 = root(t->bonds[2 * b + 1]);
+      if (r1 != r2) par[std::max(r1, r2)] = std::min(r1, r2);
+    }
+    f->comp_h.assign(n, 0);
+    for (int64_t a = 0; a < n; ++a) f->comp_h[a] = root((int32_t)a);
+  }
+  // intramolecular Coulomb correction lists
+  f->sc_off_h.assign(n + 1, 0);
+  f->sc_id_h.clear();
+  f->sc_fac_h.clear();
+  for (int64_t a = 0; a < n; ++a) {
+    const auto& g = members[t->molecule[a]];
+    if (g.size() >= 3) {
+      if (!f->special) {
+        for (int32_t j : g)
+          if (j != a) { f->sc_id_h.push_back(j); f->sc_fac_h.push_back(1.0); }
+      } else {
+        for (auto& pr : sp[a])
+          if (pr.second != 1.0 && t->molecule[pr.first] == t->molecule[a]) {
+            f->sc_id_h.push_back(pr.first);
+            f->sc_fac_h.push_back(1.0 - pr.second);
+          }
+      }
+    }
+    if (f->sc_id_h.size() >= (size_t)1 << 31) {
+      std::snprintf(g_last_error, sizeof g_last_error, "topology: intramolecular pair list too long");
+      return RBMD_ERR_ARG;
+    }
+    f->sc_off_h[a + 1] = (int32_t)f->sc_id_h.size();
+  }
+  f->topo = true;
+  if (f->bound) {
+    rbmd_status st = upload_topology(f);
+    if (st) return st;
+    f->list_valid = false;
   }
   return RBMD_OK;
 }
@@ -1937,6 +2216,10 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
     CK(dalloc(&f->d_ebond, (size_t)f->n_mol));
     CK(dalloc(&f->d_eangle, (size_t)f->n_mol));
   }
+  {
+    rbmd_status st = upload_topology(f);
+    if (st) return st;
+  }
   f->bound = true;
   f->list_valid = false;
   f->step_count = 0;
@@ -2112,7 +2395,13 @@ rbmd_status rbmd_force_energy(rbmd_force* f, rbmd_energy* out, void* stream) {
     k_sum<<<1, 1024, 0, s>>>(f->n, f->d_epair, 1, 0, f->d_esum + 5);
   }
   if (f->is_rbe()) k_sum<<<1, 1024, 0, s>>>(f->Ptot, f->d_ek, 1, 0, f->d_esum + 2);
-  if (f->n_mol > 0 && f->is_cvff()) {
+  if (f->topo && f->is_cvff()) {
+    if (f->topo_nb) k_sum<<<1, 1024, 0, s>>>(f->topo_nb, f->d_eterm, 1, 0, f->d_esum + 6);
+    if (f->topo_na) k_sum<<<1, 1024, 0, s>>>(f->topo_na, f->d_eterm + f->topo_nb, 1, 0, f->d_esum + 7);
+    if (f->topo_nd)
+      k_sum<<<1, 1024, 0, s>>>(f->topo_nd, f->d_eterm + f->topo_nb + f->topo_na, 1, 0, f->d_esum + 10);
+    k_sum<<<1, 1024, 0, s>>>(f->n, f->d_esc, 1, 0, f->d_esum + 11);
+  } else if (f->n_mol > 0 && f->is_cvff()) {
     k_sum<<<1, 1024, 0, s>>>((int)f->n_mol, f->d_ebond, 1, 0, f->d_esum + 6);
     k_sum<<<1, 1024, 0, s>>>((int)f->n_mol, f->d_eangle, 1, 0, f->d_esum + 7);
   }
@@ -2132,6 +2421,8 @@ rbmd_status rbmd_force_energy(rbmd_force* f, rbmd_energy* out, void* stream) {
   out->angle = h[7];
   out->kinetic = h[8];
   out->temperature = h[9] / f->nrep;
+  out->dihedral = h[10];
+  out->coul_special = h[11];
   return RBMD_OK;
 }
 

@@ -11,6 +11,8 @@ box lo/hi) plus the RBMD JSON configuration that selects the matching force path
 * ``water``         -- rigid 3-site water (SPC/E charges) at 1.0 g/cm^3, random orientations.
 * ``eam_fcc``       -- FCC metal with Gaussian thermal displacements, plus ``write_johnson_funcfl``
                        which tabulates Johnson's analytic EAM as a funcfl file.
+* ``molecular``     -- flexible chain molecules with bonds, angles and dihedrals of several types
+                       plus free ions, REAL units (the shape of a polymer electrolyte input).
 """
 from __future__ import annotations
 
@@ -277,6 +279,107 @@ def eam_fcc(ncell=40, a=3.615, T=300.0, k_eff=1.5, mass=63.546, seed=13):
     vel = _maxwell(rng, n, T, m, kB=8.617343e-5, mvv2e=1.0364269e-4)
     return dict(pos=pos, vel=vel, mass=m, charge=np.zeros(n), type=np.zeros(n, np.int32),
                 molecule=None, lo=np.zeros(3), hi=np.full(3, L), eps=np.ones(1), sigma=np.ones(1))
+
+
+# ------------------------------------------------------------------------------------------
+# flexible molecules
+# ------------------------------------------------------------------------------------------
+def molecular_config(P=100, cutoff=8.0, alpha=0.09, neighbor="VERLETLIST", special=(0.0, 0.0, 0.5), dt=0.5,
+                     T=298.0, precision="fp64", seed=5, r_core=4.0, sample_num=100):
+    """CVFF with a full topology: LJ + erfc near Coulomb + RBE, special-bond weights, REAL units.
+    special=None leaves out extend.special_bonds (same-molecule LJ exclusion, no dihedrals)."""
+    nb = {"type": neighbor, "cut_off": cutoff}
+    if neighbor == "RBL":
+        nb.update({"r_core": r_core, "neighbor_sample_num": sample_num})
+    cfg = {
+        "init_configuration": {"read_data": {"unit": "REAL", "atom_style": "full", "velocity_type": "GAUSS"}},
+        "hyper_parameters": {
+            "force_field": {"type": "CVFF"},
+            "neighbor": nb,
+            "coulomb": {"type": "RBE", "coulomb_sample_num": P, "alpha": alpha, "kmax": 2, "seed": seed},
+        },
+        "execution": {"ensemble": "NVE", "temperature": [T, T, 100.0], "timestep": dt, "num_steps": 1000},
+        "precision": precision,
+    }
+    if special is not None:
+        cfg["hyper_parameters"]["extend"] = {"special_bonds": list(special)}
+    return cfg
+
+
+def molecular(n_chain=64, chain_len=12, n_ion_pairs=16, step=1.6, cell=8.0, T=298.0, seed=21):
+    """Chains grown as self-avoiding walks (step `step`, 90 or 180 degree turns, no U-turns, small jitter),
+    one chain per cell of a cubic lattice of spacing `cell`, plus +/-1 ion pairs in free cells.
+    Backbone types alternate 0/1 (charges +0.2/-0.2, one end group type 2 carries the rest so
+    every chain is neutral); ions are types 3 (+1) and 4 (-1), each its own molecule.  Bonds,
+    angles and dihedrals follow the chain; their types depend on the end atom types, so several
+    coefficient rows are used.  Returns arrays plus per-type coefficient tables."""
+    rng = np.random.default_rng(seed)
+    n_sites = n_chain + 2 * n_ion_pairs
+    m = int(math.ceil(n_sites ** (1.0 / 3.0) - 1e-9))
+    while m ** 3 < n_sites:
+        m += 1
+    L = m * cell
+    order = rng.permutation(m ** 3)[:n_sites]
+    corners = np.stack(np.unravel_index(order, (m, m, m)), axis=1).astype(np.float64) * cell
+    g = int(cell / step) - 1   # sublattice points per axis inside a cell, one step of margin
+    pos, typ, q, mol, bonds, angles, dihs = [], [], [], [], [], [], []
+    moves = np.array([[1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1]])
+    for c in range(n_chain):
+        while True:   # self-avoiding walk on the g^3 sublattice of the cell
+            p = [rng.integers(0, g, size=3)]
+            seen = {tuple(p[0])}
+            ok = True
+            for _ in range(chain_len - 1):
+                cand = [p[-1] + mv for mv in moves]
+                # inside the cell, unvisited, and at least sqrt(2) steps from every site three or
+                # more bonds back (no U-turns: keeps 1-4 and farther pairs off the LJ wall)
+                cand = [x for x in cand if (x >= 0).all() and (x < g).all() and tuple(x) not in seen
+                        and all(((x - y) ** 2).sum() >= 2 for y in p[:-2])]
+                if not cand:
+                    ok = False
+                    break
+                x = cand[rng.integers(len(cand))]
+                p.append(x)
+                seen.add(tuple(x))
+            if ok:
+                break
+        base = len(pos)
+        for k, x in enumerate(p):
+            pos.append(corners[c] + (x + 0.5) * step + rng.normal(scale=0.05, size=3))
+            t = 2 if k == chain_len - 1 else k % 2
+            typ.append(t)
+            q.append(0.2 if t == 0 else -0.2)
+            mol.append(c)
+        q[-1] = -sum(q[base:-1])
+        for k in range(chain_len - 1):
+            bonds.append((base + k, base + k + 1))
+        for k in range(chain_len - 2):
+            angles.append((base + k, base + k + 1, base + k + 2))
+        for k in range(chain_len - 3):
+            dihs.append((base + k, base + k + 1, base + k + 2, base + k + 3))
+    for i in range(2 * n_ion_pairs):
+        pos.append(corners[n_chain + i] + rng.uniform(0.3, 0.7, size=3) * cell)
+        typ.append(3 + (i % 2))
+        q.append(1.0 if i % 2 == 0 else -1.0)
+        mol.append(n_chain + i)
+    pos = np.mod(np.array(pos), L)
+    typ = np.array(typ, np.int32)
+    bonds, angles, dihs = (np.array(a, np.int32).reshape(-1, w) for a, w in ((bonds, 2), (angles, 3), (dihs, 4)))
+    bond_type = (typ[bonds[:, 0]] + typ[bonds[:, 1]]).astype(np.int32)            # 0..3
+    angle_type = (typ[angles[:, 0]] + typ[angles[:, 2]]).astype(np.int32) % 3      # 0..2
+    dih_type = (typ[dihs[:, 0]] + typ[dihs[:, 3]]).astype(np.int32) % 3            # 0..2
+    mass = np.array([12.011, 15.999, 15.035, 6.94, 140.0])[typ]
+    n = len(typ)
+    return dict(pos=pos, vel=_maxwell(rng, n, T, mass, 1.9872067e-3, 1.0 / 4.186e-4), mass=mass,
+                charge=np.array(q), type=typ, molecule=np.array(mol, np.int32), lo=np.zeros(3),
+                hi=np.full(3, L), eps=np.array([0.066, 0.14, 0.17, 0.018, 0.2]),
+                sigma=np.array([3.5, 2.9, 3.9, 2.1, 4.0]),
+                bonds=bonds, bond_type=bond_type,
+                bond_coeffs=np.array([[300.0, step], [320.0, step], [280.0, 1.05 * step], [310.0, step]]),
+                angles=angles, angle_type=angle_type,
+                angle_coeffs=np.array([[50.0, 109.5], [60.0, 112.0], [45.0, 95.0]]),
+                dihedrals=dihs, dihedral_type=dih_type,
+                dihedral_coeffs=np.array([[0.15, 1, 3], [0.3, -1, 2], [0.08, 1, 1]]))
 
 
 def to_json(cfg) -> str:

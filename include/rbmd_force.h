@@ -88,6 +88,8 @@ typedef struct {
   double angle;        /* harmonic angles                                     */
   double kinetic;      /* 1/2 sum m v^2 * mvv2e (step API)                     */
   double temperature;  /* as ExecutionNVT::ComputeTempe (step API)            */
+  double dihedral;     /* harmonic dihedrals (rbmd_force_set_topology)        */
+  double coul_special; /* intramolecular Coulomb correction (set_topology)    */
 } rbmd_energy;
 
 /* Create a force path from RBMD's JSON configuration text (the same "hyper_parameters",
@@ -118,6 +120,45 @@ RBMD_API rbmd_status rbmd_force_load_funcfl(rbmd_force* f, const char* path);
 RBMD_API rbmd_status rbmd_force_set_water(rbmd_force* f, int64_t n_mol, const int32_t* hoh_triples_host,
                                  double bond_k, double bond_r0, double angle_k,
                                  double angle_theta0_deg);
+
+/* General CVFF topology (host arrays, 0-based caller atom ids, data-file section order):
+ * bonds [n_bonds][2] + type, angles [n_angles][3] + type, dihedrals [n_dihedrals][4] + type, per
+ * type coefficients bond (k, r0), angle (k, theta0 in degrees), dihedral (K, sign d = +-1,
+ * multiplicity n) of "Bond/Angle/Dihedral Coeffs # harmonic", and the molecule id of every atom.
+ * Forces added after the near pass, as ExecutionNVT::ComputeAllForce does for "CVFF"
+ * (rbmd/framework/run/ExecutionNVT.cpp:199-215):
+ *  - intramolecular Coulomb correction -332.06371 q_i q_j r/r^3 over the other members of
+ *    molecules of >= 3 atoms (ComputeSpecialCoulWorklet, RunWorklet.cpp:1386-1437);
+ *  - harmonic bonds and angles with per-type coefficients (ExecutionNVT.cpp:467-610);
+ *  - with hyper_parameters.extend.special_bonds [w12, w13, w14] in the configuration
+ *    (rbmd/framework/application/MDApplication.cpp:157-163): special-bond lists built as
+ *    ModelFileInitCondition::SetSpecialBonds does (ModelFileInitCondition.cpp:850-910), LJ pairs
+ *    weighted by w instead of excluded within the molecule (RunWorklet.cpp:570-632,816-933), the
+ *    Coulomb correction times 1 - w (ComputeSpecialCoulGeneralWorklet, RunWorklet.cpp:1439-1511)
+ *    and harmonic dihedrals E = K [1 + d cos(n phi)] (ExecutionNVT.cpp:612-680); without
+ *    special_bonds the dihedrals are ignored, as in the reference.
+ * Supersedes the water extras of rbmd_force_set_water (SHAKE still uses its triples).  Bonded
+ * forces are summed per atom in a fixed order (no atomics).  Callable before or after bind. */
+typedef struct {
+  int64_t n_atoms;
+  const int32_t* molecule;                 /* [n_atoms]                                 */
+  int64_t n_bonds;
+  const int32_t* bonds;                    /* [n_bonds][2]                              */
+  const int32_t* bond_type;                /* [n_bonds]                                 */
+  int32_t n_bond_types;
+  const double* bond_coeffs;               /* [n_bond_types][2] k, r0                   */
+  int64_t n_angles;
+  const int32_t* angles;                   /* [n_angles][3] i, j (vertex), k            */
+  const int32_t* angle_type;
+  int32_t n_angle_types;
+  const double* angle_coeffs;              /* [n_angle_types][2] k, theta0 (degrees)     */
+  int64_t n_dihedrals;
+  const int32_t* dihedrals;                /* [n_dihedrals][4]                          */
+  const int32_t* dihedral_type;
+  int32_t n_dihedral_types;
+  const double* dihedral_coeffs;           /* [n_dihedral_types][3] K, sign, multiplicity */
+} rbmd_topology;
+RBMD_API rbmd_status rbmd_force_set_topology(rbmd_force* f, const rbmd_topology* topology);
 
 /* Attach device atom arrays; sizes the cell grid, neighbour lists and k-space buffers.
  * Replaces ExecutionMD::Init (rbmd/framework/run/ExecutionMD.cpp:117-134). */
@@ -290,8 +331,8 @@ RBMD_API rbmd_status rbmd_force_get_far(rbmd_force* f, double* far_host);
 /* ---- LAMMPS data files (the reference's read_data input) ------------------------------------
  * rbmd_data_read parses a data file as ModelFileInitCondition does
  * (rbmd/framework/InitCondition/ModelFileInitCondition.cpp:120-605): header counts, Masses,
- * Pair Coeffs, Bond/Angle Coeffs, Atoms in style "atomic" | "charge" | "full", Bonds, Angles,
- * Velocities; ids, types and molecules 0-based, atoms ordered by id; unit "LJ" sets every mass
+ * Pair Coeffs, Bond/Angle/Dihedral Coeffs, Atoms in style "atomic" | "charge" | "full", Bonds,
+ * Angles, Dihedrals, Velocities; ids, types and molecules 0-based, atoms ordered by id; unit "LJ" sets every mass
  * to 1 as the reference does.  The accessors copy into caller-allocated host arrays (NULL skips
  * an array): positions/velocities [n][3], charge/mass [n], type/molecule [n], image flags [n][3]
  * (optional columns after the coordinates, 0 when absent), per-type masses / epsilon / sigma
@@ -304,6 +345,8 @@ typedef struct {
   int32_t n_atom_types, n_bond_types, n_angle_types;
   int32_t has_velocities, has_pair_coeffs, has_masses;
   rbmd_box box;
+  int64_t n_dihedrals;
+  int32_t n_dihedral_types;
 } rbmd_data_info;
 RBMD_API rbmd_status rbmd_data_read(const char* path, const char* atom_style, const char* unit, rbmd_data** out,
                                     rbmd_data_info* info);
@@ -312,6 +355,10 @@ RBMD_API rbmd_status rbmd_data_atoms(const rbmd_data* d, double* pos, double* ve
 RBMD_API rbmd_status rbmd_data_types(const rbmd_data* d, double* mass_by_type, double* epsilon, double* sigma);
 RBMD_API rbmd_status rbmd_data_topology(const rbmd_data* d, int32_t* bonds, int32_t* bond_type, int32_t* angles,
                                         int32_t* angle_type, double* bond_coeffs, double* angle_coeffs);
+/* Dihedrals [n_dihedrals][4] (caller atom ids), their types and the harmonic coefficients
+ * [n_dihedral_types][3] = (K, sign, multiplicity) of "Dihedral Coeffs". */
+RBMD_API rbmd_status rbmd_data_dihedrals(const rbmd_data* d, int32_t* dihedrals, int32_t* dihedral_type,
+                                         double* dihedral_coeffs);
 RBMD_API void rbmd_data_free(rbmd_data* d);
 RBMD_API rbmd_status rbmd_data_write(const char* path, const char* atom_style, const rbmd_data_info* info,
                                      const double* pos, const double* vel, const double* charge,

@@ -78,7 +78,9 @@ def neighbors(pos, lo, hi, cutoff, prec="fp32", cap=None, rs=None, original=Fals
 
 
 def near_force(pos, lo, hi, cutoff, nl, *, type=None, mol=None, charge=None, eps=(1.0,), sigma=(1.0,),
-               with_lj=True, with_coul=False, alpha=0.0, coul_scale=1.0, sum_mode=1, prec="fp32"):
+               with_lj=True, with_coul=False, alpha=0.0, coul_scale=1.0, sum_mode=1, prec="fp32", special=None):
+    """special = (off, ids, w) from special_lists: LJ pairs weighted by their special-bond weight
+    instead of the same-molecule exclusion."""
     dt, ct, sfx = _real(prec)
     x = np.ascontiguousarray(pos, dtype=dt)
     n = x.shape[0]
@@ -90,6 +92,14 @@ def near_force(pos, lo, hi, cutoff, nl, *, type=None, mol=None, charge=None, eps
     q = None if charge is None else np.ascontiguousarray(charge, dtype=np.float64)
     e = np.ascontiguousarray(eps, dtype=np.float64)
     s = np.ascontiguousarray(sigma, dtype=np.float64)
+    if special is not None:
+        so, si, sw = special
+        getattr(lib(), "oracle_near_sp_" + sfx)(
+            ctypes.c_int64(n), _p(x, ct), _p(np.asarray(lo, np.float64), D), _p(np.asarray(hi, np.float64), D),
+            D(cutoff), _p(t, I32), _p(q, D), len(e), _p(e, D), _p(s, D), ctypes.c_int64(cap),
+            _p(counts, I32), _p(ids, I32), _p(codes, I32), int(with_coul), D(alpha), D(coul_scale),
+            _p(so, ctypes.c_int64), _p(si, I32), _p(sw, D), _p(out, D))
+        return out
     getattr(lib(), "oracle_near_" + sfx)(
         ctypes.c_int64(n), _p(x, ct), _p(np.asarray(lo, np.float64), D), _p(np.asarray(hi, np.float64), D),
         D(cutoff), _p(t, I32), _p(m, I32), _p(q, D), len(e), _p(e, D), _p(s, D), ctypes.c_int64(cap),
@@ -240,7 +250,7 @@ def rbl_table_g(dis):
 
 def rbl_near(pos, lo, hi, cutoff, rs, pice, rl, core_cap, *, type=None, mol=None, charge=None, eps=(1.0,),
              sigma=(1.0,), with_coul=False, alpha=0.0, qqr2e=1.0, table_mode=0, shell_coul=1,
-             remove_mean=True, prec="fp32"):
+             remove_mean=True, prec="fp32", special=None):
     dt, ct, sfx = _real(prec)
     x = np.ascontiguousarray(pos, dtype=dt)
     n = x.shape[0]
@@ -250,6 +260,16 @@ def rbl_near(pos, lo, hi, cutoff, rs, pice, rl, core_cap, *, type=None, mol=None
     t = None if type is None else np.ascontiguousarray(type, dtype=np.int32)
     m = None if mol is None else np.ascontiguousarray(mol, dtype=np.int32)
     q = None if charge is None else np.ascontiguousarray(charge, dtype=np.float64)
+    if special is not None:
+        so, si, sw = special
+        getattr(lib(), "oracle_rbl_near_sp_" + sfx)(
+            ctypes.c_int64(n), _p(x, ct), _p(np.asarray(lo, np.float64), D), _p(np.asarray(hi, np.float64), D),
+            D(cutoff), D(rs), ctypes.c_int64(pice), _p(t, I32), _p(q, D),
+            _p(np.ascontiguousarray(eps, np.float64), D), _p(np.ascontiguousarray(sigma, np.float64), D),
+            ctypes.c_int64(core_cap), ctypes.c_int64(shell_cap), _p(ncore, I32), _p(nshell, I32), _p(ids, I32),
+            _p(codes, I32), int(with_coul), D(alpha), D(qqr2e), int(table_mode), int(shell_coul),
+            int(remove_mean), _p(so, ctypes.c_int64), _p(si, I32), _p(sw, D), _p(out, D))
+        return out
     getattr(lib(), "oracle_rbl_near_" + sfx)(
         ctypes.c_int64(n), _p(x, ct), _p(np.asarray(lo, np.float64), D), _p(np.asarray(hi, np.float64), D),
         D(cutoff), D(rs), ctypes.c_int64(pice), _p(t, I32), _p(m, I32), _p(q, D),
@@ -312,6 +332,48 @@ def water_extras(hoh, pos, charge, lo, hi, bond_k, bond_r0, angle_k, angle_t0):
                                   _p(np.asarray(lo, np.float64), D), _p(np.asarray(hi, np.float64), D),
                                   D(bond_k), D(bond_r0), D(angle_k), D(angle_t0), _p(out, D), _p(e, D))
     return out, e
+
+
+def special_lists(n, bonds, weights):
+    """Per-atom special-bond lists (off[n+1], ids, w) as ModelFileInitCondition::SetSpecialBonds
+    builds them, duplicates included."""
+    b = np.ascontiguousarray(bonds, np.int32).reshape(-1)
+    w3 = np.ascontiguousarray(weights, np.float64)
+    off = np.zeros(n + 1, np.int64)
+    cap = 0
+    while True:
+        ids = np.zeros(max(cap, 1), np.int32)
+        w = np.zeros(max(cap, 1))
+        m = lib().oracle_special_lists
+        m.restype = ctypes.c_int64
+        tot = m(ctypes.c_int64(n), ctypes.c_int64(len(b) // 2), _p(b, I32), _p(w3, D), ctypes.c_int64(cap),
+                _p(off, ctypes.c_int64), _p(ids, I32), _p(w, D))
+        if tot <= cap:
+            return off, ids[:tot], w[:tot]
+        cap = int(tot)
+
+
+def cvff_terms(pos, lo, hi, charge, mol, bonds, bond_type, bond_coeffs, angles, angle_type, angle_coeffs,
+               dihedrals=None, dihedral_type=None, dihedral_coeffs=None, special=None):
+    """FP64 CVFF intramolecular forces (special Coulomb, bonds, angles, dihedrals with special
+    lists) and energies {bond, angle, dihedral, special Coulomb}."""
+    x = np.ascontiguousarray(pos, np.float64)
+    n = x.shape[0]
+    out = np.zeros((n, 3))
+    e = np.zeros(4)
+    c = lambda a, t: None if a is None else np.ascontiguousarray(a, t)   # noqa: E731
+    b, bt, bc = c(bonds, np.int32), c(bond_type, np.int32), c(bond_coeffs, np.float64)
+    a, at, ac = c(angles, np.int32), c(angle_type, np.int32), c(angle_coeffs, np.float64)
+    d, dt_, dc = c(dihedrals, np.int32), c(dihedral_type, np.int32), c(dihedral_coeffs, np.float64)
+    so, si, sw = special if special is not None else (None, None, None)
+    lib().oracle_cvff_terms_f64(
+        ctypes.c_int64(n), _p(x, D), _p(np.asarray(lo, np.float64), D), _p(np.asarray(hi, np.float64), D),
+        _p(np.ascontiguousarray(charge, np.float64), D), _p(np.ascontiguousarray(mol, np.int32), I32),
+        ctypes.c_int64(0 if b is None else len(b)), _p(b, I32), _p(bt, I32), _p(bc, D),
+        ctypes.c_int64(0 if a is None else len(a)), _p(a, I32), _p(at, I32), _p(ac, D),
+        ctypes.c_int64(0 if d is None else len(d)), _p(d, I32), _p(dt_, I32), _p(dc, D),
+        _p(so, ctypes.c_int64), _p(si, I32), _p(sw, D), _p(out, D), _p(e, D))
+    return out, dict(bond=e[0], angle=e[1], dihedral=e[2], coul_special=e[3])
 
 
 def set_threads(n):

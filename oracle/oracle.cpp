@@ -419,6 +419,16 @@ EXPORT void oracle_cells_f32(int64_t n, const float* pos, const double* lo, cons
   if (upper) std::copy(c.upper.begin(), c.upper.end(), upper);
 }
 
+// Special-bond weight of pair (i, j): the LJ pair loops of ComputeSpecialBondsLJWorklet and
+// ComputeNearForceRBLERFSpecialBondsWorklet (RunWorklet.cpp:570-632, 816-933) scan i's whole
+// special list and keep the weight of the LAST entry whose id is j; 1 when j is absent.
+static double special_weight(const int64_t* off, const int32_t* ids, const double* w, int64_t i, int64_t j) {
+  double r = 1.0;
+  for (int64_t k = off[i]; k < off[i + 1]; ++k)
+    if (ids[k] == j) r = w[k];
+  return r;
+}
+
 // Near force over a full list: LJ (ComputeLJForceVerletWorklet, RunWorklet.cpp:239-303) and,
 // when with_coul, the Coulomb term of ComputeNearForceVerletWorklet (RunWorklet.cpp:170-237)
 // scaled by coul_scale (1.0 reproduces the reference's missing qqr2e; qqr2e gives the
@@ -430,7 +440,8 @@ static void near_impl(int64_t n, const Real* pos, const double* lo, const double
                       int ntypes, const double* eps, const double* sig, int64_t cap,
                       const int32_t* counts, const int32_t* ids, const int32_t* codes,
                       int with_lj, int with_coul, double alpha, double coul_scale, int sum_mode,
-                      double* force_out) {
+                      double* force_out, const int64_t* sp_off = nullptr, const int32_t* sp_ids = nullptr,
+                      const double* sp_w = nullptr) {
   Grid<Real> g = make_grid<Real>(lo, hi, cutoff, cutoff);
   const Real rc = (Real)cutoff, a = (Real)alpha;
   (void)ntypes;
@@ -459,11 +470,15 @@ static void near_impl(int64_t n, const Real* pos, const double* lo, const double
           if (sum_mode == 0) el[d] += fs; else eld[d] += (double)fs;
         }
       }
-      if (!with_lj || mi == mj) continue;
+      if (!with_lj || (!sp_off && mi == mj)) continue;
       Real r[3];
       min_dist(pj, pi, g.box, r);
       Real f[3];
       lj_force(r, eps_i, (Real)eps[tj], sig_i, (Real)sig[tj], rc, f);
+      if (sp_off) {
+        const Real w = (Real)special_weight(sp_off, sp_ids, sp_w, i, j);
+        for (int d = 0; d < 3; ++d) f[d] = w * f[d];
+      }
       for (int d = 0; d < 3; ++d) {
         if (sum_mode == 0) lj[d] += f[d]; else ljd[d] += (double)f[d];
       }
@@ -481,6 +496,26 @@ EXPORT void oracle_near_f32(int64_t n, const float* pos, const double* lo, const
                             double coul_scale, int sum_mode, double* force_out) {
   near_impl<float>(n, pos, lo, hi, cutoff, type, mol, charge, ntypes, eps, sig, cap, counts, ids,
                    codes, with_lj, with_coul, alpha, coul_scale, sum_mode, force_out);
+}
+// The same with special-bond LJ weights (no same-molecule exclusion): sp_off[n+1], sp_ids,
+// sp_w are the per-atom special lists of ModelFileInitCondition::SetSpecialBonds.
+EXPORT void oracle_near_sp_f32(int64_t n, const float* pos, const double* lo, const double* hi,
+                               double cutoff, const int32_t* type, const double* charge, int ntypes,
+                               const double* eps, const double* sig, int64_t cap, const int32_t* counts,
+                               const int32_t* ids, const int32_t* codes, int with_coul, double alpha,
+                               double coul_scale, const int64_t* sp_off, const int32_t* sp_ids,
+                               const double* sp_w, double* force_out) {
+  near_impl<float>(n, pos, lo, hi, cutoff, type, nullptr, charge, ntypes, eps, sig, cap, counts, ids,
+                   codes, 1, with_coul, alpha, coul_scale, 1, force_out, sp_off, sp_ids, sp_w);
+}
+EXPORT void oracle_near_sp_f64(int64_t n, const double* pos, const double* lo, const double* hi,
+                               double cutoff, const int32_t* type, const double* charge, int ntypes,
+                               const double* eps, const double* sig, int64_t cap, const int32_t* counts,
+                               const int32_t* ids, const int32_t* codes, int with_coul, double alpha,
+                               double coul_scale, const int64_t* sp_off, const int32_t* sp_ids,
+                               const double* sp_w, double* force_out) {
+  near_impl<double>(n, pos, lo, hi, cutoff, type, nullptr, charge, ntypes, eps, sig, cap, counts, ids,
+                    codes, 1, with_coul, alpha, coul_scale, 1, force_out, sp_off, sp_ids, sp_w);
 }
 EXPORT void oracle_near_f64(int64_t n, const double* pos, const double* lo, const double* hi,
                             double cutoff, const int32_t* type, const int32_t* mol,
@@ -1246,6 +1281,189 @@ EXPORT void oracle_water_extras_f64(int64_t n_mol, const int32_t* hoh, const dou
   if (e_out) { e_out[0] = eb; e_out[1] = ea; }
 }
 
+// Special-bond partner lists of ModelFileInitCondition::SetSpecialBonds
+// (rbmd/framework/InitCondition/ModelFileInitCondition.cpp:850-910): the bond graph as a multimap
+// filled in Bonds order (both directions, :509-511); for each atom in id order its 1-2 partners
+// (weight w3[0]), through each of them the 1-3 partners other than the atom itself (w3[1]) and
+// through those the 1-4 partners other than the 1-2 atom they came from (w3[2]); an atom without
+// bonds gets the single entry (itself, 1.0).  Duplicates are kept, as in the reference.  Writes
+// off[n+1], ids/wts up to cap entries; returns the number of entries.
+EXPORT int64_t oracle_special_lists(int64_t n, int64_t nb, const int32_t* bonds, const double* w3, int64_t cap,
+                                    int64_t* off, int32_t* ids, double* wts) {
+  std::vector<std::vector<int32_t>> adj(n);
+  for (int64_t b = 0; b < nb; ++b) {
+    adj[bonds[2 * b]].push_back(bonds[2 * b + 1]);
+    adj[bonds[2 * b + 1]].push_back(bonds[2 * b]);
+  }
+  int64_t m = 0;
+  auto put = [&](int32_t id, double w) {
+    if (m < cap) { ids[m] = id; wts[m] = w; }
+    ++m;
+  };
+  for (int64_t a = 0; a < n; ++a) {
+    off[a] = m;
+    if (adj[a].empty()) { put((int32_t)a, 1.0); continue; }
+    for (int32_t k1 : adj[a]) {
+      put(k1, w3[0]);
+      for (int32_t k2 : adj[k1]) {
+        if (k2 == a) continue;
+        put(k2, w3[1]);
+        for (int32_t k3 : adj[k2]) {
+          if (k3 == k1) continue;
+          put(k3, w3[2]);
+        }
+      }
+    }
+  }
+  off[n] = m;
+  return m;
+}
+
+// Harmonic dihedral of ComputeDihedralHarmonicWorklet::ComputeijDihedralHarmonicEnergyForce
+// (rbmd/framework/run/worklet/MolecularWorklet.h:555-818): E = K [1 + d cos(n phi)] with
+// cos_shift = d = +-1, sin_shift = 0, cos(n phi) by the angle-addition recursion.
+static double dihedral_harmonic(const double* pi, const double* pj, const double* pk, const double* pw,
+                                const double* box, double K, int sign, int mult, double f[4][3]) {
+  double vb1[3], vb2[3], vb3[3], vb2m[3];
+  md(pi, pj, box, vb1);
+  md(pk, pj, box, vb2);
+  for (int d = 0; d < 3; ++d) vb2m[d] = -vb2[d];
+  md(pw, pk, box, vb3);
+  const double ax = vb1[1] * vb2m[2] - vb1[2] * vb2m[1];
+  const double ay = vb1[2] * vb2m[0] - vb1[0] * vb2m[2];
+  const double az = vb1[0] * vb2m[1] - vb1[1] * vb2m[0];
+  const double bx = vb3[1] * vb2m[2] - vb3[2] * vb2m[1];
+  const double by = vb3[2] * vb2m[0] - vb3[0] * vb2m[2];
+  const double bz = vb3[0] * vb2m[1] - vb3[1] * vb2m[0];
+  const double rasq = ax * ax + ay * ay + az * az;
+  const double rbsq = bx * bx + by * by + bz * bz;
+  const double rgsq = vb2m[0] * vb2m[0] + vb2m[1] * vb2m[1] + vb2m[2] * vb2m[2];
+  const double rg = std::sqrt(rgsq);
+  const double rginv = rg > 0 ? 1.0 / rg : 0.0;
+  const double ra2inv = rasq > 0 ? 1.0 / rasq : 0.0;
+  const double rb2inv = rbsq > 0 ? 1.0 / rbsq : 0.0;
+  const double rabinv = std::sqrt(ra2inv * rb2inv);
+  double c = (ax * bx + ay * by + az * bz) * rabinv;
+  const double s = rg * rabinv * (ax * vb3[0] + ay * vb3[1] + az * vb3[2]);
+  c = std::min(1.0, std::max(-1.0, c));
+  const double cos_shift = sign == 1 ? 1.0 : -1.0, sin_shift = 0.0;
+  double p = 1.0, ddf1 = 0.0, df1 = 0.0;
+  for (int i = 0; i < mult; ++i) {
+    ddf1 = p * c - df1 * s;
+    df1 = p * s + df1 * c;
+    p = ddf1;
+  }
+  p = p * cos_shift + df1 * sin_shift;
+  df1 = df1 * cos_shift - ddf1 * sin_shift;
+  df1 *= -mult;
+  p += 1.0;
+  if (mult == 0) { p = 1.0 + cos_shift; df1 = 0.0; }
+  const double fg = vb1[0] * vb2m[0] + vb1[1] * vb2m[1] + vb1[2] * vb2m[2];
+  const double hg = vb3[0] * vb2m[0] + vb3[1] * vb2m[1] + vb3[2] * vb2m[2];
+  const double fga = fg * ra2inv * rginv, hgb = hg * rb2inv * rginv;
+  const double gaa = -ra2inv * rg, gbb = rb2inv * rg;
+  const double dtf[3] = {gaa * ax, gaa * ay, gaa * az};
+  const double dtg[3] = {fga * ax - hgb * bx, fga * ay - hgb * by, fga * az - hgb * bz};
+  const double dth[3] = {gbb * bx, gbb * by, gbb * bz};
+  const double df = -K * df1;
+  for (int d = 0; d < 3; ++d) {
+    const double s2 = df * dtg[d];
+    f[0][d] = df * dtf[d];
+    f[1][d] = s2 - f[0][d];
+    f[3][d] = df * dth[d];
+    f[2][d] = -s2 - f[3][d];
+  }
+  return K * p;
+}
+
+// CVFF intramolecular terms of ExecutionNVT::ComputeAllForce (ExecutionNVT.cpp:199-215), added to
+// force_out in the reference's order: special Coulomb (ComputeSpecialCoulWorklet /
+// ComputeSpecialCoulGeneralWorklet, RunWorklet.cpp:1386-1511: for every other member j of the
+// atom's molecule when the molecule has >= 3 atoms, -332.06371 q_i q_j r_ij / r^3 times 1, or
+// times (1 - w_ij) with special lists), harmonic bonds k (r - r0)^2 (ComputeBondHarmonicWorklet),
+// harmonic angles k (theta - theta0)^2 (ComputeAngleHarmonicWorklet), and, with special lists,
+// harmonic dihedrals.  Coefficients per type: bonds (k, r0), angles (k, theta0 in degrees),
+// dihedrals (K, sign, multiplicity).  e_out = {bond, angle, dihedral, special Coulomb} sums.
+EXPORT void oracle_cvff_terms_f64(int64_t n, const double* pos, const double* lo, const double* hi,
+                                  const double* charge, const int32_t* mol, int64_t nb, const int32_t* bonds,
+                                  const int32_t* btype, const double* bcoef, int64_t na, const int32_t* angles,
+                                  const int32_t* atype, const double* acoef, int64_t nd, const int32_t* dih,
+                                  const int32_t* dtype, const double* dcoef, const int64_t* sp_off,
+                                  const int32_t* sp_ids, const double* sp_w, double* force_out, double* e_out) {
+  const double box[3] = {hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]};
+  double eb = 0, ea = 0, ed = 0, es = 0;
+  // molecule groups
+  int32_t mmax = 0;
+  for (int64_t i = 0; i < n; ++i) mmax = std::max(mmax, mol[i]);
+  std::vector<std::vector<int32_t>> group((size_t)mmax + 1);
+  for (int64_t i = 0; i < n; ++i) group[mol[i]].push_back((int32_t)i);
+  std::vector<double> fsc(3 * n, 0.0), fb(3 * n, 0.0), fa(3 * n, 0.0), fd(3 * n, 0.0);
+  for (int64_t i = 0; i < n; ++i) {
+    const auto& g = group[mol[i]];
+    if (g.size() < 3) continue;
+    for (int32_t j : g) {
+      if (j == i) continue;
+      double r[3];
+      md(pos + 3 * i, pos + 3 * j, box, r);
+      const double d = std::sqrt(dot3(r, r));
+      const double fac = sp_off ? 1.0 - special_weight(sp_off, sp_ids, sp_w, i, j) : 1.0;
+      const double fc = -332.06371 * charge[i] * charge[j] / (d * d * d);
+      for (int k = 0; k < 3; ++k) fsc[3 * i + k] += fac * fc * r[k];
+      es += -0.5 * fac * 332.06371 * charge[i] * charge[j] / d;
+    }
+  }
+  for (int64_t b = 0; b < nb; ++b) {
+    const int32_t i = bonds[2 * b], j = bonds[2 * b + 1];
+    const double k = bcoef[2 * btype[b]], r0 = bcoef[2 * btype[b] + 1];
+    double r[3];
+    md(pos + 3 * i, pos + 3 * j, box, r);
+    const double d = std::sqrt(dot3(r, r));
+    const double dr = d - r0, rk = k * dr;
+    const double f = d > 0.01 ? -2.0 * rk / d : 0.0;
+    for (int c = 0; c < 3; ++c) { fb[3 * i + c] += f * r[c]; fb[3 * j + c] -= f * r[c]; }
+    eb += rk * dr;
+  }
+  for (int64_t a = 0; a < na; ++a) {
+    const int32_t i = angles[3 * a], j = angles[3 * a + 1], l = angles[3 * a + 2];
+    const double k = acoef[2 * atype[a]], t0 = acoef[2 * atype[a] + 1] * M_PI / 180.0;
+    double rij[3], rkj[3];
+    md(pos + 3 * i, pos + 3 * j, box, rij);
+    md(pos + 3 * l, pos + 3 * j, box, rkj);
+    const double dij2 = dot3(rij, rij), dij = std::sqrt(dij2), dkj2 = dot3(rkj, rkj), dkj = std::sqrt(dkj2);
+    double c = dot3(rij, rkj) / (dij * dkj);
+    c = std::min(1.0, std::max(-1.0, c));
+    double s = std::sqrt(1.0 - c * c);
+    if (s < 0.001) s = 0.001;
+    s = 1.0 / s;
+    const double dth = std::acos(c) - t0, tk = k * dth;
+    ea += tk * dth;
+    const double aa = -2.0 * tk * s, a11 = aa * c / dij2, a12 = -aa / (dij * dkj), a22 = aa * c / dkj2;
+    for (int q = 0; q < 3; ++q) {
+      const double fi = a11 * rij[q] + a12 * rkj[q], fk = a22 * rkj[q] + a12 * rij[q];
+      fa[3 * i + q] += fi;
+      fa[3 * j + q] += -fi - fk;
+      fa[3 * l + q] += fk;
+    }
+  }
+  if (sp_off)
+    for (int64_t t = 0; t < nd; ++t) {
+      const int32_t* q = dih + 4 * t;
+      const double* cf = dcoef + 3 * dtype[t];
+      double f[4][3];
+      ed += dihedral_harmonic(pos + 3 * q[0], pos + 3 * q[1], pos + 3 * q[2], pos + 3 * q[3], box, cf[0],
+                              (int)cf[1], (int)cf[2], f);
+      for (int a = 0; a < 4; ++a)
+        for (int d = 0; d < 3; ++d) fd[3 * q[a] + d] += f[a][d];
+    }
+  for (int64_t i = 0; i < 3 * n; ++i) {
+    force_out[i] += fsc[i];
+    force_out[i] += fb[i];
+    force_out[i] += fa[i];
+    force_out[i] += fd[i];
+  }
+  if (e_out) { e_out[0] = eb; e_out[1] = ea; e_out[2] = ed; e_out[3] = es; }
+}
+
 EXPORT int oracle_num_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();
@@ -1396,7 +1614,9 @@ static void rbl_near_impl(int64_t n, const Real* pos, const double* lo, const do
                           const double* sig, int64_t core_cap, int64_t shell_cap,
                           const int32_t* ncore, const int32_t* nshell, const int32_t* ids,
                           const int32_t* codes, int with_coul, double alpha, double qqr2e,
-                          int table_mode, int shell_coul, int remove_mean, double* force_out) {
+                          int table_mode, int shell_coul, int remove_mean, double* force_out,
+                          const int64_t* sp_off = nullptr, const int32_t* sp_ids = nullptr,
+                          const double* sp_w = nullptr) {
   Grid<Real> g = make_grid<Real>(lo, hi, cutoff, rs);
   const Real rc = (Real)cutoff, r_s = (Real)rs, a = (Real)alpha;
   const int64_t row = core_cap + shell_cap;
@@ -1433,7 +1653,7 @@ static void rbl_near_impl(int64_t n, const Real* pos, const double* lo, const do
           for (int d = 0; d < 3; ++d) el[d] += (double)(w * (sc * r[d] / dis));
         }
       }
-      if (mi == mj) return;
+      if (!sp_off && mi == mj) return;
       Real f[3] = {0, 0, 0};
       if (!shell) {
         lj_force(rm, eps_i, (Real)eps[tj], sig_i, (Real)sig[tj], rc, f);
@@ -1447,6 +1667,10 @@ static void rbl_near_impl(int64_t n, const Real* pos, const double* lo, const do
           Real scal = (Real)(-24) * (Real)std::sqrt(eps_i * (Real)eps[tj]) * (((Real)2 * sd6 - (Real)1) * sd6) / d2;
           for (int d = 0; d < 3; ++d) f[d] = (Real)pice * (scal * rm[d]);
         }
+      }
+      if (sp_off) {
+        const Real w = (Real)special_weight(sp_off, sp_ids, sp_w, i, j);
+        for (int d = 0; d < 3; ++d) f[d] = w * f[d];
       }
       for (int d = 0; d < 3; ++d) lj[d] += (double)f[d];
     };
@@ -1611,6 +1835,31 @@ EXPORT void oracle_rbl_near_f64(int64_t n, const double* pos, const double* lo, 
                         ncore, nshell, ids, codes, with_coul, alpha, qqr2e, table_mode, shell_coul,
                         remove_mean, out);
 }
+// RBL near force with special-bond LJ weights (ComputeNearForceRBLERFSpecialBondsWorklet,
+// RunWorklet.cpp:816-933): no same-molecule exclusion, the LJ pair force times its weight.
+EXPORT void oracle_rbl_near_sp_f32(int64_t n, const float* pos, const double* lo, const double* hi, double cutoff,
+                                   double rs, int64_t pice, const int32_t* type, const double* charge,
+                                   const double* eps, const double* sig, int64_t core_cap, int64_t shell_cap,
+                                   const int32_t* ncore, const int32_t* nshell, const int32_t* ids,
+                                   const int32_t* codes, int with_coul, double alpha, double qqr2e, int table_mode,
+                                   int shell_coul, int remove_mean, const int64_t* sp_off, const int32_t* sp_ids,
+                                   const double* sp_w, double* out) {
+  rbl_near_impl<float>(n, pos, lo, hi, cutoff, rs, pice, type, nullptr, charge, eps, sig, core_cap, shell_cap,
+                       ncore, nshell, ids, codes, with_coul, alpha, qqr2e, table_mode, shell_coul, remove_mean,
+                       out, sp_off, sp_ids, sp_w);
+}
+EXPORT void oracle_rbl_near_sp_f64(int64_t n, const double* pos, const double* lo, const double* hi, double cutoff,
+                                   double rs, int64_t pice, const int32_t* type, const double* charge,
+                                   const double* eps, const double* sig, int64_t core_cap, int64_t shell_cap,
+                                   const int32_t* ncore, const int32_t* nshell, const int32_t* ids,
+                                   const int32_t* codes, int with_coul, double alpha, double qqr2e, int table_mode,
+                                   int shell_coul, int remove_mean, const int64_t* sp_off, const int32_t* sp_ids,
+                                   const double* sp_w, double* out) {
+  rbl_near_impl<double>(n, pos, lo, hi, cutoff, rs, pice, type, nullptr, charge, eps, sig, core_cap, shell_cap,
+                        ncore, nshell, ids, codes, with_coul, alpha, qqr2e, table_mode, shell_coul, remove_mean,
+                        out, sp_off, sp_ids, sp_w);
+}
+
 EXPORT int oracle_rbl_eam_f32(const char* path, int64_t n, const float* pos, const double* lo, const double* hi,
                               double cutoff, double rs, int64_t pice, int64_t core_cap, int64_t shell_cap,
                               const int32_t* ncore, const int32_t* nshell, const int32_t* ids,
