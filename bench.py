@@ -61,7 +61,7 @@ def parse():
     ap.add_argument("--ion-frac", type=float, default=0.1,
                     help="fraction of charged atoms of the electrolyte (0.1 is the headline workload)")
     ap.add_argument("--workload", default="electrolyte",
-                    choices=["electrolyte", "lj", "water", "eam", "batched"],
+                    choices=["electrolyte", "lj", "water", "eam", "batched", "molecular"],
                     help="electrolyte: the headline metric (default); the others time the remaining "
                          "configurations (plain MD steps, atom-steps/s) beside the CPU oracle")
     ap.add_argument("--skin", type=float, default=0.3,
@@ -545,6 +545,18 @@ def config_system(name, tmpdir):
         cfg["hyper_parameters"]["neighbor"]["skin"] = 0.3
         return s, cfg, None, None, ("Johnson EAM Cu FCC 256000 atoms (5000-point funcfl), rc 5.0 A + skin 0.3, "
                                     "300 K displacements, FP32, NVE")
+    if name == "molecular":
+        # the shape of the reference's polymer-electrolyte input (rbmd/res/json_files/PEO): CVFF
+        # with bonds, angles, dihedrals and special bonds 0/0/0, RBL rc 12 A / r_core 6 A / 100
+        # samples, RBE P=100 at alpha 0.074, REAL units, 0.5 fs, Berendsen
+        s = systems.molecular(n_chain=8000, chain_len=12, n_ion_pairs=800, step=1.5, cell=6.0, seed=31)
+        cfg = systems.molecular_config(P=100, cutoff=12.0, alpha=0.074, neighbor="RBL", special=(0.0, 0.0, 0.0),
+                                       dt=0.5, precision="fp32", r_core=6.0, sample_num=100)
+        cfg["execution"].update({"ensemble": "NVT", "temp_ctrl_type": "BERENDSEN",
+                                 "temperature": [298.0, 298.0, 100.0]})
+        return s, cfg, None, None, (f"flexible chains + ions, {len(s['pos'])} atoms (8000 chains of 12, 800 ion "
+                                    "pairs, 0.041 atoms/A^3), bonds/angles/dihedrals, special bonds 0/0/0, RBL "
+                                    "rc 12 A r_core 6 A 100 samples, RBE P=100, REAL units, FP32 forces")
     r = systems.replicas(n_rep=512, seed=11)
     cfg = systems.electrolyte_config(P=100, precision="fp32", ensemble="NVE")
     cfg["hyper_parameters"]["neighbor"]["skin"] = 0.3
@@ -572,6 +584,23 @@ def cpu_config_eval(name, s, cfg, offsets, tmpdir):
         return total, atoms
     pos = s["pos"].astype(np.float32 if prec == "fp32" else np.float64)
     L = s["hi"] - s["lo"]
+    if name == "molecular":
+        nb, co = hp["neighbor"], hp["coulomb"]
+        t0 = time.perf_counter()
+        _, _, pice = oracle.rbl_sizes(len(pos), s["lo"], s["hi"], nb["r_core"], rc, nb["neighbor_sample_num"],
+                                      prec=prec)
+        sp = oracle.special_lists(len(pos), s["bonds"], hp["extend"]["special_bonds"])
+        rl = oracle.rbl_list(pos, s["lo"], s["hi"], rc, nb["r_core"], pice, 128, 160, prec=prec)
+        oracle.rbl_near(pos, s["lo"], s["hi"], rc, nb["r_core"], pice, rl, 128, type=s["type"], charge=s["charge"],
+                        eps=s["eps"], sigma=s["sigma"], with_coul=True, alpha=co["alpha"], qqr2e=332.06371,
+                        prec=prec, special=sp)
+        m = oracle.rbe_sample(co["alpha"], L, 7, 0, 0, co["coulomb_sample_num"])
+        rho = oracle.rhok(pos, s["charge"], L, m, prec=prec)
+        oracle.rbe_force(pos, s["charge"], L, co["alpha"], 332.06371, m, rho, prec=prec)
+        oracle.cvff_terms(s["pos"], s["lo"], s["hi"], s["charge"], s["molecule"], s["bonds"], s["bond_type"],
+                          s["bond_coeffs"], s["angles"], s["angle_type"], s["angle_coeffs"], s["dihedrals"],
+                          s["dihedral_type"], s["dihedral_coeffs"], special=sp)
+        return time.perf_counter() - t0, len(pos)
     t0 = time.perf_counter()
     nl = oracle.neighbors(pos, s["lo"], s["hi"], rc, prec)
     if name == "eam":
@@ -615,6 +644,10 @@ def run_config(args):
         ff.set_pair_coeffs(s["eps"], s["sigma"])
         if "hoh" in s:
             ff.set_water(s["hoh"], s["bond"][0], s["bond"][1], s["angle"][0], s["angle"][1])
+        if "bonds" in s:
+            ff.set_topology(s["molecule"], s["bonds"], s["bond_type"], s["bond_coeffs"], s["angles"],
+                            s["angle_type"], s["angle_coeffs"], s["dihedrals"], s["dihedral_type"],
+                            s["dihedral_coeffs"])
         ff.Init(t["pos"], t["force"], vel=t["vel"], mass=t["mass"], charge=t["charge"], type=t["type"],
                 molecule=t.get("molecule"), image=t["image"], replica_offsets=offs)
         run = timed_run(ff, t, dev, args.steps, args.warmup, 1, None, args.e2e_steps)
@@ -648,7 +681,8 @@ def run_config(args):
                 res[th] = atoms / sec
             line["cpu_baseline"] = {"value": res[cores], "unit": "atom-steps/s", "cores": cores, "kind": "port",
                                     "single_thread": res[1],
-                                    "sample": "one force evaluation (list + pair terms (+ RBE, water extras)) "
+                                    "sample": "one force evaluation (list + pair terms (+ RBE, water extras, "
+                                              "CVFF terms)) "
                                               "of the same system by the FP32/FP64 oracle restatement"
                                               + (", first 16 replicas" if args.workload == "batched" else "")}
     return line

@@ -88,6 +88,131 @@ __global__ void __launch_bounds__(128) k_rbl_list(
   }
 }
 
+// The same list with one warp per atom (systems of 10^4 - 10^5 atoms leave the thread-per-atom
+// build with a few thousand warps of long serial loops).  The (2 num_cycles + 1)^3 stencil cells
+// are laid out in the reference's walk order in shared memory (first slot, number of candidates
+// before the cell, periodic wrap count per axis), which flattens the atom's candidates into one
+// sequence; each round the warp's lanes take 32 consecutive candidates (cell found by binary
+// search over the running counts), classify them with the same predicates and arithmetic, and a
+// ballot prefix gives each shell pair its running index and each kept / core pair its row, so the
+// list is identical entry for entry to k_rbl_list's.
+constexpr int kRblStencilMax = 343;   // num_cycles <= 3
+constexpr int kRblWarps = 4;
+
+template <class R>
+__global__ void __launch_bounds__(32 * kRblWarps) k_rbl_list_warp(
+    int n, const typename Traits<R>::V4* __restrict__ pos4, const int* __restrict__ cell_start,
+    const RepDev* __restrict__ reps, const int* __restrict__ rep_of_slot, int num_cycles, R rc, R rs,
+    int core_cap, int shell_cap, int stride, int* __restrict__ nbr, int* __restrict__ ncore,
+    int* __restrict__ nshell, int* __restrict__ max_count, uint32_t* status) {
+  __shared__ int s_start[kRblWarps][kRblStencilMax];
+  __shared__ int s_pre[kRblWarps][kRblStencilMax + 1];
+  __shared__ int s_wrap[kRblWarps][kRblStencilMax];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = blockIdx.x * kRblWarps + w;
+  if (i >= n) return;   // uniform across the warp
+  const unsigned full = 0xffffffffu;
+  const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
+  const int pice = rp.rbl_pice;
+  const typename Traits<R>::V4 pi = pos4[i];
+  const R pix[3] = {pi.x, pi.y, pi.z};
+  int ci[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    ci[d] = (int)div_rn(sub_rn(pix[d], Traits<R>::lo(rp, d)), Traits<R>::dx(rp, d));
+  const R rc2 = mul_rn(rc, rc), rs2 = mul_rn(rs, rs);
+  const int nc = num_cycles, side = 2 * num_cycles + 1, ncs = side * side * side;
+  const int dims[3] = {rp.dims[0], rp.dims[1], rp.dims[2]};
+  // stencil table: cell k = ((a + nc) * side + (b + nc)) * side + (c + nc), x outermost
+  int carry = 0;
+  for (int k0 = 0; k0 < ncs; k0 += 32) {
+    const int k = k0 + lane;
+    int cnt = 0;
+    if (k < ncs) {
+      const int off[3] = {k / (side * side) - nc, (k / side) % side - nc, k % side - nc};
+      int wr[3], q = 0;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const int nb = ci[d] + off[d];
+        wr[d] = ((nb % dims[d]) + dims[d]) % dims[d];
+        q |= (((wr[d] - nb) / dims[d]) & 0xff) << (8 * d);   // wrap count (wx - nbx) / dims
+      }
+      const int cell = rp.cell_base + wr[0] + wr[1] * dims[0] + wr[2] * dims[0] * dims[1];
+      const int s0 = cell_start[cell];
+      cnt = cell_start[cell + 1] - s0;
+      s_start[w][k] = s0;
+      s_wrap[w][k] = q;
+    }
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(full, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (k < ncs) s_pre[w][k] = carry + incl - cnt;
+    carry += __shfl_sync(full, incl, 31);
+  }
+  if (lane == 0) s_pre[w][ncs] = carry;
+  __syncwarp();
+  const int total = carry;
+  const unsigned lt = (1u << lane) - 1u;
+  int n_core = 0, n_shell = 0, shell_index = 0;
+  for (int base = 0; base < total; base += 32) {
+    const int k = base + lane;
+    bool shell = false, core = false;
+    int entry = 0;
+    if (k < total) {
+      int lo = 0, hi = ncs;   // s_pre[lo] <= k < s_pre[hi]
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (s_pre[w][mid] <= k) lo = mid;
+        else hi = mid;
+      }
+      const int sj = s_start[w][lo] + (k - s_pre[w][lo]);
+      const int q = s_wrap[w][lo];
+      const int dd[3] = {(int)(signed char)(q & 0xff) * dims[0], (int)(signed char)((q >> 8) & 0xff) * dims[1],
+                         (int)(signed char)((q >> 16) & 0xff) * dims[2]};
+      const R off0 = mul_rn(Traits<R>::dx(rp, 0), (R)dd[0]);
+      const R off1 = mul_rn(Traits<R>::dx(rp, 1), (R)dd[1]);
+      const R off2 = mul_rn(Traits<R>::dx(rp, 2), (R)dd[2]);
+      const int code = (dd[0] > 0 ? 1 : (dd[0] < 0 ? 2 : 0)) | ((dd[1] > 0 ? 1 : (dd[1] < 0 ? 2 : 0)) << 2) |
+                       ((dd[2] > 0 ? 1 : (dd[2] < 0 ? 2 : 0)) << 4);
+      const typename Traits<R>::V4 pj = pos4[sj];
+      const R r0 = sub_rn(sub_rn(pj.x, off0), pix[0]);
+      const R r1 = sub_rn(sub_rn(pj.y, off1), pix[1]);
+      const R r2 = sub_rn(sub_rn(pj.z, off2), pix[2]);
+      const R d2 = add_rn(add_rn(mul_rn(r0, r0), mul_rn(r1, r1)), mul_rn(r2, r2));
+      shell = gt_small(sub_rn(rc2, d2)) && gt_small(sub_rn(d2, rs2));
+      core = !shell && gt_small(sub_rn(rs2, d2)) && gt_small(d2);
+      entry = (sj << kShiftBits) | code;
+    }
+    const unsigned bsh = __ballot_sync(full, shell);
+    const bool keep = shell && ((shell_index + __popc(bsh & lt)) % pice == 0);
+    const unsigned bkeep = __ballot_sync(full, keep);
+    const unsigned bcore = __ballot_sync(full, core);
+    if (keep) {
+      const int at = n_shell + __popc(bkeep & lt);
+      if (at < shell_cap) nbr[(size_t)(core_cap + at) * stride + i] = entry;
+    }
+    if (core) {
+      const int at = n_core + __popc(bcore & lt);
+      if (at < core_cap) nbr[(size_t)at * stride + i] = entry;
+    }
+    shell_index += __popc(bsh);
+    n_shell += __popc(bkeep);
+    n_core += __popc(bcore);
+  }
+  if (lane == 0) {
+    ncore[i] = n_core;
+    nshell[i] = n_shell;
+    if (n_core > core_cap || n_shell > shell_cap) {
+      set_flag(status, kFlagListOverflow);
+      atomicMax(max_count, n_core);
+      atomicMax(max_count + 1, n_shell);
+    }
+  }
+}
+
 struct RblParams {
   int n, stride, ntypes, core_cap, molecular;
   int table_mode;   // 1: G from the reference's ERF table (alpha 0.1, one value per bucket)
@@ -117,7 +242,9 @@ __device__ __forceinline__ float rbl_table_g(const float* __restrict__ tab, floa
 // rs^2 < d^2 < rc^2 (ComputeLJForceRcs) and, unless dropped, Coulomb x pice on the same range.
 // The result is the reference's corr_force = LJ + qqr2e * Coulomb; k_force_sub_mean removes its
 // mean afterwards.
-template <class R, bool COUL, bool SPW>
+// G > 1: G lanes per atom (small systems, where one thread per atom leaves most SMs idle); lane
+// s takes entries s, s + G, ... and the lanes' sums are combined in FP64 by a fixed butterfly.
+template <class R, bool COUL, bool SPW, int G>
 __global__ void __launch_bounds__(128) k_rbl_force(
     RblParams prm, const LJTable* __restrict__ ljt, const typename Traits<R>::V4* __restrict__ pos4,
     const int2* __restrict__ meta, const int* __restrict__ nbr, const int* __restrict__ ncore,
@@ -132,8 +259,11 @@ __global__ void __launch_bounds__(128) k_rbl_force(
     lj_s6[t] = sig6<R>(*ljt, t);
   }
   __syncthreads();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= prm.n) return;
+  const int gid = (int)((blockIdx.x * blockDim.x + threadIdx.x) / G);
+  const int sub = G == 1 ? 0 : (int)(threadIdx.x % G);
+  if (G == 1 && gid >= prm.n) return;
+  const bool active = gid < prm.n;   // inactive lanes of a partial group still join the shuffles
+  const int i = active ? gid : prm.n - 1;
   const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
   const R pice = (R)rp.rbl_pice;
   const V4 pi = pos4[i];
@@ -151,8 +281,9 @@ __global__ void __launch_bounds__(128) k_rbl_force(
   const size_t st = (size_t)prm.stride;
   Acc<R> fx, fy, fz;
   double e_lj = 0, e_coul = 0;
-  const int nco = min(ncore[i], prm.core_cap), nsh = min(nshell[i], shell_cap);
-  for (int p = 0; p < nco + nsh; ++p) {
+  const int nco = min(ncore[i], prm.core_cap), nsh = active ? min(nshell[i], shell_cap) : 0;
+  const int nall = active ? nco + nsh : 0;
+  for (int p = sub; p < nall; p += G) {
     const bool shell = p >= nco;
     const int row = shell ? prm.core_cap + (p - nco) : p;
     const int e = __ldg(nbr + (size_t)row * st + i);
@@ -220,7 +351,18 @@ __global__ void __launch_bounds__(128) k_rbl_force(
     }
     fx.add(t0); fy.add(t1); fz.add(t2);
   }
-  const double F[3] = {fx.value(), fy.value(), fz.value()};
+  double F[3] = {fx.value(), fy.value(), fz.value()};
+  if (G > 1) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) {
+      F[0] += __shfl_xor_sync(0xffffffffu, F[0], o);
+      F[1] += __shfl_xor_sync(0xffffffffu, F[1], o);
+      F[2] += __shfl_xor_sync(0xffffffffu, F[2], o);
+      e_lj += __shfl_xor_sync(0xffffffffu, e_lj, o);
+      e_coul += __shfl_xor_sync(0xffffffffu, e_coul, o);
+    }
+    if (!active || sub != 0) return;
+  }
   if (!isfinite(F[0]) || !isfinite(F[1]) || !isfinite(F[2])) set_flag(status, kFlagNonFinite);
   const int id = slot_atom[i];
   force[3 * id] = F[0];

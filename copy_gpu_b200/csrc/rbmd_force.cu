@@ -117,6 +117,9 @@ struct rbmd_force {
   int energy_every = 0;   // energies inside step(): every outputs.thermo_out.interval steps
   int cap_override = 0;   // neighbor.capacity: initial list capacity (grown on overflow)
   int tpa_list = 0, tpa_near = 128;
+  int rbl_list_warp = -1;               // RBL list build: 1 one warp per atom, 0 one thread per atom, -1 by size
+  int rbl_lanes = 0;                    // RBL force pass lanes per atom (0: by size)
+  int num_sms = 148;                    // SMs of the bound device (cudaDevAttrMultiProcessorCount)
   int near_lanes = 1;                   // near pass lanes per atom: 1, or 4 / 8 / 16 / 32     // list build: 0 = staged kernel, else threads per block of
                                         // k_nlist; threads per block of the force pass
   bool autotune = false;                // "autotune": true tunes them at the first compute
@@ -716,10 +719,22 @@ void launch_nlist(rbmd_force* f, cudaStream_t s) {
 template <class R>
 void launch_rbl_list(rbmd_force* f, cudaStream_t s) {
   PhaseScope ps(f, kPhList, s);
-  k_rbl_list<R><<<(f->n + 127) / 128, 128, 0, s>>>(
-      f->n, (const typename Traits<R>::V4*)f->d_pos4, f->d_cell_start, f->d_reps,
-      f->nrep > 1 ? f->d_rep_of : nullptr, f->num_cycles, (R)f->rc, (R)f->rs, f->core_cap, f->shell_cap,
-      f->stride, f->d_nbr, f->d_count, f->d_count2, f->d_maxcount, f->d_status);
+  const int* rp = f->nrep > 1 ? f->d_rep_of : nullptr;
+  const int side = 2 * f->num_cycles + 1;
+  // one warp per atom below 10 warps' worth of atoms per SM (measured crossover between 21k and
+  // 98k atoms on B200), where one thread per atom leaves most SMs idle
+  const bool warp = f->rbl_list_warp > 0 || (f->rbl_list_warp < 0 && f->n < 10 * 32 * f->num_sms);
+  if (warp && side * side * side <= kRblStencilMax) {
+    k_rbl_list_warp<R><<<(f->n + kRblWarps - 1) / kRblWarps, 32 * kRblWarps, 0, s>>>(
+        f->n, (const typename Traits<R>::V4*)f->d_pos4, f->d_cell_start, f->d_reps, rp, f->num_cycles, (R)f->rc,
+        (R)f->rs, f->core_cap, f->shell_cap, f->stride, f->d_nbr, f->d_count, f->d_count2, f->d_maxcount,
+        f->d_status);
+  } else {
+    k_rbl_list<R><<<(f->n + 127) / 128, 128, 0, s>>>(
+        f->n, (const typename Traits<R>::V4*)f->d_pos4, f->d_cell_start, f->d_reps, rp, f->num_cycles, (R)f->rc,
+        (R)f->rs, f->core_cap, f->shell_cap, f->stride, f->d_nbr, f->d_count, f->d_count2, f->d_maxcount,
+        f->d_status);
+  }
   f->launches++;
 }
 
@@ -936,6 +951,32 @@ void launch_eam(rbmd_force* f, cudaStream_t s) {
   f->launches += 2;
 }
 
+// Lanes per atom of the RBL force pass: tuning.rbl_lanes, else 16 below 10 warps' worth of atoms
+// per SM and 8 above (B200, flexible chains at rc 12 A with ~80 RBL entries per atom: 4k atoms
+// 0.191 -> 0.034 ms, 21k 0.198 -> 0.064 ms, 50k 0.217 -> 0.122 ms, 98k 0.253 -> 0.200 ms against
+// one thread per atom).
+int rbl_lanes(const rbmd_force* f) {
+  if (f->rbl_lanes > 0) return f->rbl_lanes;
+  return f->n < 10 * 32 * f->num_sms ? 16 : 8;
+}
+
+template <class R, bool C, bool SP>
+auto pick_rbl_force_g(int g) -> decltype(&k_rbl_force<R, C, SP, 1>) {
+  switch (g) {
+    case 4: return k_rbl_force<R, C, SP, 4>;
+    case 8: return k_rbl_force<R, C, SP, 8>;
+    case 16: return k_rbl_force<R, C, SP, 16>;
+    case 32: return k_rbl_force<R, C, SP, 32>;
+    default: return k_rbl_force<R, C, SP, 1>;
+  }
+}
+
+template <class R>
+auto pick_rbl_force(bool coul, bool spw, int g) -> decltype(&k_rbl_force<R, true, true, 1>) {
+  if (coul) return spw ? pick_rbl_force_g<R, true, true>(g) : pick_rbl_force_g<R, true, false>(g);
+  return spw ? pick_rbl_force_g<R, false, true>(g) : pick_rbl_force_g<R, false, false>(g);
+}
+
 template <class R>
 void launch_rbl_force(rbmd_force* f, cudaStream_t s) {
   const int* rp = f->nrep > 1 ? f->d_rep_of : nullptr;
@@ -979,10 +1020,12 @@ void launch_rbl_force(rbmd_force* f, cudaStream_t s) {
     p.two_sqrt_alpha_over_sqrt_pi = 2.0 * std::sqrt(f->alpha) / std::sqrt(M_PI);
     double* es = f->want_energy ? f->d_eslot : nullptr;
     const bool spw = p.molecular == 2;
-    auto kern = f->with_coul_near() ? (spw ? k_rbl_force<R, true, true> : k_rbl_force<R, true, false>)
-                                    : (spw ? k_rbl_force<R, false, true> : k_rbl_force<R, false, false>);
-    kern<<<nb, 128, 0, s>>>(p, f->d_ljt, (const typename Traits<R>::V4*)f->d_pos4, f->d_meta, f->d_nbr, f->d_count,
-                            f->d_count2, f->d_reps, rp, f->d_slot_atom, f->shell_cap, f->at.force, es, f->d_status);
+    const int g = rbl_lanes(f);
+    auto kern = pick_rbl_force<R>(f->with_coul_near(), spw, g);
+    const int grid = (int)(((long long)f->n * g + 127) / 128);
+    kern<<<grid, 128, 0, s>>>(p, f->d_ljt, (const typename Traits<R>::V4*)f->d_pos4, f->d_meta, f->d_nbr,
+                              f->d_count, f->d_count2, f->d_reps, rp, f->d_slot_atom, f->shell_cap, f->at.force, es,
+                              f->d_status);
     f->launches++;
   }
   // F_i -= mean_j F_j per replica (ExecutionMD.cpp:568-570)
@@ -1327,6 +1370,15 @@ rbmd_status parse_config(rbmd_force* f, const char* text) {
     if (ok(tn)) { f->tpa_near = tn; f->autotune = false; }
     const int ln = (int)num(root, "tuning.force_lanes", 0.0);
     if (ln == 1 || ln == 4 || ln == 8 || ln == 16 || ln == 32) { f->near_lanes = ln; f->autotune = false; }
+    const std::string rl = rbmdjson::text(root, "tuning.rbl_list", "auto");
+    if (rl != "warp" && rl != "thread" && rl != "auto") {
+      std::snprintf(g_last_error, sizeof g_last_error,
+                    "config: tuning.rbl_list must be \"auto\", \"warp\" or \"thread\"");
+      return RBMD_ERR_CONFIG;
+    }
+    f->rbl_list_warp = rl == "warp" ? 1 : (rl == "thread" ? 0 : -1);
+    const int rg = (int)num(root, "tuning.rbl_lanes", 0.0);
+    if (rg == 1 || rg == 4 || rg == 8 || rg == 16 || rg == 32) f->rbl_lanes = rg;
   }
   f->far = root.path("hyper_parameters.coulomb") != nullptr;
   if (f->far) {
@@ -1833,6 +1885,12 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
   if (nrep != f->nrep) return RBMD_ERR_ARG;
   if (f->is_eam() && !f->eam_loaded) return RBMD_ERR_STATE;
   free_all(f);
+  {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0)
+      f->num_sms = sms;
+  }
   f->at = *a;
   f->n = (int)a->n_atoms;
   f->rep_off.assign(nrep + 1, 0);

@@ -149,3 +149,86 @@ def test_eam_verlet_reference_pair_vector(cuda, oracle_lib, tmp_path):
     nl = oracle_lib.neighbors(s["pos"], s["lo"], s["hi"], 5.0, "fp64")
     ref, _ = oracle_lib.eam_force(pot, s["pos"], s["lo"], s["hi"], 5.0, nl, prec="fp64", ref_sign=True)
     assert rel_err(dev["force"].cpu().numpy(), ref) <= 1e-11
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("system", ["electrolyte", "molecular"])
+def test_rbl_warp_list_identical(cuda, prec, system):
+    """tuning.rbl_list "warp" (one warp per atom over the flattened stencil, ballot-ordered shell
+    selection) and "thread" (one thread per atom) build identical lists, entry for entry, and so
+    identical forces; the molecular case has 125-cell stencils (num_cycles 2) and special bonds."""
+    import torch
+    if system == "electrolyte":
+        s = systems.electrolyte(3000, seed=24)
+        base = _rbl_cfg(prec)
+    else:
+        s = systems.molecular(n_chain=343, chain_len=12, n_ion_pairs=40, step=1.5, cell=6.0, seed=25)
+        base = systems.molecular_config(P=32, precision=prec, neighbor="RBL", cutoff=12.0, r_core=6.0,
+                                        sample_num=100, special=(0.0, 0.0, 0.0))
+    out = []
+    for mode in ("thread", "warp"):
+        cfg = dict(base)
+        cfg["tuning"] = {"rbl_list": mode}
+        dev = to_dev(s, cuda)
+        ff = make_ff(cfg, s, dev)
+        if system == "molecular":
+            ff.set_topology(s["molecule"], s["bonds"], s["bond_type"], s["bond_coeffs"], s["angles"],
+                            s["angle_type"], s["angle_coeffs"], s["dihedrals"], s["dihedral_type"],
+                            s["dihedral_coeffs"])
+        ff.Execute()   # the device sampler draws the same seeded k-set in both runs
+        torch.cuda.synchronize()
+        assert ff.status() == 0
+        ncore, nshell, sizes = ff.rbl_lists()
+        counts, ids = ff.neighbors(int((ncore + nshell).max()) + 1)
+        out.append((ncore, nshell, counts, ids, dev["force"].cpu().numpy()))
+        ff.close()
+    assert out[1][0].sum() > 0 and out[1][1].sum() > 0
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("lanes", [4, 8, 16, 32])
+def test_rbl_force_lanes_parity(cuda, oracle_lib, lanes):
+    """tuning.rbl_lanes G > 1 (G lanes per atom, FP64 butterfly of the lane sums) equals one
+    thread per atom to summation-order rounding in FP64 (molecular system with special bonds),
+    and the FP32 electrolyte matches the oracle."""
+    import torch
+    s = systems.molecular(n_chain=343, chain_len=12, n_ion_pairs=40, step=1.5, cell=6.0, seed=26)
+    forces = []
+    for g in (1, lanes):
+        cfg = systems.molecular_config(P=16, precision="fp64", neighbor="RBL", cutoff=12.0, r_core=6.0,
+                                       sample_num=100, special=(0.0, 0.0, 0.5))
+        cfg["tuning"] = {"rbl_lanes": g}
+        dev = to_dev(s, cuda)
+        ff = make_ff(cfg, s, dev)
+        ff.set_topology(s["molecule"], s["bonds"], s["bond_type"], s["bond_coeffs"], s["angles"], s["angle_type"],
+                        s["angle_coeffs"], s["dihedrals"], s["dihedral_type"], s["dihedral_coeffs"])
+        ff.Execute()
+        torch.cuda.synchronize()
+        assert ff.status() == 0
+        forces.append(dev["force"].cpu().numpy())
+        ff.close()
+    assert rel_err(forces[1], forces[0]) < 1e-12
+    se = systems.electrolyte(3000, seed=27)
+    P = 32
+    cfg = _rbl_cfg("fp32", P=P)
+    cfg["tuning"] = {"rbl_lanes": lanes, "rbl_list": "thread"}
+    alpha = cfg["hyper_parameters"]["coulomb"]["alpha"]
+    L = se["hi"] - se["lo"]
+    m = oracle_lib.rbe_sample(alpha, L, seed=9, step=0, rep=0, P=P)
+    dev = to_dev(se, cuda)
+    ff = make_ff(cfg, se, dev)
+    ff.set_ksamples(m)
+    ff.Execute()
+    torch.cuda.synchronize()
+    assert ff.status() == 0
+    pice = ff.rbl_lists()[2][2]
+    f = dev["force"].cpu().numpy()
+    ff.close()
+    pr = _posr(se["pos"], "fp32")
+    rl = oracle_lib.rbl_list(pr, se["lo"], se["hi"], RC, RS, pice, 96, 96, prec="fp32")
+    near = oracle_lib.rbl_near(pr, se["lo"], se["hi"], RC, RS, pice, rl, 96, type=se["type"], charge=se["charge"],
+                               eps=se["eps"], sigma=se["sigma"], with_coul=True, alpha=alpha, qqr2e=1.0, prec="fp32")
+    rho = oracle_lib.rhok(se["pos"], se["charge"], L, m, prec="fp64")
+    far = oracle_lib.rbe_force(se["pos"], se["charge"], L, alpha, 1.0, m, rho, prec="fp64")
+    assert rel_err(f, near + far) <= TOL["fp32"]

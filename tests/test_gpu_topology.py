@@ -153,3 +153,50 @@ def test_water_as_topology_equals_water_path(cuda):
     assert rel_err(out[1][0], out[0][0]) <= 1e-13
     for k in ("bond", "angle", "lj", "coul_real"):
         assert abs(out[1][1][k] - out[0][1][k]) <= 1e-12 * max(1.0, abs(out[0][1][k])), k
+
+
+def test_topology_nve_energy_conservation_fp64(cuda):
+    """Flexible chains (bonds, angles, dihedrals, special bonds 0 / 0 / 0.5, intramolecular
+    Coulomb correction) with LJ + erfc + Ewald k-space (deterministic), FP64, Verlet skin and
+    CUDA-graph steps: 2000 Berendsen steps relax the lattice-grown chains, then 2000 NVE steps of
+    0.5 fs keep the total energy (kinetic + LJ + Coulomb real / k-space / self / correction +
+    bonded) within 1 % of the kinetic energy of its start value.  A force that is not minus the
+    gradient of the energy (a sign, a weight or a missing term) drifts by far more."""
+    import copy
+    import torch
+    s = systems.molecular(n_chain=64, chain_len=12, n_ion_pairs=0, seed=21)
+    cfg = systems.molecular_config(precision="fp64", cutoff=10.0, special=(0.0, 0.0, 0.5), dt=0.5)
+    cfg["hyper_parameters"]["coulomb"] = {"type": "EWALD", "alpha": 0.09, "kmax": 6}
+    cfg["hyper_parameters"]["neighbor"]["skin"] = 1.0
+    nvt = copy.deepcopy(cfg)
+    nvt["execution"].update({"ensemble": "NVT", "temp_ctrl_type": "BERENDSEN", "temperature": [298.0, 298.0, 10.0]})
+    dev = to_dev(s, cuda)
+    topo = (s["molecule"], s["bonds"], s["bond_type"], s["bond_coeffs"], s["angles"], s["angle_type"],
+            s["angle_coeffs"], s["dihedrals"], s["dihedral_type"], s["dihedral_coeffs"])
+    ff = make_ff(nvt, s, dev)
+    ff.set_topology(*topo)
+    ff.Execute()
+    ff.step(2000)
+    ff.sync_velocities()
+    torch.cuda.synchronize()
+    assert ff.status() == 0
+    ff.close()
+    ff = make_ff(cfg, s, dev)
+    ff.set_topology(*topo)
+    keys = ("lj", "coul_real", "coul_kspace", "coul_self", "bond", "angle", "dihedral", "coul_special")
+
+    def total():
+        ff.step(1)
+        ff.Execute()
+        e = ff.energy()
+        return e["kinetic"] + sum(e[k] for k in keys), e
+
+    e0, d0 = total()
+    assert all(d0[k] != 0.0 for k in keys), d0
+    for _ in range(4):
+        ff.step(500)
+        torch.cuda.synchronize()
+        assert ff.status() == 0
+        e, d = total()
+        assert abs(e - e0) <= 1e-2 * d0["kinetic"], (e, e0, d0["kinetic"], d)
+    ff.close()
