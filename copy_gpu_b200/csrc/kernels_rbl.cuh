@@ -19,6 +19,8 @@ namespace rbmd {
 // rs^2 - d^2 > 1e-4 && d^2 > 1e-4 is a core pair.  d^2 is formed with uncontracted ops on
 // (p_j - offset) - p_i, as in the full list.  Core entries fill rows [0, core_cap) of the
 // transposed list, kept shell entries rows [core_cap, core_cap + shell_cap).
+constexpr int kRblBatch = 4;   // candidate positions loaded ahead of their classification (8: slower)
+
 template <class R>
 __global__ void __launch_bounds__(128) k_rbl_list(
     int n, const typename Traits<R>::V4* __restrict__ pos4, const int* __restrict__ cell_start,
@@ -59,21 +61,31 @@ __global__ void __launch_bounds__(128) k_rbl_list(
         const int code = cx | (cy << 2) | ((ddz > 0 ? 1 : (ddz < 0 ? 2 : 0)) << 4);
         const int cell = rp.cell_base + wx + wy * dx0 + wz * dx0 * dx1;
         const int s1 = cell_start[cell + 1];
-        for (int s = cell_start[cell]; s < s1; ++s) {
-          const typename Traits<R>::V4 pj = pos4[s];
-          const R r0 = sub_rn(sub_rn(pj.x, off0), pix[0]);
-          const R r1 = sub_rn(sub_rn(pj.y, off1), pix[1]);
-          const R r2 = sub_rn(sub_rn(pj.z, off2), pix[2]);
-          const R d2 = add_rn(add_rn(mul_rn(r0, r0), mul_rn(r1, r1)), mul_rn(r2, r2));
-          if (gt_small(sub_rn(rc2, d2)) && gt_small(sub_rn(d2, rs2))) {
-            if (shell_index % pice == 0) {
-              if (n_shell < shell_cap) nbr[(size_t)(core_cap + n_shell) * stride + i] = (s << kShiftBits) | code;
-              ++n_shell;
+        // the candidates of a cell in groups of kRblBatch: the positions are loaded before any
+        // is classified (kRblBatch loads in flight), then classified in slot order
+        for (int s = cell_start[cell]; s < s1; s += kRblBatch) {
+          typename Traits<R>::V4 pj[kRblBatch];
+#pragma unroll
+          for (int u = 0; u < kRblBatch; ++u) pj[u] = pos4[s + u < s1 ? s + u : s];
+#pragma unroll
+          for (int u = 0; u < kRblBatch; ++u) {
+            if (s + u < s1) {
+              const R r0 = sub_rn(sub_rn(pj[u].x, off0), pix[0]);
+              const R r1 = sub_rn(sub_rn(pj[u].y, off1), pix[1]);
+              const R r2 = sub_rn(sub_rn(pj[u].z, off2), pix[2]);
+              const R d2 = add_rn(add_rn(mul_rn(r0, r0), mul_rn(r1, r1)), mul_rn(r2, r2));
+              const int e = ((s + u) << kShiftBits) | code;
+              if (gt_small(sub_rn(rc2, d2)) && gt_small(sub_rn(d2, rs2))) {
+                if (shell_index % pice == 0) {
+                  if (n_shell < shell_cap) nbr[(size_t)(core_cap + n_shell) * stride + i] = e;
+                  ++n_shell;
+                }
+                ++shell_index;
+              } else if (gt_small(sub_rn(rs2, d2)) && gt_small(d2)) {
+                if (n_core < core_cap) nbr[(size_t)n_core * stride + i] = e;
+                ++n_core;
+              }
             }
-            ++shell_index;
-          } else if (gt_small(sub_rn(rs2, d2)) && gt_small(d2)) {
-            if (n_core < core_cap) nbr[(size_t)n_core * stride + i] = (s << kShiftBits) | code;
-            ++n_core;
           }
         }
       }
