@@ -11,6 +11,27 @@
 
 namespace rbmd {
 
+// Squared lower bound of the distance from coordinate x to the cells of unwrapped index u
+// (wrapped index w) along axis d, less a rounding allowance `slack`; a boundary cell is open on
+// its outer side, because atoms outside the box are binned into it.  A stencil cell whose bound
+// summed over the axes exceeds rc^2 holds no pair (the predicate needs d^2 < rc^2 - 1e-4), so
+// the list builds skip it without changing which pairs are found or their order.
+template <class R>
+__device__ __forceinline__ R rbl_gap2(const RepDev& rp, int d, int u, int w, R x, R slack) {
+  const R dx = Traits<R>::dx(rp, d);
+  const R sl = Traits<R>::lo(rp, d) + (R)u * dx, sh = sl + dx;
+  R g = (R)0;
+  if (w != 0 && x < sl) g = sl - x;
+  else if (w != rp.dims[d] - 1 && x > sh) g = x - sh;
+  g -= slack;
+  return g > (R)0 ? g * g : (R)0;
+}
+
+template <class R>
+__device__ __forceinline__ R rbl_slack(const RepDev& rp, int d, R x, R rc) {
+  return (R)1e-5 * (fabs(x) + fabs(Traits<R>::lo(rp, d)) + (R)rp.dims[d] * Traits<R>::dx(rp, d) + rc) + (R)1e-6;
+}
+
 // RBL list of slot i: ComputeRBLNeighboursOnceWorklet (rbmd/framework/run/worklet/RunWorklet.cpp:
 // 634-708).  The stencil is walked as the reference walks it (x offset outermost, z innermost,
 // the points of a cell in slot order = ascending caller id), because which shell pairs are kept
@@ -40,6 +61,7 @@ __global__ void __launch_bounds__(128) k_rbl_list(
   const R rc2 = mul_rn(rc, rc), rs2 = mul_rn(rs, rs);
   const int nc = num_cycles;
   const int dx0 = rp.dims[0], dx1 = rp.dims[1], dx2 = rp.dims[2];
+  const R sl0 = rbl_slack(rp, 0, pix[0], rc), sl1 = rbl_slack(rp, 1, pix[1], rc), sl2 = rbl_slack(rp, 2, pix[2], rc);
   int n_core = 0, n_shell = 0, shell_index = 0;
   for (int a = -nc; a <= nc; ++a) {
     const int nbx = ci[0] + a;
@@ -47,15 +69,19 @@ __global__ void __launch_bounds__(128) k_rbl_list(
     const int ddx = wx - nbx;
     const R off0 = mul_rn(Traits<R>::dx(rp, 0), (R)ddx);
     const int cx = ddx > 0 ? 1 : (ddx < 0 ? 2 : 0);
+    const R gx2 = rbl_gap2(rp, 0, nbx, wx, pix[0], sl0);
     for (int b = -nc; b <= nc; ++b) {
       const int nby = ci[1] + b;
       const int wy = ((nby % dx1) + dx1) % dx1;
       const int ddy = wy - nby;
       const R off1 = mul_rn(Traits<R>::dx(rp, 1), (R)ddy);
       const int cy = ddy > 0 ? 1 : (ddy < 0 ? 2 : 0);
+      const R gxy2 = gx2 + rbl_gap2(rp, 1, nby, wy, pix[1], sl1);
+      if (gxy2 > rc2) continue;
       for (int c = -nc; c <= nc; ++c) {
         const int nbz = ci[2] + c;
         const int wz = ((nbz % dx2) + dx2) % dx2;
+        if (gxy2 + rbl_gap2(rp, 2, nbz, wz, pix[2], sl2) > rc2) continue;   // no pair in this cell
         const int ddz = wz - nbz;
         const R off2 = mul_rn(Traits<R>::dx(rp, 2), (R)ddz);
         const int code = cx | (cy << 2) | ((ddz > 0 ? 1 : (ddz < 0 ? 2 : 0)) << 4);
@@ -151,7 +177,11 @@ __global__ void __launch_bounds__(32 * kRblWarps) k_rbl_list_warp(
       }
       const int cell = rp.cell_base + wr[0] + wr[1] * dims[0] + wr[2] * dims[0] * dims[1];
       const int s0 = cell_start[cell];
-      cnt = cell_start[cell + 1] - s0;
+      R g2 = (R)0;
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        g2 += rbl_gap2(rp, d, ci[d] + off[d], wr[d], pix[d], rbl_slack(rp, d, pix[d], rc));
+      cnt = g2 > rc2 ? 0 : cell_start[cell + 1] - s0;   // a cell beyond rc contributes no candidate
       s_start[w][k] = s0;
       s_wrap[w][k] = q;
     }

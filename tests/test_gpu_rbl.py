@@ -232,3 +232,35 @@ def test_rbl_force_lanes_parity(cuda, oracle_lib, lanes):
     rho = oracle_lib.rhok(se["pos"], se["charge"], L, m, prec="fp64")
     far = oracle_lib.rbe_force(se["pos"], se["charge"], L, alpha, 1.0, m, rho, prec="fp64")
     assert rel_err(f, near + far) <= TOL["fp32"]
+
+
+@pytest.mark.parametrize("mode", ["thread", "warp"])
+def test_rbl_lists_atoms_outside_box(cuda, oracle_lib, mode):
+    """Atoms up to one r_core outside the box are binned into the boundary cells; the list builds
+    skip stencil cells beyond rc from the atom, with boundary cells open on their outer side, so
+    the lists still equal the oracle's entry for entry."""
+    import torch
+    rng = np.random.default_rng(12)
+    L = 12.0
+    n = 2000
+    pos = rng.uniform(0, L, size=(n, 3))
+    pos[:150] += rng.uniform(-RS, RS, size=(150, 3))
+    s = dict(pos=pos, vel=np.zeros_like(pos), mass=np.ones(n), charge=np.zeros(n), type=np.zeros(n, np.int32),
+             molecule=None, lo=np.zeros(3), hi=np.full(3, L), eps=np.ones(1), sigma=np.ones(1))
+    cfg = systems.lj_config(cutoff=RC, precision="fp32")
+    cfg["hyper_parameters"]["neighbor"] = {"type": "RBL", "cut_off": RC, "r_core": RS, "neighbor_sample_num": SAMPLE}
+    cfg["tuning"] = {"rbl_list": mode}
+    dev = to_dev(s, cuda)
+    ff = make_ff(cfg, s, dev)
+    ff.Execute()
+    torch.cuda.synchronize()
+    ncore, nshell, sizes = ff.rbl_lists()
+    pice = sizes[2]
+    pr = pos.astype(np.float32)
+    oc, osh, oids, _ = oracle_lib.rbl_list(pr, s["lo"], s["hi"], RC, RS, pice, 96, 96)
+    assert np.array_equal(ncore, oc) and np.array_equal(nshell, osh)
+    counts, ids = ff.neighbors(int((ncore + nshell).max()) + 1)
+    for i in range(n):
+        ref = np.concatenate([oids[i, :oc[i]], oids[i, 96:96 + osh[i]]])
+        assert np.array_equal(ids[i, :counts[i]], ref), f"atom {i}"
+    ff.close()
