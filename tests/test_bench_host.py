@@ -7,7 +7,7 @@ import bench
 from copy_gpu_b200 import systems
 
 
-@pytest.mark.parametrize("name", ["lj", "water", "eam", "batched"])
+@pytest.mark.parametrize("name", ["lj", "water", "eam", "batched", "molecular"])
 def test_config_systems(tmp_path, name):
     s, cfg, boxes, offs, desc = bench.config_system(name, str(tmp_path))
     n = s["pos"].shape[0]
@@ -19,10 +19,20 @@ def test_config_systems(tmp_path, name):
         assert boxes is None and offs is None
     if name == "eam":
         assert cfg["hyper_parameters"]["force_field"]["type"] == "EAM"
+    if name == "molecular":
+        assert cfg["hyper_parameters"]["neighbor"]["type"] == "RBL"
+        assert len(s["dihedrals"]) > 0 and abs(s["charge"].sum()) < 1e-9
 
 
-@pytest.mark.parametrize("name", ["lj", "water", "eam", "batched"])
+@pytest.mark.parametrize("name", ["lj", "water", "eam", "batched", "molecular"])
 def test_cpu_config_eval_small(tmp_path, name, oracle_lib):
+    if name == "molecular":   # the workload's configuration on a small system of the same kind
+        cfg = systems.molecular_config(P=100, cutoff=12.0, alpha=0.074, neighbor="RBL", special=(0.0, 0.0, 0.0),
+                                       precision="fp32", r_core=6.0, sample_num=100)
+        s = systems.molecular(n_chain=64, chain_len=12, n_ion_pairs=16, step=1.5, cell=6.0, seed=3)
+        sec, atoms = bench.cpu_config_eval(name, s, cfg, None, str(tmp_path))
+        assert sec > 0 and atoms == s["pos"].shape[0]
+        return
     s, cfg, boxes, offs, _ = bench.config_system(name, str(tmp_path))
     if name == "water":
         s = systems.water(n_mol=300, seed=2)
