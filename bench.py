@@ -251,26 +251,30 @@ def timed_run(ff, t, dev, steps, warmup, world, dist, e2e_steps):
     ff.Execute()
     cnt, _ = ff.neighbors(0)
     n_nbr = float(cnt.mean())
-    # end-to-end through the host-buffer C-ABI call: pinned positions in, pinned forces out
-    pos_h = torch.empty((n, 3), dtype=torch.float64, pin_memory=True)
-    pos_h.copy_(t["pos"].cpu())
-    frc_h = torch.empty((n, 3), dtype=torch.float64, pin_memory=True)
-    ph, fh = pos_h.numpy(), frc_h.numpy()
-    ff.compute_host(ph, fh, stream=stream.cuda_stream)
-    torch.cuda.synchronize(dev)
-    w0 = time.perf_counter()
-    a0 = torch.cuda.Event(enable_timing=True)
-    a1 = torch.cuda.Event(enable_timing=True)
-    a0.record(stream)
-    for _ in range(e2e_steps):
+    # end-to-end through the host-buffer C-ABI call: pinned positions in, pinned forces out, in the
+    # reference's own Vec3f (float32) layout (rbmd_force_compute_host_f32) and in float64
+    e2e = {}
+    for dt in (torch.float32, torch.float64):
+        pos_h = torch.empty((n, 3), dtype=dt, pin_memory=True)
+        pos_h.copy_(t["pos"].cpu())
+        frc_h = torch.empty((n, 3), dtype=dt, pin_memory=True)
+        ph, fh = pos_h.numpy(), frc_h.numpy()
         ff.compute_host(ph, fh, stream=stream.cuda_stream)
-    a1.record(stream)
-    torch.cuda.synchronize(dev)
-    e2e_ms = max(a0.elapsed_time(a1), (time.perf_counter() - w0) * 1e3) / e2e_steps
-    if world > 1:
-        e2e_ms = max_over_ranks(e2e_ms, dist, dev)
-    return dict(ms=ms, builds=builds, phases=phases, flags=flags, clk=clk, n_nbr=n_nbr, e2e_ms=e2e_ms,
-                k_per_step=k_per_step, blocks=blocks)
+        torch.cuda.synchronize(dev)
+        w0 = time.perf_counter()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(e2e_steps):
+            ff.compute_host(ph, fh, stream=stream.cuda_stream)
+        a1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms_e = max(a0.elapsed_time(a1), (time.perf_counter() - w0) * 1e3) / e2e_steps
+        if world > 1:
+            ms_e = max_over_ranks(ms_e, dist, dev)
+        e2e[dt] = ms_e
+    return dict(ms=ms, builds=builds, phases=phases, flags=flags, clk=clk, n_nbr=n_nbr, e2e_ms=e2e[torch.float32],
+                e2e64_ms=e2e[torch.float64], k_per_step=k_per_step, blocks=blocks)
 
 
 def roofline(run, n, nq, P, steps, dev):
@@ -430,8 +434,12 @@ def run_ours(args):
                                       "plain": plain["phases"][k][0] / args.steps}
                                   for k in learned["phases"] if k in plain["phases"]},
             "e2e": {"value": world * n / (learned["e2e_ms"] / 1e3), "unit": "atom-steps/s",
-                    "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n,
-                    "what": "rbmd_force_compute_host: pinned host positions in, forces out, one force evaluation per step"},
+                    "h2d_bytes_per_step": 12 * n, "d2h_bytes_per_step": 12 * n,
+                    "what": "rbmd_force_compute_host_f32: pinned host positions in, forces out, in the reference's "
+                            "Vec3f (float32) layout, one force evaluation per step",
+                    "fp64_host_buffers": {"value": world * n / (learned["e2e64_ms"] / 1e3),
+                                          "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n,
+                                          "what": "rbmd_force_compute_host (float64 host arrays)"}},
             "gpu_launches": learned["k_per_step"] * args.steps,
             "kernels_per_step": learned["k_per_step"],
             "status_flags": learned["flags"] | plain["flags"],
@@ -662,9 +670,12 @@ def run_config(args):
                        "list_builds_per_step": run["builds"] / args.steps / (len(boxes) if boxes else 1),
                        "threads_per_block": {"list": run["blocks"][0], "force": run["blocks"][1]},
                        "step_launch": "cuda graph replay (one launch per step)"},
-            "e2e": {"value": n / (run["e2e_ms"] / 1e3), "unit": "atom-steps/s", "h2d_bytes_per_step": 24 * n,
-                    "d2h_bytes_per_step": 24 * n,
-                    "what": "rbmd_force_compute_host: pinned host positions in, forces out, one force evaluation"},
+            "e2e": {"value": n / (run["e2e_ms"] / 1e3), "unit": "atom-steps/s", "h2d_bytes_per_step": 12 * n,
+                    "d2h_bytes_per_step": 12 * n,
+                    "what": "rbmd_force_compute_host_f32: pinned host positions in, forces out (the reference's "
+                            "Vec3f layout), one force evaluation",
+                    "fp64_host_buffers": {"value": n / (run["e2e64_ms"] / 1e3), "h2d_bytes_per_step": 24 * n,
+                                          "d2h_bytes_per_step": 24 * n}},
             "phase_ms_per_step": {k: v[0] / args.steps for k, v in run["phases"].items() if v[1]},
             "status_flags": run["flags"], "clocks": run["clk"], "mean_neighbors": run["n_nbr"],
         }

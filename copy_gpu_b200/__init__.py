@@ -37,7 +37,8 @@ EXPORTED = [
     "rbmd_force_create", "rbmd_force_set_pair_coeffs", "rbmd_force_load_funcfl",
     "rbmd_force_set_water", "rbmd_force_set_topology", "rbmd_force_bind", "rbmd_force_set_ksamples",
     "rbmd_force_set_kweights", "rbmd_force_get_ksamples", "rbmd_force_sample_k",
-    "rbmd_force_compute", "rbmd_force_autotune", "rbmd_force_compute_host", "rbmd_force_step",
+    "rbmd_force_compute", "rbmd_force_autotune", "rbmd_force_compute_host", "rbmd_force_compute_host_f32",
+    "rbmd_force_step",
     "rbmd_force_sync_velocities", "rbmd_force_energy", "rbmd_force_status",
     "rbmd_force_get_neighbors", "rbmd_force_get_rbl", "rbmd_force_get_rhok", "rbmd_force_profile",
     "rbmd_force_phase_ms", "rbmd_force_list_builds", "rbmd_force_launch_count",
@@ -134,6 +135,7 @@ def library() -> ctypes.CDLL:
         "rbmd_force_compute": (I32, [V, V]),
         "rbmd_force_autotune": (I32, [V, V, P(I32), P(I32)]),
         "rbmd_force_compute_host": (I32, [V, P(D), P(D), V]),
+        "rbmd_force_compute_host_f32": (I32, [V, P(ctypes.c_float), P(ctypes.c_float), V]),
         "rbmd_force_step": (I32, [V, I32, V]),
         "rbmd_force_sync_velocities": (I32, [V, V]),
         "rbmd_force_energy": (I32, [V, P(rbmd_energy), V]),
@@ -316,6 +318,16 @@ class ForceField:
         return int(a.value), int(b.value)
 
     def compute_host(self, pos_host, force_host, stream=None):
+        """Force of host positions into host forces: float64 arrays use rbmd_force_compute_host,
+        float32 arrays (the reference's Vec3f layout) rbmd_force_compute_host_f32."""
+        import numpy as np
+        if pos_host.dtype == np.float32:
+            if force_host.dtype != np.float32:
+                raise RbmdError("compute_host: float32 positions need float32 forces")
+            _check(library().rbmd_force_compute_host_f32(self._h, _ptr(pos_host, ctypes.c_float),
+                                                         _ptr(force_host, ctypes.c_float),
+                                                         self._stream(stream)), "compute_host_f32")
+            return
         _check(library().rbmd_force_compute_host(self._h, _ptr(pos_host, ctypes.c_double),
                                                  _ptr(force_host, ctypes.c_double),
                                                  self._stream(stream)), "compute_host")

@@ -223,6 +223,7 @@ struct rbmd_force {
   float4 *d_frho = nullptr, *d_rhor = nullptr, *d_z2r = nullptr;
   void* d_fp = nullptr;
   double *d_emb = nullptr, *d_epair = nullptr;
+  float* d_host32 = nullptr;   // [3 n] staging of rbmd_force_compute_host_f32 (positions in, forces out)
   // topology device
   int *d_term_atom = nullptr, *d_tmult = nullptr, *d_sc_off = nullptr, *d_sc_id = nullptr, *d_row_off = nullptr,
       *d_row_idx = nullptr, *d_sp_off = nullptr, *d_sp_id = nullptr, *d_comp = nullptr;
@@ -373,6 +374,7 @@ void free_all(rbmd_force* f) {
   f->d_fp = nullptr;
   dfree(f->d_emb); dfree(f->d_epair); dfree(f->d_hoh); dfree(f->d_ebond); dfree(f->d_eangle);
   free_topology(f);
+  dfree(f->d_host32);
   dfree(f->d_snap); dfree(f->d_snap_img); dfree(f->d_step); dfree(f->d_lstep);
   if (f->graph_exec) cudaGraphExecDestroy(f->graph_exec);
   f->graph_exec = nullptr;
@@ -1033,6 +1035,16 @@ void launch_rbl_force(rbmd_force* f, cudaStream_t s) {
   k_force_sub_mean<<<f->nchunks, 256, 0, s>>>(f->d_chunks, f->d_chunk_rep_begin, f->d_reps, f->d_mean_partial,
                                               f->at.force);
   f->launches += 2;
+}
+
+// float <-> double copies of the host-buffer call in the reference's own Vec3f layout.
+__global__ void k_f32_to_f64(long long m, const float* __restrict__ a, double* __restrict__ b) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < m; k += (long long)gridDim.x * blockDim.x)
+    b[k] = (double)a[k];
+}
+__global__ void k_f64_to_f32(long long m, const double* __restrict__ a, float* __restrict__ b) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < m; k += (long long)gridDim.x * blockDim.x)
+    b[k] = (float)a[k];
 }
 
 // General topology: per-term forces, then the per-atom gather with the Coulomb correction.
@@ -2278,6 +2290,7 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
     rbmd_status st = upload_topology(f);
     if (st) return st;
   }
+  CK(dalloc(&f->d_host32, (size_t)3 * f->n));
   f->bound = true;
   f->list_valid = false;
   f->step_count = 0;
@@ -2376,6 +2389,29 @@ rbmd_status rbmd_force_compute_host(rbmd_force* f, const double* pos_host, doubl
     launch_compute_any(f, s);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(force_host, f->at.force, sizeof(double) * 3 * f->n, cudaMemcpyDeviceToHost, s));
+    bool redo = false;
+    rbmd_status st = check_overflow(f, s, &redo);
+    if (st) return st;
+    if (!redo) return RBMD_OK;
+  }
+  return RBMD_ERR_DEVICE;
+}
+
+rbmd_status rbmd_force_compute_host_f32(rbmd_force* f, const float* pos_host, float* force_host, void* stream) {
+  if (!f || !pos_host || !force_host) return RBMD_ERR_ARG;
+  if (!f->bound) return RBMD_ERR_STATE;
+  cudaStream_t s = (cudaStream_t)stream;
+  const long long m = 3LL * f->n;
+  const int grid = (int)std::min<long long>((m + 255) / 256, 8LL * f->num_sms);
+  CK(cudaMemcpyAsync(f->d_host32, pos_host, sizeof(float) * m, cudaMemcpyHostToDevice, s));
+  k_f32_to_f64<<<grid, 256, 0, s>>>(m, f->d_host32, f->at.pos);
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    f->launches = 1;
+    launch_compute_any(f, s);
+    k_f64_to_f32<<<grid, 256, 0, s>>>(m, f->at.force, f->d_host32);
+    f->launches++;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(force_host, f->d_host32, sizeof(float) * m, cudaMemcpyDeviceToHost, s));
     bool redo = false;
     rbmd_status st = check_overflow(f, s, &redo);
     if (st) return st;

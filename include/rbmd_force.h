@@ -206,6 +206,14 @@ RBMD_API rbmd_status rbmd_force_autotune(rbmd_force* f, void* stream, int32_t* l
 RBMD_API rbmd_status rbmd_force_compute_host(rbmd_force* f, const double* pos_host, double* force_host,
                                     void* stream);
 
+/* The same with FP32 host arrays [n_atoms][3], the layout of the reference's
+ * vtkm::cont::ArrayHandle<Vec3f> positions and forces (Real = float, rbmd/framework/Types.h:48),
+ * so a host driver passes its arrays without converting them: half the PCIe bytes of the FP64
+ * call.  Positions are widened to the FP64 master positions on the device and forces narrowed
+ * there; the bound device arrays hold the FP64 values afterwards. */
+RBMD_API rbmd_status rbmd_force_compute_host_f32(rbmd_force* f, const float* pos_host, float* force_host,
+                                                 void* stream);
+
 /* Advance n_steps velocity-Verlet steps in the order of ExecutionNVT::Solve
  * (rbmd/framework/run/ExecutionNVT.cpp:133-159): kick, drift+wrap, SHAKE, force, kick,
  * RATTLE, temperature, thermostat.  Requires vel and mass in the bound atoms. */

@@ -298,3 +298,29 @@ def test_original_neighbor_type(cuda, oracle_lib, prec):
         counts[orig] = (int(c[0]), 1 in set(ids[0, :c[0]].tolist()))
     assert counts[True][1] and not counts[False][1], counts
     assert counts[True][0] == counts[False][0] + 1, counts
+
+
+def test_compute_host_f32_and_f64(cuda):
+    """The host-buffer calls: float64 arrays (rbmd_force_compute_host) give the device-resident
+    compute's forces exactly; float32 arrays in the reference's Vec3f layout
+    (rbmd_force_compute_host_f32) give the forces of the float-rounded positions, rounded to
+    float."""
+    import torch
+    se, cfg = _electrolyte(3000, 32, "fp32")
+    se = dict(se)
+    se["pos"] = se["pos"].astype(np.float32).astype(np.float64)   # positions a float array can hold
+    dev = to_dev(se, cuda)
+    ff = make_ff(cfg, se, dev)
+    m = np.array([[1, 0, 0], [0, 1, -2], [3, 1, 1]] * 10 + [[1, 1, 1], [2, 0, 1]], np.int32)
+    ff.set_ksamples(m)
+    ff.Execute()
+    torch.cuda.synchronize()
+    ref = dev["force"].cpu().numpy()
+    f64 = np.zeros_like(ref)
+    ff.compute_host(np.ascontiguousarray(se["pos"]), f64)
+    assert np.array_equal(f64, ref)
+    f32 = np.zeros(ref.shape, np.float32)
+    ff.compute_host(np.ascontiguousarray(se["pos"], np.float32), f32)
+    assert ff.status() == 0
+    assert np.array_equal(f32, ref.astype(np.float32))
+    ff.close()
