@@ -1561,10 +1561,18 @@ rbmd_status autotune_impl(rbmd_force* f, cudaStream_t s) {
   const bool prof = f->prof_on;
   f->prof_on = false;
   const int cand[3] = {64, 128, 256};
+  // rebuild pattern of the timed list builds: every replica of a single system; in a batch with
+  // a Verlet skin about one replica in five rebuilds per step (each decides alone), and the list
+  // variants rank differently on such partial rebuilds than on full ones, so one in five is
+  // flagged there
+  std::vector<int> rb_pattern(f->nrep + 1, 1);
+  if (f->nrep > 1 && f->skin > 0)
+    for (int r = 0; r < f->nrep; ++r) rb_pattern[r] = r % 5 == 0 ? 1 : 0;
   auto best_of = [&](auto launch) -> float {
     float best = 1e30f;
     for (int rep = 0; rep < 4; ++rep) {
-      if (f->d_rebuild) cudaMemsetAsync(f->d_rebuild, 1, sizeof(int) * (f->nrep + 1), s);
+      if (f->d_rebuild)
+        cudaMemcpyAsync(f->d_rebuild, rb_pattern.data(), sizeof(int) * (f->nrep + 1), cudaMemcpyHostToDevice, s);
       cudaEventRecord(a, s);
       launch();
       cudaEventRecord(b, s);
