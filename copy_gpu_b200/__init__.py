@@ -45,7 +45,7 @@ EXPORTED = [
     "rbmd_force_train_proposal", "rbmd_force_proposal_params", "rbmd_force_get_far",
     "rbmd_force_destroy", "rbmd_rhok_noalloc", "rbmd_proposal_mlp_eval", "rbmd_data_read",
     "rbmd_data_atoms", "rbmd_data_types", "rbmd_data_topology", "rbmd_data_dihedrals", "rbmd_data_free",
-    "rbmd_data_write",
+    "rbmd_data_write", "rbmd_data_write_arrays",
     "rbmd_version",
     "rbmd_last_error",
 ]
@@ -86,6 +86,13 @@ class rbmd_data_info(ctypes.Structure):
                 ("n_atom_types", ctypes.c_int32), ("n_bond_types", ctypes.c_int32), ("n_angle_types", ctypes.c_int32),
                 ("has_velocities", ctypes.c_int32), ("has_pair_coeffs", ctypes.c_int32), ("has_masses", ctypes.c_int32),
                 ("box", rbmd_box), ("n_dihedrals", ctypes.c_int64), ("n_dihedral_types", ctypes.c_int32)]
+
+
+class rbmd_data_arrays(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in (
+        "pos", "vel", "charge", "type", "molecule", "image", "mass_by_type", "epsilon", "sigma",
+        "bonds", "bond_type", "bond_coeffs", "angles", "angle_type", "angle_coeffs",
+        "dihedrals", "dihedral_type", "dihedral_coeffs")]
 
 
 class rbmd_topology(ctypes.Structure):
@@ -159,6 +166,7 @@ def library() -> ctypes.CDLL:
         "rbmd_data_topology": (I32, [V, V, V, V, V, V, V]),
         "rbmd_data_dihedrals": (I32, [V, V, V, V]),
         "rbmd_data_free": (None, [V]),
+        "rbmd_data_write_arrays": (I32, [ctypes.c_char_p, ctypes.c_char_p, P(rbmd_data_info), P(rbmd_data_arrays)]),
         "rbmd_data_write": (I32, [ctypes.c_char_p, ctypes.c_char_p, P(rbmd_data_info), V, V, V, V, V, V, V, V, V,
                                   V, V]),
         "rbmd_version": (ctypes.c_char_p, []),
@@ -520,25 +528,34 @@ def read_data(path, atom_style, unit="LJ"):
 
 
 def write_data(path, atom_style, d):
-    """Write arrays in the dict form of read_data as a LAMMPS data file (rbmd_data_write)."""
+    """Write arrays in the dict form of read_data as a LAMMPS data file (rbmd_data_write_arrays):
+    bonds, angles and dihedrals with their types and coefficients when the dict holds them."""
     import numpy as np
     info = rbmd_data_info()
     n = d["pos"].shape[0]
     info.n_atoms = n
     mt = np.ascontiguousarray(d.get("mass_by_type", np.ones(int(d["type"].max()) + 1)), np.float64)
     info.n_atom_types = len(mt)
-    bonds = d.get("bonds")
-    angles = d.get("angles")
+    c = lambda a, t: None if a is None else np.ascontiguousarray(a, t)   # noqa: E731
+    bonds, angles, dihs = c(d.get("bonds"), np.int32), c(d.get("angles"), np.int32), c(d.get("dihedrals"), np.int32)
+    bc, ac, dc = (c(d.get(k), np.float64) for k in ("bond_coeffs", "angle_coeffs", "dihedral_coeffs"))
     info.n_bonds = 0 if bonds is None else len(bonds)
     info.n_angles = 0 if angles is None else len(angles)
-    info.n_bond_types = 1
-    info.n_angle_types = 1
+    info.n_dihedrals = 0 if dihs is None else len(dihs)
+    info.n_bond_types = len(bc) if bc is not None and len(bc) else 1
+    info.n_angle_types = len(ac) if ac is not None and len(ac) else 1
+    info.n_dihedral_types = len(dc) if dc is not None and len(dc) else 1
     info.box = rbmd_box(tuple(d["lo"]), tuple(d["hi"]))
-    c = lambda a, t: None if a is None else np.ascontiguousarray(a, t)   # noqa: E731
-    arrs = [c(d["pos"], np.float64), c(d.get("vel"), np.float64), c(d.get("charge"), np.float64),
-            c(d["type"], np.int32), c(d.get("molecule"), np.int32), c(d.get("image"), np.int32), mt,
-            c(d.get("eps"), np.float64), c(d.get("sigma"), np.float64),
-            c(bonds, np.int32) if info.n_bonds else None, c(angles, np.int32) if info.n_angles else None]
-    ptrs = [None if a is None else a.ctypes.data_as(ctypes.c_void_p) for a in arrs]
-    _check(library().rbmd_data_write(str(path).encode(), atom_style.encode(), ctypes.byref(info), *ptrs),
-           "rbmd_data_write")
+    keep = dict(pos=c(d["pos"], np.float64), vel=c(d.get("vel"), np.float64), charge=c(d.get("charge"), np.float64),
+                type=c(d["type"], np.int32), molecule=c(d.get("molecule"), np.int32), image=c(d.get("image"), np.int32),
+                mass_by_type=mt, epsilon=c(d.get("eps"), np.float64), sigma=c(d.get("sigma"), np.float64),
+                bonds=bonds if info.n_bonds else None, bond_type=c(d.get("bond_type"), np.int32),
+                bond_coeffs=bc if bc is not None and len(bc) else None,
+                angles=angles if info.n_angles else None, angle_type=c(d.get("angle_type"), np.int32),
+                angle_coeffs=ac if ac is not None and len(ac) else None,
+                dihedrals=dihs if info.n_dihedrals else None, dihedral_type=c(d.get("dihedral_type"), np.int32),
+                dihedral_coeffs=dc if dc is not None and len(dc) else None)
+    arrs = rbmd_data_arrays(**{k: (None if v is None else v.ctypes.data_as(ctypes.c_void_p).value)
+                               for k, v in keep.items()})
+    _check(library().rbmd_data_write_arrays(str(path).encode(), atom_style.encode(), ctypes.byref(info),
+                                            ctypes.byref(arrs)), "rbmd_data_write")

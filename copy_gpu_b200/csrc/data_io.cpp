@@ -322,67 +322,107 @@ RBMD_API rbmd_status rbmd_data_dihedrals(const rbmd_data* d, int32_t* dihedrals,
 
 RBMD_API void rbmd_data_free(rbmd_data* d) { delete d; }
 
+RBMD_API rbmd_status rbmd_data_write_arrays(const char* path, const char* atom_style, const rbmd_data_info* h,
+                                            const rbmd_data_arrays* a) {
+  if (!path || !atom_style || !h || !a || !a->pos || !a->type || h->n_atoms < 1 || h->n_atom_types < 1)
+    return RBMD_ERR_ARG;
+  const std::string style = atom_style;
+  if (style != "atomic" && style != "charge" && style != "full") return RBMD_ERR_ARG;
+  if (style != "atomic" && !a->charge) return RBMD_ERR_ARG;
+  FILE* fp = std::fopen(path, "w");
+  if (!fp) return fail("cannot write", path);
+  const int64_t n = h->n_atoms;
+  const int nt = h->n_atom_types;
+  const int64_t nb = a->bonds ? h->n_bonds : 0, na = a->angles ? h->n_angles : 0;
+  const int64_t nd = a->dihedrals ? h->n_dihedrals : 0;
+  const int nbt = h->n_bond_types > 0 ? h->n_bond_types : 1, nat = h->n_angle_types > 0 ? h->n_angle_types : 1;
+  const int ndt = h->n_dihedral_types > 0 ? h->n_dihedral_types : 1;
+  std::fprintf(fp, "LAMMPS data file written by the B200 force library\n\n");
+  std::fprintf(fp, "%lld atoms\n%d atom types\n", (long long)n, nt);
+  if (nb) std::fprintf(fp, "%lld bonds\n%d bond types\n", (long long)nb, nbt);
+  if (na) std::fprintf(fp, "%lld angles\n%d angle types\n", (long long)na, nat);
+  if (nd) std::fprintf(fp, "%lld dihedrals\n%d dihedral types\n", (long long)nd, ndt);
+  const char* ax[3] = {"xlo xhi", "ylo yhi", "zlo zhi"};
+  std::fprintf(fp, "\n");
+  for (int k = 0; k < 3; ++k) std::fprintf(fp, "%.17g %.17g %s\n", h->box.lo[k], h->box.hi[k], ax[k]);
+  if (a->mass_by_type) {
+    std::fprintf(fp, "\nMasses\n\n");
+    for (int t = 0; t < nt; ++t) std::fprintf(fp, "%d %.17g\n", t + 1, a->mass_by_type[t]);
+  }
+  if (a->epsilon && a->sigma) {
+    std::fprintf(fp, "\nPair Coeffs\n\n");
+    for (int t = 0; t < nt; ++t) std::fprintf(fp, "%d %.17g %.17g\n", t + 1, a->epsilon[t], a->sigma[t]);
+  }
+  if (nb && a->bond_coeffs) {
+    std::fprintf(fp, "\nBond Coeffs # harmonic\n\n");
+    for (int t = 0; t < nbt; ++t)
+      std::fprintf(fp, "%d %.17g %.17g\n", t + 1, a->bond_coeffs[2 * t], a->bond_coeffs[2 * t + 1]);
+  }
+  if (na && a->angle_coeffs) {
+    std::fprintf(fp, "\nAngle Coeffs # harmonic\n\n");
+    for (int t = 0; t < nat; ++t)
+      std::fprintf(fp, "%d %.17g %.17g\n", t + 1, a->angle_coeffs[2 * t], a->angle_coeffs[2 * t + 1]);
+  }
+  if (nd && a->dihedral_coeffs) {
+    std::fprintf(fp, "\nDihedral Coeffs # harmonic\n\n");
+    for (int t = 0; t < ndt; ++t)
+      std::fprintf(fp, "%d %.17g %d %d\n", t + 1, a->dihedral_coeffs[3 * t], (int)a->dihedral_coeffs[3 * t + 1],
+                   (int)a->dihedral_coeffs[3 * t + 2]);
+  }
+  std::fprintf(fp, "\nAtoms # %s\n\n", style.c_str());
+  const double* pos = a->pos;
+  for (int64_t i = 0; i < n; ++i) {
+    const int32_t* im = a->image;
+    const int ix = im ? im[3 * i] : 0, iy = im ? im[3 * i + 1] : 0, iz = im ? im[3 * i + 2] : 0;
+    if (style == "atomic")
+      std::fprintf(fp, "%lld %d %.17g %.17g %.17g %d %d %d\n", (long long)i + 1, a->type[i] + 1, pos[3 * i],
+                   pos[3 * i + 1], pos[3 * i + 2], ix, iy, iz);
+    else if (style == "charge")
+      std::fprintf(fp, "%lld %d %.17g %.17g %.17g %.17g %d %d %d\n", (long long)i + 1, a->type[i] + 1,
+                   a->charge[i], pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], ix, iy, iz);
+    else
+      std::fprintf(fp, "%lld %d %d %.17g %.17g %.17g %.17g %d %d %d\n", (long long)i + 1,
+                   (a->molecule ? a->molecule[i] : (int32_t)i) + 1, a->type[i] + 1, a->charge[i], pos[3 * i],
+                   pos[3 * i + 1], pos[3 * i + 2], ix, iy, iz);
+  }
+  if (a->vel) {
+    std::fprintf(fp, "\nVelocities\n\n");
+    for (int64_t i = 0; i < n; ++i)
+      std::fprintf(fp, "%lld %.17g %.17g %.17g\n", (long long)i + 1, a->vel[3 * i], a->vel[3 * i + 1],
+                   a->vel[3 * i + 2]);
+  }
+  if (nb) {
+    std::fprintf(fp, "\nBonds\n\n");
+    for (int64_t b = 0; b < nb; ++b)
+      std::fprintf(fp, "%lld %d %d %d\n", (long long)b + 1, a->bond_type ? a->bond_type[b] + 1 : 1,
+                   a->bonds[2 * b] + 1, a->bonds[2 * b + 1] + 1);
+  }
+  if (na) {
+    std::fprintf(fp, "\nAngles\n\n");
+    for (int64_t b = 0; b < na; ++b)
+      std::fprintf(fp, "%lld %d %d %d %d\n", (long long)b + 1, a->angle_type ? a->angle_type[b] + 1 : 1,
+                   a->angles[3 * b] + 1, a->angles[3 * b + 1] + 1, a->angles[3 * b + 2] + 1);
+  }
+  if (nd) {
+    std::fprintf(fp, "\nDihedrals\n\n");
+    for (int64_t b = 0; b < nd; ++b)
+      std::fprintf(fp, "%lld %d %d %d %d %d\n", (long long)b + 1, a->dihedral_type ? a->dihedral_type[b] + 1 : 1,
+                   a->dihedrals[4 * b] + 1, a->dihedrals[4 * b + 1] + 1, a->dihedrals[4 * b + 2] + 1,
+                   a->dihedrals[4 * b + 3] + 1);
+  }
+  const bool ok = std::fclose(fp) == 0;
+  return ok ? RBMD_OK : fail("error writing", path);
+}
+
 RBMD_API rbmd_status rbmd_data_write(const char* path, const char* atom_style, const rbmd_data_info* h,
                                      const double* pos, const double* vel, const double* charge,
                                      const int32_t* type, const int32_t* molecule, const int32_t* image,
                                      const double* mass_by_type, const double* epsilon, const double* sigma,
                                      const int32_t* bonds, const int32_t* angles) {
-  if (!path || !atom_style || !h || !pos || !type || h->n_atoms < 1 || h->n_atom_types < 1) return RBMD_ERR_ARG;
-  const std::string style = atom_style;
-  if (style != "atomic" && style != "charge" && style != "full") return RBMD_ERR_ARG;
-  if (style != "atomic" && !charge) return RBMD_ERR_ARG;
-  FILE* fp = std::fopen(path, "w");
-  if (!fp) return fail("cannot write", path);
-  const int64_t n = h->n_atoms;
-  const int nt = h->n_atom_types;
-  const int64_t nb = bonds ? h->n_bonds : 0, na = angles ? h->n_angles : 0;
-  std::fprintf(fp, "LAMMPS data file written by the B200 force library\n\n");
-  std::fprintf(fp, "%lld atoms\n%d atom types\n", (long long)n, nt);
-  if (nb) std::fprintf(fp, "%lld bonds\n%d bond types\n", (long long)nb, h->n_bond_types > 0 ? h->n_bond_types : 1);
-  if (na) std::fprintf(fp, "%lld angles\n%d angle types\n", (long long)na, h->n_angle_types > 0 ? h->n_angle_types : 1);
-  const char* ax[3] = {"xlo xhi", "ylo yhi", "zlo zhi"};
-  std::fprintf(fp, "\n");
-  for (int k = 0; k < 3; ++k) std::fprintf(fp, "%.17g %.17g %s\n", h->box.lo[k], h->box.hi[k], ax[k]);
-  if (mass_by_type) {
-    std::fprintf(fp, "\nMasses\n\n");
-    for (int t = 0; t < nt; ++t) std::fprintf(fp, "%d %.17g\n", t + 1, mass_by_type[t]);
-  }
-  if (epsilon && sigma) {
-    std::fprintf(fp, "\nPair Coeffs\n\n");
-    for (int t = 0; t < nt; ++t) std::fprintf(fp, "%d %.17g %.17g\n", t + 1, epsilon[t], sigma[t]);
-  }
-  std::fprintf(fp, "\nAtoms # %s\n\n", style.c_str());
-  for (int64_t a = 0; a < n; ++a) {
-    const int ix = image ? image[3 * a] : 0, iy = image ? image[3 * a + 1] : 0, iz = image ? image[3 * a + 2] : 0;
-    if (style == "atomic")
-      std::fprintf(fp, "%lld %d %.17g %.17g %.17g %d %d %d\n", (long long)a + 1, type[a] + 1, pos[3 * a],
-                   pos[3 * a + 1], pos[3 * a + 2], ix, iy, iz);
-    else if (style == "charge")
-      std::fprintf(fp, "%lld %d %.17g %.17g %.17g %.17g %d %d %d\n", (long long)a + 1, type[a] + 1, charge[a],
-                   pos[3 * a], pos[3 * a + 1], pos[3 * a + 2], ix, iy, iz);
-    else
-      std::fprintf(fp, "%lld %d %d %.17g %.17g %.17g %.17g %d %d %d\n", (long long)a + 1,
-                   (molecule ? molecule[a] : (int32_t)a) + 1, type[a] + 1, charge[a], pos[3 * a], pos[3 * a + 1],
-                   pos[3 * a + 2], ix, iy, iz);
-  }
-  if (vel) {
-    std::fprintf(fp, "\nVelocities\n\n");
-    for (int64_t a = 0; a < n; ++a)
-      std::fprintf(fp, "%lld %.17g %.17g %.17g\n", (long long)a + 1, vel[3 * a], vel[3 * a + 1], vel[3 * a + 2]);
-  }
-  if (nb) {
-    std::fprintf(fp, "\nBonds\n\n");
-    for (int64_t b = 0; b < nb; ++b)
-      std::fprintf(fp, "%lld 1 %d %d\n", (long long)b + 1, bonds[2 * b] + 1, bonds[2 * b + 1] + 1);
-  }
-  if (na) {
-    std::fprintf(fp, "\nAngles\n\n");
-    for (int64_t b = 0; b < na; ++b)
-      std::fprintf(fp, "%lld 1 %d %d %d\n", (long long)b + 1, angles[3 * b] + 1, angles[3 * b + 1] + 1,
-                   angles[3 * b + 2] + 1);
-  }
-  const bool ok = std::fclose(fp) == 0;
-  return ok ? RBMD_OK : fail("error writing", path);
+  rbmd_data_arrays a{};
+  a.pos = pos; a.vel = vel; a.charge = charge; a.type = type; a.molecule = molecule; a.image = image;
+  a.mass_by_type = mass_by_type; a.epsilon = epsilon; a.sigma = sigma; a.bonds = bonds; a.angles = angles;
+  return rbmd_data_write_arrays(path, atom_style, h, &a);
 }
 
 }  // extern "C"

@@ -19,6 +19,7 @@
 #include <sstream>
 #include <string>
 #include <type_traits>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/rbmd_force.h"
@@ -1801,18 +1802,9 @@ rbmd_status rbmd_force_set_topology(rbmd_force* f, const rbmd_topology* t) {
     std::vector<int32_t> cur(f->row_off_h.begin(), f->row_off_h.end() - 1);
     for (int64_t e = 0; e < nrow; ++e) f->row_idx_h[cur[f->term_atom_h[e]]++] = (int32_t)e;
   }
-  // molecules
-  std::vector<std::vector<int32_t>> members;
-  {
-    std::vector<int32_t> mol(t->molecule, t->molecule + n);
-    int32_t mmax = -1;
-    for (int32_t m : mol) {
-      if (m < 0) { std::snprintf(g_last_error, sizeof g_last_error, "topology: negative molecule id"); return RBMD_ERR_ARG; }
-      mmax = std::max(mmax, m);
-    }
-    members.assign((size_t)mmax + 1, {});
-    for (int64_t a = 0; a < n; ++a) members[mol[a]].push_back((int32_t)a);
-  }
+  // molecules (ids may be sparse): members of each, in atom order
+  std::unordered_map<int32_t, std::vector<int32_t>> members;
+  for (int64_t a = 0; a < n; ++a) members[t->molecule[a]].push_back((int32_t)a);
   // special-bond lists (ModelFileInitCondition::SetSpecialBonds), reduced to one entry per partner
   // carrying the weight of its last occurrence, the one the reference's pair loops keep
   std::vector<std::vector<std::pair<int32_t, double>>> sp(f->special ? n : 0);
@@ -1870,7 +1862,7 @@ rbmd_status rbmd_force_set_topology(rbmd_force* f, const rbmd_topology* t) {
   f->sc_id_h.clear();
   f->sc_fac_h.clear();
   for (int64_t a = 0; a < n; ++a) {
-    const auto& g = members[t->molecule[a]];
+    const auto& g = members.at(t->molecule[a]);
     if (g.size() >= 3) {
       if (!f->special) {
         for (int32_t j : g)

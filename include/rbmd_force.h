@@ -374,6 +374,25 @@ RBMD_API rbmd_status rbmd_data_write(const char* path, const char* atom_style, c
                                      const double* mass_by_type, const double* epsilon, const double* sigma,
                                      const int32_t* bonds, const int32_t* angles);
 
+/* Every section the reader returns, including bond / angle / dihedral types and the harmonic
+ * coefficients of "Bond/Angle/Dihedral Coeffs" (a checkpoint of a molecular system that reads
+ * back identically).  NULL arrays are left out; missing term types are written as type 1.  Counts
+ * come from `info` (n_bonds, n_bond_types, ... n_dihedral_types).  rbmd_data_write is this call
+ * without types, coefficients and dihedrals. */
+typedef struct {
+  const double *pos, *vel, *charge;
+  const int32_t *type, *molecule, *image;
+  const double *mass_by_type, *epsilon, *sigma;
+  const int32_t *bonds, *bond_type;
+  const double* bond_coeffs;       /* [n_bond_types][2] k, r0 */
+  const int32_t *angles, *angle_type;
+  const double* angle_coeffs;      /* [n_angle_types][2] k, theta0 (degrees) */
+  const int32_t *dihedrals, *dihedral_type;
+  const double* dihedral_coeffs;   /* [n_dihedral_types][3] K, sign, multiplicity */
+} rbmd_data_arrays;
+RBMD_API rbmd_status rbmd_data_write_arrays(const char* path, const char* atom_style, const rbmd_data_info* info,
+                                            const rbmd_data_arrays* arrays);
+
 /* Version string of the library build. */
 RBMD_API const char* rbmd_version(void);
 

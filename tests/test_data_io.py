@@ -80,3 +80,18 @@ def test_setfl_and_funcfl_files_load(tmp_path):
     bad.write_text("".join(open(ps).readlines()[:9]))
     with pytest.raises(c.RbmdError, match="ERR_FILE"):
         c.ForceField(systems.eam_config(str(bad)), box)
+
+
+def test_molecular_roundtrip_with_topology(tmp_path):
+    """A flexible-chain system with bond / angle / dihedral types and harmonic coefficients writes
+    (rbmd_data_write_arrays) and reads back identically: a checkpoint of a CVFF system."""
+    from copy_gpu_b200 import systems
+    s = systems.molecular(n_chain=20, chain_len=10, n_ion_pairs=5, seed=7)
+    d = dict(s)
+    d["mass_by_type"] = np.array([12.011, 15.999, 15.035, 6.94, 140.0])
+    p = tmp_path / "mol.data"
+    c.write_data(p, "full", d)
+    r = c.read_data(p, "full", unit="REAL")
+    for k in ("pos", "vel", "charge", "type", "molecule", "bonds", "bond_type", "angles", "angle_type",
+              "dihedrals", "dihedral_type", "bond_coeffs", "angle_coeffs", "dihedral_coeffs"):
+        assert np.array_equal(r[k], d[k]), k
