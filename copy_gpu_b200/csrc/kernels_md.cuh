@@ -461,7 +461,8 @@ struct WaterParams {
 __global__ void k_water_extras(WaterParams wp, const int* __restrict__ hoh, const double* __restrict__ pos,
                                const double* __restrict__ charge, const int* __restrict__ rep_of,
                                const RepDev* __restrict__ reps, double* __restrict__ force,
-                               double* __restrict__ e_bond, double* __restrict__ e_angle) {
+                               double* __restrict__ e_bond, double* __restrict__ e_angle,
+                               double* __restrict__ e_coul) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= wp.n_mol) return;
   const int id[3] = {hoh[3 * w], hoh[3 * w + 1], hoh[3 * w + 2]};
@@ -472,6 +473,7 @@ __global__ void k_water_extras(WaterParams wp, const int* __restrict__ hoh, cons
     q[a] = charge ? charge[id[a]] : 0.0;
     for (int d = 0; d < 3; ++d) x[a][d] = pos[3 * id[a] + d];
   }
+  double ec = 0;   // energy of the removed bare Coulomb pairs, -332.06371 q_a q_b / r per pair
   for (int a = 0; a < 3; ++a)
     for (int b = 0; b < 3; ++b) {
       if (a == b) continue;
@@ -480,6 +482,7 @@ __global__ void k_water_extras(WaterParams wp, const int* __restrict__ hoh, cons
       const double d = sqrt(dot3(r, r));
       const double fc = -wp.coul_const * q[a] * q[b] / (d * d * d);
       for (int k = 0; k < 3; ++k) f[a][k] += fc * r[k];
+      ec += -0.5 * wp.coul_const * q[a] * q[b] / d;
     }
   double eb = 0;
   const int bonds[2][2] = {{0, 1}, {2, 1}};
@@ -515,6 +518,7 @@ __global__ void k_water_extras(WaterParams wp, const int* __restrict__ hoh, cons
     for (int k = 0; k < 3; ++k) force[3 * id[a] + k] += f[a][k];
   if (e_bond) e_bond[w] = eb;
   if (e_angle) e_angle[w] = tk * dth;
+  if (e_coul) e_coul[w] = ec;
 }
 
 // Deterministic sum of a double array into out[0] (one block).

@@ -233,7 +233,7 @@ struct rbmd_force {
   float* d_sp_wf = nullptr;
   // water device
   int* d_hoh = nullptr;
-  double *d_ebond = nullptr, *d_eangle = nullptr;
+  double *d_ebond = nullptr, *d_eangle = nullptr, *d_ewcoul = nullptr;
   // snapshot for step replay
   double *d_snap = nullptr;
   int* d_snap_img = nullptr;
@@ -373,7 +373,7 @@ void free_all(rbmd_force* f) {
   dfree(f->d_frho); dfree(f->d_rhor); dfree(f->d_z2r);
   if (f->d_fp) cudaFree(f->d_fp);
   f->d_fp = nullptr;
-  dfree(f->d_emb); dfree(f->d_epair); dfree(f->d_hoh); dfree(f->d_ebond); dfree(f->d_eangle);
+  dfree(f->d_emb); dfree(f->d_epair); dfree(f->d_hoh); dfree(f->d_ebond); dfree(f->d_eangle); dfree(f->d_ewcoul);
   free_topology(f);
   dfree(f->d_host32);
   dfree(f->d_snap); dfree(f->d_snap_img); dfree(f->d_step); dfree(f->d_lstep);
@@ -1082,7 +1082,7 @@ void launch_water(rbmd_force* f, cudaStream_t s) {
   wp.coul_const = 332.06371;
   k_water_extras<<<(wp.n_mol + 127) / 128, 128, 0, s>>>(wp, f->d_hoh, f->at.pos, f->at.charge,
                                                         f->nrep > 1 ? f->d_rep_of : nullptr, f->d_reps,
-                                                        f->at.force, f->d_ebond, f->d_eangle);
+                                                        f->at.force, f->d_ebond, f->d_eangle, f->d_ewcoul);
   f->launches++;
 }
 
@@ -1688,9 +1688,10 @@ rbmd_status rbmd_force_set_water(rbmd_force* f, int64_t n_mol, const int32_t* ho
     dfree(f->d_hoh);
     CK(dalloc(&f->d_hoh, (size_t)3 * n_mol));
     CK(cudaMemcpy(f->d_hoh, f->hoh_h.data(), sizeof(int) * 3 * n_mol, cudaMemcpyHostToDevice));
-    dfree(f->d_ebond); dfree(f->d_eangle);
+    dfree(f->d_ebond); dfree(f->d_eangle); dfree(f->d_ewcoul);
     CK(dalloc(&f->d_ebond, (size_t)n_mol));
     CK(dalloc(&f->d_eangle, (size_t)n_mol));
+    CK(dalloc(&f->d_ewcoul, (size_t)n_mol));
   }
   return RBMD_OK;
 }
@@ -2285,6 +2286,7 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
     CK(cudaMemcpy(f->d_hoh, f->hoh_h.data(), sizeof(int) * 3 * f->n_mol, cudaMemcpyHostToDevice));
     CK(dalloc(&f->d_ebond, (size_t)f->n_mol));
     CK(dalloc(&f->d_eangle, (size_t)f->n_mol));
+    CK(dalloc(&f->d_ewcoul, (size_t)f->n_mol));
   }
   {
     rbmd_status st = upload_topology(f);
@@ -2498,6 +2500,7 @@ rbmd_status rbmd_force_energy(rbmd_force* f, rbmd_energy* out, void* stream) {
   } else if (f->n_mol > 0 && f->is_cvff()) {
     k_sum<<<1, 1024, 0, s>>>((int)f->n_mol, f->d_ebond, 1, 0, f->d_esum + 6);
     k_sum<<<1, 1024, 0, s>>>((int)f->n_mol, f->d_eangle, 1, 0, f->d_esum + 7);
+    k_sum<<<1, 1024, 0, s>>>((int)f->n_mol, f->d_ewcoul, 1, 0, f->d_esum + 11);
   }
   k_sum<<<1, 1024, 0, s>>>(f->nrep, f->d_ke, 1, 0, f->d_esum + 8);
   k_sum<<<1, 1024, 0, s>>>(f->nrep, f->d_T, 1, 0, f->d_esum + 9);

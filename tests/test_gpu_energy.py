@@ -129,3 +129,11 @@ def test_water_bond_angle_energies(cuda, oracle_lib):
                                           *s["angle"])
     assert abs(e["bond"] - eb) <= 1e-10 * abs(eb) + 1e-12, (e["bond"], eb)
     assert abs(e["angle"] - ea) <= 1e-10 * abs(ea) + 1e-12, (e["angle"], ea)
+    # energy of the removed intramolecular bare Coulomb pairs (ComputeSpecialCoulWorklet)
+    hoh = s["hoh"]
+    bonds = np.concatenate([hoh[:, [0, 1]], hoh[:, [2, 1]]])
+    _, eo = oracle_lib.cvff_terms(s["pos"], s["lo"], s["hi"], s["charge"], s["molecule"], bonds,
+                                  np.zeros(len(bonds), np.int32), np.array([s["bond"]]), hoh,
+                                  np.zeros(len(hoh), np.int32), np.array([s["angle"]]))
+    assert abs(e["coul_special"] - eo["coul_special"]) <= 1e-10 * abs(eo["coul_special"]), \
+        (e["coul_special"], eo["coul_special"])
