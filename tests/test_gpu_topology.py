@@ -200,3 +200,73 @@ def test_topology_nve_energy_conservation_fp64(cuda):
         e, d = total()
         assert abs(e - e0) <= 1e-2 * d0["kinetic"], (e, e0, d0["kinetic"], d)
     ff.close()
+
+
+def test_topology_original_neighbor_type(cuda, oracle_lib):
+    """neighbor.type "ORIGINAL" with special bonds (ComputeSpecialBondsLJWorklet, RunWorklet.cpp:
+    570-632): pairs d^2 < rc^2 with special-bond LJ weights, FP64, against the oracle."""
+    s = systems.molecular(n_chain=64, chain_len=12, n_ion_pairs=16, seed=28)
+    cfg = systems.molecular_config(P=32, precision="fp64", special=(0.0, 0.0, 0.5))
+    cfg["hyper_parameters"]["neighbor"]["type"] = "ORIGINAL"
+    m = _ksamples(oracle_lib, s, cfg)
+    f, _ = _run(s, cfg, cuda, m)
+    hp = cfg["hyper_parameters"]
+    rc, alpha = hp["neighbor"]["cut_off"], hp["coulomb"]["alpha"]
+    sp = oracle_lib.special_lists(len(s["pos"]), s["bonds"], [0.0, 0.0, 0.5])
+    nl = oracle_lib.neighbors(s["pos"], s["lo"], s["hi"], rc, "fp64", original=True)
+    near = oracle_lib.near_force(s["pos"], s["lo"], s["hi"], rc, nl, type=s["type"], charge=s["charge"], eps=s["eps"],
+                                 sigma=s["sigma"], with_coul=True, alpha=alpha, coul_scale=QQR2E, prec="fp64",
+                                 special=sp)
+    L = s["hi"] - s["lo"]
+    far = oracle_lib.rbe_force(s["pos"], s["charge"], L, alpha, QQR2E, m, oracle_lib.rhok(s["pos"], s["charge"], L, m))
+    intra, _ = oracle_lib.cvff_terms(s["pos"], s["lo"], s["hi"], s["charge"], s["molecule"], s["bonds"], s["bond_type"],
+                                     s["bond_coeffs"], s["angles"], s["angle_type"], s["angle_coeffs"], s["dihedrals"],
+                                     s["dihedral_type"], s["dihedral_coeffs"], special=sp)
+    assert rel_err(f, near + far + intra) <= TOL["fp64"]
+
+
+def test_topology_batched_replicas_equal_single(cuda):
+    """Two molecular replicas of different sizes and boxes in one batch (Ewald k-space, so both
+    runs use the same k-vectors): the bonded terms, special weights and Coulomb correction of
+    each replica equal the single-replica run's forces (FP64)."""
+    import torch
+    from copy_gpu_b200 import Box
+    sa = systems.molecular(n_chain=27, chain_len=10, n_ion_pairs=4, seed=31)
+    sb = systems.molecular(n_chain=64, chain_len=8, n_ion_pairs=8, seed=32)
+    cfg = systems.molecular_config(precision="fp64", cutoff=8.0, special=(0.0, 0.0, 0.5))
+    cfg["hyper_parameters"]["coulomb"] = {"type": "EWALD", "alpha": 0.09, "kmax": 3}
+    topo_keys = ("bonds", "bond_type", "bond_coeffs", "angles", "angle_type", "angle_coeffs", "dihedrals",
+                 "dihedral_type", "dihedral_coeffs")
+
+    def single(s):
+        dev = to_dev(s, cuda)
+        ff = make_ff(cfg, s, dev)
+        ff.set_topology(s["molecule"], *[s[k] for k in topo_keys])
+        ff.Execute()
+        torch.cuda.synchronize()
+        assert ff.status() == 0
+        f = dev["force"].cpu().numpy()
+        ff.close()
+        return f
+
+    fa, fb = single(sa), single(sb)
+    na = len(sa["pos"])
+    b = {k: np.concatenate([sa[k], sb[k]]) for k in ("pos", "vel", "mass", "charge", "type")}
+    b["molecule"] = np.concatenate([sa["molecule"], sb["molecule"] + sa["molecule"].max() + 1]).astype(np.int32)
+    b.update(eps=sa["eps"], sigma=sa["sigma"], lo=sa["lo"], hi=sa["hi"])
+    offs = np.array([0, na, na + len(sb["pos"])])
+    boxes = [Box(tuple(sa["lo"]), tuple(sa["hi"])), Box(tuple(sb["lo"]), tuple(sb["hi"]))]
+    dev = to_dev(b, cuda)
+    ff = make_ff(cfg, b, dev, boxes=boxes, offsets=offs)
+    ff.set_topology(b["molecule"], np.concatenate([sa["bonds"], sb["bonds"] + na]),
+                    np.concatenate([sa["bond_type"], sb["bond_type"]]), sa["bond_coeffs"],
+                    np.concatenate([sa["angles"], sb["angles"] + na]),
+                    np.concatenate([sa["angle_type"], sb["angle_type"]]), sa["angle_coeffs"],
+                    np.concatenate([sa["dihedrals"], sb["dihedrals"] + na]),
+                    np.concatenate([sa["dihedral_type"], sb["dihedral_type"]]), sa["dihedral_coeffs"])
+    ff.Execute()
+    torch.cuda.synchronize()
+    assert ff.status() == 0
+    f = dev["force"].cpu().numpy()
+    ff.close()
+    assert rel_err(f[:na], fa) <= 1e-12 and rel_err(f[na:], fb) <= 1e-12
