@@ -1746,6 +1746,11 @@ static rbmd_status upload_topology(rbmd_force* f) {
 rbmd_status rbmd_force_set_topology(rbmd_force* f, const rbmd_topology* t) {
   if (!f || !t || t->n_atoms < 1 || !t->molecule || t->n_bonds < 0 || t->n_angles < 0 || t->n_dihedrals < 0)
     return RBMD_ERR_ARG;
+  if (!f->is_cvff()) {   // the reference adds intramolecular terms for "CVFF" only (ExecutionNVT.cpp:199-215)
+    std::snprintf(g_last_error, sizeof g_last_error, "topology: force_field.type %s has no bonded terms (CVFF does)",
+                  f->ff.c_str());
+    return RBMD_ERR_STATE;
+  }
   const int64_t n = t->n_atoms;
   const int64_t nb = t->n_bonds, na = t->n_angles, nd = f->special ? t->n_dihedrals : 0;
   if ((nb && (!t->bonds || !t->bond_type || !t->bond_coeffs)) ||

@@ -138,7 +138,8 @@ RBMD_API rbmd_status rbmd_force_set_water(rbmd_force* f, int64_t n_mol, const in
  *    and harmonic dihedrals E = K [1 + d cos(n phi)] (ExecutionNVT.cpp:612-680); without
  *    special_bonds the dihedrals are ignored, as in the reference.
  * Supersedes the water extras of rbmd_force_set_water (SHAKE still uses its triples).  Bonded
- * forces are summed per atom in a fixed order (no atomics).  Callable before or after bind. */
+ * forces are summed per atom in a fixed order (no atomics).  Callable before or after bind;
+ * RBMD_ERR_STATE unless force_field.type is "CVFF". */
 typedef struct {
   int64_t n_atoms;
   const int32_t* molecule;                 /* [n_atoms]                                 */

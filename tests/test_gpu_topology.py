@@ -270,3 +270,16 @@ def test_topology_batched_replicas_equal_single(cuda):
     f = dev["force"].cpu().numpy()
     ff.close()
     assert rel_err(f[:na], fa) <= 1e-12 and rel_err(f[na:], fb) <= 1e-12
+
+
+def test_topology_needs_cvff(cuda):
+    """Only force_field CVFF carries bonded terms: set_topology on LJ/CUT/COUL/LONG is an error,
+    not a silent no-op."""
+    from copy_gpu_b200 import Box, ForceField, RbmdError
+    s = systems.molecular(n_chain=8, chain_len=6, n_ion_pairs=2, seed=33)
+    cfg = systems.molecular_config(precision="fp64")
+    cfg["hyper_parameters"]["force_field"]["type"] = "LJ/CUT/COUL/LONG"
+    ff = ForceField(cfg, Box(tuple(s["lo"]), tuple(s["hi"])))
+    with pytest.raises(RbmdError):
+        ff.set_topology(s["molecule"], s["bonds"], s["bond_type"], s["bond_coeffs"])
+    ff.close()
