@@ -1501,7 +1501,9 @@ rbmd_status parse_config(rbmd_force* f, const char* text) {
   //  * compat.rbl_drop_shell_coulomb: the shell Coulomb term is computed and discarded
   //    (RunWorklet.cpp:782);
   //  * compat.eam_verlet_pair_vector: the Verlet EAM force on MinDistanceVec(p_j, p_i)
-  //    (RunWorklet.cpp:402), which reverses it (the RBL pass uses p_i - p_j, :1180).
+  //    (RunWorklet.cpp:402), which reverses it (the RBL pass uses p_i - p_j, :1180);
+  //  * compat.special_bonds_integer: extend.special_bonds read as integers, as Extend does
+  //    (GetVectorValueJudge<int>, rbmd/framework/hyperparameters/Extend.cpp:39): 0.5 becomes 0.
   auto flag = [&](const char* key) {
     const Value* v = root.path(key);
     return v && v->kind == Value::Bool && v->b;
@@ -1509,6 +1511,8 @@ rbmd_status parse_config(rbmd_force* f, const char* text) {
   f->rbl_table = flag("compat.rbl_erf_table");
   f->rbl_shell_coul = !flag("compat.rbl_drop_shell_coulomb");
   f->eam_ref_sign = flag("compat.eam_verlet_pair_vector");
+  if (flag("compat.special_bonds_integer"))
+    for (double& w : f->special_w) w = std::trunc(w);
   if (f->P < 1 || f->P > 65536) return RBMD_ERR_CONFIG;
   return RBMD_OK;
 }

@@ -283,3 +283,20 @@ def test_topology_needs_cvff(cuda):
     with pytest.raises(RbmdError):
         ff.set_topology(s["molecule"], s["bonds"], s["bond_type"], s["bond_coeffs"])
     ff.close()
+
+
+def test_special_bonds_integer_compat(cuda):
+    """compat.special_bonds_integer reads extend.special_bonds as the reference does (integers:
+    [0, 0, 0.5] acts as [0, 0, 0]); by default the 0.5 weight reaches the 1-4 LJ pairs."""
+    s = systems.molecular(n_chain=27, chain_len=8, n_ion_pairs=4, seed=34)
+    f = {}
+    for name, special, compat in (("half", (0.0, 0.0, 0.5), False), ("zero", (0.0, 0.0, 0.0), False),
+                                  ("compat", (0.0, 0.0, 0.5), True)):
+        cfg = systems.molecular_config(P=8, precision="fp64", special=special)
+        if compat:
+            cfg["compat"] = {"special_bonds_integer": True}
+        m = np.array([[1, 0, 0], [0, 1, 0], [0, 0, 1], [1, 1, 0], [1, 0, 1], [0, 1, 1], [1, 1, 1], [2, 0, 0]],
+                     np.int32)
+        f[name], _ = _run(s, cfg, cuda, m)
+    assert np.array_equal(f["compat"], f["zero"])
+    assert not np.array_equal(f["half"], f["zero"])
