@@ -677,6 +677,7 @@ def run_config(args):
                     "fp64_host_buffers": {"value": n / (run["e2e64_ms"] / 1e3), "h2d_bytes_per_step": 24 * n,
                                           "d2h_bytes_per_step": 24 * n}},
             "phase_ms_per_step": {k: v[0] / args.steps for k, v in run["phases"].items() if v[1]},
+            "gpu_launches": run["k_per_step"] * args.steps, "kernels_per_step": run["k_per_step"],
             "status_flags": run["flags"], "clocks": run["clk"], "mean_neighbors": run["n_nbr"],
         }
         del ff

@@ -252,6 +252,10 @@ struct rbmd_force {
   bool in_step = false;          // launches belong to rbmd_force_step (advance d_step)
   bool use_graph = true;         // execution.cuda_graph: replay a captured step
   cudaGraphExec_t graph_exec = nullptr;
+  cudaGraphExec_t graph_multi = nullptr;   // graph_steps consecutive steps in one graph
+  int graph_steps = 8;                     // execution.graph_steps
+  int graph_multi_launches = 0;
+  bool graph_multi_pending = false;
   int graph_launches = 0;
   bool graph_pending = false;    // pending_scale the graph was captured with
   bool capturing = false;
@@ -379,6 +383,8 @@ void free_all(rbmd_force* f) {
   dfree(f->d_snap); dfree(f->d_snap_img); dfree(f->d_step); dfree(f->d_lstep);
   if (f->graph_exec) cudaGraphExecDestroy(f->graph_exec);
   f->graph_exec = nullptr;
+  if (f->graph_multi) cudaGraphExecDestroy(f->graph_multi);
+  f->graph_multi = nullptr;
   if (f->gstream) cudaStreamDestroy(f->gstream);
   f->gstream = nullptr;
   if (f->ev_begin) cudaEventDestroy(f->ev_begin);
@@ -1159,11 +1165,19 @@ void launch_compute_any(rbmd_force* f, cudaStream_t s) {
   else launch_compute<float>(f, s);
 }
 
+// The captured steps bake in buffers, kernel variants and host-side choices (injected
+// k-samples, importance weights, proposal, topology); whatever changes one of them drops them,
+// and the next multi-step call captures again.
+void drop_graphs(rbmd_force* f) {
+  if (f->graph_exec || f->graph_multi) cudaDeviceSynchronize();   // none still in flight
+  if (f->graph_exec) cudaGraphExecDestroy(f->graph_exec);
+  f->graph_exec = nullptr;
+  if (f->graph_multi) cudaGraphExecDestroy(f->graph_multi);
+  f->graph_multi = nullptr;
+}
+
 rbmd_status grow_list(rbmd_force* f, const int* need) {
-  if (f->graph_exec) {
-    cudaGraphExecDestroy(f->graph_exec);   // buffers move: the captured step is stale
-    f->graph_exec = nullptr;
-  }
+  drop_graphs(f);   // buffers move: the captured steps are stale
   auto grown = [](int cur, int want) { return std::max(cur, ((int)(want * 1.2) + 8 + 7) & ~7); };
   if (f->is_rbl()) {
     f->core_cap = grown(f->core_cap, need[0]);
@@ -1304,21 +1318,21 @@ rbmd_status run_steps(rbmd_force* f, int n_steps, cudaStream_t s) {
   }
   launch_step<R>(f, s);
   const int per_step = f->launches;
-  if (!f->graph_exec || f->graph_pending != f->pending_scale) {
-    if (f->graph_exec) cudaGraphExecDestroy(f->graph_exec);
-    f->graph_exec = nullptr;
-    if (!f->gstream) CK(cudaStreamCreateWithFlags(&f->gstream, cudaStreamNonBlocking));
-    if (!f->ev_begin) CK(cudaEventCreateWithFlags(&f->ev_begin, cudaEventDisableTiming));
+  if (!f->gstream) CK(cudaStreamCreateWithFlags(&f->gstream, cudaStreamNonBlocking));
+  if (!f->ev_begin) CK(cudaEventCreateWithFlags(&f->ev_begin, cudaEventDisableTiming));
+  // capture `steps` consecutive steps into *exec (host-side state restored afterwards: the
+  // kernels take the step index, rebuild flags and noise counters from device memory)
+  auto capture = [&](int steps, cudaGraphExec_t* exec, int* launches) -> rbmd_status {
     const long long sc = f->step_count;
     const bool pend = f->pending_scale;
     const int l0 = f->launches;
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(f->gstream, cudaStreamCaptureModeThreadLocal));
     f->capturing = true;
-    launch_step<R>(f, f->gstream);
+    for (int k = 0; k < steps; ++k) launch_step<R>(f, f->gstream);
     f->capturing = false;
     const cudaError_t e = cudaStreamEndCapture(f->gstream, &g);
-    f->graph_launches = f->launches - l0;
+    *launches = f->launches - l0;
     f->launches = l0;
     f->step_count = sc;
     f->pending_scale = pend;
@@ -1327,16 +1341,40 @@ rbmd_status run_steps(rbmd_force* f, int n_steps, cudaStream_t s) {
       if (g) cudaGraphDestroy(g);
       return RBMD_ERR_CUDA;
     }
-    const cudaError_t ei = cudaGraphInstantiate(&f->graph_exec, g, 0);
+    const cudaError_t ei = cudaGraphInstantiate(exec, g, 0);
     cudaGraphDestroy(g);
     if (ei != cudaSuccess) {
       std::snprintf(g_last_error, sizeof g_last_error, "step graph: %s", cudaGetErrorString(ei));
-      f->graph_exec = nullptr;
+      *exec = nullptr;
       return RBMD_ERR_CUDA;
     }
-    f->graph_pending = pend;
+    return RBMD_OK;
+  };
+  if (!f->graph_exec || f->graph_pending != f->pending_scale) {
+    if (f->graph_exec) cudaGraphExecDestroy(f->graph_exec);
+    f->graph_exec = nullptr;
+    rbmd_status st = capture(1, &f->graph_exec, &f->graph_launches);
+    if (st) return st;
+    f->graph_pending = f->pending_scale;
   }
-  for (int k = 1; k < n_steps; ++k) {
+  int remaining = n_steps - 1;
+  const int m = f->graph_steps;
+  if (m > 1 && remaining >= m) {
+    // several steps per graph launch: small systems pay the graph launch once per m steps
+    if (!f->graph_multi || f->graph_multi_pending != f->pending_scale) {
+      if (f->graph_multi) cudaGraphExecDestroy(f->graph_multi);
+      f->graph_multi = nullptr;
+      rbmd_status st = capture(m, &f->graph_multi, &f->graph_multi_launches);
+      if (st) return st;
+      f->graph_multi_pending = f->pending_scale;
+    }
+    for (; remaining >= m; remaining -= m) {
+      CK(cudaGraphLaunch(f->graph_multi, s));
+      f->step_count += m;
+      f->launches += f->graph_multi_launches;
+    }
+  }
+  for (; remaining > 0; --remaining) {
     CK(cudaGraphLaunch(f->graph_exec, s));
     f->step_count++;
     f->launches += f->graph_launches ? f->graph_launches : per_step;
@@ -1433,6 +1471,12 @@ rbmd_status parse_config(rbmd_force* f, const char* text) {
     if (kp && kp->kind == Value::Bool) f->kspace_priority = kp->b;
     const Value* g = root.path("execution.cuda_graph");
     if (g && g->kind == Value::Bool) f->use_graph = g->b;
+    const int gs = (int)num(root, "execution.graph_steps", 8.0);
+    if (gs < 1 || gs > 64) {
+      std::snprintf(g_last_error, sizeof g_last_error, "config: execution.graph_steps must be 1..64");
+      return RBMD_ERR_CONFIG;
+    }
+    f->graph_steps = gs;
   }
   std::vector<double> T = nums(root, "execution.temperature");
   f->T0 = T.size() > 0 ? T[0] : 1.0;
@@ -1664,6 +1708,7 @@ rbmd_status rbmd_force_create(const char* json_text, int32_t n_replicas, const r
 
 rbmd_status rbmd_force_set_pair_coeffs(rbmd_force* f, int32_t n_types, const double* epsilon,
                                        const double* sigma) {
+  if (f) drop_graphs(f);
   if (!f || !epsilon || !sigma || n_types < 1 || n_types > kMaxReplicaTypes) return RBMD_ERR_ARG;
   fill_lj(f, n_types, epsilon, sigma);
   f->have_pair_coeffs = true;
@@ -1681,6 +1726,7 @@ rbmd_status rbmd_force_load_funcfl(rbmd_force* f, const char* path) {
 
 rbmd_status rbmd_force_set_water(rbmd_force* f, int64_t n_mol, const int32_t* hoh, double bond_k,
                                  double bond_r0, double angle_k, double angle_theta0_deg) {
+  if (f) drop_graphs(f);
   if (!f || n_mol < 0 || (n_mol > 0 && !hoh)) return RBMD_ERR_ARG;
   f->n_mol = n_mol;
   f->hoh_h.assign(hoh, hoh + 3 * n_mol);
@@ -1748,6 +1794,7 @@ static rbmd_status upload_topology(rbmd_force* f) {
 }
 
 rbmd_status rbmd_force_set_topology(rbmd_force* f, const rbmd_topology* t) {
+  if (f) drop_graphs(f);
   if (!f || !t || t->n_atoms < 1 || !t->molecule || t->n_bonds < 0 || t->n_angles < 0 || t->n_dihedrals < 0)
     return RBMD_ERR_ARG;
   if (!f->is_cvff()) {   // the reference adds intramolecular terms for "CVFF" only (ExecutionNVT.cpp:199-215)
@@ -2310,6 +2357,7 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
 }
 
 rbmd_status rbmd_force_set_ksamples(rbmd_force* f, const int32_t* m_xyz, int32_t P) {
+  if (f) drop_graphs(f);
   if (!f) return RBMD_ERR_ARG;
   if (!m_xyz || P == 0) {
     f->injected = false;
@@ -2320,6 +2368,7 @@ rbmd_status rbmd_force_set_ksamples(rbmd_force* f, const int32_t* m_xyz, int32_t
 }
 
 rbmd_status rbmd_force_set_kweights(rbmd_force* f, const double* w_host) {
+  if (f) drop_graphs(f);
   if (!f || !f->bound || !f->is_rbe()) return RBMD_ERR_ARG;
   if (!w_host) { dfree(f->d_weights); return RBMD_OK; }
   if (!f->d_weights) CK(dalloc(&f->d_weights, (size_t)f->Ptot));
@@ -2349,6 +2398,7 @@ rbmd_status rbmd_force_sample_k(rbmd_force* f, int64_t step, int32_t* m_xyz, int
 }
 
 rbmd_status rbmd_force_autotune(rbmd_force* f, void* stream, int32_t* list_lanes, int32_t* force_lanes) {
+  if (f) drop_graphs(f);
   if (!f) return RBMD_ERR_ARG;
   if (!f->bound) return RBMD_ERR_STATE;
   cudaStream_t s = (cudaStream_t)stream;
@@ -2594,6 +2644,7 @@ rbmd_status rbmd_force_get_rbl(rbmd_force* f, int32_t* ncore, int32_t* nshell, i
 
 rbmd_status rbmd_force_train_proposal(rbmd_force* f, const rbmd_train_opts* o, rbmd_train_report* rep,
                                       void* stream) {
+  if (f) drop_graphs(f);
   if (!f || !o) return RBMD_ERR_ARG;
   if (!f->bound || f->proposal != "learned" || !f->d_prep) return RBMD_ERR_STATE;
   if (o->n_snapshots < 1 || o->k_per_snapshot < 256 || o->iterations < 1 || o->steps_between < 0 ||
@@ -2661,6 +2712,7 @@ rbmd_status rbmd_force_train_proposal(rbmd_force* f, const rbmd_train_opts* o, r
 }
 
 rbmd_status rbmd_force_proposal_params(rbmd_force* f, float* get_host, const float* set_host) {
+  if (f && set_host) drop_graphs(f);
   if (!f || (!get_host && !set_host)) return RBMD_ERR_ARG;
   if (!f->bound || !f->d_mlp) return RBMD_ERR_STATE;
   if (set_host) {

@@ -486,3 +486,33 @@ def test_cuda_graph_water_shake(cuda):
         assert ff.status() == 0
         out.append(dev["pos"].cpu().numpy())
     assert np.array_equal(out[0], out[1])
+
+
+def test_graph_steps_and_state_changes(cuda):
+    """execution.graph_steps: 8 steps per graph launch give the same trajectory bit for bit as one
+    step per graph launch; a k-set injected between step() calls reaches the replayed steps
+    (the captured graphs are dropped when host-side state they depend on changes)."""
+    import torch
+    out = []
+    for gs in (1, 8, None):
+        s = systems.electrolyte(3000, seed=18)
+        cfg = systems.electrolyte_config(P=32, precision="fp32", seed=5)
+        cfg["hyper_parameters"]["neighbor"]["skin"] = 0.3
+        if gs is None:
+            cfg["execution"]["cuda_graph"] = False
+        else:
+            cfg["execution"]["graph_steps"] = gs
+        dev = to_dev(s, cuda)
+        ff = make_ff(cfg, s, dev)
+        ff.Execute()
+        ff.step(20)
+        m = np.array([[1, 0, 0], [0, 1, 0], [0, 0, 1], [1, 1, 0]] * 8, np.int32)
+        ff.set_ksamples(m)
+        ff.step(20)
+        ff.sync_velocities()
+        torch.cuda.synchronize()
+        assert ff.status() == 0
+        out.append((dev["pos"].cpu().numpy(), dev["vel"].cpu().numpy()))
+        ff.close()
+    for o in out[1:]:
+        assert np.array_equal(out[0][0], o[0]) and np.array_equal(out[0][1], o[1])
