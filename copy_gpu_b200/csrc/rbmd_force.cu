@@ -1717,6 +1717,7 @@ rbmd_status rbmd_force_set_pair_coeffs(rbmd_force* f, int32_t n_types, const dou
 }
 
 rbmd_status rbmd_force_load_funcfl(rbmd_force* f, const char* path) {
+  if (f) drop_graphs(f);
   if (!f || !path) return RBMD_ERR_ARG;
   if (eam_load(path, f->eam_h, f->potential_format) != 0) return RBMD_ERR_FILE;
   f->eam_loaded = true;
