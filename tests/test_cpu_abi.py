@@ -121,3 +121,36 @@ def test_as_7_1_26_erfc_bound():
     approx = poly * t * np.exp(-x * x)
     exact = np.array([math.erfc(v) for v in x])
     assert np.abs(approx - exact).max() <= 1.5e-7
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """Every public struct of include/rbmd_force.h has the size and field offsets of its ctypes
+    mirror in copy_gpu_b200 (a C program compiled against the header prints them)."""
+    import ctypes
+    import shutil
+    import subprocess
+    import copy_gpu_b200 as c
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    structs = {"rbmd_box": c.rbmd_box, "rbmd_atoms_dev": c.rbmd_atoms_dev, "rbmd_energy": c.rbmd_energy,
+               "rbmd_topology": c.rbmd_topology, "rbmd_train_opts": c.rbmd_train_opts,
+               "rbmd_train_report": c.rbmd_train_report, "rbmd_data_info": c.rbmd_data_info,
+               "rbmd_data_arrays": c.rbmd_data_arrays}
+    lines = ['#include <stdio.h>', '#include "rbmd_force.h"', "int main(void) {"]
+    for name, cls in structs.items():
+        lines.append(f'  printf("{name} size %zu\\n", sizeof({name}));')
+        for field, _ in cls._fields_:
+            lines.append(f'  printf("{name} {field} %zu\\n", offsetof({name}, {field}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    subprocess.run([cc, "-std=c11", "-I", inc, "-o", str(exe), str(src)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    for line in filter(None, out):
+        name, what, val = line.split()
+        cls = structs[name]
+        got = ctypes.sizeof(cls) if what == "size" else getattr(cls, what).offset
+        assert got == int(val), (name, what, got, val)
