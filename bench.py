@@ -61,7 +61,7 @@ def parse():
     ap.add_argument("--ion-frac", type=float, default=0.1,
                     help="fraction of charged atoms of the electrolyte (0.1 is the headline workload)")
     ap.add_argument("--workload", default="electrolyte",
-                    choices=["electrolyte", "lj", "water", "eam", "batched", "molecular"],
+                    choices=["electrolyte", "lj", "water", "eam", "batched", "molecular", "molecular_verlet"],
                     help="electrolyte: the headline metric (default); the others time the remaining "
                          "configurations (plain MD steps, atom-steps/s) beside the CPU oracle")
     ap.add_argument("--skin", type=float, default=0.3,
@@ -553,6 +553,12 @@ def config_system(name, tmpdir):
         cfg["hyper_parameters"]["neighbor"]["skin"] = 0.3
         return s, cfg, None, None, ("Johnson EAM Cu FCC 256000 atoms (5000-point funcfl), rc 5.0 A + skin 0.3, "
                                     "300 K displacements, FP32, NVE")
+    if name == "molecular_verlet":
+        # the same system with the Verlet list (rc 12 A + skin 1 A, list reuse) instead of RBL
+        s, cfg, _, _, _ = config_system("molecular", tmpdir)
+        cfg["hyper_parameters"]["neighbor"] = {"type": "VERLETLIST", "cut_off": 12.0, "skin": 1.0}
+        return s, cfg, None, None, (f"flexible chains + ions, {len(s['pos'])} atoms, CVFF topology, special bonds "
+                                    "0/0/0, VERLETLIST rc 12 A + skin 1.0 A, RBE P=100, REAL units, FP32 forces")
     if name == "molecular":
         # the shape of the reference's polymer-electrolyte input (rbmd/res/json_files/PEO): CVFF
         # with bonds, angles, dihedrals and special bonds 0/0/0, RBL rc 12 A / r_core 6 A / 100
@@ -592,6 +598,21 @@ def cpu_config_eval(name, s, cfg, offsets, tmpdir):
         return total, atoms
     pos = s["pos"].astype(np.float32 if prec == "fp32" else np.float64)
     L = s["hi"] - s["lo"]
+    if name == "molecular_verlet":
+        co = hp["coulomb"]
+        t0 = time.perf_counter()
+        sp = oracle.special_lists(len(pos), s["bonds"], hp["extend"]["special_bonds"])
+        nl = oracle.neighbors(pos, s["lo"], s["hi"], rc, prec)
+        oracle.near_force(pos, s["lo"], s["hi"], rc, nl, type=s["type"], charge=s["charge"], eps=s["eps"],
+                          sigma=s["sigma"], with_coul=True, alpha=co["alpha"], coul_scale=332.06371, prec=prec,
+                          special=sp)
+        m = oracle.rbe_sample(co["alpha"], L, 7, 0, 0, co["coulomb_sample_num"])
+        rho = oracle.rhok(pos, s["charge"], L, m, prec=prec)
+        oracle.rbe_force(pos, s["charge"], L, co["alpha"], 332.06371, m, rho, prec=prec)
+        oracle.cvff_terms(s["pos"], s["lo"], s["hi"], s["charge"], s["molecule"], s["bonds"], s["bond_type"],
+                          s["bond_coeffs"], s["angles"], s["angle_type"], s["angle_coeffs"], s["dihedrals"],
+                          s["dihedral_type"], s["dihedral_coeffs"], special=sp)
+        return time.perf_counter() - t0, len(pos)
     if name == "molecular":
         nb, co = hp["neighbor"], hp["coulomb"]
         t0 = time.perf_counter()

@@ -7,7 +7,7 @@ import bench
 from copy_gpu_b200 import systems
 
 
-@pytest.mark.parametrize("name", ["lj", "water", "eam", "batched", "molecular"])
+@pytest.mark.parametrize("name", ["lj", "water", "eam", "batched", "molecular", "molecular_verlet"])
 def test_config_systems(tmp_path, name):
     s, cfg, boxes, offs, desc = bench.config_system(name, str(tmp_path))
     n = s["pos"].shape[0]
@@ -19,8 +19,8 @@ def test_config_systems(tmp_path, name):
         assert boxes is None and offs is None
     if name == "eam":
         assert cfg["hyper_parameters"]["force_field"]["type"] == "EAM"
-    if name == "molecular":
-        assert cfg["hyper_parameters"]["neighbor"]["type"] == "RBL"
+    if name.startswith("molecular"):
+        assert cfg["hyper_parameters"]["neighbor"]["type"] == ("RBL" if name == "molecular" else "VERLETLIST")
         assert len(s["dihedrals"]) > 0 and abs(s["charge"].sum()) < 1e-9
 
 
