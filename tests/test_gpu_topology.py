@@ -300,3 +300,32 @@ def test_special_bonds_integer_compat(cuda):
         f[name], _ = _run(s, cfg, cuda, m)
     assert np.array_equal(f["compat"], f["zero"])
     assert not np.array_equal(f["half"], f["zero"])
+
+
+def test_water_special_bonds_zero_equals_exclusion_rbl(cuda):
+    """The reference's H2O example shape (CVFF, RBL, special_bonds [0, 0, 0], rbmd/examples/H2O):
+    water given as a general topology takes the special-bond path, where every intramolecular
+    pair is a 1-2 or 1-3 partner with weight 0; its forces equal those of the molecule-exclusion
+    water path to summation order (FP64)."""
+    import torch
+    s = systems.water(n_mol=400, seed=6)
+    out = []
+    for general in (False, True):
+        cfg = systems.water_config(P=16, precision="fp64")
+        cfg["hyper_parameters"]["neighbor"] = {"type": "RBL", "cut_off": 10.0, "r_core": 5.0,
+                                               "neighbor_sample_num": 100}
+        if not general:
+            del cfg["hyper_parameters"]["extend"]["special_bonds"]
+        dev = to_dev(s, cuda)
+        ff = make_ff(cfg, s, dev)
+        if general:
+            hoh = s["hoh"]
+            bonds = np.concatenate([hoh[:, [0, 1]], hoh[:, [2, 1]]])
+            ff.set_topology(s["molecule"], bonds, np.zeros(len(bonds), np.int32), np.array([s["bond"]]), hoh,
+                            np.zeros(len(hoh), np.int32), np.array([s["angle"]]))
+        ff.Execute()
+        torch.cuda.synchronize()
+        assert ff.status() == 0
+        out.append(dev["force"].cpu().numpy())
+        ff.close()
+    assert rel_err(out[1], out[0]) <= 1e-12
