@@ -195,7 +195,10 @@ def water(n_mol=10000, density=1.0, T=298.0, seed=9):
 # ------------------------------------------------------------------------------------------
 # EAM
 # ------------------------------------------------------------------------------------------
-JOHNSON_CU = dict(re=2.556, fe=1.0, rho_e=12.0, phi_e=0.59, Ec=3.54, beta=5.85, gamma=8.0,
+# phi_e solves dE/da = 0 at a = 3.615 A for the three FCC neighbour shells inside the 5.0 A
+# cutoff (E per atom = F(rho) + 1/2 sum phi; stable: d2E/da2 = 4.2 eV/A^2, E = -2.29 eV per atom),
+# so the benchmark crystal starts at the potential's equilibrium lattice constant.
+JOHNSON_CU = dict(re=2.556, fe=1.0, rho_e=12.0, phi_e=0.2235, Ec=3.54, beta=5.85, gamma=8.0,
                   cutoff=5.0, npts=5000, rho_max=30.0, mass=63.546, a=3.615)
 
 

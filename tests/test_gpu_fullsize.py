@@ -8,7 +8,10 @@
   the same forces, although cells, slots, list order and fixed-point phases all change.  In FP64
   runs to 1e-9; in FP32 runs the positions themselves round differently once shifted (an ulp of
   a 100-sigma coordinate is 8e-6 sigma, and r^-13 pair forces of close contacts amplify it), so
-  the bar is 2e-3 there;
+  the bar is 2e-3 there, and 5e-3 for the EAM crystal, whose forces at its equilibrium lattice
+  constant come from the thermal displacements alone (rms 0.5 eV/A) while the rounding of 144 A
+  coordinates (1.5e-5 A) times the pair curvature stays the same; a cell, slot or list error
+  would be of order one;
 * momentum conservation: NVE steps of the batch keep every replica's momentum.
 """
 import numpy as np
@@ -68,7 +71,7 @@ def test_eam_256k_newton_and_translation(cuda, tmp_path):
     f0 = _forces(cfg, s, cuda)
     assert _net(f0) < 1e-7, _net(f0)
     f1 = _forces(cfg, _shifted(s, SHIFT), cuda)
-    assert rel_err(f1, f0) < 2e-3, rel_err(f1, f0)
+    assert rel_err(f1, f0) < 5e-3, rel_err(f1, f0)
 
 
 def test_batched_512_newton_and_momentum(cuda):
