@@ -61,6 +61,19 @@ template <> struct Traits<double> {
 struct Frac32 { uint32_t x, y, z; float q; };               // 16 B
 struct Frac64 { unsigned long long x, y, z; double q; };     // 32 B
 
+// Fixed-point turn of a fractional coordinate f in [0, 1]: floor(f * 2^32) (2^64).  f can round
+// up to exactly 1.0 (f = u - floor(u) for u a hair below an integer); that is a whole turn and
+// wraps to 0, as periodicity requires.  A NaN coordinate gives an unspecified turn (the status
+// word's non-finite flag is raised by the force passes).
+__host__ __device__ __forceinline__ uint32_t turn32(double f) {
+  const double s = f * 4294967296.0;
+  return s >= 4294967296.0 ? 0u : (uint32_t)s;
+}
+__host__ __device__ __forceinline__ unsigned long long turn64(double f) {
+  const double s = f * 18446744073709551616.0;
+  return s >= 18446744073709551616.0 ? 0ull : (unsigned long long)s;
+}
+
 // exact-rounding arithmetic (never contracted into FMA): used wherever the result must equal
 // the oracle bit for bit (cell index, neighbour predicate)
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }

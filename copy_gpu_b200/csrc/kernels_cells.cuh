@@ -230,9 +230,7 @@ __global__ void __launch_bounds__(32 * kSortWarps) k_cell_sort_gather(
         uint32_t U[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-          double f = u[d] - floor(u[d]);
-          double s = f * 4294967296.0;
-          U[d] = s >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)s;
+          U[d] = turn32(u[d] - floor(u[d]));
         }
         Frac32 fr{U[0], U[1], U[2], (float)q};
         reinterpret_cast<Frac32*>(frac_out)[slot] = fr;
@@ -240,9 +238,7 @@ __global__ void __launch_bounds__(32 * kSortWarps) k_cell_sort_gather(
         unsigned long long U[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-          double f = u[d] - floor(u[d]);
-          double s = f * 18446744073709551616.0;
-          U[d] = s >= 18446744073709549568.0 ? 0xFFFFFFFFFFFFF800ull : (unsigned long long)s;
+          U[d] = turn64(u[d] - floor(u[d]));
         }
         Frac64 fr{U[0], U[1], U[2], q};
         reinterpret_cast<Frac64*>(frac_out)[slot] = fr;
@@ -292,17 +288,13 @@ __global__ void k_regather(int n, const int* __restrict__ slot_atom, const doubl
     if (sizeof(R) == 4) {
       uint32_t U[3];
       for (int d = 0; d < 3; ++d) {
-        double f = u[d] - floor(u[d]);
-        double s = f * 4294967296.0;
-        U[d] = s >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)s;
+        U[d] = turn32(u[d] - floor(u[d]));
       }
       reinterpret_cast<Frac32*>(frac_out)[slot] = Frac32{U[0], U[1], U[2], (float)q};
     } else {
       unsigned long long U[3];
       for (int d = 0; d < 3; ++d) {
-        double f = u[d] - floor(u[d]);
-        double s = f * 18446744073709551616.0;
-        U[d] = s >= 18446744073709549568.0 ? 0xFFFFFFFFFFFFF800ull : (unsigned long long)s;
+        U[d] = turn64(u[d] - floor(u[d]));
       }
       reinterpret_cast<Frac64*>(frac_out)[slot] = Frac64{U[0], U[1], U[2], q};
     }
@@ -679,16 +671,14 @@ __global__ void k_frac(int nq, const int* __restrict__ qidx, const double* __res
     uint32_t U[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      const double s = u[d] * 4294967296.0;
-      U[d] = s >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)s;
+      U[d] = turn32(u[d]);
     }
     reinterpret_cast<Frac32*>(frac_out)[c] = Frac32{U[0], U[1], U[2], (float)q};
   } else {
     unsigned long long U[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      const double s = u[d] * 18446744073709551616.0;
-      U[d] = s >= 18446744073709549568.0 ? 0xFFFFFFFFFFFFF800ull : (unsigned long long)s;
+      U[d] = turn64(u[d]);
     }
     reinterpret_cast<Frac64*>(frac_out)[c] = Frac64{U[0], U[1], U[2], q};
   }

@@ -17,13 +17,20 @@
 //   * every call on a device shares the one array and leaves its contents behind; all of it is
 //     overwritten before it is read, so nothing needs clearing between calls, but calls that
 //     overlap on the GPU (different streams, or different host threads) race on it;
-//   * the first call on each device looks up the array's device address with
-//     cudaGetSymbolAddress (the array's name is only a host-side stand-in in host code); make
-//     that first call before any stream capture begins.
+//   * the array's device address comes from cudaGetSymbolAddress (in host code the array's
+//     name is only a host-side stand-in).  Each call made while its stream is not capturing
+//     looks the address up again in the current context, so a device reset or another context
+//     on the device never leaves a stale address behind; the first call on a device (and after a
+//     reset) does this set-up, so make it before any stream capture begins.  A call made during
+//     capture reuses the address recorded for the current context and refuses (RBMD_ERR_CUDA)
+//     when none is recorded;
+//   * a NaN position gives unspecified structure factors (its fixed-point turn is undefined).
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstdint>
+#include <cstdarg>
 #include <cstdio>
 #include <mutex>
 
@@ -47,8 +54,44 @@ constexpr int kMaxDevices = 64;
 // name is a stand-in, the device address comes from cudaGetSymbolAddress.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
+// Per device: the scratch address and the id of the context it was looked up in.
 std::mutex g_mu;
 void* g_scratch_ptr[kMaxDevices] = {};
+unsigned long long g_scratch_ctx[kMaxDevices] = {};
+
+void set_error(const char* fmt, ...) __attribute__((format(printf, 1, 2)));
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(rbmd_internal::g_last_error, sizeof rbmd_internal::g_last_error, fmt, ap);
+  va_end(ap);
+}
+
+// Unique id of the calling thread's current context (cuCtxGetId, CUDA 12.0+), reached through
+// the runtime's driver entry points so that the library needs no link to libcuda.  0 if unknown.
+unsigned long long current_context_id() {
+  using GetCurrent = CUresult (*)(CUcontext*);
+  using GetId = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrent>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetId>(f);
+  });
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS)
+    return 0;
+  return id;
+}
 
 __global__ void k_na_frac(int n, const double* __restrict__ pos, const double* __restrict__ charge,
                           double lo0, double lo1, double lo2, double L0, double L1, double L2,
@@ -59,10 +102,8 @@ __global__ void k_na_frac(int n, const double* __restrict__ pos, const double* _
   uint32_t U[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    double u = (pos[3 * i + d] - lo[d]) / L[d];
-    u -= floor(u);
-    const double s = u * 4294967296.0;
-    U[d] = s >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)s;
+    const double u = (pos[3 * i + d] - lo[d]) / L[d];
+    U[d] = rbmd::turn32(u - floor(u));   // a whole turn wraps to 0
   }
   frac[i] = rbmd::Frac32{U[0], U[1], U[2], (float)charge[i]};
 }
@@ -130,37 +171,69 @@ extern "C" {
 RBMD_API rbmd_status rbmd_rhok_noalloc(const double* pos_dev, const double* charge_dev, int32_t n,
                                        const rbmd_box* box, const int32_t* m_dev, int32_t P,
                                        double* rho_dev, void* stream) {
-  if (!pos_dev || !charge_dev || !box || !m_dev || !rho_dev || n < 1 || P < 1) return RBMD_ERR_ARG;
+  if (!pos_dev || !charge_dev || !box || !m_dev || !rho_dev || n < 1 || P < 1) {
+    set_error("rbmd_rhok_noalloc: null pointer or non-positive size (n=%d, P=%d)", n, P);
+    return RBMD_ERR_ARG;
+  }
   const int nchunks = (n + kNoAllocChunk - 1) / kNoAllocChunk;
   const size_t partial_bytes = (size_t)nchunks * P * 2 * sizeof(float);
   if (n > kNoAllocMaxAtoms || P > kNoAllocMaxK || kNoAllocFracBytes + partial_bytes > kNoAllocScratchBytes) {
-    std::snprintf(rbmd_internal::g_last_error, sizeof rbmd_internal::g_last_error, "rbmd_rhok_noalloc: n=%d, P=%d exceed the fixed scratch (n <= %d, P <= %d)",
-                  n, P, kNoAllocMaxAtoms, kNoAllocMaxK);
+    set_error("rbmd_rhok_noalloc: n=%d, P=%d exceed the fixed scratch (n <= %d, P <= %d)", n, P,
+              kNoAllocMaxAtoms, kNoAllocMaxK);
     return RBMD_ERR_ARG;
   }
   double L[3];
   for (int d = 0; d < 3; ++d) {
     L[d] = box->hi[d] - box->lo[d];
-    if (!(L[d] > 0)) return RBMD_ERR_ARG;
+    if (!(L[d] > 0)) {
+      set_error("rbmd_rhok_noalloc: box length %g along axis %d is not positive", L[d], d);
+      return RBMD_ERR_ARG;
+    }
+  }
+  // an error left pending by the caller's earlier work is reported as such, not as ours
+  const cudaError_t pending = cudaGetLastError();
+  if (pending != cudaSuccess) {
+    set_error("rbmd_rhok_noalloc: a CUDA error from earlier work was pending (nothing launched): %s",
+              cudaGetErrorString(pending));
+    return RBMD_ERR_CUDA;
   }
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return RBMD_ERR_CUDA;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    set_error("rbmd_rhok_noalloc: cudaGetDevice: %s", cudaGetErrorString(e));
+    return RBMD_ERR_CUDA;
+  }
+  if (dev < 0 || dev >= kMaxDevices) {
+    set_error("rbmd_rhok_noalloc: device %d is beyond the %d devices this entry point serves", dev, kMaxDevices);
+    return RBMD_ERR_CUDA;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
+    cudaGetLastError();                       // the query's own error; treat as capturing
+    cap = cudaStreamCaptureStatusActive;
+  }
+  const unsigned long long ctx = current_context_id();
   void* base = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_ptr[dev]) {
-      // once per device, with that device current: the device address of the static array
+    if (cap == cudaStreamCaptureStatusNone) {
+      // with the device current: the static array's address in the current context
       void* p = nullptr;
-      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
       if (e != cudaSuccess || !p) {
-        std::snprintf(rbmd_internal::g_last_error, sizeof rbmd_internal::g_last_error, "rbmd_rhok_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+        set_error("rbmd_rhok_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
         return RBMD_ERR_CUDA;
       }
       g_scratch_ptr[dev] = p;
+      g_scratch_ctx[dev] = ctx;
+    } else if (!g_scratch_ptr[dev] || ctx == 0 || g_scratch_ctx[dev] != ctx) {
+      set_error("rbmd_rhok_noalloc: called during stream capture before any call in this context "
+                "(make the first call outside capture)");
+      return RBMD_ERR_CUDA;
     }
     base = g_scratch_ptr[dev];
   }
-  cudaStream_t s = (cudaStream_t)stream;
   rbmd::Frac32* frac = reinterpret_cast<rbmd::Frac32*>(base);
   float* partial = reinterpret_cast<float*>(static_cast<unsigned char*>(base) + kNoAllocFracBytes);
   k_na_frac<<<(n + 255) / 256, 256, 0, s>>>(n, pos_dev, charge_dev, box->lo[0], box->lo[1], box->lo[2], L[0],
@@ -168,9 +241,9 @@ RBMD_API rbmd_status rbmd_rhok_noalloc(const double* pos_dev, const double* char
   const int threads = ((P + 31) / 32) * 32;
   k_na_rho<<<nchunks, threads, 0, s>>>(n, P, frac, m_dev, partial);
   k_na_finish<<<(P + 3) / 4, 128, 0, s>>>(P, nchunks, partial, rho_dev);
-  const cudaError_t e = cudaGetLastError();
+  e = cudaGetLastError();
   if (e != cudaSuccess) {
-    std::snprintf(rbmd_internal::g_last_error, sizeof rbmd_internal::g_last_error, "rbmd_rhok_noalloc: %s", cudaGetErrorString(e));
+    set_error("rbmd_rhok_noalloc: launch failed: %s", cudaGetErrorString(e));
     return RBMD_ERR_CUDA;
   }
   return RBMD_OK;

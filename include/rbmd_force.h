@@ -280,8 +280,12 @@ RBMD_API void rbmd_force_destroy(rbmd_force* f);
  * memory through its own pool or a fixed budget, or a step loop that cannot take the device-wide
  * synchronisation of cudaFree.  Limits: n <= 262144, P <= 1024, else
  * RBMD_ERR_ARG.  All calls on a device share the array: calls that overlap on the GPU race.
- * The first call on each device resolves the array's address and should precede any stream
- * capture.  No counterpart in the reference. */
+ * Every call made outside stream capture resolves the array's address in the current context
+ * (so a device reset leaves nothing stale); the first call on each device, and the first after
+ * a reset, should precede any stream capture, since a call during capture only reuses the
+ * address recorded for its context (RBMD_ERR_CUDA if there is none).  A CUDA error already
+ * pending from the caller's earlier work is returned as RBMD_ERR_CUDA before anything is
+ * launched.  NaN positions give unspecified rho.  No counterpart in the reference. */
 RBMD_API rbmd_status rbmd_rhok_noalloc(const double* pos_dev, const double* charge_dev, int32_t n,
                                        const rbmd_box* box, const int32_t* m_dev, int32_t P,
                                        double* rho_dev, void* stream);

@@ -5,12 +5,13 @@ and as text (rbmd/res/json_files/Gnear_table_leq2_2.txt for 0.1 <= d < 2,
 Gnear_table_geq2_2.txt for 2 <= d < 12; columns: entry index, distance, spacing, G, dG).  This
 script keeps every second row (and the last) of each text file as (index, distance, G) so that
 the oracle's reconstruction of the table is pinned against the reference's own numbers.
-Run it in a checkout that has the reference at REF (default /root/reference).
+Run it in a checkout that has the reference at REF (first argument, else $RBMD_REFERENCE,
+default /root/reference).
 """
 import os
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("RBMD_REFERENCE", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 

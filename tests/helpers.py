@@ -36,15 +36,28 @@ def make_ff(cfg, sysd, dev, boxes=None, offsets=None):
     return ff
 
 
-def pair_sets_equal(c_a, ids_a, c_b, ids_b):
-    """Per-atom neighbour sets (as sorted lists) identical; returns the first mismatching atom or -1."""
+def pair_sets_equal(c_a, ids_a, c_b, ids_b, rows=1 << 16):
+    """Per-atom neighbour sets (as sorted lists) identical; returns the first mismatching atom or -1.
+    Rows are compared in blocks (sorted with the unused tail padded), so that a million atoms take
+    seconds."""
+    c_a = np.asarray(c_a)
+    c_b = np.asarray(c_b)
     if not np.array_equal(c_a, c_b):
         return int(np.nonzero(c_a != c_b)[0][0])
-    for i in range(len(c_a)):
-        a = np.sort(ids_a[i, :c_a[i]])
-        b = np.sort(ids_b[i, :c_b[i]])
-        if not np.array_equal(a, b):
-            return i
+    w = int(c_a.max()) if len(c_a) else 0
+    if w == 0:
+        return -1
+    big = np.iinfo(np.int32).max
+    for r0 in range(0, len(c_a), rows):
+        r1 = min(len(c_a), r0 + rows)
+        tail = np.arange(w)[None, :] >= c_a[r0:r1, None]
+        a = np.where(tail, big, ids_a[r0:r1, :w]).astype(np.int64)
+        b = np.where(tail, big, ids_b[r0:r1, :w]).astype(np.int64)
+        a.sort(axis=1)
+        b.sort(axis=1)
+        bad = np.nonzero((a != b).any(axis=1))[0]
+        if len(bad):
+            return r0 + int(bad[0])
     return -1
 
 

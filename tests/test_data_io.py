@@ -10,7 +10,7 @@ import pytest
 import copy_gpu_b200 as c
 from copy_gpu_b200 import systems
 
-REF = "/root/reference/rbmd/res/json_files"
+REF = os.path.join(os.environ.get("RBMD_REFERENCE", "/root/reference"), "rbmd", "res", "json_files")
 
 
 @pytest.mark.parametrize("style", ["atomic", "charge", "full"])

@@ -214,7 +214,7 @@ def test_data_reader_dihedrals(tmp_path):
     assert d["bond_type"].tolist() == [0] * 5 and d["angle_type"].tolist() == [0] * 4
 
 
-PEO = "/root/reference/rbmd/res/json_files/PEO/rbmd.data"
+PEO = os.path.join(os.environ.get("RBMD_REFERENCE", "/root/reference"), "rbmd", "res", "json_files", "PEO", "rbmd.data")
 
 
 @pytest.mark.skipif(not os.path.exists(PEO), reason="reference tree not present")

@@ -54,6 +54,38 @@ def test_rhok_noalloc_matches_force_path(cuda, oracle_lib):
         assert np.abs(got - ref64).max() / np.abs(ref64).max() <= TOL
 
 
+def test_rhok_noalloc_at_its_limits(cuda, oracle_lib):
+    """The fixed scratch at its stated limits (n = 262144 atoms, all charged: 128 chunks, the
+    partials at the 4 MiB offset; P = 1024: a 1024-thread block) and a P that is not a multiple
+    of 32 (a partly filled last warp), against the FP64 oracle, two calls in a row each."""
+    import torch
+    import copy_gpu_b200 as c
+
+    lib = c.library()
+    stream = torch.cuda.current_stream()
+    rng = np.random.default_rng(31)
+    for n, P in ((262144, 1024), (5000, 77)):
+        L = np.array([60.0, 64.0, 70.0])
+        lo = np.array([-3.0, 1.5, 0.25])
+        pos = lo + rng.random((n, 3)) * L
+        q = rng.choice([-1.0, 1.0], size=n)
+        m = rng.integers(-12, 13, size=(P, 3)).astype(np.int32)
+        m[np.all(m == 0, axis=1)] = (1, 0, 0)
+        ref64 = oracle_lib.rhok(pos, q, L, m, origin=lo)
+        box = c.Box(tuple(lo), tuple(lo + L)).c()
+        x_d = torch.tensor(pos, dtype=torch.float64, device=cuda).contiguous()
+        q_d = torch.tensor(q, dtype=torch.float64, device=cuda)
+        m_d = torch.tensor(m, dtype=torch.int32, device=cuda).contiguous()
+        for call in range(2):
+            rho = torch.full((P, 2), float("nan"), dtype=torch.float64, device=cuda)
+            st = lib.rbmd_rhok_noalloc(x_d.data_ptr(), q_d.data_ptr(), n, ctypes.byref(box), m_d.data_ptr(), P,
+                                       rho.data_ptr(), stream.cuda_stream)
+            assert st == c.RBMD_OK, lib.rbmd_last_error()
+            torch.cuda.synchronize()
+            err = np.abs(rho.cpu().numpy() - ref64).max() / np.abs(ref64).max()
+            assert err <= TOL, f"n={n} P={P} call {call}: rel err {err:.3e}"
+
+
 def test_rhok_noalloc_rejects_oversize(cuda):
     import torch
     import copy_gpu_b200 as c
@@ -69,3 +101,11 @@ def test_rhok_noalloc_rejects_oversize(cuda):
     assert b"exceed" in lib.rbmd_last_error()
     assert lib.rbmd_rhok_noalloc(x.data_ptr(), q.data_ptr(), 8, ctypes.byref(box), m.data_ptr(), 1025,
                                  rho.data_ptr(), None) == c.RBMD_ERR_ARG
+    # every refusal leaves its own message (not a stale one from an earlier call)
+    flat = c.Box((0.0, 0.0, 0.0), (10.0, 0.0, 10.0)).c()
+    assert lib.rbmd_rhok_noalloc(x.data_ptr(), q.data_ptr(), 8, ctypes.byref(flat), m.data_ptr(), 8,
+                                 rho.data_ptr(), None) == c.RBMD_ERR_ARG
+    assert b"not positive" in lib.rbmd_last_error()
+    assert lib.rbmd_rhok_noalloc(x.data_ptr(), q.data_ptr(), 0, ctypes.byref(box), m.data_ptr(), 8,
+                                 rho.data_ptr(), None) == c.RBMD_ERR_ARG
+    assert b"non-positive size" in lib.rbmd_last_error()
