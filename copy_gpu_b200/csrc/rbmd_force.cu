@@ -13,6 +13,7 @@
 #include <random>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <functional>
@@ -467,9 +468,10 @@ void rbl_sizes(const rbmd_force* f, int r, int64_t* z) {
 // (bits 15..25 of the float distance) holds Gnear(alpha = 0.1, d_k) evaluated as the reference's
 // ExecForceFunction::Gnear does in float ((1.0 - erf(x)) / d^2 in double, the rest in float,
 // rbmd/framework/forceFunction/ExecForceFunction.h:217-224) at d_k = the bucket's lower edge
-// rounded up to 4 decimals below d = 2 and to 3 decimals above, and not below 0.1.  Entries
-// 921..2047 cover 0.1 <= d < 2, entries 0..639 cover 2 <= d < 12; that rule reproduces every
-// entry of the reference's tables to their printed 6 significant digits.
+// rounded up to 4 decimals below d = 2 and to 3 decimals above, and not below 0.1, then rounded
+// to the 6 significant decimal digits the reference's table literals carry.  Entries 921..2047
+// cover 0.1 <= d < 2, entries 0..639 cover 2 <= d < 12; the rule reproduces 1734 of the 1766
+// entries exactly and the other 32 to one unit in their sixth digit (at most 5e-6 relative).
 std::vector<float> rbl_erf_table() {
   std::vector<float> t(2048, 0.f);
   auto fill = [&](int k0, int k1, int exp_base, int dec) {
@@ -488,7 +490,9 @@ std::vector<float> rbl_erf_table() {
       const double t1 = (1.0 - (double)std::erf(x)) / (double)(df * df);
       const float pif = 3.14159265358979323846f;
       const float t2 = 2.0f * std::sqrt(a) * std::exp(-a * df * df) / (std::sqrt(pif) * df);
-      t[k] = (float)(t1 + (double)t2);
+      char buf[32];
+      std::snprintf(buf, sizeof buf, "%.6g", (double)(float)(t1 + (double)t2));
+      t[k] = (float)std::strtod(buf, nullptr);
     }
   };
   fill(921, 2048, 123, 4);   // exponents 123..127 -> index high bits 3..7

@@ -116,6 +116,22 @@ def rbe_sample(alpha, L, seed, step, rep, P):
     return out
 
 
+def rbe_sample_trace(alpha, L, seed, step, rep, P):
+    """rbe_sample plus the uniforms it used, in the order RBEPSAMPLE consumes them."""
+    out = np.zeros((P, 3), np.int32)
+    Lb = np.ascontiguousarray(L, dtype=np.float64)
+    f = lib().oracle_rbe_sample_trace
+    f.restype = ctypes.c_int64
+    cap = 16 * P + 64
+    while True:
+        tr = np.zeros(cap)
+        k = f(D(alpha), _p(Lb, D), ctypes.c_uint64(seed), ctypes.c_int64(step), int(rep), int(P), _p(out, I32),
+              _p(tr, D), ctypes.c_int64(cap))
+        if k <= cap:
+            return out, tr[:k]
+        cap = int(k)
+
+
 def rbe_S(alpha, box, prec="fp64"):
     b = np.ascontiguousarray(box, dtype=np.float64)
     return getattr(lib(), "oracle_rbe_S_" + ("f32" if prec == "fp32" else "f64"))(D(alpha), _p(b, D))
@@ -250,7 +266,8 @@ def rbl_table_g(dis):
 
 def rbl_near(pos, lo, hi, cutoff, rs, pice, rl, core_cap, *, type=None, mol=None, charge=None, eps=(1.0,),
              sigma=(1.0,), with_coul=False, alpha=0.0, qqr2e=1.0, table_mode=0, shell_coul=1,
-             remove_mean=True, prec="fp32", special=None):
+             remove_mean=True, prec="fp32", special=None, sum_mode=1):
+    """sum_mode 1: pair terms summed in FP64; 0 (FP32 only): the reference's float accumulators."""
     dt, ct, sfx = _real(prec)
     x = np.ascontiguousarray(pos, dtype=dt)
     n = x.shape[0]
@@ -270,7 +287,8 @@ def rbl_near(pos, lo, hi, cutoff, rs, pice, rl, core_cap, *, type=None, mol=None
             _p(codes, I32), int(with_coul), D(alpha), D(qqr2e), int(table_mode), int(shell_coul),
             int(remove_mean), _p(so, ctypes.c_int64), _p(si, I32), _p(sw, D), _p(out, D))
         return out
-    getattr(lib(), "oracle_rbl_near_" + sfx)(
+    name = "oracle_rbl_near_ref_f32" if (sum_mode == 0 and sfx == "f32") else "oracle_rbl_near_" + sfx
+    getattr(lib(), name)(
         ctypes.c_int64(n), _p(x, ct), _p(np.asarray(lo, np.float64), D), _p(np.asarray(hi, np.float64), D),
         D(cutoff), D(rs), ctypes.c_int64(pice), _p(t, I32), _p(m, I32), _p(q, D),
         _p(np.ascontiguousarray(eps, np.float64), D), _p(np.ascontiguousarray(sigma, np.float64), D),

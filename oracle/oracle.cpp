@@ -308,8 +308,11 @@ SamplerTables sampler_tables(double alpha, const double* L) {
   return t;
 }
 
+// trace (nullable): the uniforms in the order RBEPSAMPLE consumes them (FetchSample_1D's U1,
+// re-drawn while below 1e-6, then U2; MH_Algorithm's acceptance u after them), so that the
+// reference's sampler can be run on the same draws.
 inline double gauss_draw(uint32_t k0, uint32_t k1, int64_t step, int rep, int axis, int64_t draw,
-                         double* ua) {
+                         double* ua, std::vector<double>* trace = nullptr, bool mh = false) {
   U4 c;
   c.v[0] = (uint32_t)draw;
   c.v[1] = (uint32_t)axis | ((uint32_t)rep << 2);
@@ -317,10 +320,21 @@ inline double gauss_draw(uint32_t k0, uint32_t k1, int64_t step, int rep, int ax
   c.v[3] = (uint32_t)((uint64_t)step >> 32);
   U4 r = philox(c, k0, k1);
   double U1 = u01(r.v[0]);
-  if (U1 < 1e-6) U1 = u01(r.v[3]);
-  if (U1 < 1e-6) U1 = 1e-6;
+  if (trace) trace->push_back(U1);
+  if (U1 < 1e-6) {
+    U1 = u01(r.v[3]);
+    if (trace) trace->push_back(U1);
+  }
+  if (U1 < 1e-6) {
+    U1 = 1e-6;
+    if (trace) trace->push_back(U1);
+  }
   double U2 = u01(r.v[1]);
   *ua = u01(r.v[2]);
+  if (trace) {
+    trace->push_back(U2);
+    if (mh) trace->push_back(*ua);
+  }
   return std::sqrt(-2.0 * std::log(U1)) * std::cos(2.0 * M_PI * U2);
 }
 
@@ -329,14 +343,15 @@ inline double gval(const SamplerTables& t, int d, int m) {
   return m <= t.qmax ? t.G[d][m] : INFINITY;
 }
 
-void rbe_sample(const SamplerTables& t, uint64_t seed, int64_t step, int rep, int P, int32_t* out) {
+void rbe_sample(const SamplerTables& t, uint64_t seed, int64_t step, int rep, int P, int32_t* out,
+                std::vector<double>* trace = nullptr) {
   uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
   int64_t draw = 0;
   int X0[3];
   for (;;) {
     for (int d = 0; d < 3; ++d) {
       double ua;
-      double g = gauss_draw(k0, k1, step, rep, d, draw, &ua);
+      double g = gauss_draw(k0, k1, step, rep, d, draw, &ua, trace, false);
       X0[d] = (int)std::round(t.sigma[d] * g);
     }
     ++draw;
@@ -348,7 +363,7 @@ void rbe_sample(const SamplerTables& t, uint64_t seed, int64_t step, int rep, in
     int X1[3];
     for (int d = 0; d < 3; ++d) {
       double ua;
-      double g = gauss_draw(k0, k1, step, rep, d, draw, &ua);
+      double g = gauss_draw(k0, k1, step, rep, d, draw, &ua, trace, true);
       int mw = (int)std::round(t.sigma[d] * g);
       X1[d] = (ua * gval(t, d, X0[d]) <= gval(t, d, mw)) ? mw : X0[d];
     }
@@ -527,6 +542,17 @@ EXPORT void oracle_near_f64(int64_t n, const double* pos, const double* lo, cons
                     codes, with_lj, with_coul, alpha, coul_scale, sum_mode, force_out);
 }
 
+// The same draw, also returning the uniforms it used in RBEPSAMPLE's consumption order
+// (trace[cap]); returns their number (the trace is cut at cap).
+EXPORT int64_t oracle_rbe_sample_trace(double alpha, const double* L, uint64_t seed, int64_t step, int rep,
+                                       int P, int32_t* m_out, double* trace, int64_t cap) {
+  SamplerTables t = sampler_tables(alpha, L);
+  std::vector<double> tr;
+  rbe_sample(t, seed, step, rep, P, m_out, &tr);
+  for (int64_t i = 0; i < (int64_t)tr.size() && i < cap; ++i) trace[i] = tr[i];
+  return (int64_t)tr.size();
+}
+
 // RBE k-sampler (see rbe_sample above).
 EXPORT void oracle_rbe_sample(double alpha, const double* L, uint64_t seed, int64_t step, int rep,
                               int P, int32_t* m_out) {
@@ -602,6 +628,36 @@ static void rbe_force_impl(int64_t n, const Real* pos, const double* charge, con
     k2[l] = kx[l] * kx[l] + ky[l] * ky[l] + kz[l] * kz[l];
   }
   const Real fourpi = (Real)(4.0 * M_PI);
+  if constexpr (sizeof(Real) == 4) {
+    // The reference's FP32 operation order: per k, factor_a = (float)((-4 pi q) k_d) in double
+    // (a Float64 scalar times a Vec3f), term = (factor_a / (V |k|^2)) * (cos(k.r) Im rho -
+    // sin(k.r) Re rho), summed over k in float, then times S and divided by P in double
+    // (ComputeRBEForceSum / ComputeRBEForce, ExecForceFunction.h:247-264).
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+      const float x = pos[3 * i] - (float)origin[0], y = pos[3 * i + 1] - (float)origin[1],
+                  z = pos[3 * i + 2] - (float)origin[2];
+      const double a4 = -4.0 * M_PI * (double)(float)charge[i];
+      float f[3] = {0, 0, 0};
+      for (int l = 0; l < P; ++l) {
+        const float k[3] = {kx[l], ky[l], kz[l]};
+        const float ph = k[0] * x + k[1] * y + k[2] * z;
+        const float fb = std::cos(ph) * (float)rho[2 * l + 1];
+        const float fc = std::sin(ph) * (float)rho[2 * l];
+        const float den = volume * k2[l];
+        const float w = weights ? (float)weights[l] : 1.0f;
+        for (int d = 0; d < 3; ++d) {
+          const float fa = (float)(a4 * (double)k[d]);
+          float t = fa / den * (fb - fc);
+          if (weights) t *= w;
+          f[d] += t;
+        }
+      }
+      for (int d = 0; d < 3; ++d)
+        force_out[3 * i + d] = (double)(float)((double)(f[d] * S) / (double)P) * qqr2e;
+    }
+    return;
+  }
 #pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < n; ++i) {
     Real x = pos[3 * i] - (Real)origin[0], y = pos[3 * i + 1] - (Real)origin[1],
@@ -1587,7 +1643,8 @@ void rbl_list(const Grid<Real>& g, const Cells<Real>& c, int64_t n, const Real* 
 // TableGnearValue, rbmd/framework/staticTable/ExecStaticTable.h:37-39,96-135): the entry of a
 // float distance is its bits 15..25; the entry's value is the reference's float Gnear(0.1, d_k)
 // with d_k the entry's lower bucket edge rounded up to 4 decimals (d < 2) or 3 decimals (d >= 2),
-// and at least 0.1.  The reference's tables hold entries for 0.1 <= d < 12 only; outside, this
+// and at least 0.1, rounded to the 6 significant digits of the table's literals (1734 of the
+// 1766 entries exact, the others within one unit of the sixth digit).  The reference's tables hold entries for 0.1 <= d < 12 only; outside, this
 // evaluates G(0.1, d) in FP64 (the reference would read past its arrays).
 inline float rbl_table_g(float dis) {
   if (!(dis >= 0.1f && dis < 12.0f)) {
@@ -1604,7 +1661,10 @@ inline float rbl_table_g(float dis) {
   const double v = (double)edge * sc, rv = std::nearbyint(v);
   double d = (std::fabs(v - rv) < 1e-6 ? rv : std::ceil(v)) / sc;
   if (d < 0.1) d = 0.1;
-  return gnear<float>(0.1f, (float)d);
+  // the table's literals carry 6 significant decimal digits
+  char buf[32];
+  std::snprintf(buf, sizeof buf, "%.6g", (double)gnear<float>(0.1f, (float)d));
+  return (float)std::strtod(buf, nullptr);
 }
 
 template <class Real>
@@ -1616,7 +1676,7 @@ static void rbl_near_impl(int64_t n, const Real* pos, const double* lo, const do
                           const int32_t* codes, int with_coul, double alpha, double qqr2e,
                           int table_mode, int shell_coul, int remove_mean, double* force_out,
                           const int64_t* sp_off = nullptr, const int32_t* sp_ids = nullptr,
-                          const double* sp_w = nullptr) {
+                          const double* sp_w = nullptr, int sum_mode = 1) {
   Grid<Real> g = make_grid<Real>(lo, hi, cutoff, rs);
   const Real rc = (Real)cutoff, r_s = (Real)rs, a = (Real)alpha;
   const int64_t row = core_cap + shell_cap;
@@ -1628,6 +1688,10 @@ static void rbl_near_impl(int64_t n, const Real* pos, const double* lo, const do
     const Real eps_i = (Real)eps[ti], sig_i = (Real)sig[ti];
     const Real qi = charge ? (Real)charge[i] : (Real)0;
     double lj[3] = {0, 0, 0}, el[3] = {0, 0, 0};
+    // sum_mode 0: the reference's accumulators in Real (core LJ, shell LJ, core Coulomb, shell
+    // Coulomb), combined as (core + shell LJ) + qqr2e (core + shell Coulomb)
+    // (ComputeNearForceRBLERFWorklet, RunWorklet.cpp:754-812)
+    Real acc[4][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
     auto pair = [&](int64_t slot, bool shell) {
       const int j = ids[i * row + slot];
       Real off[3];
@@ -1650,7 +1714,10 @@ static void rbl_near_impl(int64_t n, const Real* pos, const double* lo, const do
           else gv = sizeof(Real) == 4 ? gnear<Real>(a, dism) : gnear_fp64<Real>(a, dism);
           const Real sc = -qi * qj * gv;
           const Real w = shell ? (Real)pice : (Real)1;
-          for (int d = 0; d < 3; ++d) el[d] += (double)(w * (sc * r[d] / dis));
+          for (int d = 0; d < 3; ++d) {
+            if (sum_mode == 0) acc[shell ? 3 : 2][d] += w * (sc * r[d] / dis);
+            else el[d] += (double)(w * (sc * r[d] / dis));
+          }
         }
       }
       if (!sp_off && mi == mj) return;
@@ -1672,11 +1739,17 @@ static void rbl_near_impl(int64_t n, const Real* pos, const double* lo, const do
         const Real w = (Real)special_weight(sp_off, sp_ids, sp_w, i, j);
         for (int d = 0; d < 3; ++d) f[d] = w * f[d];
       }
-      for (int d = 0; d < 3; ++d) lj[d] += (double)f[d];
+      for (int d = 0; d < 3; ++d) {
+        if (sum_mode == 0) acc[shell ? 1 : 0][d] += f[d];
+        else lj[d] += (double)f[d];
+      }
     };
     for (int32_t p = 0; p < std::min<int64_t>(ncore[i], core_cap); ++p) pair(p, false);
     for (int32_t p = 0; p < std::min<int64_t>(nshell[i], shell_cap); ++p) pair(core_cap + p, true);
-    for (int d = 0; d < 3; ++d) force_out[3 * i + d] = lj[d] + qqr2e * el[d];
+    for (int d = 0; d < 3; ++d)
+      force_out[3 * i + d] = sum_mode == 0
+          ? (double)((acc[0][d] + acc[1][d]) + (Real)qqr2e * (acc[2][d] + acc[3][d]))
+          : lj[d] + qqr2e * el[d];
   }
   if (remove_mean) {
     double m[3] = {0, 0, 0};
@@ -1824,6 +1897,17 @@ EXPORT void oracle_rbl_near_f32(int64_t n, const float* pos, const double* lo, c
   rbl_near_impl<float>(n, pos, lo, hi, cutoff, rs, pice, type, mol, charge, eps, sig, core_cap, shell_cap,
                        ncore, nshell, ids, codes, with_coul, alpha, qqr2e, table_mode, shell_coul,
                        remove_mean, out);
+}
+// The same in the reference's float accumulation order (the worklet's four accumulators).
+EXPORT void oracle_rbl_near_ref_f32(int64_t n, const float* pos, const double* lo, const double* hi, double cutoff,
+                                    double rs, int64_t pice, const int32_t* type, const int32_t* mol,
+                                    const double* charge, const double* eps, const double* sig, int64_t core_cap,
+                                    int64_t shell_cap, const int32_t* ncore, const int32_t* nshell,
+                                    const int32_t* ids, const int32_t* codes, int with_coul, double alpha,
+                                    double qqr2e, int table_mode, int shell_coul, int remove_mean, double* out) {
+  rbl_near_impl<float>(n, pos, lo, hi, cutoff, rs, pice, type, mol, charge, eps, sig, core_cap, shell_cap,
+                       ncore, nshell, ids, codes, with_coul, alpha, qqr2e, table_mode, shell_coul,
+                       remove_mean, out, nullptr, nullptr, nullptr, 0);
 }
 EXPORT void oracle_rbl_near_f64(int64_t n, const double* pos, const double* lo, const double* hi, double cutoff,
                                 double rs, int64_t pice, const int32_t* type, const int32_t* mol,

@@ -31,14 +31,15 @@ def _posr(pos, prec):
     return pos.astype(np.float32) if prec == "fp32" else pos.astype(np.float64)
 
 
-def _kspace(pos, charge, L, alpha, qqr2e, m, origin=(0.0, 0.0, 0.0), oracle=None):
-    """FP64 RBE force of the charged atoms, scattered back to all atoms."""
+def _kspace(pos, charge, L, alpha, qqr2e, m, origin=(0.0, 0.0, 0.0), oracle=None, prec="fp64"):
+    """RBE force of the charged atoms (FP64, or the reference's FP32 terms), scattered back to all
+    atoms."""
     q = np.nonzero(charge != 0)[0]
     out = np.zeros((pos.shape[0], 3))
     if len(q) == 0:
         return out
-    rho = oracle.rhok(pos[q], charge[q], L, m, origin=origin)
-    out[q] = oracle.rbe_force(pos[q], charge[q], L, alpha, qqr2e, m, rho, origin=origin)
+    rho = oracle.rhok(pos[q], charge[q], L, m, origin=origin, prec=prec)
+    out[q] = oracle.rbe_force(pos[q], charge[q], L, alpha, qqr2e, m, rho, origin=origin, prec=prec)
     return out
 
 
@@ -135,8 +136,13 @@ def test_water_30k_pairs_and_force(cuda, oracle_lib):
                                  coul_scale=qqr2e, prec="fp32", sum_mode=1)
     far = _kspace(s["pos"], s["charge"], L, alpha, qqr2e, m, oracle=oracle_lib)
     ex, _ = oracle_lib.water_extras(s["hoh"], s["pos"], s["charge"], s["lo"], s["hi"], *s["bond"], *s["angle"])
-    err = rel_err(g["force"], near + far + ex)
-    assert err <= TOL["fp32"], f"30k water force rel err {err:.3e}"
+    ref = near + far + ex
+    err = rel_err(g["force"], ref)
+    # The k-space rule of the FP32 tests: no larger than the error of the reference's own FP32
+    # k-space arithmetic (float cos(k.r) at |k.r| up to ~100 rad in this 67 A box) against FP64.
+    far32 = _kspace(pr, s["charge"], L, alpha, qqr2e, m, oracle=oracle_lib, prec="fp32")
+    err_ref = rel_err(near + far32 + ex, ref)
+    assert err <= max(TOL["fp32"], err_ref), f"30k water force rel err {err:.3e} (reference FP32 k-space {err_ref:.3e})"
 
 
 def test_lj_4000_fcc_fp64_pairs_force_and_trajectory(cuda, oracle_lib):
@@ -157,7 +163,9 @@ def test_lj_4000_fcc_fp64_pairs_force_and_trajectory(cuda, oracle_lib):
     nl = oracle_lib.neighbors(s["pos"], s["lo"], s["hi"], 2.5, "fp64")
     assert pair_sets_equal(c, ids, nl[0], nl[1]) == -1
     F = oracle_lib.near_force(s["pos"], s["lo"], s["hi"], 2.5, nl, prec="fp64")
-    assert rel_err(dev["force"].cpu().numpy(), F) <= TOL["fp64"]
+    # the perfect lattice: every force vanishes by symmetry (rounding of about 1e-13 left), so the
+    # start is checked in absolute terms against the nearest-neighbour pair force (about 4)
+    assert np.abs(dev["force"].cpu().numpy() - F).max() <= 1e-11
     x, v = s["pos"].copy(), s["vel"].copy()
     lo, hi = s["lo"], s["hi"]
     m = s["mass"][:, None]
