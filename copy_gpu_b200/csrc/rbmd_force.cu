@@ -1549,7 +1549,8 @@ rbmd_status parse_config(rbmd_force* f, const char* text) {
   //  * compat.rbl_drop_shell_coulomb: the shell Coulomb term is computed and discarded
   //    (RunWorklet.cpp:782);
   //  * compat.eam_verlet_pair_vector: the Verlet EAM force on MinDistanceVec(p_j, p_i)
-  //    (RunWorklet.cpp:402), which reverses it (the RBL pass uses p_i - p_j, :1180);
+  //    (RunWorklet.cpp:402), which reverses it (the RBL pass uses p_i - p_j, :1180, and so do the
+  //    ORIGINAL type's on-the-fly worklets, :419-524, which the flag therefore leaves alone);
   //  * compat.special_bonds_integer: extend.special_bonds read as integers, as Extend does
   //    (GetVectorValueJudge<int>, rbmd/framework/hyperparameters/Extend.cpp:39): 0.5 becomes 0.
   auto flag = [&](const char* key) {
@@ -1558,7 +1559,7 @@ rbmd_status parse_config(rbmd_force* f, const char* text) {
   };
   f->rbl_table = flag("compat.rbl_erf_table");
   f->rbl_shell_coul = !flag("compat.rbl_drop_shell_coulomb");
-  f->eam_ref_sign = flag("compat.eam_verlet_pair_vector");
+  f->eam_ref_sign = flag("compat.eam_verlet_pair_vector") && f->nbr_type == "VERLETLIST";
   if (flag("compat.special_bonds_integer"))
     for (double& w : f->special_w) w = std::trunc(w);
   if (f->P < 1 || f->P > 65536) return RBMD_ERR_CONFIG;

@@ -234,3 +234,18 @@ def erf_table(dis):
     out = np.zeros_like(d)
     lib().ref_erf_table(ctypes.c_int64(d.shape[0]), _p(d, F), _p(out, F))
     return out
+
+
+def eam_original(tables, pos, lo, hi, cutoff):
+    """The ORIGINAL neighbour type's EAM worklets (cells walked on the fly); (force, fp) float32."""
+    x = _f32(pos)
+    n = x.shape[0]
+    fp = np.zeros(n, np.float32)
+    out = np.zeros((n, 3), np.float32)
+    fr, rr, zr = _f32(tables["frho"]), _f32(tables["rhor"]), _f32(tables["z2r"])
+    lib().ref_eam_original(ctypes.c_int64(n), _p(x, F), _p(_f64(lo), D), _p(_f64(hi), D), ctypes.c_double(cutoff),
+                           int(tables["nrho"]), ctypes.c_double(tables["drho"]), int(tables["nr"]),
+                           ctypes.c_double(tables["dr"]), ctypes.c_double(tables["rhomax"]), _p(fr, F),
+                           ctypes.c_int64(fr.shape[0]), _p(rr, F), ctypes.c_int64(rr.shape[0]), _p(zr, F),
+                           ctypes.c_int64(zr.shape[0]), _p(fp, F), _p(out, F))
+    return out, fp

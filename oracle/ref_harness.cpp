@@ -488,3 +488,47 @@ EXPORT void ref_erf_table(int64_t n, const float* dis, float* g) {
     g[i] = table.TableGnearValue(dis[i], k);
   }
 }
+
+// The ORIGINAL neighbour type's EAM (ExecutionMD::ComputeOriginalEAMForce,
+// rbmd/framework/run/ExecutionMD.cpp:863-893): ComputeEAMrhoWorklet, ComputeEAMfpWorklet and
+// ComputeEAMforceWorklet (RunWorklet.cpp:419-524), each walking the cells on the fly
+// (ExecPointLocator::ExecuteOnNeighbor).  fp[n], force[n*3].
+EXPORT void ref_eam_original(int64_t n, const float* pos, const double* lo, const double* hi, double cut, int nrho,
+                             double drho, int nr, double dr, double rhomax, const float* frho, int64_t frho_rows,
+                             const float* rhor, int64_t rhor_rows, const float* z2r, int64_t z2r_rows, float* fp_out,
+                             float* force) {
+  Grid g = make_grid(lo, hi, cut, cut);
+  auto p = to_vec3(n, pos);
+  Cells c = build_cells(g, p);
+  ExecPointLocator loc = make_locator(g, c, p);
+  std::vector<vtkm::Id> zi((size_t)n, 0);
+  std::vector<Real> zr((size_t)n, 0.0f), one(1, 1.0f);
+  ExecTopology topo(ExecTopology::GroupIdPortalTypeId{}, portal(zi), portal(zi), portal(zr), portal(one), portal(one));
+  ExecForceFunction ff = make_force_function(g, cut, 0.0, 0, rhomax, nrho, drho, nr, dr);
+  auto tab = [](const float* t, int64_t rows) {
+    std::vector<Vec7f> v((size_t)rows);
+    for (int64_t r = 0; r < rows; ++r)
+      for (int k = 0; k < 7; ++k) v[r][k] = t[r * 7 + k];
+    return v;
+  };
+  const auto tf = tab(frho, frho_rows), tr = tab(rhor, rhor_rows), tz = tab(z2r, z2r_rows);
+  const auto tfp = portal(tf), trp = portal(tr), tzp = portal(tz);
+  const vtkm::Vec3f box = g.hi - g.lo;
+  RunWorklet::ComputeEAMrhoWorklet wr((Real)cut, box);
+  RunWorklet::ComputeEAMfpWorklet wfp;
+  RunWorklet::ComputeEAMforceWorklet wf((Real)cut, box);
+  std::vector<Real> rho((size_t)n), fp((size_t)n);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t i = 0; i < n; ++i) wr((vtkm::Id)i, trp, loc, topo, ff, rho[i]);
+  const auto rhop = portal(rho);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; ++i) wfp((vtkm::Id)i, rhop, tfp, loc, topo, ff, fp[i]);
+  const auto fpp = portal(fp);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t i = 0; i < n; ++i) {
+    vtkm::Vec3f f;
+    wf((vtkm::Id)i, fpp, trp, tzp, loc, topo, ff, f);
+    for (int d = 0; d < 3; ++d) force[3 * i + d] = f[d];
+  }
+  for (int64_t i = 0; i < n; ++i) fp_out[i] = fp[i];
+}

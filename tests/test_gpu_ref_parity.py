@@ -5,7 +5,8 @@ force functions compiled from the reference tree; see tests/test_oracle_ref_pin.
 * near forces (LJ + erfc Coulomb, LJ units, qqr2e = 1): within the FP32 bar (1e-5 of the rms force,
   max-norm) of ComputeNearForceVerletWorklet's float sums;
 * EAM with the reference's Verlet pair vector (compat.eam_verlet_pair_vector): within the FP32 bar
-  of ComputeEAMfpVerletWorklet / ComputeEAMForceVerletWorklet;
+  of ComputeEAMfpVerletWorklet / ComputeEAMForceVerletWorklet; neighbor.type ORIGINAL EAM within
+  the FP32 bar of the on-the-fly worklets (ComputeEAMrho/fp/forceWorklet);
 * RBE k-space with injected samples: the device error against the FP64 oracle is no larger than
   the reference's own FP32 k-space error (ComputePnumberChargeStructureFactorWorklet +
   ComputeNewRBEForceWorklet) and at most 1e-5;
@@ -75,6 +76,23 @@ def test_eam_vs_reference(cuda, ref, oracle_lib, tmp_path):
     rl = ref.neighbors(pr, s["lo"], s["hi"], 5.0)
     assert pair_sets_equal(c, ids, rl[0], rl[1]) == -1
     fr, _ = ref.eam(oracle_lib.eam_tables(pot), pr, s["lo"], s["hi"], 5.0, rl)
+    assert rel_err(f, fr.astype(np.float64)) <= 1e-5, rel_err(f, fr)
+
+
+@pytest.mark.parametrize("compat", [False, True])
+def test_eam_original_neighbor_type_vs_reference(cuda, ref, oracle_lib, tmp_path, compat):
+    """neighbor.type ORIGINAL with EAM (ExecutionMD::ComputeOriginalEAMForce): the reference's
+    on-the-fly worklets use p_i - p_j, so the result is the physical force with or without
+    compat.eam_verlet_pair_vector (that flag reproduces only the Verlet worklet's reversal)."""
+    pot = systems.write_johnson_funcfl(str(tmp_path / "johnson.eam"))
+    s = systems.eam_fcc(ncell=8, seed=7)
+    cfg = systems.eam_config(pot, precision="fp32")
+    cfg["hyper_parameters"]["neighbor"]["type"] = "ORIGINAL"
+    if compat:
+        cfg["compat"] = {"eam_verlet_pair_vector": True}
+    ff, _, _, f = _run(cfg, s, cuda)
+    ff.close()
+    fr, _ = ref.eam_original(oracle_lib.eam_tables(pot), s["pos"].astype(np.float32), s["lo"], s["hi"], 5.0)
     assert rel_err(f, fr.astype(np.float64)) <= 1e-5, rel_err(f, fr)
 
 

@@ -11,8 +11,9 @@ feed identical FP32 inputs to it and to the oracle's restatement (oracle/oracle.
   identical ids in identical traversal order, offsets matching the oracle's shift codes;
 * near forces (ComputeNearForceVerletWorklet, ComputeLJForceVerletWorklet, the RBL LJ worklet),
   structure-factor terms, the RBE normaliser S, the RBE force (ComputeNewRBEForceWorklet), EAM
-  F'(rho) and forces (ComputeEAMfpVerletWorklet / ComputeEAMForceVerletWorklet): bit for bit
-  (the oracle in its reference-order accumulation);
+  F'(rho) and forces (ComputeEAMfpVerletWorklet / ComputeEAMForceVerletWorklet, and the ORIGINAL
+  type's ComputeEAMrho/fp/forceWorklet): bit for bit (the oracle in its reference-order
+  accumulation);
 * the RBE sampler: the oracle's seeded sampler (which the device sampler reproduces exactly) and
   RBEPSAMPLE::Fetch_P_Sample run on the same uniforms give identical k-sets;
 * the RBL ERF table and the RBL erfc force: the oracle's reconstruction of the table equals the
@@ -163,6 +164,19 @@ def test_eam_passes(oracle_lib, ref, tmp_path):
     assert np.array_equal(f_o.astype(np.float32), f_r)
     f_p, _ = oracle_lib.eam_force(pot, pr, s["lo"], s["hi"], 5.0, nl, prec="fp32", sum_mode=0, ref_sign=False)
     assert np.array_equal(f_p.astype(np.float32), -f_r)
+
+
+def test_eam_original_neighbor_type(oracle_lib, ref, tmp_path):
+    """The ORIGINAL type's EAM (cells walked on the fly, ComputeEAMrho/fp/forceWorklet) equals the
+    oracle over the ORIGINAL pair set with the physical pair vector p_i - p_j, bit for bit."""
+    pot = systems.write_johnson_funcfl(str(tmp_path / "johnson.eam"))
+    s = systems.eam_fcc(ncell=6, seed=9)
+    pr = s["pos"].astype(np.float32)
+    nl = oracle_lib.neighbors(pr, s["lo"], s["hi"], 5.0, "fp32", original=True)
+    f_o, fp_o = oracle_lib.eam_force(pot, pr, s["lo"], s["hi"], 5.0, nl, prec="fp32", sum_mode=0, ref_sign=False)
+    f_r, fp_r = ref.eam_original(oracle_lib.eam_tables(pot), pr, s["lo"], s["hi"], 5.0)
+    assert np.array_equal(fp_o.astype(np.float32), fp_r)
+    assert np.array_equal(f_o.astype(np.float32), f_r)
 
 
 @pytest.mark.parametrize("L,alpha,P", [(107.72, None, 500), (66.88, 0.09, 200), (15.5, None, 64)])
