@@ -450,10 +450,10 @@ class ForceField:
 
     def phase_ms(self):
         import numpy as np
-        ms = np.zeros(8)
-        cnt = np.zeros(8, np.int64)
+        ms = np.zeros(len(self.PHASES))
+        cnt = np.zeros(len(self.PHASES), np.int64)
         _check(library().rbmd_force_phase_ms(self._h, _ptr(ms, ctypes.c_double),
-                                             _ptr(cnt, ctypes.c_int64), 8), "phase_ms")
+                                             _ptr(cnt, ctypes.c_int64), len(self.PHASES)), "phase_ms")
         return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(self.PHASES)}
 
     def list_builds(self):

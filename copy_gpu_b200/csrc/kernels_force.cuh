@@ -76,12 +76,12 @@ __device__ __forceinline__ float erfc_shared(float x, float e) {
 }
 __device__ __forceinline__ double erfc_shared(double x, double) { return erfc(x); }
 
-template <class R> __device__ __forceinline__ R lj24(const LJTable& t, int k);
-template <> __device__ __forceinline__ float lj24<float>(const LJTable& t, int k) { return t.lj24_f[k]; }
-template <> __device__ __forceinline__ double lj24<double>(const LJTable& t, int k) { return t.lj24_d[k]; }
-template <class R> __device__ __forceinline__ R sig6(const LJTable& t, int k);
-template <> __device__ __forceinline__ float sig6<float>(const LJTable& t, int k) { return t.sig6_f[k]; }
-template <> __device__ __forceinline__ double sig6<double>(const LJTable& t, int k) { return t.sig6_d[k]; }
+template <class R> __host__ __device__ __forceinline__ R lj24(const LJTable& t, int k);
+template <> __host__ __device__ __forceinline__ float lj24<float>(const LJTable& t, int k) { return t.lj24_f[k]; }
+template <> __host__ __device__ __forceinline__ double lj24<double>(const LJTable& t, int k) { return t.lj24_d[k]; }
+template <class R> __host__ __device__ __forceinline__ R sig6(const LJTable& t, int k);
+template <> __host__ __device__ __forceinline__ float sig6<float>(const LJTable& t, int k) { return t.sig6_f[k]; }
+template <> __host__ __device__ __forceinline__ double sig6<double>(const LJTable& t, int k) { return t.sig6_d[k]; }
 
 // RBE force terms of one atom over k records [0, P) of `kr` (shared or global memory).
 template <class R>
@@ -261,6 +261,123 @@ __global__ void __launch_bounds__(256) k_near_force(
     }
   }
   fx.add(gx); fy.add(gy); fz.add(gz);
+  const double F[3] = {fx.value(), fy.value(), fz.value()};
+  if (!isfinite(F[0]) || !isfinite(F[1]) || !isfinite(F[2])) set_flag(status, kFlagNonFinite);
+  const int id = slot_atom[i];
+  force[3 * id] = F[0];
+  force[3 * id + 1] = F[1];
+  force[3 * id + 2] = F[2];
+  if (ENERGY) {
+    energy_slot[2 * i] = 0.5 * (double)e_lj;
+    energy_slot[2 * i + 1] = 0.5 * (double)e_coul;
+  }
+}
+
+// Near force, one thread per atom, for the common case of one LJ coefficient pair for every type
+// pair and no molecules (the electrolyte benchmarks): the same pair set,
+// predicates and pair arithmetic as k_near_force, with less work per listed pair:
+//   * the LJ coefficients live in registers (no per-pair shared-memory lookups);
+//   * the list is walked four entries at a time, software-pipelined by whole chunks: the entries
+//     of chunk c + 2 and the neighbour positions of chunk c + 1 are in flight while chunk c is
+//     evaluated; the last chunk repeats the row's last entry and masks the repeats (a variant
+//     with rows padded by the atom's own slot instead held more registers and ran 15 % slower);
+//   * the LJ term is evaluated branch-free and selected by the pair predicate (the predicate of
+//     the list at rc under list reuse), so skin pairs cost no divergent branch;
+//   * the periodic image offsets are decoded only when some lane of the warp holds an image
+//     entry in the chunk (most warps hold none);
+//   * the four pair forces of a chunk are summed in R and folded into the two-float accumulator.
+// Pair physics as k_near_force: ComputeNearForceVerletWorklet / ComputeLJForceVerletWorklet
+// (rbmd/framework/run/worklet/RunWorklet.cpp:170-303), ExecForceFunction::ComputeLJForce and
+// ComputeNearEnergyForce (rbmd/framework/forceFunction/ExecForceFunction.h:74-140).
+template <class R, bool COUL, int MI, bool ENERGY>
+__global__ void __launch_bounds__(256) k_near_lean(
+    NearParams prm, R a24, R s6, const typename Traits<R>::V4* __restrict__ pos4, const int* __restrict__ nbr,
+    const int* __restrict__ count, const RepDev* __restrict__ reps, const int* __restrict__ rep_of_slot,
+    const int* __restrict__ slot_atom, double* __restrict__ force, double* __restrict__ energy_slot,
+    uint32_t* status) {
+  static_assert((MI & 3) != kMiLJ && (MI & kMiSpecial) == 0, "k_near_lean: no per-pair minimum image, no weights");
+  using V4 = typename Traits<R>::V4;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= prm.n) return;
+  const RepDev& rp = reps[rep_of_slot ? rep_of_slot[i] : 0];
+  const V4 pi = pos4[i];
+  const R rc = (R)prm.rc;
+  const R cut2 = rc * rc;
+  const R w0 = Traits<R>::wrap(rp, 0), w1 = Traits<R>::wrap(rp, 1), w2 = Traits<R>::wrap(rp, 2);
+  const R sa = (R)prm.sqrt_alpha, aa = (R)prm.alpha, c2 = (R)prm.two_sqrt_alpha_over_sqrt_pi;
+  const R cs = (R)prm.coul_scale;
+  const R qi = pi.w;
+  const int cnt = min(count[i], prm.cap);
+  Acc<R> fx, fy, fz;
+  R e_lj = 0, e_coul = 0;
+  // a chunk's entries; indices past the end repeat the last entry (valid memory), masked below
+  const unsigned ust = (unsigned)prm.stride;
+  auto load_chunk = [&](int p0, int (&e)[4]) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) e[k] = __ldg(nbr + i + (size_t)min(p0 + k, cnt - 1) * (size_t)ust);
+  };
+  int e_cur[4] = {0, 0, 0, 0}, e_nxt[4] = {0, 0, 0, 0};
+  V4 pj[4];
+  if (cnt > 0) {
+    load_chunk(0, e_cur);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) pj[k] = pos4[e_cur[k] >> kShiftBits];
+    if (cnt > 4) load_chunk(4, e_nxt);
+  }
+  for (int p = 0; p < cnt; p += 4) {
+    const unsigned act = __activemask();
+    const bool img = __any_sync(act, ((e_cur[0] | e_cur[1] | e_cur[2] | e_cur[3]) & 63) != 0);
+    R gx = 0, gy = 0, gz = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      R px = pj[k].x, py = pj[k].y, pz = pj[k].z;
+      if (img) {   // p_j - PeriodicCoordOffset
+        const int e = e_cur[k];
+        const int c0 = e & 3, c1 = (e >> 2) & 3, c2b = (e >> 4) & 3;
+        px = px - (c0 == 1 ? w0 : (c0 == 2 ? -w0 : (R)0));
+        py = py - (c1 == 1 ? w1 : (c1 == 2 ? -w1 : (R)0));
+        pz = pz - (c2b == 1 ? w2 : (c2b == 2 ? -w2 : (R)0));
+      }
+      const R r0 = px - pi.x, r1 = py - pi.y, r2 = pz - pi.z;
+      const R d2 = r0 * r0 + r1 * r1 + r2 * r2;
+      bool in = (p + k < cnt) && d2 > (R)1.0e-4;
+      if ((MI & 3) == kMiAll) in = in && (prm.orig ? cut2 - d2 > (R)0 : cut2 - d2 > (R)1.0e-4);
+      else in = in && d2 < cut2;
+      const R inv2 = rcp_r(d2);
+      const R sd6 = s6 * inv2 * inv2 * inv2;
+      const R scal = in ? a24 * (((R)2 * sd6 - (R)1) * sd6) * inv2 : (R)0;
+      // 4 eps (s6 - 1) s6 with 4 eps = -lj24/6
+      if (ENERGY && in) e_lj += -a24 / (R)6 * (sd6 - (R)1) * sd6;
+      R f = 0;
+      if (COUL) {
+        const R qq = qi * pj[k].w;
+        if (in && qq != (R)0) {
+          const R inv = rsqrt_r(d2);
+          const R dis = d2 * inv;
+          if (dis < rc && dis > (R)0.01) {
+            const R ex = exp_r(-aa * d2);
+            const R erfcv = erfc_shared(sa * dis, ex);
+            const R g = (erfcv * inv + c2 * ex) * inv;
+            f = -qq * g * inv * cs;
+            if (ENERGY) e_coul += qq * erfcv * inv * cs;
+          }
+        }
+      }
+      const R t = scal + f;
+      gx += t * r0;
+      gy += t * r1;
+      gz += t * r2;
+    }
+    fx.add(gx); fy.add(gy); fz.add(gz);
+    // advance the pipeline: positions of the next chunk, entries of the one after
+#pragma unroll
+    for (int k = 0; k < 4; ++k) e_cur[k] = e_nxt[k];
+    if (p + 4 < cnt) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) pj[k] = pos4[e_cur[k] >> kShiftBits];
+      if (p + 8 < cnt) load_chunk(p + 8, e_nxt);
+    }
+  }
   const double F[3] = {fx.value(), fy.value(), fz.value()};
   if (!isfinite(F[0]) || !isfinite(F[1]) || !isfinite(F[2])) set_flag(status, kFlagNonFinite);
   const int id = slot_atom[i];

@@ -122,6 +122,7 @@ struct rbmd_force {
   int rbl_list_warp = -1;               // RBL list build: 1 one warp per atom, 0 one thread per atom, -1 by size
   int rbl_lanes = 0;                    // RBL force pass lanes per atom (0: by size)
   int num_sms = 148;                    // SMs of the bound device (cudaDevAttrMultiProcessorCount)
+  int near_variant = 1;                 // 1: k_near_lean where it applies (lean_ok), 0: k_near_force
   int near_lanes = 1;                   // near pass lanes per atom: 1, or 4 / 8 / 16 / 32     // list build: 0 = staged kernel, else threads per block of
                                         // k_nlist; threads per block of the force pass
   bool autotune = false;                // "autotune": true tunes them at the first compute
@@ -343,6 +344,13 @@ SpecialDev special_dev(const rbmd_force* f) {
 int molecular_mode(const rbmd_force* f) {
   if (f->topo && f->special && f->is_cvff()) return 2;
   return f->at.molecule != nullptr ? 1 : 0;
+}
+
+// k_near_lean applies: one LJ coefficient pair for all types, no molecules, one thread per atom,
+// no per-pair minimum image (a Verlet skin, or boxes of >= 3 cells per axis).
+bool lean_ok(const rbmd_force* f) {
+  return f->near_variant >= 1 && !f->is_rbl() && !f->is_eam() && f->nt_eff == 1 && molecular_mode(f) == 0 &&
+         f->near_lanes == 1 && (f->skin > 0 || !f->minimg);
 }
 
 void free_topology(rbmd_force* f) {
@@ -911,6 +919,18 @@ void launch_near_t(rbmd_force* f, cudaStream_t s) {
     return;
   }
   const int bs = f->tpa_near;
+  if constexpr ((MI & 3) != kMiLJ && (MI & kMiSpecial) == 0) {
+    // one LJ coefficient pair for all types, no molecules: the lean pass
+    if (lean_ok(f)) {
+      auto kern = f->want_energy ? k_near_lean<R, COUL, MI, true> : k_near_lean<R, COUL, MI, false>;
+      kern<<<(f->n + bs - 1) / bs, bs, 0, s>>>(
+          p, lj24<R>(f->ljt_h, 0), sig6<R>(f->ljt_h, 0), (const typename Traits<R>::V4*)f->d_pos4, f->d_nbr,
+          f->d_count, f->d_reps, f->nrep > 1 ? f->d_rep_of : nullptr, f->d_slot_atom, f->at.force,
+          f->want_energy ? f->d_eslot : nullptr, f->d_status);
+      f->launches++;
+      return;
+    }
+  }
   k_near_force<R, COUL, MI><<<(f->n + bs - 1) / bs, bs, 0, s>>>(
       p, f->d_ljt, (const typename Traits<R>::V4*)f->d_pos4, f->d_meta, f->d_nbr, f->d_count,
       f->d_reps, f->nrep > 1 ? f->d_rep_of : nullptr, f->d_slot_atom, f->at.force,
@@ -1105,14 +1125,15 @@ void launch_force_tail(rbmd_force* f, cudaStream_t s, bool bin, bool regather) {
   if (kspace) {
     cudaEventRecord(f->ev_fork, s);
     launch_kspace<R>(f, f->side, f->ev_fork);
-    cudaEventRecord(f->ev_join, f->side);
   }
   launch_sort<R>(f, s, bin, regather);
   if (f->is_rbl()) {
+    if (kspace) cudaEventRecord(f->ev_join, f->side);
     launch_rbl_list<R>(f, s);
     PhaseScope ps(f, kPhForce, s);
     launch_rbl_force<R>(f, s);
   } else {
+    if (kspace) cudaEventRecord(f->ev_join, f->side);
     launch_nlist<R>(f, s);
     PhaseScope ps(f, kPhForce, s);
     if (f->is_eam()) launch_eam<R>(f, s);
@@ -1423,6 +1444,8 @@ rbmd_status parse_config(rbmd_force* f, const char* text) {
     const Value* tlv = root.path("tuning.list_block");
     if (ok(tl) || (tlv && (tl == 0 || tl == 1))) { f->tpa_list = tl; f->autotune = false; }
     if (ok(tn)) { f->tpa_near = tn; f->autotune = false; }
+    const Value* nv = root.path("tuning.near_variant");
+    if (nv) f->near_variant = (int)num(root, "tuning.near_variant", 1.0) == 0 ? 0 : 1;
     const int ln = (int)num(root, "tuning.force_lanes", 0.0);
     if (ln == 1 || ln == 4 || ln == 8 || ln == 16 || ln == 32) { f->near_lanes = ln; f->autotune = false; }
     const std::string rl = rbmdjson::text(root, "tuning.rbl_list", "auto");
@@ -1559,7 +1582,7 @@ rbmd_status parse_config(rbmd_force* f, const char* text) {
   };
   f->rbl_table = flag("compat.rbl_erf_table");
   f->rbl_shell_coul = !flag("compat.rbl_drop_shell_coulomb");
-  f->eam_ref_sign = flag("compat.eam_verlet_pair_vector") && f->nbr_type == "VERLETLIST";
+  f->eam_ref_sign = flag("compat.eam_verlet_pair_vector") && !f->orig_pred;
   if (flag("compat.special_bonds_integer"))
     for (double& w : f->special_w) w = std::trunc(w);
   if (f->P < 1 || f->P > 65536) return RBMD_ERR_CONFIG;
