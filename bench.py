@@ -39,7 +39,6 @@ sys.path.insert(0, ROOT)
 METRIC = "atom-steps/s at equal force RMSE vs FP64 Ewald: learned vs plain RBE"
 N_ATOMS = 1_000_000
 P_PLAIN = 500
-CPU_SAMPLE_ATOMS = 100_000
 
 
 def parse():
@@ -51,7 +50,9 @@ def parse():
     ap.add_argument("--atoms", type=int, default=N_ATOMS)
     ap.add_argument("--P", type=int, default=P_PLAIN)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=20,
+                    help="host-buffer force calls of the end-to-end leg, cycling through as many position "
+                         "frames recorded along the trajectory (list rebuilds at their natural rate)")
     ap.add_argument("--snapshots", type=int, default=200, help="training snapshots of the learned proposal")
     ap.add_argument("--train-iters", type=int, default=1500, help="Adam steps of the proposal network")
     ap.add_argument("--no-graph", action="store_true", help="launch every kernel of a step directly "
@@ -61,9 +62,14 @@ def parse():
     ap.add_argument("--ion-frac", type=float, default=0.1,
                     help="fraction of charged atoms of the electrolyte (0.1 is the headline workload)")
     ap.add_argument("--workload", default="electrolyte",
-                    choices=["electrolyte", "lj", "water", "eam", "batched", "molecular", "molecular_verlet"],
+                    choices=["electrolyte", "electrolyte_plain", "lj", "water", "eam", "batched", "molecular",
+                             "molecular_verlet"],
                     help="electrolyte: the headline metric (default); the others time the remaining "
-                         "configurations (plain MD steps, atom-steps/s) beside the CPU oracle")
+                         "configurations (plain MD steps, atom-steps/s) beside the CPU reference path; "
+                         "electrolyte_plain: the headline system (--atoms) with the plain Gaussian RBE sampler")
+    ap.add_argument("--tuning", default=None,
+                    help="JSON object of kernel variants (the configuration's \"tuning\" keys, e.g. "
+                         "'{\"list_block\": 256, \"force_block\": 64}') instead of the autotuner")
     ap.add_argument("--skin", type=float, default=0.3,
                     help="Verlet skin; the list is rebuilt when an atom moved more than skin/2 "
                          "(forces are those of a per-step rebuild); 0 rebuilds every step")
@@ -132,14 +138,23 @@ def measured_peaks():
 
 # Algorithmic bytes / sincos per unit of each phase: the bytes a launch must move per unit it
 # processes (each listed in the entry below).  "units" is the number of atoms (or charged atoms)
-# one launch processes.
-def algorithmic(n, nq, n_nbr_mean, P):
+# one launch processes.  `pair` is the force pass: "near" (LJ / LJ + erfc over a Verlet or RBL
+# list), "near_typed" (the same reading the (type, molecule) record of every atom once more),
+# "eam" (two passes over the list).
+def algorithmic(n, nq, n_nbr_mean, P, pair="near"):
+    force = {
+        # list entries (4 B/nbr), own pos4 (16 B), count + slot id (8 B), force (24 B); each
+        # neighbour position is some atom's own pos4, counted once
+        "near": 4 * n_nbr_mean + 16 + 8 + 24,
+        "near_typed": 4 * n_nbr_mean + 16 + 8 + 8 + 24,
+        # pass 1: entries + own pos4 + count + F'(rho) out; pass 2: entries + own pos4 + count +
+        # F'(rho) + force out (tables and neighbour F' are L2-resident)
+        "eam": (4 * n_nbr_mean + 16 + 4 + 4) + (4 * n_nbr_mean + 16 + 4 + 4 + 24),
+    }[pair]
     return {
         # list build: own pos4 (16 B) + cell ranges (8 B) + list entries written (4 B each) + count
         "neighbor_list": {"units": n, "bytes": 16 + 8 + 4 * n_nbr_mean + 4},
-        # near pass: list entries (4 B/nbr), own pos4 (16 B), count + slot id (8 B), force (24 B);
-        # each neighbour position is some atom's own pos4, counted once
-        "force": {"units": n, "bytes": 4 * n_nbr_mean + 16 + 8 + 24},
+        "force": {"units": n, "bytes": force},
         # structure factors over charged atoms: position (24 B) -> frac (16 B) written and read
         "kspace": {"units": nq, "bytes": 24 + 16 + 16, "sincos": P},
         # RBE force over charged atoms: frac (16 B) + far force (24 B)
@@ -149,10 +164,23 @@ def algorithmic(n, nq, n_nbr_mean, P):
     }
 
 
-# Per-atom DRAM traffic of the near-force pass measured by ncu on the 200,000-atom case
-# (dram__bytes_read.sum + dram__bytes_write.sum = 70.19 MB per launch); the full-size launch
-# has the same per-atom traffic (same density and neighbour count).
-NEAR_TRAFFIC_BYTES_PER_ATOM = 70.19e6 / 200_000
+# Per-atom DRAM traffic and warp instructions of the dominant pair kernel of each workload,
+# measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum, smsp__inst_executed.sum) on the
+# case named beside each entry; a full-size launch has the same per-atom work (same density and
+# neighbour count), so the figures scale by atoms.  Summaries under profiles/.
+PAIR_PROFILE = {
+    # profiles/k_near_lean_electrolyte_200k.md, profiles/pair_kernels_all_workloads.md
+    "electrolyte": {"kernel": "k_near_lean", "atoms": 200_000, "dram_bytes": 68.64e6, "warp_inst": 45.68e6},
+    "batched": {"kernel": "k_near_lean", "atoms": 2_164_302, "dram_bytes": 775.98e6, "warp_inst": 556.30e6},
+    "eam": {"kernel": "k_eam_fp + k_eam_force", "atoms": 256_000, "dram_bytes": 124.95e6, "warp_inst": 91.38e6},
+    "water": {"kernel": "k_near_force_group (16 lanes)", "atoms": 30_000, "dram_bytes": 70.59e6,
+              "warp_inst": 89.23e6},
+    "lj": {"kernel": "k_near_force_group (32 lanes, FP64)", "atoms": 4_000, "dram_bytes": 1.42e6,
+           "warp_inst": 2.09e6},
+    "molecular": {"kernel": "k_rbl_force (8 lanes)", "atoms": 97_600, "dram_bytes": 44.68e6, "warp_inst": 81.31e6},
+    "molecular_verlet": {"kernel": "k_near_force_group (16 lanes)", "atoms": 97_600, "dram_bytes": 175.68e6,
+                         "warp_inst": 233.34e6},
+}
 
 
 def max_over_ranks(value, dist, device):
@@ -168,6 +196,32 @@ def max_over_ranks(value, dist, device):
 def aggregate_rate(world, atoms_per_rank, steps, max_ms):
     """Whole-job atom-steps/s: every rank advanced its own replica for `steps` steps."""
     return world * atoms_per_rank * steps / (max_ms / 1e3)
+
+
+def partition_replicas(sizes, world):
+    """Independent replicas of uneven atom counts split over `world` ranks by atom count (longest
+    first, each to the rank holding the fewest atoms; ties to the lowest rank): per rank the
+    ascending list of its replica indices.  The batch has no exchange between replicas, so each
+    rank advances its share alone and the job needs no data-path collective."""
+    order = sorted(range(len(sizes)), key=lambda k: (-int(sizes[k]), k))
+    load = [0] * world
+    parts = [[] for _ in range(world)]
+    for k in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        parts[r].append(k)
+        load[r] += int(sizes[k])
+    return [sorted(p) for p in parts]
+
+
+def replica_subset(r, boxes, keep):
+    """The batch r (systems.replicas) restricted to the replicas in `keep`: system, boxes, offsets."""
+    off = r["offsets"]
+    idx = np.concatenate([np.arange(off[k], off[k + 1]) for k in keep])
+    sub = {key: r[key][idx] for key in ("pos", "vel", "mass", "charge", "type")}
+    sub.update(molecule=None, eps=r["eps"], sigma=r["sigma"], lo=r["lo"][keep], hi=r["hi"][keep])
+    sizes = np.diff(off)[keep]
+    sub["offsets"] = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    return sub, [boxes[k] for k in keep], sub["offsets"]
 
 
 def make_handle(s, dev, P, proposal, seed, skin, dt=None, ensemble="NVT", params=None, graph=True):
@@ -200,25 +254,27 @@ def kspace_noise(ff, steps, warm=3):
     mean squared error against the exact Ewald k-space force."""
     import torch
     ff.step(warm)
-    prev, acc, cnt = None, 0.0, 0
+    prev, acc, cnt, sq = None, 0.0, 0, 0.0
     for _ in range(steps):
         ff.step(1)
         torch.cuda.synchronize()
         f = ff.far_force()
+        sq += float((f ** 2).sum())
         if prev is not None:
             acc += float(((f - prev) ** 2).sum()) / 2.0
             cnt += 1
         prev = f
+    kspace_noise.mean_sq = sq / steps   # E |F_estimate|^2 summed over atoms = |F_exact|^2 + noise
     return acc / cnt
 
 
-def timed_run(ff, t, dev, steps, warmup, world, dist, e2e_steps):
+def timed_run(ff, t, dev, steps, warmup, world, dist, e2e_steps, autotune=True):
     """Warm-up, then `steps` timed MD steps (CUDA events, max over ranks), phases, clocks and the
     end-to-end host-buffer force call."""
     import torch
     local = dev.index or 0
     stream = torch.cuda.current_stream(dev)
-    blocks = ff.autotune()
+    blocks = ff.autotune() if autotune else ("fixed", "fixed")
     ff.Execute()
     ff.step(warmup)
     torch.cuda.synchronize(dev)
@@ -252,39 +308,55 @@ def timed_run(ff, t, dev, steps, warmup, world, dist, e2e_steps):
     cnt, _ = ff.neighbors(0)
     n_nbr = float(cnt.mean())
     # end-to-end through the host-buffer C-ABI call: pinned positions in, pinned forces out, in the
-    # reference's own Vec3f (float32) layout (rbmd_force_compute_host_f32) and in float64
-    e2e = {}
-    for dt in (torch.float32, torch.float64):
-        pos_h = torch.empty((n, 3), dtype=dt, pin_memory=True)
-        pos_h.copy_(t["pos"].cpu())
-        frc_h = torch.empty((n, 3), dtype=dt, pin_memory=True)
-        ph, fh = pos_h.numpy(), frc_h.numpy()
-        ff.compute_host(ph, fh, stream=stream.cuda_stream)
+    # reference's own Vec3f (float32) layout (rbmd_force_compute_host_f32) and in float64.  The
+    # positions cycle through e2e_steps frames recorded one MD step apart along the trajectory, so
+    # the Verlet-skin check rebuilds the list at its natural rate inside the timed calls.
+    nf = max(1, e2e_steps)
+    frames = []
+    for _ in range(nf):
+        ff.step(1)
         torch.cuda.synchronize(dev)
+        frames.append(t["pos"].cpu())
+    e2e, e2e_builds = {}, {}
+    for dt in (torch.float32, torch.float64):
+        pins = []
+        for fr in frames:
+            ph = torch.empty((n, 3), dtype=dt, pin_memory=True)
+            ph.copy_(fr)
+            pins.append(ph.numpy())
+        frc_h = torch.empty((n, 3), dtype=dt, pin_memory=True)
+        fh = frc_h.numpy()
+        ff.compute_host(pins[-1], fh, stream=stream.cuda_stream)
+        torch.cuda.synchronize(dev)
+        b0 = ff.list_builds()
         w0 = time.perf_counter()
         a0 = torch.cuda.Event(enable_timing=True)
         a1 = torch.cuda.Event(enable_timing=True)
         a0.record(stream)
-        for _ in range(e2e_steps):
-            ff.compute_host(ph, fh, stream=stream.cuda_stream)
+        for k in range(nf):
+            ff.compute_host(pins[k], fh, stream=stream.cuda_stream)
         a1.record(stream)
         torch.cuda.synchronize(dev)
-        ms_e = max(a0.elapsed_time(a1), (time.perf_counter() - w0) * 1e3) / e2e_steps
+        ms_e = max(a0.elapsed_time(a1), (time.perf_counter() - w0) * 1e3) / nf
         if world > 1:
             ms_e = max_over_ranks(ms_e, dist, dev)
         e2e[dt] = ms_e
+        e2e_builds[dt] = (ff.list_builds() - b0) / nf
     return dict(ms=ms, builds=builds, phases=phases, flags=flags, clk=clk, n_nbr=n_nbr, e2e_ms=e2e[torch.float32],
-                e2e64_ms=e2e[torch.float64], k_per_step=k_per_step, blocks=blocks)
+                e2e64_ms=e2e[torch.float64], e2e_builds=e2e_builds[torch.float32], e2e_frames=nf,
+                k_per_step=k_per_step, blocks=blocks)
 
 
-def roofline(run, n, nq, P, steps, dev):
+def roofline(run, n, nq, P, steps, dev, pair="near", profile=None, kernel=None, nrep=1):
     """Per-phase achieved GB/s and sin/cos rates from the CUDA-event phase times, and the roofline
     object of the dominant kernel.  The k-space phases run on a second stream concurrently with
     the list build and near pass, so their event intervals include time shared with those
-    kernels; the dominant kernel is taken among the caller-stream force kernels."""
+    kernels; the dominant kernel is taken among the caller-stream force kernels.  With a profile
+    (PAIR_PROFILE) the pair kernel's DRAM traffic and its fraction of the instruction-issue
+    ceiling (warp instructions / (SMs x 4 schedulers x SM clock x time)) are added."""
     import torch
     peaks, src = measured_peaks()
-    alg = algorithmic(n, nq, run["n_nbr"], P)
+    alg = algorithmic(n, nq, run["n_nbr"], P, pair)
     phases = run["phases"]
     launches = {k: phases[k][1] for k in phases}
     sm_mhz = run["clk"]["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0)
@@ -298,8 +370,10 @@ def roofline(run, n, nq, P, steps, dev):
         per_launch_s = tot_ms / 1e3 / launches[k]
         if k == "integrate":
             per_launch_s = tot_ms / 1e3 / steps
-        if k == "neighbor_list":      # early-exit launches on list-reuse steps are ~3 us
-            per_launch_s = tot_ms / 1e3 / max(run["builds"], 1)
+        if k == "neighbor_list" and run["builds"] > 0:
+            # with a Verlet skin: time per full build (replica builds / replicas); the launches of
+            # list-reuse steps exit early (a few us each)
+            per_launch_s = tot_ms / 1e3 / max(run["builds"] / nrep, 1e-9)
         ent = {"ms_per_step": tot_ms / steps, "launches": launches[k], "ms_per_launch": per_launch_s * 1e3}
         ent["hbm_gbs"] = a["bytes"] * a["units"] / per_launch_s / 1e9
         ent["hbm_frac"] = ent["hbm_gbs"] / peaks["hbm_gbs"]
@@ -312,17 +386,24 @@ def roofline(run, n, nq, P, steps, dev):
     dom = max(single, key=lambda k: rl[k]["ms_per_step"])
     d = rl[dom]
     roof = {"bound": "hbm", "achieved": d["hbm_gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
-            "frac": d["hbm_frac"], "kernel": "k_near_force" if dom == "force" else "k_nlist",
+            "frac": d["hbm_frac"], "kernel": (kernel or "near/EAM pass") if dom == "force" else
+            f"neighbour-list build ({'per build' if run['builds'] > 0 else 'every step'})",
             "peak_source": f"{src} hbm_gbs (MEASURED_PEAKS.json)", "traffic": None,
-            "algorithmic_bytes_per_launch": alg[dom]["bytes"] * alg[dom]["units"]}
-    if dom == "force":
-        roof["traffic"] = NEAR_TRAFFIC_BYTES_PER_ATOM * n
-        roof["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the 200,000-atom "
-                                  "launch (summary committed under profiles/) scaled by atoms")
-        # what limits the kernel instead of HBM (same ncu capture): instruction issue
-        roof["limiter"] = {"what": "instruction issue and dependent-latency waits in the pair arithmetic",
-                           "smsp__issue_active_pct": 66.7, "sm__throughput_pct": 57.1,
-                           "gpu__dram_throughput_pct": 8.6}
+            "algorithmic_bytes_per_launch": alg[dom]["bytes"] * alg[dom]["units"],
+            "ms_per_launch": d["ms_per_launch"]}
+    if dom == "force" and profile is not None:
+        scale = n / profile["atoms"]
+        roof["kernel"] = profile["kernel"]
+        roof["traffic"] = profile["dram_bytes"] * scale
+        roof["traffic_source"] = (f"ncu dram__bytes_read.sum + dram__bytes_write.sum of the {profile['atoms']}-atom "
+                                  "launch (summary under profiles/) scaled by atoms")
+        inst = profile["warp_inst"] * scale
+        ceiling_s = inst / (n_sm * 4 * sm_mhz * 1e6)
+        roof["issue"] = {"warp_instructions_per_launch": inst, "issue_ceiling_ms": ceiling_s * 1e3,
+                         "issue_frac": ceiling_s / (d["ms_per_launch"] / 1e3),
+                         "what": "the pair kernel is bound by instruction issue and dependent latency, not "
+                                 "HBM: its fraction of the issue ceiling (SMs x 4 schedulers x clock) beside "
+                                 "the HBM fraction"}
     return roof, rl, mufu_peak
 
 
@@ -363,6 +444,9 @@ def run_ours(args):
     ffn, tn, _ = make_handle(s, dev, P0, "gauss", 13 + rank, 0.0, dt=0.0, ensemble="NVE")
     ffn.Execute()
     mse_plain = kspace_noise(ffn, args.noise_steps) / nq
+    # RMS of the exact k-space force per charged atom: E|F_est|^2 = |F_exact|^2 + MSE (unbiased
+    # estimator), so the scale against which the RMSE reads as a relative error
+    exact_rms = float(np.sqrt(max(kspace_noise.mean_sq / nq - mse_plain, 0.0)))
     ffn.close()
     ffn, tn, _ = make_handle(s, dev, P0, "learned", 17 + rank, 0.0, dt=0.0, ensemble="NVE", params=params)
     ffn.Execute()
@@ -387,7 +471,7 @@ def run_ours(args):
     v_learned = aggregate_rate(world, n, args.steps, learned["ms"])
     out = None
     if rank == 0:
-        roof, rl, _ = roofline(learned, n, nq, P_eq, args.steps, dev)
+        roof, rl, _ = roofline(learned, n, nq, P_eq, args.steps, dev, profile=PAIR_PROFILE["electrolyte"])
         out = {
             "metric": METRIC,
             "value": v_learned,
@@ -428,6 +512,13 @@ def run_ours(args):
                             "the exact Ewald k-space force): half the mean squared difference of two "
                             f"independent k-sets at fixed positions, {args.noise_steps - 1} pairs",
             },
+            # the north-star comparison, flat: learned vs plain RBE at equal k-space force RMSE
+            "speedup_at_equal_rmse": v_learned / v_plain,
+            "plain_value": v_plain,
+            "variance_ratio_at_P_plain": ratio,
+            "kspace_force_rmse": float(np.sqrt(mse_plain)),
+            "kspace_force_rms_exact": exact_rms,
+            "kspace_force_rel_rmse": float(np.sqrt(mse_plain)) / exact_rms if exact_rms > 0 else None,
             "roofline": roof,
             "phases": rl,
             "phase_ms_per_step": {k: {"learned": learned["phases"][k][0] / args.steps,
@@ -436,7 +527,10 @@ def run_ours(args):
             "e2e": {"value": world * n / (learned["e2e_ms"] / 1e3), "unit": "atom-steps/s",
                     "h2d_bytes_per_step": 12 * n, "d2h_bytes_per_step": 12 * n,
                     "what": "rbmd_force_compute_host_f32: pinned host positions in, forces out, in the reference's "
-                            "Vec3f (float32) layout, one force evaluation per step",
+                            f"Vec3f (float32) layout, one force evaluation per step, positions cycling through "
+                            f"{learned['e2e_frames']} frames recorded one MD step apart (list rebuilds at their "
+                            f"natural rate: {learned['e2e_builds']:.2f} per call)",
+                    "list_builds_per_call": learned["e2e_builds"],
                     "fp64_host_buffers": {"value": world * n / (learned["e2e64_ms"] / 1e3),
                                           "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n,
                                           "what": "rbmd_force_compute_host (float64 host arrays)"}},
@@ -454,42 +548,78 @@ def run_ours(args):
     return out
 
 
-def cpu_force_eval(n_atoms, P, seed=3, sysd=None):
-    """One force evaluation of the reference path's CPU restatement (FP32 semantics):
-    neighbour list, LJ + erfc near force, RBE structure factors and force.  Returns seconds."""
-    import oracle
+def _electrolyte_sample(n_atoms, seed=3):
     from copy_gpu_b200 import systems
-    s = sysd if sysd is not None else systems.electrolyte(n_atoms, seed=seed)
+    return systems.electrolyte(n_atoms, seed=seed)
+
+
+def cpu_force_eval(n_atoms, P, seed=3, sysd=None, use_ref=None):
+    """One force evaluation of the reference path on the host cores: neighbour list, LJ + erfc
+    near force, RBE k-sampling, structure factors and force.  With the reference's own code
+    compiled here (oracle/_ref, use_ref) its worklets run (ComputeNeighboursWorklet,
+    ComputeNearForceVerletWorklet, RBEPSAMPLE::Fetch_P_Sample, ComputePnumberChargeStructureFactor-
+    Worklet over all N x P terms, ComputeNewRBEForceWorklet); otherwise the oracle restatement in
+    FP32.  Returns seconds."""
+    import oracle
+    from oracle import ref
+    from copy_gpu_b200 import systems
+    s = sysd if sysd is not None else _electrolyte_sample(n_atoms, seed)
     cfg = systems.electrolyte_config(P=P)
     alpha = cfg["hyper_parameters"]["coulomb"]["alpha"]
     L = s["hi"] - s["lo"]
-    m = oracle.rbe_sample(alpha, L, 7, 0, 0, P)
     pos32 = s["pos"].astype(np.float32)
+    use_ref = ref.available() if use_ref is None else use_ref
     t0 = time.perf_counter()
-    nl = oracle.neighbors(pos32, s["lo"], s["hi"], 2.5, "fp32")
-    oracle.near_force(pos32, s["lo"], s["hi"], 2.5, nl, type=s["type"], charge=s["charge"], eps=s["eps"],
-                      sigma=s["sigma"], with_coul=True, alpha=alpha, sum_mode=0, prec="fp32")
-    rho = oracle.rhok(pos32, s["charge"], L, m, prec="fp32")
-    oracle.rbe_force(pos32, s["charge"], L, alpha, 1.0, m, rho, prec="fp32")
+    if use_ref:
+        nl = ref.neighbors(pos32, s["lo"], s["hi"], 2.5, cap=128)
+        ref.near_force(pos32, s["lo"], s["hi"], 2.5, nl, type=s["type"], charge=s["charge"], eps=s["eps"],
+                       sigma=s["sigma"], alpha=alpha, with_coul=True)
+        m, _ = ref.rbe_sample(alpha, L, P, np.random.default_rng(seed).random(64 * P))
+        rho = ref.rhok(pos32, s["charge"], L, m)
+        ref.rbe_force(pos32, s["charge"], s["lo"], s["hi"], alpha, m, rho)
+    else:
+        m = oracle.rbe_sample(alpha, L, 7, 0, 0, P)
+        nl = oracle.neighbors(pos32, s["lo"], s["hi"], 2.5, "fp32")
+        oracle.near_force(pos32, s["lo"], s["hi"], 2.5, nl, type=s["type"], charge=s["charge"], eps=s["eps"],
+                          sigma=s["sigma"], with_coul=True, alpha=alpha, sum_mode=0, prec="fp32")
+        rho = oracle.rhok(pos32, s["charge"], L, m, prec="fp32")
+        oracle.rbe_force(pos32, s["charge"], L, alpha, 1.0, m, rho, prec="fp32")
     return time.perf_counter() - t0
 
 
+def _cpu_kind():
+    from oracle import ref
+    return ("reference", "the reference's own force-path worklets compiled from its source (oracle/_ref)") \
+        if ref.available() else ("port", "the oracle's FP32 restatement of the reference path")
+
+
+def _sample_size(P, evals, budget_s, cap_atoms=N_ATOMS):
+    """Atoms per evaluation so that `evals` evaluations take about budget_s seconds (the reference
+    materialises N x P structure-factor terms, 8 bytes each: at most 2 GB of them)."""
+    t = cpu_force_eval(100_000, P, sysd=_electrolyte_sample(100_000))
+    n = int(100_000 * budget_s / max(evals, 1) / max(t, 1e-3))
+    n = min(n, cap_atoms, int(2e9 / (8 * P)))
+    return max(20_000, (n // 10_000) * 10_000)
+
+
 def cpu_baseline(P, n_atoms=N_ATOMS, min_seconds=10.0, max_evals=10):
-    """The oracle on the host cores: force evaluations (list + near + RBE) of the full workload
-    repeated until about min_seconds of CPU work (at most max_evals)."""
+    """The reference path on the host cores (its own code where it compiled here): force
+    evaluations of a sample of the workload repeated until about min_seconds of CPU work."""
     import oracle
-    from copy_gpu_b200 import systems
     oracle.build()
     cores = os.cpu_count() or 1
     oracle.set_threads(cores)
-    sysd = systems.electrolyte(n_atoms, seed=3)
+    kind, what = _cpu_kind()
+    n = _sample_size(P, 5, min_seconds, n_atoms)
+    sysd = _electrolyte_sample(n)
     tot, evals = 0.0, 0
     while evals < max_evals and (evals == 0 or tot < min_seconds):
-        tot += cpu_force_eval(n_atoms, P, sysd=sysd)
+        tot += cpu_force_eval(n, P, sysd=sysd)
         evals += 1
-    return {"value": n_atoms * evals / tot, "unit": "atom-steps/s", "cores": cores, "kind": "port",
-            "sample": f"{evals} force evaluations (list + LJ/erfc near + RBE P={P}) of the {n_atoms}-atom "
-                      f"electrolyte, FP32 oracle, {cores} OpenMP threads, {tot:.1f} s"}
+    return {"value": n * evals / tot, "unit": "atom-steps/s", "cores": cores, "kind": kind,
+            "sample": f"{evals} force evaluations (neighbour list, LJ/erfc near force, RBE sampling, structure "
+                      f"factors and force, P={P}) of a {n}-atom sample of the {n_atoms}-atom electrolyte (same "
+                      f"composition and density): {what}, {cores} OpenMP threads, {tot:.1f} s"}
 
 
 def run_reference(args):
@@ -501,12 +631,16 @@ def run_reference(args):
     oracle.build()
     cores = os.cpu_count() or 1
     oracle.set_threads(cores)
-    n = CPU_SAMPLE_ATOMS
-    for _ in range(max(args.warmup, 0) and 1):
-        cpu_force_eval(n, args.P)
-    times = [cpu_force_eval(n, args.P, seed=3) for _ in range(args.steps)]
+    kind, what = _cpu_kind()
+    n = _sample_size(args.P, args.steps + 1, 45.0, args.atoms)
+    sysd = _electrolyte_sample(n)
+    cpu_force_eval(n, args.P, sysd=sysd)
+    times = [cpu_force_eval(n, args.P, sysd=sysd, seed=3 + k) for k in range(args.steps)]
     tot = sum(times)
     value = n * args.steps / tot
+    sample = (f"per step one force evaluation (neighbour list, LJ/erfc near force, RBE k-sampling, structure "
+              f"factors and force, P={args.P}) of a {n}-atom sample of the {args.atoms}-atom electrolyte (same "
+              f"composition and density), no integration: {what}, {cores} OpenMP threads")
     return {
         "impl": "reference",
         "metric": METRIC,
@@ -521,20 +655,24 @@ def run_reference(args):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": f"electrolyte {args.atoms} atoms, plain Gaussian RBE P={args.P}, full MD step",
+        "config": {"workload": f"electrolyte force evaluation (neighbour list + LJ/erfc near + RBE P={args.P}) "
+                               f"on a {n}-atom sample of the {args.atoms}-atom workload, plain Gaussian RBE",
                    "sample_atoms": n, "P": args.P},
-        "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": cores, "kind": "port",
-                         "sample": f"per step one force evaluation of a {n}-atom sample of the workload "
-                                   f"(same composition and density), FP32 oracle restatement of the "
-                                   f"reference path, {cores} OpenMP threads"},
+        "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
 
 # ---- the other configurations: plain MD steps, GPU vs the CPU oracle -------------------------
-def config_system(name, tmpdir):
+def config_system(name, tmpdir, atoms=N_ATOMS):
     """(system, config, boxes, offsets, description) of a secondary configuration."""
     from copy_gpu_b200 import Box, systems
+    if name == "electrolyte_plain":
+        s = systems.electrolyte(atoms, seed=3)
+        cfg = systems.electrolyte_config(P=P_PLAIN, precision="fp32", seed=7, ensemble="NVT")
+        cfg["hyper_parameters"]["neighbor"]["skin"] = 0.3
+        return s, cfg, None, None, (f"electrolyte {atoms} atoms, plain Gaussian RBE P={P_PLAIN} (the reference's "
+                                    "sampler), rc 2.5 + skin 0.3, FP32 forces, full MD step")
     if name == "lj":
         s = systems.lj_fcc(ncell=10, seed=1)
         cfg = systems.lj_config(cutoff=2.5, skin=0.3, precision="fp64", ensemble="NVE")
@@ -630,6 +768,28 @@ def cpu_config_eval(name, s, cfg, offsets, tmpdir):
                           s["bond_coeffs"], s["angles"], s["angle_type"], s["angle_coeffs"], s["dihedrals"],
                           s["dihedral_type"], s["dihedral_coeffs"], special=sp)
         return time.perf_counter() - t0, len(pos)
+    from oracle import ref
+    if ref.available() and name in ("lj", "eam", "water", "electrolyte_plain", "electrolyte_sub"):
+        # the reference's own worklets (FP32 -- its Real), compiled from its source
+        p32 = s["pos"].astype(np.float32)
+        t0 = time.perf_counter()
+        nl = ref.neighbors(p32, s["lo"], s["hi"], rc)
+        if name == "eam":
+            ref.eam(oracle.eam_tables(hp["force_field"]["potential_file"]), p32, s["lo"], s["hi"], rc, nl)
+            return time.perf_counter() - t0, len(pos)
+        coul = "coulomb" in hp and name != "lj"
+        alpha = hp["coulomb"]["alpha"] if coul else 0.0
+        ref.near_force(p32, s["lo"], s["hi"], rc, nl, type=s["type"], mol=s.get("molecule"),
+                       charge=s["charge"] if coul else None, eps=s["eps"], sigma=s["sigma"], alpha=alpha,
+                       with_coul=coul)
+        if coul:
+            P = hp["coulomb"]["coulomb_sample_num"]
+            m, _ = ref.rbe_sample(alpha, L, P, np.random.default_rng(7).random(64 * P))
+            rho = ref.rhok(p32, s["charge"], L, m)
+            ref.rbe_force(p32, s["charge"], s["lo"], s["hi"], alpha, m, rho)
+        if "hoh" in s:
+            oracle.water_extras(s["hoh"], s["pos"], s["charge"], s["lo"], s["hi"], *s["bond"], *s["angle"])
+        return time.perf_counter() - t0, len(pos)
     t0 = time.perf_counter()
     nl = oracle.neighbors(pos, s["lo"], s["hi"], rc, prec)
     if name == "eam":
@@ -656,10 +816,29 @@ def run_config(args):
     and on all cores."""
     import tempfile
     import torch
-    dev = torch.device("cuda", 0)
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     with tempfile.TemporaryDirectory() as tmpdir:
-        s, cfg, boxes, offs, desc = config_system(args.workload, tmpdir)
+        s, cfg, boxes, offs, desc = config_system(args.workload, tmpdir, args.atoms)
+        parallel = "single"
+        if world > 1 and args.workload == "batched":
+            # the 512 replicas split over the ranks by atom count; no exchange between them
+            parts = partition_replicas(np.diff(offs), world)
+            s, boxes, offs = replica_subset(s, boxes, parts[rank])
+            parallel = f"replicas partitioned over {world} ranks by atom count"
+        elif world > 1:
+            parallel = f"one independent copy per rank ({world} ranks)"
+        if args.tuning:
+            cfg["tuning"] = json.loads(args.tuning)
+        if args.no_graph:
+            cfg.setdefault("execution", {})["cuda_graph"] = False
         from copy_gpu_b200 import Box, ForceField
         n_all = s["pos"].shape[0]
         t = {k: torch.tensor(s[k], device=dev, dtype=torch.float64).contiguous()
@@ -679,31 +858,53 @@ def run_config(args):
                             s["dihedral_coeffs"])
         ff.Init(t["pos"], t["force"], vel=t["vel"], mass=t["mass"], charge=t["charge"], type=t["type"],
                 molecule=t.get("molecule"), image=t["image"], replica_offsets=offs)
-        run = timed_run(ff, t, dev, args.steps, args.warmup, 1, None, args.e2e_steps)
+        run = timed_run(ff, t, dev, args.steps, args.warmup, world, dist if world > 1 else None, args.e2e_steps,
+                        autotune=not args.tuning)
         n = ff.n
-        value = n * args.steps / (run["ms"] / 1e3)
+        n_job = n
+        if world > 1:
+            cnt = torch.tensor([float(n)], device=dev, dtype=torch.float64)
+            dist.all_reduce(cnt)
+            n_job = int(cnt.item())
+        value = n_job * args.steps / (run["ms"] / 1e3)
         line = {
-            "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": 1, "steps": args.steps,
+            "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": run["ms"] / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if cfg.get("precision") == "fp64" else "f32",
             "data": "synthetic",
-            "config": {"workload": desc, "atoms": n,
+            "config": {"workload": desc, "atoms": n_job, "atoms_rank0": n, "parallelism": parallel,
                        "list_builds_per_step": run["builds"] / args.steps / (len(boxes) if boxes else 1),
                        "threads_per_block": {"list": run["blocks"][0], "force": run["blocks"][1]},
                        "step_launch": "cuda graph replay (one launch per step)"},
-            "e2e": {"value": n / (run["e2e_ms"] / 1e3), "unit": "atom-steps/s", "h2d_bytes_per_step": 12 * n,
+            "e2e": {"value": n_job / (run["e2e_ms"] / 1e3), "unit": "atom-steps/s", "h2d_bytes_per_step": 12 * n,
                     "d2h_bytes_per_step": 12 * n,
                     "what": "rbmd_force_compute_host_f32: pinned host positions in, forces out (the reference's "
-                            "Vec3f layout), one force evaluation",
-                    "fp64_host_buffers": {"value": n / (run["e2e64_ms"] / 1e3), "h2d_bytes_per_step": 24 * n,
+                            f"Vec3f layout), one force evaluation per call, positions cycling through "
+                            f"{run['e2e_frames']} frames recorded one MD step apart",
+                    "list_builds_per_call": run["e2e_builds"],
+                    "fp64_host_buffers": {"value": n_job / (run["e2e64_ms"] / 1e3), "h2d_bytes_per_step": 24 * n,
                                           "d2h_bytes_per_step": 24 * n}},
             "phase_ms_per_step": {k: v[0] / args.steps for k, v in run["phases"].items() if v[1]},
             "gpu_launches": run["k_per_step"] * args.steps, "kernels_per_step": run["k_per_step"],
             "status_flags": run["flags"], "clocks": run["clk"], "mean_neighbors": run["n_nbr"],
         }
+        hp = cfg["hyper_parameters"]
+        pair = {"eam": "eam", "water": "near_typed", "molecular": "near_typed",
+                "molecular_verlet": "near_typed"}.get(args.workload, "near")
+        prof = PAIR_PROFILE.get("electrolyte" if args.workload == "electrolyte_plain" else args.workload)
+        nq = int((np.asarray(s["charge"]) != 0).sum())
+        P = int(hp.get("coulomb", {}).get("coulomb_sample_num", 0)) if "coulomb" in hp else 0
+        roof, rl, _ = roofline(run, n, nq, max(P, 1), args.steps, dev, pair=pair, profile=prof,
+                               nrep=len(boxes) if boxes else 1)
+        line["roofline"] = roof
+        line["phases"] = rl
         del ff
         torch.cuda.synchronize(dev)
-        if not args.no_cpu:
+        if world > 1:
+            dist.destroy_process_group()
+            if rank != 0:
+                return None
+        if not args.no_cpu and world == 1:
             import oracle
             oracle.build()
             cores = os.cpu_count() or 1
@@ -712,11 +913,16 @@ def run_config(args):
                 oracle.set_threads(th)
                 sec, atoms = cpu_config_eval(args.workload, s, cfg, offs, tmpdir)
                 res[th] = atoms / sec
-            line["cpu_baseline"] = {"value": res[cores], "unit": "atom-steps/s", "cores": cores, "kind": "port",
+            from oracle import ref
+            on_ref = ref.available() and args.workload in ("lj", "eam", "water", "electrolyte_plain", "batched")
+            line["cpu_baseline"] = {"value": res[cores], "unit": "atom-steps/s", "cores": cores,
+                                    "kind": "reference" if on_ref else "port",
                                     "single_thread": res[1],
                                     "sample": "one force evaluation (list + pair terms (+ RBE, water extras, "
-                                              "CVFF terms)) "
-                                              "of the same system by the FP32/FP64 oracle restatement"
+                                              "CVFF terms)) of the same system by "
+                                              + ("the reference's own worklets compiled from its source (FP32; "
+                                                 "the water's intramolecular terms by the oracle)" if on_ref else
+                                                 "the FP32/FP64 oracle restatement")
                                               + (", first 16 replicas" if args.workload == "batched" else "")}
     return line
 
@@ -724,7 +930,9 @@ def run_config(args):
 def main():
     args = parse()
     if args.impl != "reference" and args.workload != "electrolyte":
-        print(json.dumps(run_config(args)), flush=True)
+        line = run_config(args)
+        if line is not None:
+            print(json.dumps(line), flush=True)
         return
     out = run_reference(args) if args.impl == "reference" else run_ours(args)
     if out is not None:

@@ -708,12 +708,16 @@ __global__ void k_rho_finish(int nk_total, int ktile, const int* __restrict__ kr
 // on the host (FP64); u <= min(1, ratio) is evaluated as u * G(m) <= G(m').
 // One block per replica: phase 1 draws the Gaussian proposals, their G values and the
 // acceptance uniforms of the first D steps in parallel (they do not depend on the chain);
-// phase 2 (one thread) walks the three per-axis chains in lockstep (the all-zero retry couples
-// the axes) carrying G(m) in registers, so a step has no dependent memory access.  Steps past
-// D draw inline.
+// phase 2 resolves every per-axis chain state of those D steps in parallel (a step with
+// u gmax <= G(m) accepts whatever the state, and the states between two such steps are replayed
+// exactly), then assigns sample indices to the states that are not all zero (the all-zero retry
+// of the reference couples the axes only there) with a block scan.  Steps past D, and windows
+// holding a proposal beyond the tables, run the chain sequentially on one thread as the
+// reference does.  Same k-sets as the sequential chain, bit for bit.
 // ------------------------------------------------------------------------------------------
 struct SamplerRep {
   double sigma[3];
+  double gmax[3];   // largest finite G of each axis' table
   int qmax;
   int g_offset;     // offset of this replica's G tables (3 * (qmax+1) doubles)
 };
@@ -764,7 +768,6 @@ __global__ void __launch_bounds__(256) k_sample(int nrep, const SamplerRep* __re
     gw[axis][d] = sampler_g(g, s.qmax, axis, m);
   }
   __syncthreads();
-  if (threadIdx.x != 0) return;
   auto prop = [&](int axis, long long d, double* u, double* gm) -> int {
     if (d < D) { *u = ua[axis][d]; *gm = gw[axis][d]; return mw[axis][d]; }
     const double gs = sampler_draw(k0, k1, step, r, axis, d, u);
@@ -772,16 +775,6 @@ __global__ void __launch_bounds__(256) k_sample(int nrep, const SamplerRep* __re
     *gm = sampler_g(g, s.qmax, axis, m);
     return m;
   };
-  long long draw = 0;
-  int X0[3];
-  double G0[3];
-  for (int guard = 0;; ++guard) {
-    double u;
-    for (int a = 0; a < 3; ++a) X0[a] = prop(a, draw, &u, &G0[a]);
-    ++draw;
-    if (!(X0[0] == 0 && X0[1] == 0 && X0[2] == 0)) break;
-    if (guard > 100000) { set_flag(status, kFlagSampler); X0[0] = 1; G0[0] = sampler_g(g, s.qmax, 0, 1); break; }
-  }
   auto emit = [&](int i, const int* X) {
     int* o = kvec_out + 3 * (kb + i);
     o[0] = X[0]; o[1] = X[1]; o[2] = X[2];
@@ -789,10 +782,120 @@ __global__ void __launch_bounds__(256) k_sample(int nrep, const SamplerRep* __re
     rec[0] = X[0]; rec[1] = X[1]; rec[2] = X[2];
     krep[kb + i] = r;
   };
-  emit(0, X0);
-  int i = 1;
-  long long guard = 0;
-  while (i < P) {
+  // first sample: the first draw that is not all zero (the reference's Fetch_P_Sample do-while)
+  __shared__ int s_d0, s_x0[3], s_seq, s_total;
+  __shared__ double s_g0[3];
+  if (threadIdx.x == 0) {
+    long long draw = 0;
+    int X0[3];
+    double G0[3];
+    for (int guard = 0;; ++guard) {
+      double u;
+      for (int a = 0; a < 3; ++a) X0[a] = prop(a, draw, &u, &G0[a]);
+      ++draw;
+      if (!(X0[0] == 0 && X0[1] == 0 && X0[2] == 0)) break;
+      if (guard > 100000) { set_flag(status, kFlagSampler); X0[0] = 1; G0[0] = sampler_g(g, s.qmax, 0, 1); break; }
+    }
+    emit(0, X0);
+    s_d0 = (int)min(draw, (long long)D);
+    for (int a = 0; a < 3; ++a) { s_x0[a] = X0[a]; s_g0[a] = G0[a]; }
+    // the parallel chain below needs a non-empty window and every state in it with a finite G
+    s_seq = draw >= D || !(isfinite(G0[0]) && isfinite(G0[1]) && isfinite(G0[2]));
+    s_total = 1;
+  }
+  __syncthreads();
+  const int d0 = s_d0;
+  // The Metropolis-Hastings chain of each axis (MH_Algorithm, RBEPSample.h:63-85) is an
+  // independence sampler: proposals do not depend on the state, and a step accepts when
+  // u G(X_prev) <= G(m).  A step with u gmax <= G(m) accepts whatever the state (rounding is
+  // monotonic, and every state of the window has G <= gmax), so each state is resolved in
+  // parallel from the nearest such step before it, replaying the few steps in between exactly as
+  // the sequential chain would.  Draws whose G is infinite (proposals past the table) fall back
+  // to the sequential chain.
+  int bad = 0;
+  for (int t = threadIdx.x; t < 3 * (D - d0); t += blockDim.x) bad |= !isfinite(gw[t / (D - d0)][d0 + t % (D - d0)]);
+  if (__syncthreads_or(bad) || s_seq) {
+    if (threadIdx.x != 0) return;
+    // sequential chain from the first sample (the reference's loop, Fetch_P_Sample:155-172)
+    int X0[3] = {s_x0[0], s_x0[1], s_x0[2]};
+    double G0[3] = {s_g0[0], s_g0[1], s_g0[2]};
+    long long draw = d0;
+    int i = 1;
+    long long guard = 0;
+    while (i < P) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        double u, gm;
+        const int m_w = prop(a, draw, &u, &gm);
+        if (u * G0[a] <= gm) { X0[a] = m_w; G0[a] = gm; }
+      }
+      ++draw;
+      if (++guard > 64LL * P + 100000) { set_flag(status, kFlagSampler); break; }
+      if (X0[0] == 0 && X0[1] == 0 && X0[2] == 0) continue;
+      emit(i, X0);
+      ++i;
+    }
+    return;
+  }
+  __shared__ int chain[3][D];
+  for (int t = threadIdx.x; t < 3 * (D - d0); t += blockDim.x) {
+    const int a = t / (D - d0), d = d0 + t % (D - d0);
+    int sidx = d;
+    while (sidx >= d0 && !(ua[a][sidx] * s.gmax[a] <= gw[a][sidx])) --sidx;
+    int X;
+    double G;
+    if (sidx < d0) { X = s_x0[a]; G = s_g0[a]; sidx = d0 - 1; }
+    else { X = mw[a][sidx]; G = gw[a][sidx]; }
+    for (int k = sidx + 1; k <= d; ++k)
+      if (ua[a][k] * G <= gw[a][k]) { X = mw[a][k]; G = gw[a][k]; }
+    chain[a][d] = X;
+  }
+  __syncthreads();
+  // emission: samples 1, 2, ... are the states of the draws that are not all zero, in draw order
+  constexpr int kPer = (D + 255) / 256;
+  const int base = d0 + threadIdx.x * kPer;
+  int cnt = 0;
+#pragma unroll
+  for (int j = 0; j < kPer; ++j) {
+    const int d = base + j;
+    if (d < D && !(chain[0][d] == 0 && chain[1][d] == 0 && chain[2][d] == 0)) ++cnt;
+  }
+  // block exclusive scan of cnt (blockDim.x == 256)
+  __shared__ int wsum[8];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) wsum[wid] = incl;
+  __syncthreads();
+  int off = 0;
+  for (int w = 0; w < wid; ++w) off += wsum[w];
+  int i = 1 + off + incl - cnt;
+#pragma unroll
+  for (int j = 0; j < kPer; ++j) {
+    const int d = base + j;
+    if (d < D && !(chain[0][d] == 0 && chain[1][d] == 0 && chain[2][d] == 0)) {
+      if (i < P) {
+        const int X[3] = {chain[0][d], chain[1][d], chain[2][d]};
+        emit(i, X);
+      }
+      ++i;
+    }
+  }
+  if (threadIdx.x == 255) s_total = i;   // 1 + every non-zero state of the window
+  __syncthreads();
+  if (threadIdx.x != 0 || s_total >= P) return;
+  // more samples than the window holds: continue the chain sequentially from its last state
+  int X0[3] = {chain[0][D - 1], chain[1][D - 1], chain[2][D - 1]};
+  double G0[3];
+  for (int a = 0; a < 3; ++a) G0[a] = sampler_g(g, s.qmax, a, X0[a]);
+  long long draw = D;
+  int k = s_total;
+  long long guard = D - d0;
+  while (k < P) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       double u, gm;
@@ -802,8 +905,8 @@ __global__ void __launch_bounds__(256) k_sample(int nrep, const SamplerRep* __re
     ++draw;
     if (++guard > 64LL * P + 100000) { set_flag(status, kFlagSampler); break; }
     if (X0[0] == 0 && X0[1] == 0 && X0[2] == 0) continue;
-    emit(i, X0);
-    ++i;
+    emit(k, X0);
+    ++k;
   }
 }
 

@@ -2268,10 +2268,13 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
       for (int d = 0; d < 3; ++d) {
         const double sc = std::sqrt(f->alpha * L[d] * L[d] / (M_PI * M_PI));
         const double c = M_PI * M_PI / (f->alpha * L[d] * L[d]);
+        s.gmax[d] = 0.0;
         for (int m = 0; m <= s.qmax; ++m) {
           const double q = m == 0 ? std::erf(0.5 / sc)
                                   : (std::erf((0.5 + m) / sc) - std::erf((m - 0.5) / sc)) / 2.0;
-          qtab.push_back(q > 0 ? std::exp(-c * (double)m * (double)m) / q : INFINITY);
+          const double gv = q > 0 ? std::exp(-c * (double)m * (double)m) / q : INFINITY;
+          qtab.push_back(gv);
+          if (std::isfinite(gv)) s.gmax[d] = std::max(s.gmax[d], gv);
         }
       }
     }
