@@ -301,6 +301,16 @@ __global__ void k_regather(int n, const int* __restrict__ slot_atom, const doubl
   }
 }
 
+// Periodic cell index: v mod d in [0, d).  Stencil rows stay within one period of the box for
+// atoms inside or near it, where one compare and add replace the integer division; atoms
+// further out take the division.
+__device__ __forceinline__ int wrap_cell(int v, int d) {
+  if (v >= 0 && v < d) return v;
+  if (v < 0 && v >= -d) return v + d;
+  if (v >= d && v < 2 * d) return v - d;
+  return ((v % d) + d) % d;
+}
+
 // 1e-4 threshold of the neighbour predicate: the reference compares a float against the double
 // literal 0.0001; for float x, (double)x > 1e-4 <=> x > 1e-4f (1e-4f < 1e-4 < nextafterf(1e-4f)).
 __device__ __forceinline__ bool gt_small(float x) { return x > 1.0e-4f; }
@@ -329,7 +339,7 @@ __device__ __forceinline__ int nlist_range(int s, const int s1, const typename T
     const R r2 = sub_rn(sub_rn(pj.z, off[2]), pix[2]);
     const R d2 = add_rn(add_rn(mul_rn(r0, r0), mul_rn(r1, r1)), mul_rn(r2, r2));
     if (inside_cut(sub_rn(cut2, d2), orig) && gt_small(d2)) {
-      if (idx < cap) nbr[(size_t)idx * stride + i] = (s << kShiftBits) | code;
+      if (idx < cap) __stcs(nbr + (size_t)idx * stride + i, (s << kShiftBits) | code);
       ++idx;
     }
   }
@@ -368,12 +378,13 @@ __device__ int nlist_thread(int i, const typename Traits<R>::V4 pi, const RepDev
   const int dx0 = rp.dims[0], dx1 = rp.dims[1], dx2 = rp.dims[2];
   const bool x_contig = ci[0] - nc >= 0 && ci[0] + nc < dx0;
   int idx = 0;
-  for (int b = -nc; b <= nc; ++b)
+  for (int b = -nc; b <= nc; ++b) {
+    const int nby = ci[1] + b;
+    const int wy = wrap_cell(nby, dx1), dy = wy - nby;
     for (int c = -nc; c <= nc; ++c) {
       R off[3];
-      const int nby = ci[1] + b, nbz = ci[2] + c;
-      const int wy = ((nby % dx1) + dx1) % dx1, wz = ((nbz % dx2) + dx2) % dx2;
-      const int dy = wy - nby, dz = wz - nbz;
+      const int nbz = ci[2] + c;
+      const int wz = wrap_cell(nbz, dx2), dz = wz - nbz;
       off[1] = mul_rn(Traits<R>::dx(rp, 1), (R)dy);
       off[2] = mul_rn(Traits<R>::dx(rp, 2), (R)dz);
       const int code_yz = ((dy > 0 ? 1 : (dy < 0 ? 2 : 0)) << 2) | ((dz > 0 ? 1 : (dz < 0 ? 2 : 0)) << 4);
@@ -389,7 +400,7 @@ __device__ int nlist_thread(int i, const typename Traits<R>::V4 pi, const RepDev
       } else {
         for (int a = -nc; a <= nc; ++a) {
           const int nbx = ci[0] + a;
-          const int wx = ((nbx % dx0) + dx0) % dx0;
+          const int wx = wrap_cell(nbx, dx0);
           const int ddx = wx - nbx;
           off[0] = mul_rn(Traits<R>::dx(rp, 0), (R)ddx);
           const int code = code_yz | (ddx > 0 ? 1 : (ddx < 0 ? 2 : 0));
@@ -403,6 +414,7 @@ __device__ int nlist_thread(int i, const typename Traits<R>::V4 pi, const RepDev
         }
       }
     }
+  }
   return idx;
 }
 
@@ -478,7 +490,7 @@ __global__ void __launch_bounds__(256) k_nlist_warp(
       const unsigned m = __ballot_sync(0xffffffffu, ok);
       if (ok) {
         const int at = idx + __popc(m & below);
-        if (at < cap) nbr[(size_t)at * stride + i] = (sj << kShiftBits) | code;
+        if (at < cap) __stcs(nbr + (size_t)at * stride + i, (sj << kShiftBits) | code);
       }
       idx += __popc(m);
     }
@@ -486,7 +498,7 @@ __global__ void __launch_bounds__(256) k_nlist_warp(
   for (int b = -1; b <= 1; ++b)
     for (int c = -1; c <= 1; ++c) {
       const int nby = ci[1] + b, nbz = ci[2] + c;
-      const int wy = ((nby % dx1) + dx1) % dx1, wz = ((nbz % dx2) + dx2) % dx2;
+      const int wy = wrap_cell(nby, dx1), wz = wrap_cell(nbz, dx2);
       const int dy = wy - nby, dz = wz - nbz;
       const R o1 = mul_rn(Traits<R>::dx(rp, 1), (R)dy), o2 = mul_rn(Traits<R>::dx(rp, 2), (R)dz);
       const int code_yz = ((dy > 0 ? 1 : (dy < 0 ? 2 : 0)) << 2) | ((dz > 0 ? 1 : (dz < 0 ? 2 : 0)) << 4);
@@ -496,7 +508,7 @@ __global__ void __launch_bounds__(256) k_nlist_warp(
       } else {
         for (int a = -1; a <= 1; ++a) {
           const int nbx = ci[0] + a;
-          const int wx = ((nbx % dx0) + dx0) % dx0;
+          const int wx = wrap_cell(nbx, dx0);
           const int ddx = wx - nbx;
           scan(cell_start[row + wx], cell_start[row + wx + 1], mul_rn(Traits<R>::dx(rp, 0), (R)ddx), o1, o2,
                code_yz | (ddx > 0 ? 1 : (ddx < 0 ? 2 : 0)));
@@ -545,8 +557,8 @@ __global__ void __launch_bounds__(kStageThreads, 2) k_nlist_staged(
   const int d0 = rp.dims[0], d1 = rp.dims[1], d2 = rp.dims[2];
   for (int k = threadIdx.x; k < K; k += blockDim.x) {
     const int r = k / W, u = k - r * W;
-    const int wy = ((sg.y + r / 3 - 1) % d1 + d1) % d1, wz = ((sg.z + r % 3 - 1) % d2 + d2) % d2;
-    const int wx = ((sg.x0 - 1 + u) % d0 + d0) % d0;
+    const int wy = wrap_cell(sg.y + r / 3 - 1, d1), wz = wrap_cell(sg.z + r % 3 - 1, d2);
+    const int wx = wrap_cell(sg.x0 - 1 + u, d0);
     const int cell = rp.cell_base + wx + wy * d0 + wz * d0 * d1;
     cell_k[k] = cell;
     cnt_k[k] = cell_start[cell + 1] - cell_start[cell];
@@ -578,8 +590,8 @@ __global__ void __launch_bounds__(kStageThreads, 2) k_nlist_staged(
     for (int k = warp; k < K; k += nw) {
       const int r = k / W, u = k - r * W;
       const int nby = sg.y + r / 3 - 1, nbz = sg.z + r % 3 - 1, nbx = sg.x0 - 1 + u;
-      const int dy = ((nby % d1) + d1) % d1 - nby, dz = ((nbz % d2) + d2) % d2 - nbz;
-      const int dx = ((nbx % d0) + d0) % d0 - nbx;
+      const int dy = wrap_cell(nby, d1) - nby, dz = wrap_cell(nbz, d2) - nbz;
+      const int dx = wrap_cell(nbx, d0) - nbx;
       const R o0 = mul_rn(Traits<R>::dx(rp, 0), (R)dx), o1 = mul_rn(Traits<R>::dx(rp, 1), (R)dy),
               o2 = mul_rn(Traits<R>::dx(rp, 2), (R)dz);
       const int code = (dx > 0 ? 1 : (dx < 0 ? 2 : 0)) | ((dy > 0 ? 1 : (dy < 0 ? 2 : 0)) << 2) |
@@ -636,7 +648,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) k_nlist_staged(
           const R r2 = sub_rn(q.z, pix[2]);
           const R dd = add_rn(add_rn(mul_rn(r0, r0), mul_rn(r1, r1)), mul_rn(r2, r2));
           if (inside_cut(sub_rn(cut2, dd), orig) && gt_small(dd)) {
-            if (idx < cap) nbr[(size_t)idx * stride + i] = unpack_tag(q.w);
+            if (idx < cap) __stcs(nbr + (size_t)idx * stride + i, unpack_tag(q.w));
             ++idx;
           }
         }

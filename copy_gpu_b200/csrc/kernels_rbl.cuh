@@ -27,14 +27,6 @@ __device__ __forceinline__ R rbl_gap2(const RepDev& rp, int d, int u, int w, R x
   return g > (R)0 ? g * g : (R)0;
 }
 
-// ((nb % d) + d) % d without integer division: nb lies within num_cycles cells of the grid, so
-// one step wraps it unless the grid has fewer cells than that (bounded loop for such grids).
-__device__ __forceinline__ int wrap_cell(int nb, int d) {
-  while (nb < 0) nb += d;
-  while (nb >= d) nb -= d;
-  return nb;
-}
-
 template <class R>
 __device__ __forceinline__ R rbl_slack(const RepDev& rp, int d, R x, R rc) {
   return (R)1e-5 * (fabs(x) + fabs(Traits<R>::lo(rp, d)) + (R)rp.dims[d] * Traits<R>::dx(rp, d) + rc) + (R)1e-6;
