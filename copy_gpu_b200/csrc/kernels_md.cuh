@@ -160,6 +160,12 @@ __global__ void k_langevin(LangevinParams lp, const double* __restrict__ vel, co
 // Advance the device step counter the k-samplers read (end of a step's k-space chain).
 __global__ void k_step_inc(long long* step) { *step += 1; }
 
+// Open the rebuild body of a captured step (an IF conditional graph node) when some replica
+// rebuilds its list this step: any = rebuild[n_replicas], raised by the drift kernel.
+__global__ void k_open_rebuild(cudaGraphConditionalHandle h, const int* __restrict__ any) {
+  cudaGraphSetConditional(h, *any != 0 ? 1u : 0u);
+}
+
 // Chunk of atoms inside one replica (kinetic-energy partials, ordered per replica).
 struct MdChunk { int begin, end, rep, pad; };
 

@@ -263,6 +263,11 @@ struct rbmd_force {
   bool capturing = false;
   cudaStream_t gstream = nullptr;
   cudaEvent_t ev_begin = nullptr;
+  // captured steps put the cell sort and list build of a Verlet-skin step in a conditional graph
+  // node (cond_rebuild); cstream captures its body.  Cleared for good when a capture with it fails.
+  bool cond_rebuild = true;
+  bool cond_failed = false;
+  cudaStream_t cstream = nullptr;
   int launches = 0;
   // per-phase CUDA-event profiler (rbmd_force_profile / rbmd_force_phase_ms)
   bool prof_on = false;
@@ -404,6 +409,8 @@ void free_all(rbmd_force* f) {
   f->h_maxcount = nullptr;
   if (f->side) cudaStreamDestroy(f->side);
   f->side = nullptr;
+  if (f->cstream) cudaStreamDestroy(f->cstream);
+  f->cstream = nullptr;
   for (auto e : f->ev_pool) cudaEventDestroy(e);
   f->ev_pool.clear();
   f->ev_used = 0;
@@ -759,6 +766,17 @@ void launch_rbl_list(rbmd_force* f, cudaStream_t s) {
   f->launches++;
 }
 
+// List reuse under a Verlet skin: refresh the slot caches of the replicas that keep their list
+// from the new positions (the cell sort refreshes the others).
+template <class R>
+void launch_regather(rbmd_force* f, cudaStream_t s) {
+  const int n = f->n;
+  k_regather<R><<<(n + 255) / 256, 256, 0, s>>>(
+      n, f->d_slot_atom, f->at.pos, f->at.charge, f->nrep > 1 ? f->d_rep_of : nullptr, f->d_reps,
+      (typename Traits<R>::V4*)f->d_pos4, nullptr, f->d_xref, f->d_rebuild);
+  f->launches++;
+}
+
 // bin: run k_bin (positions given by the caller, or a Verlet skin whose drift does not bin);
 // regather: refresh the slot caches on list-reuse steps (the drift did not write them).
 template <class R>
@@ -794,13 +812,7 @@ void launch_sort(rbmd_force* f, cudaStream_t s, bool bin, bool regather) {
       rep_of, f->d_reps, f->d_slot_atom, f->d_atom_slot, (typename Traits<R>::V4*)f->d_pos4, nullptr,
       f->d_meta, f->d_xref, rb, f->sort_x() ? 1 : 0, f->d_cell_rep);
   f->launches += 4;
-  if (rb && regather) {
-    // list reuse: refresh the slot caches from the new positions (no-op on rebuild steps)
-    k_regather<R><<<(n + 255) / 256, 256, 0, s>>>(
-        n, f->d_slot_atom, f->at.pos, f->at.charge, f->nrep > 1 ? f->d_rep_of : nullptr, f->d_reps,
-        (typename Traits<R>::V4*)f->d_pos4, nullptr, f->d_xref, rb);
-    f->launches++;
-  }
+  if (rb && regather) launch_regather<R>(f, s);
 }
 
 // Samples of the own proposal for `step`: with a trained network the per-bin log-weights h come
@@ -1116,6 +1128,55 @@ void launch_water(rbmd_force* f, cudaStream_t s) {
   f->launches++;
 }
 
+// Cell sort + list build of a Verlet-skin step captured into a graph: whether any replica
+// rebuilds is decided on the device (the drift kernel's skin check), so the two run in the body
+// of an IF conditional node that k_open_rebuild opens only on rebuild steps; list-reuse steps
+// then skip them instead of launching kernels that read the flag and exit.  The list-reuse
+// re-gather stays outside, after the node.  Returns false when nothing was added to the capture
+// or only an empty node (the caller then launches the two directly, after it); a failure past
+// that point sets cond_failed, and the step is captured again without the node.
+template <class R>
+bool launch_rebuild_conditional(rbmd_force* f, cudaStream_t s, bool bin) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  if (cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd) != cudaSuccess || cs != cudaStreamCaptureStatusActive)
+    return false;
+  if (!f->cstream && cudaStreamCreateWithFlags(&f->cstream, cudaStreamNonBlocking) != cudaSuccess) return false;
+  cudaGraphConditionalHandle h;
+  if (cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) return false;
+  k_open_rebuild<<<1, 1, 0, s>>>(h, f->d_rebuild + f->nrep);
+  f->launches++;
+  if (cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd) != cudaSuccess) {
+    f->cond_failed = true;
+    return true;
+  }
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeIf;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  if (cudaGraphAddNode(&node, g, deps, nd, &cp) != cudaSuccess) {
+    f->cond_failed = true;
+    return true;
+  }
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  if (cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies) != cudaSuccess) {
+    f->cond_failed = true;
+    return true;
+  }
+  if (cudaStreamBeginCaptureToGraph(f->cstream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
+      cudaSuccess)
+    return false;   // an empty body: the sort and list follow the node unconditionally
+  launch_sort<R>(f, f->cstream, bin, false);
+  launch_nlist<R>(f, f->cstream);
+  cudaGraph_t out = nullptr;
+  if (cudaStreamEndCapture(f->cstream, &out) != cudaSuccess) f->cond_failed = true;
+  return true;
+}
+
 // Force evaluation from the current master positions: the k-space chain forks onto the side
 // stream, the cell sort / neighbour list / near pass / intramolecular terms run on the caller's
 // stream, and the far force is folded in after the join.
@@ -1126,7 +1187,15 @@ void launch_force_tail(rbmd_force* f, cudaStream_t s, bool bin, bool regather) {
     cudaEventRecord(f->ev_fork, s);
     launch_kspace<R>(f, f->side, f->ev_fork);
   }
-  launch_sort<R>(f, s, bin, regather);
+  // a captured Verlet-skin step: sort + list in a conditional node (not for RBL, whose list is
+  // rebuilt every step)
+  const bool cond = f->capturing && f->cond_rebuild && f->skin > 0 && !f->is_rbl() && bin &&
+                    launch_rebuild_conditional<R>(f, s, bin);
+  if (cond) {
+    if (regather) launch_regather<R>(f, s);
+  } else {
+    launch_sort<R>(f, s, bin, regather);
+  }
   if (f->is_rbl()) {
     if (kspace) cudaEventRecord(f->ev_join, f->side);
     launch_rbl_list<R>(f, s);
@@ -1134,7 +1203,7 @@ void launch_force_tail(rbmd_force* f, cudaStream_t s, bool bin, bool regather) {
     launch_rbl_force<R>(f, s);
   } else {
     if (kspace) cudaEventRecord(f->ev_join, f->side);
-    launch_nlist<R>(f, s);
+    if (!cond) launch_nlist<R>(f, s);
     PhaseScope ps(f, kPhForce, s);
     if (f->is_eam()) launch_eam<R>(f, s);
     else launch_near<R>(f, s);
@@ -1351,29 +1420,34 @@ rbmd_status run_steps(rbmd_force* f, int n_steps, cudaStream_t s) {
     const long long sc = f->step_count;
     const bool pend = f->pending_scale;
     const int l0 = f->launches;
-    cudaGraph_t g = nullptr;
-    CK(cudaStreamBeginCapture(f->gstream, cudaStreamCaptureModeThreadLocal));
-    f->capturing = true;
-    for (int k = 0; k < steps; ++k) launch_step<R>(f, f->gstream);
-    f->capturing = false;
-    const cudaError_t e = cudaStreamEndCapture(f->gstream, &g);
-    *launches = f->launches - l0;
-    f->launches = l0;
-    f->step_count = sc;
-    f->pending_scale = pend;
-    if (e != cudaSuccess || !g) {
-      std::snprintf(g_last_error, sizeof g_last_error, "step capture: %s", cudaGetErrorString(e));
+    // a second attempt runs without the conditional rebuild node when the first could not
+    // build it (cond_failed) or its graph does not capture or instantiate here
+    for (int attempt = 0;; ++attempt) {
+      cudaGraph_t g = nullptr;
+      CK(cudaStreamBeginCapture(f->gstream, cudaStreamCaptureModeThreadLocal));
+      f->capturing = true;
+      for (int k = 0; k < steps; ++k) launch_step<R>(f, f->gstream);
+      f->capturing = false;
+      const cudaError_t e = cudaStreamEndCapture(f->gstream, &g);
+      *launches = f->launches - l0;
+      f->launches = l0;
+      f->step_count = sc;
+      f->pending_scale = pend;
+      cudaError_t ei = e;
+      if (e == cudaSuccess && g && !f->cond_failed) ei = cudaGraphInstantiate(exec, g, 0);
       if (g) cudaGraphDestroy(g);
-      return RBMD_ERR_CUDA;
-    }
-    const cudaError_t ei = cudaGraphInstantiate(exec, g, 0);
-    cudaGraphDestroy(g);
-    if (ei != cudaSuccess) {
-      std::snprintf(g_last_error, sizeof g_last_error, "step graph: %s", cudaGetErrorString(ei));
+      if (ei == cudaSuccess && g && !f->cond_failed) return RBMD_OK;
+      const bool retry = attempt == 0 && f->cond_rebuild;
+      f->cond_failed = false;
+      f->cond_rebuild = false;
+      cudaGetLastError();
       *exec = nullptr;
-      return RBMD_ERR_CUDA;
+      if (!retry) {
+        std::snprintf(g_last_error, sizeof g_last_error, "step graph: %s",
+                      cudaGetErrorString(ei != cudaSuccess ? ei : cudaErrorUnknown));
+        return RBMD_ERR_CUDA;
+      }
     }
-    return RBMD_OK;
   };
   if (!f->graph_exec || f->graph_pending != f->pending_scale) {
     if (f->graph_exec) cudaGraphExecDestroy(f->graph_exec);

@@ -473,22 +473,28 @@ def test_cuda_graph_replay_is_bit_identical(cuda, proposal):
     assert out[0][2] == out[1][2]
 
 
-def test_cuda_graph_water_shake(cuda):
+@pytest.mark.parametrize("skin", [0.0, 1.0])
+def test_cuda_graph_water_shake(cuda, skin):
+    """SHAKE water through graph replay equals direct launches bit for bit; with a Verlet skin the
+    captured steps hold the cell sort and list build in a conditional node and re-gather the slot
+    caches after it on list-reuse steps."""
     import torch
     out = []
     for graph in (True, False):
         s = systems.water(n_mol=300, seed=4)
         cfg = systems.water_config(P=32, precision="fp32")
+        cfg["hyper_parameters"]["neighbor"]["skin"] = skin
         cfg["execution"]["cuda_graph"] = graph
         dev = to_dev(s, cuda)
         ff = make_ff(cfg, s, dev)
         ff.Execute()
-        ff.step(12)
+        ff.step(40)
         ff.sync_velocities()
         torch.cuda.synchronize()
         assert ff.status() == 0
-        out.append(dev["pos"].cpu().numpy())
-    assert np.array_equal(out[0], out[1])
+        out.append((dev["pos"].cpu().numpy(), ff.list_builds()))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[0][1] == out[1][1] and (skin == 0 or out[0][1] >= 2)
 
 
 def test_graph_steps_and_state_changes(cuda):
