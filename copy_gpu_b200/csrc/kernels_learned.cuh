@@ -12,6 +12,7 @@
 
 #include "common.cuh"
 #include "kernels_force.cuh"
+#include "mlp_forward.cuh"
 #include "mlp_types.cuh"
 
 namespace rbmd {
@@ -90,62 +91,86 @@ __device__ __forceinline__ int cdf_search(const double* cdf, int n, double u) {
   return lo;
 }
 
-// Draw the P k-samples of each replica (one block of 256 threads per replica).  Candidates are
-// exact draws from p (inverse CDF per axis, 53-bit uniforms from Philox4x32-10 keyed by seed,
-// counter (round * 256 + thread, replica, step)); m = 0 is rejected; a candidate in bin b is
+// Draw the P k-samples of each replica (one block of kSampThreads threads per replica: a round of
+// that many candidates usually completes the set, and the block's 32 warps keep their share of an
+// SM that the near pass also occupies).  Candidates are exact draws from p (inverse CDF per axis,
+// 53-bit uniforms from Philox4x32-10 keyed by seed, counter (round * kSampThreads + thread,
+// replica, step)); m = 0 is rejected; a candidate in bin b is
 // accepted with probability e^{h_b - h_max} (h clamped below at h_max - 8), so accepted samples
 // follow q; they are emitted in (round, thread) order, which makes the draw deterministic.
 // Weight w = Z / e^{h_b - h_max} with Z = sum_b W_b e^{h_b - h_max} (W_b = p-mass of bin b),
-// i.e. p / q.  h == nullptr samples p itself with unit weights.  When max_rounds run out the
-// remaining samples get weight 0 and RBMD_FLAG_SAMPLER is raised.
-__global__ void __launch_bounds__(256) k_prop_sample(
+// i.e. p / q.  With mlp (the network's parameters) the block first evaluates h itself from the
+// conditioning spectrum spec (bin features in shared memory, four lanes per bin through
+// mlp_row_forward4), so the sampler is one launch; otherwise h is read from h[], and h == nullptr
+// samples p itself with unit weights.  When max_rounds run out the remaining samples get weight 0
+// and RBMD_FLAG_SAMPLER is raised.
+constexpr int kSampThreads = 1024;
+__global__ void __launch_bounds__(kSampThreads) k_prop_sample(
     int nrep, const RepDev* __restrict__ reps, const PropRep* __restrict__ prep, const double* __restrict__ cdf,
-    const float* __restrict__ h, const double* __restrict__ wbin, unsigned long long seed, long long step_arg,
+    const float* __restrict__ h, const float* __restrict__ mlp, const float* __restrict__ spec,
+    const double* __restrict__ wbin, unsigned long long seed, long long step_arg,
     const long long* __restrict__ step_dev, int max_rounds, int* __restrict__ kvec_out, void* __restrict__ krec, int rec_bytes, int* __restrict__ krep,
     double* __restrict__ weights, uint32_t* status) {
   const int r = blockIdx.x;
   if (r >= nrep) return;
   const long long step = step_dev ? *step_dev : step_arg;   // device counter under graph replay
   const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  constexpr int kW = kSampThreads / 32;
   const PropRep pr = prep[r];
   const int P = reps[r].P, kb = reps[r].k_begin;
   __shared__ float acc_s[kPropBins];
-  __shared__ double red[8];
+  __shared__ double red[kW];
   __shared__ double zsum;
-  __shared__ int wcount[8];
+  __shared__ int wcount[kW];
   __shared__ int total;
   __shared__ double cdf_s[3 * (2 * kPropMaxM + 1)];
   const int n0 = 2 * pr.M[0] + 1, n1 = 2 * pr.M[1] + 1, n2 = 2 * pr.M[2] + 1;
   const bool staged = pr.M[0] <= kPropMaxM && pr.M[1] <= kPropMaxM && pr.M[2] <= kPropMaxM;
+  const bool learned = mlp != nullptr || h != nullptr;
+  if (mlp) {
+    // h of every bin: inputs in the CDF buffer (staged only afterwards), h into acc_s
+    static_assert(sizeof(cdf_s) >= sizeof(float) * kPropBins * kMlpIn, "bin inputs fit the CDF buffer");
+    float* xs = reinterpret_cast<float*>(cdf_s);
+    if (t < kPropBins) prop_features(t, spec + (size_t)r * kPropBands, xs + t * kMlpIn);
+    __syncthreads();
+    static_assert(kSampThreads == 4 * kPropBins, "four lanes per bin");
+    const float hb = mlp_row_forward4(mlp, xs + (t >> 2) * kMlpIn, t & 3);
+    if ((t & 3) == 0) acc_s[t >> 2] = hb;
+    __syncthreads();
+  }
   const double *c0 = cdf + pr.cdf_off[0], *c1 = cdf + pr.cdf_off[1], *c2 = cdf + pr.cdf_off[2];
   if (staged) {
-    for (int i = t; i < n0; i += 256) cdf_s[i] = c0[i];
-    for (int i = t; i < n1; i += 256) cdf_s[n0 + i] = c1[i];
-    for (int i = t; i < n2; i += 256) cdf_s[n0 + n1 + i] = c2[i];
+    for (int i = t; i < n0; i += kSampThreads) cdf_s[i] = c0[i];
+    for (int i = t; i < n1; i += kSampThreads) cdf_s[n0 + i] = c1[i];
+    for (int i = t; i < n2; i += kSampThreads) cdf_s[n0 + n1 + i] = c2[i];
     c0 = cdf_s;
     c1 = cdf_s + n0;
     c2 = cdf_s + n0 + n1;
   }
-  // acceptance per bin and the normaliser Z (block reduction in a fixed order)
-  float hv = h ? h[(size_t)r * kPropBins + t] : 0.f;
+  // acceptance per bin and the normaliser Z (threads t < kPropBins, one bin each; block
+  // reductions over their 8 warps in a fixed order)
+  constexpr int kBW = kPropBins / 32;
+  const bool bin_t = t < kPropBins;
+  float hv = 0.f;
+  if (bin_t) hv = mlp ? acc_s[t] : (h ? h[(size_t)r * kPropBins + t] : 0.f);
   float hmax = hv;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) hmax = fmaxf(hmax, __shfl_xor_sync(0xffffffffu, hmax, o));
-  if (lane == 0) red[wid] = hmax;
+  if (lane == 0 && bin_t) red[wid] = hmax;
   __syncthreads();
   hmax = (float)red[0];
-  for (int k = 1; k < 8; ++k) hmax = fmaxf(hmax, (float)red[k]);
+  for (int k = 1; k < kBW; ++k) hmax = fmaxf(hmax, (float)red[k]);
   __syncthreads();
-  const float acc = h ? __expf(fmaxf(hv - hmax, -8.0f)) : 1.0f;
-  acc_s[t] = acc;
-  double zpart = wbin[(size_t)r * kPropBins + t] * (double)acc;
+  const float acc = learned ? __expf(fmaxf(hv - hmax, -8.0f)) : 1.0f;
+  if (bin_t) acc_s[t] = acc;
+  double zpart = bin_t ? wbin[(size_t)r * kPropBins + t] * (double)acc : 0.0;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) zpart += __shfl_xor_sync(0xffffffffu, zpart, o);
-  if (lane == 0) red[wid] = zpart;
+  if (lane == 0 && bin_t) red[wid] = zpart;
   __syncthreads();
   if (t == 0) {
     double z = 0;
-    for (int k = 0; k < 8; ++k) z += red[k];
+    for (int k = 0; k < kBW; ++k) z += red[k];
     zsum = z;
     total = 0;
   }
@@ -155,7 +180,7 @@ __global__ void __launch_bounds__(256) k_prop_sample(
   for (int round = 0; round < max_rounds; ++round) {
     const int done = total;
     if (done >= P) break;
-    uint32_t ca[4] = {(uint32_t)(round * 256 + t), (uint32_t)r, (uint32_t)(unsigned long long)step,
+    uint32_t ca[4] = {(uint32_t)(round * kSampThreads + t), (uint32_t)r, (uint32_t)(unsigned long long)step,
                       (uint32_t)((unsigned long long)step >> 32)};
     uint32_t cb[4] = {ca[0], ca[1] | 0x80000000u, ca[2], ca[3]};
     philox4x32(ca, k0, k1);
@@ -174,7 +199,7 @@ __global__ void __launch_bounds__(256) k_prop_sample(
     if (lane == 0) wcount[wid] = __popc(bal);
     __syncthreads();
     int before = 0, sum = 0;
-    for (int k = 0; k < 8; ++k) {
+    for (int k = 0; k < kW; ++k) {
       if (k < wid) before += wcount[k];
       sum += wcount[k];
     }
@@ -186,7 +211,7 @@ __global__ void __launch_bounds__(256) k_prop_sample(
       int* rec = reinterpret_cast<int*>(reinterpret_cast<char*>(krec) + (size_t)g * rec_bytes);
       rec[0] = mx; rec[1] = my; rec[2] = mz;
       krep[g] = r;
-      weights[g] = h ? Z / (double)acc_s[b] : 1.0;
+      weights[g] = learned ? Z / (double)acc_s[b] : 1.0;
     }
     __syncthreads();
     if (t == 0) total = done + sum;
@@ -194,7 +219,7 @@ __global__ void __launch_bounds__(256) k_prop_sample(
   }
   if (total < P) {
     if (t == 0) set_flag(status, kFlagSampler);
-    for (int i = total + t; i < P; i += 256) {
+    for (int i = total + t; i < P; i += kSampThreads) {
       const int g = kb + i;
       int* o = kvec_out + 3 * g;
       o[0] = 1; o[1] = 0; o[2] = 0;

@@ -26,6 +26,12 @@ cudaError_t mlp_launch(const MlpArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+cudaError_t mlp_infer(int groups, const float* params, const float* x, float* h, cudaStream_t s) {
+  const int rows = groups * kMlpRows;
+  k_mlp_infer<<<(4 * rows + 127) / 128, 128, 0, s>>>(rows, params, x, h);
+  return cudaGetLastError();
+}
+
 cudaError_t mlp_grad_sum(int groups, const float* partial, float* grad, cudaStream_t s) {
   k_mlp_grad_sum<<<(kMlpNParam + 255) / 256, 256, 0, s>>>(groups, partial, grad);
   return cudaGetLastError();
@@ -44,15 +50,26 @@ RBMD_API rbmd_status rbmd_proposal_mlp_eval(const float* params, const float* x,
                                             const float* cbin, int32_t groups, int32_t train, float* h,
                                             double* loss, float* grad, uint32_t* status, void* stream) {
   using namespace rbmd;
-  if (!params || !x || groups < 1 || !status || (train && (!wbin || !cbin || !loss || !grad)))
+  if (!params || !x || groups < 1 || !status || (train > 0 && (!wbin || !cbin || !loss || !grad)) ||
+      (train < 0 && !h))
     return RBMD_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
+  if (train < 0) {   // the sampler's per-step forward pass on the CUDA cores
+    cudaError_t e = mlp_infer(groups, params, x, h, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+      std::snprintf(rbmd_internal::g_last_error, sizeof rbmd_internal::g_last_error, "mlp_eval: %s",
+                    cudaGetErrorString(e));
+      return RBMD_ERR_CUDA;
+    }
+    return RBMD_OK;
+  }
   float* partial = nullptr;
   if (train && cudaMalloc(&partial, sizeof(float) * (size_t)groups * kMlpNParam) != cudaSuccess)
     return RBMD_ERR_CUDA;
   MlpArgs a{};
   a.groups = groups;
-  a.train = train;
+  a.train = train > 0;
   a.gscale = 1.0f / (float)groups;
   a.params = params;
   a.x = x;

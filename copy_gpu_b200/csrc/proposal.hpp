@@ -6,6 +6,8 @@
 
 namespace rbmd {
 cudaError_t mlp_launch(const MlpArgs& a, cudaStream_t s);
+// forward pass on the CUDA cores (k_mlp_infer): h[groups * 256] from x
+cudaError_t mlp_infer(int groups, const float* params, const float* x, float* h, cudaStream_t s);
 cudaError_t mlp_grad_sum(int groups, const float* partial, float* grad, cudaStream_t s);
 cudaError_t mlp_adam(float* params, const float* grad, float* m, float* v, float lr, int step, cudaStream_t s);
 }  // namespace rbmd

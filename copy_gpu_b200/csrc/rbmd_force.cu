@@ -107,7 +107,7 @@ struct rbmd_force {
   double* d_wbin = nullptr;         // [nrep][256] Gaussian mass per bin
   std::vector<double> wbin_h;
   double* d_pw = nullptr;           // [Ptot] importance weights of the drawn samples
-  float *d_mlp = nullptr, *d_h = nullptr, *d_feat = nullptr, *d_spec = nullptr;
+  float *d_mlp = nullptr, *d_spec = nullptr;
   int* d_spec_init = nullptr;
   int P = 100, kmax = 2;
   unsigned long long seed = 20240101ull;
@@ -245,6 +245,7 @@ struct rbmd_force {
   // streams
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_tail = nullptr;   // end of the k-space stream's work of a step (after the join)
   long long step_count = 0;
   long long* d_step = nullptr;   // step index of the k-samplers on the device (graph replay)
   long long* d_lstep = nullptr;  // Langevin noise counter (advanced after every application)
@@ -252,6 +253,9 @@ struct rbmd_force {
   bool langevin_shared = false;  // compat.langevin_reference: m = 1, kBT = 1, one xi for all
   double langevin_xi[3] = {0, 0, 0};
   bool in_step = false;          // launches belong to rbmd_force_step (advance d_step)
+  // the k-set of the next step was drawn at the end of the last step's k-space chain (own
+  // samplers); any host-side change of sampler state clears it (drop_graphs)
+  bool presampled = false;
   bool use_graph = true;         // execution.cuda_graph: replay a captured step
   cudaGraphExec_t graph_exec = nullptr;
   cudaGraphExec_t graph_multi = nullptr;   // graph_steps consecutive steps in one graph
@@ -374,8 +378,8 @@ void free_all(rbmd_force* f) {
   f->d_frac = nullptr;
   dfree(f->d_meta); dfree(f->d_nbr); dfree(f->d_count); dfree(f->d_maxcount); dfree(f->d_status);
   dfree(f->d_count2); dfree(f->d_mean_partial); dfree(f->d_erf_tab);
-  dfree(f->d_prep); dfree(f->d_cdf); dfree(f->d_wbin); dfree(f->d_pw); dfree(f->d_mlp); dfree(f->d_h);
-  dfree(f->d_feat); dfree(f->d_spec); dfree(f->d_spec_init);
+  dfree(f->d_prep); dfree(f->d_cdf); dfree(f->d_wbin); dfree(f->d_pw); dfree(f->d_mlp);
+  dfree(f->d_spec); dfree(f->d_spec_init);
   dfree(f->d_rebuild); dfree(f->d_block_sums); dfree(f->d_cell_rep); dfree(f->d_xref); dfree(f->d_nbuilds);
   dfree(f->d_segs);
   f->nsegs = 0;
@@ -417,7 +421,8 @@ void free_all(rbmd_force* f) {
   f->prof_pairs.clear();
   if (f->ev_fork) cudaEventDestroy(f->ev_fork);
   if (f->ev_join) cudaEventDestroy(f->ev_join);
-  f->ev_fork = f->ev_join = nullptr;
+  if (f->ev_tail) cudaEventDestroy(f->ev_tail);
+  f->ev_fork = f->ev_join = f->ev_tail = nullptr;
 }
 
 // Replica geometry: ContPointLocator::SetRange/SetCutOff/SetRs in the reference's float
@@ -573,8 +578,6 @@ rbmd_status build_proposal_tables(rbmd_force* f, const std::vector<int64_t>& qof
   CK(dalloc(&f->d_pw, (size_t)f->Ptot));
   CK(dalloc(&f->d_mlp, (size_t)kMlpNParam));
   CK(cudaMemset(f->d_mlp, 0, sizeof(float) * kMlpNParam));
-  CK(dalloc(&f->d_h, (size_t)nrep * kPropBins));
-  CK(dalloc(&f->d_feat, (size_t)nrep * kPropBins * kMlpIn));
   CK(dalloc(&f->d_spec, (size_t)nrep * kPropBands));
   CK(cudaMemset(f->d_spec, 0, sizeof(float) * nrep * kPropBands));
   CK(dalloc(&f->d_spec_init, (size_t)nrep));
@@ -689,6 +692,7 @@ rbmd_status train_fit(rbmd_force* f, const rbmd_train_opts* o, rbmd_train_report
   std::vector<int> ones(f->nrep, 1);
   CK(cudaMemcpy(f->d_spec_init, ones.data(), sizeof(int) * f->nrep, cudaMemcpyHostToDevice));
   f->prop_trained = true;
+  f->presampled = false;
   if (rep) {
     rep->loss_gauss = lg;
     rep->loss_first = l_first;
@@ -820,23 +824,10 @@ void launch_sort(rbmd_force* f, cudaStream_t s, bool bin, bool regather) {
 // sampler draws from q = p e^h / Z with weights p / q; otherwise it draws from p.
 void launch_prop_sample(rbmd_force* f, cudaStream_t s, long long step, int rec_bytes,
                         const long long* step_dev = nullptr) {
-  const float* h = nullptr;
-  if (f->proposal == "learned" && f->prop_trained) {
-    k_prop_features<<<(f->nrep * kPropBins + 255) / 256, 256, 0, s>>>(f->nrep, f->d_spec, f->d_feat);
-    MlpArgs a{};
-    a.groups = f->nrep;
-    a.train = 0;
-    a.gscale = 1.f;
-    a.params = f->d_mlp;
-    a.x = f->d_feat;
-    a.h = f->d_h;
-    a.status = f->d_status;
-    mlp_launch(a, s);
-    h = f->d_h;
-    f->launches += 2;
-  }
-  k_prop_sample<<<f->nrep, 256, 0, s>>>(f->nrep, f->d_reps, f->d_prep, f->d_cdf, h, f->d_wbin, f->seed, step,
-                                        step_dev, 4096, f->d_kvec, f->d_krec, rec_bytes, f->d_krep, f->d_pw, f->d_status);
+  const float* mlp = f->proposal == "learned" && f->prop_trained ? f->d_mlp : nullptr;
+  k_prop_sample<<<f->nrep, kSampThreads, 0, s>>>(f->nrep, f->d_reps, f->d_prep, f->d_cdf, nullptr, mlp, f->d_spec,
+                                                 f->d_wbin, f->seed, step, step_dev, 4096, f->d_kvec, f->d_krec,
+                                                 rec_bytes, f->d_krep, f->d_pw, f->d_status);
   f->launches++;
 }
 
@@ -847,8 +838,10 @@ template <class R>
 void launch_kspace(rbmd_force* f, cudaStream_t s, cudaEvent_t ready) {
   const int rec_bytes = sizeof(typename KRec<R>::T);
   if (f->capturing) cudaStreamWaitEvent(s, f->ev_begin, 0);   // the side stream joins the capture
-  const bool own_prop = !f->injected && f->coul_type == "RBE" && f->proposal != "gauss";
-  if (!f->injected && f->coul_type == "RBE") {
+  const bool own = !f->injected && f->coul_type == "RBE";
+  const bool own_prop = own && f->proposal != "gauss";
+  // the own sampler for the step index in the device counter
+  auto sample = [&] {
     PhaseScope ps(f, kPhSample, s);
     if (!own_prop) {
       k_sample<kSamplerD><<<f->nrep, 256, 0, s>>>(f->nrep, f->d_srep, f->d_qtab, f->d_reps, f->seed,
@@ -858,13 +851,18 @@ void launch_kspace(rbmd_force* f, cudaStream_t s, cudaEvent_t ready) {
     } else {
       launch_prop_sample(f, s, f->step_count, rec_bytes, f->d_step);
     }
-  }
+  };
+  // this step's k-set, unless the last step's chain drew it already
+  if (own && !f->presampled) sample();
+  f->presampled = false;
   cudaStreamWaitEvent(s, ready, 0);
   if (f->nq == 0) {
+    cudaEventRecord(f->ev_join, s);
     if (f->in_step) {
       k_step_inc<<<1, 1, 0, s>>>(f->d_step);
       f->launches++;
     }
+    cudaEventRecord(f->ev_tail, s);
     return;
   }
   const int* rep_of = f->nrep > 1 ? f->d_rep_of : nullptr;
@@ -893,10 +891,20 @@ void launch_kspace(rbmd_force* f, cudaStream_t s, cudaEvent_t ready) {
                                             f->d_spec, f->d_spec_init);
     f->launches++;
   }
+  // the caller stream joins here (ev_join): the step counter and the next step's k-set come after
+  cudaEventRecord(f->ev_join, s);
   if (f->in_step) {
     k_step_inc<<<1, 1, 0, s>>>(f->d_step);
     f->launches++;
+    // the next step's k-set, drawn behind the join: the sampler depends only on the step counter
+    // and the conditioning spectrum just updated, so it overlaps the caller's kick, thermostat and
+    // next drift instead of opening the next step's chain ahead of its structure factors
+    if (own) {
+      sample();
+      f->presampled = true;
+    }
   }
+  cudaEventRecord(f->ev_tail, s);
 }
 
 template <class R, bool COUL, int MI>
@@ -1197,12 +1205,10 @@ void launch_force_tail(rbmd_force* f, cudaStream_t s, bool bin, bool regather) {
     launch_sort<R>(f, s, bin, regather);
   }
   if (f->is_rbl()) {
-    if (kspace) cudaEventRecord(f->ev_join, f->side);
     launch_rbl_list<R>(f, s);
     PhaseScope ps(f, kPhForce, s);
     launch_rbl_force<R>(f, s);
   } else {
-    if (kspace) cudaEventRecord(f->ev_join, f->side);
     if (!cond) launch_nlist<R>(f, s);
     PhaseScope ps(f, kPhForce, s);
     if (f->is_eam()) launch_eam<R>(f, s);
@@ -1239,6 +1245,7 @@ void launch_force_tail(rbmd_force* f, cudaStream_t s, bool bin, bool regather) {
 template <class R>
 void launch_compute(rbmd_force* f, cudaStream_t s) {
   f->want_energy = true;
+  f->presampled = false;   // a force call draws the k-set of the current step counter itself
   cudaMemsetAsync(f->d_maxcount, 0, 2 * sizeof(int), s);
   if (f->skin > 0 && f->list_valid) {
     // reuse the list when no atom moved more than skin/2 since it was built
@@ -1263,6 +1270,7 @@ void launch_compute_any(rbmd_force* f, cudaStream_t s) {
 // k-samples, importance weights, proposal, topology); whatever changes one of them drops them,
 // and the next multi-step call captures again.
 void drop_graphs(rbmd_force* f) {
+  f->presampled = false;
   if (f->graph_exec || f->graph_multi) cudaDeviceSynchronize();   // none still in flight
   if (f->graph_exec) cudaGraphExecDestroy(f->graph_exec);
   f->graph_exec = nullptr;
@@ -1408,9 +1416,11 @@ rbmd_status run_steps(rbmd_force* f, int n_steps, cudaStream_t s) {
   const bool graph = f->use_graph && f->energy_every == 0 && !f->prof_on && n_steps > 1;
   if (!graph) {
     for (int k = 0; k < n_steps; ++k) launch_step<R>(f, s);
+    if (f->is_rbe()) cudaStreamWaitEvent(s, f->ev_tail, 0);   // the k-space stream's tail joins s
     return RBMD_OK;
   }
   launch_step<R>(f, s);
+  if (f->is_rbe()) cudaStreamWaitEvent(s, f->ev_tail, 0);   // graph launches on s follow the whole step
   const int per_step = f->launches;
   if (!f->gstream) CK(cudaStreamCreateWithFlags(&f->gstream, cudaStreamNonBlocking));
   if (!f->ev_begin) CK(cudaEventCreateWithFlags(&f->ev_begin, cudaEventDisableTiming));
@@ -1427,6 +1437,7 @@ rbmd_status run_steps(rbmd_force* f, int n_steps, cudaStream_t s) {
       CK(cudaStreamBeginCapture(f->gstream, cudaStreamCaptureModeThreadLocal));
       f->capturing = true;
       for (int k = 0; k < steps; ++k) launch_step<R>(f, f->gstream);
+      if (f->is_rbe()) cudaStreamWaitEvent(f->gstream, f->ev_tail, 0);   // the last step's k-space tail
       f->capturing = false;
       const cudaError_t e = cudaStreamEndCapture(f->gstream, &g);
       *launches = f->launches - l0;
@@ -2216,6 +2227,7 @@ rbmd_status rbmd_force_bind(rbmd_force* f, const rbmd_atoms_dev* a) {
   }
   CK(cudaEventCreateWithFlags(&f->ev_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&f->ev_join, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&f->ev_tail, cudaEventDisableTiming));
   // host-side range checks: every device index derived from these arrays stays in bounds
   if (a->type) {
     std::vector<int> ty(n);
@@ -2492,6 +2504,7 @@ rbmd_status rbmd_force_get_ksamples(rbmd_force* f, int32_t* m_xyz, int32_t P) {
 rbmd_status rbmd_force_sample_k(rbmd_force* f, int64_t step, int32_t* m_xyz, int32_t P) {
   if (!f || !f->bound || !f->is_rbe() || P != f->P || f->coul_type != "RBE") return RBMD_ERR_ARG;
   const int recb = f->fp64 ? sizeof(KRec64) : sizeof(KRec32);
+  f->presampled = false;   // overwrites the k-set buffers
   if (f->proposal != "gauss")
     launch_prop_sample(f, nullptr, step, recb);
   else
@@ -2803,7 +2816,7 @@ rbmd_status rbmd_force_train_proposal(rbmd_force* f, const rbmd_train_opts* o, r
     }
     k_frac<float><<<(nq0 + 255) / 256, 256, 0, s>>>(nq0, f->d_qidx, f->at.pos, f->at.charge, rep_of, f->d_reps,
                                                      frac);
-    k_prop_sample<<<1, 256, 0, s>>>(1, rep1, f->d_prep, f->d_cdf, nullptr, f->d_wbin, o->seed,
+    k_prop_sample<<<1, kSampThreads, 0, s>>>(1, rep1, f->d_prep, f->d_cdf, nullptr, nullptr, nullptr, f->d_wbin, o->seed,
                                     (1LL << 40) + sn, nullptr, 4096, kv, krec, 12, krep, kw, f->d_status);
     const dim3 grid((K + 255) / 256, nch);
     for (int pass = 0; pass < 2; ++pass) {
@@ -2824,6 +2837,7 @@ rbmd_status rbmd_force_proposal_params(rbmd_force* f, float* get_host, const flo
   if (set_host) {
     CK(cudaMemcpy(f->d_mlp, set_host, sizeof(float) * kMlpNParam, cudaMemcpyHostToDevice));
     f->prop_trained = true;
+  f->presampled = false;
   }
   if (get_host) CK(cudaMemcpy(get_host, f->d_mlp, sizeof(float) * kMlpNParam, cudaMemcpyDeviceToHost));
   return RBMD_OK;

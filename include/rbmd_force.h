@@ -295,7 +295,10 @@ RBMD_API rbmd_status rbmd_rhok_noalloc(const double* pos_dev, const double* char
  * params[5313] (W1[64][16], b1[64], W2[64][64], b2[64], w3[64], b3), x[groups*256][16] inputs,
  * h[groups*256] outputs.  With train != 0 also the group losses
  * loss[g] = log sum_b wbin_b e^{h_b} + log sum_b cbin_b e^{-h_b} and the gradient of their mean
- * into grad[5313].  status receives 0x80 when an internal wait gave up.  Synchronises the stream.
+ * into grad[5313].  status receives 0x80 when an internal wait gave up.  train < 0 evaluates h
+ * alone on the CUDA cores instead, as the sampler does every step (same BF16 roundings, FP32 sums
+ * in another order; no shared memory, so it shares SMs with a running near pass).  Synchronises
+ * the stream.
  * No reference counterpart (the reference samples k from the Gaussian only,
  * rbmd/framework/model/RBEPSample.h:63-175). */
 RBMD_API rbmd_status rbmd_proposal_mlp_eval(const float* params, const float* x, const float* wbin,

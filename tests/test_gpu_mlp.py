@@ -1,5 +1,6 @@
 """The tcgen05 proposal network against its CPU restatement (oracle/mlp.py, FP64 with the same
-BF16 roundings): outputs h to 1e-3 of max|h|, group losses to 1e-4, and the parameter gradient
+BF16 roundings): outputs h to 1e-3 of max|h| (the tensor-core pass and the CUDA-core forward
+pass of the sampler), group losses to 1e-4, and the parameter gradient
 of the mean group loss to 2e-3 norm-wise (FP32 accumulation order and tanhf are the only
 differences)."""
 import ctypes
@@ -48,3 +49,8 @@ def test_mlp_forward_backward_matches_oracle(cuda, G, seed):
     # forward-only launch returns the same outputs
     h2, _, _ = _run(cuda, p, x, w, c, train=False)
     assert np.array_equal(h, h2)
+    # the sampler's per-step forward pass on the CUDA cores (train < 0): same roundings, other
+    # summation order
+    h3, _, _ = _run(cuda, p, x, w, c, train=-1)
+    assert np.abs(h3 - hr).max() <= 1e-3 * np.abs(hr).max()
+    assert np.abs(h3 - h).max() <= 1e-3 * np.abs(h).max()
