@@ -177,7 +177,9 @@ RBMD_API rbmd_status rbmd_force_set_ksamples(rbmd_force* f, const int32_t* m_xyz
  * counterpart (the reference samples only from the Gaussian, RBEPSample.h:63-175). */
 RBMD_API rbmd_status rbmd_force_set_kweights(rbmd_force* f, const double* w_host);
 
-/* Read the k-samples of the last compute (n_replicas*P*3 int32 into host memory). */
+/* Read the k-samples of the last compute (n_replicas*P*3 int32 into host memory).  After
+ * rbmd_force_step with the library's own sampler these are the samples drawn for the next step:
+ * each step's k-space chain draws the following step's set once its own forces are done. */
 RBMD_API rbmd_status rbmd_force_get_ksamples(rbmd_force* f, int32_t* m_xyz_host, int32_t P);
 
 /* Draw the k-samples for `step` with the on-device Metropolis-Hastings sampler (seeded
