@@ -75,6 +75,22 @@ __global__ void k_prop_features(int groups, const float* __restrict__ spec, floa
   prop_features(row % kPropBins, spec + (size_t)(row / kPropBins) * kPropBands, x + (size_t)row * kMlpIn);
 }
 
+// h of every (replica, bin) row under the replica's conditioning spectrum: the bin's inputs
+// (prop_features) and the network's forward pass on the CUDA cores (mlp_row_forward4, four lanes
+// per row, 128-thread blocks over several SMs).  The sampler's per-step evaluation: a tensor-core
+// launch with its 94 KB of shared memory and TMEM only finds an SM once one drains under the near
+// pass, and would open the k-space chain late.
+__global__ void __launch_bounds__(128) k_prop_h(int nrep, const float* __restrict__ mlp, const float* __restrict__ spec,
+                                               float* __restrict__ h) {
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int rows = nrep * kPropBins;
+  const int row = min(gt >> 2, rows - 1);   // every lane joins the shuffles
+  float x[kMlpIn];
+  prop_features(row % kPropBins, spec + (size_t)(row / kPropBins) * kPropBands, x);
+  const float v = mlp_row_forward4(mlp, x, gt & 3);
+  if ((gt >> 2) < rows && (gt & 3) == 0) h[row] = v;
+}
+
 // 53-bit uniform in (0, 1) from two 32-bit words
 __device__ __forceinline__ double u53(uint32_t a, uint32_t b) {
   return ((double)(((unsigned long long)a << 21) | (b >> 11)) + 0.5) * (1.0 / 9007199254740992.0);
@@ -99,16 +115,12 @@ __device__ __forceinline__ int cdf_search(const double* cdf, int n, double u) {
 // accepted with probability e^{h_b - h_max} (h clamped below at h_max - 8), so accepted samples
 // follow q; they are emitted in (round, thread) order, which makes the draw deterministic.
 // Weight w = Z / e^{h_b - h_max} with Z = sum_b W_b e^{h_b - h_max} (W_b = p-mass of bin b),
-// i.e. p / q.  With mlp (the network's parameters) the block first evaluates h itself from the
-// conditioning spectrum spec (bin features in shared memory, four lanes per bin through
-// mlp_row_forward4), so the sampler is one launch; otherwise h is read from h[], and h == nullptr
-// samples p itself with unit weights.  When max_rounds run out the remaining samples get weight 0
-// and RBMD_FLAG_SAMPLER is raised.
+// i.e. p / q.  h == nullptr samples p itself with unit weights.  When max_rounds run out the
+// remaining samples get weight 0 and RBMD_FLAG_SAMPLER is raised.
 constexpr int kSampThreads = 1024;
 __global__ void __launch_bounds__(kSampThreads) k_prop_sample(
     int nrep, const RepDev* __restrict__ reps, const PropRep* __restrict__ prep, const double* __restrict__ cdf,
-    const float* __restrict__ h, const float* __restrict__ mlp, const float* __restrict__ spec,
-    const double* __restrict__ wbin, unsigned long long seed, long long step_arg,
+    const float* __restrict__ h, const double* __restrict__ wbin, unsigned long long seed, long long step_arg,
     const long long* __restrict__ step_dev, int max_rounds, int* __restrict__ kvec_out, void* __restrict__ krec, int rec_bytes, int* __restrict__ krep,
     double* __restrict__ weights, uint32_t* status) {
   const int r = blockIdx.x;
@@ -126,18 +138,7 @@ __global__ void __launch_bounds__(kSampThreads) k_prop_sample(
   __shared__ double cdf_s[3 * (2 * kPropMaxM + 1)];
   const int n0 = 2 * pr.M[0] + 1, n1 = 2 * pr.M[1] + 1, n2 = 2 * pr.M[2] + 1;
   const bool staged = pr.M[0] <= kPropMaxM && pr.M[1] <= kPropMaxM && pr.M[2] <= kPropMaxM;
-  const bool learned = mlp != nullptr || h != nullptr;
-  if (mlp) {
-    // h of every bin: inputs in the CDF buffer (staged only afterwards), h into acc_s
-    static_assert(sizeof(cdf_s) >= sizeof(float) * kPropBins * kMlpIn, "bin inputs fit the CDF buffer");
-    float* xs = reinterpret_cast<float*>(cdf_s);
-    if (t < kPropBins) prop_features(t, spec + (size_t)r * kPropBands, xs + t * kMlpIn);
-    __syncthreads();
-    static_assert(kSampThreads == 4 * kPropBins, "four lanes per bin");
-    const float hb = mlp_row_forward4(mlp, xs + (t >> 2) * kMlpIn, t & 3);
-    if ((t & 3) == 0) acc_s[t >> 2] = hb;
-    __syncthreads();
-  }
+  const bool learned = h != nullptr;
   const double *c0 = cdf + pr.cdf_off[0], *c1 = cdf + pr.cdf_off[1], *c2 = cdf + pr.cdf_off[2];
   if (staged) {
     for (int i = t; i < n0; i += kSampThreads) cdf_s[i] = c0[i];
@@ -151,8 +152,7 @@ __global__ void __launch_bounds__(kSampThreads) k_prop_sample(
   // reductions over their 8 warps in a fixed order)
   constexpr int kBW = kPropBins / 32;
   const bool bin_t = t < kPropBins;
-  float hv = 0.f;
-  if (bin_t) hv = mlp ? acc_s[t] : (h ? h[(size_t)r * kPropBins + t] : 0.f);
+  const float hv = (h && bin_t) ? h[(size_t)r * kPropBins + t] : 0.f;
   float hmax = hv;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) hmax = fmaxf(hmax, __shfl_xor_sync(0xffffffffu, hmax, o));

@@ -107,7 +107,7 @@ struct rbmd_force {
   double* d_wbin = nullptr;         // [nrep][256] Gaussian mass per bin
   std::vector<double> wbin_h;
   double* d_pw = nullptr;           // [Ptot] importance weights of the drawn samples
-  float *d_mlp = nullptr, *d_spec = nullptr;
+  float *d_mlp = nullptr, *d_h = nullptr, *d_spec = nullptr;
   int* d_spec_init = nullptr;
   int P = 100, kmax = 2;
   unsigned long long seed = 20240101ull;
@@ -378,7 +378,7 @@ void free_all(rbmd_force* f) {
   f->d_frac = nullptr;
   dfree(f->d_meta); dfree(f->d_nbr); dfree(f->d_count); dfree(f->d_maxcount); dfree(f->d_status);
   dfree(f->d_count2); dfree(f->d_mean_partial); dfree(f->d_erf_tab);
-  dfree(f->d_prep); dfree(f->d_cdf); dfree(f->d_wbin); dfree(f->d_pw); dfree(f->d_mlp);
+  dfree(f->d_prep); dfree(f->d_cdf); dfree(f->d_wbin); dfree(f->d_pw); dfree(f->d_mlp); dfree(f->d_h);
   dfree(f->d_spec); dfree(f->d_spec_init);
   dfree(f->d_rebuild); dfree(f->d_block_sums); dfree(f->d_cell_rep); dfree(f->d_xref); dfree(f->d_nbuilds);
   dfree(f->d_segs);
@@ -578,6 +578,7 @@ rbmd_status build_proposal_tables(rbmd_force* f, const std::vector<int64_t>& qof
   CK(dalloc(&f->d_pw, (size_t)f->Ptot));
   CK(dalloc(&f->d_mlp, (size_t)kMlpNParam));
   CK(cudaMemset(f->d_mlp, 0, sizeof(float) * kMlpNParam));
+  CK(dalloc(&f->d_h, (size_t)nrep * kPropBins));
   CK(dalloc(&f->d_spec, (size_t)nrep * kPropBands));
   CK(cudaMemset(f->d_spec, 0, sizeof(float) * nrep * kPropBands));
   CK(dalloc(&f->d_spec_init, (size_t)nrep));
@@ -824,10 +825,15 @@ void launch_sort(rbmd_force* f, cudaStream_t s, bool bin, bool regather) {
 // sampler draws from q = p e^h / Z with weights p / q; otherwise it draws from p.
 void launch_prop_sample(rbmd_force* f, cudaStream_t s, long long step, int rec_bytes,
                         const long long* step_dev = nullptr) {
-  const float* mlp = f->proposal == "learned" && f->prop_trained ? f->d_mlp : nullptr;
-  k_prop_sample<<<f->nrep, kSampThreads, 0, s>>>(f->nrep, f->d_reps, f->d_prep, f->d_cdf, nullptr, mlp, f->d_spec,
-                                                 f->d_wbin, f->seed, step, step_dev, 4096, f->d_kvec, f->d_krec,
-                                                 rec_bytes, f->d_krep, f->d_pw, f->d_status);
+  const float* h = nullptr;
+  if (f->proposal == "learned" && f->prop_trained) {
+    k_prop_h<<<(4 * f->nrep * kPropBins + 127) / 128, 128, 0, s>>>(f->nrep, f->d_mlp, f->d_spec, f->d_h);
+    h = f->d_h;
+    f->launches++;
+  }
+  k_prop_sample<<<f->nrep, kSampThreads, 0, s>>>(f->nrep, f->d_reps, f->d_prep, f->d_cdf, h, f->d_wbin, f->seed,
+                                                 step, step_dev, 4096, f->d_kvec, f->d_krec, rec_bytes, f->d_krep,
+                                                 f->d_pw, f->d_status);
   f->launches++;
 }
 
@@ -2816,7 +2822,7 @@ rbmd_status rbmd_force_train_proposal(rbmd_force* f, const rbmd_train_opts* o, r
     }
     k_frac<float><<<(nq0 + 255) / 256, 256, 0, s>>>(nq0, f->d_qidx, f->at.pos, f->at.charge, rep_of, f->d_reps,
                                                      frac);
-    k_prop_sample<<<1, kSampThreads, 0, s>>>(1, rep1, f->d_prep, f->d_cdf, nullptr, nullptr, nullptr, f->d_wbin, o->seed,
+    k_prop_sample<<<1, kSampThreads, 0, s>>>(1, rep1, f->d_prep, f->d_cdf, nullptr, f->d_wbin, o->seed,
                                     (1LL << 40) + sn, nullptr, 4096, kv, krec, 12, krep, kw, f->d_status);
     const dim3 grid((K + 255) / 256, nch);
     for (int pass = 0; pass < 2; ++pass) {
