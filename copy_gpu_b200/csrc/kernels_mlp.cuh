@@ -373,14 +373,14 @@ done:
 }
 
 // Sum of the per-group gradients in group order (deterministic), one thread per parameter.
-// Forward pass alone on the CUDA cores (mlp_row_forward4), four lanes per row: the entry point's
-// train < 0 evaluation, the same arithmetic as the sampler's per-step evaluation in k_prop_sample.
-__global__ void __launch_bounds__(128) k_mlp_infer(int rows, const float* __restrict__ P,
+// Forward pass alone on the CUDA cores (mlp_row_forward, kMlpLanes lanes per row): the entry
+// point's train < 0 evaluation, the same arithmetic as the sampler's per-step evaluation k_prop_h.
+__global__ void __launch_bounds__(256) k_mlp_infer(int rows, const float* __restrict__ P,
                                                   const float* __restrict__ x, float* __restrict__ h) {
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-  const int row = gt >> 2, part = gt & 3;
+  const int row = gt / kMlpLanes, part = gt % kMlpLanes;
   const int r = row < rows ? row : rows - 1;   // every lane joins the shuffles
-  const float v = mlp_row_forward4(P, x + (size_t)r * kMlpIn, part);
+  const float v = mlp_row_forward<kMlpLanes>(P, x + (size_t)r * kMlpIn, part);
   if (row < rows && part == 0) h[row] = v;
 }
 

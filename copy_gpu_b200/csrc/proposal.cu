@@ -28,7 +28,7 @@ cudaError_t mlp_launch(const MlpArgs& a, cudaStream_t s) {
 
 cudaError_t mlp_infer(int groups, const float* params, const float* x, float* h, cudaStream_t s) {
   const int rows = groups * kMlpRows;
-  k_mlp_infer<<<(4 * rows + 127) / 128, 128, 0, s>>>(rows, params, x, h);
+  k_mlp_infer<<<(kMlpLanes * rows + 255) / 256, 256, 0, s>>>(rows, params, x, h);
   return cudaGetLastError();
 }
 

@@ -827,7 +827,7 @@ void launch_prop_sample(rbmd_force* f, cudaStream_t s, long long step, int rec_b
                         const long long* step_dev = nullptr) {
   const float* h = nullptr;
   if (f->proposal == "learned" && f->prop_trained) {
-    k_prop_h<<<(4 * f->nrep * kPropBins + 127) / 128, 128, 0, s>>>(f->nrep, f->d_mlp, f->d_spec, f->d_h);
+    k_prop_h<<<(kMlpLanes * f->nrep * kPropBins + 255) / 256, 256, 0, s>>>(f->nrep, f->d_mlp, f->d_spec, f->d_h);
     h = f->d_h;
     f->launches++;
   }
