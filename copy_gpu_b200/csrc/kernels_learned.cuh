@@ -77,17 +77,17 @@ __global__ void k_prop_features(int groups, const float* __restrict__ spec, floa
 
 // h of every (replica, bin) row under the replica's conditioning spectrum: the bin's inputs
 // (prop_features) and the network's forward pass on the CUDA cores (mlp_row_forward, kMlpLanes
-// lanes per row, 256-thread blocks over several SMs).  The sampler's per-step evaluation: a
+// lanes per row, 256-thread blocks over several SMs; mlp_t = the prepared weights, k_mlp_prep).  The sampler's per-step evaluation: a
 // tensor-core launch with its 94 KB of shared memory and TMEM only finds an SM once one drains
 // under the near pass, and would open the k-space chain late.
-__global__ void __launch_bounds__(256) k_prop_h(int nrep, const float* __restrict__ mlp, const float* __restrict__ spec,
-                                               float* __restrict__ h) {
+__global__ void __launch_bounds__(256) k_prop_h(int nrep, const float* __restrict__ mlp_t,
+                                               const float* __restrict__ spec, float* __restrict__ h) {
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int rows = nrep * kPropBins;
   const int row = min(gt / kMlpLanes, rows - 1);   // every lane joins the shuffles
   float x[kMlpIn];
   prop_features(row % kPropBins, spec + (size_t)(row / kPropBins) * kPropBands, x);
-  const float v = mlp_row_forward<kMlpLanes>(mlp, x, gt % kMlpLanes);
+  const float v = mlp_row_forward<kMlpLanes>(mlp_t, x, gt % kMlpLanes);
   if (gt / kMlpLanes < rows && gt % kMlpLanes == 0) h[row] = v;
 }
 

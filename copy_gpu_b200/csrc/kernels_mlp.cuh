@@ -373,14 +373,30 @@ done:
 }
 
 // Sum of the per-group gradients in group order (deterministic), one thread per parameter.
-// Forward pass alone on the CUDA cores (mlp_row_forward, kMlpLanes lanes per row): the entry
-// point's train < 0 evaluation, the same arithmetic as the sampler's per-step evaluation k_prop_h.
-__global__ void __launch_bounds__(256) k_mlp_infer(int rows, const float* __restrict__ P,
+// T from the parameter vector P (layout in mlp_forward.cuh), one thread per word
+__global__ void k_mlp_prep(const float* __restrict__ P, float* __restrict__ T) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= kMlpNParam) return;
+  if (e >= kTW1 && e < kTW1 + kMlpHid * kMlpIn) {          // T[kTW1 + f * 64 + j] = W1[j][f]
+    const int k = e - kTW1, f = k / kMlpHid, j = k % kMlpHid;
+    T[e] = mlp_bf16(P[kOW1 + j * kMlpIn + f]);
+  } else if (e >= kTW2 && e < kTW2 + kMlpHid * kMlpHid) {   // T[kTW2 + i * 64 + j] = W2[j][i]
+    const int k = e - kTW2, i = k / kMlpHid, j = k % kMlpHid;
+    T[e] = mlp_bf16(P[kOW2 + j * kMlpHid + i]);
+  } else {
+    T[e] = P[e];
+  }
+}
+
+// Forward pass alone on the CUDA cores (mlp_row_forward, kMlpLanes lanes per row, prepared weights
+// T): the entry point's train < 0 evaluation, the same arithmetic as the sampler's per-step
+// evaluation k_prop_h.
+__global__ void __launch_bounds__(256) k_mlp_infer(int rows, const float* __restrict__ T,
                                                   const float* __restrict__ x, float* __restrict__ h) {
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int row = gt / kMlpLanes, part = gt % kMlpLanes;
   const int r = row < rows ? row : rows - 1;   // every lane joins the shuffles
-  const float v = mlp_row_forward<kMlpLanes>(P, x + (size_t)r * kMlpIn, part);
+  const float v = mlp_row_forward<kMlpLanes>(T, x + (size_t)r * kMlpIn, part);
   if (row < rows && part == 0) h[row] = v;
 }
 

@@ -26,9 +26,14 @@ cudaError_t mlp_launch(const MlpArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t mlp_infer(int groups, const float* params, const float* x, float* h, cudaStream_t s) {
+cudaError_t mlp_prepare(const float* params, float* prepared, cudaStream_t s) {
+  k_mlp_prep<<<(kMlpNParam + 255) / 256, 256, 0, s>>>(params, prepared);
+  return cudaGetLastError();
+}
+
+cudaError_t mlp_infer(int groups, const float* prepared, const float* x, float* h, cudaStream_t s) {
   const int rows = groups * kMlpRows;
-  k_mlp_infer<<<(kMlpLanes * rows + 255) / 256, 256, 0, s>>>(rows, params, x, h);
+  k_mlp_infer<<<(kMlpLanes * rows + 255) / 256, 256, 0, s>>>(rows, prepared, x, h);
   return cudaGetLastError();
 }
 
@@ -55,8 +60,12 @@ RBMD_API rbmd_status rbmd_proposal_mlp_eval(const float* params, const float* x,
     return RBMD_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   if (train < 0) {   // the sampler's per-step forward pass on the CUDA cores
-    cudaError_t e = mlp_infer(groups, params, x, h, s);
+    float* prepared = nullptr;
+    if (cudaMalloc(&prepared, sizeof(float) * kMlpNParam) != cudaSuccess) return RBMD_ERR_CUDA;
+    cudaError_t e = mlp_prepare(params, prepared, s);
+    if (e == cudaSuccess) e = mlp_infer(groups, prepared, x, h, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(prepared);
     if (e != cudaSuccess) {
       std::snprintf(rbmd_internal::g_last_error, sizeof rbmd_internal::g_last_error, "mlp_eval: %s",
                     cudaGetErrorString(e));

@@ -107,7 +107,7 @@ struct rbmd_force {
   double* d_wbin = nullptr;         // [nrep][256] Gaussian mass per bin
   std::vector<double> wbin_h;
   double* d_pw = nullptr;           // [Ptot] importance weights of the drawn samples
-  float *d_mlp = nullptr, *d_h = nullptr, *d_spec = nullptr;
+  float *d_mlp = nullptr, *d_mlp_t = nullptr, *d_h = nullptr, *d_spec = nullptr;   // d_mlp_t: k_mlp_prep layout
   int* d_spec_init = nullptr;
   int P = 100, kmax = 2;
   unsigned long long seed = 20240101ull;
@@ -378,7 +378,7 @@ void free_all(rbmd_force* f) {
   f->d_frac = nullptr;
   dfree(f->d_meta); dfree(f->d_nbr); dfree(f->d_count); dfree(f->d_maxcount); dfree(f->d_status);
   dfree(f->d_count2); dfree(f->d_mean_partial); dfree(f->d_erf_tab);
-  dfree(f->d_prep); dfree(f->d_cdf); dfree(f->d_wbin); dfree(f->d_pw); dfree(f->d_mlp); dfree(f->d_h);
+  dfree(f->d_prep); dfree(f->d_cdf); dfree(f->d_wbin); dfree(f->d_pw); dfree(f->d_mlp); dfree(f->d_mlp_t); dfree(f->d_h);
   dfree(f->d_spec); dfree(f->d_spec_init);
   dfree(f->d_rebuild); dfree(f->d_block_sums); dfree(f->d_cell_rep); dfree(f->d_xref); dfree(f->d_nbuilds);
   dfree(f->d_segs);
@@ -577,6 +577,7 @@ rbmd_status build_proposal_tables(rbmd_force* f, const std::vector<int64_t>& qof
   CK(cudaMemcpy(f->d_wbin, f->wbin_h.data(), sizeof(double) * f->wbin_h.size(), cudaMemcpyHostToDevice));
   CK(dalloc(&f->d_pw, (size_t)f->Ptot));
   CK(dalloc(&f->d_mlp, (size_t)kMlpNParam));
+  CK(dalloc(&f->d_mlp_t, (size_t)kMlpNParam));
   CK(cudaMemset(f->d_mlp, 0, sizeof(float) * kMlpNParam));
   CK(dalloc(&f->d_h, (size_t)nrep * kPropBins));
   CK(dalloc(&f->d_spec, (size_t)nrep * kPropBands));
@@ -692,6 +693,7 @@ rbmd_status train_fit(rbmd_force* f, const rbmd_train_opts* o, rbmd_train_report
   CK(cudaMemcpy(f->d_spec, spec_all.data(), sizeof(float) * spec_all.size(), cudaMemcpyHostToDevice));
   std::vector<int> ones(f->nrep, 1);
   CK(cudaMemcpy(f->d_spec_init, ones.data(), sizeof(int) * f->nrep, cudaMemcpyHostToDevice));
+  CK(mlp_prepare(f->d_mlp, f->d_mlp_t, s));
   f->prop_trained = true;
   f->presampled = false;
   if (rep) {
@@ -827,7 +829,7 @@ void launch_prop_sample(rbmd_force* f, cudaStream_t s, long long step, int rec_b
                         const long long* step_dev = nullptr) {
   const float* h = nullptr;
   if (f->proposal == "learned" && f->prop_trained) {
-    k_prop_h<<<(kMlpLanes * f->nrep * kPropBins + 255) / 256, 256, 0, s>>>(f->nrep, f->d_mlp, f->d_spec, f->d_h);
+    k_prop_h<<<(kMlpLanes * f->nrep * kPropBins + 255) / 256, 256, 0, s>>>(f->nrep, f->d_mlp_t, f->d_spec, f->d_h);
     h = f->d_h;
     f->launches++;
   }
@@ -2842,8 +2844,10 @@ rbmd_status rbmd_force_proposal_params(rbmd_force* f, float* get_host, const flo
   if (!f->bound || !f->d_mlp) return RBMD_ERR_STATE;
   if (set_host) {
     CK(cudaMemcpy(f->d_mlp, set_host, sizeof(float) * kMlpNParam, cudaMemcpyHostToDevice));
+    CK(mlp_prepare(f->d_mlp, f->d_mlp_t, nullptr));
+    CK(cudaDeviceSynchronize());
     f->prop_trained = true;
-  f->presampled = false;
+    f->presampled = false;
   }
   if (get_host) CK(cudaMemcpy(get_host, f->d_mlp, sizeof(float) * kMlpNParam, cudaMemcpyDeviceToHost));
   return RBMD_OK;
