@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <mutex>
+#include <set>
 
 #include "../../include/rbmd_force.h"
 #include "kernels_mlp.cuh"
@@ -15,12 +17,20 @@ extern char g_last_error[512];
 namespace rbmd {
 
 cudaError_t mlp_launch(const MlpArgs& a, cudaStream_t s) {
-  static bool attr_set = false;
+  // the shared-memory limit is a per-device attribute of the kernel: set once on each device
+  static std::mutex mu;
+  static std::set<int> devices_set;
   const size_t smem = sizeof(MlpSmem) + 1024;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(k_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    attr_set = true;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (!devices_set.count(dev)) {
+      e = cudaFuncSetAttribute(k_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      devices_set.insert(dev);
+    }
   }
   k_mlp<<<a.groups, 256, smem, s>>>(a);
   return cudaGetLastError();
