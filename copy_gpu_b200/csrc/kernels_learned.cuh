@@ -32,6 +32,13 @@ struct PropRep {
   int pad;
 };
 
+// shared memory of k_prop_sample for a replica: its three CDF tables when they are staged
+// (|m_d| <= kPropMaxM), else none
+__host__ __device__ __forceinline__ int prop_stage_doubles(const PropRep& pr) {
+  if (pr.M[0] > kPropMaxM || pr.M[1] > kPropMaxM || pr.M[2] > kPropMaxM) return 0;
+  return (2 * pr.M[0] + 1) + (2 * pr.M[1] + 1) + (2 * pr.M[2] + 1);
+}
+
 // |k| bin of an integer vector; identical arithmetic on host and device (no contraction)
 __host__ __device__ __forceinline__ double prop_kappa(const PropRep& pr, int mx, int my, int mz) {
 #ifdef __CUDA_ARCH__
@@ -135,7 +142,9 @@ __global__ void __launch_bounds__(kSampThreads) k_prop_sample(
   __shared__ double zsum;
   __shared__ int wcount[kW];
   __shared__ int total;
-  __shared__ double cdf_s[3 * (2 * kPropMaxM + 1)];
+  // the three per-axis CDF tables, sized by the launch (prop_stage_bytes) for the largest
+  // staged replica, so that the block asks for no more shared memory than it uses
+  extern __shared__ double cdf_s[];
   const int n0 = 2 * pr.M[0] + 1, n1 = 2 * pr.M[1] + 1, n2 = 2 * pr.M[2] + 1;
   const bool staged = pr.M[0] <= kPropMaxM && pr.M[1] <= kPropMaxM && pr.M[2] <= kPropMaxM;
   const bool learned = h != nullptr;
@@ -235,7 +244,8 @@ __global__ void __launch_bounds__(kSampThreads) k_prop_sample(
 // importance-weighted mean of |rho_k|^2 / N_q over this step's samples in band j (weights w make
 // it an estimate of the p-average, the quantity the training data record), folded into an
 // exponential moving average of its logarithm (rate beta; the first update replaces).  Thread t
-// accumulates samples t, t + 256, ...; the per-band partials are summed in thread order.
+// accumulates samples t, t + 256, ...; the per-band partials are summed in a fixed order (warp
+// butterflies, then the warps in order).
 __global__ void __launch_bounds__(256) k_prop_spectrum(int nrep, const RepDev* __restrict__ reps,
                                                        const PropRep* __restrict__ prep,
                                                        const int* __restrict__ kvec, const double2* __restrict__ rho,
@@ -245,7 +255,7 @@ __global__ void __launch_bounds__(256) k_prop_spectrum(int nrep, const RepDev* _
   if (r >= nrep) return;
   const PropRep pr = prep[r];
   const int P = reps[r].P, kb = reps[r].k_begin;
-  __shared__ double sw_s[kPropBands][256], ss_s[kPropBands][256];
+  __shared__ double wsw[8][kPropBands], wss[8][kPropBands];   // per-warp band sums
   double sw[kPropBands], ss[kPropBands];
 #pragma unroll
   for (int j = 0; j < kPropBands; ++j) sw[j] = ss[j] = 0.0;
@@ -261,17 +271,26 @@ __global__ void __launch_bounds__(256) k_prop_spectrum(int nrep, const RepDev* _
         ss[b] += w * (z.x * z.x + z.y * z.y);
       }
   }
+  // fixed-order reduction: a butterfly within each warp, then the 8 warp sums in warp order
 #pragma unroll
-  for (int j = 0; j < kPropBands; ++j) {
-    sw_s[j][t] = sw[j];
-    ss_s[j][t] = ss[j];
-  }
+  for (int j = 0; j < kPropBands; ++j)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      sw[j] += __shfl_xor_sync(0xffffffffu, sw[j], o);
+      ss[j] += __shfl_xor_sync(0xffffffffu, ss[j], o);
+    }
+  if ((t & 31) == 0)
+#pragma unroll
+    for (int j = 0; j < kPropBands; ++j) {
+      wsw[t >> 5][j] = sw[j];
+      wss[t >> 5][j] = ss[j];
+    }
   __syncthreads();
   if (t < kPropBands) {
     double a = 0, b = 0;
-    for (int k = 0; k < 256; ++k) {
-      a += sw_s[t][k];
-      b += ss_s[t][k];
+    for (int k = 0; k < 8; ++k) {
+      a += wsw[k][t];
+      b += wss[k][t];
     }
     if (a > 0 && pr.nq > 0) {
       const float v = (float)log(fmax(b / (a * (double)pr.nq), 1e-6));

@@ -104,6 +104,7 @@ struct rbmd_force {
   std::string proposal = "gauss";
   bool prop_trained = false;
   PropRep* d_prep = nullptr;
+  int prop_stage_bytes = 0;            // shared memory of k_prop_sample (largest replica's CDFs)
   std::vector<PropRep> prep_h;
   double* d_cdf = nullptr;
   double* d_wbin = nullptr;         // [nrep][256] Gaussian mass per bin
@@ -591,6 +592,9 @@ rbmd_status build_proposal_tables(rbmd_force* f, const std::vector<int64_t>& qof
       }
     for (int k = 0; k < kPropBins; ++k) W[k] /= Z;
   }
+  f->prop_stage_bytes = 0;
+  for (const PropRep& pr : f->prep_h)
+    f->prop_stage_bytes = std::max(f->prop_stage_bytes, (int)sizeof(double) * prop_stage_doubles(pr));
   CK(dalloc(&f->d_prep, (size_t)nrep));
   CK(cudaMemcpy(f->d_prep, f->prep_h.data(), sizeof(PropRep) * nrep, cudaMemcpyHostToDevice));
   CK(dalloc(&f->d_cdf, cdf.size()));
@@ -856,7 +860,7 @@ void launch_prop_sample(rbmd_force* f, cudaStream_t s, long long step, int rec_b
     h = f->d_h;
     f->launches++;
   }
-  k_prop_sample<<<f->nrep, kSampThreads, 0, s>>>(f->nrep, f->d_reps, f->d_prep, f->d_cdf, h, f->d_wbin, f->seed,
+  k_prop_sample<<<f->nrep, kSampThreads, f->prop_stage_bytes, s>>>(f->nrep, f->d_reps, f->d_prep, f->d_cdf, h, f->d_wbin, f->seed,
                                                  step, step_dev, 4096, f->d_kvec, f->d_krec, rec_bytes, f->d_krep,
                                                  f->d_pw, f->d_status);
   f->launches++;
@@ -2848,7 +2852,7 @@ rbmd_status rbmd_force_train_proposal(rbmd_force* f, const rbmd_train_opts* o, r
     }
     k_frac<float><<<(nq0 + 255) / 256, 256, 0, s>>>(nq0, f->d_qidx, f->at.pos, f->at.charge, rep_of, f->d_reps,
                                                      frac);
-    k_prop_sample<<<1, kSampThreads, 0, s>>>(1, rep1, f->d_prep, f->d_cdf, nullptr, f->d_wbin, o->seed,
+    k_prop_sample<<<1, kSampThreads, f->prop_stage_bytes, s>>>(1, rep1, f->d_prep, f->d_cdf, nullptr, f->d_wbin, o->seed,
                                     (1LL << 40) + sn, nullptr, 4096, kv, krec, 12, krep, kw, f->d_status);
     const dim3 grid((K + 255) / 256, nch);
     for (int pass = 0; pass < 2; ++pass) {
